@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Laplace3D FMM matvec throughput on B200 (one JSON line on stdout).
+
+Workload (the metric's configuration): SphericalHarmonics(Laplace3D(); p=10), ppl=64,
+1,000,000 points uniform in the unit cube (seed 3), FP64 charges N(0,1), potential and
+gradient at the sources. A step is one matvec = build_expansions + evaluate_at_sources
+(the reference's definition, bench/bench.jl:44-50), the tree/plan built once beforehand.
+
+  value      evaluations/s of the mixed path (tensor-core TF32x3 M2L, FP32 compensated P2P),
+             inputs resident in HBM, device time (CUDA events on the library's stream), L2
+             flushed (256 MB write) between steps, max over ranks
+  e2e        the same through the host-pointer C ABI call (fmmb_matvec) with pinned host
+             buffers: copies in and out inside the timed region
+  fp64       the plain FP64 path on the same inputs; mixed_vs_fp64 = the ratio
+  error      relative L2 error of both paths against FP64 direct sums at 4096 sampled
+             sources (computed on the device, fmmb_direct_dev)
+  roofline   the dominant kernel of the mixed path (the M2L) against the measured peak
+  cpu_baseline  the CPU oracle (C++ restatement of the reference CPU path) on this host
+
+--impl reference times that CPU path alone (all host threads) as the reference arm.
+--gpus N: N independent replicas (the single FMM is not sharded: replicas only), one
+process per GPU under torch.distributed; value = N·1e6 / max-over-ranks step time.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "flexiblefmm.jl_b200"))
+
+METRIC = "Laplace3D 1M-pt FMM evals/s @1e-6 err, mixed vs FP64 GPU; p50/p99 latency"
+UNIT = "evals/s"
+
+
+def args_():
+    a = argparse.ArgumentParser()
+    a.add_argument("--gpus", type=int, default=1)
+    a.add_argument("--steps", type=int, default=10)
+    a.add_argument("--warmup", type=int, default=3)
+    a.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    a.add_argument("--n", type=int, default=1_000_000)
+    a.add_argument("--p", type=int, default=10)
+    a.add_argument("--ppl", type=int, default=64)
+    a.add_argument("--samples", type=int, default=4096)
+    a.add_argument("--no-cpu-baseline", action="store_true")
+    return a.parse_args()
+
+
+def workload(n, seed=3):
+    rng = np.random.default_rng(seed)
+    pts = rng.random((n, 3))
+    tau = rng.standard_normal(n)
+    return pts, tau
+
+
+def config(a, extra=None):
+    c = {"workload": f"Laplace3D SphericalHarmonics p={a.p}, ppl={a.ppl}, {a.n:,} points uniform in the unit cube "
+                     f"(seed 3), charges N(0,1), potential+gradient at the sources; step = build_expansions + "
+                     f"evaluate_at_sources", "n_points": a.n, "p": a.p, "ppl": a.ppl,
+         "l2": "flushed between steps (256 MB device write)", "parallelism": f"replicas{a.gpus}"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------- the CPU oracle (baseline / reference arm)
+def cpu_oracle(pts, tau, p, ppl, reps, warmup=1):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    threads = oracle.set_threads(0)
+    t0 = time.perf_counter()
+    f = oracle.FMM(p, pts, ppl)
+    t_tree = time.perf_counter() - t0
+    times = []
+    for r in range(warmup + reps):
+        t0 = time.perf_counter()
+        f.build_expansions(pts, tau)
+        f.evaluate_at_sources()
+        dt = time.perf_counter() - t0
+        if r >= warmup:
+            times.append(dt)
+    return dict(times=times, threads=threads, tree_s=t_tree)
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    pts, tau = workload(a.n)
+    r = cpu_oracle(pts, tau, a.p, a.ppl, reps=a.steps, warmup=a.warmup)
+    ms = 1e3 * statistics.mean(r["times"])
+    v = a.n / (ms / 1e3)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": config(a, {"precision": "fp64 (the reference CPU path restated in C++/OpenMP)"}),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["threads"], "kind": "port",
+                             "sample": f"full {a.n:,}-point matvec per step, mean of {a.steps} after {a.warmup} warm-up; "
+                                       f"tree + operators {r['tree_s']:.2f} s untimed"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- clocks during the timed region
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                                       "-i", str(device)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        rows = [r.split(", ") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(a):
+    import torch
+    import fmmb
+
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    L = fmmb.lib()
+    ctx = fmmb.default_context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    pts, tau = workload(a.n)
+    m = fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=a.p)
+    t0 = time.perf_counter()
+    f = fmmb.FMM(m, pts, ppl=a.ppl, bbox=((0.0, 0.0, 0.0), 1.0))
+    plan_s = time.perf_counter() - t0
+    xyz_d = torch.from_numpy(pts).cuda()
+    tau_d = torch.from_numpy(tau).cuda()
+    pot_d = torch.zeros(a.n, dtype=torch.float64, device="cuda")
+    grad_d = torch.zeros((a.n, 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    P = lambda t: C.c_void_p(t.data_ptr())
+    states = {"mixed": fmmb.FMMState(f, "mixed"), "fp64": fmmb.FMMState(f, "fp64")}
+
+    def step(st):
+        rc = L.fmmb_matvec_dev(st._h, P(xyz_d), P(tau_d), a.n, 3, P(pot_d), P(grad_d))
+        if rc:
+            fmmb._check(rc)
+
+    def timed(st, k):
+        times = []
+        for _ in range(k):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step(st)
+                e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+        return [e0.elapsed_time(e1) for e0, e1 in times]
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for name in ("mixed", "fp64"):
+        for _ in range(a.warmup):
+            step(states[name])
+    torch.cuda.synchronize()
+    clocks = Clocks(local) if rank == 0 else None
+    barrier()
+    t_mixed = timed(states["mixed"], a.steps)
+    barrier()
+    clk = clocks.stop() if clocks else None
+    t_fp64 = timed(states["fp64"], a.steps)
+    barrier()
+    ms_mixed = max_over_ranks(statistics.mean(t_mixed))
+    ms_fp64 = max_over_ranks(statistics.mean(t_fp64))
+
+    # accuracy: both paths against FP64 direct sums at sampled sources (device)
+    rng = np.random.default_rng(7)
+    sel = np.sort(rng.choice(a.n, size=min(a.samples, a.n), replace=False)).astype(np.int64)
+    sel_d = torch.from_numpy(sel).cuda()
+    tg_d = xyz_d[sel_d].contiguous()
+    dp = torch.zeros(len(sel), dtype=torch.float64, device="cuda")
+    dg = torch.zeros((len(sel), 3), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    fmmb._check(L.fmmb_direct_dev(ctx._h, P(xyz_d), P(tau_d), a.n, P(tg_d), P(sel_d), len(sel), P(dp), P(dg)))
+    dp_h, dg_h = dp.cpu().numpy(), dg.cpu().numpy()
+    err = {}
+    for name in ("mixed", "fp64"):
+        step(states[name])
+        torch.cuda.synchronize()
+        u = pot_d.cpu().numpy()[sel]
+        g = grad_d.cpu().numpy()[sel]
+        err[name] = {"pot_rel_l2": float(np.linalg.norm(u - dp_h) / np.linalg.norm(dp_h)),
+                     "grad_rel_l2": float(np.linalg.norm(g - dg_h) / np.linalg.norm(dg_h))}
+
+    # stage times of one matvec per path (median of 3) and the launches per step
+    stages, launches = {}, {}
+    names = ("gather", "p2m", "m2m", "m2l", "l2l", "eval")
+    for name in ("mixed", "fp64"):
+        runs = []
+        for _ in range(3):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            ms = (C.c_double * 6)()
+            nl = C.c_int()
+            fmmb._check(L.fmmb_profile_matvec(states[name]._h, P(xyz_d), P(tau_d), a.n, 3, P(pot_d), P(grad_d), ms, 6,
+                                               C.byref(nl)))
+            runs.append(list(ms))
+            launches[name] = nl.value
+        stages[name] = {k: statistics.median(r[i] for r in runs) for i, k in enumerate(names)}
+
+    # end to end through the host-pointer C ABI call, pinned buffers
+    xyz_h = torch.from_numpy(pts).pin_memory()
+    tau_h = torch.from_numpy(tau).pin_memory()
+    pot_h = torch.zeros(a.n, dtype=torch.float64).pin_memory()
+    grad_h = torch.zeros((a.n, 3), dtype=torch.float64).pin_memory()
+    st = states["mixed"]
+    for _ in range(a.warmup):
+        fmmb._check(L.fmmb_matvec(st._h, P(xyz_h), P(tau_h), a.n, 3, P(pot_h), P(grad_h)))
+    e2e = []
+    for _ in range(a.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fmmb._check(L.fmmb_matvec(st._h, P(xyz_h), P(tau_h), a.n, 3, P(pot_h), P(grad_h)))
+        e2e.append(time.perf_counter() - t0)
+    barrier()
+    e2e_s = max_over_ranks(statistics.mean(e2e))
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+    np_ = (a.p + 1) ** 2
+    m2l_flops = 2.0 * f.npairs * np_ * np_                    # the algorithmic FP64-equivalent M2L work
+    t_m2l = stages["mixed"]["m2l"] / 1e3
+    achieved = m2l_flops / t_m2l / 1e12
+    peak = peaks.get("bf16_tflops", 1590.0)
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "m2l_traffic.json")
+    if os.path.exists(tp):
+        tj = json.load(open(tp))
+        traffic = tj.get("dram_bytes_per_launch_full") or tj.get("dram_bytes_per_launch")
+    lat = sorted(t_mixed)
+    pct = lambda q: lat[min(len(lat) - 1, int(round(q * (len(lat) - 1))))]
+    cpu = None
+    if world == 1 and not a.no_cpu_baseline:
+        r = cpu_oracle(pts, tau, a.p, a.ppl, reps=2, warmup=1)
+        cpu = {"value": a.n / min(r["times"]), "unit": UNIT, "cores": r["threads"], "kind": "port",
+               "sample": f"full {a.n:,}-point matvec (the same points and charges), best of 2 after 1 warm-up, "
+                         f"tree + operators {r['tree_s']:.2f} s untimed"}
+    line = {
+        "metric": METRIC, "value": world * a.n / (ms_mixed / 1e3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "tf32x3 M2L + f32 P2P, f64 elsewhere", "data": "synthetic (seeded uniform points, N(0,1) charges)",
+        "config": config(a, {"precision": "mixed", "plan_s": plan_s, "levels": f.nlevels, "nodes": f.nnodes,
+                             "far_pairs": f.npairs}),
+        "latency_ms": {"p50": pct(0.5), "p99": pct(0.99)},
+        "fp64": {"value": world * a.n / (ms_fp64 / 1e3), "ms_per_step": ms_fp64},
+        "mixed_vs_fp64": ms_fp64 / ms_mixed,
+        "error": {"samples": len(sel), **{k: v for k, v in err.items()}},
+        "stages_ms": stages,
+        "roofline": {"bound": "tensor", "kernel": "k_m2l_tc (M2L, all levels, one launch)", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if "bf16_tflops" in peaks else "fallback",
+                     "work": f"{f.npairs:,} far pairs x 2 x {np_}^2 flop"},
+        "e2e": {"value": world * a.n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": a.n * 32, "d2h_bytes_per_step": a.n * 32},
+        "gpu_launches": launches["mixed"] * a.steps,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    del states, f
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,580 @@
+// The C ABI of fmmb (include/fmmb.h): handles, validation with the reference's error
+// semantics, host↔device staging, and the order of the passes.
+#include <cstring>
+
+#include "passes.cuh"
+
+using namespace fmmb;
+
+struct fmmb_ctx { Ctx c; };
+struct fmmb_cache { Cache c; };
+struct fmmb_plan { Plan p; };
+struct fmmb_state { State s; };
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return FMMB_OK;
+  } catch (const Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return FMMB_ERR_MEMORY;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return FMMB_ERR_DEVICE;
+  }
+}
+
+void set_device(const Ctx& c) { FMMB_CUDA(cudaSetDevice(c.device)); }
+
+// square_bbox (src/tree/tree.jl:97-114) from the points' bounds
+void square_bbox(const double lo[3], const double hi[3], double origin[3], double& W0) {
+  W0 = 0;
+  for (int d = 0; d < 3; ++d) W0 = std::max(W0, hi[d] - lo[d]);
+  require(std::isfinite(W0), FMMB_ERR_ARGUMENT, "the points' extent overflows");
+  if (!(W0 > 0)) W0 = 1.0;
+  double c[3];
+  for (int d = 0; d < 3; ++d) c[d] = lo[d] + (hi[d] - lo[d]) / 2;
+  for (int it = 0; it < 64; ++it) {
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+      origin[d] = c[d] - W0 / 2;
+      ok = ok && origin[d] <= lo[d] && origin[d] + W0 >= hi[d];
+    }
+    if (ok) return;
+    W0 *= 1 + 4 * 2.220446049250313e-16;
+  }
+  throw Error(FMMB_ERR_ARGUMENT, "could not fit a box around the points");
+}
+
+// fit_box! (src/operators/cache.jl:293-313): a box of width ldexp(cache W0, e) containing the bounds
+void fit_box(Cache& C, const double lo[3], const double hi[3], const double bo[3], double bw, double origin[3], double& W,
+             int& e) {
+  require(bw > 0, FMMB_ERR_ARGUMENT, "box width must be positive");
+  for (int d = 0; d < 3; ++d)
+    require(bo[d] <= lo[d] && bo[d] + bw >= hi[d], FMMB_ERR_ARGUMENT, "points lie outside the requested box");
+  std::lock_guard<std::mutex> lk(C.mu);
+  if (std::isnan(C.W0)) {
+    C.W0 = bw;
+    for (int d = 0; d < 3; ++d) origin[d] = bo[d];
+    W = bw;
+    e = 0;
+    return;
+  }
+  int ex;
+  double f = std::frexp(bw / C.W0, &ex);
+  e = f == 0.5 ? ex - 1 : ex;
+  double cen[3];
+  for (int d = 0; d < 3; ++d) cen[d] = bo[d] + bw / 2;
+  for (int it = 0; it < 2; ++it) {
+    double Wn = std::ldexp(C.W0, e);
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+      origin[d] = std::min(cen[d] - Wn / 2, lo[d]);
+      ok = ok && origin[d] + Wn >= hi[d];
+    }
+    if (ok) { W = Wn; return; }
+    ++e;
+  }
+  throw Error(FMMB_ERR_ARGUMENT, "could not fit a box");
+}
+
+void plan_from_device_points(fmmb_cache* cache, const double* xyz, int64_t n, const fmmb_tree_opts* opts, fmmb_plan** out) {
+  require(cache && opts && out, FMMB_ERR_ARGUMENT, "null argument");
+  Cache& C = cache->c;
+  Ctx& ctx = *C.ctx;
+  set_device(ctx);
+  require(n > 0, FMMB_ERR_ARGUMENT, "no points");
+  require(opts->ppl >= 1, FMMB_ERR_ARGUMENT, "ppl must be positive");
+  require(opts->max_levels >= 1, FMMB_ERR_ARGUMENT, "max_levels must be positive");
+  double lo[3], hi[3];
+  int64_t bad = 0;
+  bounds(ctx, xyz, n, lo, hi, &bad);
+  require(bad == 0, FMMB_ERR_ARGUMENT, "the points must be finite");
+  double bo[3], bw;
+  if (opts->has_bbox) {
+    for (int d = 0; d < 3; ++d) bo[d] = opts->origin[d];
+    bw = opts->width;
+  } else {
+    square_bbox(lo, hi, bo, bw);
+  }
+  std::unique_ptr<fmmb_plan> h(new fmmb_plan());
+  Plan& P = h->p;
+  P.cache = &C;
+  P.ctx = &ctx;
+  P.N = n;
+  fit_box(C, lo, hi, bo, bw, P.origin, P.W0, P.e0);
+  {
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (!C.uploaded) {
+      C.host = build_operators(C.p, C.W0);
+      upload_operators(C);
+    }
+  }
+  build_tree(P, xyz, opts->ppl, opts->max_levels);
+  P.scale.resize(P.L);
+  P.m2l_scale.resize(P.L);
+  for (int l = 0; l < P.L; ++l) {
+    int e = P.e0 - l;                       // the level's width is ldexp(cache W0, e)
+    double lam = std::ldexp(1.0, e);        // w / W_ref (src/operators/harmonics.jl:414-418)
+    P.scale[l] = e == 0 ? 1.0 / C.W0 : (1.0 / C.W0) / lam;
+    P.m2l_scale[l] = e == 0 ? 1.0 : 1.0 / lam;
+  }
+  build_lists(P);
+  *out = h.release();
+}
+
+void check_outputs(int outputs) {
+  require(outputs >= 1 && outputs <= 3, FMMB_ERR_ARGUMENT, "outputs must be POTENTIAL, GRADIENT or both");
+}
+
+// after a synchronisation: a bounded device wait that gave up is reported as a timeout
+void check_state_errors(State& S) {
+  if (S.precision == FMMB_PRECISION_MIXED && mixed_error_flag(S))
+    throw Error(FMMB_ERR_TIMEOUT, "a bounded wait of the tensor-core M2L gave up; the expansions are incomplete");
+}
+
+void state_build(State& S, const double* xyz, const double* tau) {
+  gather_inputs(S, xyz, tau);
+  upward_pass(S);
+  downward_pass(S);
+  S.built = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fmmb_last_error(void) { return g_last_error.c_str(); }
+const char* fmmb_version(void) { return "fmmb 0.1 (sm_100a)"; }
+
+int fmmb_ctx_create(int device, fmmb_ctx** out) {
+  return guard([&] {
+    require(out != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    int nd = 0;
+    FMMB_CUDA(cudaGetDeviceCount(&nd));
+    require(device >= 0 && device < nd, FMMB_ERR_ARGUMENT, "no such device");
+    std::unique_ptr<fmmb_ctx> h(new fmmb_ctx());
+    h->c.device = device;
+    FMMB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    FMMB_CUDA(cudaGetDeviceProperties(&prop, device));
+    require(prop.major == 10, FMMB_ERR_UNSUPPORTED, "this build targets sm_100a (B200)");
+    h->c.num_sms = prop.multiProcessorCount;
+    FMMB_CUDA(cudaStreamCreateWithFlags(&h->c.stream, cudaStreamNonBlocking));
+    h->c.own_stream = true;
+    init_device_constants(h->c.stream);
+    *out = h.release();
+  });
+}
+
+int fmmb_ctx_destroy(fmmb_ctx* ctx) {
+  return guard([&] {
+    if (!ctx) return;
+    set_device(ctx->c);
+    if (ctx->c.own_stream) { cudaStreamSynchronize(ctx->c.stream); cudaStreamDestroy(ctx->c.stream); }
+    delete ctx;
+  });
+}
+
+int fmmb_ctx_stream(fmmb_ctx* ctx, void** stream) {
+  return guard([&] {
+    require(ctx && stream, FMMB_ERR_ARGUMENT, "null argument");
+    *stream = (void*)ctx->c.stream;
+  });
+}
+
+int fmmb_ctx_synchronize(fmmb_ctx* ctx) {  // state errors surface at the next host-pointer call on the state
+  return guard([&] {
+    require(ctx != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    set_device(ctx->c);
+    FMMB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
+int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* m, fmmb_cache** out) {
+  return guard([&] {
+    require(ctx && m && out, FMMB_ERR_ARGUMENT, "null argument");
+    require(m->method == FMMB_METHOD_SPHERICAL_HARMONICS, FMMB_ERR_UNSUPPORTED, "only SphericalHarmonics is provided");
+    require(m->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "only Laplace3D is provided");
+    require(m->p >= 1, FMMB_ERR_ARGUMENT, "p must be at least 1");
+    require(m->p <= PMAX, FMMB_ERR_UNSUPPORTED, "p above 20 is not provided");
+    require(m->tol >= 0 && m->tol < 1, FMMB_ERR_ARGUMENT, "tol must lie in [0, 1)");
+    require(m->tol == 0, FMMB_ERR_UNSUPPORTED, "low-rank class operators (tol > 0) are not provided");
+    std::unique_ptr<fmmb_cache> h(new fmmb_cache());
+    h->c.ctx = &ctx->c;
+    h->c.p = m->p;
+    h->c.np = (m->p + 1) * (m->p + 1);
+    h->c.ld = ld_of(m->p);
+    *out = h.release();
+  });
+}
+
+int fmmb_cache_destroy(fmmb_cache* cache) {
+  return guard([&] {
+    if (!cache) return;
+    set_device(*cache->c.ctx);
+    delete cache;
+  });
+}
+
+int fmmb_cache_base_width(const fmmb_cache* cache, double* w) {
+  return guard([&] {
+    require(cache && w, FMMB_ERR_ARGUMENT, "null argument");
+    *w = cache->c.W0;
+  });
+}
+
+int fmmb_plan_create(fmmb_cache* cache, const double* xyz, int64_t n, const fmmb_tree_opts* opts, fmmb_plan** out) {
+  return guard([&] {
+    require(cache && xyz && opts && out, FMMB_ERR_ARGUMENT, "null argument");
+    require(n > 0, FMMB_ERR_ARGUMENT, "no points");
+    Ctx& ctx = *cache->c.ctx;
+    set_device(ctx);
+    DBuf<double> d(3 * n);
+    FMMB_CUDA(cudaMemcpyAsync(d.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx.stream));
+    plan_from_device_points(cache, d.p, n, opts, out);
+  });
+}
+
+int fmmb_plan_create_dev(fmmb_cache* cache, const double* xyz_dev, int64_t n, const fmmb_tree_opts* opts, fmmb_plan** out) {
+  return guard([&] {
+    require(xyz_dev != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    plan_from_device_points(cache, xyz_dev, n, opts, out);
+  });
+}
+
+int fmmb_plan_destroy(fmmb_plan* plan) {
+  return guard([&] {
+    if (!plan) return;
+    set_device(*plan->p.ctx);
+    FMMB_CUDA(cudaStreamSynchronize(plan->p.ctx->stream));
+    delete plan;
+  });
+}
+
+int fmmb_plan_info(const fmmb_plan* plan, int64_t* info, int cap) {
+  return guard([&] {
+    require(plan && info, FMMB_ERR_ARGUMENT, "null argument");
+    const Plan& P = plan->p;
+    require(cap >= 5 + P.L, FMMB_ERR_DIMENSION, "info needs 5 + levels entries");
+    info[0] = P.L;
+    info[1] = P.nnodes;
+    info[2] = P.N;
+    info[3] = P.npairs;
+    for (int l = 0; l <= P.L; ++l) info[4 + l] = P.level_start[l];
+  });
+}
+
+int fmmb_plan_box(const fmmb_plan* plan, double* origin3, double* width) {
+  return guard([&] {
+    require(plan && origin3 && width, FMMB_ERR_ARGUMENT, "null argument");
+    for (int d = 0; d < 3; ++d) origin3[d] = plan->p.origin[d];
+    *width = plan->p.W0;
+  });
+}
+
+int fmmb_plan_tree(const fmmb_plan* plan, int32_t* cell, int32_t* level, int32_t* parent, int32_t* child_first,
+                   int32_t* plo, int32_t* phi, uint8_t* flags, int32_t* colleagues, int32_t* perm, int32_t* point_node) {
+  return guard([&] {
+    require(plan != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    const Plan& P = plan->p;
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    int n = P.nnodes;
+    if (cell || level) {
+      std::vector<int4> c = to_host(P.cell.p, n, s);
+      for (int i = 0; i < n; ++i) {
+        if (cell) { cell[3 * i] = c[i].x; cell[3 * i + 1] = c[i].y; cell[3 * i + 2] = c[i].z; }
+        if (level) level[i] = c[i].w;
+      }
+    }
+    auto dl = [&](int32_t* dst, const int* src, size_t cnt) {
+      if (dst) FMMB_CUDA(cudaMemcpyAsync(dst, src, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    };
+    dl(parent, P.parent.p, n);
+    dl(child_first, P.cf.p, n);
+    dl(plo, P.plo.p, n);
+    dl(phi, P.phi.p, n);
+    dl(colleagues, P.col.p, (size_t)NCOL * n);
+    dl(perm, P.perm.p, P.N);
+    dl(point_node, P.point_node.p, P.N);
+    if (flags) FMMB_CUDA(cudaMemcpyAsync(flags, P.flags.p, n, cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int fmmb_plan_pairs(const fmmb_plan* plan, int level, int32_t* tgt, int32_t* src, int32_t* far, int64_t cap, int64_t* npairs) {
+  return guard([&] {
+    require(plan && npairs, FMMB_ERR_ARGUMENT, "null argument");
+    const Plan& P = plan->p;
+    require(level >= 0 && level < P.L, FMMB_ERR_ARGUMENT, "no such level");
+    *npairs = P.level_pairs.empty() ? 0 : P.level_pairs[level];
+    if (!tgt || !src || !far) return;
+    require(cap >= *npairs, FMMB_ERR_DIMENSION, "the pair arrays are too short");
+    set_device(*P.ctx);
+    std::vector<int2> pr = to_host(P.pairs.p, (size_t)std::max<int64_t>(P.npairs, 0), P.ctx->stream);
+    int64_t k = 0;
+    for (const M2LBlock& b : P.h_blocks) {
+      if (b.level != level) continue;
+      int64_t next = P.npairs;
+      for (const M2LBlock& b2 : P.h_blocks) if (b2.pair_base > b.pair_base) { next = std::min<int64_t>(next, b2.pair_base); }
+      for (int64_t q = b.pair_base; q < next; ++q) {
+        tgt[k] = b.first + (pr[q].y & 0xff);
+        src[k] = pr[q].x;
+        far[k] = pr[q].y >> 8;
+        ++k;
+      }
+    }
+  });
+}
+
+int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
+  return guard([&] {
+    require(plan && out, FMMB_ERR_ARGUMENT, "null argument");
+    require(precision == FMMB_PRECISION_FP64 || precision == FMMB_PRECISION_MIXED, FMMB_ERR_ARGUMENT, "unknown precision path");
+    Plan& P = plan->p;
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    std::unique_ptr<fmmb_state> h(new fmmb_state());
+    State& S = h->s;
+    S.plan = &P;
+    S.precision = precision;
+    S.xs.alloc(P.N); S.ys.alloc(P.N); S.zs.alloc(P.N); S.q.alloc(P.N);
+    size_t ne = (size_t)P.nnodes * P.cache->ld;
+    S.M.alloc(ne);
+    S.Pl.alloc(ne);
+    FMMB_CUDA(cudaMemsetAsync(S.M.p, 0, S.M.bytes(), s));
+    FMMB_CUDA(cudaMemsetAsync(S.Pl.p, 0, S.Pl.bytes(), s));
+    if (precision == FMMB_PRECISION_MIXED) {
+      std::lock_guard<std::mutex> lk(P.cache->mu);
+      prepare_mixed_operators(*P.cache);
+    }
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    *out = h.release();
+  });
+}
+
+int fmmb_state_destroy(fmmb_state* state) {
+  return guard([&] {
+    if (!state) return;
+    set_device(*state->s.plan->ctx);
+    FMMB_CUDA(cudaStreamSynchronize(state->s.plan->ctx->stream));
+    delete state;
+  });
+}
+
+int fmmb_build_expansions_dev(fmmb_state* state, const double* xyz, const double* tau, int64_t n) {
+  return guard([&] {
+    require(state && xyz && tau, FMMB_ERR_ARGUMENT, "null argument");
+    State& S = state->s;
+    require(n == S.plan->N, FMMB_ERR_DIMENSION, "expected " + std::to_string(S.plan->N) + " sources and densities");
+    set_device(*S.plan->ctx);
+    state_build(S, xyz, tau);
+  });
+}
+
+int fmmb_build_expansions(fmmb_state* state, const double* xyz, const double* tau, int64_t n) {
+  return guard([&] {
+    require(state && xyz && tau, FMMB_ERR_ARGUMENT, "null argument");
+    State& S = state->s;
+    Plan& P = *S.plan;
+    require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and densities");
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    if (S.h_in_xyz.n < (size_t)(3 * n)) { S.h_in_xyz.alloc(3 * n); S.h_in_tau.alloc(n); }
+    FMMB_CUDA(cudaMemcpyAsync(S.h_in_xyz.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    FMMB_CUDA(cudaMemcpyAsync(S.h_in_tau.p, tau, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    state_build(S, S.h_in_xyz.p, S.h_in_tau.p);
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    check_state_errors(S);
+  });
+}
+
+int fmmb_evaluate_at_sources_dev(fmmb_state* state, int outputs, double* pot, double* grad) {
+  return guard([&] {
+    require(state != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    check_outputs(outputs);
+    State& S = state->s;
+    require(S.built, FMMB_ERR_ARGUMENT, "the state has no expansions yet (build_expansions first)");
+    require(!(outputs & FMMB_OUTPUT_POTENTIAL) || pot, FMMB_ERR_ARGUMENT, "null potential output");
+    require(!(outputs & FMMB_OUTPUT_GRADIENT) || grad, FMMB_ERR_ARGUMENT, "null gradient output");
+    set_device(*S.plan->ctx);
+    evaluate_sources(S, outputs, pot, grad);
+  });
+}
+
+int fmmb_evaluate_at_sources(fmmb_state* state, int outputs, double* pot, double* grad) {
+  return guard([&] {
+    require(state != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    check_outputs(outputs);
+    State& S = state->s;
+    Plan& P = *S.plan;
+    require(S.built, FMMB_ERR_ARGUMENT, "the state has no expansions yet (build_expansions first)");
+    require(!(outputs & FMMB_OUTPUT_POTENTIAL) || pot, FMMB_ERR_ARGUMENT, "null potential output");
+    require(!(outputs & FMMB_OUTPUT_GRADIENT) || grad, FMMB_ERR_ARGUMENT, "null gradient output");
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    if (S.d_pot.n < (size_t)P.N) { S.d_pot.alloc(P.N); S.d_grad.alloc(3 * P.N); }
+    evaluate_sources(S, outputs, S.d_pot.p, S.d_grad.p);
+    if (outputs & FMMB_OUTPUT_POTENTIAL)
+      FMMB_CUDA(cudaMemcpyAsync(pot, S.d_pot.p, sizeof(double) * P.N, cudaMemcpyDeviceToHost, s));
+    if (outputs & FMMB_OUTPUT_GRADIENT)
+      FMMB_CUDA(cudaMemcpyAsync(grad, S.d_grad.p, sizeof(double) * 3 * P.N, cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    check_state_errors(S);
+  });
+}
+
+int fmmb_matvec_dev(fmmb_state* state, const double* xyz, const double* tau, int64_t n, int outputs, double* pot, double* grad) {
+  int rc = fmmb_build_expansions_dev(state, xyz, tau, n);
+  return rc != FMMB_OK ? rc : fmmb_evaluate_at_sources_dev(state, outputs, pot, grad);
+}
+
+int fmmb_matvec(fmmb_state* state, const double* xyz, const double* tau, int64_t n, int outputs, double* pot, double* grad) {
+  return guard([&] {
+    require(state && xyz && tau, FMMB_ERR_ARGUMENT, "null argument");
+    check_outputs(outputs);
+    State& S = state->s;
+    Plan& P = *S.plan;
+    require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and densities");
+    require(!(outputs & FMMB_OUTPUT_POTENTIAL) || pot, FMMB_ERR_ARGUMENT, "null potential output");
+    require(!(outputs & FMMB_OUTPUT_GRADIENT) || grad, FMMB_ERR_ARGUMENT, "null gradient output");
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    if (S.h_in_xyz.n < (size_t)(3 * n)) { S.h_in_xyz.alloc(3 * n); S.h_in_tau.alloc(n); }
+    if (S.d_pot.n < (size_t)P.N) { S.d_pot.alloc(P.N); S.d_grad.alloc(3 * P.N); }
+    FMMB_CUDA(cudaMemcpyAsync(S.h_in_xyz.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    FMMB_CUDA(cudaMemcpyAsync(S.h_in_tau.p, tau, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    state_build(S, S.h_in_xyz.p, S.h_in_tau.p);
+    evaluate_sources(S, outputs, S.d_pot.p, S.d_grad.p);
+    if (outputs & FMMB_OUTPUT_POTENTIAL)
+      FMMB_CUDA(cudaMemcpyAsync(pot, S.d_pot.p, sizeof(double) * P.N, cudaMemcpyDeviceToHost, s));
+    if (outputs & FMMB_OUTPUT_GRADIENT)
+      FMMB_CUDA(cudaMemcpyAsync(grad, S.d_grad.p, sizeof(double) * 3 * P.N, cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    check_state_errors(S);
+  });
+}
+
+int fmmb_evaluate_dev(fmmb_state* state, const double* tg, int64_t nt, int outputs, double* pot, double* grad) {
+  return guard([&] {
+    require(state != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    check_outputs(outputs);
+    require(nt >= 0, FMMB_ERR_DIMENSION, "negative target count");
+    State& S = state->s;
+    require(S.built, FMMB_ERR_ARGUMENT, "the state has no expansions yet (build_expansions first)");
+    if (nt == 0) return;
+    require(tg != nullptr, FMMB_ERR_ARGUMENT, "null targets");
+    set_device(*S.plan->ctx);
+    evaluate_targets(S, tg, nt, outputs, pot, grad);
+  });
+}
+
+int fmmb_evaluate(fmmb_state* state, const double* tg, int64_t nt, int outputs, double* pot, double* grad) {
+  return guard([&] {
+    require(state != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    check_outputs(outputs);
+    require(nt >= 0, FMMB_ERR_DIMENSION, "negative target count");
+    State& S = state->s;
+    Plan& P = *S.plan;
+    require(S.built, FMMB_ERR_ARGUMENT, "the state has no expansions yet (build_expansions first)");
+    if (nt == 0) return;
+    require(tg != nullptr, FMMB_ERR_ARGUMENT, "null targets");
+    require(!(outputs & FMMB_OUTPUT_POTENTIAL) || pot, FMMB_ERR_ARGUMENT, "null potential output");
+    require(!(outputs & FMMB_OUTPUT_GRADIENT) || grad, FMMB_ERR_ARGUMENT, "null gradient output");
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    DBuf<double> dt(3 * nt), dp(nt), dg(3 * nt);
+    FMMB_CUDA(cudaMemcpyAsync(dt.p, tg, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+    evaluate_targets(S, dt.p, nt, outputs, dp.p, dg.p);
+    if (outputs & FMMB_OUTPUT_POTENTIAL) FMMB_CUDA(cudaMemcpyAsync(pot, dp.p, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
+    if (outputs & FMMB_OUTPUT_GRADIENT) FMMB_CUDA(cudaMemcpyAsync(grad, dg.p, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    check_state_errors(S);
+  });
+}
+
+int fmmb_profile_matvec(fmmb_state* state, const double* xyz, const double* tau, int64_t n, int outputs, double* pot,
+                        double* grad, double* stage_ms, int cap, int* launches) {
+  return guard([&] {
+    require(state && xyz && tau && stage_ms, FMMB_ERR_ARGUMENT, "null argument");
+    require(cap >= 6, FMMB_ERR_DIMENSION, "stage_ms needs 6 entries");
+    check_outputs(outputs);
+    State& S = state->s;
+    Plan& P = *S.plan;
+    require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and densities");
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    cudaEvent_t ev[7];
+    for (auto& e : ev) FMMB_CUDA(cudaEventCreate(&e));
+    int nl = 0;
+    FMMB_CUDA(cudaEventRecord(ev[0], s));
+    gather_inputs(S, xyz, tau);
+    nl += 1;
+    FMMB_CUDA(cudaEventRecord(ev[1], s));
+    nl += p2m(S);
+    FMMB_CUDA(cudaEventRecord(ev[2], s));
+    nl += m2m_sweep(S);
+    FMMB_CUDA(cudaEventRecord(ev[3], s));
+    nl += m2l_stage(S);
+    FMMB_CUDA(cudaEventRecord(ev[4], s));
+    nl += l2l_sweep(S);
+    FMMB_CUDA(cudaEventRecord(ev[5], s));
+    S.built = true;
+    evaluate_sources(S, outputs, pot, grad);
+    nl += P.n_leaves > 0;
+    FMMB_CUDA(cudaEventRecord(ev[6], s));
+    FMMB_CUDA(cudaEventSynchronize(ev[6]));
+    for (int i = 0; i < 6; ++i) {
+      float ms = 0;
+      FMMB_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+      stage_ms[i] = ms;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    check_state_errors(S);
+    if (launches) *launches = nl;
+  });
+}
+
+int fmmb_state_expansions(const fmmb_state* state, double* multipoles, double* locals) {
+  return guard([&] {
+    require(state != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    const State& S = state->s;
+    const Plan& P = *S.plan;
+    set_device(*P.ctx);
+    int LD = P.cache->ld, NP = P.cache->np, n = P.nnodes;
+    cudaStream_t s = P.ctx->stream;
+    if (multipoles) {
+      std::vector<double> h = to_host(S.M.p, (size_t)n * LD, s);
+      for (int i = 0; i < n; ++i) std::memcpy(multipoles + (size_t)i * NP, &h[(size_t)i * LD], sizeof(double) * NP);
+    }
+    if (locals) {
+      std::vector<double> h = to_host(S.Pl.p, (size_t)n * LD, s);
+      for (int i = 0; i < n; ++i) {
+        if (P.h_flags[i] & F_LEAF) std::memcpy(locals + (size_t)i * NP, &h[(size_t)i * LD], sizeof(double) * NP);
+        else std::memset(locals + (size_t)i * NP, 0, sizeof(double) * NP);
+      }
+    }
+  });
+}
+
+int fmmb_direct_dev(fmmb_ctx* ctx, const double* src, const double* tau, int64_t ns, const double* tgt,
+                    const int64_t* self_index, int64_t nt, double* pot, double* grad) {
+  return guard([&] {
+    require(ctx && src && tau && tgt, FMMB_ERR_ARGUMENT, "null argument");
+    require(ns >= 0 && nt >= 0, FMMB_ERR_DIMENSION, "negative count");
+    set_device(ctx->c);
+    direct(ctx->c, src, tau, ns, tgt, self_index, nt, pot, grad);
+  });
+}
+
+}  // extern "C"

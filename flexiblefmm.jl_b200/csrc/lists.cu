@@ -1,0 +1,197 @@
+// The node lists and the M2L interaction lists of a plan.
+//
+// Far pairs (src/tree/lists.jl:71-124, src/device_lists.jl:261-312): a non-ghost target on
+// level ≥ 2 (0-based) pairs with every sourced child of its parent's colleagues at a far
+// offset (Chebyshev norm ≥ 2). The reference lists them class-major per level and cuts
+// chunks for one GEMM each (src/device_lists.jl:219-278). Here the targets of every level
+// ≥ 2 are cut into blocks of TB consecutive nodes, each block owning the pairs of its
+// targets grouped by symmetry class, and inside a class by target, then by the enumeration
+// order. A block is the unit of the M2L kernels: it owns its targets' partial locals, so
+// the scatter is deterministic and needs no atomics, and one launch covers all levels.
+#include <numeric>
+
+#include "plan.cuh"
+#include "scan_sort.cuh"
+
+namespace fmmb {
+namespace {
+
+__constant__ int c_far_index[343];   // m2l table slot → far offset index, -1 for a near offset
+__constant__ int c_class[NFAR];      // far offset → symmetry class
+
+__device__ __forceinline__ int far_of(int4 t, int4 s) {
+  int ox = s.x - t.x, oy = s.y - t.y, oz = s.z - t.z;
+  if (max(abs(ox), max(abs(oy), abs(oz))) < 2) return -1;
+  return c_far_index[(ox + 3) + 7 * (oy + 3) + 49 * (oz + 3)];
+}
+
+// visits the far pairs (source node, far index) of target t in the reference's order
+template <class F>
+__device__ __forceinline__ void for_far_pairs(int t, const int4* __restrict__ cell, const int* __restrict__ parent,
+                                              const int* __restrict__ cf, const int* __restrict__ col,
+                                              const uint8_t* __restrict__ flags, F&& fn) {
+  if (flags[t] & F_GHOST) return;
+  int p = parent[t];
+  int4 ct = cell[t];
+  for (int k = 0; k < NCOL; ++k) {
+    int pc = col[(int64_t)p * NCOL + k];
+    if (pc < 0) continue;
+    int s0 = cf[pc];
+    if (s0 < 0) continue;
+    for (int s = s0; s < s0 + NCH; ++s) {
+      if (!(flags[s] & F_SOURCE)) continue;
+      int f = far_of(ct, cell[s]);
+      if (f >= 0) fn(s, f);
+    }
+  }
+}
+
+__global__ void k_pair_count(const int4* __restrict__ cell, const int* __restrict__ parent, const int* __restrict__ cf,
+                             const int* __restrict__ col, const uint8_t* __restrict__ flags, int first, int n,
+                             int* __restrict__ cnt) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  int c = 0;
+  for_far_pairs(first + q, cell, parent, cf, col, flags, [&](int, int) { ++c; });
+  cnt[first + q] = c;
+}
+
+// one CTA per block, one thread per target: counts per (target, class), the class-major
+// offsets, and the fill
+__global__ void k_block_fill(const int4* __restrict__ blocks, const int4* __restrict__ cell, const int* __restrict__ parent,
+                             const int* __restrict__ cf, const int* __restrict__ col, const uint8_t* __restrict__ flags,
+                             int* __restrict__ cls_off, int2* __restrict__ pairs) {
+  extern __shared__ int sm[];
+  const int TB = blockDim.x;
+  int* cnt = sm;                 // [NCLASS][TB]
+  int* tot = sm + NCLASS * TB;   // [NCLASS + 1]
+  int4 b = blocks[blockIdx.x];
+  int t = threadIdx.x;
+  for (int c = 0; c < NCLASS; ++c) cnt[c * TB + t] = 0;
+  if (t < b.z)
+    for_far_pairs(b.y + t, cell, parent, cf, col, flags, [&](int, int f) { cnt[c_class[f] * TB + t]++; });
+  __syncthreads();
+  if (t < NCLASS) {        // exclusive scan down each class column
+    int run = 0;
+    for (int q = 0; q < TB; ++q) { int v = cnt[t * TB + q]; cnt[t * TB + q] = run; run += v; }
+    tot[t] = run;
+  }
+  __syncthreads();
+  if (t == 0) {
+    int run = 0;
+    for (int c = 0; c < NCLASS; ++c) { int v = tot[c]; tot[c] = run; run += v; }
+    tot[NCLASS] = run;
+  }
+  __syncthreads();
+  if (t <= NCLASS) cls_off[(int64_t)blockIdx.x * (NCLASS + 1) + t] = tot[t];
+  if (t < b.z) {
+    int cur[NCLASS];
+#pragma unroll
+    for (int c = 0; c < NCLASS; ++c) cur[c] = tot[c] + cnt[c * TB + t];
+    int2* out = pairs + b.w;
+    for_far_pairs(b.y + t, cell, parent, cf, col, flags, [&](int s, int f) {
+      int c = c_class[f];
+      int pos = 0;
+#pragma unroll
+      for (int k = 0; k < NCLASS; ++k)
+        if (k == c) pos = cur[k]++;
+      out[pos] = make_int2(s, (f << 8) | t);
+    });
+  }
+}
+
+}  // namespace
+
+void build_lists(Plan& P) {
+  cudaStream_t s = P.ctx->stream;
+  const int n = P.nnodes, L = P.L;
+  P.h_parent = to_host(P.parent.p, n, s);
+  P.h_cf = to_host(P.cf.p, n, s);
+  P.h_plo = to_host(P.plo.p, n, s);
+  P.h_phi = to_host(P.phi.p, n, s);
+  P.h_flags = to_host(P.flags.p, n, s);
+
+  // childless nodes with sources on levels ≥ 2 (src/fmm.jl:45-46), real leaves with points
+  std::vector<int> s2m, leaves, lstart, lcount;
+  for (int l = 0; l < L; ++l)
+    for (int g = P.level_start[l]; g < P.level_start[l + 1]; ++g) {
+      bool src = (P.h_flags[g] & F_SOURCE) != 0;
+      if (l >= 2 && P.h_cf[g] < 0 && src) s2m.push_back(g);
+      if ((P.h_flags[g] & F_LEAF) && src) {
+        leaves.push_back(g);
+        lstart.push_back(P.h_plo[g]);
+        lcount.push_back(P.h_phi[g] - P.h_plo[g] + 1);
+      }
+    }
+  P.n_s2m = (int)s2m.size();
+  P.n_leaves = (int)leaves.size();
+  to_device(P.s2m_nodes, s2m, s);
+  to_device(P.leaves, leaves, s);
+  to_device(P.leaf_start, lstart, s);
+  to_device(P.leaf_count, lcount, s);
+  P.group_parent.clear();
+  P.group_parent.resize(L);
+  for (int l = 1; l < L; ++l) {
+    int nl = P.level_start[l + 1] - P.level_start[l];
+    std::vector<int> gp(nl / NCH);
+    for (int g = 0; g < nl / NCH; ++g) gp[g] = P.h_parent[P.level_start[l] + NCH * g];
+    to_device(P.group_parent[l], gp, s);
+  }
+
+  // the offset tables
+  {
+    std::vector<int> fidx(343, -1);
+    int k = 0;
+    for (int t = 0; t < 343; ++t) {
+      int o[3] = {t % 7 - 3, (t / 7) % 7 - 3, (t / 49) % 7 - 3};
+      if (std::max(std::abs(o[0]), std::max(std::abs(o[1]), std::abs(o[2]))) >= 2) fidx[t] = k++;
+    }
+    FMMB_CUDA(cudaMemcpyToSymbolAsync(c_far_index, fidx.data(), sizeof(int) * 343, 0, cudaMemcpyHostToDevice, s));
+    FMMB_CUDA(cudaMemcpyToSymbolAsync(c_class, P.cache->host.cls.data(), sizeof(int) * NFAR, 0, cudaMemcpyHostToDevice, s));
+  }
+
+  // pairs per target, then the blocks and their bases
+  DBuf<int> cnt(std::max(n, 1));
+  FMMB_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * n, s));
+  for (int l = 2; l < L; ++l) {
+    int first = P.level_start[l], nl = P.level_start[l + 1] - first;
+    k_pair_count<<<(nl + 127) / 128, 128, 0, s>>>(P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p, first, nl, cnt.p);
+    FMMB_LAUNCH_CHECK();
+  }
+  std::vector<int> hc = to_host(cnt.p, n, s);
+  P.h_blocks.clear();
+  P.level_pairs.assign(L, 0);
+  int64_t base = 0;
+  for (int l = 2; l < L; ++l) {
+    for (int b0 = P.level_start[l]; b0 < P.level_start[l + 1]; b0 += P.TB) {
+      int c = std::min(P.TB, P.level_start[l + 1] - b0);
+      int64_t np = 0;
+      for (int g = b0; g < b0 + c; ++g) np += hc[g];
+      if (np == 0) continue;
+      P.h_blocks.push_back({l, b0, c, (int)base});
+      base += np;
+      P.level_pairs[l] += np;
+    }
+  }
+  require(base < (1ll << 31), FMMB_ERR_ARGUMENT, "too many far pairs for 32-bit offsets");
+  P.npairs = base;
+  int nb = (int)P.h_blocks.size();
+  std::vector<int4> hb(nb);
+  for (int b = 0; b < nb; ++b) hb[b] = make_int4(P.h_blocks[b].level, P.h_blocks[b].first, P.h_blocks[b].count, P.h_blocks[b].pair_base);
+  to_device(P.blocks, hb, s);
+  P.cls_off.alloc((size_t)std::max(nb, 1) * (NCLASS + 1));
+  P.pairs.alloc(std::max<int64_t>(base, 1));
+  if (nb) {
+    size_t smem = sizeof(int) * (NCLASS * P.TB + NCLASS + 1);
+    k_block_fill<<<nb, P.TB, smem, s>>>(P.blocks.p, P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p, P.cls_off.p, P.pairs.p);
+    FMMB_LAUNCH_CHECK();
+  }
+  // per level factors
+  std::vector<double> sc(L), ms(L);
+  for (int l = 0; l < L; ++l) { sc[l] = P.scale[l]; ms[l] = P.m2l_scale[l]; }
+  to_device(P.d_scale, sc, s);
+  to_device(P.d_m2l_scale, ms, s);
+  FMMB_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace fmmb

@@ -1,0 +1,686 @@
+// The FP64 passes of the plain path (the drop-in) and the shared pieces of both paths:
+//   gather    inputs into tree order                         (src/device_passes.jl:644-665)
+//   P2M       multipoles of the childless nodes              (src/device_passes.jl:343-373)
+//   M2M, L2L  one GEMM per level, gather/scatter fused       (src/device_passes.jl:539-611)
+//   M2L       one launch for all levels: per block of targets and per symmetry class, the
+//             signed-permutation gather, the class GEMM and the target-owned scatter
+//                                                            (src/device_passes.jl:428-473,565-580)
+//   L2P+P2P   the evaluation at the sources or at located targets
+//                                                            (src/device.jl:89-100,189-206)
+//   locate    the leaf of each target                        (src/tree/locate.jl:10-22)
+//   direct    FP64 direct sums                               (src/kernels.jl:442-487)
+// HBM layout: sources SoA (x, y, z, q) in tree order; expansions node-major with a padded
+// leading dimension LD (a multiple of 64 ≥ (p+1)²), rows ≥ (p+1)² kept zero.
+#include <algorithm>
+
+#include "passes.cuh"
+#include "scan_sort.cuh"
+
+namespace fmmb {
+
+__constant__ double c_tab[5 * TRI_MAX];  // a, b, cz, cm, cp of the Schmidt recurrences, up to degree PMAX
+__constant__ double c_e[PMAX];           // the sectoral factors e_m, m = 1..PMAX
+
+void init_device_constants(cudaStream_t s) {
+  std::vector<double> t(5 * TRI_MAX, 0.0), e(PMAX);
+  for (int n = 0; n <= PMAX; ++n)
+    for (int m = 0; m <= n; ++m) {
+      int k = tri(n, m);
+      double c = std::sqrt((double)((n - m) * (n + m)));
+      t[2 * TRI_MAX + k] = c;
+      if (n > m) {
+        t[k] = (double)(2 * n - 1) / c;
+        t[TRI_MAX + k] = std::sqrt((double)((n - m - 1) * (n + m - 1))) / c;
+      }
+      t[3 * TRI_MAX + k] = n + m >= 2 ? std::sqrt((double)((n + m) * (n + m - 1))) : 0.0;
+      t[4 * TRI_MAX + k] = n - m >= 2 ? std::sqrt((double)((n - m) * (n - m - 1))) : 0.0;
+    }
+  for (int m = 1; m <= PMAX; ++m) e[m - 1] = std::sqrt((double)(2 * m - 1) / (double)(2 * m));
+  FMMB_CUDA(cudaMemcpyToSymbolAsync(c_tab, t.data(), sizeof(double) * t.size(), 0, cudaMemcpyHostToDevice, s));
+  FMMB_CUDA(cudaMemcpyToSymbolAsync(c_e, e.data(), sizeof(double) * e.size(), 0, cudaMemcpyHostToDevice, s));
+  FMMB_CUDA(cudaStreamSynchronize(s));
+}
+
+namespace {
+
+inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+// ---------------------------------------------------------------- gather
+__global__ void k_gather_inputs(const double* __restrict__ xyz, const double* __restrict__ tau, const int* __restrict__ perm,
+                                int64_t n, double* __restrict__ xs, double* __restrict__ ys, double* __restrict__ zs,
+                                double* __restrict__ q) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t j = perm[k];
+  xs[k] = xyz[3 * j];
+  ys[k] = xyz[3 * j + 1];
+  zs[k] = xyz[3 * j + 2];
+  q[k] = tau[j];
+}
+
+// ---------------------------------------------------------------- P2M
+// one thread per (node, order m): M_n^m += τ conj Υ̃_n^m((y − c)/w) over the node's sources,
+// n = m..P, the chain of order m started from its own sectoral value (harmonics.jl:682-743)
+template <int P>
+__global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restrict__ cell, const int* __restrict__ plo,
+                      const int* __restrict__ phi, const double* __restrict__ xs, const double* __restrict__ ys,
+                      const double* __restrict__ zs, const double* __restrict__ q, Geometry geo,
+                      const double* __restrict__ scale, int LD, double* __restrict__ M) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  int qn = g / (P + 1), m = g % (P + 1);
+  if (qn >= nn) return;
+  int node = nodes[qn];
+  int4 c = cell[node];
+  double w = ldexp(geo.W0, -c.w), s = scale[c.w];
+  double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  double ar[P + 1], ai[P + 1];
+#pragma unroll
+  for (int n = 0; n <= P; ++n) { ar[n] = 0; ai[n] = 0; }
+  int j1 = phi[node];
+  for (int j = plo[node]; j <= j1; ++j) {
+    double x = (xs[j] - cx) * s, y = (ys[j] - cy) * s, z = (zs[j] - cz) * s;
+    double r2 = x * x + y * y + z * z;
+    double sr = 1.0, si = 0.0;
+    for (int k = 1; k <= m; ++k) {
+      double e = c_e[k - 1];
+      double nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
+      sr = nr; si = ni;
+    }
+    double tau = q[j];
+    double pr = 0, pi = 0, cr = 0, ci = 0;
+#pragma unroll
+    for (int n = 0; n <= P; ++n) {
+      if (n == m) {
+        cr = sr; ci = si; pr = 0; pi = 0;
+        ar[n] += tau * cr; ai[n] -= tau * ci;
+      } else if (n > m) {
+        int t = tri(n, m);
+        double az = c_tab[t] * z, br = c_tab[TRI_MAX + t] * r2;
+        double nr = az * cr - br * pr, ni = az * ci - br * pi;
+        pr = cr; pi = ci; cr = nr; ci = ni;
+        ar[n] += tau * nr; ai[n] -= tau * ni;
+      }
+    }
+  }
+  double* col = M + (int64_t)node * LD;
+#pragma unroll
+  for (int n = 0; n <= P; ++n) {
+    if (n < m) continue;
+    if (m == 0) col[n * n] = ar[n];
+    else { col[n * n + 2 * m - 1] = ar[n]; col[n * n + 2 * m] = ai[n]; }
+  }
+}
+
+// ---------------------------------------------------------------- GEMM over mapped columns (M2M, L2L)
+struct ColMap {
+  double* base;
+  const int* idx;  // column g at base + (idx ? idx[g] : off + stride·g)·LD
+  int off, stride;
+  __device__ __forceinline__ double* col(int g, int LD) const {
+    return base + (int64_t)(idx ? idx[g] : off + stride * g) * LD;
+  }
+};
+
+// C(:, g) (=|+=) A · B(:, g); A column-major M × K; rows r with r mod LD ≥ NP written as 0
+__global__ void __launch_bounds__(256) k_gemm_cols(int M, int K, const double* __restrict__ A, ColMap bm, ColMap cm,
+                                                   int ncols, int LD, int NP, int accumulate) {
+  constexpr int BM = 64, BN = 64, BK = 16;
+  __shared__ double As[BK][BM];
+  __shared__ double Bs[BK][BN + 1];
+  int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    for (int e = tid; e < BM * BK; e += 256) {
+      int i = e % BM, k = e / BM;
+      As[k][i] = (row0 + i < M && k0 + k < K) ? A[(int64_t)(k0 + k) * M + row0 + i] : 0.0;
+    }
+    for (int e = tid; e < BN * BK; e += 256) {
+      int k = e % BK, j = e / BK;
+      int g = col0 + j;
+      Bs[k][j] = (g < ncols && k0 + k < K) ? bm.col(g, LD)[k0 + k] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      double a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) a[r] = As[k][ty + 16 * r];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) b[c] = Bs[k][tx + 16 * c];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    int g = col0 + tx + 16 * c;
+    if (g >= ncols) continue;
+    double* C = cm.col(g, LD);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      int row = row0 + ty + 16 * r;
+      if (row >= M) continue;
+      double v = (row % LD) < NP ? acc[r][c] : 0.0;
+      C[row] = accumulate ? C[row] + v : v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- M2L, FP64
+// One CTA per block of targets. Per class: the pairs in chunks of NB columns; the gathered
+// B operand G = P_sᵀ M_src and the class representative A stream through shared memory in
+// K-chunks of 16; the product Y = A G is staged and scattered with P_t, each thread owning
+// one output row and summing the consecutive pairs of a target before one update of its
+// partial local (no atomics: the block owns its targets).
+template <int LD, int NB>
+__global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks, const int* __restrict__ cls_off,
+                                                 const int2* __restrict__ pairs, const double* __restrict__ reps,
+                                                 const int16_t* __restrict__ gidx, const int8_t* __restrict__ gsgn,
+                                                 const int16_t* __restrict__ sidx, const int8_t* __restrict__ ssgn,
+                                                 const double* __restrict__ m2l_scale, int NP, const double* __restrict__ M,
+                                                 double* __restrict__ Pl) {
+  constexpr int BK = 16, RPT = LD / 16, CPT = NB / 16;
+  extern __shared__ double sm[];
+  double* As = sm;                    // [BK][LD]
+  double* Gs = As + BK * LD;          // [BK][NB]
+  double* Ys = Gs + BK * NB;          // [NB][LD + 1]
+  int* ps = (int*)(Ys + NB * (LD + 1));  // src[NB], f[NB], t[NB]
+  int* pf = ps + NB;
+  int* pt = pf + NB;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int4 b = blocks[blockIdx.x];  // level, first node, count, pair base
+  const double alpha = m2l_scale[b.x];
+  const int* co = cls_off + (int64_t)blockIdx.x * (NCLASS + 1);
+  const int kmax = (NP + BK - 1) / BK * BK;
+  for (int c = 0; c < NCLASS; ++c) {
+    int a0 = co[c], a1 = co[c + 1];
+    const double* A = reps + (int64_t)c * LD * LD;
+    for (int q0 = a0; q0 < a1; q0 += NB) {
+      int nc = min(NB, a1 - q0);
+      __syncthreads();
+      for (int j = tid; j < NB; j += 256) {
+        if (j < nc) {
+          int2 pr = pairs[b.w + q0 + j];
+          ps[j] = pr.x; pf[j] = pr.y >> 8; pt[j] = pr.y & 0xff;
+        } else { ps[j] = -1; pf[j] = 0; pt[j] = -1; }
+      }
+      double acc[RPT][CPT];
+#pragma unroll
+      for (int r = 0; r < RPT; ++r)
+#pragma unroll
+        for (int cc = 0; cc < CPT; ++cc) acc[r][cc] = 0;
+      for (int k0 = 0; k0 < kmax; k0 += BK) {
+        __syncthreads();
+        for (int e = tid; e < BK * LD; e += 256) {
+          int i = e % LD, k = e / LD;
+          As[k * LD + i] = A[(int64_t)(k0 + k) * LD + i];
+        }
+        for (int e = tid; e < BK * NB; e += 256) {
+          int k = e % BK, j = e / BK;
+          double v = 0.0;
+          if (j < nc) {
+            int f = pf[j], row = k0 + k;
+            int gi = gidx[f * LD + row];
+            if (gi >= 0) v = (double)gsgn[f * LD + row] * M[(int64_t)ps[j] * LD + gi];
+          }
+          Gs[k * NB + j] = v;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int k = 0; k < BK; ++k) {
+          double av[RPT], bv[CPT];
+#pragma unroll
+          for (int r = 0; r < RPT; ++r) av[r] = As[k * LD + ty + 16 * r];
+#pragma unroll
+          for (int cc = 0; cc < CPT; ++cc) bv[cc] = Gs[k * NB + tx + 16 * cc];
+#pragma unroll
+          for (int r = 0; r < RPT; ++r)
+#pragma unroll
+            for (int cc = 0; cc < CPT; ++cc) acc[r][cc] = fma(av[r], bv[cc], acc[r][cc]);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < RPT; ++r)
+#pragma unroll
+        for (int cc = 0; cc < CPT; ++cc) Ys[(tx + 16 * cc) * (LD + 1) + ty + 16 * r] = acc[r][cc];
+      __syncthreads();
+      for (int j = tid; j < NP; j += 256) {
+        int cur = -1;
+        double run = 0.0;
+        for (int qq = 0; qq < nc; ++qq) {
+          int t = pt[qq], f = pf[qq];
+          if (t != cur) {
+            if (cur >= 0) Pl[(int64_t)(b.y + cur) * LD + j] += alpha * run;
+            cur = t;
+            run = 0.0;
+          }
+          int si = sidx[f * LD + j];
+          run += (double)ssgn[f * LD + j] * Ys[qq * (LD + 1) + si];
+        }
+        if (cur >= 0) Pl[(int64_t)(b.y + cur) * LD + j] += alpha * run;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- evaluation, FP64
+// one warp per group of targets in one real leaf; lanes over the targets, the sources of
+// the 27 colleagues read in lockstep (warp-uniform addresses: broadcast loads)
+template <int P, bool SELF>
+__global__ void __launch_bounds__(256) k_eval_f64(const int* __restrict__ gnode, const int* __restrict__ gstart,
+                                                  const int* __restrict__ gcount, int ngroups, const double* __restrict__ tx,
+                                                  const double* __restrict__ ty, const double* __restrict__ tz,
+                                                  const int* __restrict__ tout, const double* __restrict__ xs,
+                                                  const double* __restrict__ ys, const double* __restrict__ zs,
+                                                  const double* __restrict__ q, const int4* __restrict__ cell,
+                                                  const int* __restrict__ plo, const int* __restrict__ phi,
+                                                  const int* __restrict__ col, const double* __restrict__ Pl, int LD,
+                                                  Geometry geo, const double* __restrict__ scale, int outputs,
+                                                  double* __restrict__ pot, double* __restrict__ grad) {
+  extern __shared__ double sl[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (grp >= ngroups) return;
+  double* L = sl + warp * LD;
+  const int leaf = gnode[grp];
+  for (int i = lane; i < LD; i += 32) L[i] = Pl[(int64_t)leaf * LD + i];
+  __syncwarp();
+  const int4 c = cell[leaf];
+  const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
+  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const int t0 = gstart[grp], nt = gcount[grp];
+  for (int base = 0; base < nt; base += 32) {
+    const int k = t0 + base + lane;
+    const bool act = base + lane < nt;
+    const double x = act ? tx[k] : cx, y = act ? ty[k] : cy, z = act ? tz[k] : cz;
+    double u, gx, gy, gz;
+    l2p_f64<P>(L, (x - cx) * s, (y - cy) * s, (z - cz) * s, u, gx, gy, gz);
+    double np = 0, nx = 0, ny = 0, nz = 0;
+#pragma unroll 1
+    for (int kk = 0; kk < NCOL; ++kk) {
+      const int cn = col[(int64_t)leaf * NCOL + kk];
+      if (cn < 0) continue;
+      const int j1 = phi[cn];
+      for (int j = plo[cn]; j <= j1; ++j) {
+        const double dx = x - xs[j], dy = y - ys[j], dz = z - zs[j];
+        const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+        double ir = rsqrt(r2);
+        if (SELF && j == k) ir = 0.0;
+        const double qir = q[j] * ir;
+        const double qir3 = qir * ir * ir;
+        np += qir;
+        nx = fma(qir3, dx, nx);
+        ny = fma(qir3, dy, ny);
+        nz = fma(qir3, dz, nz);
+      }
+    }
+    if (act) {
+      const int o = tout[k];
+      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = u + KC * np;
+      if (outputs & FMMB_OUTPUT_GRADIENT) {
+        grad[3 * (int64_t)o] = gx * s - KC * nx;
+        grad[3 * (int64_t)o + 1] = gy * s - KC * ny;
+        grad[3 * (int64_t)o + 2] = gz * s - KC * nz;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- locate and bucketing
+__global__ void k_locate(const double* __restrict__ tg, int64_t nt, const int4* __restrict__ cell,
+                         const int* __restrict__ cf, const uint8_t* __restrict__ flags, Geometry geo,
+                         uint64_t* __restrict__ keys, uint32_t* __restrict__ idx, int* __restrict__ bad) {
+  int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nt) return;
+  double x[3] = {tg[3 * q], tg[3 * q + 1], tg[3 * q + 2]};
+  bool inside = true;
+  for (int d = 0; d < 3; ++d) inside = inside && geo.origin[d] <= x[d] && x[d] <= geo.origin[d] + geo.W0;
+  int i = 0;
+  if (!inside) { atomicExch(bad, 1); i = 0; }
+  else {
+    while (!(flags[i] & F_LEAF)) {
+      int4 c = cell[i];
+      double w = ldexp(geo.W0, -c.w);
+      int k = (x[0] > geo.center(0, c.x, w)) | ((x[1] > geo.center(1, c.y, w)) << 1) | ((x[2] > geo.center(2, c.z, w)) << 2);
+      i = cf[i] + k;
+    }
+  }
+  keys[q] = ((uint64_t)i << 32) | (uint64_t)q;
+  idx[q] = (uint32_t)q;
+}
+
+__global__ void k_bucket_gather(const uint64_t* __restrict__ keys, int64_t nt, const double* __restrict__ tg,
+                                double* __restrict__ tx, double* __restrict__ ty, double* __restrict__ tz,
+                                int* __restrict__ tout, int* __restrict__ start_flag) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nt) return;
+  uint64_t key = keys[k];
+  int64_t q = (int64_t)(uint32_t)key;
+  tx[k] = tg[3 * q];
+  ty[k] = tg[3 * q + 1];
+  tz[k] = tg[3 * q + 2];
+  tout[k] = (int)q;
+  start_flag[k] = (k == 0) || ((keys[k - 1] >> 32) != (key >> 32));
+}
+
+__global__ void k_groups(const uint64_t* __restrict__ keys, const int* __restrict__ start_flag, const int* __restrict__ pos,
+                         int64_t nt, int ng, int* __restrict__ gnode, int* __restrict__ gstart, int* __restrict__ gcount) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nt || !start_flag[k]) return;
+  int g = pos[k];
+  gnode[g] = (int)(keys[k] >> 32);
+  gstart[g] = (int)k;
+  // the count: up to the next start
+  int64_t e = k + 1;
+  while (e < nt && !start_flag[e]) ++e;
+  gcount[g] = (int)(e - k);
+}
+
+// ---------------------------------------------------------------- bounds
+__global__ void k_bounds(const double* __restrict__ xyz, int64_t n, double* __restrict__ out, unsigned long long* __restrict__ bad) {
+  __shared__ double s[6][256];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  unsigned long long nb = 0;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+    for (int d = 0; d < 3; ++d) {
+      double v = xyz[3 * j + d];
+      if (!isfinite(v)) { ++nb; continue; }
+      lo[d] = fmin(lo[d], v);
+      hi[d] = fmax(hi[d], v);
+    }
+  for (int d = 0; d < 3; ++d) { s[d][threadIdx.x] = lo[d]; s[3 + d][threadIdx.x] = hi[d]; }
+  if (nb) atomicAdd(bad, nb);
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (threadIdx.x < h)
+      for (int d = 0; d < 3; ++d) {
+        s[d][threadIdx.x] = fmin(s[d][threadIdx.x], s[d][threadIdx.x + h]);
+        s[3 + d][threadIdx.x] = fmax(s[3 + d][threadIdx.x], s[3 + d][threadIdx.x + h]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) out[blockIdx.x * 6 + threadIdx.x] = s[threadIdx.x][0];
+}
+
+// ---------------------------------------------------------------- direct sums, FP64
+constexpr int DT = 128;  // targets per CTA and sources per shared-memory tile
+__global__ void __launch_bounds__(DT) k_direct(const double* __restrict__ src, const double* __restrict__ tau, int64_t ns,
+                                               const double* __restrict__ tgt, const int64_t* __restrict__ self_idx,
+                                               int64_t nt, int nsplit, double* __restrict__ part) {
+  __shared__ double sx[DT], sy[DT], sz[DT], sq[DT];
+  int64_t t = (int64_t)blockIdx.x * DT + threadIdx.x;
+  int sp = blockIdx.y;
+  int64_t s0 = ns * sp / nsplit, s1 = ns * (sp + 1) / nsplit;
+  bool act = t < nt;
+  double x = act ? tgt[3 * t] : 0, y = act ? tgt[3 * t + 1] : 0, z = act ? tgt[3 * t + 2] : 0;
+  int64_t me = (act && self_idx) ? self_idx[t] : -1;
+  double u = 0, gx = 0, gy = 0, gz = 0;
+  for (int64_t b = s0; b < s1; b += DT) {
+    __syncthreads();
+    int64_t j = b + threadIdx.x;
+    if (j < s1) { sx[threadIdx.x] = src[3 * j]; sy[threadIdx.x] = src[3 * j + 1]; sz[threadIdx.x] = src[3 * j + 2]; sq[threadIdx.x] = tau[j]; }
+    __syncthreads();
+    int m = (int)min((int64_t)DT, s1 - b);
+    for (int i = 0; i < m; ++i) {
+      double dx = x - sx[i], dy = y - sy[i], dz = z - sz[i];
+      double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+      double ir = (b + i == me) ? 0.0 : 1.0 / sqrt(r2);
+      double qi = sq[i] * ir, qi3 = qi * ir * ir;
+      u += qi; gx += qi3 * dx; gy += qi3 * dy; gz += qi3 * dz;
+    }
+  }
+  if (act) {
+    double* o = part + ((int64_t)sp * nt + t) * 4;
+    o[0] = u; o[1] = gx; o[2] = gy; o[3] = gz;
+  }
+}
+
+__global__ void k_direct_reduce(const double* __restrict__ part, int64_t nt, int nsplit, double* __restrict__ pot,
+                                double* __restrict__ grad) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  double u = 0, gx = 0, gy = 0, gz = 0;
+  for (int sp = 0; sp < nsplit; ++sp) {
+    const double* o = part + ((int64_t)sp * nt + t) * 4;
+    u += o[0]; gx += o[1]; gy += o[2]; gz += o[3];
+  }
+  if (pot) pot[t] = KC * u;
+  if (grad) { grad[3 * t] = -KC * gx; grad[3 * t + 1] = -KC * gy; grad[3 * t + 2] = -KC * gz; }
+}
+
+template <int P>
+void launch_p2m(State& S) {
+  Plan& P_ = *S.plan;
+  int nth = P_.n_s2m * (P + 1);
+  if (nth == 0) return;
+  k_p2m<P><<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p, S.ys.p,
+                                                     S.zs.p, S.q.p, geometry(P_), P_.d_scale.p, P_.cache->ld, S.M.p);
+  FMMB_LAUNCH_CHECK();
+}
+
+template <int P, bool SELF>
+void launch_eval_f64(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
+                     const double* ty, const double* tz, const int* tout, int outputs, double* pot, double* grad) {
+  Plan& P_ = *S.plan;
+  if (ng == 0) return;
+  const int warps = 8;
+  size_t smem = sizeof(double) * warps * P_.cache->ld;
+  k_eval_f64<P, SELF><<<(ng + warps - 1) / warps, 32 * warps, smem, P_.ctx->stream>>>(
+      gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p, S.zs.p, S.q.p, P_.cell.p, P_.plo.p, P_.phi.p, P_.col.p,
+      S.Pl.p, P_.cache->ld, geometry(P_), P_.d_scale.p, outputs, pot, grad);
+  FMMB_LAUNCH_CHECK();
+}
+
+template <int LD, int NB>
+void launch_m2l_f64(State& S) {
+  Plan& P_ = *S.plan;
+  Cache& C = *P_.cache;
+  int nb = (int)P_.h_blocks.size();
+  if (nb == 0) return;
+  size_t smem = sizeof(double) * (16 * LD + 16 * NB + NB * (LD + 1)) + sizeof(int) * 3 * NB;
+  auto kern = k_m2l_f64<LD, NB>;
+  FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<nb, 256, smem, P_.ctx->stream>>>(P_.blocks.p, P_.cls_off.p, P_.pairs.p, C.reps.p, C.gidx.p, C.gsgn.p, C.sidx.p,
+                                          C.ssgn.p, P_.d_m2l_scale.p, C.np, S.M.p, S.Pl.p);
+  FMMB_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+Geometry geometry(const Plan& P) {
+  Geometry g;
+  for (int d = 0; d < 3; ++d) g.origin[d] = P.origin[d];
+  g.W0 = P.W0;
+  return g;
+}
+
+void upload_operators(Cache& C) {
+  cudaStream_t s = C.ctx->stream;
+  const HostOperators& h = C.host;
+  to_device(C.m2m, h.m2m, s);
+  to_device(C.l2l, h.l2l, s);
+  to_device(C.reps, h.reps, s);
+  to_device(C.tables, h.tables, s);
+  to_device(C.gidx, h.gidx, s);
+  to_device(C.gsgn, h.gsgn, s);
+  to_device(C.sidx, h.sidx, s);
+  to_device(C.ssgn, h.ssgn, s);
+  to_device(C.cls, h.cls, s);
+  FMMB_CUDA(cudaStreamSynchronize(s));
+  C.uploaded = true;
+}
+
+void gather_inputs(State& S, const double* xyz_dev, const double* tau_dev) {
+  Plan& P = *S.plan;
+  k_gather_inputs<<<nblk(P.N), 256, 0, P.ctx->stream>>>(xyz_dev, tau_dev, P.perm.p, P.N, S.xs.p, S.ys.p, S.zs.p, S.q.p);
+  FMMB_LAUNCH_CHECK();
+}
+
+#define FMMB_P_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20)
+
+int p2m(State& S) {
+  switch (S.plan->cache->p) {
+#define X(p) case p: launch_p2m<p>(S); break;
+    FMMB_P_CASES(X)
+#undef X
+    default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
+  }
+  return S.plan->n_s2m > 0;
+}
+
+int m2m_sweep(State& S) {
+  Plan& P = *S.plan;
+  Cache& C = *P.cache;
+  cudaStream_t s = P.ctx->stream;
+  int launches = 0;
+  for (int l = P.L - 2; l >= 2; --l) {
+    int c0 = P.level_start[l + 1], ng = (P.level_start[l + 2] - c0) / NCH;
+    if (ng == 0) continue;
+    ColMap bm{S.M.p, nullptr, c0, NCH}, cm{S.M.p, P.group_parent[l + 1].p, 0, 0};
+    dim3 grid((ng + 63) / 64, (C.ld + 63) / 64);
+    k_gemm_cols<<<grid, 256, 0, s>>>(C.ld, NCH * C.ld, C.m2m.p, bm, cm, ng, C.ld, C.np, 0);
+    FMMB_LAUNCH_CHECK();
+    ++launches;
+  }
+  return launches;
+}
+
+void upward_pass(State& S) {
+  p2m(S);
+  m2m_sweep(S);
+}
+
+void m2l_f64(State& S) {
+  switch (S.plan->cache->ld) {
+    case 64: launch_m2l_f64<64, 64>(S); break;
+    case 128: launch_m2l_f64<128, 64>(S); break;
+    case 192: launch_m2l_f64<192, 32>(S); break;
+    case 256: launch_m2l_f64<256, 32>(S); break;
+    case 320: launch_m2l_f64<320, 16>(S); break;
+    case 384: launch_m2l_f64<384, 16>(S); break;
+    case 448: launch_m2l_f64<448, 16>(S); break;
+    default: throw Error(FMMB_ERR_UNSUPPORTED, "no M2L kernel for this expansion length");
+  }
+}
+
+int l2l_sweep(State& S) {
+  Plan& P = *S.plan;
+  Cache& C = *P.cache;
+  cudaStream_t s = P.ctx->stream;
+  int launches = 0;
+  for (int l = 3; l < P.L; ++l) {
+    int c0 = P.level_start[l], ng = (P.level_start[l + 1] - c0) / NCH;
+    if (ng == 0) continue;
+    ColMap bm{S.Pl.p, P.group_parent[l].p, 0, 0}, cm{S.Pl.p, nullptr, c0, NCH};
+    dim3 grid((ng + 63) / 64, (NCH * C.ld + 63) / 64);
+    k_gemm_cols<<<grid, 256, 0, s>>>(NCH * C.ld, C.ld, C.l2l.p, bm, cm, ng, C.ld, C.np, 1);
+    FMMB_LAUNCH_CHECK();
+    ++launches;
+  }
+  return launches;
+}
+
+// the partial locals zeroed, then the M2L of every level in one launch (plus the FP32
+// copy of the multipoles on the mixed path); returns the kernel launches
+int m2l_stage(State& S) {
+  Plan& P = *S.plan;
+  FMMB_CUDA(cudaMemsetAsync(S.Pl.p, 0, S.Pl.bytes(), P.ctx->stream));
+  if (P.h_blocks.empty()) return 0;
+  if (S.precision == FMMB_PRECISION_MIXED) {
+    m2l_mixed(S);
+    return 2;
+  }
+  m2l_f64(S);
+  return 1;
+}
+
+void downward_pass(State& S) {
+  m2l_stage(S);
+  l2l_sweep(S);
+}
+
+void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
+                     const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad) {
+  int p = S.plan->cache->p;
+  if (S.precision == FMMB_PRECISION_MIXED) {
+    eval_mixed(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, self, outputs, pot, grad);
+    return;
+  }
+  switch (p) {
+#define X(pp) case pp: if (self) launch_eval_f64<pp, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad); \
+                       else launch_eval_f64<pp, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad); break;
+    FMMB_P_CASES(X)
+#undef X
+    default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
+  }
+}
+
+void evaluate_sources(State& S, int outputs, double* pot, double* grad) {
+  Plan& P = *S.plan;
+  evaluate_groups(S, P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, S.xs.p, S.ys.p, S.zs.p, P.perm.p, true, outputs,
+                  pot, grad);
+}
+
+void evaluate_targets(State& S, const double* tg, int64_t nt, int outputs, double* pot, double* grad) {
+  Plan& P = *S.plan;
+  cudaStream_t s = P.ctx->stream;
+  if (nt == 0) return;
+  require(nt < (1ll << 31) - 1, FMMB_ERR_ARGUMENT, "too many targets");
+  if ((int64_t)S.t_x.n < nt) {
+    S.t_x.alloc(nt); S.t_y.alloc(nt); S.t_z.alloc(nt); S.t_out.alloc(nt); S.t_node.alloc(nt);
+    S.t_keys.alloc(nt); S.t_vals.alloc(nt); S.t_groups.alloc(3 * nt + 3);
+  }
+  DBuf<int> bad(1), pos(nt);
+  FMMB_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+  k_locate<<<nblk(nt), 256, 0, s>>>(tg, nt, P.cell.p, P.cf.p, P.flags.p, geometry(P), S.t_keys.p, S.t_vals.p, bad.p);
+  FMMB_LAUNCH_CHECK();
+  require(read_one(bad.p, s) == 0, FMMB_ERR_ARGUMENT, "a target lies outside the tree's box");
+  int nbits = 1;
+  while ((1ll << nbits) < (int64_t)P.nnodes) ++nbits;
+  radix_sort_pairs(S.t_keys.p, S.t_vals.p, nt, 32 + nbits, s);
+  k_bucket_gather<<<nblk(nt), 256, 0, s>>>(S.t_keys.p, nt, tg, S.t_x.p, S.t_y.p, S.t_z.p, S.t_out.p, S.t_node.p);
+  FMMB_LAUNCH_CHECK();
+  int ng = (int)scan_exclusive_total(S.t_node.p, pos.p, nt, s);
+  int* gnode = S.t_groups.p;
+  int* gstart = gnode + ng;
+  int* gcount = gstart + ng;
+  k_groups<<<nblk(nt), 256, 0, s>>>(S.t_keys.p, S.t_node.p, pos.p, nt, ng, gnode, gstart, gcount);
+  FMMB_LAUNCH_CHECK();
+  evaluate_groups(S, gnode, gstart, gcount, ng, S.t_x.p, S.t_y.p, S.t_z.p, S.t_out.p, false, outputs, pot, grad);
+  FMMB_CUDA(cudaStreamSynchronize(s));
+}
+
+void bounds(Ctx& ctx, const double* xyz, int64_t n, double lo[3], double hi[3], int64_t* nonfinite) {
+  cudaStream_t s = ctx.stream;
+  int nb = (int)std::min<int64_t>(std::max<int64_t>(1, (n + 255) / 256), 4 * ctx.num_sms);
+  DBuf<double> out((size_t)nb * 6);
+  DBuf<unsigned long long> bad(1);
+  FMMB_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(unsigned long long), s));
+  k_bounds<<<nb, 256, 0, s>>>(xyz, n, out.p, bad.p);
+  FMMB_LAUNCH_CHECK();
+  std::vector<double> h = to_host(out.p, (size_t)nb * 6, s);
+  *nonfinite = (int64_t)read_one(bad.p, s);
+  for (int d = 0; d < 3; ++d) { lo[d] = INFINITY; hi[d] = -INFINITY; }
+  for (int b = 0; b < nb; ++b)
+    for (int d = 0; d < 3; ++d) { lo[d] = std::min(lo[d], h[b * 6 + d]); hi[d] = std::max(hi[d], h[b * 6 + 3 + d]); }
+}
+
+void direct(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
+            int64_t nt, double* pot, double* grad) {
+  cudaStream_t s = ctx.stream;
+  if (nt == 0) return;
+  int tb = (int)((nt + DT - 1) / DT);
+  int nsplit = std::max(1, std::min<int>(256, (4 * ctx.num_sms + tb - 1) / tb));
+  DBuf<double> part((size_t)nsplit * nt * 4);
+  k_direct<<<dim3(tb, nsplit), DT, 0, s>>>(src, tau, ns, tgt, self_idx, nt, nsplit, part.p);
+  FMMB_LAUNCH_CHECK();
+  k_direct_reduce<<<nblk(nt), 256, 0, s>>>(part.p, nt, nsplit, pot, grad);
+  FMMB_LAUNCH_CHECK();
+  FMMB_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace fmmb

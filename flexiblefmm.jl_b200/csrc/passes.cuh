@@ -1,0 +1,96 @@
+// Declarations shared by the pass kernels (passes.cu, m2l_tc.cu, eval_mixed.cu).
+#pragma once
+#include "plan.cuh"
+
+namespace fmmb {
+
+constexpr double KC = 0.079577471545947667884;  // 1/(4π), the Laplace3D constant (src/kernels.jl:182)
+__host__ __device__ constexpr int tri(int n, int m) { return n * (n + 1) / 2 + m; }
+constexpr int TRI_MAX = PMAX * (PMAX + 1) / 2 + PMAX + 1;
+
+// the root box; centres formed exactly as the tree builder forms them
+struct Geometry {
+  double origin[3];
+  double W0;
+  __device__ __forceinline__ double center(int d, int c, double w) const {
+    return __dadd_rn(origin[d], __dmul_rn(__dadd_rn((double)c, 0.5), w));
+  }
+};
+Geometry geometry(const Plan& P);
+
+extern __constant__ double c_tab[5 * TRI_MAX];
+extern __constant__ double c_e[PMAX];
+void init_device_constants(cudaStream_t s);
+
+// L2P at x̂ (potential and the gradient before the 1/w factor) from the local L in shared
+// memory; the orders run as a loop (a full unroll keeps too many coefficients in registers)
+template <int P>
+__device__ __forceinline__ void l2p_f64(const double* __restrict__ L, double x, double y, double z, double& u, double& gx,
+                                        double& gy, double& gz) {
+  double r2 = x * x + y * y + z * z;
+  double sr = 1.0, si = 0.0;
+  u = 0; gx = 0; gy = 0; gz = 0;
+#pragma unroll 1
+  for (int m = 0; m <= P; ++m) {
+    double pr = 0, pi = 0, cr = sr, ci = si;
+#pragma unroll 2
+    for (int n = m; n <= P; ++n) {
+      double vr, vi;
+      if (n == m) { vr = sr; vi = si; }
+      else {
+        const int t = tri(n, m);
+        double az = c_tab[t] * z, br = c_tab[TRI_MAX + t] * r2;
+        vr = az * cr - br * pr; vi = az * ci - br * pi;
+        pr = cr; pi = ci; cr = vr; ci = vi;
+      }
+      // potential: Σ L_n^m conj Υ̃ (harmonics.jl:455-462)
+      if (m == 0) u += L[n * n] * vr;
+      else u += 2 * (L[n * n + 2 * m - 1] * vr + L[n * n + 2 * m] * vi);
+      // gradient from degree n + 1 (harmonics.jl:465-486)
+      if (n < P) {
+        const int n1 = n + 1;
+        if (m == 0) {
+          double cmv = c_tab[3 * TRI_MAX + tri(n1, 1)];
+          double lr = L[n1 * n1 + 1], li = L[n1 * n1 + 2];
+          gx += -cmv * lr * vr;
+          gy += -cmv * li * vr;
+          gz += c_tab[2 * TRI_MAX + tri(n1, 0)] * L[n1 * n1] * vr;
+        } else {
+          double ur = L[n1 * n1 + 2 * (m + 1) - 1], ui = L[n1 * n1 + 2 * (m + 1)];
+          double dr, di;
+          if (m == 1) { dr = L[n1 * n1]; di = 0.0; }
+          else { dr = L[n1 * n1 + 2 * (m - 1) - 1]; di = L[n1 * n1 + 2 * (m - 1)]; }
+          double cu = 0.5 * c_tab[3 * TRI_MAX + tri(n1, m + 1)], cd = 0.5 * c_tab[4 * TRI_MAX + tri(n1, m - 1)];
+          double axr = -cu * ur + cd * dr, axi = -cu * ui + cd * di;
+          double ayr = -(cu * ui + cd * di), ayi = cu * ur + cd * dr;
+          double czv = c_tab[2 * TRI_MAX + tri(n1, m)];
+          double zr = L[n1 * n1 + 2 * m - 1], zi = L[n1 * n1 + 2 * m];
+          gx += 2 * (axr * vr + axi * vi);
+          gy += 2 * (ayr * vr + ayi * vi);
+          gz += 2 * czv * (zr * vr + zi * vi);
+        }
+      }
+    }
+    if (m < P) {
+      double e = c_e[m];
+      double nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
+      sr = nr; si = ni;
+    }
+  }
+}
+
+void m2l_f64(State& S);
+int p2m(State& S);          // the stages of the passes; each returns its kernel launches
+int m2m_sweep(State& S);
+int m2l_stage(State& S);
+int l2l_sweep(State& S);
+void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
+                     const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad);
+// the mixed path (m2l_tc.cu, eval_mixed.cu)
+void prepare_mixed_operators(Cache& C);
+void m2l_mixed(State& S);
+int mixed_error_flag(State& S);   // 1 when a bounded wait of the tensor-core M2L gave up
+void eval_mixed(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
+                const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad);
+
+}  // namespace fmmb

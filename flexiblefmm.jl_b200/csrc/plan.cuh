@@ -1,0 +1,110 @@
+// The context, operator cache, plan (tree + lists) and state (expansions) of the library.
+#pragma once
+#include <memory>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace fmmb {
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 148;
+};
+
+// OperatorCache (src/operators/cache.jl:5-83): the base width, the host operators at the base
+// width and their device copies, shared by every plan built with the cache.
+struct Cache {
+  Ctx* ctx = nullptr;
+  int p = 0, np = 0, ld = 0;
+  double W0 = NAN;           // base width, fixed by the first fitted box
+  std::mutex mu;             // the cache is shared by plans; fitting and uploads are locked
+  bool uploaded = false;
+  HostOperators host;
+  DBuf<double> m2m, l2l, reps, tables;
+  DBuf<int16_t> gidx, sidx;
+  DBuf<int8_t> gsgn, ssgn;
+  DBuf<int> cls;
+  // the mixed path's class operators: per class, the split (hi, lo) TF32 copies in the
+  // canonical K-major layout the tensor-core M2L reads (m2l_tc.cu)
+  DBuf<float> reps_split;
+  bool split_ready = false;
+};
+
+// One M2L work block: TB consecutive nodes of one level (the targets), their far pairs
+// grouped by symmetry class.
+struct M2LBlock {
+  int level;
+  int first;     // first node (global)
+  int count;     // nodes in the block
+  int pair_base; // first pair of the block in the plan's pair array
+};
+
+struct Plan {
+  Cache* cache = nullptr;
+  Ctx* ctx = nullptr;
+  int64_t N = 0;
+  int L = 0, nnodes = 0, KL = 21;
+  double origin[3] = {0, 0, 0}, W0 = 1;
+  int e0 = 0;                             // the plan's root width is ldexp(cache W0, e0)
+  std::vector<int> level_start;           // L + 1
+  std::vector<double> scale, m2l_scale;   // per level: 1/w, and the M2L factor W_ref / w
+  // the flat tree on the device
+  DBuf<int4> cell;                        // x, y, z, level
+  DBuf<int> parent, cf, plo, phi, col, perm, point_node;
+  DBuf<uint8_t> flags;
+  // host copies of the node arrays the host-side scheduling needs
+  std::vector<int> h_parent, h_cf, h_plo, h_phi;
+  std::vector<uint8_t> h_flags;
+  // upward: childless nodes with sources (all levels); per level the sibling-group parents
+  DBuf<int> s2m_nodes;
+  int n_s2m = 0;
+  std::vector<DBuf<int>> group_parent;    // per level l ≥ 1: parent of each sibling group
+  // evaluation: real leaves with points
+  DBuf<int> leaves, leaf_start, leaf_count;
+  int n_leaves = 0;
+  // M2L: blocks, per block the class offsets of its pairs, the pairs (src, f << 8 | target)
+  int TB = 64;
+  std::vector<M2LBlock> h_blocks;
+  DBuf<int4> blocks;
+  DBuf<int> cls_off;                      // nblocks × 35, relative to the block's pair_base
+  DBuf<int2> pairs;
+  int64_t npairs = 0;
+  std::vector<int64_t> level_pairs;       // far pairs per level
+  DBuf<double> d_scale, d_m2l_scale;      // per level
+};
+
+struct State {
+  Plan* plan = nullptr;
+  int precision = FMMB_PRECISION_FP64;
+  DBuf<double> xs, ys, zs, q;             // sources and charges in tree order
+  DBuf<double> M, Pl;                     // nnodes × LD: multipoles, partial locals
+  DBuf<float> Mf;                         // the mixed path: an FP32 copy of the multipoles
+  DBuf<int> err;                          // the mixed path: the bounded-wait error flag
+  bool built = false;
+  // staging of the host-pointer entry points and the evaluation at targets
+  DBuf<double> h_in_xyz, h_in_tau, d_pot, d_grad;
+  DBuf<double> t_x, t_y, t_z;
+  DBuf<int> t_node, t_groups, t_out;
+  DBuf<uint64_t> t_keys;
+  DBuf<uint32_t> t_vals;
+};
+
+// tree.cu
+void build_tree(Plan& P, const double* xyz_dev, int ppl, int max_levels);
+// lists.cu
+void build_lists(Plan& P);
+// passes.cu
+void upload_operators(Cache& C);
+void gather_inputs(State& S, const double* xyz_dev, const double* tau_dev);
+void upward_pass(State& S);
+void downward_pass(State& S);
+void evaluate_sources(State& S, int outputs, double* pot_dev, double* grad_dev);
+void evaluate_targets(State& S, const double* tg_dev, int64_t nt, int outputs, double* pot_dev, double* grad_dev);
+void bounds(Ctx& ctx, const double* xyz_dev, int64_t n, double lo[3], double hi[3], int64_t* nonfinite);
+void direct(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
+            int64_t nt, double* pot, double* grad);
+
+}  // namespace fmmb

@@ -1,0 +1,400 @@
+"""fmmb: the host-side mirror of FlexibleFMM.jl's API over the sm_100a C ABI (include/fmmb.h).
+
+The names, argument meanings and errors follow the reference (src/FlexibleFMM.jl:37-47):
+
+    m = SphericalHarmonics(Laplace3D(), p=10)
+    cache = OperatorCache(m)
+    f = FMM(m, points, ppl=64, bbox=((0, 0, 0), 1.0), cache=cache)   # src/fmm.jl:31-49
+    st = build_expansions(f, points, tau)                             # src/fmm.jl:306-314
+    u = evaluate_at_sources(f, st)                                    # src/evaluate.jl:111-132
+    g = evaluate(f, st, targets, output=Gradient())                   # src/evaluate.jl:81-102
+
+Points are (N, 3) float64 arrays (the memory of Vector{SVector{3,Float64}}); gradients come
+back as (N, 3). ArgumentError and DimensionMismatch mirror the reference's exceptions.
+Everything runs on the GPU through libfmmb.so; there is no CPU path, and importing this
+module fails when the library is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(os.path.dirname(_HERE), "libfmmb.so")
+
+FMMB_OK = 0
+_CODES = {1: "ArgumentError", 2: "DimensionMismatch", 3: "OutOfMemory", 4: "DeviceError", 5: "Timeout",
+          6: "Unsupported"}
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+OUTPUT_POTENTIAL = 1
+OUTPUT_GRADIENT = 2
+
+
+class FMMBError(RuntimeError):
+    """A device, memory or timeout failure reported by libfmmb."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"{_CODES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class ArgumentError(FMMBError, ValueError):
+    pass
+
+
+class DimensionMismatch(FMMBError, ValueError):
+    pass
+
+
+class Unsupported(FMMBError, NotImplementedError):
+    pass
+
+
+class _MethodDesc(C.Structure):
+    _fields_ = [("method", C.c_int32), ("kernel", C.c_int32), ("p", C.c_int32), ("reserved", C.c_int32),
+                ("tol", C.c_double)]
+
+
+class _TreeOpts(C.Structure):
+    _fields_ = [("ppl", C.c_int32), ("max_levels", C.c_int32), ("has_bbox", C.c_int32), ("reserved", C.c_int32),
+                ("origin", C.c_double * 3), ("width", C.c_double)]
+
+
+_lib = None
+EXPORTS = (
+    "fmmb_last_error", "fmmb_version", "fmmb_ctx_create", "fmmb_ctx_destroy", "fmmb_ctx_stream", "fmmb_ctx_synchronize",
+    "fmmb_cache_create", "fmmb_cache_destroy", "fmmb_cache_base_width", "fmmb_plan_create", "fmmb_plan_create_dev",
+    "fmmb_plan_destroy", "fmmb_plan_info", "fmmb_plan_box", "fmmb_plan_tree", "fmmb_plan_pairs", "fmmb_state_create",
+    "fmmb_state_destroy", "fmmb_build_expansions", "fmmb_build_expansions_dev", "fmmb_evaluate_at_sources",
+    "fmmb_evaluate_at_sources_dev", "fmmb_matvec", "fmmb_matvec_dev", "fmmb_evaluate", "fmmb_evaluate_dev",
+    "fmmb_state_expansions", "fmmb_direct_dev", "fmmb_profile_matvec",
+)
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def lib():
+    """The loaded libfmmb.so; raises if it was not built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"libfmmb.so is missing at {_LIB_PATH}: build it (python flexiblefmm.jl_b200/build.py)")
+    L = C.CDLL(_LIB_PATH)
+    vp, i64, i32, dp = C.c_void_p, C.c_int64, C.c_int, C.c_void_p
+    L.fmmb_last_error.restype = C.c_char_p
+    L.fmmb_version.restype = C.c_char_p
+    sig = {
+        "fmmb_ctx_create": [i32, C.POINTER(vp)],
+        "fmmb_ctx_destroy": [vp],
+        "fmmb_ctx_stream": [vp, C.POINTER(vp)],
+        "fmmb_ctx_synchronize": [vp],
+        "fmmb_cache_create": [vp, C.POINTER(_MethodDesc), C.POINTER(vp)],
+        "fmmb_cache_destroy": [vp],
+        "fmmb_cache_base_width": [vp, C.POINTER(C.c_double)],
+        "fmmb_plan_create": [vp, dp, i64, C.POINTER(_TreeOpts), C.POINTER(vp)],
+        "fmmb_plan_create_dev": [vp, dp, i64, C.POINTER(_TreeOpts), C.POINTER(vp)],
+        "fmmb_plan_destroy": [vp],
+        "fmmb_plan_info": [vp, dp, i32],
+        "fmmb_plan_box": [vp, dp, dp],
+        "fmmb_plan_tree": [vp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp],
+        "fmmb_plan_pairs": [vp, i32, dp, dp, dp, i64, C.POINTER(i64)],
+        "fmmb_state_create": [vp, i32, C.POINTER(vp)],
+        "fmmb_state_destroy": [vp],
+        "fmmb_build_expansions": [vp, dp, dp, i64],
+        "fmmb_build_expansions_dev": [vp, dp, dp, i64],
+        "fmmb_evaluate_at_sources": [vp, i32, dp, dp],
+        "fmmb_evaluate_at_sources_dev": [vp, i32, dp, dp],
+        "fmmb_matvec": [vp, dp, dp, i64, i32, dp, dp],
+        "fmmb_matvec_dev": [vp, dp, dp, i64, i32, dp, dp],
+        "fmmb_evaluate": [vp, dp, i64, i32, dp, dp],
+        "fmmb_evaluate_dev": [vp, dp, i64, i32, dp, dp],
+        "fmmb_state_expansions": [vp, dp, dp],
+        "fmmb_direct_dev": [vp, dp, dp, i64, dp, dp, i64, dp, dp],
+        "fmmb_profile_matvec": [vp, dp, dp, i64, i32, dp, dp, dp, i32, C.POINTER(C.c_int)],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc == FMMB_OK:
+        return
+    msg = lib().fmmb_last_error().decode()
+    cls = {1: ArgumentError, 2: DimensionMismatch, 6: Unsupported}.get(rc, FMMBError)
+    raise cls(rc, msg)
+
+
+def _ptr(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _points(x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.ndim != 2 or x.shape[1] != 3:
+        raise DimensionMismatch(2, f"expected an (N, 3) array of points, got {x.shape}")
+    return x
+
+
+# ---------------------------------------------------------------- kernels, methods, outputs
+class Laplace3D:
+    """Free-space Laplace Green's function 1/(4π|t − s|) (src/kernels.jl:179-200)."""
+    c = 1.0 / (4.0 * np.pi)
+
+
+class SphericalHarmonics:
+    """SphericalHarmonics(kernel; p=16, tol=0) (src/operators/harmonics.jl:303-308)."""
+
+    def __init__(self, kernel, p=16, tol=0.0):
+        if not isinstance(kernel, Laplace3D):
+            raise ArgumentError(1, "the device method is written for Laplace3D")
+        if p < 1:
+            raise ArgumentError(1, "p must be at least 1")
+        if not (0 <= tol < 1):
+            raise ArgumentError(1, "tol must lie in [0, 1)")
+        self.kernel, self.p, self.tol = kernel, int(p), float(tol)
+
+
+class Potential:
+    pass
+
+
+class Gradient:
+    pass
+
+
+def _output_flag(output):
+    if isinstance(output, Potential) or output is Potential:
+        return OUTPUT_POTENTIAL
+    if isinstance(output, Gradient) or output is Gradient:
+        return OUTPUT_GRADIENT
+    raise ArgumentError(1, f"output {output!r} is not available with SphericalHarmonics")
+
+
+# ---------------------------------------------------------------- device context
+class Context:
+    """One GPU and its stream (fmmb_ctx)."""
+
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        _check(lib().fmmb_ctx_create(int(device), C.byref(h)))
+        self._h = h
+        self.device = device
+
+    @property
+    def stream(self):
+        s = C.c_void_p()
+        _check(lib().fmmb_ctx_stream(self._h, C.byref(s)))
+        return s.value
+
+    def synchronize(self):
+        _check(lib().fmmb_ctx_synchronize(self._h))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.fmmb_ctx_destroy(self._h)
+            self._h = None
+
+
+_default_ctx = {}
+
+
+def default_context(device=0):
+    if device not in _default_ctx:
+        _default_ctx[device] = Context(device)
+    return _default_ctx[device]
+
+
+class OperatorCache:
+    """OperatorCache(method) (src/operators/cache.jl:19-22): shared by the plans built with it."""
+
+    def __init__(self, method, ctx=None):
+        self.method = method
+        self.ctx = ctx or default_context()
+        d = _MethodDesc(1, 1, method.p, 0, method.tol)
+        h = C.c_void_p()
+        _check(lib().fmmb_cache_create(self.ctx._h, C.byref(d), C.byref(h)))
+        self._h = h
+
+    @property
+    def W0(self):
+        w = C.c_double()
+        _check(lib().fmmb_cache_base_width(self._h, C.byref(w)))
+        return w.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.fmmb_cache_destroy(self._h)
+            self._h = None
+
+
+class FMM:
+    """FMM(method, sources; ppl=50, bbox=None, cache=OperatorCache(method), max_levels=30)
+    (src/fmm.jl:31-49): the tree built on the device, the lists and the operators."""
+
+    def __init__(self, method, sources, ppl=50, bbox=None, cache=None, max_levels=30, device_points=None):
+        cache = cache if cache is not None else OperatorCache(method)
+        if cache.method is not method:
+            raise ArgumentError(1, "the cache was built for a different method")
+        self.method, self.cache = method, cache
+        opts = _TreeOpts()
+        opts.ppl, opts.max_levels = int(ppl), int(max_levels)
+        if bbox is not None:
+            opts.has_bbox = 1
+            for d in range(3):
+                opts.origin[d] = float(bbox[0][d])
+            opts.width = float(bbox[1])
+        h = C.c_void_p()
+        if device_points is not None:           # (pointer, n) of a 3×n device array
+            ptr, n = device_points
+            _check(lib().fmmb_plan_create_dev(cache._h, C.c_void_p(ptr), int(n), C.byref(opts), C.byref(h)))
+            self.N = int(n)
+        else:
+            x = _points(sources)
+            if x.shape[0] == 0:
+                raise ArgumentError(1, "no points")
+            _check(lib().fmmb_plan_create(cache._h, _ptr(x), x.shape[0], C.byref(opts), C.byref(h)))
+            self.N = x.shape[0]
+        self._h = h
+        info = np.zeros(4 + 64, np.int64)
+        _check(lib().fmmb_plan_info(self._h, _ptr(info), len(info)))
+        self.nlevels, self.nnodes, self.npairs = int(info[0]), int(info[1]), int(info[3])
+        self.level_start = info[4:4 + self.nlevels + 1].copy()
+        o = np.zeros(3)
+        w = C.c_double()
+        _check(lib().fmmb_plan_box(self._h, _ptr(o), C.byref(w)))
+        self.origin, self.width = o, w.value
+
+    def tree(self):
+        """The flat tree as numpy arrays (node indices 0-based, -1 for none)."""
+        n, N = self.nnodes, self.N
+        t = dict(cell=np.zeros((n, 3), np.int32), level=np.zeros(n, np.int32), parent=np.zeros(n, np.int32),
+                 child_first=np.zeros(n, np.int32), plo=np.zeros(n, np.int32), phi=np.zeros(n, np.int32),
+                 flags=np.zeros(n, np.uint8), colleagues=np.zeros((n, 27), np.int32), perm=np.zeros(N, np.int32),
+                 point_node=np.zeros(N, np.int32))
+        _check(lib().fmmb_plan_tree(self._h, *[_ptr(t[k]) for k in ("cell", "level", "parent", "child_first", "plo", "phi",
+                                                                       "flags", "colleagues", "perm", "point_node")]))
+        fl = t.pop("flags")
+        t["leaf"], t["ghost"] = (fl & 1).astype(np.uint8), ((fl >> 1) & 1).astype(np.uint8)
+        t["xlist"], t["has_source"] = ((fl >> 2) & 1).astype(np.uint8), ((fl >> 3) & 1).astype(np.uint8)
+        return t
+
+    def pairs(self, level):
+        n = C.c_int64()
+        _check(lib().fmmb_plan_pairs(self._h, int(level), None, None, None, 0, C.byref(n)))
+        t, s, f = (np.zeros(n.value, np.int32) for _ in range(3))
+        if n.value:
+            _check(lib().fmmb_plan_pairs(self._h, int(level), _ptr(t), _ptr(s), _ptr(f), n.value, C.byref(n)))
+        return t, s, f
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.fmmb_plan_destroy(self._h)
+            self._h = None
+
+
+class FMMState:
+    """FMMState (src/fmm.jl:64-94): the expansions of one right-hand side on the device.
+    precision: "fp64" (the plain drop-in path) or "mixed"."""
+
+    def __init__(self, fmm, precision="fp64"):
+        self.fmm = fmm
+        self.precision = precision
+        prec = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}.get(precision)
+        if prec is None:
+            raise ArgumentError(1, f"unknown precision {precision!r}")
+        h = C.c_void_p()
+        _check(lib().fmmb_state_create(fmm._h, prec, C.byref(h)))
+        self._h = h
+
+    def expansions(self):
+        n, np_ = self.fmm.nnodes, (self.fmm.method.p + 1) ** 2
+        M = np.zeros((n, np_))
+        Lc = np.zeros((n, np_))
+        _check(lib().fmmb_state_expansions(self._h, _ptr(M), _ptr(Lc)))
+        return M, Lc
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.fmmb_state_destroy(self._h)
+            self._h = None
+
+
+def _densities(tau, n):
+    t = np.asarray(tau)
+    if np.iscomplexobj(t) or t.dtype == object or t.ndim != 1:
+        raise ArgumentError(1, f"densities of type {t.dtype} are not supported by SphericalHarmonics")
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    if t.shape[0] != n:
+        raise DimensionMismatch(2, f"expected {n} densities in group 1")
+    return t
+
+
+def build_expansions_(state, fmm, sources, tau):
+    """build_expansions!(state, fmm, sources, τ) (src/fmm.jl:270-298)."""
+    x = _points(sources)
+    if x.shape[0] != fmm.N:
+        raise DimensionMismatch(2, f"expected {fmm.N} sources in group 1")
+    t = _densities(tau, fmm.N)
+    _check(lib().fmmb_build_expansions(state._h, _ptr(x), _ptr(t), fmm.N))
+    return state
+
+
+def build_expansions(fmm, sources, tau, precision="fp64"):
+    """build_expansions(fmm, sources, τ) -> FMMState (src/fmm.jl:306-314)."""
+    return build_expansions_(FMMState(fmm, precision), fmm, sources, tau)
+
+
+def evaluate_at_sources(fmm, state, g=1, output=Potential()):
+    """evaluate_at_sources(fmm, state; output) (src/evaluate.jl:111-132), original order."""
+    if g != 1:
+        raise ArgumentError(1, f"group {g} of 1")
+    flag = _output_flag(output)
+    if flag == OUTPUT_POTENTIAL:
+        out = np.zeros(fmm.N)
+        _check(lib().fmmb_evaluate_at_sources(state._h, flag, _ptr(out), None))
+    else:
+        out = np.zeros((fmm.N, 3))
+        _check(lib().fmmb_evaluate_at_sources(state._h, flag, None, _ptr(out)))
+    return out
+
+
+def evaluate_at_sources_both(fmm, state):
+    """Potential and gradient at the sources in one pass."""
+    pot, grad = np.zeros(fmm.N), np.zeros((fmm.N, 3))
+    _check(lib().fmmb_evaluate_at_sources(state._h, 3, _ptr(pot), _ptr(grad)))
+    return pot, grad
+
+
+def evaluate(fmm, state, targets, output=Potential()):
+    """evaluate(fmm, state, targets; output) (src/evaluate.jl:81-102)."""
+    flag = _output_flag(output)
+    tg = _points(targets)
+    nt = tg.shape[0]
+    if flag == OUTPUT_POTENTIAL:
+        out = np.zeros(nt)
+        _check(lib().fmmb_evaluate(state._h, _ptr(tg), nt, flag, _ptr(out), None))
+    else:
+        out = np.zeros((nt, 3))
+        _check(lib().fmmb_evaluate(state._h, _ptr(tg), nt, flag, None, _ptr(out)))
+    return out
+
+
+def device_matvec(fmm, state, sources, tau, output=Potential()):
+    """device_matvec!(out, plan, (sources, τ)) (src/device_passes.jl:619-640)."""
+    flag = _output_flag(output)
+    x = _points(sources)
+    t = _densities(tau, fmm.N)
+    if x.shape[0] != fmm.N:
+        raise DimensionMismatch(2, f"expected {fmm.N} sources")
+    pot = np.zeros(fmm.N) if flag == OUTPUT_POTENTIAL else None
+    grad = np.zeros((fmm.N, 3)) if flag == OUTPUT_GRADIENT else None
+    _check(lib().fmmb_matvec(state._h, _ptr(x), _ptr(t), fmm.N, flag, _ptr(pot), _ptr(grad)))
+    return pot if flag == OUTPUT_POTENTIAL else grad

@@ -1,0 +1,143 @@
+/*
+ * fmmb — a B200-native (sm_100a) fast multipole backend for FlexibleFMM.jl.
+ *
+ * C ABI. Every entry point returns a status code (FMMB_OK = 0) and leaves a message
+ * for the calling thread in fmmb_last_error(). Handles are opaque; the caller owns its
+ * arrays. Host-pointer entry points copy in and out and return when the results are in
+ * host memory; `_dev` entry points take device pointers and only enqueue work on the
+ * context's stream (synchronise with fmmb_ctx_synchronize or on the stream).
+ *
+ * Layouts follow the Julia memory of the reference types: points are D×N interleaved
+ * (Vector{SVector{3,Float64}}), gradients 3×N interleaved (Vector{SVector{3,Float64}}),
+ * node arrays are 0-based with -1 for "none". Inputs and outputs are in the caller's
+ * original order; the tree order is internal (src/evaluate.jl:111-127 of the reference).
+ *
+ * Status codes map to the reference's exceptions: FMMB_ERR_ARGUMENT ↔ ArgumentError,
+ * FMMB_ERR_DIMENSION ↔ DimensionMismatch.
+ */
+#ifndef FMMB_H
+#define FMMB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FMMB_OK 0
+#define FMMB_ERR_ARGUMENT 1    /* ArgumentError: non-finite points, outside the box, max_levels, bad option */
+#define FMMB_ERR_DIMENSION 2   /* DimensionMismatch: lengths that do not match the plan */
+#define FMMB_ERR_MEMORY 3      /* device or host allocation failed */
+#define FMMB_ERR_DEVICE 4      /* a CUDA error */
+#define FMMB_ERR_TIMEOUT 5     /* a bounded device wait gave up */
+#define FMMB_ERR_UNSUPPORTED 6 /* a method, kernel, density or output this build does not provide */
+
+#define FMMB_KERNEL_LAPLACE3D 1
+#define FMMB_METHOD_SPHERICAL_HARMONICS 1
+
+#define FMMB_PRECISION_FP64 0  /* the plain path: FP64 everywhere (the drop-in) */
+#define FMMB_PRECISION_MIXED 1 /* split-precision tensor-core M2L, FP32 compensated near field */
+
+#define FMMB_OUTPUT_POTENTIAL 1 /* bit flags; both may be requested in one call */
+#define FMMB_OUTPUT_GRADIENT 2
+
+typedef struct fmmb_ctx fmmb_ctx;
+typedef struct fmmb_cache fmmb_cache;
+typedef struct fmmb_plan fmmb_plan;
+typedef struct fmmb_state fmmb_state;
+
+/* The method: SphericalHarmonics(Laplace3D(); p) (src/operators/harmonics.jl:303-308). */
+typedef struct {
+  int32_t method;  /* FMMB_METHOD_SPHERICAL_HARMONICS */
+  int32_t kernel;  /* FMMB_KERNEL_LAPLACE3D */
+  int32_t p;       /* expansion degree, 1..20 */
+  int32_t reserved;
+  double tol;      /* 0: dense class operators (the only form this build provides) */
+} fmmb_method_desc;
+
+/* Tree options: FMM(m, sources; ppl, bbox, max_levels) (src/fmm.jl:31-49). */
+typedef struct {
+  int32_t ppl;        /* points per leaf; a node with more is split */
+  int32_t max_levels; /* the reference default is 30 */
+  int32_t has_bbox;   /* 0: the points' own square box (square_bbox) */
+  int32_t reserved;
+  double origin[3];   /* bbox = (origin, width) */
+  double width;
+} fmmb_tree_opts;
+
+const char* fmmb_last_error(void);
+const char* fmmb_version(void);
+
+/* A device context: one GPU, one stream, the device-side scratch of the entry points. */
+int fmmb_ctx_create(int device, fmmb_ctx** out);
+int fmmb_ctx_destroy(fmmb_ctx* ctx);
+int fmmb_ctx_stream(fmmb_ctx* ctx, void** stream); /* the cudaStream_t all work goes to */
+int fmmb_ctx_synchronize(fmmb_ctx* ctx);
+
+/* OperatorCache(method) (src/operators/cache.jl:19-22): operators by box width, their device
+ * copies shared by every plan built with the cache. The first plan fixes the base width. */
+int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* method, fmmb_cache** out);
+int fmmb_cache_destroy(fmmb_cache* cache);
+int fmmb_cache_base_width(const fmmb_cache* cache, double* width); /* NaN until a box was fitted */
+
+/* FMM(method, sources; ppl, bbox, cache, max_levels) (src/fmm.jl:31-49) and
+ * DevicePlan(m, xs; ...) (src/device_passes.jl:112-134): the tree of the points, built on
+ * the device, the box snapped by fit_box! (src/operators/cache.jl:57-83), the interaction
+ * lists and the operators of every level. xyz: 3×n interleaved. */
+int fmmb_plan_create(fmmb_cache* cache, const double* xyz, int64_t n, const fmmb_tree_opts* opts, fmmb_plan** out);
+int fmmb_plan_create_dev(fmmb_cache* cache, const double* xyz_dev, int64_t n, const fmmb_tree_opts* opts, fmmb_plan** out);
+int fmmb_plan_destroy(fmmb_plan* plan);
+/* info[0] = levels, info[1] = nodes, info[2] = points, info[3] = far pairs,
+ * info[4 .. 4+levels] = first node of each level and the node count (cap: entries of info). */
+int fmmb_plan_info(const fmmb_plan* plan, int64_t* info, int cap);
+int fmmb_plan_box(const fmmb_plan* plan, double* origin3, double* width);
+/* The flat tree (src/tree/tree.jl:40-71), downloaded: any pointer may be NULL.
+ * cell 3×nnodes, level (0 = root), parent, child_first, plo/phi (0-based inclusive point
+ * range, phi < plo when empty), flags (bit 0 leaf, 1 ghost, 2 xlist, 3 has_source),
+ * colleagues 27×nnodes, perm (sorted position → original index), point_node. */
+int fmmb_plan_tree(const fmmb_plan* plan, int32_t* cell, int32_t* level, int32_t* parent, int32_t* child_first,
+                   int32_t* plo, int32_t* phi, uint8_t* flags, int32_t* colleagues, int32_t* perm, int32_t* point_node);
+/* The far pairs of one level as (target node, source node, far offset index) in an
+ * unspecified order (src/tree/lists.jl:15-70); returns the count in *npairs. */
+int fmmb_plan_pairs(const fmmb_plan* plan, int level, int32_t* tgt, int32_t* src, int32_t* far, int64_t cap, int64_t* npairs);
+
+/* FMMState (src/fmm.jl:64-94): the expansions of one right-hand side, in a precision path. */
+int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out);
+int fmmb_state_destroy(fmmb_state* state);
+
+/* build_expansions!(state, fmm, sources, τ) (src/fmm.jl:270-298) with charges τ. */
+int fmmb_build_expansions(fmmb_state* state, const double* xyz, const double* tau, int64_t n);
+int fmmb_build_expansions_dev(fmmb_state* state, const double* xyz_dev, const double* tau_dev, int64_t n);
+/* evaluate_at_sources!(out, fmm, state; output) (src/evaluate.jl:111-127): pot (n) and/or
+ * grad (3×n) in the original order, self excluded. */
+int fmmb_evaluate_at_sources(fmmb_state* state, int outputs, double* pot, double* grad);
+int fmmb_evaluate_at_sources_dev(fmmb_state* state, int outputs, double* pot_dev, double* grad_dev);
+/* device_matvec! (src/device_passes.jl:619-640): build_expansions then evaluate_at_sources. */
+int fmmb_matvec(fmmb_state* state, const double* xyz, const double* tau, int64_t n, int outputs, double* pot, double* grad);
+int fmmb_matvec_dev(fmmb_state* state, const double* xyz_dev, const double* tau_dev, int64_t n, int outputs,
+                    double* pot_dev, double* grad_dev);
+/* evaluate!(out, fmm, state, targets; output) (src/evaluate.jl:81-96): targets 3×nt, located
+ * on the device (src/tree/locate.jl:10-22). */
+int fmmb_evaluate(fmmb_state* state, const double* targets, int64_t nt, int outputs, double* pot, double* grad);
+int fmmb_evaluate_dev(fmmb_state* state, const double* targets_dev, int64_t nt, int outputs, double* pot_dev, double* grad_dev);
+/* One device matvec (fmmb_matvec_dev) with CUDA events between its stages, on the context's
+ * stream, synchronised: stage_ms[0..5] = gather, P2M, M2M, M2L (with the zeroing of the partial
+ * locals and, on the mixed path, the FP32 copy of the multipoles), L2L, evaluation (L2P + P2P).
+ * *launches = the kernels launched (the reference times the same phases: bench/bench.jl:44-56). */
+int fmmb_profile_matvec(fmmb_state* state, const double* xyz_dev, const double* tau_dev, int64_t n, int outputs,
+                        double* pot_dev, double* grad_dev, double* stage_ms, int cap, int* launches);
+/* The multipoles and locals of the last build (nnodes × (p+1)² each, node order, the real
+ * storage of src/operators/harmonics.jl:20-27; locals are zero outside the real leaves). */
+int fmmb_state_expansions(const fmmb_state* state, double* multipoles, double* locals);
+
+/* direct!(out, K, sources, τ, targets) / direct_self! (src/kernels.jl:463-487) for Laplace3D on
+ * the device in FP64, device pointers: sources 3×ns, targets 3×nt. self_index (device, may be
+ * NULL): per target, the source index it excludes (-1 for none). */
+int fmmb_direct_dev(fmmb_ctx* ctx, const double* src_dev, const double* tau_dev, int64_t ns, const double* tgt_dev,
+                    const int64_t* self_index_dev, int64_t nt, double* pot_dev, double* grad_dev);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMMB_H */

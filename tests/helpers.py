@@ -1,0 +1,159 @@
+"""Point distributions and structural checks for the tests, restating the reference's
+test utilities (test/testutils.jl:1-76) and tree invariants (test/test_tree.jl:7-131)."""
+import numpy as np
+
+# ---------------------------------------------------------------- distributions (test/testutils.jl:50-76)
+def uniform3(rng, n):
+    return rng.random((n, 3))
+
+
+def clustered3(rng, n, nclusters=10, spread=0.01):
+    c = 0.1 + 0.8 * rng.random((nclusters, 3))
+    x = c[np.arange(n) % nclusters] + spread * rng.standard_normal((n, 3))
+    return np.clip(x, 0.0, 1.0)
+
+
+def sphere3(rng, n, center=(0.5, 0.5, 0.5), radius=0.4):
+    v = rng.standard_normal((n, 3))
+    return np.asarray(center) + radius * v / np.linalg.norm(v, axis=1)[:, None]
+
+
+def helix3(rng, n):
+    th = 6 * np.pi * rng.random(n)
+    x = np.stack([0.5 + 0.3 * np.cos(th), 0.5 + 0.3 * np.sin(th), 0.05 + 0.9 * th / (6 * np.pi)], axis=1)
+    return np.clip(x + 1e-3 * rng.standard_normal((n, 3)), 0.0, 1.0)
+
+
+def one_octant3(rng, n):
+    return 0.3 * rng.random((n, 3))
+
+
+def mixed3(rng, n):
+    ns, nk = n // 2, n // 4
+    s = sphere3(rng, ns, radius=0.3)
+    k = np.clip(0.9 + 0.002 * rng.standard_normal((nk, 3)), 0.0, 1.0)
+    return np.vstack([s, k, uniform3(rng, n - ns - nk)])
+
+
+DISTRIBUTIONS3 = dict(uniform=uniform3, clustered=clustered3, sphere=sphere3, helix=helix3, one_octant=one_octant3,
+                      mixed=mixed3)
+
+
+def mrd(a, b):
+    """max-norm relative difference (test/testutils.jl:9)"""
+    a, b = np.asarray(a), np.asarray(b)
+    if a.ndim == 2:
+        return np.max(np.linalg.norm(a - b, axis=1)) / np.max(np.linalg.norm(b, axis=1))
+    return np.max(np.abs(a - b)) / np.max(np.abs(b))
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+# ---------------------------------------------------------------- tree invariants (test/test_tree.jl:7-131)
+def child_slot(x, c):
+    return (x[..., 0] > c[..., 0]).astype(int) | ((x[..., 1] > c[..., 1]).astype(int) << 1) | \
+           ((x[..., 2] > c[..., 2]).astype(int) << 2)
+
+
+def centers(t, origin, W0):
+    w = np.ldexp(W0, -t["level"].astype(int))
+    return np.asarray(origin) + (t["cell"] + 0.5) * w[:, None]
+
+
+def check_tree_invariants(t, pts, origin=(0.0, 0.0, 0.0), W0=1.0):
+    """Every structural invariant of the ghost-cell tree, brute force. `t` is a dict of
+    arrays with 0-based indices (-1 for none)."""
+    N = pts.shape[0]
+    n = len(t["level"])
+    perm = t["perm"]
+    assert sorted(perm) == list(range(N))
+    sp = pts[perm]
+    lev = t["level"]
+    assert lev[0] == 0 and t["parent"][0] == -1 and tuple(t["cell"][0]) == (0, 0, 0)
+    assert np.all(np.diff(lev) >= 0)
+    assert t["plo"][0] == 0 and t["phi"][0] == N - 1
+    leaf, ghost, xlist, hs = (t[k].astype(bool) for k in ("leaf", "ghost", "xlist", "has_source"))
+    cf = t["child_first"]
+    w = np.ldexp(W0, -lev.astype(int))
+    assert np.all((t["cell"] >= 0) & (t["cell"] < (1 << lev)[:, None]))
+    assert np.all(hs == (t["phi"] >= t["plo"]))
+    assert not np.any(ghost & leaf)
+    cen = centers(t, origin, W0)
+    for i in range(n):
+        lo, hi = t["plo"][i], t["phi"][i]
+        if hi >= lo:
+            blo = np.asarray(origin) + t["cell"][i] * w[i]
+            bhi = np.asarray(origin) + (t["cell"][i] + 1) * w[i]
+            assert np.all((sp[lo:hi + 1] >= blo) & (sp[lo:hi + 1] <= bhi))
+        if cf[i] >= 0:
+            ch = np.arange(cf[i], cf[i] + 8)
+            assert np.all(t["parent"][ch] == i) and np.all(lev[ch] == lev[i] + 1)
+            offs = np.array([[(k >> d) & 1 for d in range(3)] for k in range(8)])
+            assert np.array_equal(t["cell"][ch], 2 * t["cell"][i] + offs)
+            assert t["plo"][ch[0]] == lo and t["phi"][ch[-1]] == hi
+            assert np.all(t["phi"][ch[:-1]] + 1 == t["plo"][ch[1:]])
+            for k in range(8):
+                a, b = t["plo"][ch[k]], t["phi"][ch[k]]
+                if b >= a:
+                    assert np.all(child_slot(sp[a:b + 1], cen[i]) == k)
+            assert not ghost[i]
+            if leaf[i]:
+                assert xlist[i] and np.all(ghost[ch])
+            else:
+                assert not np.any(ghost[ch])
+        else:
+            assert not xlist[i]
+            assert leaf[i] or ghost[i]
+    # unique cells and brute-force colleagues
+    col = t["colleagues"]
+    L = lev.max() + 1
+    coffs = np.array([[k % 3 - 1, (k // 3) % 3 - 1, k // 9 - 1] for k in range(27)])
+    for l in range(L):
+        idx = np.nonzero(lev == l)[0]
+        lookup = {tuple(t["cell"][i]): i for i in idx}
+        assert len(lookup) == len(idx)
+        for i in idx:
+            assert col[i, 13] == i
+            for k in range(27):
+                assert col[i, k] == lookup.get(tuple(t["cell"][i] + coffs[k]), -1)
+    # 2:1 balance of real depths between colleagues
+    rdepth = np.zeros(n, int)
+    for i in range(n - 1, -1, -1):
+        if cf[i] >= 0 and not leaf[i]:
+            rdepth[i] = 1 + rdepth[cf[i]:cf[i] + 8].max()
+    for i in np.nonzero(leaf)[0]:
+        for j in col[i]:
+            if j < 0 or ghost[j]:
+                continue
+            assert abs(rdepth[i] - rdepth[j]) <= 1
+    # ghosts and xlist flags
+    for i in range(n):
+        if not leaf[i] and not ghost[i]:
+            for j in col[i]:
+                if j >= 0:
+                    assert not ghost[j] and cf[j] >= 0
+        if leaf[i]:
+            nonleaf = any(j >= 0 and not leaf[j] and not ghost[j] for j in col[i])
+            assert xlist[i] == nonleaf
+    # point_node
+    pn = t["point_node"]
+    for j in range(N):
+        p = pn[j]
+        assert leaf[p] and t["plo"][p] <= j <= t["phi"][p]
+
+
+def same_structure(a, b, keys=("cell", "level", "parent", "child_first", "plo", "phi", "leaf", "ghost", "xlist",
+                                "has_source", "colleagues", "point_node")):
+    """test/test_device_tree.jl:110-112: every structural field equal."""
+    for k in keys:
+        if not np.array_equal(np.asarray(a[k]), np.asarray(b[k])):
+            return k
+    return None
+
+
+def oracle_tree_dict(T):
+    return {k: getattr(T, k) for k in ("cell", "level", "parent", "child_first", "plo", "phi", "leaf", "ghost", "xlist",
+                                       "has_source", "colleagues", "perm", "point_node")}

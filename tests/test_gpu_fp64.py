@@ -1,0 +1,228 @@
+"""The device tree and the plain FP64 path against the CPU oracle.
+
+Mirrors the reference's device tests: test/test_device_tree.jl (the tree equal to the host
+tree field by field), test/test_device_passes.jl (lists as sets, robustness) and
+test/test_device_harmonics.jl (multipoles < 1e-13, locals < 1e-11, matvec and evaluation
+at targets < 1e-11, gradient < 1e-10). The FP64 path's bar here is 1e-12 (max-norm relative)
+on potentials.
+"""
+import numpy as np
+import pytest
+
+from helpers import DISTRIBUTIONS3, check_tree_invariants, mrd, oracle_tree_dict, same_structure
+
+pytestmark = pytest.mark.gpu
+BOX = ((0.0, 0.0, 0.0), 1.0)
+
+TREE_CASES = [("uniform", 20000, 40, 1), ("mixed", 8000, 40, 2), ("sphere", 8000, 60, 3), ("helix", 8000, 50, 4),
+              ("clustered", 6000, 30, 5), ("one_octant", 5000, 20, 6), ("mixed", 3000, 8, 7)]
+
+
+def _method(F, p):
+    return F.SphericalHarmonics(F.Laplace3D(), p=p)
+
+
+@pytest.mark.parametrize("name,n,ppl,seed", TREE_CASES)
+def test_device_tree_equals_host_tree(oracle, fmmb, name, n, ppl, seed):
+    rng = np.random.default_rng(seed)
+    pts = DISTRIBUTIONS3[name](rng, n)
+    T = oracle.Tree.build(pts, ppl)
+    f = fmmb.FMM(_method(fmmb, 4), pts, ppl=ppl, bbox=BOX)
+    t = f.tree()
+    ref = oracle_tree_dict(T)
+    assert f.nlevels == T.L and f.nnodes == T.n
+    assert same_structure(t, ref) is None, same_structure(t, ref)
+    # the order of the points within the childless nodes too (the host tree's perm)
+    assert np.array_equal(t["perm"], ref["perm"])
+    # the far pairs of every level, as sets of (target, source, far offset)
+    for l in range(T.L):
+        a = sorted(zip(*[x.tolist() for x in f.pairs(l)]))
+        b = sorted(zip(*[x.tolist() for x in T.pairs(l)]))
+        assert a == b, f"level {l}"
+
+
+def test_device_tree_invariants(fmmb):
+    rng = np.random.default_rng(11)
+    pts = DISTRIBUTIONS3["mixed"](rng, 2500)
+    f = fmmb.FMM(_method(fmmb, 4), pts, ppl=10, bbox=BOX)
+    t = f.tree()
+    assert t["ghost"].sum() > 0 and t["xlist"].sum() > 0 and f.nlevels >= 5
+    check_tree_invariants(t, pts)
+
+
+def test_device_tree_deterministic(fmmb):
+    rng = np.random.default_rng(12)
+    pts = DISTRIBUTIONS3["sphere"](rng, 20000)
+    m = _method(fmmb, 4)
+    a = fmmb.FMM(m, pts, ppl=30, bbox=BOX).tree()
+    b = fmmb.FMM(m, pts, ppl=30, bbox=BOX).tree()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_small_trees(oracle, fmmb):
+    rng = np.random.default_rng(13)
+    m = _method(fmmb, 6)
+    for n, ppl in ((1, 5), (10, 50), (64, 64), (65, 64), (300, 4)):
+        pts = rng.random((n, 3))
+        tau = rng.standard_normal(n)
+        f = fmmb.FMM(m, pts, ppl=ppl, bbox=BOX)
+        T = oracle.Tree.build(pts, ppl)
+        assert same_structure(f.tree(), oracle_tree_dict(T)) is None
+        st = fmmb.build_expansions(f, pts, tau)
+        u, g = fmmb.evaluate_at_sources_both(f, st)
+        du, dg = oracle.direct(pts, tau)
+        if n == 1:
+            assert u[0] == 0 and np.all(g == 0)
+            continue
+        O = oracle.FMM(6, pts, ppl)
+        O.build_expansions(pts, tau)
+        ou, og = O.evaluate_at_sources()
+        assert mrd(u, ou) < 1e-12 and mrd(g, og) < 1e-11
+        assert mrd(u, du) < 1e-3 and mrd(g, dg) < 1e-2
+
+
+PARITY_CASES = [("uniform", 30000, 40, 10, 21), ("mixed", 12000, 40, 10, 22), ("helix", 8000, 30, 8, 23),
+                ("sphere", 10000, 60, 12, 24), ("clustered", 8000, 30, 16, 25)]
+
+
+@pytest.mark.parametrize("name,n,ppl,p,seed", PARITY_CASES)
+def test_fp64_path_matches_oracle(oracle, fmmb, name, n, ppl, p, seed):
+    rng = np.random.default_rng(seed)
+    pts = DISTRIBUTIONS3[name](rng, n)
+    tau = rng.standard_normal(n)
+    targets = rng.random((500, 3))
+    O = oracle.FMM(p, pts, ppl)
+    O.build_expansions(pts, tau)
+    ou, og = O.evaluate_at_sources()
+    tu, tg = O.evaluate(targets)
+    OM, OL = O.expansions()
+    f = fmmb.FMM(_method(fmmb, p), pts, ppl=ppl, bbox=BOX)
+    st = fmmb.build_expansions(f, pts, tau)
+    M, Lc = st.expansions()
+    assert np.max(np.abs(M - OM)) < 1e-13 * np.max(np.abs(OM))
+    assert np.max(np.abs(Lc - OL)) < 1e-11 * np.max(np.abs(OL))
+    u, g = fmmb.evaluate_at_sources_both(f, st)
+    assert mrd(u, ou) < 1e-12
+    assert mrd(g, og) < 1e-11
+    assert mrd(fmmb.evaluate(f, st, targets), tu) < 1e-12
+    assert mrd(fmmb.evaluate(f, st, targets, output=fmmb.Gradient()), tg) < 1e-11
+    # the separate-output calls agree with the combined one bitwise
+    assert np.array_equal(fmmb.evaluate_at_sources(f, st), u)
+    assert np.array_equal(fmmb.evaluate_at_sources(f, st, output=fmmb.Gradient()), g)
+
+
+def test_fp64_accuracy_vs_direct(oracle, fmmb):
+    """test/test_harmonics.jl:129-152: p = 16, 6000 points, potential < 1e-5, gradient < 1e-4."""
+    rng = np.random.default_rng(31)
+    for name in DISTRIBUTIONS3:
+        pts = DISTRIBUTIONS3[name](rng, 6000)
+        tau = rng.standard_normal(6000)
+        targets = rng.random((500, 3))
+        f = fmmb.FMM(_method(fmmb, 16), pts, ppl=40, bbox=BOX)
+        st = fmmb.build_expansions(f, pts, tau)
+        du, _ = oracle.direct(pts, tau)
+        tu, tg = oracle.direct(pts, tau, targets)
+        assert mrd(fmmb.evaluate_at_sources(f, st), du) < 1e-5, name
+        assert mrd(fmmb.evaluate(f, st, targets), tu) < 1e-5, name
+        assert mrd(fmmb.evaluate(f, st, targets, output=fmmb.Gradient()), tg) < 1e-4, name
+
+
+def test_device_direct(oracle, fmmb):
+    import ctypes as C
+    import torch
+    rng = np.random.default_rng(41)
+    src = rng.random((3000, 3))
+    tau = rng.standard_normal(3000)
+    tg = rng.random((700, 3))
+    du, dg = oracle.direct(src, tau, tg)
+    ctx = fmmb.default_context()
+    s_d = torch.from_numpy(src).cuda()
+    t_d = torch.from_numpy(tau).cuda()
+    g_d = torch.from_numpy(tg).cuda()
+    pot = torch.zeros(700, dtype=torch.float64, device="cuda")
+    grad = torch.zeros((700, 3), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rc = fmmb.lib().fmmb_direct_dev(ctx._h, C.c_void_p(s_d.data_ptr()), C.c_void_p(t_d.data_ptr()), 3000,
+                                    C.c_void_p(g_d.data_ptr()), None, 700, C.c_void_p(pot.data_ptr()),
+                                    C.c_void_p(grad.data_ptr()))
+    assert rc == 0
+    assert mrd(pot.cpu().numpy(), du) < 1e-13 and mrd(grad.cpu().numpy(), dg) < 1e-13
+
+
+def test_errors(fmmb):
+    rng = np.random.default_rng(51)
+    m = _method(fmmb, 6)
+    pts = rng.random((3000, 3))
+    tau = rng.standard_normal(3000)
+    for bad in ((np.nan, 0.5, 0.5), (0.5, np.inf, 0.5)):
+        q = pts.copy()
+        q[17] = bad
+        with pytest.raises(fmmb.ArgumentError, match="finite"):
+            fmmb.FMM(m, q, ppl=40, bbox=BOX)
+    with pytest.raises(fmmb.ArgumentError, match="outside"):
+        fmmb.FMM(m, pts, ppl=40, bbox=((0.5, 0.5, 0.5), 1.0))
+    with pytest.raises(fmmb.ArgumentError, match="max_levels"):
+        fmmb.FMM(m, np.full((20, 3), 0.3), ppl=5, bbox=BOX, max_levels=10)
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.FMM(m, pts, ppl=0, bbox=BOX)
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.FMM(m, np.zeros((0, 3)), ppl=5, bbox=BOX)
+    f = fmmb.FMM(m, pts, ppl=40, bbox=BOX)
+    with pytest.raises(fmmb.DimensionMismatch):
+        fmmb.build_expansions(f, pts[:-1], tau[:-1])
+    with pytest.raises(fmmb.DimensionMismatch):
+        fmmb.build_expansions(f, pts, tau[:-1])
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.build_expansions(f, pts, tau.astype(np.complex128))
+    st = fmmb.FMMState(f)
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.evaluate_at_sources(f, st)
+    fmmb.build_expansions_(st, f, pts, tau)
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.evaluate_at_sources(f, st, output="pressure")
+    with pytest.raises(fmmb.ArgumentError, match="outside"):
+        fmmb.evaluate(f, st, np.array([[1.0 + 1e-12, 0.5, 0.5]]))
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.OperatorCache(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=0))
+    other = fmmb.OperatorCache(_method(fmmb, 6))
+    with pytest.raises(fmmb.ArgumentError, match="different method"):
+        fmmb.FMM(m, pts, ppl=40, cache=other)
+
+
+def test_nan_density_poisons_one_application(fmmb):
+    """test/test_device_passes.jl:187-196: a plan recovers bitwise after a non-finite density."""
+    rng = np.random.default_rng(61)
+    pts = DISTRIBUTIONS3["mixed"](rng, 5000)
+    tau = rng.standard_normal(5000)
+    f = fmmb.FMM(_method(fmmb, 8), pts, ppl=40, bbox=BOX)
+    st = fmmb.FMMState(f)
+    u0 = fmmb.device_matvec(f, st, pts, tau)
+    bad = tau.copy()
+    bad[5] = np.nan
+    assert np.any(np.isnan(fmmb.device_matvec(f, st, pts, bad)))
+    assert np.array_equal(fmmb.device_matvec(f, st, pts, tau), u0)
+    # a fresh plan gives the same result bitwise (determinism)
+    f2 = fmmb.FMM(_method(fmmb, 8), pts, ppl=40, bbox=BOX)
+    assert np.array_equal(fmmb.device_matvec(f2, fmmb.FMMState(f2), pts, tau), u0)
+
+
+def test_shared_cache_snaps_boxes(oracle, fmmb):
+    """src/operators/cache.jl:57-83: the second box is snapped to ldexp(W0, e)."""
+    rng = np.random.default_rng(71)
+    m = _method(fmmb, 8)
+    cache = fmmb.OperatorCache(m)
+    pts = rng.random((4000, 3))
+    tau = rng.standard_normal(4000)
+    f1 = fmmb.FMM(m, pts, ppl=40, bbox=BOX, cache=cache)
+    assert cache.W0 == 1.0
+    pts2 = 0.2 + 0.3 * rng.random((4000, 3))
+    f2 = fmmb.FMM(m, pts2, ppl=40, cache=cache)          # square_bbox then snapped
+    assert f2.width in (0.25, 0.5)
+    st = fmmb.build_expansions(f2, pts2, tau)
+    du, _ = oracle.direct(pts2, tau)
+    assert mrd(fmmb.evaluate_at_sources(f2, st), du) < 1e-5
+    O = oracle.FMM(8, pts2, 40, origin=tuple(f2.origin), width=f2.width, ref_width=1.0)
+    O.build_expansions(pts2, tau)
+    assert mrd(fmmb.evaluate_at_sources(f2, st), O.evaluate_at_sources()[0]) < 1e-12
+    del f1

@@ -1,0 +1,76 @@
+"""The mixed path (tensor-core TF32x3 M2L, FP32 compensated near field) against the FP64
+path and FP64 direct sums. Tolerances: the locals within 2e-6 (max-norm relative) of the
+FP64 path's; potentials within 1e-6 relative L2 of FP64 direct sums at p = 10 (the metric's
+target), gradients within 1e-5."""
+import numpy as np
+import pytest
+
+from helpers import DISTRIBUTIONS3, mrd, rel_l2
+
+pytestmark = pytest.mark.gpu
+BOX = ((0.0, 0.0, 0.0), 1.0)
+
+
+@pytest.mark.parametrize("name,n,ppl,seed", [("uniform", 60000, 64, 1), ("mixed", 20000, 40, 2), ("sphere", 20000, 40, 3),
+                                             ("clustered", 15000, 30, 4)])
+def test_mixed_locals_match_fp64(fmmb, name, n, ppl, seed):
+    rng = np.random.default_rng(seed)
+    pts = DISTRIBUTIONS3[name](rng, n)
+    tau = rng.standard_normal(n)
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=10), pts, ppl=ppl, bbox=BOX)
+    s64 = fmmb.build_expansions(f, pts, tau, precision="fp64")
+    s32 = fmmb.build_expansions(f, pts, tau, precision="mixed")
+    M64, L64 = s64.expansions()
+    M32, L32 = s32.expansions()
+    assert np.array_equal(M64, M32)                      # the upward pass is FP64 on both paths
+    assert np.max(np.abs(L32 - L64)) < 2e-6 * np.max(np.abs(L64))
+    u64, g64 = fmmb.evaluate_at_sources_both(f, s64)
+    u32, g32 = fmmb.evaluate_at_sources_both(f, s32)
+    assert rel_l2(u32, u64) < 5e-7
+    assert rel_l2(g32, g64) < 5e-6
+
+
+def test_mixed_accuracy_vs_direct(oracle, fmmb):
+    rng = np.random.default_rng(9)
+    n = 100000
+    pts = rng.random((n, 3))
+    tau = rng.standard_normal(n)
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=10), pts, ppl=64, bbox=BOX)
+    st = fmmb.build_expansions(f, pts, tau, precision="mixed")
+    u, g = fmmb.evaluate_at_sources_both(f, st)
+    sel = np.sort(rng.choice(n, 512, replace=False))
+    du, dg = oracle.direct_sample(pts, tau, sel)
+    assert rel_l2(u[sel], du) < 1e-6
+    assert rel_l2(g[sel], dg) < 1e-5
+    tg = rng.random((300, 3))
+    tu, tgr = oracle.direct(pts, tau, tg)
+    assert rel_l2(fmmb.evaluate(f, st, tg), tu) < 1e-6
+    assert rel_l2(fmmb.evaluate(f, st, tg, output=fmmb.Gradient()), tgr) < 1e-5
+
+
+def test_mixed_deterministic_and_recovers(fmmb):
+    rng = np.random.default_rng(10)
+    pts = DISTRIBUTIONS3["mixed"](rng, 20000)
+    tau = rng.standard_normal(20000)
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=8), pts, ppl=40, bbox=BOX)
+    st = fmmb.FMMState(f, "mixed")
+    u0 = fmmb.device_matvec(f, st, pts, tau)
+    bad = tau.copy()
+    bad[3] = np.inf
+    assert not np.all(np.isfinite(fmmb.device_matvec(f, st, pts, bad)))
+    assert np.array_equal(fmmb.device_matvec(f, st, pts, tau), u0)
+    assert np.array_equal(fmmb.device_matvec(f, fmmb.FMMState(f, "mixed"), pts, tau), u0)
+
+
+def test_mixed_supported_orders(fmmb):
+    rng = np.random.default_rng(12)
+    pts = rng.random((5000, 3))
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=12), pts, ppl=40, bbox=BOX)
+    with pytest.raises(fmmb.Unsupported):
+        fmmb.FMMState(f, "mixed")
+    for p in (4, 6):
+        tau = rng.standard_normal(5000)
+        g = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=p), pts, ppl=40, bbox=BOX)
+        u32 = fmmb.evaluate_at_sources(g, fmmb.build_expansions(g, pts, tau, precision="mixed"))
+        u64 = fmmb.evaluate_at_sources(g, fmmb.build_expansions(g, pts, tau, precision="fp64"))
+        assert rel_l2(u32, u64) < 1e-6
