@@ -109,6 +109,22 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- replicas
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The largest value of x over the ranks of the process group (x itself without one)."""
+    import torch
+    if dist is None or not dist.is_initialized():
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(n_per_rank, ms_per_step, world):
+    """Whole-job evaluations/s of `world` independent replicas timed at the slowest rank."""
+    return world * n_per_rank / (ms_per_step / 1e3)
+
+
 # ---------------------------------------------------------------- clocks during the timed region
 class Clocks:
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -204,13 +220,6 @@ def run_ours(a):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     for name in ("mixed", "fp64"):
         for _ in range(a.warmup):
             step(states[name])
@@ -222,8 +231,8 @@ def run_ours(a):
     clk = clocks.stop() if clocks else None
     t_fp64 = timed(states["fp64"], a.steps)
     barrier()
-    ms_mixed = max_over_ranks(statistics.mean(t_mixed))
-    ms_fp64 = max_over_ranks(statistics.mean(t_fp64))
+    ms_mixed = max_over_ranks(statistics.mean(t_mixed), dist, "cuda")
+    ms_fp64 = max_over_ranks(statistics.mean(t_fp64), dist, "cuda")
 
     # accuracy: both paths against FP64 direct sums at sampled sources (device)
     rng = np.random.default_rng(7)
@@ -277,7 +286,7 @@ def run_ours(a):
         fmmb._check(L.fmmb_matvec(st._h, P(xyz_h), P(tau_h), a.n, 3, P(pot_h), P(grad_h)))
         e2e.append(time.perf_counter() - t0)
     barrier()
-    e2e_s = max_over_ranks(statistics.mean(e2e))
+    e2e_s = max_over_ranks(statistics.mean(e2e), dist, "cuda")
 
     if rank != 0:
         if dist:
@@ -304,13 +313,13 @@ def run_ours(a):
                "sample": f"full {a.n:,}-point matvec (the same points and charges), best of 2 after 1 warm-up, "
                          f"tree + operators {r['tree_s']:.2f} s untimed"}
     line = {
-        "metric": METRIC, "value": world * a.n / (ms_mixed / 1e3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "tf32x3 M2L + f32 P2P, f64 elsewhere", "data": "synthetic (seeded uniform points, N(0,1) charges)",
         "config": config(a, {"precision": "mixed", "plan_s": plan_s, "levels": f.nlevels, "nodes": f.nnodes,
                              "far_pairs": f.npairs}),
         "latency_ms": {"p50": pct(0.5), "p99": pct(0.99)},
-        "fp64": {"value": world * a.n / (ms_fp64 / 1e3), "ms_per_step": ms_fp64},
+        "fp64": {"value": replica_throughput(a.n, ms_fp64, world), "ms_per_step": ms_fp64},
         "mixed_vs_fp64": ms_fp64 / ms_mixed,
         "error": {"samples": len(sel), **{k: v for k, v in err.items()}},
         "stages_ms": stages,

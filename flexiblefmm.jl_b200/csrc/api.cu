@@ -6,12 +6,41 @@
 
 using namespace fmmb;
 
-struct fmmb_ctx { Ctx c; };
-struct fmmb_cache { Cache c; };
-struct fmmb_plan { Plan p; };
-struct fmmb_state { State s; };
+// Handles may be destroyed in any order (a garbage collector finalises in any order): each
+// handle counts the handles built on it (a context its caches, a cache its plans, a plan its
+// states) and is freed once it was destroyed and nothing depends on it any more.
+struct fmmb_ctx { Ctx c; int deps = 0; bool released = false; };
+struct fmmb_cache { Cache c; fmmb_ctx* parent = nullptr; int deps = 0; bool released = false; };
+struct fmmb_plan { Plan p; fmmb_cache* parent = nullptr; int deps = 0; bool released = false; };
+struct fmmb_state { State s; fmmb_plan* parent = nullptr; };
 
 namespace {
+
+std::mutex g_handles;   // guards the dependency counts
+
+void free_ctx_locked(fmmb_ctx* x) {
+  if (!x->released || x->deps > 0) return;
+  cudaSetDevice(x->c.device);
+  if (x->c.own_stream) { cudaStreamSynchronize(x->c.stream); cudaStreamDestroy(x->c.stream); }
+  delete x;
+}
+void free_cache_locked(fmmb_cache* x) {
+  if (!x->released || x->deps > 0) return;
+  fmmb_ctx* parent = x->parent;
+  cudaSetDevice(parent->c.device);
+  delete x;
+  --parent->deps;
+  free_ctx_locked(parent);
+}
+void free_plan_locked(fmmb_plan* x) {
+  if (!x->released || x->deps > 0) return;
+  fmmb_cache* parent = x->parent;
+  cudaSetDevice(x->p.ctx->device);
+  cudaStreamSynchronize(x->p.ctx->stream);
+  delete x;
+  --parent->deps;
+  free_cache_locked(parent);
+}
 
 thread_local std::string g_last_error;
 
@@ -129,6 +158,9 @@ void plan_from_device_points(fmmb_cache* cache, const double* xyz, int64_t n, co
     P.m2l_scale[l] = e == 0 ? 1.0 : 1.0 / lam;
   }
   build_lists(P);
+  h->parent = cache;
+  std::lock_guard<std::mutex> lk(g_handles);
+  ++cache->deps;
   *out = h.release();
 }
 
@@ -179,9 +211,9 @@ int fmmb_ctx_create(int device, fmmb_ctx** out) {
 int fmmb_ctx_destroy(fmmb_ctx* ctx) {
   return guard([&] {
     if (!ctx) return;
-    set_device(ctx->c);
-    if (ctx->c.own_stream) { cudaStreamSynchronize(ctx->c.stream); cudaStreamDestroy(ctx->c.stream); }
-    delete ctx;
+    std::lock_guard<std::mutex> lk(g_handles);
+    ctx->released = true;
+    free_ctx_locked(ctx);
   });
 }
 
@@ -211,9 +243,12 @@ int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* m, fmmb_cache** out
     require(m->tol == 0, FMMB_ERR_UNSUPPORTED, "low-rank class operators (tol > 0) are not provided");
     std::unique_ptr<fmmb_cache> h(new fmmb_cache());
     h->c.ctx = &ctx->c;
+    h->parent = ctx;
     h->c.p = m->p;
     h->c.np = (m->p + 1) * (m->p + 1);
     h->c.ld = ld_of(m->p);
+    std::lock_guard<std::mutex> lk(g_handles);
+    ++ctx->deps;
     *out = h.release();
   });
 }
@@ -221,8 +256,9 @@ int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* m, fmmb_cache** out
 int fmmb_cache_destroy(fmmb_cache* cache) {
   return guard([&] {
     if (!cache) return;
-    set_device(*cache->c.ctx);
-    delete cache;
+    std::lock_guard<std::mutex> lk(g_handles);
+    cache->released = true;
+    free_cache_locked(cache);
   });
 }
 
@@ -255,9 +291,9 @@ int fmmb_plan_create_dev(fmmb_cache* cache, const double* xyz_dev, int64_t n, co
 int fmmb_plan_destroy(fmmb_plan* plan) {
   return guard([&] {
     if (!plan) return;
-    set_device(*plan->p.ctx);
-    FMMB_CUDA(cudaStreamSynchronize(plan->p.ctx->stream));
-    delete plan;
+    std::lock_guard<std::mutex> lk(g_handles);
+    plan->released = true;
+    free_plan_locked(plan);
   });
 }
 
@@ -359,6 +395,9 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
       prepare_mixed_operators(*P.cache);
     }
     FMMB_CUDA(cudaStreamSynchronize(s));
+    h->parent = plan;
+    std::lock_guard<std::mutex> lk(g_handles);
+    ++plan->deps;
     *out = h.release();
   });
 }
@@ -366,9 +405,13 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
 int fmmb_state_destroy(fmmb_state* state) {
   return guard([&] {
     if (!state) return;
-    set_device(*state->s.plan->ctx);
-    FMMB_CUDA(cudaStreamSynchronize(state->s.plan->ctx->stream));
+    std::lock_guard<std::mutex> lk(g_handles);
+    fmmb_plan* parent = state->parent;
+    cudaSetDevice(parent->p.ctx->device);
+    cudaStreamSynchronize(parent->p.ctx->stream);
     delete state;
+    --parent->deps;
+    free_plan_locked(parent);
   });
 }
 

@@ -213,6 +213,7 @@ HostOperators build_operators(int p, double ref_width) {
     if (ey) { A2[0][1] = -A2[0][1]; A2[1][1] = -A2[1][1]; }
     // the rotation index: A2 = [[cos, −sin], [sin, cos]] of kπ/2
     int k = (A2[0][0] == 1) ? 0 : (A2[1][0] == 1) ? 1 : (A2[0][0] == -1) ? 2 : 3;
+    op.d4h.push_back((uint8_t)(k | (ey ? 4 : 0) | (ez ? 8 : 0)));
     std::vector<int> is, ss, it, st;
     d4h_permutation(p, k, ey, ez, false, is, ss);
     d4h_permutation(p, k, ey, ez, true, it, st);

@@ -13,6 +13,7 @@
 // leading dimension LD (a multiple of 64 ≥ (p+1)²), rows ≥ (p+1)² kept zero.
 #include <algorithm>
 
+#include "d4h.cuh"
 #include "passes.cuh"
 #include "scan_sort.cuh"
 
@@ -66,6 +67,13 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
                       const int* __restrict__ phi, const double* __restrict__ xs, const double* __restrict__ ys,
                       const double* __restrict__ zs, const double* __restrict__ q, Geometry geo,
                       const double* __restrict__ scale, int LD, double* __restrict__ M) {
+  // the recurrence tables in shared memory: the lanes of a warp run different orders and would
+  // serialise on the constant cache
+  __shared__ double s_ab[2 * TRI_MAX];
+  __shared__ double s_e[PMAX];
+  for (int i = threadIdx.x; i < 2 * TRI_MAX; i += blockDim.x) s_ab[i] = c_tab[i];
+  for (int i = threadIdx.x; i < PMAX; i += blockDim.x) s_e[i] = c_e[i];
+  __syncthreads();
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   int qn = g / (P + 1), m = g % (P + 1);
   if (qn >= nn) return;
@@ -82,7 +90,7 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
     double r2 = x * x + y * y + z * z;
     double sr = 1.0, si = 0.0;
     for (int k = 1; k <= m; ++k) {
-      double e = c_e[k - 1];
+      double e = s_e[k - 1];
       double nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
       sr = nr; si = ni;
     }
@@ -95,7 +103,7 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
         ar[n] += tau * cr; ai[n] -= tau * ci;
       } else if (n > m) {
         int t = tri(n, m);
-        double az = c_tab[t] * z, br = c_tab[TRI_MAX + t] * r2;
+        double az = s_ab[t] * z, br = s_ab[TRI_MAX + t] * r2;
         double nr = az * cr - br * pr, ni = az * ci - br * pi;
         pr = cr; pi = ci; cr = nr; ci = ni;
         ar[n] += tau * nr; ai[n] -= tau * ni;
@@ -121,150 +129,92 @@ struct ColMap {
   }
 };
 
-// C(:, g) (=|+=) A · B(:, g); A column-major M × K; rows r with r mod LD ≥ NP written as 0
-__global__ void __launch_bounds__(256) k_gemm_cols(int M, int K, const double* __restrict__ A, ColMap bm, ColMap cm,
-                                                   int ncols, int LD, int NP, int accumulate) {
-  constexpr int BM = 64, BN = 64, BK = 16;
+// C(:, g) (=|+=) A · B(:, g) for mapped columns g; A column-major M × K (M a multiple of 128);
+// rows r with r mod LD ≥ NP written as 0. 128 × BN tiles, K-steps of 32 with the next step's
+// tiles prefetched into registers; each thread an RM × CN register tile.
+template <int BN>
+__global__ void __launch_bounds__(256) k_gemm_tiles(int M, int K, const double* __restrict__ A, ColMap bm, ColMap cm,
+                                                    int ncols, int LD, int NP, int accumulate) {
+  constexpr int BM = 128, BK = 32;
+  constexpr int CN = BN >= 16 ? 2 : 1, TC = BN / CN, TR = 256 / TC, RM = BM / TR;
+  constexpr int AL = BM * BK / 256, BL = (BK * BN + 255) / 256;
   __shared__ double As[BK][BM];
   __shared__ double Bs[BK][BN + 1];
-  int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
-  double acc[4][4] = {};
+  const int tid = threadIdx.x, tx = tid % TC, ty = tid / TC;
+  const int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
+  double acc[RM][CN];
+#pragma unroll
+  for (int r = 0; r < RM; ++r)
+#pragma unroll
+    for (int c = 0; c < CN; ++c) acc[r][c] = 0.0;
+  double ra[AL], rb[BL];
+  const double* bcol[BL];
+#pragma unroll
+  for (int u = 0; u < BL; ++u) {
+    const int e = tid + 256 * u, j = e / BK;
+    bcol[u] = (e < BK * BN && col0 + j < ncols) ? bm.col(col0 + j, LD) : nullptr;
+  }
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int u = 0; u < AL; ++u) {
+      const int e = tid + 256 * u, i = e % BM, k = e / BM;
+      ra[u] = (k0 + k < K && row0 + i < M) ? A[(int64_t)(k0 + k) * M + row0 + i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < BL; ++u) {
+      const int e = tid + 256 * u, k = e % BK;
+      rb[u] = (bcol[u] && k0 + k < K) ? bcol[u][k0 + k] : 0.0;
+    }
+  };
+  load(0);
   for (int k0 = 0; k0 < K; k0 += BK) {
-    for (int e = tid; e < BM * BK; e += 256) {
-      int i = e % BM, k = e / BM;
-      As[k][i] = (row0 + i < M && k0 + k < K) ? A[(int64_t)(k0 + k) * M + row0 + i] : 0.0;
-    }
-    for (int e = tid; e < BN * BK; e += 256) {
-      int k = e % BK, j = e / BK;
-      int g = col0 + j;
-      Bs[k][j] = (g < ncols && k0 + k < K) ? bm.col(g, LD)[k0 + k] : 0.0;
-    }
     __syncthreads();
 #pragma unroll
+    for (int u = 0; u < AL; ++u) { const int e = tid + 256 * u; As[e / BM][e % BM] = ra[u]; }
+#pragma unroll
+    for (int u = 0; u < BL; ++u) { const int e = tid + 256 * u; if (e < BK * BN) Bs[e % BK][e / BK] = rb[u]; }
+    __syncthreads();
+    if (k0 + BK < K) load(k0 + BK);
+#pragma unroll 8
     for (int k = 0; k < BK; ++k) {
-      double a[4], b[4];
+      double a[RM], b[CN];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = As[k][ty + 16 * r];
+      for (int r = 0; r < RM; ++r) a[r] = As[k][ty + TR * r];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = Bs[k][tx + 16 * c];
+      for (int c = 0; c < CN; ++c) b[c] = Bs[k][tx + TC * c];
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+      for (int r = 0; r < RM; ++r)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        for (int c = 0; c < CN; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
     }
-    __syncthreads();
   }
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    int g = col0 + tx + 16 * c;
+  for (int c = 0; c < CN; ++c) {
+    const int g = col0 + tx + TC * c;
     if (g >= ncols) continue;
     double* C = cm.col(g, LD);
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      int row = row0 + ty + 16 * r;
+    for (int r = 0; r < RM; ++r) {
+      const int row = row0 + ty + TR * r;
       if (row >= M) continue;
-      double v = (row % LD) < NP ? acc[r][c] : 0.0;
+      const double v = (row % LD) < NP ? acc[r][c] : 0.0;
       C[row] = accumulate ? C[row] + v : v;
     }
   }
 }
 
-// ---------------------------------------------------------------- M2L, FP64
-// One CTA per block of targets. Per class: the pairs in chunks of NB columns; the gathered
-// B operand G = P_sᵀ M_src and the class representative A stream through shared memory in
-// K-chunks of 16; the product Y = A G is staged and scattered with P_t, each thread owning
-// one output row and summing the consecutive pairs of a target before one update of its
-// partial local (no atomics: the block owns its targets).
-template <int LD, int NB>
-__global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks, const int* __restrict__ cls_off,
-                                                 const int2* __restrict__ pairs, const double* __restrict__ reps,
-                                                 const int16_t* __restrict__ gidx, const int8_t* __restrict__ gsgn,
-                                                 const int16_t* __restrict__ sidx, const int8_t* __restrict__ ssgn,
-                                                 const double* __restrict__ m2l_scale, int NP, const double* __restrict__ M,
-                                                 double* __restrict__ Pl) {
-  constexpr int BK = 16, RPT = LD / 16, CPT = NB / 16;
-  extern __shared__ double sm[];
-  double* As = sm;                    // [BK][LD]
-  double* Gs = As + BK * LD;          // [BK][NB]
-  double* Ys = Gs + BK * NB;          // [NB][LD + 1]
-  int* ps = (int*)(Ys + NB * (LD + 1));  // src[NB], f[NB], t[NB]
-  int* pf = ps + NB;
-  int* pt = pf + NB;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  const int4 b = blocks[blockIdx.x];  // level, first node, count, pair base
-  const double alpha = m2l_scale[b.x];
-  const int* co = cls_off + (int64_t)blockIdx.x * (NCLASS + 1);
-  const int kmax = (NP + BK - 1) / BK * BK;
-  for (int c = 0; c < NCLASS; ++c) {
-    int a0 = co[c], a1 = co[c + 1];
-    const double* A = reps + (int64_t)c * LD * LD;
-    for (int q0 = a0; q0 < a1; q0 += NB) {
-      int nc = min(NB, a1 - q0);
-      __syncthreads();
-      for (int j = tid; j < NB; j += 256) {
-        if (j < nc) {
-          int2 pr = pairs[b.w + q0 + j];
-          ps[j] = pr.x; pf[j] = pr.y >> 8; pt[j] = pr.y & 0xff;
-        } else { ps[j] = -1; pf[j] = 0; pt[j] = -1; }
-      }
-      double acc[RPT][CPT];
-#pragma unroll
-      for (int r = 0; r < RPT; ++r)
-#pragma unroll
-        for (int cc = 0; cc < CPT; ++cc) acc[r][cc] = 0;
-      for (int k0 = 0; k0 < kmax; k0 += BK) {
-        __syncthreads();
-        for (int e = tid; e < BK * LD; e += 256) {
-          int i = e % LD, k = e / LD;
-          As[k * LD + i] = A[(int64_t)(k0 + k) * LD + i];
-        }
-        for (int e = tid; e < BK * NB; e += 256) {
-          int k = e % BK, j = e / BK;
-          double v = 0.0;
-          if (j < nc) {
-            int f = pf[j], row = k0 + k;
-            int gi = gidx[f * LD + row];
-            if (gi >= 0) v = (double)gsgn[f * LD + row] * M[(int64_t)ps[j] * LD + gi];
-          }
-          Gs[k * NB + j] = v;
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int k = 0; k < BK; ++k) {
-          double av[RPT], bv[CPT];
-#pragma unroll
-          for (int r = 0; r < RPT; ++r) av[r] = As[k * LD + ty + 16 * r];
-#pragma unroll
-          for (int cc = 0; cc < CPT; ++cc) bv[cc] = Gs[k * NB + tx + 16 * cc];
-#pragma unroll
-          for (int r = 0; r < RPT; ++r)
-#pragma unroll
-            for (int cc = 0; cc < CPT; ++cc) acc[r][cc] = fma(av[r], bv[cc], acc[r][cc]);
-        }
-      }
-#pragma unroll
-      for (int r = 0; r < RPT; ++r)
-#pragma unroll
-        for (int cc = 0; cc < CPT; ++cc) Ys[(tx + 16 * cc) * (LD + 1) + ty + 16 * r] = acc[r][cc];
-      __syncthreads();
-      for (int j = tid; j < NP; j += 256) {
-        int cur = -1;
-        double run = 0.0;
-        for (int qq = 0; qq < nc; ++qq) {
-          int t = pt[qq], f = pf[qq];
-          if (t != cur) {
-            if (cur >= 0) Pl[(int64_t)(b.y + cur) * LD + j] += alpha * run;
-            cur = t;
-            run = 0.0;
-          }
-          int si = sidx[f * LD + j];
-          run += (double)ssgn[f * LD + j] * Ys[qq * (LD + 1) + si];
-        }
-        if (cur >= 0) Pl[(int64_t)(b.y + cur) * LD + j] += alpha * run;
-      }
-    }
+// the column-tile width: enough tiles to cover the SMs
+void gemm_cols(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols, int LD, int NP, int accumulate, int num_sms,
+               cudaStream_t s) {
+  const int rows = (M + 127) / 128;
+  if ((int64_t)rows * ((ncols + 31) / 32) >= num_sms) {
+    k_gemm_tiles<32><<<dim3((ncols + 31) / 32, rows), 256, 0, s>>>(M, K, A, bm, cm, ncols, LD, NP, accumulate);
+  } else if ((int64_t)rows * ((ncols + 15) / 16) >= num_sms) {
+    k_gemm_tiles<16><<<dim3((ncols + 15) / 16, rows), 256, 0, s>>>(M, K, A, bm, cm, ncols, LD, NP, accumulate);
+  } else {
+    k_gemm_tiles<8><<<dim3((ncols + 7) / 8, rows), 256, 0, s>>>(M, K, A, bm, cm, ncols, LD, NP, accumulate);
   }
+  FMMB_LAUNCH_CHECK();
 }
 
 // ---------------------------------------------------------------- evaluation, FP64
@@ -475,19 +425,6 @@ void launch_eval_f64(State& S, const int* gnode, const int* gstart, const int* g
   FMMB_LAUNCH_CHECK();
 }
 
-template <int LD, int NB>
-void launch_m2l_f64(State& S) {
-  Plan& P_ = *S.plan;
-  Cache& C = *P_.cache;
-  int nb = (int)P_.h_blocks.size();
-  if (nb == 0) return;
-  size_t smem = sizeof(double) * (16 * LD + 16 * NB + NB * (LD + 1)) + sizeof(int) * 3 * NB;
-  auto kern = k_m2l_f64<LD, NB>;
-  FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<nb, 256, smem, P_.ctx->stream>>>(P_.blocks.p, P_.cls_off.p, P_.pairs.p, C.reps.p, C.gidx.p, C.gsgn.p, C.sidx.p,
-                                          C.ssgn.p, P_.d_m2l_scale.p, C.np, S.M.p, S.Pl.p);
-  FMMB_LAUNCH_CHECK();
-}
 
 }  // namespace
 
@@ -510,6 +447,7 @@ void upload_operators(Cache& C) {
   to_device(C.sidx, h.sidx, s);
   to_device(C.ssgn, h.ssgn, s);
   to_device(C.cls, h.cls, s);
+  upload_d4h(h, s);
   FMMB_CUDA(cudaStreamSynchronize(s));
   C.uploaded = true;
 }
@@ -541,9 +479,7 @@ int m2m_sweep(State& S) {
     int c0 = P.level_start[l + 1], ng = (P.level_start[l + 2] - c0) / NCH;
     if (ng == 0) continue;
     ColMap bm{S.M.p, nullptr, c0, NCH}, cm{S.M.p, P.group_parent[l + 1].p, 0, 0};
-    dim3 grid((ng + 63) / 64, (C.ld + 63) / 64);
-    k_gemm_cols<<<grid, 256, 0, s>>>(C.ld, NCH * C.ld, C.m2m.p, bm, cm, ng, C.ld, C.np, 0);
-    FMMB_LAUNCH_CHECK();
+    gemm_cols(C.ld, NCH * C.ld, C.m2m.p, bm, cm, ng, C.ld, C.np, 0, P.ctx->num_sms, s);
     ++launches;
   }
   return launches;
@@ -554,18 +490,6 @@ void upward_pass(State& S) {
   m2m_sweep(S);
 }
 
-void m2l_f64(State& S) {
-  switch (S.plan->cache->ld) {
-    case 64: launch_m2l_f64<64, 64>(S); break;
-    case 128: launch_m2l_f64<128, 64>(S); break;
-    case 192: launch_m2l_f64<192, 32>(S); break;
-    case 256: launch_m2l_f64<256, 32>(S); break;
-    case 320: launch_m2l_f64<320, 16>(S); break;
-    case 384: launch_m2l_f64<384, 16>(S); break;
-    case 448: launch_m2l_f64<448, 16>(S); break;
-    default: throw Error(FMMB_ERR_UNSUPPORTED, "no M2L kernel for this expansion length");
-  }
-}
 
 int l2l_sweep(State& S) {
   Plan& P = *S.plan;
@@ -576,9 +500,7 @@ int l2l_sweep(State& S) {
     int c0 = P.level_start[l], ng = (P.level_start[l + 1] - c0) / NCH;
     if (ng == 0) continue;
     ColMap bm{S.Pl.p, P.group_parent[l].p, 0, 0}, cm{S.Pl.p, nullptr, c0, NCH};
-    dim3 grid((ng + 63) / 64, (NCH * C.ld + 63) / 64);
-    k_gemm_cols<<<grid, 256, 0, s>>>(NCH * C.ld, C.ld, C.l2l.p, bm, cm, ng, C.ld, C.np, 1);
-    FMMB_LAUNCH_CHECK();
+    gemm_cols(NCH * C.ld, C.ld, C.l2l.p, bm, cm, ng, C.ld, C.np, 1, P.ctx->num_sms, s);
     ++launches;
   }
   return launches;

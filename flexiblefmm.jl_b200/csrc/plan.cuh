@@ -66,7 +66,7 @@ struct Plan {
   DBuf<int> leaves, leaf_start, leaf_count;
   int n_leaves = 0;
   // M2L: blocks, per block the class offsets of its pairs, the pairs (src, f << 8 | target)
-  int TB = 64;
+  int TB = 128;
   std::vector<M2LBlock> h_blocks;
   DBuf<int4> blocks;
   DBuf<int> cls_off;                      // nblocks × 35, relative to the block's pair_base

@@ -1,0 +1,166 @@
+# FlexibleFMMB200: the drop-in of FlexibleFMM.jl's FMM entry points onto libfmmb (sm_100a),
+# through `ccall` into the C ABI of include/fmmb.h.
+#
+#   using FlexibleFMM, FlexibleFMMB200
+#   m = SphericalHarmonics(Laplace3D(); p=10)
+#   f = FlexibleFMMB200.FMM(m, points; ppl=64, bbox=(SVector(0.0, 0.0, 0.0), 1.0))
+#   st = FlexibleFMMB200.build_expansions(f, points, τ)                 # src/fmm.jl:306-314
+#   u = FlexibleFMMB200.evaluate_at_sources(f, st)                      # src/evaluate.jl:111-132
+#   g = FlexibleFMMB200.evaluate(f, st, targets; output=Gradient())     # src/evaluate.jl:81-102
+#
+# The argument meanings and the exceptions are the reference's: status 1 → ArgumentError,
+# 2 → DimensionMismatch. Points are `Vector{SVector{3,Float64}}` (their memory is the 3 × N
+# interleaved array the ABI takes); outputs come back in the original order.
+module FlexibleFMMB200
+
+using FlexibleFMM: FlexibleFMM, SphericalHarmonics, Laplace3D, Potential, Gradient
+using StaticArrays: SVector
+
+const libfmmb = get(ENV, "FMMB_LIB", joinpath(@__DIR__, "..", "libfmmb.so"))
+
+const FMMB_PRECISION_FP64 = Cint(0)
+const FMMB_PRECISION_MIXED = Cint(1)
+const FMMB_OUTPUT_POTENTIAL = Cint(1)
+const FMMB_OUTPUT_GRADIENT = Cint(2)
+
+struct MethodDesc
+    method::Int32
+    kernel::Int32
+    p::Int32
+    reserved::Int32
+    tol::Float64
+end
+
+struct TreeOpts
+    ppl::Int32
+    max_levels::Int32
+    has_bbox::Int32
+    reserved::Int32
+    origin::NTuple{3,Float64}
+    width::Float64
+end
+
+function check(rc::Cint)
+    rc == 0 && return nothing
+    msg = unsafe_string(ccall((:fmmb_last_error, libfmmb), Cstring, ()))
+    rc == 1 && throw(ArgumentError(msg))
+    rc == 2 && throw(DimensionMismatch(msg))
+    error("fmmb error $rc: $msg")
+end
+
+mutable struct Context
+    h::Ptr{Cvoid}
+    function Context(device::Integer=0)
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:fmmb_ctx_create, libfmmb), Cint, (Cint, Ref{Ptr{Cvoid}}), device, r))
+        c = new(r[])
+        finalizer(x -> ccall((:fmmb_ctx_destroy, libfmmb), Cint, (Ptr{Cvoid},), x.h), c)
+    end
+end
+const DEFAULT_CONTEXT = Ref{Union{Nothing,Context}}(nothing)
+default_context() = something(DEFAULT_CONTEXT[], (DEFAULT_CONTEXT[] = Context(0)))
+
+"""
+    OperatorCache(method)  (src/operators/cache.jl:19-22)
+"""
+mutable struct OperatorCache
+    method::SphericalHarmonics
+    ctx::Context
+    h::Ptr{Cvoid}
+    function OperatorCache(m::SphericalHarmonics; ctx::Context=default_context())
+        m.kernel isa Laplace3D || throw(ArgumentError("the device method is written for Laplace3D"))
+        d = Ref(MethodDesc(1, 1, Int32(m.p), 0, m.tol))
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:fmmb_cache_create, libfmmb), Cint, (Ptr{Cvoid}, Ref{MethodDesc}, Ref{Ptr{Cvoid}}), ctx.h, d, r))
+        c = new(m, ctx, r[])
+        finalizer(x -> ccall((:fmmb_cache_destroy, libfmmb), Cint, (Ptr{Cvoid},), x.h), c)
+    end
+end
+
+"""
+    FMM(method, sources; ppl=50, bbox=nothing, cache=OperatorCache(method), max_levels=30)  (src/fmm.jl:31-49)
+"""
+mutable struct FMM
+    method::SphericalHarmonics
+    cache::OperatorCache
+    h::Ptr{Cvoid}
+    n::Int
+end
+function FMM(m::SphericalHarmonics, sources::AbstractVector{SVector{3,Float64}}; ppl::Integer=50, bbox=nothing,
+             cache::OperatorCache=OperatorCache(m), max_levels::Integer=30)
+    cache.method === m || throw(ArgumentError("the cache was built for a different method"))
+    pts = collect(sources)
+    o = bbox === nothing ? TreeOpts(ppl, max_levels, 0, 0, (0.0, 0.0, 0.0), 0.0) :
+        TreeOpts(ppl, max_levels, 1, 0, Tuple(Float64.(bbox[1])), Float64(bbox[2]))
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:fmmb_plan_create, libfmmb), Cint, (Ptr{Cvoid}, Ptr{Float64}, Int64, Ref{TreeOpts}, Ref{Ptr{Cvoid}}),
+                cache.h, pts, length(pts), Ref(o), r))
+    f = FMM(m, cache, r[], length(pts))
+    finalizer(x -> ccall((:fmmb_plan_destroy, libfmmb), Cint, (Ptr{Cvoid},), x.h), f)
+end
+
+"""
+    FMMState  (src/fmm.jl:64-94): the expansions of one right-hand side on the device.
+"""
+mutable struct FMMState
+    fmm::FMM
+    h::Ptr{Cvoid}
+    function FMMState(f::FMM; precision::Symbol=:fp64)
+        prec = precision === :mixed ? FMMB_PRECISION_MIXED : FMMB_PRECISION_FP64
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:fmmb_state_create, libfmmb), Cint, (Ptr{Cvoid}, Cint, Ref{Ptr{Cvoid}}), f.h, prec, r))
+        s = new(f, r[])
+        finalizer(x -> ccall((:fmmb_state_destroy, libfmmb), Cint, (Ptr{Cvoid},), x.h), s)
+    end
+end
+
+function build_expansions!(st::FMMState, f::FMM, sources::AbstractVector{SVector{3,Float64}}, τ::AbstractVector{<:Real})
+    length(sources) == f.n || throw(DimensionMismatch("expected $(f.n) sources in group 1"))
+    length(τ) == f.n || throw(DimensionMismatch("expected $(f.n) densities in group 1"))
+    pts = collect(sources)
+    tau = Vector{Float64}(τ)
+    check(ccall((:fmmb_build_expansions, libfmmb), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64),
+                st.h, pts, tau, f.n))
+    return st
+end
+build_expansions!(st::FMMState, f::FMM, sources, τ) =
+    throw(ArgumentError("densities of type $(eltype(τ)) are not supported by SphericalHarmonics"))
+build_expansions(f::FMM, sources, τ; precision::Symbol=:fp64) = build_expansions!(FMMState(f; precision), f, sources, τ)
+
+_flag(::Potential) = FMMB_OUTPUT_POTENTIAL
+_flag(::Gradient) = FMMB_OUTPUT_GRADIENT
+_flag(out) = throw(ArgumentError("output $(typeof(out)) is not available with SphericalHarmonics"))
+
+function evaluate_at_sources(f::FMM, st::FMMState, g::Int=1; output=Potential())
+    g == 1 || throw(ArgumentError("group $g of 1"))
+    flag = _flag(output)
+    if output isa Potential
+        out = Vector{Float64}(undef, f.n)
+        check(ccall((:fmmb_evaluate_at_sources, libfmmb), Cint, (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}),
+                    st.h, flag, out, C_NULL))
+    else
+        out = Vector{SVector{3,Float64}}(undef, f.n)
+        check(ccall((:fmmb_evaluate_at_sources, libfmmb), Cint, (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{SVector{3,Float64}}),
+                    st.h, flag, C_NULL, out))
+    end
+    return out
+end
+
+function evaluate(f::FMM, st::FMMState, targets::AbstractVector{SVector{3,Float64}}; output=Potential())
+    flag = _flag(output)
+    tg = collect(targets)
+    nt = length(tg)
+    if output isa Potential
+        out = Vector{Float64}(undef, nt)
+        check(ccall((:fmmb_evaluate, libfmmb), Cint, (Ptr{Cvoid}, Ptr{SVector{3,Float64}}, Int64, Cint, Ptr{Float64}, Ptr{Float64}),
+                    st.h, tg, nt, flag, out, C_NULL))
+    else
+        out = Vector{SVector{3,Float64}}(undef, nt)
+        check(ccall((:fmmb_evaluate, libfmmb), Cint,
+                    (Ptr{Cvoid}, Ptr{SVector{3,Float64}}, Int64, Cint, Ptr{Float64}, Ptr{SVector{3,Float64}}),
+                    st.h, tg, nt, flag, C_NULL, out))
+    end
+    return out
+end
+
+end # module

@@ -39,3 +39,16 @@ def test_version_and_no_device_error(fmmb):
         pytest.skip("a GPU is present")
     with pytest.raises(fmmb.FMMBError):
         fmmb.Context(0)
+
+
+def test_julia_shim_binds_declared_symbols():
+    """The ccall shim (flexiblefmm.jl_b200/julia/FlexibleFMMB200.jl) names only entry points the header declares;
+    Julia is absent here, so its calls are checked against the header by text."""
+    src = open(os.path.join(ROOT, "flexiblefmm.jl_b200", "julia", "FlexibleFMMB200.jl")).read()
+    called = set(re.findall(r"ccall\(\(:(fmmb_[a-z_0-9]+), libfmmb\)", src))
+    assert called and called <= set(declared())
+
+
+def test_struct_layouts(fmmb):
+    import ctypes as C
+    assert C.sizeof(fmmb._MethodDesc) == 24 and C.sizeof(fmmb._TreeOpts) == 48

@@ -221,8 +221,44 @@ def test_shared_cache_snaps_boxes(oracle, fmmb):
     assert f2.width in (0.25, 0.5)
     st = fmmb.build_expansions(f2, pts2, tau)
     du, _ = oracle.direct(pts2, tau)
-    assert mrd(fmmb.evaluate_at_sources(f2, st), du) < 1e-5
+    assert mrd(fmmb.evaluate_at_sources(f2, st), du) < 2e-4            # p = 8
     O = oracle.FMM(8, pts2, 40, origin=tuple(f2.origin), width=f2.width, ref_width=1.0)
     O.build_expansions(pts2, tau)
     assert mrd(fmmb.evaluate_at_sources(f2, st), O.evaluate_at_sources()[0]) < 1e-12
     del f1
+
+
+def test_handles_destroyed_in_any_order(fmmb):
+    """A garbage collector finalises in any order: destroying a context, cache or plan before
+    the handles built on it must defer their release, not crash."""
+    import ctypes as C
+    L = fmmb.lib()
+    rng = np.random.default_rng(81)
+    pts = rng.random((5000, 3))
+    tau = rng.standard_normal(5000)
+    for order in ("ctx_first", "plan_first", "cache_first"):
+        ctx = C.c_void_p()
+        assert L.fmmb_ctx_create(0, C.byref(ctx)) == 0
+        d = fmmb._MethodDesc(1, 1, 6, 0, 0.0)
+        cache = C.c_void_p()
+        assert L.fmmb_cache_create(ctx, C.byref(d), C.byref(cache)) == 0
+        o = fmmb._TreeOpts()
+        o.ppl, o.max_levels, o.has_bbox, o.width = 40, 30, 1, 1.0
+        plan = C.c_void_p()
+        assert L.fmmb_plan_create(cache, fmmb._ptr(pts), 5000, C.byref(o), C.byref(plan)) == 0
+        st = C.c_void_p()
+        assert L.fmmb_state_create(plan, 0, C.byref(st)) == 0
+        if order == "ctx_first":
+            assert L.fmmb_ctx_destroy(ctx) == 0
+        elif order == "plan_first":
+            assert L.fmmb_plan_destroy(plan) == 0
+        else:
+            assert L.fmmb_cache_destroy(cache) == 0
+        u = np.zeros(5000)
+        assert L.fmmb_matvec(st, fmmb._ptr(pts), fmmb._ptr(tau), 5000, 1, fmmb._ptr(u), None) == 0   # still usable
+        assert np.all(np.isfinite(u))
+        assert L.fmmb_state_destroy(st) == 0
+        for name, h in (("fmmb_plan_destroy", plan), ("fmmb_cache_destroy", cache), ("fmmb_ctx_destroy", ctx)):
+            if not ((order == "ctx_first" and name == "fmmb_ctx_destroy") or (order == "plan_first" and name == "fmmb_plan_destroy")
+                    or (order == "cache_first" and name == "fmmb_cache_destroy")):
+                assert getattr(L, name)(h) == 0
