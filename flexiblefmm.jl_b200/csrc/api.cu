@@ -620,4 +620,14 @@ int fmmb_direct_dev(fmmb_ctx* ctx, const double* src, const double* tau, int64_t
   });
 }
 
+int fmmb_direct_noalloc_dev(fmmb_ctx* ctx, const double* src, const double* tau, int64_t ns, const double* tgt,
+                            const int64_t* self_index, int64_t nt, double* pot, double* grad) {
+  return guard([&] {
+    require(ctx && src && tau && tgt, FMMB_ERR_ARGUMENT, "null argument");
+    require(ns >= 0 && nt >= 0, FMMB_ERR_DIMENSION, "negative count");
+    set_device(ctx->c);
+    direct_noalloc(ctx->c, src, tau, ns, tgt, self_index, nt, pot, grad);
+  });
+}
+
 }  // extern "C"

@@ -106,5 +106,8 @@ void evaluate_targets(State& S, const double* tg_dev, int64_t nt, int outputs, d
 void bounds(Ctx& ctx, const double* xyz_dev, int64_t n, double lo[3], double hi[3], int64_t* nonfinite);
 void direct(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
             int64_t nt, double* pot, double* grad);
+// direct_noalloc.cu: the same sums with the partials in a fixed array compiled into the library
+void direct_noalloc(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
+                    int64_t nt, double* pot, double* grad);
 
 }  // namespace fmmb

@@ -68,7 +68,7 @@ EXPORTS = (
     "fmmb_plan_destroy", "fmmb_plan_info", "fmmb_plan_box", "fmmb_plan_tree", "fmmb_plan_pairs", "fmmb_state_create",
     "fmmb_state_destroy", "fmmb_build_expansions", "fmmb_build_expansions_dev", "fmmb_evaluate_at_sources",
     "fmmb_evaluate_at_sources_dev", "fmmb_matvec", "fmmb_matvec_dev", "fmmb_evaluate", "fmmb_evaluate_dev",
-    "fmmb_state_expansions", "fmmb_direct_dev", "fmmb_profile_matvec",
+    "fmmb_state_expansions", "fmmb_direct_dev", "fmmb_profile_matvec", "fmmb_direct_noalloc_dev",
 )
 
 
@@ -115,6 +115,7 @@ def lib():
         "fmmb_state_expansions": [vp, dp, dp],
         "fmmb_direct_dev": [vp, dp, dp, i64, dp, dp, i64, dp, dp],
         "fmmb_profile_matvec": [vp, dp, dp, i64, i32, dp, dp, dp, i32, C.POINTER(C.c_int)],
+        "fmmb_direct_noalloc_dev": [vp, dp, dp, i64, dp, dp, i64, dp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

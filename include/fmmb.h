@@ -136,6 +136,19 @@ int fmmb_state_expansions(const fmmb_state* state, double* multipoles, double* l
 int fmmb_direct_dev(fmmb_ctx* ctx, const double* src_dev, const double* tau_dev, int64_t ns, const double* tgt_dev,
                     const int64_t* self_index_dev, int64_t nt, double* pot_dev, double* grad_dev);
 
+/* fmmb_direct_dev without any device allocation, for callers that cannot call cudaMalloc: an
+ * application whose device memory is held by its own pool (CUDA.jl's allocator keeps what it
+ * reserved) or a time-stepping loop that must not pay cudaMalloc's implicit synchronisation.
+ * No counterpart in the reference. Same arguments and results as fmmb_direct_dev; enqueues on
+ * the context's stream and returns without synchronising. The partial sums live in a 4 MiB
+ * array compiled into the library (held by every GPU that loads it until exit), so nt is
+ * limited to 131,072 targets (FMMB_ERR_ARGUMENT above). All calls share that array: calls that
+ * overlap on the GPU race. The first call on a device looks up the array's device address;
+ * make it before any stream capture. */
+int fmmb_direct_noalloc_dev(fmmb_ctx* ctx, const double* src_dev, const double* tau_dev, int64_t ns,
+                            const double* tgt_dev, const int64_t* self_index_dev, int64_t nt, double* pot_dev,
+                            double* grad_dev);
+
 #ifdef __cplusplus
 }
 #endif
