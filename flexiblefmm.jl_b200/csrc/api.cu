@@ -64,6 +64,23 @@ int guard(F&& f) {
 
 void set_device(const Ctx& c) { FMMB_CUDA(cudaSetDevice(c.device)); }
 
+// A device-pointer argument must be memory the context's device can read and write: its own
+// device memory, managed memory, or host memory allocated or registered by CUDA. A plain host
+// pointer (or another device's memory) would fault in the first kernel that touches it; this
+// turns that mistake into FMMB_ERR_ARGUMENT before anything is enqueued.
+void require_device_ptr(const Ctx& c, const void* p, const char* what) {
+  if (!p) return;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(FMMB_ERR_ARGUMENT, std::string(what) + ": not a CUDA pointer");
+  }
+  const bool ok = (a.type == cudaMemoryTypeDevice && a.device == c.device) || a.type == cudaMemoryTypeManaged ||
+                  (a.type == cudaMemoryTypeHost && a.devicePointer != nullptr);
+  require(ok, FMMB_ERR_ARGUMENT,
+          std::string(what) + ": not memory the context's device can access (the _dev entry points take device pointers)");
+}
+
 // square_bbox (src/tree/tree.jl:97-114) from the points' bounds
 void square_bbox(const double lo[3], const double hi[3], double origin[3], double& W0) {
   W0 = 0;
@@ -283,7 +300,9 @@ int fmmb_plan_create(fmmb_cache* cache, const double* xyz, int64_t n, const fmmb
 
 int fmmb_plan_create_dev(fmmb_cache* cache, const double* xyz_dev, int64_t n, const fmmb_tree_opts* opts, fmmb_plan** out) {
   return guard([&] {
-    require(xyz_dev != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    require(cache && xyz_dev != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    set_device(cache->parent->c);
+    require_device_ptr(cache->parent->c, xyz_dev, "points");
     plan_from_device_points(cache, xyz_dev, n, opts, out);
   });
 }
@@ -421,6 +440,8 @@ int fmmb_build_expansions_dev(fmmb_state* state, const double* xyz, const double
     State& S = state->s;
     require(n == S.plan->N, FMMB_ERR_DIMENSION, "expected " + std::to_string(S.plan->N) + " sources and densities");
     set_device(*S.plan->ctx);
+    require_device_ptr(*S.plan->ctx, xyz, "points");
+    require_device_ptr(*S.plan->ctx, tau, "densities");
     state_build(S, xyz, tau);
   });
 }
@@ -451,6 +472,8 @@ int fmmb_evaluate_at_sources_dev(fmmb_state* state, int outputs, double* pot, do
     require(!(outputs & FMMB_OUTPUT_POTENTIAL) || pot, FMMB_ERR_ARGUMENT, "null potential output");
     require(!(outputs & FMMB_OUTPUT_GRADIENT) || grad, FMMB_ERR_ARGUMENT, "null gradient output");
     set_device(*S.plan->ctx);
+    if (outputs & FMMB_OUTPUT_POTENTIAL) require_device_ptr(*S.plan->ctx, pot, "potential output");
+    if (outputs & FMMB_OUTPUT_GRADIENT) require_device_ptr(*S.plan->ctx, grad, "gradient output");
     evaluate_sources(S, outputs, pot, grad);
   });
 }
@@ -517,7 +540,12 @@ int fmmb_evaluate_dev(fmmb_state* state, const double* tg, int64_t nt, int outpu
     require(S.built, FMMB_ERR_ARGUMENT, "the state has no expansions yet (build_expansions first)");
     if (nt == 0) return;
     require(tg != nullptr, FMMB_ERR_ARGUMENT, "null targets");
+    require(!(outputs & FMMB_OUTPUT_POTENTIAL) || pot, FMMB_ERR_ARGUMENT, "null potential output");
+    require(!(outputs & FMMB_OUTPUT_GRADIENT) || grad, FMMB_ERR_ARGUMENT, "null gradient output");
     set_device(*S.plan->ctx);
+    require_device_ptr(*S.plan->ctx, tg, "targets");
+    if (outputs & FMMB_OUTPUT_POTENTIAL) require_device_ptr(*S.plan->ctx, pot, "potential output");
+    if (outputs & FMMB_OUTPUT_GRADIENT) require_device_ptr(*S.plan->ctx, grad, "gradient output");
     evaluate_targets(S, tg, nt, outputs, pot, grad);
   });
 }
@@ -555,7 +583,13 @@ int fmmb_profile_matvec(fmmb_state* state, const double* xyz, const double* tau,
     State& S = state->s;
     Plan& P = *S.plan;
     require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and densities");
+    require(!(outputs & FMMB_OUTPUT_POTENTIAL) || pot, FMMB_ERR_ARGUMENT, "null potential output");
+    require(!(outputs & FMMB_OUTPUT_GRADIENT) || grad, FMMB_ERR_ARGUMENT, "null gradient output");
     set_device(*P.ctx);
+    require_device_ptr(*P.ctx, xyz, "points");
+    require_device_ptr(*P.ctx, tau, "densities");
+    if (outputs & FMMB_OUTPUT_POTENTIAL) require_device_ptr(*P.ctx, pot, "potential output");
+    if (outputs & FMMB_OUTPUT_GRADIENT) require_device_ptr(*P.ctx, grad, "gradient output");
     cudaStream_t s = P.ctx->stream;
     cudaEvent_t ev[7];
     for (auto& e : ev) FMMB_CUDA(cudaEventCreate(&e));
@@ -616,6 +650,12 @@ int fmmb_direct_dev(fmmb_ctx* ctx, const double* src, const double* tau, int64_t
     require(ctx && src && tau && tgt, FMMB_ERR_ARGUMENT, "null argument");
     require(ns >= 0 && nt >= 0, FMMB_ERR_DIMENSION, "negative count");
     set_device(ctx->c);
+    require_device_ptr(ctx->c, src, "sources");
+    require_device_ptr(ctx->c, tau, "densities");
+    require_device_ptr(ctx->c, tgt, "targets");
+    require_device_ptr(ctx->c, self_index, "self index");
+    require_device_ptr(ctx->c, pot, "potential output");
+    require_device_ptr(ctx->c, grad, "gradient output");
     direct(ctx->c, src, tau, ns, tgt, self_index, nt, pot, grad);
   });
 }
@@ -626,6 +666,9 @@ int fmmb_direct_noalloc_dev(fmmb_ctx* ctx, const double* src, const double* tau,
     require(ctx && src && tau && tgt, FMMB_ERR_ARGUMENT, "null argument");
     require(ns >= 0 && nt >= 0, FMMB_ERR_DIMENSION, "negative count");
     set_device(ctx->c);
+    for (const void* p : {(const void*)src, (const void*)tau, (const void*)tgt, (const void*)self_index, (const void*)pot,
+                          (const void*)grad})
+      require_device_ptr(ctx->c, p, "fmmb_direct_noalloc_dev argument");
     direct_noalloc(ctx->c, src, tau, ns, tgt, self_index, nt, pot, grad);
   });
 }

@@ -262,3 +262,36 @@ def test_handles_destroyed_in_any_order(fmmb):
             if not ((order == "ctx_first" and name == "fmmb_ctx_destroy") or (order == "plan_first" and name == "fmmb_plan_destroy")
                     or (order == "cache_first" and name == "fmmb_cache_destroy")):
                 assert getattr(L, name)(h) == 0
+
+
+def test_dev_entry_points_reject_host_pointers(fmmb):
+    """A plain host array handed to a _dev entry point is an ArgumentError raised before any
+    launch (the library checks every pointer's attributes), not a device fault."""
+    import ctypes as C
+    import torch
+    from cuda.bindings import runtime as cudart
+    rng = np.random.default_rng(61)
+    pts = rng.random((4000, 3))
+    tau = rng.standard_normal(4000)
+    host = np.zeros(3 * 4000)
+    err, attr = cudart.cudaPointerGetAttributes(host.ctypes.data)
+    if err != cudart.cudaError_t.cudaSuccess or attr.type != cudart.cudaMemoryType.cudaMemoryTypeUnregistered:
+        pytest.skip("plain host memory is device-accessible here")
+    L = fmmb.lib()
+    f = fmmb.FMM(_method(fmmb, 6), pts, ppl=40, bbox=BOX)
+    st = fmmb.FMMState(f)
+    x_d = torch.from_numpy(pts).cuda()
+    t_d = torch.from_numpy(tau).cuda()
+    u_d = torch.zeros(4000, dtype=torch.float64, device="cuda")
+    P = lambda t: C.c_void_p(t.data_ptr())
+    H = C.c_void_p(host.ctypes.data)
+    assert L.fmmb_build_expansions_dev(st._h, H, P(t_d), 4000) == 1
+    assert L.fmmb_build_expansions_dev(st._h, P(x_d), H, 4000) == 1
+    assert b"device pointers" in L.fmmb_last_error()
+    assert L.fmmb_matvec_dev(st._h, P(x_d), P(t_d), 4000, 1, H, None) == 1
+    assert L.fmmb_evaluate_dev(st._h, H, 10, 1, P(u_d), None) == 1
+    assert L.fmmb_direct_dev(fmmb.default_context()._h, H, P(t_d), 4000, P(x_d), None, 10, P(u_d), None) == 1
+    # the state is still usable and correct afterwards
+    assert L.fmmb_matvec_dev(st._h, P(x_d), P(t_d), 4000, 1, P(u_d), None) == 0
+    ref = fmmb.evaluate_at_sources(f, fmmb.build_expansions(f, pts, tau))
+    assert np.array_equal(u_d.cpu().numpy(), ref)
