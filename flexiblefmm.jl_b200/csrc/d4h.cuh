@@ -13,7 +13,7 @@ extern __constant__ int c_d4h[NFAR];
 void upload_d4h(const HostOperators& h, cudaStream_t s);
 
 // (n, m, part) of entry k of the real storage: part 0 for m = 0, 1 for Re, 2 for Im
-__device__ __forceinline__ void coef_nmp(int k, int& n, int& m, int& part) {
+__host__ __device__ __forceinline__ void coef_nmp(int k, int& n, int& m, int& part) {
   n = (int)sqrtf((float)k + 0.5f);
   while (n * n > k) --n;
   while ((n + 1) * (n + 1) <= k) ++n;
@@ -23,7 +23,7 @@ __device__ __forceinline__ void coef_nmp(int k, int& n, int& m, int& part) {
 }
 
 // the sign of an entry of the given part, for q quarter-turns and n + m
-__device__ __forceinline__ int perm_sign(int part, int q, int npm, int fac) {
+__host__ __device__ __forceinline__ int perm_sign(int part, int q, int npm, int fac) {
   const int s = ((fac & 8) && (npm & 1)) ? -1 : 1;
   if (part == 0) return s;
   if (part == 1) return q < 2 ? s : -s;

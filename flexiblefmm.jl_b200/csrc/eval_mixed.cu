@@ -151,9 +151,9 @@ void eval_mixed(State& S, const int* gnode, const int* gstart, const int* gcount
     if (self) launch<pp, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad); \
     else launch<pp, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);     \
     break;
-    X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
+    X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11)
 #undef X
-    default: throw Error(FMMB_ERR_UNSUPPORTED, "the mixed path is built for p ≤ 10");
+    default: throw Error(FMMB_ERR_UNSUPPORTED, "the mixed path is built for p ≤ 11");
   }
 }
 

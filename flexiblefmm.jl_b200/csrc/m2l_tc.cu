@@ -1,32 +1,40 @@
-// The mixed path's M2L on the 5th-generation tensor cores (tcgen05, kind::tf32).
+// The mixed path's M2L on the 5th-generation tensor cores (tcgen05, kind::f16).
 //
 // Same work decomposition as the FP64 kernel (one CTA per block of targets, the block's far
 // pairs grouped by symmetry class; src/device_passes.jl:565-580, harmonics.jl:589-645), with
-// the class product on the tensor cores in three-term split precision: every operand x is
-// split into a TF32 head and a TF32 tail, x ≈ hi(x) + lo(x) (22 significant bits), and
-//   A·B ≈ hi(A)·hi(B) + hi(A)·lo(B) + lo(A)·hi(B)
-// accumulated in FP32 in tensor memory.
+// the class product on the tensor cores in three-term split precision over FP16:
+//   - every multipole column is scaled by a power of two (per node, so that its largest entry
+//     lies in [2^13, 2^14)) and split into an FP16 head and tail, x·2^e ≈ hi + lo (22
+//     significant bits over FP16's range; the scale keeps every column inside it);
+//   - every row of a class operator is scaled the same way (per class and (n, m) pair of rows);
+//   - A·B ≈ hi(A)·hi(B) + hi(A)·lo(B) + lo(A)·hi(B), accumulated in FP32 in tensor memory;
+//     FP16 products are exact in FP32. The read-back removes both scales (exact powers of two).
+// Orders with (p+1)² ≤ 128 use one 128-row tile of outputs; up to (p+1)² = 144 (p = 11) a
+// second tile covers rows 128..(p+1)²-1.
 //
-// Per CTA, three roles connected by mbarriers over a two-stage ring (warp specialisation):
-//   - warps 4-7 gather chunk i (≤ 48 pairs of one class: P_sᵀ M_src from the FP32 multipoles,
-//     one float4 per lane, split into head and tail) into B stage i mod 2, in the UMMA K-major
-//     canonical layout (8-row × 16-byte core matrices), and arrive on full[s];
-//   - one thread of warp 8 loads the class representative (split and laid out on the host)
-//     by one bulk copy (cp.async.bulk, no tensor map, no multicast) when the class changes,
-//     after the previous class's MMAs completed; then per chunk waits full[s] and tempty[s],
-//     issues 16 K-steps × 3 MMAs (M = 128, N = chunk rounded to 16, K = 8) into accumulator
-//     stage s of tensor memory and commits them to done[s];
-//   - warps 0-3 wait done[s], read the accumulator back (tcgen05.ld 32x32b: thread = output
-//     row), apply P_t, sum the consecutive pairs of each target and add the sum to its FP64
+// Per CTA, three roles connected by mbarriers over a ring of STAGES (warp specialisation):
+//   - 4 gather warps build chunk i (≤ 64 pairs of one class) in B stage i mod STAGES, in the
+//     UMMA K-major canonical layout (8-row × 16-byte core matrices, no swizzle): 8 consecutive
+//     lanes write the 8 pairs of one core matrix (one 128-byte row of banks), 4 lanes read 64
+//     contiguous bytes of one source column. The source-side signed permutation P_sᵀ is applied
+//     on the way: for odd quarter-turn rotations the two entries of every odd-order pair swap
+//     (two byte permutes per 32-bit word, the neighbour words from the adjacent lanes), then
+//     the signs are flipped by one XOR per word;
+//   - one thread loads the class operator (head and tail, laid out on the host) with one bulk
+//     copy (cp.async.bulk, no tensor map, no multicast) when the class changes, after the
+//     previous class's MMAs completed; then per chunk issues (p+1)²/16 K-steps × tiles × 3 MMAs
+//     (M = 128, N = chunk rounded to 16, K = 16) into accumulator stage s and commits them;
+//   - the read-back warps (thread = output row) load the stage from tensor memory, apply the
+//     target-side permutation P_t (one shuffle), sum the consecutive pairs of each target in
+//     FP32 and add the sum, with both scales and the level factor W_ref/w applied, to the FP64
 //     partial local with a reduction (the block owns its targets and each entry has one
-//     writing thread, so the additions apply in program order: deterministic), then arrive on
-//     tempty[s], which frees the stage for the next gather and MMAs.
-// The signed permutations are per-thread 32-bit masks indexed by the offset's D4h element
-// (2 bits per element: swap the (n, m) pair's entries, negate).
+//     writing thread, so the additions apply in program order: deterministic).
 // Every wait on an mbarrier is bounded and also gives up when another role has given up; the
 // CTA then waits (bounded) for the copies and MMAs it issued, records an error in a device
 // flag, frees its tensor memory and returns; the host turns the flag into FMMB_ERR_TIMEOUT.
 #include <cstring>
+
+#include <cuda_fp16.h>
 
 #include "d4h.cuh"
 #include "passes.cuh"
@@ -34,46 +42,37 @@
 namespace fmmb {
 namespace {
 
-constexpr int KT = 128;           // padded expansion length (rows of A, K of the product)
-constexpr int NCH_MAX = 48;       // pairs per MMA chunk
+constexpr int NCHK = 64;          // pairs per MMA chunk (the N of the MMA)
 constexpr int CORE = 128;         // bytes of one 8 × 16 B core matrix
-constexpr int KCH = KT / 4;       // 16-byte K-chunks per row (fp32)
-constexpr int A_BYTES = KT * KT * 4;             // one split half of a representative
-constexpr int B_BYTES = NCH_MAX * KT * 4;        // one split half of a chunk
+constexpr int NPMAX = 144;        // (p+1)² supported: p ≤ 11
+constexpr int GROUP = 32;         // entries one gather lane octet covers per instruction (4 core columns)
 constexpr unsigned long long SPIN_LIMIT = 1ull << 26;
 constexpr uint64_t WAIT_NS = 1000000000ull;  // one second: a wait in a working pipeline takes microseconds
-constexpr int TC_THREADS = 288;   // 9 warps: read-back, gather, issue
-constexpr int TMEM_COLS = 128;
+constexpr int TMEM_COLS = 512;
+constexpr uint32_t SEL_IDENTITY = 0x32107654u;  // selA = 0x7654 (the word itself), selB = 0x3210 (kept)
 
-// canonical K-major offset (bytes) of element (row, k) in a tile with KT columns
-__host__ __device__ __forceinline__ uint32_t canon_off(int row, int k) {
-  return (uint32_t)(((row >> 3) * KCH + (k >> 2)) * CORE + (row & 7) * 16 + (k & 3) * 4);
-}
+__host__ __device__ constexpr int kp_of(int np) { return (np + 15) / 16 * 16; }          // K, padded to the MMA's K
+__host__ __device__ constexpr int rows_of(int np) { return np > 128 ? 128 + (np - 128 + 7) / 8 * 8 : 128; }  // rows stored
 
-// round-to-nearest (ties away) to TF32, as cvt.rna.tf32.f32 does
-__host__ __device__ __forceinline__ float tf32_round(float x) {
-  uint32_t u;
-  memcpy(&u, &x, 4);
-  if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
-  float r;
-  memcpy(&r, &u, 4);
-  return r;
+// canonical K-major offset (bytes) of FP16 element (row, k) in a tile with kp columns
+__host__ __device__ __forceinline__ uint32_t canon16(int row, int k, int kp) {
+  return (uint32_t)((row >> 3) * (kp / 8) * CORE + (k >> 3) * CORE + (row & 7) * 16 + (k & 7) * 2);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3fff);               // start address
   d |= (uint64_t)((CORE >> 4) & 0x3fff) << 16;          // leading byte offset: next core matrix along K
-  d |= (uint64_t)(((KCH * CORE) >> 4) & 0x3fff) << 32;  // stride byte offset: next 8-row group
+  d |= (uint64_t)((sbo >> 4) & 0x3fff) << 32;           // stride byte offset: next 8-row group
   d |= (uint64_t)1 << 46;                               // descriptor version (sm_100)
   return d;                                             // base offset 0, no swizzle
 }
 
-// instruction descriptor: D f32, A/B tf32, both K-major, M = 128, N = n
+// instruction descriptor: D f32, A/B f16, both K-major, M = 128, N = n
 __device__ __forceinline__ uint32_t instr_desc(int n) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
@@ -113,6 +112,27 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
+// a bounded wait that also gives up when another role aborted
+__device__ __forceinline__ bool mbar_wait_abortable(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  const uint32_t a = smem_u32(bar);
+  uint64_t t0 = 0;
+  for (unsigned long long it = 0; it < SPIN_LIMIT; ++it) {
+    if (mbar_try(a, parity)) return true;
+    if ((it & 63) == 63) {
+      if (*abort_flag) return false;
+      const uint64_t t = global_ns();
+      if (t0 == 0) t0 = t;
+      else if (t - t0 > WAIT_NS) break;
+    }
+  }
+  *abort_flag = 1;
+  return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
@@ -120,11 +140,11 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                : "memory");
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
 }
 
@@ -150,7 +170,7 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 
 // the 16 D4h elements' (swap, negate) codes for one entry, 2 bits per element; the source
 // side (gather, phase conjugated) or the target side (scatter, sign of the partner when swapped)
-__device__ __forceinline__ uint32_t perm_mask(int k, bool target) {
+__host__ __device__ __forceinline__ uint32_t perm_mask(int k, bool target) {
   int n, m, part;
   coef_nmp(k, n, m, part);
   uint32_t mask = 0;
@@ -164,65 +184,63 @@ __device__ __forceinline__ uint32_t perm_mask(int k, bool target) {
   return mask;
 }
 
-struct __align__(16) PairInfo { int src[NCH_MAX]; int fac[NCH_MAX]; int tgt[NCH_MAX]; int n; };
+struct __align__(16) PairInfo { float cs[NCHK]; int fac[NCHK]; int tgt[NCHK]; int n; };
 
-constexpr int STAGES = 2;            // B operand / accumulator ring
-constexpr int STAGE_COLS = 64;       // tensor-memory columns per accumulator stage
-constexpr int STAGE_BYTES = 2 * B_BYTES;
-constexpr size_t TC_SMEM = 2 * (size_t)A_BYTES + STAGES * (size_t)STAGE_BYTES + STAGES * sizeof(PairInfo) +
-                           NFAR * sizeof(int) + 16 * sizeof(uint64_t);
+template <int KP, int MT>
+struct TcCfg {
+  static constexpr int KC = KP / 8;                        // 16-byte core columns along K
+  static constexpr int SBO = KC * CORE;                    // bytes between 8-row groups
+  static constexpr int U = (KC + 3) / 4;                   // gather instructions per column and half
+  static constexpr int A_BYTES = 2 * (MT == 1 ? 128 : NPMAX) * KP * 2;   // head + tail of one class
+  static constexpr int B_HALF = NCHK * KP * 2;
+  static constexpr int STAGE_BYTES = 2 * B_HALF;
+  static constexpr int STAGES = MT == 1 ? 4 : 3;
+  static constexpr int NEPI = 4 + (MT - 1);                // read-back warps
+  static constexpr int THREADS = 32 * (NEPI + 5);          // + 4 gather warps + 1 issuing warp
+  static constexpr int B_OFF = (A_BYTES + 1023) / 1024 * 1024;
+  static constexpr int PI_OFF = B_OFF + STAGES * STAGE_BYTES;
+  static constexpr int SGN_OFF = PI_OFF + STAGES * (int)sizeof(PairInfo);
+  static constexpr int D4H_OFF = SGN_OFF + 16 * KC * 16;
+  static constexpr int BAR_OFF = D4H_OFF + NFAR * 4;
+  static constexpr int SMEM = BAR_OFF + (1 + 3 * STAGES) * 8 + 16;
+  static_assert(STAGES * MT * NCHK <= TMEM_COLS, "tensor memory");
+  static_assert(SMEM <= 227 * 1024, "shared memory");
+};
 
-// roles: warps 0-3 read back and scatter (thread = output row), warps 4-7 gather, warp 8 issues
-constexpr int N_EPI = 128, N_PROD = 128;
-
-// a bounded wait that also gives up when another role aborted
-__device__ __forceinline__ bool mbar_wait_abortable(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
-  const uint32_t a = smem_u32(bar);
-  uint64_t t0 = 0;
-  for (unsigned long long it = 0; it < SPIN_LIMIT; ++it) {
-    if (mbar_try(a, parity)) return true;
-    if ((it & 63) == 63) {
-      if (*abort_flag) return false;
-      const uint64_t t = global_ns();
-      if (t0 == 0) t0 = t;
-      else if (t - t0 > WAIT_NS) break;
-    }
-  }
-  *abort_flag = 1;
-  return false;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__global__ void __launch_bounds__(TC_THREADS, 1)
+// perm16 (global): KC × 4 byte selectors of the odd quarter-turn swaps (selA | selB << 16 per
+// 32-bit word), then 16 × KC × 4 sign words (0x8000 in each FP16 half that is negated)
+template <int KP, int MT>
+__global__ void __launch_bounds__(TcCfg<KP, MT>::THREADS, 1)
 k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const int2* __restrict__ pairs,
-         const float* __restrict__ reps_split, const double* __restrict__ m2l_scale, int NP, int LD,
-         const float* __restrict__ Mf, double* __restrict__ Pl, int* __restrict__ err) {
+         const uint16_t* __restrict__ reps16, const float* __restrict__ row_scale, const uint32_t* __restrict__ perm16,
+         const double* __restrict__ m2l_scale, int NP, int LD, int lo_off, const uint16_t* __restrict__ Mh,
+         const uint16_t* __restrict__ Ml, const float* __restrict__ Msc, double* __restrict__ Pl, int* __restrict__ err) {
+  using G = TcCfg<KP, MT>;
   extern __shared__ __align__(1024) unsigned char sm[];
-  unsigned char* sA = sm;                                         // hi then lo, A_BYTES each
-  unsigned char* sB = sm + 2 * A_BYTES;                           // stage s: hi at s·STAGE_BYTES, lo after it
-  PairInfo* pinfo = (PairInfo*)(sB + STAGES * STAGE_BYTES);       // per stage
-  int* s_d4h = (int*)(pinfo + STAGES);
-  uint64_t* bars = (uint64_t*)(s_d4h + NFAR);                     // 8-byte aligned: NFAR is even
+  unsigned char* sA = sm;                                         // head rows, then the tail at lo_off
+  unsigned char* sB = sm + G::B_OFF;                              // stage s: head at s·STAGE_BYTES, tail after it
+  PairInfo* pinfo = (PairInfo*)(sm + G::PI_OFF);                  // per stage
+  uint4* s_sgn = (uint4*)(sm + G::SGN_OFF);                       // [16][KC]
+  int* s_d4h = (int*)(sm + G::D4H_OFF);
+  uint64_t* bars = (uint64_t*)(sm + G::BAR_OFF);
   uint64_t* bar_a = bars;                                         // operator load
-  uint64_t* full = bars + 1;                                      // [STAGES] gathered (N_PROD arrivals)
-  uint64_t* done = bars + 1 + STAGES;                             // [STAGES] MMAs complete (commit)
-  uint64_t* tempty = bars + 1 + 2 * STAGES;                       // [STAGES] read back (N_EPI arrivals)
-  uint32_t* tmem_slot = (uint32_t*)(bars + 1 + 3 * STAGES);
+  uint64_t* full = bars + 1;                                      // [STAGES] gathered (128 arrivals)
+  uint64_t* done = bars + 1 + G::STAGES;                          // [STAGES] MMAs complete (commit)
+  uint64_t* tempty = bars + 1 + 2 * G::STAGES;                    // [STAGES] read back (NEPI·32 arrivals)
+  uint32_t* tmem_slot = (uint32_t*)(bars + 1 + 3 * G::STAGES);
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int4 b = blocks[blockIdx.x];
   const int* co = cls_off + (int64_t)blockIdx.x * (NCLASS + 1);
 
-  for (int f = tid; f < NFAR; f += TC_THREADS) s_d4h[f] = c_d4h[f];
+  for (int f = tid; f < NFAR; f += G::THREADS) s_d4h[f] = c_d4h[f];
+  for (int e = tid; e < 16 * G::KC; e += G::THREADS) s_sgn[e] = reinterpret_cast<const uint4*>(perm16 + 4 * G::KC)[e];
   if (tid == 0) {
     mbar_init(bar_a, 1);
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], N_PROD);
+    for (int s = 0; s < G::STAGES; ++s) {
+      mbar_init(&full[s], 128);
       mbar_init(&done[s], 1);
-      mbar_init(&tempty[s], N_EPI);
+      mbar_init(&tempty[s], 32 * G::NEPI);
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -237,125 +255,137 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
 
-  if (warp < 4) {
-    // ---------------- read back and scatter: thread = output row
-    const int row = tid;
+  if (warp < G::NEPI) {
+    // ---------------- read back and scatter: thread = output row of tile `tile`
+    const int tile = warp >> 2, quad = warp & 3;
+    const int row = 128 * tile + 32 * quad + lane;
+    const bool live = row < NP;
     const double alpha = m2l_scale[b.x];
-    const uint32_t emask = perm_mask(row, true);
-    int en, em, epart;
-    coef_nmp(row, en, em, epart);
-    const int partner = epart == 0 ? row : (epart == 1 ? row + 1 : row - 1);
-    const int src_lane = (partner - 32 * warp) & 31;   // the partner is in the same warp for rows < 121
+    uint32_t emask = 0;
+    int src_lane = lane;
+    if (live) {
+      int en, em, epart;
+      coef_nmp(row, en, em, epart);
+      emask = perm_mask(row, true);
+      const int partner = epart == 0 ? row : (epart == 1 ? row + 1 : row - 1);
+      src_lane = partner & 31;                       // pairs never straddle a 32-row boundary (p ≤ 11)
+    }
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
       const int a0 = co[c], a1 = co[c + 1];
-      for (int q0 = a0; q0 < a1; q0 += NCH_MAX, ++i) {
-        const int s = i % STAGES;
-        const uint32_t ph = (uint32_t)(i / STAGES) & 1;
+      if (a0 == a1) continue;
+      const double rs = live ? alpha * (double)row_scale[c * NP + row] : 0.0;
+      for (int q0 = a0; q0 < a1; q0 += NCHK, ++i) {
+        const int s = i % G::STAGES;
+        const uint32_t ph = (uint32_t)(i / G::STAGES) & 1;
         const bool w = mbar_wait_abortable(&full[s], ph, abort_flag) && mbar_wait_abortable(&done[s], ph, abort_flag);
         if (!__all_sync(0xffffffffu, w)) { ok = false; break; }   // the warp leaves together (tcgen05.ld is warp-wide)
         tc_fence_after();
         const PairInfo& pi = pinfo[s];
         const int nc = pi.n;
-        float d[NCH_MAX];
-        const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(s * STAGE_COLS);
+        float d[NCHK];
+        const uint32_t ta = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)((s * MT + tile) * NCHK);
 #pragma unroll
-        for (int c16 = 0; c16 < NCH_MAX / 16; ++c16) tmem_ld16(ta + 16 * c16, d + 16 * c16);
+        for (int c16 = 0; c16 < NCHK / 16; ++c16) tmem_ld16(ta + 16 * c16, d + 16 * c16);
         tmem_wait_ld();
         int cur = -1;
         float run = 0.f;
 #pragma unroll
-        for (int q = 0; q < NCH_MAX; ++q) {
+        for (int q = 0; q < NCHK; ++q) {
           if (q < nc) {                                   // uniform across the warp
             const float other = __shfl_sync(0xffffffffu, d[q], src_lane);
-            if (row < NP) {
+            if (live) {
               const int t = pi.tgt[q];
               if (t != cur) {
-                if (cur >= 0) atomicAdd(&Pl[(int64_t)(b.y + cur) * LD + row], alpha * (double)run);
+                if (cur >= 0) atomicAdd(&Pl[(int64_t)(b.y + cur) * LD + row], rs * (double)run);
                 cur = t;
                 run = 0.f;
               }
               const uint32_t code = emask >> (2 * pi.fac[q]);
-              const float y = (code & 1) ? other : d[q];
+              const float y = ((code & 1) ? other : d[q]) * pi.cs[q];
               run += (code & 2) ? -y : y;
             }
           }
         }
         // the only writer of these entries: the reductions apply in program order
-        if (cur >= 0) atomicAdd(&Pl[(int64_t)(b.y + cur) * LD + row], alpha * (double)run);
+        if (cur >= 0) atomicAdd(&Pl[(int64_t)(b.y + cur) * LD + row], rs * (double)run);
         tc_fence_before();
         mbar_arrive(&tempty[s]);
       }
     }
-  } else if (warp < 8) {
-    // ---------------- gather: warp w the columns (w − 4) + 4u; lane l the entries 4l..4l+3
-    const int pt = tid - N_EPI, pw = warp - 4;
-    uint32_t gmask[4];
-    int gpart[4];
+  } else if (warp < G::NEPI + 4) {
+    // ---------------- gather: lane octet o = lane & 7 the pairs, cq = lane >> 3 the core column
+    const int gw = warp - G::NEPI, o = lane & 7, cq = lane >> 3;
+    uint32_t sel[G::U][4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      int n, m;
-      gmask[e] = perm_mask(4 * lane + e, false);
-      coef_nmp(4 * lane + e, n, m, gpart[e]);
+    for (int u = 0; u < G::U; ++u) {
+      const int kc = 4 * u + cq;
+#pragma unroll
+      for (int w = 0; w < 4; ++w) sel[u][w] = kc < G::KC ? perm16[4 * kc + w] : SEL_IDENTITY;
     }
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
       const int a0 = co[c], a1 = co[c + 1];
-      for (int q0 = a0; q0 < a1; q0 += NCH_MAX, ++i) {
-        const int s = i % STAGES;
-        if (i >= STAGES) {
-          const bool w = mbar_wait_abortable(&tempty[s], (uint32_t)(i / STAGES - 1) & 1, abort_flag);
+      for (int q0 = a0; q0 < a1; q0 += NCHK, ++i) {
+        const int s = i % G::STAGES;
+        if (i >= G::STAGES) {
+          const bool w = mbar_wait_abortable(&tempty[s], (uint32_t)(i / G::STAGES - 1) & 1, abort_flag);
           if (!__all_sync(0xffffffffu, w)) { ok = false; break; }   // the warp leaves together (shuffles below)
         }
-        const int nc = min(NCH_MAX, a1 - q0), nn = (nc + 15) & ~15;
+        const int nc = min(NCHK, a1 - q0), nn = (nc + 15) & ~15;
         PairInfo& pi = pinfo[s];
-        // lane u < 12 of warp w reads the pair of column w + 4u and publishes it for the other roles
-        int my_src = 0, my_fac = 0;
-        if (lane < NCH_MAX / 4) {
-          const int j = pw + 4 * lane;
-          if (j < nc) {
-            const int2 pr = pairs[b.w + q0 + j];
-            my_src = pr.x;
-            my_fac = s_d4h[pr.y >> 8];
-            pi.src[j] = pr.x; pi.fac[j] = my_fac; pi.tgt[j] = pr.y & 0xff;
-          } else {
-            pi.src[j] = -1; pi.fac[j] = 0; pi.tgt[j] = -1;
+        if (gw == 0 && lane == 0) pi.n = nc;
+        unsigned char* bh = sB + s * G::STAGE_BYTES;
+#pragma unroll
+        for (int gi = 0; gi < NCHK / 32; ++gi) {
+          const int j0 = 8 * (gw + 4 * gi);
+          if (j0 >= nn) break;                           // uniform across the warp
+          int src = -1, fac = 0;
+          if (lane < 8 && j0 + lane < nc) {
+            const int2 pr = pairs[b.w + q0 + j0 + lane];
+            src = pr.x;
+            fac = s_d4h[pr.y >> 8];
+            pi.cs[j0 + lane] = Msc[src];
+            pi.fac[j0 + lane] = fac;
+            pi.tgt[j0 + lane] = pr.y & 0xff;
           }
-        }
-        if (pt == 0) pi.n = nc;
-        unsigned char* bh = sB + s * STAGE_BYTES;
-        constexpr int U = NCH_MAX / 4;
-        float4 v[U];
+          src = __shfl_sync(0xffffffffu, src, o);
+          fac = __shfl_sync(0xffffffffu, fac, o);
+          const bool odd = fac & 1;                      // odd quarter-turns swap the odd-order pairs
+          const int j = j0 + o;
+          uint4 vh[G::U], vl[G::U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int j = pw + 4 * u;
-          const int src = __shfl_sync(0xffffffffu, my_src, u);
-          v[u] = (j < nc && 4 * lane < LD) ? __ldg(reinterpret_cast<const float4*>(Mf + (int64_t)src * LD) + lane)
-                                           : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int j = pw + 4 * u;
-          if (j >= nn) continue;                          // uniform across the warp
-          const float nxt = __shfl_down_sync(0xffffffffu, v[u].x, 1);
-          const float prv = __shfl_up_sync(0xffffffffu, v[u].w, 1);
-          const int fac = __shfl_sync(0xffffffffu, my_fac, u);
-          const float a[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
-          float g[4];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const uint32_t code = gmask[e] >> (2 * fac);
-            // the partner of entry 4l+e: the next entry for a real part, the previous for an imaginary part
-            const float pv = gpart[e] == 1 ? (e < 3 ? a[e + 1] : nxt) : (e > 0 ? a[e - 1] : prv);
-            g[e] = (code & 1) ? pv : a[e];
-            if (code & 2) g[e] = -g[e];
+          for (int u = 0; u < G::U; ++u) {
+            const int kc = 4 * u + cq;
+            vh[u] = vl[u] = make_uint4(0, 0, 0, 0);
+            if (src >= 0 && kc < G::KC) {
+              vh[u] = __ldg(reinterpret_cast<const uint4*>(Mh + (int64_t)src * KP) + kc);
+              vl[u] = __ldg(reinterpret_cast<const uint4*>(Ml + (int64_t)src * KP) + kc);
+            }
           }
-          const float4 hi = make_float4(tf32_round(g[0]), tf32_round(g[1]), tf32_round(g[2]), tf32_round(g[3]));
-          const float4 lo = make_float4(tf32_round(g[0] - hi.x), tf32_round(g[1] - hi.y), tf32_round(g[2] - hi.z),
-                                        tf32_round(g[3] - hi.w));
-          const uint32_t off = canon_off(j, 4 * lane);
-          *(float4*)(bh + off) = hi;
-          *(float4*)(bh + B_BYTES + off) = lo;
+#pragma unroll
+          for (int u = 0; u < G::U; ++u) {
+            const int kc = 4 * u + cq;
+            // neighbouring words: the last of the previous core column, the first of the next
+            const uint32_t hp = __shfl_up_sync(0xffffffffu, vh[u].w, 8), hn = __shfl_down_sync(0xffffffffu, vh[u].x, 8);
+            const uint32_t lp = __shfl_up_sync(0xffffffffu, vl[u].w, 8), ln = __shfl_down_sync(0xffffffffu, vl[u].x, 8);
+            if (kc >= G::KC) continue;
+            const uint4 sg = s_sgn[fac * G::KC + kc];
+            const uint32_t wh[6] = {hp, vh[u].x, vh[u].y, vh[u].z, vh[u].w, hn};
+            const uint32_t wl[6] = {lp, vl[u].x, vl[u].y, vl[u].z, vl[u].w, ln};
+            const uint32_t sgw[4] = {sg.x, sg.y, sg.z, sg.w};
+            uint32_t oh[4], ol[4];
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+              const uint32_t sl = odd ? sel[u][w] : SEL_IDENTITY;
+              const uint32_t sa = sl & 0xffffu, sb = sl >> 16;
+              oh[w] = __byte_perm(__byte_perm(wh[w], wh[w + 1], sa), wh[w + 2], sb) ^ sgw[w];
+              ol[w] = __byte_perm(__byte_perm(wl[w], wl[w + 1], sa), wl[w + 2], sb) ^ sgw[w];
+            }
+            const uint32_t off = canon16(j, 8 * kc, KP);
+            *(uint4*)(bh + off) = make_uint4(oh[0], oh[1], oh[2], oh[3]);
+            *(uint4*)(bh + G::B_HALF + off) = make_uint4(ol[0], ol[1], ol[2], ol[3]);
+          }
         }
         fence_async_smem();
         mbar_arrive(&full[s]);
@@ -369,30 +399,37 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
       const int a0 = co[c], a1 = co[c + 1];
       if (a0 == a1) continue;
       // the previous class's MMAs must have completed before its operator is replaced
-      if (i > 0 && !mbar_wait_abortable(&done[(i - 1) % STAGES], (uint32_t)((i - 1) / STAGES) & 1, abort_flag)) { ok = false; break; }
-      bulk_load(sA, reps_split + (size_t)c * 2 * KT * KT, 2 * A_BYTES, bar_a);
+      if (i > 0 && !mbar_wait_abortable(&done[(i - 1) % G::STAGES], (uint32_t)((i - 1) / G::STAGES) & 1, abort_flag)) {
+        ok = false;
+        break;
+      }
+      bulk_load(sA, reps16 + (size_t)c * lo_off, 2u * (uint32_t)lo_off, bar_a);   // lo_off bytes = lo_off/2 elements per half
       a_pending = true;
       if (!mbar_wait_abortable(bar_a, (uint32_t)ncls & 1, abort_flag)) { ok = false; break; }
       a_pending = false;
       ++ncls;
-      for (int q0 = a0; q0 < a1; q0 += NCH_MAX, ++i) {
-        const int s = i % STAGES;
-        const uint32_t ph = (uint32_t)(i / STAGES) & 1;
+      for (int q0 = a0; q0 < a1; q0 += NCHK, ++i) {
+        const int s = i % G::STAGES;
+        const uint32_t ph = (uint32_t)(i / G::STAGES) & 1;
         if (!mbar_wait_abortable(&full[s], ph, abort_flag)) { ok = false; break; }
-        if (i >= STAGES && !mbar_wait_abortable(&tempty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+        if (i >= G::STAGES && !mbar_wait_abortable(&tempty[s], ph ^ 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
         const int nn = (pinfo[s].n + 15) & ~15;
         const uint32_t id = instr_desc(nn);
-        unsigned char* bh = sB + s * STAGE_BYTES;
-        const uint64_t dah = umma_desc(smem_u32(sA)), dal = umma_desc(smem_u32(sA + A_BYTES));
-        const uint64_t dbh = umma_desc(smem_u32(bh)), dbl = umma_desc(smem_u32(bh + B_BYTES));
-        const uint32_t td = tmem + (uint32_t)(s * STAGE_COLS);
-#pragma unroll 4
-        for (int k = 0; k < KT / 8; ++k) {
-          const uint64_t ko = (uint64_t)(k * 2 * CORE) >> 4;   // the start address advances 2 core matrices
-          mma_tf32(td, dah + ko, dbh + ko, id, k > 0 ? 1u : 0u);
-          mma_tf32(td, dah + ko, dbl + ko, id, 1u);
-          mma_tf32(td, dal + ko, dbh + ko, id, 1u);
+        const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB + s * G::STAGE_BYTES);
+#pragma unroll 2
+        for (int ks = 0; ks < KP / 16; ++ks) {
+          const uint32_t ko = (uint32_t)ks * 2 * CORE;   // 16 FP16 along K: two core matrices
+          const uint64_t dbh = umma_desc(b_base + ko, G::SBO), dbl = umma_desc(b_base + G::B_HALF + ko, G::SBO);
+#pragma unroll
+          for (int t = 0; t < MT; ++t) {
+            const uint32_t ah = a_base + (uint32_t)(t * 16 * G::SBO) + ko;
+            const uint64_t dah = umma_desc(ah, G::SBO), dal = umma_desc(ah + (uint32_t)lo_off, G::SBO);
+            const uint32_t td = tmem + (uint32_t)((s * MT + t) * NCHK);
+            mma_f16(td, dah, dbh, id, ks > 0 ? 1u : 0u);
+            mma_f16(td, dah, dbl, id, 1u);
+            mma_f16(td, dal, dbh, id, 1u);
+          }
         }
         mma_commit(&done[s]);
       }
@@ -400,7 +437,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
     if (!ok) {
       // give the work already issued a bounded time to finish before the memory is released
       if (a_pending) mbar_wait(bar_a, (uint32_t)ncls & 1);
-      if (i > 0) mbar_wait(&done[(i - 1) % STAGES], (uint32_t)((i - 1) / STAGES) & 1);
+      if (i > 0) mbar_wait(&done[(i - 1) % G::STAGES], (uint32_t)((i - 1) / G::STAGES) & 1);
     }
   }
   if (!ok) *abort_flag = 1;
@@ -410,36 +447,143 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
-__global__ void k_to_f32(const double* __restrict__ in, int64_t n, float* __restrict__ out) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = (float)in[i];
+// the multipoles of every node, scaled by a power of two so that the largest entry of the
+// column lies in [2^13, 2^14), as FP16 head and tail (one warp per node); Msc = the inverse scale
+__global__ void k_split16(const double* __restrict__ M, int nnodes, int NP, int LD, int KP, uint16_t* __restrict__ Mh,
+                          uint16_t* __restrict__ Ml, float* __restrict__ Msc) {
+  const int node = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (node >= nnodes) return;
+  const double* m = M + (int64_t)node * LD;
+  double mx = 0.0;
+  for (int k = lane; k < NP; k += 32) mx = fmax(mx, fabs(m[k]));
+  for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  int e = 0;
+  if (mx > 0.0 && mx <= 1.7e308) {                 // finite and nonzero; otherwise unscaled (0 or non-finite)
+    int ex;
+    frexp(mx, &ex);                                // mx = f·2^ex, f ∈ [0.5, 1)
+    e = 14 - ex;                                   // mx·2^e ∈ [2^13, 2^14)
+    e = max(-100, min(100, e));                    // keeps the inverse scale inside FP32's range
+  }
+  for (int k = lane; k < KP; k += 32) {
+    const double x = k < NP ? ldexp(m[k], e) : 0.0;
+    const __half h = __double2half(x);
+    const __half l = __double2half(x - (double)__half2float(h));
+    Mh[(int64_t)node * KP + k] = __half_as_ushort(h);
+    Ml[(int64_t)node * KP + k] = __half_as_ushort(l);
+  }
+  if (lane == 0) Msc[node] = (float)ldexp(1.0, -e);
 }
 
 }  // namespace
 
+// the source-side permutation of the gather for (p+1)² = np: per 16-byte core column kc and
+// 32-bit word w, the byte selectors of the odd quarter-turn swaps (selA | selB << 16, applied
+// as byte_perm(byte_perm(w[-1], w, selA), w[+1], selB)); then per D4h element g the sign words
+std::vector<uint32_t> build_perm16(int np) {
+  const int KC = kp_of(np) / 8;
+  std::vector<uint32_t> perm((size_t)4 * KC + (size_t)16 * KC * 4, 0);
+  for (int kc = 0; kc < KC; ++kc)
+    for (int w = 0; w < 4; ++w) {
+      const int k0 = 8 * kc + 2 * w, k1 = k0 + 1;
+      int loB = 4, hiB = 6, hb = 2;                    // identity: the word itself, kept
+      auto swap_of = [&](int k, int& part) {
+        int n, m;
+        coef_nmp(k, n, m, part);
+        return k < np && part != 0 && (m & 1);
+      };
+      int p0, p1;
+      if (swap_of(k0, p0)) loB = p0 == 1 ? 6 : 2;      // Re: the next entry (this word), Im: the previous word
+      if (swap_of(k1, p1)) {
+        if (p1 == 1) hb = 4;                           // Re: the first entry of the next word
+        else hiB = 4;                                  // Im: the first entry of this word
+      }
+      const uint32_t sa = (uint32_t)(loB | (loB + 1) << 4 | hiB << 8 | (hiB + 1) << 12);
+      const uint32_t sb = (uint32_t)(0 | 1 << 4 | hb << 8 | (hb + 1) << 12);
+      perm[4 * kc + w] = sa | sb << 16;
+    }
+  for (int k = 0; k < np; ++k) {
+    const uint32_t mask = perm_mask(k, false);
+    for (int g = 0; g < 16; ++g)
+      if ((mask >> (2 * g)) & 2) perm[4 * KC + ((size_t)g * KC + k / 8) * 4 + (k & 7) / 2] |= (k & 1) ? 0x80000000u : 0x8000u;
+  }
+  return perm;
+}
+
+// the class operators of the mixed path: per class, every row scaled by a power of two (its
+// largest entry in [2^13, 2^14)) and split into FP16 head then tail, in the canonical K-major
+// layout of the tensor-core M2L; rsc = the inverse row scales [class][row]
+void build_reps16(const HostOperators& op, std::vector<uint16_t>& h, std::vector<float>& rsc) {
+  const int np = op.np, LD = op.ld;
+  const int KP = kp_of(np), rows = rows_of(np);
+  const size_t half = (size_t)rows * KP;             // elements of one half (head or tail) of a class
+  // per class: row-scaled head then tail in the canonical K-major layout; inverse row scales
+  h.assign((size_t)NCLASS * 2 * half, 0);
+  rsc.assign((size_t)NCLASS * np, 1.0f);
+  for (int c = 0; c < NCLASS; ++c) {
+    uint16_t* hi = &h[(size_t)c * 2 * half];
+    uint16_t* lo = hi + half;
+    const double* A = &op.reps[(size_t)c * LD * LD];   // column-major: A[r, k] at k·LD + r
+    for (int r = 0; r < np; ++r) {
+      // the two rows of an (n, m) pair share their scale: the read-back swaps them
+      int n, m, part;
+      coef_nmp(r, n, m, part);
+      const int r2 = part == 0 ? r : (part == 1 ? r + 1 : r - 1);
+      double mx = 0.0;
+      for (int k = 0; k < np; ++k) mx = std::max(mx, std::max(std::fabs(A[(size_t)k * LD + r]), std::fabs(A[(size_t)k * LD + r2])));
+      int e = 0;
+      if (mx > 0.0) {
+        int ex;
+        std::frexp(mx, &ex);
+        e = 14 - ex;
+      }
+      rsc[(size_t)c * np + r] = (float)std::ldexp(1.0, -e);
+      for (int k = 0; k < np; ++k) {
+        const double a = std::ldexp(A[(size_t)k * LD + r], e);
+        const __half ah = __double2half(a);
+        const __half al = __double2half(a - (double)__half2float(ah));
+        const uint32_t off = canon16(r, k, KP) / 2;
+        hi[off] = __half_as_ushort(ah);
+        lo[off] = __half_as_ushort(al);
+      }
+    }
+  }
+}
+
 void prepare_mixed_operators(Cache& C) {
   if (C.split_ready) return;
-  require(C.np <= KT, FMMB_ERR_UNSUPPORTED, "the mixed path is built for p ≤ 10");
-  const int LD = C.ld;
-  // per class: the hi then the lo half, each KT × KT in the canonical K-major layout
-  std::vector<float> h((size_t)NCLASS * 2 * KT * KT, 0.0f);
-  for (int c = 0; c < NCLASS; ++c) {
-    float* hi = &h[(size_t)c * 2 * KT * KT];
-    float* lo = hi + KT * KT;
-    for (int k = 0; k < C.np; ++k)
-      for (int r = 0; r < C.np; ++r) {
-        const double a = C.host.reps[(size_t)c * LD * LD + (size_t)k * LD + r];   // column-major: A[r, k]
-        const float ah = tf32_round((float)a);
-        const float al = tf32_round((float)(a - (double)ah));
-        const uint32_t off = canon_off(r, k) / 4;
-        hi[off] = ah;
-        lo[off] = al;
-      }
+  const int np = C.np;
+  require(np <= NPMAX, FMMB_ERR_UNSUPPORTED, "the mixed path is built for p ≤ 11");
+  // the gather's lane octets and the read-back warps exchange partners inside 32 entries
+  for (int k = GROUP; k < np; k += GROUP) {
+    int n, m, part;
+    coef_nmp(k, n, m, part);
+    require(part != 2, FMMB_ERR_UNSUPPORTED, "the mixed path does not support this order");
   }
-  to_device(C.reps_split, h, C.ctx->stream);
+  std::vector<uint16_t> h;
+  std::vector<float> rsc;
+  build_reps16(C.host, h, rsc);
+  std::vector<uint32_t> perm = build_perm16(np);
+  to_device(C.reps16, h, C.ctx->stream);
+  to_device(C.row_scale, rsc, C.ctx->stream);
+  to_device(C.perm16, perm, C.ctx->stream);
   FMMB_CUDA(cudaStreamSynchronize(C.ctx->stream));
   C.split_ready = true;
 }
+
+namespace {
+template <int KP, int MT>
+void launch_tc(State& S, int nb) {
+  using G = TcCfg<KP, MT>;
+  Plan& P = *S.plan;
+  Cache& C = *P.cache;
+  const int lo_off = rows_of(C.np) * KP * 2;
+  FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc<KP, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
+  k_m2l_tc<KP, MT><<<nb, G::THREADS, G::SMEM, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps16.p, C.row_scale.p,
+                                                               C.perm16.p, P.d_m2l_scale.p, C.np, C.ld, lo_off, S.Mh.p,
+                                                               S.Ml.p, S.Msc.p, S.Pl.p, S.err.p);
+  FMMB_LAUNCH_CHECK();
+}
+}  // namespace
 
 void m2l_mixed(State& S) {
   Plan& P = *S.plan;
@@ -447,16 +591,26 @@ void m2l_mixed(State& S) {
   cudaStream_t s = P.ctx->stream;
   const int nb = (int)P.h_blocks.size();
   if (nb == 0) return;
-  const size_t ne = (size_t)P.nnodes * C.ld;
-  if (S.Mf.n < ne) S.Mf.alloc(ne);
+  const int KP = kp_of(C.np);
+  const size_t ne = (size_t)P.nnodes * KP;
+  if (S.Mh.n < ne) { S.Mh.alloc(ne); S.Ml.alloc(ne); }
+  if (S.Msc.n < (size_t)P.nnodes) S.Msc.alloc(P.nnodes);
   if (!S.err.p) S.err.alloc(1);
-  k_to_f32<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(S.M.p, (int64_t)ne, S.Mf.p);
+  k_split16<<<(unsigned)(((int64_t)P.nnodes * 32 + 255) / 256), 256, 0, s>>>(S.M.p, P.nnodes, C.np, C.ld, KP, S.Mh.p, S.Ml.p,
+                                                                              S.Msc.p);
   FMMB_LAUNCH_CHECK();
   FMMB_CUDA(cudaMemsetAsync(S.err.p, 0, sizeof(int), s));
-  FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-  k_m2l_tc<<<nb, TC_THREADS, TC_SMEM, s>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps_split.p, P.d_m2l_scale.p, C.np, C.ld,
-                                          S.Mf.p, S.Pl.p, S.err.p);
-  FMMB_LAUNCH_CHECK();
+  switch (KP) {
+    case 16: launch_tc<16, 1>(S, nb); break;
+    case 32: launch_tc<32, 1>(S, nb); break;
+    case 48: launch_tc<48, 1>(S, nb); break;
+    case 64: launch_tc<64, 1>(S, nb); break;
+    case 96: launch_tc<96, 1>(S, nb); break;
+    case 112: launch_tc<112, 1>(S, nb); break;
+    case 128: launch_tc<128, 1>(S, nb); break;
+    case 144: launch_tc<144, 2>(S, nb); break;
+    default: throw Error(FMMB_ERR_UNSUPPORTED, "the mixed path does not support this order");
+  }
 }
 
 int mixed_error_flag(State& S) {

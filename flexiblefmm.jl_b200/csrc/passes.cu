@@ -506,7 +506,7 @@ int l2l_sweep(State& S) {
   return launches;
 }
 
-// the partial locals zeroed, then the M2L of every level in one launch (plus the FP32
+// the partial locals zeroed, then the M2L of every level in one launch (plus the FP16
 // copy of the multipoles on the mixed path); returns the kernel launches
 int m2l_stage(State& S) {
   Plan& P = *S.plan;

@@ -27,9 +27,12 @@ struct Cache {
   DBuf<int16_t> gidx, sidx;
   DBuf<int8_t> gsgn, ssgn;
   DBuf<int> cls;
-  // the mixed path's class operators: per class, the split (hi, lo) TF32 copies in the
-  // canonical K-major layout the tensor-core M2L reads (m2l_tc.cu)
-  DBuf<float> reps_split;
+  // the mixed path's class operators (m2l_tc.cu): per class, the row-scaled FP16 head and
+  // tail in the canonical K-major layout of the tensor-core M2L; the inverse row scales; the
+  // source-side sign words and byte selectors of the D4h permutations
+  DBuf<uint16_t> reps16;
+  DBuf<float> row_scale;
+  DBuf<uint32_t> perm16;
   bool split_ready = false;
 };
 
@@ -81,7 +84,8 @@ struct State {
   int precision = FMMB_PRECISION_FP64;
   DBuf<double> xs, ys, zs, q;             // sources and charges in tree order
   DBuf<double> M, Pl;                     // nnodes × LD: multipoles, partial locals
-  DBuf<float> Mf;                         // the mixed path: an FP32 copy of the multipoles
+  DBuf<uint16_t> Mh, Ml;                  // the mixed path: the multipoles scaled by a power of two
+  DBuf<float> Msc;                        //   per node, as FP16 head and tail; the inverse scales
   DBuf<int> err;                          // the mixed path: the bounded-wait error flag
   bool built = false;
   // staging of the host-pointer entry points and the evaluation at targets

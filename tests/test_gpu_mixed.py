@@ -1,7 +1,8 @@
-"""The mixed path (tensor-core TF32x3 M2L, FP32 compensated near field) against the FP64
-path and FP64 direct sums. Tolerances: the locals within 2e-6 (max-norm relative) of the
-FP64 path's; potentials within 1e-6 relative L2 of FP64 direct sums at p = 10 (the metric's
-target), gradients within 1e-5."""
+"""The mixed path (tensor-core FP16x3 M2L with power-of-two scaling, FP32 compensated near
+field) against the FP64 path and FP64 direct sums. Tolerances: the locals within 2e-6
+(max-norm relative) of the FP64 path's; potentials within 1e-6 relative L2 of the FP64 path
+and of FP64 direct sums beyond the truncation error (the metric's target), gradients within
+1e-5."""
 import numpy as np
 import pytest
 
@@ -11,13 +12,15 @@ pytestmark = pytest.mark.gpu
 BOX = ((0.0, 0.0, 0.0), 1.0)
 
 
-@pytest.mark.parametrize("name,n,ppl,seed", [("uniform", 60000, 64, 1), ("mixed", 20000, 40, 2), ("sphere", 20000, 40, 3),
-                                             ("clustered", 15000, 30, 4)])
-def test_mixed_locals_match_fp64(fmmb, name, n, ppl, seed):
+@pytest.mark.parametrize("name,n,ppl,seed,p", [("uniform", 60000, 64, 1, 10), ("mixed", 20000, 40, 2, 10),
+                                               ("sphere", 20000, 40, 3, 10), ("clustered", 15000, 30, 4, 10),
+                                               ("uniform", 60000, 64, 5, 11), ("mixed", 20000, 40, 6, 11),
+                                               ("helix", 20000, 40, 7, 9), ("one_octant", 20000, 40, 8, 7)])
+def test_mixed_locals_match_fp64(fmmb, name, n, ppl, seed, p):
     rng = np.random.default_rng(seed)
     pts = DISTRIBUTIONS3[name](rng, n)
     tau = rng.standard_normal(n)
-    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=10), pts, ppl=ppl, bbox=BOX)
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=p), pts, ppl=ppl, bbox=BOX)
     s64 = fmmb.build_expansions(f, pts, tau, precision="fp64")
     s32 = fmmb.build_expansions(f, pts, tau, precision="mixed")
     M64, L64 = s64.expansions()
@@ -72,7 +75,7 @@ def test_mixed_supported_orders(fmmb):
     f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=12), pts, ppl=40, bbox=BOX)
     with pytest.raises(fmmb.Unsupported):
         fmmb.FMMState(f, "mixed")
-    for p in (4, 6):
+    for p in (1, 2, 3, 4, 5, 6, 8, 11):
         tau = rng.standard_normal(5000)
         g = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=p), pts, ppl=40, bbox=BOX)
         u32 = fmmb.evaluate_at_sources(g, fmmb.build_expansions(g, pts, tau, precision="mixed"))
