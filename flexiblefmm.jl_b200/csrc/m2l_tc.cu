@@ -13,10 +13,11 @@
 // second tile covers rows 128..(p+1)²-1.
 //
 // Per CTA, three roles connected by mbarriers over a ring of STAGES (warp specialisation):
-//   - 4 gather warps build chunk i (≤ 64 pairs of one class) in B stage i mod STAGES, in the
-//     UMMA K-major canonical layout (8-row × 16-byte core matrices, no swizzle): 8 consecutive
-//     lanes write the 8 pairs of one core matrix (one 128-byte row of banks), 4 lanes read 64
-//     contiguous bytes of one source column. The source-side signed permutation P_sᵀ is applied
+//   - one gather warp per stage builds chunk i (≤ 64 pairs of one class) in B stage i mod
+//     STAGES, so STAGES chunks are gathered at once; in the UMMA K-major canonical layout
+//     (8-row × 16-byte core matrices, no swizzle): 8 consecutive lanes write the 8 pairs of one
+//     core matrix (one 128-byte row of banks), 4 lanes read 64 contiguous bytes of one source
+//     column, and the loads of two groups of 8 pairs are in flight together. The source-side signed permutation P_sᵀ is applied
 //     on the way: for odd quarter-turn rotations the two entries of every odd-order pair swap
 //     (two byte permutes per 32-bit word, the neighbour words from the adjacent lanes), then
 //     the signs are flipped by one XOR per word;
@@ -57,6 +58,17 @@ __host__ __device__ constexpr int rows_of(int np) { return np > 128 ? 128 + (np 
 // canonical K-major offset (bytes) of FP16 element (row, k) in a tile with kp columns
 __host__ __device__ __forceinline__ uint32_t canon16(int row, int k, int kp) {
   return (uint32_t)((row >> 3) * (kp / 8) * CORE + (k >> 3) * CORE + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// bit i of x moved to bit 2i
+__device__ __forceinline__ uint64_t spread_bits(uint32_t x32) {
+  uint64_t x = x32;
+  x = (x | (x << 16)) & 0x0000ffff0000ffffull;
+  x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
+  x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
+  x = (x | (x << 2)) & 0x3333333333333333ull;
+  x = (x | (x << 1)) & 0x5555555555555555ull;
+  return x;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -163,6 +175,23 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+      "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+      "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+
+__device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
+  uint32_t r;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -184,7 +213,17 @@ __host__ __device__ __forceinline__ uint32_t perm_mask(int k, bool target) {
   return mask;
 }
 
-struct __align__(16) PairInfo { float cs[NCHK]; int fac[NCHK]; int tgt[NCHK]; int n; };
+// per chunk: the source scale, D4h element and target of every column; the target runs (bit q
+// of `starts` set where column q begins a run; per run its last column and its target)
+struct __align__(16) PairInfo {
+  float cs[NCHK];
+  int fac[NCHK];
+  int tgt[NCHK];
+  int rend[NCHK];
+  int rtgt[NCHK];
+  unsigned long long starts;
+  int n, nruns;
+};
 
 template <int KP, int MT>
 struct TcCfg {
@@ -196,14 +235,15 @@ struct TcCfg {
   static constexpr int STAGE_BYTES = 2 * B_HALF;
   static constexpr int STAGES = MT == 1 ? 4 : 3;
   static constexpr int NEPI = 4 + (MT - 1);                // read-back warps
-  static constexpr int THREADS = 32 * (NEPI + 5);          // + 4 gather warps + 1 issuing warp
+  static constexpr int THREADS = 32 * (NEPI + STAGES + 1); // + one gather warp per stage + 1 issuing warp
   static constexpr int B_OFF = (A_BYTES + 1023) / 1024 * 1024;
   static constexpr int PI_OFF = B_OFF + STAGES * STAGE_BYTES;
   static constexpr int SGN_OFF = PI_OFF + STAGES * (int)sizeof(PairInfo);
   static constexpr int D4H_OFF = SGN_OFF + 16 * KC * 16;
   static constexpr int BAR_OFF = D4H_OFF + NFAR * 4;
   static constexpr int SMEM = BAR_OFF + (1 + 3 * STAGES) * 8 + 16;
-  static_assert(STAGES * MT * NCHK <= TMEM_COLS, "tensor memory");
+  static constexpr int SCAN_COL = STAGES * MT * NCHK;    // per tile NCHK columns of run sums
+  static_assert(SCAN_COL + MT * NCHK <= TMEM_COLS, "tensor memory");
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
@@ -224,7 +264,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   int* s_d4h = (int*)(sm + G::D4H_OFF);
   uint64_t* bars = (uint64_t*)(sm + G::BAR_OFF);
   uint64_t* bar_a = bars;                                         // operator load
-  uint64_t* full = bars + 1;                                      // [STAGES] gathered (128 arrivals)
+  uint64_t* full = bars + 1;                                      // [STAGES] gathered (32 arrivals)
   uint64_t* done = bars + 1 + G::STAGES;                          // [STAGES] MMAs complete (commit)
   uint64_t* tempty = bars + 1 + 2 * G::STAGES;                    // [STAGES] read back (NEPI·32 arrivals)
   uint32_t* tmem_slot = (uint32_t*)(bars + 1 + 3 * G::STAGES);
@@ -238,7 +278,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   if (tid == 0) {
     mbar_init(bar_a, 1);
     for (int s = 0; s < G::STAGES; ++s) {
-      mbar_init(&full[s], 128);
+      mbar_init(&full[s], 32);
       mbar_init(&done[s], 1);
       mbar_init(&tempty[s], 32 * G::NEPI);
     }
@@ -270,6 +310,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
       const int partner = epart == 0 ? row : (epart == 1 ? row + 1 : row - 1);
       src_lane = partner & 31;                       // pairs never straddle a 32-row boundary (p ≤ 11)
     }
+    const uint32_t scan = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(G::SCAN_COL + tile * NCHK);
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
       const int a0 = co[c], a1 = co[c + 1];
@@ -282,39 +323,57 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         if (!__all_sync(0xffffffffu, w)) { ok = false; break; }   // the warp leaves together (tcgen05.ld is warp-wide)
         tc_fence_after();
         const PairInfo& pi = pinfo[s];
-        const int nc = pi.n;
-        float d[NCHK];
+        const int nc = pi.n, nruns = pi.nruns;
+        const uint64_t starts = pi.starts;
         const uint32_t ta = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)((s * MT + tile) * NCHK);
+        // phase 1 (branch-free): per column the permuted, unscaled value, and the running sum of
+        // the column's target run (reset where a run starts), parked in this tile's scan columns
+        float acc = 0.f;
 #pragma unroll
-        for (int c16 = 0; c16 < NCHK / 16; ++c16) tmem_ld16(ta + 16 * c16, d + 16 * c16);
-        tmem_wait_ld();
-        int cur = -1;
-        float run = 0.f;
+        for (int c16 = 0; c16 < NCHK / 16; ++c16) {
+          if (16 * c16 >= nc) break;                      // uniform across the warp
+          float d[16], a[16];
+          tmem_ld16(ta + 16 * c16, d);
+          tmem_wait_ld();
 #pragma unroll
-        for (int q = 0; q < NCHK; ++q) {
-          if (q < nc) {                                   // uniform across the warp
-            const float other = __shfl_sync(0xffffffffu, d[q], src_lane);
-            if (live) {
-              const int t = pi.tgt[q];
-              if (t != cur) {
-                if (cur >= 0) atomicAdd(&Pl[(int64_t)(b.y + cur) * LD + row], rs * (double)run);
-                cur = t;
-                run = 0.f;
-              }
-              const uint32_t code = emask >> (2 * pi.fac[q]);
-              const float y = ((code & 1) ? other : d[q]) * pi.cs[q];
-              run += (code & 2) ? -y : y;
+          for (int e4 = 0; e4 < 4; ++e4) {
+            const int4 f4 = reinterpret_cast<const int4*>(pi.fac)[4 * c16 + e4];
+            const float4 c4 = reinterpret_cast<const float4*>(pi.cs)[4 * c16 + e4];
+            const int ff[4] = {f4.x, f4.y, f4.z, f4.w};
+            const float cc[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int q = 16 * c16 + 4 * e4 + e;
+              const float v = d[4 * e4 + e];
+              const float other = __shfl_sync(0xffffffffu, v, src_lane);
+              const uint32_t code = emask >> (2 * ff[e]);
+              float y = ((code & 1) ? other : v) * cc[e];
+              y = (code & 2) ? -y : y;
+              acc = ((starts >> q) & 1) ? y : acc + y;
+              a[4 * e4 + e] = acc;
             }
           }
+          tmem_st16(scan + 16 * c16, a);
         }
-        // the only writer of these entries: the reductions apply in program order
-        if (cur >= 0) atomicAdd(&Pl[(int64_t)(b.y + cur) * LD + row], rs * (double)run);
+        tmem_wait_st();
+        // phase 2: the sum of each run is the scan at its last column; one reduction per run
+        // (the only writer of these entries: the reductions apply in program order)
+        for (int k0 = 0; k0 < nruns; k0 += 4) {
+          float v[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) v[k] = tmem_ld1(scan + (uint32_t)pi.rend[min(k0 + k, nruns - 1)]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (live && k0 + k < nruns) atomicAdd(&Pl[(int64_t)(b.y + pi.rtgt[k0 + k]) * LD + row], rs * (double)v[k]);
+        }
         tc_fence_before();
         mbar_arrive(&tempty[s]);
       }
     }
-  } else if (warp < G::NEPI + 4) {
-    // ---------------- gather: lane octet o = lane & 7 the pairs, cq = lane >> 3 the core column
+  } else if (warp < G::NEPI + G::STAGES) {
+    // ---------------- gather: warp gw builds the chunks i ≡ gw (mod STAGES), always in stage gw;
+    // lane octet o = lane & 7 the pairs of a group of 8, cq = lane >> 3 the core column
     const int gw = warp - G::NEPI, o = lane & 7, cq = lane >> 3;
     uint32_t sel[G::U][4];
 #pragma unroll
@@ -323,71 +382,116 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
 #pragma unroll
       for (int w = 0; w < 4; ++w) sel[u][w] = kc < G::KC ? perm16[4 * kc + w] : SEL_IDENTITY;
     }
+    const int s = gw;
+    unsigned char* bh = sB + s * G::STAGE_BYTES;
+    PairInfo& pi = pinfo[s];
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
       const int a0 = co[c], a1 = co[c + 1];
       for (int q0 = a0; q0 < a1; q0 += NCHK, ++i) {
-        const int s = i % G::STAGES;
+        if (i % G::STAGES != gw) continue;
         if (i >= G::STAGES) {
           const bool w = mbar_wait_abortable(&tempty[s], (uint32_t)(i / G::STAGES - 1) & 1, abort_flag);
           if (!__all_sync(0xffffffffu, w)) { ok = false; break; }   // the warp leaves together (shuffles below)
         }
-        const int nc = min(NCHK, a1 - q0), nn = (nc + 15) & ~15;
-        PairInfo& pi = pinfo[s];
-        if (gw == 0 && lane == 0) pi.n = nc;
-        unsigned char* bh = sB + s * G::STAGE_BYTES;
-#pragma unroll
-        for (int gi = 0; gi < NCHK / 32; ++gi) {
-          const int j0 = 8 * (gw + 4 * gi);
-          if (j0 >= nn) break;                           // uniform across the warp
-          int src = -1, fac = 0;
-          if (lane < 8 && j0 + lane < nc) {
-            const int2 pr = pairs[b.w + q0 + j0 + lane];
-            src = pr.x;
-            fac = s_d4h[pr.y >> 8];
-            pi.cs[j0 + lane] = Msc[src];
-            pi.fac[j0 + lane] = fac;
-            pi.tgt[j0 + lane] = pr.y & 0xff;
+        const int nc = min(NCHK, a1 - q0), ng = (nc + 15) / 16 * 2;   // groups of 8 up to N = nc rounded to 16
+        // the chunk's pairs: lane l holds columns 2l and 2l + 1
+        int srcA = -1, srcB = -1, facA = 0, facB = 0, tA = -1, tB = -1;
+        const bool vA = 2 * lane < nc, vB = 2 * lane + 1 < nc;
+        if (vA) {
+          const int2 pr = pairs[b.w + q0 + 2 * lane];
+          srcA = pr.x;
+          facA = s_d4h[pr.y >> 8];
+          tA = pr.y & 0xff;
+          pi.fac[2 * lane] = facA;
+          pi.tgt[2 * lane] = tA;
+        }
+        if (vB) {
+          const int2 pr = pairs[b.w + q0 + 2 * lane + 1];
+          srcB = pr.x;
+          facB = s_d4h[pr.y >> 8];
+          tB = pr.y & 0xff;
+          pi.fac[2 * lane + 1] = facB;
+          pi.tgt[2 * lane + 1] = tB;
+        }
+        {
+          // the target runs of the chunk (pairs are sorted by target within a class)
+          const int tprev = __shfl_up_sync(0xffffffffu, tB, 1);
+          const bool stA = vA && (lane == 0 || tA != tprev), stB = vB && tB != tA;
+          const uint64_t starts = spread_bits(__ballot_sync(0xffffffffu, stA)) | (spread_bits(__ballot_sync(0xffffffffu, stB)) << 1);
+          const bool endA = vA && (2 * lane + 1 == nc || stB);
+          const bool endB = vB && (2 * lane + 2 == nc || ((starts >> (2 * lane + 2)) & 1));
+          if (endA) {
+            const int k = __popcll(starts & ((2ull << (2 * lane)) - 1)) - 1;
+            pi.rend[k] = 2 * lane;
+            pi.rtgt[k] = tA;
           }
-          src = __shfl_sync(0xffffffffu, src, o);
-          fac = __shfl_sync(0xffffffffu, fac, o);
-          const bool odd = fac & 1;                      // odd quarter-turns swap the odd-order pairs
-          const int j = j0 + o;
-          uint4 vh[G::U], vl[G::U];
-#pragma unroll
-          for (int u = 0; u < G::U; ++u) {
-            const int kc = 4 * u + cq;
-            vh[u] = vl[u] = make_uint4(0, 0, 0, 0);
-            if (src >= 0 && kc < G::KC) {
-              vh[u] = __ldg(reinterpret_cast<const uint4*>(Mh + (int64_t)src * KP) + kc);
-              vl[u] = __ldg(reinterpret_cast<const uint4*>(Ml + (int64_t)src * KP) + kc);
-            }
+          if (endB) {
+            const int k = __popcll(starts & ((2ull << (2 * lane + 1)) - 1)) - 1;
+            pi.rend[k] = 2 * lane + 1;
+            pi.rtgt[k] = tB;
           }
-#pragma unroll
-          for (int u = 0; u < G::U; ++u) {
-            const int kc = 4 * u + cq;
-            // neighbouring words: the last of the previous core column, the first of the next
-            const uint32_t hp = __shfl_up_sync(0xffffffffu, vh[u].w, 8), hn = __shfl_down_sync(0xffffffffu, vh[u].x, 8);
-            const uint32_t lp = __shfl_up_sync(0xffffffffu, vl[u].w, 8), ln = __shfl_down_sync(0xffffffffu, vl[u].x, 8);
-            if (kc >= G::KC) continue;
-            const uint4 sg = s_sgn[fac * G::KC + kc];
-            const uint32_t wh[6] = {hp, vh[u].x, vh[u].y, vh[u].z, vh[u].w, hn};
-            const uint32_t wl[6] = {lp, vl[u].x, vl[u].y, vl[u].z, vl[u].w, ln};
-            const uint32_t sgw[4] = {sg.x, sg.y, sg.z, sg.w};
-            uint32_t oh[4], ol[4];
-#pragma unroll
-            for (int w = 0; w < 4; ++w) {
-              const uint32_t sl = odd ? sel[u][w] : SEL_IDENTITY;
-              const uint32_t sa = sl & 0xffffu, sb = sl >> 16;
-              oh[w] = __byte_perm(__byte_perm(wh[w], wh[w + 1], sa), wh[w + 2], sb) ^ sgw[w];
-              ol[w] = __byte_perm(__byte_perm(wl[w], wl[w + 1], sa), wl[w + 2], sb) ^ sgw[w];
-            }
-            const uint32_t off = canon16(j, 8 * kc, KP);
-            *(uint4*)(bh + off) = make_uint4(oh[0], oh[1], oh[2], oh[3]);
-            *(uint4*)(bh + G::B_HALF + off) = make_uint4(ol[0], ol[1], ol[2], ol[3]);
+          if (lane == 0) {
+            pi.starts = starts;
+            pi.nruns = __popcll(starts);
           }
         }
+        const float csA = srcA >= 0 ? Msc[srcA] : 0.f, csB = srcB >= 0 ? Msc[srcB] : 0.f;
+        for (int g0 = 0; g0 < ng; g0 += 2) {
+          uint4 vh[2][G::U], vl[2][G::U];
+          int facg[2];
+#pragma unroll
+          for (int gg = 0; gg < 2; ++gg) {
+            const int j = 8 * (g0 + gg) + o;
+            const int s1 = __shfl_sync(0xffffffffu, srcA, j >> 1), s2 = __shfl_sync(0xffffffffu, srcB, j >> 1);
+            const int f1 = __shfl_sync(0xffffffffu, facA, j >> 1), f2 = __shfl_sync(0xffffffffu, facB, j >> 1);
+            const int src = (j & 1) ? s2 : s1;
+            facg[gg] = (j & 1) ? f2 : f1;
+#pragma unroll
+            for (int u = 0; u < G::U; ++u) {
+              const int kc = 4 * u + cq;
+              vh[gg][u] = vl[gg][u] = make_uint4(0, 0, 0, 0);
+              if (src >= 0 && kc < G::KC) {
+                vh[gg][u] = __ldg(reinterpret_cast<const uint4*>(Mh + (int64_t)src * KP) + kc);
+                vl[gg][u] = __ldg(reinterpret_cast<const uint4*>(Ml + (int64_t)src * KP) + kc);
+              }
+            }
+          }
+#pragma unroll
+          for (int gg = 0; gg < 2; ++gg) {
+            const int j = 8 * (g0 + gg) + o;
+            const int fac = facg[gg];
+            const bool odd = fac & 1;                      // odd quarter-turns swap the odd-order pairs
+#pragma unroll
+            for (int u = 0; u < G::U; ++u) {
+              const int kc = 4 * u + cq;
+              // neighbouring words: the last of the previous core column, the first of the next
+              const uint32_t hp = __shfl_up_sync(0xffffffffu, vh[gg][u].w, 8), hn = __shfl_down_sync(0xffffffffu, vh[gg][u].x, 8);
+              const uint32_t lp = __shfl_up_sync(0xffffffffu, vl[gg][u].w, 8), ln = __shfl_down_sync(0xffffffffu, vl[gg][u].x, 8);
+              if (kc >= G::KC) continue;
+              const uint4 sg = s_sgn[fac * G::KC + kc];
+              const uint32_t wh[6] = {hp, vh[gg][u].x, vh[gg][u].y, vh[gg][u].z, vh[gg][u].w, hn};
+              const uint32_t wl[6] = {lp, vl[gg][u].x, vl[gg][u].y, vl[gg][u].z, vl[gg][u].w, ln};
+              const uint32_t sgw[4] = {sg.x, sg.y, sg.z, sg.w};
+              uint32_t oh[4], ol[4];
+#pragma unroll
+              for (int w = 0; w < 4; ++w) {
+                const uint32_t sl = odd ? sel[u][w] : SEL_IDENTITY;
+                const uint32_t sa = sl & 0xffffu, sb = sl >> 16;
+                oh[w] = __byte_perm(__byte_perm(wh[w], wh[w + 1], sa), wh[w + 2], sb) ^ sgw[w];
+                ol[w] = __byte_perm(__byte_perm(wl[w], wl[w + 1], sa), wl[w + 2], sb) ^ sgw[w];
+              }
+              const uint32_t off = canon16(j, 8 * kc, KP);
+              *(uint4*)(bh + off) = make_uint4(oh[0], oh[1], oh[2], oh[3]);
+              *(uint4*)(bh + G::B_HALF + off) = make_uint4(ol[0], ol[1], ol[2], ol[3]);
+            }
+          }
+        }
+        if (2 * lane < nc) pi.cs[2 * lane] = csA;
+        if (2 * lane + 1 < nc) pi.cs[2 * lane + 1] = csB;
+        if (lane == 0) pi.n = nc;
         fence_async_smem();
+        __syncwarp();
         mbar_arrive(&full[s]);
       }
     }
