@@ -222,7 +222,7 @@ struct __align__(16) PairInfo {
   int rend[NCHK];
   int rtgt[NCHK];
   unsigned long long starts;
-  int n, nruns;
+  int n, nruns, split;      // split: the first run start at or after column n/2 (n if none)
 };
 
 template <int KP, int MT>
@@ -234,7 +234,8 @@ struct TcCfg {
   static constexpr int B_HALF = NCHK * KP * 2;
   static constexpr int STAGE_BYTES = 2 * B_HALF;
   static constexpr int STAGES = MT == 1 ? 4 : 3;
-  static constexpr int NEPI = 4 + (MT - 1);                // read-back warps
+  static constexpr int HALVES = MT == 1 ? 2 : 1;           // read-back warps per lane quadrant and tile
+  static constexpr int NEPI = 4 * HALVES + (MT - 1);       // read-back warps
   static constexpr int THREADS = 32 * (NEPI + STAGES + 1); // + one gather warp per stage + 1 issuing warp
   static constexpr int B_OFF = (A_BYTES + 1023) / 1024 * 1024;
   static constexpr int PI_OFF = B_OFF + STAGES * STAGE_BYTES;
@@ -242,13 +243,13 @@ struct TcCfg {
   static constexpr int D4H_OFF = SGN_OFF + 16 * KC * 16;
   static constexpr int BAR_OFF = D4H_OFF + NFAR * 4;
   static constexpr int SMEM = BAR_OFF + (1 + 3 * STAGES) * 8 + 16;
-  static constexpr int SCAN_COL = STAGES * MT * NCHK;    // per tile NCHK columns of run sums
-  static_assert(SCAN_COL + MT * NCHK <= TMEM_COLS, "tensor memory");
+  static constexpr int SCAN_COL = STAGES * MT * NCHK;    // per tile and half NCHK columns of run sums
+  static_assert(SCAN_COL + MT * HALVES * NCHK <= TMEM_COLS, "tensor memory");
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
 // perm16 (global): KC × 4 byte selectors of the odd quarter-turn swaps (selA | selB << 16 per
-// 32-bit word), then 16 × KC × 4 sign words (0x8000 in each FP16 half that is negated)
+// 32-bit word), then KC × 16 × 4 sign words (0x8000 in each FP16 half that is negated)
 template <int KP, int MT>
 __global__ void __launch_bounds__(TcCfg<KP, MT>::THREADS, 1)
 k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const int2* __restrict__ pairs,
@@ -260,7 +261,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   unsigned char* sA = sm;                                         // head rows, then the tail at lo_off
   unsigned char* sB = sm + G::B_OFF;                              // stage s: head at s·STAGE_BYTES, tail after it
   PairInfo* pinfo = (PairInfo*)(sm + G::PI_OFF);                  // per stage
-  uint4* s_sgn = (uint4*)(sm + G::SGN_OFF);                       // [16][KC]
+  uint4* s_sgn = (uint4*)(sm + G::SGN_OFF);                       // [KC][16]
   int* s_d4h = (int*)(sm + G::D4H_OFF);
   uint64_t* bars = (uint64_t*)(sm + G::BAR_OFF);
   uint64_t* bar_a = bars;                                         // operator load
@@ -297,7 +298,9 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
 
   if (warp < G::NEPI) {
     // ---------------- read back and scatter: thread = output row of tile `tile`
-    const int tile = warp >> 2, quad = warp & 3;
+    // with two halves per quadrant (p ≤ 10), warps 0-3 take the columns before the chunk's split and
+    // warps 4-7 the rest: the split is a run start, so every entry still has one writer per chunk
+    const int half = G::HALVES == 2 ? warp >> 2 : 0, tile = G::HALVES == 2 ? 0 : warp >> 2, quad = warp & 3;
     const int row = 128 * tile + 32 * quad + lane;
     const bool live = row < NP;
     const double alpha = m2l_scale[b.x];
@@ -310,7 +313,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
       const int partner = epart == 0 ? row : (epart == 1 ? row + 1 : row - 1);
       src_lane = partner & 31;                       // pairs never straddle a 32-row boundary (p ≤ 11)
     }
-    const uint32_t scan = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(G::SCAN_COL + tile * NCHK);
+    const uint32_t scan = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(G::SCAN_COL + (tile * G::HALVES + half) * NCHK);
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
       const int a0 = co[c], a1 = co[c + 1];
@@ -323,15 +326,17 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         if (!__all_sync(0xffffffffu, w)) { ok = false; break; }   // the warp leaves together (tcgen05.ld is warp-wide)
         tc_fence_after();
         const PairInfo& pi = pinfo[s];
-        const int nc = pi.n, nruns = pi.nruns;
+        const int nc = pi.n;
         const uint64_t starts = pi.starts;
+        const int lo = half ? pi.split : 0, hi = (G::HALVES == 2 && !half) ? pi.split : nc;
         const uint32_t ta = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)((s * MT + tile) * NCHK);
         // phase 1 (branch-free): per column the permuted, unscaled value, and the running sum of
         // the column's target run (reset where a run starts), parked in this tile's scan columns
         float acc = 0.f;
 #pragma unroll
         for (int c16 = 0; c16 < NCHK / 16; ++c16) {
-          if (16 * c16 >= nc) break;                      // uniform across the warp
+          if (16 * c16 >= hi) break;                      // uniform across the warp
+          if (16 * c16 + 16 <= lo) continue;
           float d[16], a[16];
           tmem_ld16(ta + 16 * c16, d);
           tmem_wait_ld();
@@ -358,14 +363,16 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         tmem_wait_st();
         // phase 2: the sum of each run is the scan at its last column; one reduction per run
         // (the only writer of these entries: the reductions apply in program order)
-        for (int k0 = 0; k0 < nruns; k0 += 4) {
+        const int k_lo = lo >= 64 ? __popcll(starts) : __popcll(starts & ((1ull << lo) - 1));
+        const int k_hi = hi >= 64 ? __popcll(starts) : __popcll(starts & ((1ull << hi) - 1));
+        for (int k0 = k_lo; k0 < k_hi; k0 += 4) {
           float v[4];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) v[k] = tmem_ld1(scan + (uint32_t)pi.rend[min(k0 + k, nruns - 1)]);
+          for (int k = 0; k < 4; ++k) v[k] = tmem_ld1(scan + (uint32_t)pi.rend[min(k0 + k, k_hi - 1)]);
           tmem_wait_ld();
 #pragma unroll
           for (int k = 0; k < 4; ++k)
-            if (live && k0 + k < nruns) atomicAdd(&Pl[(int64_t)(b.y + pi.rtgt[k0 + k]) * LD + row], rs * (double)v[k]);
+            if (live && k0 + k < k_hi) atomicAdd(&Pl[(int64_t)(b.y + pi.rtgt[k0 + k]) * LD + row], rs * (double)v[k]);
         }
         tc_fence_before();
         mbar_arrive(&tempty[s]);
@@ -432,8 +439,11 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
             pi.rtgt[k] = tB;
           }
           if (lane == 0) {
+            const int h = (nc + 1) / 2;
+            const uint64_t later = h >= 64 ? 0ull : starts & (~0ull << h);
             pi.starts = starts;
             pi.nruns = __popcll(starts);
+            pi.split = later ? __ffsll((long long)later) - 1 : nc;
           }
         }
         const float csA = srcA >= 0 ? Msc[srcA] : 0.f, csB = srcB >= 0 ? Msc[srcB] : 0.f;
@@ -469,7 +479,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
               const uint32_t hp = __shfl_up_sync(0xffffffffu, vh[gg][u].w, 8), hn = __shfl_down_sync(0xffffffffu, vh[gg][u].x, 8);
               const uint32_t lp = __shfl_up_sync(0xffffffffu, vl[gg][u].w, 8), ln = __shfl_down_sync(0xffffffffu, vl[gg][u].x, 8);
               if (kc >= G::KC) continue;
-              const uint4 sg = s_sgn[fac * G::KC + kc];
+              const uint4 sg = s_sgn[kc * 16 + fac];
               const uint32_t wh[6] = {hp, vh[gg][u].x, vh[gg][u].y, vh[gg][u].z, vh[gg][u].w, hn};
               const uint32_t wl[6] = {lp, vl[gg][u].x, vl[gg][u].y, vl[gg][u].z, vl[gg][u].w, ln};
               const uint32_t sgw[4] = {sg.x, sg.y, sg.z, sg.w};
@@ -582,7 +592,7 @@ __global__ void k_split16(const double* __restrict__ M, int nnodes, int NP, int 
 
 // the source-side permutation of the gather for (p+1)² = np: per 16-byte core column kc and
 // 32-bit word w, the byte selectors of the odd quarter-turn swaps (selA | selB << 16, applied
-// as byte_perm(byte_perm(w[-1], w, selA), w[+1], selB)); then per D4h element g the sign words
+// as byte_perm(byte_perm(w[-1], w, selA), w[+1], selB)); then per kc and D4h element g the sign words
 std::vector<uint32_t> build_perm16(int np) {
   const int KC = kp_of(np) / 8;
   std::vector<uint32_t> perm((size_t)4 * KC + (size_t)16 * KC * 4, 0);
@@ -608,7 +618,7 @@ std::vector<uint32_t> build_perm16(int np) {
   for (int k = 0; k < np; ++k) {
     const uint32_t mask = perm_mask(k, false);
     for (int g = 0; g < 16; ++g)
-      if ((mask >> (2 * g)) & 2) perm[4 * KC + ((size_t)g * KC + k / 8) * 4 + (k & 7) / 2] |= (k & 1) ? 0x80000000u : 0x8000u;
+      if ((mask >> (2 * g)) & 2) perm[4 * KC + ((size_t)(k / 8) * 16 + g) * 4 + (k & 7) / 2] |= (k & 1) ? 0x80000000u : 0x8000u;
   }
   return perm;
 }
