@@ -17,10 +17,9 @@
 //     STAGES, so STAGES chunks are gathered at once; in the UMMA K-major canonical layout
 //     (8-row × 16-byte core matrices, no swizzle): 8 consecutive lanes write the 8 pairs of one
 //     core matrix (one 128-byte row of banks), 4 lanes read 64 contiguous bytes of one source
-//     column, and the loads of two groups of 8 pairs are in flight together. The source-side signed permutation P_sᵀ is applied
-//     on the way: for odd quarter-turn rotations the two entries of every odd-order pair swap
-//     (two byte permutes per 32-bit word, the neighbour words from the adjacent lanes), then
-//     the signs are flipped by one XOR per word;
+//     column, and the loads of two groups of 8 pairs are in flight together. The source-side
+//     signed permutation P_sᵀ costs one XOR per word: odd quarter-turn rotations read a second
+//     copy of the multipoles in which the two entries of every odd-order pair are swapped;
 //   - one thread loads the class operator (head and tail, laid out on the host) with one bulk
 //     copy (cp.async.bulk, no tensor map, no multicast) when the class changes, after the
 //     previous class's MMAs completed; then per chunk issues (p+1)²/16 K-steps × tiles × 3 MMAs
@@ -50,7 +49,6 @@ constexpr int GROUP = 32;         // entries one gather lane octet covers per in
 constexpr unsigned long long SPIN_LIMIT = 1ull << 26;
 constexpr uint64_t WAIT_NS = 1000000000ull;  // one second: a wait in a working pipeline takes microseconds
 constexpr int TMEM_COLS = 512;
-constexpr uint32_t SEL_IDENTITY = 0x32107654u;  // selA = 0x7654 (the word itself), selB = 0x3210 (kept)
 
 __host__ __device__ constexpr int kp_of(int np) { return (np + 15) / 16 * 16; }          // K, padded to the MMA's K
 __host__ __device__ constexpr int rows_of(int np) { return np > 128 ? 128 + (np - 128 + 7) / 8 * 8 : 128; }  // rows stored
@@ -248,13 +246,14 @@ struct TcCfg {
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
-// perm16 (global): KC × 4 byte selectors of the odd quarter-turn swaps (selA | selB << 16 per
-// 32-bit word), then KC × 16 × 4 sign words (0x8000 in each FP16 half that is negated)
+// perm16 (global): KC × 16 × 4 sign words of the source-side permutation (0x8000 in each FP16
+// half that is negated); Mh/Ml: two copies of the split multipoles vstride apart, the second
+// with the two entries of every odd-order pair swapped (what odd quarter-turns read)
 template <int KP, int MT>
 __global__ void __launch_bounds__(TcCfg<KP, MT>::THREADS, 1)
 k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const int2* __restrict__ pairs,
          const uint16_t* __restrict__ reps16, const float* __restrict__ row_scale, const uint32_t* __restrict__ perm16,
-         const double* __restrict__ m2l_scale, int NP, int LD, int lo_off, const uint16_t* __restrict__ Mh,
+         const double* __restrict__ m2l_scale, int NP, int LD, int lo_off, int64_t vstride, const uint16_t* __restrict__ Mh,
          const uint16_t* __restrict__ Ml, const float* __restrict__ Msc, double* __restrict__ Pl, int* __restrict__ err) {
   using G = TcCfg<KP, MT>;
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -275,7 +274,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   const int* co = cls_off + (int64_t)blockIdx.x * (NCLASS + 1);
 
   for (int f = tid; f < NFAR; f += G::THREADS) s_d4h[f] = c_d4h[f];
-  for (int e = tid; e < 16 * G::KC; e += G::THREADS) s_sgn[e] = reinterpret_cast<const uint4*>(perm16 + 4 * G::KC)[e];
+  for (int e = tid; e < 16 * G::KC; e += G::THREADS) s_sgn[e] = reinterpret_cast<const uint4*>(perm16)[e];
   if (tid == 0) {
     mbar_init(bar_a, 1);
     for (int s = 0; s < G::STAGES; ++s) {
@@ -382,13 +381,6 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
     // ---------------- gather: warp gw builds the chunks i ≡ gw (mod STAGES), always in stage gw;
     // lane octet o = lane & 7 the pairs of a group of 8, cq = lane >> 3 the core column
     const int gw = warp - G::NEPI, o = lane & 7, cq = lane >> 3;
-    uint32_t sel[G::U][4];
-#pragma unroll
-    for (int u = 0; u < G::U; ++u) {
-      const int kc = 4 * u + cq;
-#pragma unroll
-      for (int w = 0; w < 4; ++w) sel[u][w] = kc < G::KC ? perm16[4 * kc + w] : SEL_IDENTITY;
-    }
     const int s = gw;
     unsigned char* bh = sB + s * G::STAGE_BYTES;
     PairInfo& pi = pinfo[s];
@@ -457,43 +449,29 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
             const int f1 = __shfl_sync(0xffffffffu, facA, j >> 1), f2 = __shfl_sync(0xffffffffu, facB, j >> 1);
             const int src = (j & 1) ? s2 : s1;
             facg[gg] = (j & 1) ? f2 : f1;
+            // odd quarter-turns read the copy with the odd-order pairs swapped
+            const int64_t base = src >= 0 ? (int64_t)(facg[gg] & 1) * vstride + (int64_t)src * KP : 0;
 #pragma unroll
             for (int u = 0; u < G::U; ++u) {
               const int kc = 4 * u + cq;
               vh[gg][u] = vl[gg][u] = make_uint4(0, 0, 0, 0);
               if (src >= 0 && kc < G::KC) {
-                vh[gg][u] = __ldg(reinterpret_cast<const uint4*>(Mh + (int64_t)src * KP) + kc);
-                vl[gg][u] = __ldg(reinterpret_cast<const uint4*>(Ml + (int64_t)src * KP) + kc);
+                vh[gg][u] = __ldg(reinterpret_cast<const uint4*>(Mh + base) + kc);
+                vl[gg][u] = __ldg(reinterpret_cast<const uint4*>(Ml + base) + kc);
               }
             }
           }
 #pragma unroll
           for (int gg = 0; gg < 2; ++gg) {
             const int j = 8 * (g0 + gg) + o;
-            const int fac = facg[gg];
-            const bool odd = fac & 1;                      // odd quarter-turns swap the odd-order pairs
 #pragma unroll
             for (int u = 0; u < G::U; ++u) {
               const int kc = 4 * u + cq;
-              // neighbouring words: the last of the previous core column, the first of the next
-              const uint32_t hp = __shfl_up_sync(0xffffffffu, vh[gg][u].w, 8), hn = __shfl_down_sync(0xffffffffu, vh[gg][u].x, 8);
-              const uint32_t lp = __shfl_up_sync(0xffffffffu, vl[gg][u].w, 8), ln = __shfl_down_sync(0xffffffffu, vl[gg][u].x, 8);
               if (kc >= G::KC) continue;
-              const uint4 sg = s_sgn[kc * 16 + fac];
-              const uint32_t wh[6] = {hp, vh[gg][u].x, vh[gg][u].y, vh[gg][u].z, vh[gg][u].w, hn};
-              const uint32_t wl[6] = {lp, vl[gg][u].x, vl[gg][u].y, vl[gg][u].z, vl[gg][u].w, ln};
-              const uint32_t sgw[4] = {sg.x, sg.y, sg.z, sg.w};
-              uint32_t oh[4], ol[4];
-#pragma unroll
-              for (int w = 0; w < 4; ++w) {
-                const uint32_t sl = odd ? sel[u][w] : SEL_IDENTITY;
-                const uint32_t sa = sl & 0xffffu, sb = sl >> 16;
-                oh[w] = __byte_perm(__byte_perm(wh[w], wh[w + 1], sa), wh[w + 2], sb) ^ sgw[w];
-                ol[w] = __byte_perm(__byte_perm(wl[w], wl[w + 1], sa), wl[w + 2], sb) ^ sgw[w];
-              }
+              const uint4 sg = s_sgn[kc * 16 + facg[gg]];
               const uint32_t off = canon16(j, 8 * kc, KP);
-              *(uint4*)(bh + off) = make_uint4(oh[0], oh[1], oh[2], oh[3]);
-              *(uint4*)(bh + G::B_HALF + off) = make_uint4(ol[0], ol[1], ol[2], ol[3]);
+              *(uint4*)(bh + off) = make_uint4(vh[gg][u].x ^ sg.x, vh[gg][u].y ^ sg.y, vh[gg][u].z ^ sg.z, vh[gg][u].w ^ sg.w);
+              *(uint4*)(bh + G::B_HALF + off) = make_uint4(vl[gg][u].x ^ sg.x, vl[gg][u].y ^ sg.y, vl[gg][u].z ^ sg.z, vl[gg][u].w ^ sg.w);
             }
           }
         }
@@ -562,9 +540,10 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
 }
 
 // the multipoles of every node, scaled by a power of two so that the largest entry of the
-// column lies in [2^13, 2^14), as FP16 head and tail (one warp per node); Msc = the inverse scale
-__global__ void k_split16(const double* __restrict__ M, int nnodes, int NP, int LD, int KP, uint16_t* __restrict__ Mh,
-                          uint16_t* __restrict__ Ml, float* __restrict__ Msc) {
+// column lies in [2^13, 2^14), as FP16 head and tail (one warp per node), twice: as they are and
+// with the two entries of every odd-order pair swapped (vstride further); Msc = the inverse scale
+__global__ void k_split16(const double* __restrict__ M, int nnodes, int NP, int LD, int KP, int64_t vstride,
+                          uint16_t* __restrict__ Mh, uint16_t* __restrict__ Ml, float* __restrict__ Msc) {
   const int node = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (node >= nnodes) return;
   const double* m = M + (int64_t)node * LD;
@@ -579,48 +558,36 @@ __global__ void k_split16(const double* __restrict__ M, int nnodes, int NP, int 
     e = max(-100, min(100, e));                    // keeps the inverse scale inside FP32's range
   }
   for (int k = lane; k < KP; k += 32) {
-    const double x = k < NP ? ldexp(m[k], e) : 0.0;
-    const __half h = __double2half(x);
-    const __half l = __double2half(x - (double)__half2float(h));
-    Mh[(int64_t)node * KP + k] = __half_as_ushort(h);
-    Ml[(int64_t)node * KP + k] = __half_as_ushort(l);
+    int n, mm, part;
+    coef_nmp(k, n, mm, part);
+    const int ks = (part != 0 && (mm & 1)) ? (part == 1 ? k + 1 : k - 1) : k;
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const int kk = v ? ks : k;
+      const double x = k < NP ? ldexp(m[kk], e) : 0.0;
+      const __half h = __double2half(x);
+      const __half l = __double2half(x - (double)__half2float(h));
+      Mh[v * vstride + (int64_t)node * KP + k] = __half_as_ushort(h);
+      Ml[v * vstride + (int64_t)node * KP + k] = __half_as_ushort(l);
+    }
   }
   if (lane == 0) Msc[node] = (float)ldexp(1.0, -e);
 }
 
 }  // namespace
 
-// the source-side permutation of the gather for (p+1)² = np: per 16-byte core column kc and
-// 32-bit word w, the byte selectors of the odd quarter-turn swaps (selA | selB << 16, applied
-// as byte_perm(byte_perm(w[-1], w, selA), w[+1], selB)); then per kc and D4h element g the sign words
-std::vector<uint32_t> build_perm16(int np) {
+// the signs of the source-side permutation for (p+1)² = np: per 16-byte core column kc, D4h
+// element g and 32-bit word, 0x8000 in each FP16 half that is negated (the swaps of odd
+// quarter-turns are in the multipole copy the gather reads)
+std::vector<uint32_t> build_sign16(int np) {
   const int KC = kp_of(np) / 8;
-  std::vector<uint32_t> perm((size_t)4 * KC + (size_t)16 * KC * 4, 0);
-  for (int kc = 0; kc < KC; ++kc)
-    for (int w = 0; w < 4; ++w) {
-      const int k0 = 8 * kc + 2 * w, k1 = k0 + 1;
-      int loB = 4, hiB = 6, hb = 2;                    // identity: the word itself, kept
-      auto swap_of = [&](int k, int& part) {
-        int n, m;
-        coef_nmp(k, n, m, part);
-        return k < np && part != 0 && (m & 1);
-      };
-      int p0, p1;
-      if (swap_of(k0, p0)) loB = p0 == 1 ? 6 : 2;      // Re: the next entry (this word), Im: the previous word
-      if (swap_of(k1, p1)) {
-        if (p1 == 1) hb = 4;                           // Re: the first entry of the next word
-        else hiB = 4;                                  // Im: the first entry of this word
-      }
-      const uint32_t sa = (uint32_t)(loB | (loB + 1) << 4 | hiB << 8 | (hiB + 1) << 12);
-      const uint32_t sb = (uint32_t)(0 | 1 << 4 | hb << 8 | (hb + 1) << 12);
-      perm[4 * kc + w] = sa | sb << 16;
-    }
+  std::vector<uint32_t> sg((size_t)KC * 16 * 4, 0);
   for (int k = 0; k < np; ++k) {
     const uint32_t mask = perm_mask(k, false);
     for (int g = 0; g < 16; ++g)
-      if ((mask >> (2 * g)) & 2) perm[4 * KC + ((size_t)(k / 8) * 16 + g) * 4 + (k & 7) / 2] |= (k & 1) ? 0x80000000u : 0x8000u;
+      if ((mask >> (2 * g)) & 2) sg[((size_t)(k / 8) * 16 + g) * 4 + (k & 7) / 2] |= (k & 1) ? 0x80000000u : 0x8000u;
   }
-  return perm;
+  return sg;
 }
 
 // the class operators of the mixed path: per class, every row scaled by a power of two (its
@@ -676,7 +643,7 @@ void prepare_mixed_operators(Cache& C) {
   std::vector<uint16_t> h;
   std::vector<float> rsc;
   build_reps16(C.host, h, rsc);
-  std::vector<uint32_t> perm = build_perm16(np);
+  std::vector<uint32_t> perm = build_sign16(np);
   to_device(C.reps16, h, C.ctx->stream);
   to_device(C.row_scale, rsc, C.ctx->stream);
   to_device(C.perm16, perm, C.ctx->stream);
@@ -693,7 +660,7 @@ void launch_tc(State& S, int nb) {
   const int lo_off = rows_of(C.np) * KP * 2;
   FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc<KP, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
   k_m2l_tc<KP, MT><<<nb, G::THREADS, G::SMEM, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps16.p, C.row_scale.p,
-                                                               C.perm16.p, P.d_m2l_scale.p, C.np, C.ld, lo_off, S.Mh.p,
+                                                               C.perm16.p, P.d_m2l_scale.p, C.np, C.ld, lo_off, (int64_t)P.nnodes * KP, S.Mh.p,
                                                                S.Ml.p, S.Msc.p, S.Pl.p, S.err.p);
   FMMB_LAUNCH_CHECK();
 }
@@ -707,10 +674,10 @@ void m2l_mixed(State& S) {
   if (nb == 0) return;
   const int KP = kp_of(C.np);
   const size_t ne = (size_t)P.nnodes * KP;
-  if (S.Mh.n < ne) { S.Mh.alloc(ne); S.Ml.alloc(ne); }
+  if (S.Mh.n < 2 * ne) { S.Mh.alloc(2 * ne); S.Ml.alloc(2 * ne); }
   if (S.Msc.n < (size_t)P.nnodes) S.Msc.alloc(P.nnodes);
   if (!S.err.p) S.err.alloc(1);
-  k_split16<<<(unsigned)(((int64_t)P.nnodes * 32 + 255) / 256), 256, 0, s>>>(S.M.p, P.nnodes, C.np, C.ld, KP, S.Mh.p, S.Ml.p,
+  k_split16<<<(unsigned)(((int64_t)P.nnodes * 32 + 255) / 256), 256, 0, s>>>(S.M.p, P.nnodes, C.np, C.ld, KP, (int64_t)ne, S.Mh.p, S.Ml.p,
                                                                               S.Msc.p);
   FMMB_LAUNCH_CHECK();
   FMMB_CUDA(cudaMemsetAsync(S.err.p, 0, sizeof(int), s));
