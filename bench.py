@@ -1,12 +1,14 @@
 #!/usr/bin/env python
 """Laplace3D FMM matvec throughput on B200 (one JSON line on stdout).
 
-Workload (the metric's configuration): SphericalHarmonics(Laplace3D(); p=10), ppl=64,
-1,000,000 points uniform in the unit cube (seed 3), FP64 charges N(0,1), potential and
-gradient at the sources. A step is one matvec = build_expansions + evaluate_at_sources
-(the reference's definition, bench/bench.jl:44-50), the tree/plan built once beforehand.
+Workload: SphericalHarmonics(Laplace3D(); p), ppl=64, 1,000,000 points uniform in the unit cube
+(seed 3), FP64 charges N(0,1), potential and gradient at the sources. A step is one matvec =
+build_expansions + evaluate_at_sources (the reference's definition, bench/bench.jl:44-50), the
+tree/plan built once beforehand. The headline order is p = 11: the metric asks for ≤ 1e-6
+relative error, and the configured p = 10 stays above it even in FP64 (1.7e-6 against direct
+sums; p = 11 gives 7.3e-7). The configured order is measured beside it (configured_order_p10).
 
-  value      evaluations/s of the mixed path (tensor-core TF32x3 M2L, FP32 compensated P2P),
+  value      evaluations/s of the mixed path (tensor-core FP16x3 M2L, FP32 near field),
              inputs resident in HBM, device time (CUDA events on the library's stream), L2
              flushed (256 MB write) between steps, max over ranks
   e2e        the same through the host-pointer C ABI call (fmmb_matvec) with pinned host
@@ -43,14 +45,15 @@ UNIT = "evals/s"
 def args_():
     a = argparse.ArgumentParser()
     a.add_argument("--gpus", type=int, default=1)
-    a.add_argument("--steps", type=int, default=10)
+    a.add_argument("--steps", type=int, default=20)
     a.add_argument("--warmup", type=int, default=3)
     a.add_argument("--impl", default="ours", choices=["ours", "reference"])
     a.add_argument("--n", type=int, default=1_000_000)
-    a.add_argument("--p", type=int, default=10)
+    a.add_argument("--p", type=int, default=11)
     a.add_argument("--ppl", type=int, default=64)
     a.add_argument("--samples", type=int, default=4096)
     a.add_argument("--no-cpu-baseline", action="store_true")
+    a.add_argument("--no-p10", action="store_true", help="skip the side measurement at the configured order p = 10")
     return a.parse_args()
 
 
@@ -134,7 +137,7 @@ class Clocks:
         self.device = device
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "100",
                                        "-i", str(device)], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
@@ -184,10 +187,6 @@ def run_ours(a):
     ctx = fmmb.default_context(local)
     stream = torch.cuda.ExternalStream(ctx.stream)
     pts, tau = workload(a.n)
-    m = fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=a.p)
-    t0 = time.perf_counter()
-    f = fmmb.FMM(m, pts, ppl=a.ppl, bbox=((0.0, 0.0, 0.0), 1.0))
-    plan_s = time.perf_counter() - t0
     xyz_d = torch.from_numpy(pts).cuda()
     tau_d = torch.from_numpy(tau).cuda()
     pot_d = torch.zeros(a.n, dtype=torch.float64, device="cuda")
@@ -195,46 +194,13 @@ def run_ours(a):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
     P = lambda t: C.c_void_p(t.data_ptr())
-    states = {"mixed": fmmb.FMMState(f, "mixed"), "fp64": fmmb.FMMState(f, "fp64")}
-
-    def step(st):
-        rc = L.fmmb_matvec_dev(st._h, P(xyz_d), P(tau_d), a.n, 3, P(pot_d), P(grad_d))
-        if rc:
-            fmmb._check(rc)
-
-    def timed(st, k):
-        times = []
-        for _ in range(k):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                step(st)
-                e1.record(stream)
-            times.append((e0, e1))
-        torch.cuda.synchronize()
-        return [e0.elapsed_time(e1) for e0, e1 in times]
 
     def barrier():
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
 
-    for name in ("mixed", "fp64"):
-        for _ in range(a.warmup):
-            step(states[name])
-    torch.cuda.synchronize()
-    clocks = Clocks(local) if rank == 0 else None
-    barrier()
-    t_mixed = timed(states["mixed"], a.steps)
-    barrier()
-    clk = clocks.stop() if clocks else None
-    t_fp64 = timed(states["fp64"], a.steps)
-    barrier()
-    ms_mixed = max_over_ranks(statistics.mean(t_mixed), dist, "cuda")
-    ms_fp64 = max_over_ranks(statistics.mean(t_fp64), dist, "cuda")
-
-    # accuracy: both paths against FP64 direct sums at sampled sources (device)
+    # FP64 direct sums at sampled sources (device), the error oracle of every path and order
     rng = np.random.default_rng(7)
     sel = np.sort(rng.choice(a.n, size=min(a.samples, a.n), replace=False)).astype(np.int64)
     sel_d = torch.from_numpy(sel).cuda()
@@ -244,30 +210,87 @@ def run_ours(a):
     torch.cuda.synchronize()
     fmmb._check(L.fmmb_direct_dev(ctx._h, P(xyz_d), P(tau_d), a.n, P(tg_d), P(sel_d), len(sel), P(dp), P(dg)))
     dp_h, dg_h = dp.cpu().numpy(), dg.cpu().numpy()
-    err = {}
-    for name in ("mixed", "fp64"):
-        step(states[name])
-        torch.cuda.synchronize()
-        u = pot_d.cpu().numpy()[sel]
-        g = grad_d.cpu().numpy()[sel]
-        err[name] = {"pot_rel_l2": float(np.linalg.norm(u - dp_h) / np.linalg.norm(dp_h)),
-                     "grad_rel_l2": float(np.linalg.norm(g - dg_h) / np.linalg.norm(dg_h))}
 
-    # stage times of one matvec per path (median of 3) and the launches per step
-    stages, launches = {}, {}
-    names = ("gather", "p2m", "m2m", "m2l", "l2l", "eval")
-    for name in ("mixed", "fp64"):
-        runs = []
-        for _ in range(3):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            ms = (C.c_double * 6)()
-            nl = C.c_int()
-            fmmb._check(L.fmmb_profile_matvec(states[name]._h, P(xyz_d), P(tau_d), a.n, 3, P(pot_d), P(grad_d), ms, 6,
-                                               C.byref(nl)))
-            runs.append(list(ms))
-            launches[name] = nl.value
-        stages[name] = {k: statistics.median(r[i] for r in runs) for i, k in enumerate(names)}
+    def measure(p, sample_clocks):
+        """Both precision paths at order p: device step times, errors, stage times, launches."""
+        m = fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=p)
+        t0 = time.perf_counter()
+        f = fmmb.FMM(m, pts, ppl=a.ppl, bbox=((0.0, 0.0, 0.0), 1.0))
+        plan_s = time.perf_counter() - t0
+        states = {"mixed": fmmb.FMMState(f, "mixed"), "fp64": fmmb.FMMState(f, "fp64")}
+
+        def step(st):
+            rc = L.fmmb_matvec_dev(st._h, P(xyz_d), P(tau_d), a.n, 3, P(pot_d), P(grad_d))
+            if rc:
+                fmmb._check(rc)
+
+        def timed(st, k):
+            times = []
+            for _ in range(k):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    step(st)
+                    e1.record(stream)
+                times.append((e0, e1))
+            torch.cuda.synchronize()
+            return [e0.elapsed_time(e1) for e0, e1 in times]
+
+        for name in ("mixed", "fp64"):
+            for _ in range(a.warmup):
+                step(states[name])
+        torch.cuda.synchronize()
+        clocks = Clocks(local) if (rank == 0 and sample_clocks) else None
+        barrier()
+        t_mixed = timed(states["mixed"], a.steps)
+        barrier()
+        t_fp64 = timed(states["fp64"], a.steps)
+        barrier()
+        clk = clocks.stop() if clocks else None
+        r = {"p": p, "f": f, "states": states, "step": step, "plan_s": plan_s, "t_mixed": t_mixed, "clocks": clk,
+             "ms_mixed": max_over_ranks(statistics.mean(t_mixed), dist, "cuda"),
+             "ms_fp64": max_over_ranks(statistics.mean(t_fp64), dist, "cuda")}
+        err = {}
+        for name in ("mixed", "fp64"):
+            step(states[name])
+            torch.cuda.synchronize()
+            u = pot_d.cpu().numpy()[sel]
+            g = grad_d.cpu().numpy()[sel]
+            err[name] = {"pot_rel_l2": float(np.linalg.norm(u - dp_h) / np.linalg.norm(dp_h)),
+                         "grad_rel_l2": float(np.linalg.norm(g - dg_h) / np.linalg.norm(dg_h))}
+        r["error"] = err
+        # stage times of one matvec per path (median of 3, CUDA events on the library's stream)
+        stages, launches = {}, {}
+        names = ("gather", "p2m", "m2m", "m2l", "l2l", "eval")
+        for name in ("mixed", "fp64"):
+            runs = []
+            for _ in range(3):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                ms = (C.c_double * 6)()
+                nl = C.c_int()
+                fmmb._check(L.fmmb_profile_matvec(states[name]._h, P(xyz_d), P(tau_d), a.n, 3, P(pot_d), P(grad_d), ms, 6,
+                                                   C.byref(nl)))
+                runs.append(list(ms))
+                launches[name] = nl.value
+            stages[name] = {k: statistics.median(x[i] for x in runs) for i, k in enumerate(names)}
+        r["stages"], r["launches"] = stages, launches
+        return r
+
+    # the configured order (p = 10) first, then the headline order
+    side = None
+    if a.p != 10 and not a.no_p10:
+        r10 = measure(10, False)
+        side = {"p": 10, "value": replica_throughput(a.n, r10["ms_mixed"], world), "ms_per_step": r10["ms_mixed"],
+                "fp64": {"value": replica_throughput(a.n, r10["ms_fp64"], world), "ms_per_step": r10["ms_fp64"]},
+                "mixed_vs_fp64": r10["ms_fp64"] / r10["ms_mixed"], "error": {"samples": len(sel), **r10["error"]},
+                "stages_ms": r10["stages"]}
+        del r10
+    R = measure(a.p, True)
+    f, states, t_mixed = R["f"], R["states"], R["t_mixed"]
+    ms_mixed, ms_fp64, stages, launches, err, clk = R["ms_mixed"], R["ms_fp64"], R["stages"], R["launches"], R["error"], R["clocks"]
+    plan_s = R["plan_s"]
 
     # end to end through the host-pointer C ABI call, pinned buffers
     xyz_h = torch.from_numpy(pts).pin_memory()
@@ -315,9 +338,11 @@ def run_ours(a):
     line = {
         "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "tf32x3 M2L + f32 P2P, f64 elsewhere", "data": "synthetic (seeded uniform points, N(0,1) charges)",
+        "dtype": "fp16x3 M2L (tcgen05 kind::f16, FP32 accumulation) + f32 near field (FP64 batch sums), f64 elsewhere",
+        "data": "synthetic (seeded uniform points, N(0,1) charges)",
         "config": config(a, {"precision": "mixed", "plan_s": plan_s, "levels": f.nlevels, "nodes": f.nnodes,
                              "far_pairs": f.npairs}),
+        "configured_order_p10": side,
         "latency_ms": {"p50": pct(0.5), "p99": pct(0.99)},
         "fp64": {"value": replica_throughput(a.n, ms_fp64, world), "ms_per_step": ms_fp64},
         "mixed_vs_fp64": ms_fp64 / ms_mixed,

@@ -1,0 +1,270 @@
+// Evaluation at the targets of one leaf (src/evaluate.jl:12-48, src/device.jl:89-100,185-206),
+// in two kernels:
+//   k_l2p   the far field: L2P of the leaf's local expansion (harmonics.jl:447-486), one warp
+//           per leaf group with the local staged in shared memory, lanes over the targets; FP64 on
+//           the plain path, FP32 on the mixed path (tolerances ≥ 1e-8); writes the outputs
+//   k_near  the near field: the sources of the 27 colleagues, flattened into batches of 32 that
+//           each warp stages once in shared memory while the next batch's loads are in flight;
+//           lanes over the targets; adds to the outputs. The self term is skipped by index
+//           (evaluate_at_sources, src/evaluate.jl:1-10), checked only in the batches that hold
+//           the leaf's own points.
+// Two precisions of the near field:
+//   double  the plain path: absolute coordinates, the reference's FMA square norm
+//           (src/kernels.jl:20-24) and its summation order (colleagues in order, points in order)
+//   float   the mixed path: coordinates relative to the target leaf's centre, converted from FP64
+//           when staged (the FP32 differences carry an absolute error of ~2⁻²⁴·w instead of
+//           2⁻²⁴·|x|, so close pairs keep their accuracy); each batch summed in FP32, the batch
+//           sums accumulated in FP64
+// Splitting the two keeps the near-field loop at a low register count (high occupancy); the
+// outputs are u then u + KC·near, the same arithmetic as one fused pass.
+#include "passes.cuh"
+
+namespace fmmb {
+namespace {
+
+constexpr int NEAR_WARPS = 4;
+
+template <int P, typename R>
+__global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, const int* __restrict__ gstart,
+                                             const int* __restrict__ gcount, int ngroups, const double* __restrict__ tx,
+                                             const double* __restrict__ ty, const double* __restrict__ tz,
+                                             const int* __restrict__ tout, const int4* __restrict__ cell,
+                                             const double* __restrict__ Pl, int LD, Geometry geo,
+                                             const double* __restrict__ scale, int outputs, double* __restrict__ pot,
+                                             double* __restrict__ grad) {
+  extern __shared__ __align__(16) unsigned char sl_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (grp >= ngroups) return;
+  R* L = reinterpret_cast<R*>(sl_raw) + warp * LD;
+  const int leaf = gnode[grp];
+  for (int i = lane; i < LD; i += 32) L[i] = (R)Pl[(int64_t)leaf * LD + i];
+  __syncwarp();
+  const int4 c = cell[leaf];
+  const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
+  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const int t0 = gstart[grp], nt = gcount[grp];
+  for (int base = 0; base < nt; base += 32) {
+    const int k = t0 + base + lane;
+    const bool act = base + lane < nt;
+    const double x = act ? tx[k] : cx, y = act ? ty[k] : cy, z = act ? tz[k] : cz;
+    R u, gx, gy, gz;
+    l2p<P, R>(L, (R)((x - cx) * s), (R)((y - cy) * s), (R)((z - cz) * s), u, gx, gy, gz);
+    if (act) {
+      const int o = tout[k];
+      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = (double)u;
+      if (outputs & FMMB_OUTPUT_GRADIENT) {
+        grad[3 * (int64_t)o] = (double)gx * s;
+        grad[3 * (int64_t)o + 1] = (double)gy * s;
+        grad[3 * (int64_t)o + 2] = (double)gz * s;
+      }
+    }
+  }
+}
+
+template <typename R>
+struct R4 { R x, y, z, w; };
+
+// the hardware reciprocal square root (PTX rsqrt.approx, relative error below 2^-22), with
+// subnormal inputs flushed: squared distances of distinct points in leaf-centred coordinates are
+// far above FP32's subnormal range, and the self term (r² = 0 → ∞) is masked by index
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+template <typename R>
+struct NearWarp {
+  R4<R> stg[2][32];   // double-buffered batch of staged sources
+  int lo[32];         // first point of each colleague (27 used)
+  int pre[32];        // flat index of each colleague's first point (total for the unused slots)
+};
+
+// the sources of batch b (flat indices 32b + lane) from global memory, in FP64
+template <typename R>
+__device__ __forceinline__ void load_batch(const NearWarp<R>& sw, int b, int lane, int S, const double* __restrict__ xs,
+                                           const double* __restrict__ ys, const double* __restrict__ zs,
+                                           const double* __restrict__ q, double& x, double& y, double& z, double& w) {
+  const int f = 32 * b + lane;
+  x = y = z = w = 0.0;
+  if (f < S) {
+    int idx = 0;   // the last colleague whose flat start is ≤ f
+#pragma unroll
+    for (int step = 16; step; step >>= 1)
+      if (sw.pre[idx + step] <= f) idx += step;
+    const int j = sw.lo[idx] + (f - sw.pre[idx]);
+    x = xs[j];
+    y = ys[j];
+    z = zs[j];
+    w = q[j];
+  }
+}
+
+// one batch of m staged sources against this lane's target; CHECK skips flat index `is`
+template <typename R, bool CHECK>
+__device__ __forceinline__ void near_batch(const R4<R>* __restrict__ stg, int m, int is, R fx, R fy, R fz, R& bp, R& bx,
+                                           R& by, R& bz) {
+  auto body = [&](int i) {
+    const R4<R> sv = stg[i];
+    const R dx = fx - sv.x, dy = fy - sv.y, dz = fz - sv.z;
+    R r2, ir;
+    if constexpr (sizeof(R) == 8) {
+      r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+      ir = rsqrt(r2);
+    } else {
+      r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      ir = rsqrt_ftz(r2);
+    }
+    if (CHECK && i == is) ir = R(0);
+    const R qir = sv.w * ir;
+    const R qir3 = qir * ir * ir;
+    bp += qir;
+    bx = fma(qir3, dx, bx);
+    by = fma(qir3, dy, by);
+    bz = fma(qir3, dz, bz);
+  };
+  if (m == 32) {
+#pragma unroll 8
+    for (int i = 0; i < 32; ++i) body(i);
+  } else {
+#pragma unroll 4
+    for (int i = 0; i < m; ++i) body(i);
+  }
+}
+
+template <typename R, bool SELF>
+__global__ void __launch_bounds__(NEAR_WARPS * 32) k_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
+                                                         const int* __restrict__ gcount, int ngroups,
+                                                         const double* __restrict__ tx, const double* __restrict__ ty,
+                                                         const double* __restrict__ tz, const int* __restrict__ tout,
+                                                         const double* __restrict__ xs, const double* __restrict__ ys,
+                                                         const double* __restrict__ zs, const double* __restrict__ q,
+                                                         const int4* __restrict__ cell, const int* __restrict__ plo,
+                                                         const int* __restrict__ phi, const int* __restrict__ col,
+                                                         Geometry geo, int outputs, double* __restrict__ pot,
+                                                         double* __restrict__ grad) {
+  constexpr bool REL = sizeof(R) == 4;   // the mixed path works relative to the leaf's centre
+  __shared__ NearWarp<R> sws[NEAR_WARPS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x * NEAR_WARPS + warp;
+  if (grp >= ngroups) return;                      // the whole warp
+  NearWarp<R>& sw = sws[warp];
+  const int leaf = gnode[grp];
+  double cx = 0, cy = 0, cz = 0;
+  if (REL) {
+    const int4 c = cell[leaf];
+    const double w = ldexp(geo.W0, -c.w);
+    cx = geo.center(0, c.x, w);
+    cy = geo.center(1, c.y, w);
+    cz = geo.center(2, c.z, w);
+  }
+  // the colleagues' point ranges, flattened in colleague order
+  const int cn = lane < NCOL ? col[(int64_t)leaf * NCOL + lane] : -1;
+  int lo = 0, len = 0;
+  if (cn >= 0) {
+    lo = plo[cn];
+    len = max(0, phi[cn] - lo + 1);
+  }
+  int incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int S = __shfl_sync(0xffffffffu, incl, 31);
+  sw.lo[lane] = lo;
+  sw.pre[lane] = incl - len;
+  // the leaf's own slot: its points are the self terms
+  const unsigned selfm = __ballot_sync(0xffffffffu, cn == leaf);
+  const int slot = selfm ? __ffs(selfm) - 1 : 0;
+  const int pself = selfm ? __shfl_sync(0xffffffffu, incl - len, slot) : -1;
+  const int loself = __shfl_sync(0xffffffffu, lo, slot), lenself = selfm ? __shfl_sync(0xffffffffu, len, slot) : 0;
+  __syncwarp();
+  const int t0 = gstart[grp], nt = gcount[grp];
+  for (int base = 0; base < nt; base += 32) {
+    const int k = t0 + base + lane;
+    const bool act = base + lane < nt;
+    const double x = act ? tx[k] : cx, y = act ? ty[k] : cy, z = act ? tz[k] : cz;
+    const R fx = (R)(x - cx), fy = (R)(y - cy), fz = (R)(z - cz);
+    const int fself = SELF && act && selfm ? pself + (k - loself) : -1;
+    double np = 0, nx = 0, ny = 0, nz = 0;
+    double sx, sy, sz, sq;
+    load_batch(sw, 0, lane, S, xs, ys, zs, q, sx, sy, sz, sq);
+    for (int b = 0; 32 * b < S; ++b) {
+      R4<R>* stg = sw.stg[b & 1];
+      stg[lane] = R4<R>{(R)(sx - cx), (R)(sy - cy), (R)(sz - cz), (R)sq};
+      __syncwarp();
+      if (32 * (b + 1) < S) load_batch(sw, b + 1, lane, S, xs, ys, zs, q, sx, sy, sz, sq);
+      const int m = min(32, S - 32 * b);
+      const bool chk = SELF && selfm && 32 * b < pself + lenself && 32 * b + 32 > pself;   // uniform
+      if constexpr (sizeof(R) == 8) {
+        // the plain path sums straight into the FP64 totals, in the reference's order
+        if (chk) near_batch<R, true>(stg, m, fself - 32 * b, fx, fy, fz, np, nx, ny, nz);
+        else near_batch<R, false>(stg, m, 0, fx, fy, fz, np, nx, ny, nz);
+      } else {
+        R bp = 0, bx = 0, by = 0, bz = 0;
+        if (chk) near_batch<R, true>(stg, m, fself - 32 * b, fx, fy, fz, bp, bx, by, bz);
+        else near_batch<R, false>(stg, m, 0, fx, fy, fz, bp, bx, by, bz);
+        np += bp;
+        nx += bx;
+        ny += by;
+        nz += bz;
+      }
+    }
+    if (act) {
+      const int o = tout[k];
+      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = pot[o] + KC * np;
+      if (outputs & FMMB_OUTPUT_GRADIENT) {
+        grad[3 * (int64_t)o] = grad[3 * (int64_t)o] - KC * nx;
+        grad[3 * (int64_t)o + 1] = grad[3 * (int64_t)o + 1] - KC * ny;
+        grad[3 * (int64_t)o + 2] = grad[3 * (int64_t)o + 2] - KC * nz;
+      }
+    }
+    __syncwarp();   // the staging buffers are reused by the next group of targets
+  }
+}
+
+template <int P>
+void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
+                const double* tz, const int* tout, int outputs, double* pot, double* grad) {
+  Plan& P_ = *S.plan;
+  const int warps = 8;
+  const bool mixed = S.precision == FMMB_PRECISION_MIXED;
+  const size_t smem = (mixed ? sizeof(float) : sizeof(double)) * warps * P_.cache->ld;
+  auto kern = mixed ? k_l2p<P, float> : k_l2p<P, double>;
+  kern<<<(ng + warps - 1) / warps, 32 * warps, smem, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, P_.cell.p,
+                                                                      S.Pl.p, P_.cache->ld, geometry(P_), P_.d_scale.p,
+                                                                      outputs, pot, grad);
+  FMMB_LAUNCH_CHECK();
+}
+
+template <typename R, bool SELF>
+void launch_near(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
+                 const double* tz, const int* tout, int outputs, double* pot, double* grad) {
+  Plan& P_ = *S.plan;
+  k_near<R, SELF><<<(ng + NEAR_WARPS - 1) / NEAR_WARPS, 32 * NEAR_WARPS, 0, P_.ctx->stream>>>(
+      gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p, S.zs.p, S.q.p, P_.cell.p, P_.plo.p, P_.phi.p, P_.col.p,
+      geometry(P_), outputs, pot, grad);
+  FMMB_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
+                     const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad) {
+  if (ng == 0) return;
+  switch (S.plan->cache->p) {
+#define X(pp) case pp: launch_l2p<pp>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad); break;
+    FMMB_P_CASES(X)
+#undef X
+    default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
+  }
+  const bool mixed = S.precision == FMMB_PRECISION_MIXED;
+  if (mixed && self) launch_near<float, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+  else if (mixed) launch_near<float, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+  else if (self) launch_near<double, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+  else launch_near<double, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+}
+
+}  // namespace fmmb

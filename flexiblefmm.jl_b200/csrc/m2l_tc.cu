@@ -232,9 +232,14 @@ struct TcCfg {
   static constexpr int B_HALF = NCHK * KP * 2;
   static constexpr int STAGE_BYTES = 2 * B_HALF;
   static constexpr int STAGES = MT == 1 ? 4 : 3;
-  static constexpr int HALVES = MT == 1 ? 2 : 1;           // read-back warps per lane quadrant and tile
+  // warp roles (a warp reads the tensor-memory lane quadrant warp % 4): read-back warps [0, NEPI):
+  // one tile, two per quadrant (HALVES), or two tiles (p = 11), one per quadrant plus warp 4 for the
+  // second tile's rows (quadrant 0); then one gather warp per stage from GB; the issuing warp IW
+  static constexpr int HALVES = MT == 1 ? 2 : 1;           // read-back warps per lane quadrant of the first tile
   static constexpr int NEPI = 4 * HALVES + (MT - 1);       // read-back warps
-  static constexpr int THREADS = 32 * (NEPI + STAGES + 1); // + one gather warp per stage + 1 issuing warp
+  static constexpr int GB = NEPI;
+  static constexpr int IW = NEPI + STAGES;
+  static constexpr int THREADS = 32 * (IW + 1);
   static constexpr int B_OFF = (A_BYTES + 1023) / 1024 * 1024;
   static constexpr int PI_OFF = B_OFF + STAGES * STAGE_BYTES;
   static constexpr int SGN_OFF = PI_OFF + STAGES * (int)sizeof(PairInfo);
@@ -297,9 +302,10 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
 
   if (warp < G::NEPI) {
     // ---------------- read back and scatter: thread = output row of tile `tile`
-    // with two halves per quadrant (p ≤ 10), warps 0-3 take the columns before the chunk's split and
-    // warps 4-7 the rest: the split is a run start, so every entry still has one writer per chunk
-    const int half = G::HALVES == 2 ? warp >> 2 : 0, tile = G::HALVES == 2 ? 0 : warp >> 2, quad = warp & 3;
+    // with two warps per lane quadrant, one takes the columns before the chunk's split, the other
+    // the rest; the split is a run start, so every entry still has one writer per chunk
+    const int tile = warp < 4 * G::HALVES ? 0 : 1;
+    const int half = tile == 0 ? warp >> 2 : 0, quad = warp & 3;
     const int row = 128 * tile + 32 * quad + lane;
     const bool live = row < NP;
     const double alpha = m2l_scale[b.x];
@@ -377,10 +383,10 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         mbar_arrive(&tempty[s]);
       }
     }
-  } else if (warp < G::NEPI + G::STAGES) {
+  } else if (warp >= G::GB && warp < G::GB + G::STAGES) {
     // ---------------- gather: warp gw builds the chunks i ≡ gw (mod STAGES), always in stage gw;
     // lane octet o = lane & 7 the pairs of a group of 8, cq = lane >> 3 the core column
-    const int gw = warp - G::NEPI, o = lane & 7, cq = lane >> 3;
+    const int gw = warp - G::GB, o = lane & 7, cq = lane >> 3;
     const int s = gw;
     unsigned char* bh = sB + s * G::STAGE_BYTES;
     PairInfo& pi = pinfo[s];
@@ -483,7 +489,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         mbar_arrive(&full[s]);
       }
     }
-  } else if (lane == 0) {
+  } else if (warp == G::IW && lane == 0) {
     // ---------------- issue: the class operator when the class changes, then the chunk's MMAs
     int i = 0, ncls = 0;
     bool a_pending = false;

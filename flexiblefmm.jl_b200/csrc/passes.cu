@@ -21,6 +21,8 @@ namespace fmmb {
 
 __constant__ double c_tab[5 * TRI_MAX];  // a, b, cz, cm, cp of the Schmidt recurrences, up to degree PMAX
 __constant__ double c_e[PMAX];           // the sectoral factors e_m, m = 1..PMAX
+__constant__ float c_tabf[5 * TRI_MAX];
+__constant__ float c_ef[PMAX];
 
 void init_device_constants(cudaStream_t s) {
   std::vector<double> t(5 * TRI_MAX, 0.0), e(PMAX);
@@ -39,6 +41,9 @@ void init_device_constants(cudaStream_t s) {
   for (int m = 1; m <= PMAX; ++m) e[m - 1] = std::sqrt((double)(2 * m - 1) / (double)(2 * m));
   FMMB_CUDA(cudaMemcpyToSymbolAsync(c_tab, t.data(), sizeof(double) * t.size(), 0, cudaMemcpyHostToDevice, s));
   FMMB_CUDA(cudaMemcpyToSymbolAsync(c_e, e.data(), sizeof(double) * e.size(), 0, cudaMemcpyHostToDevice, s));
+  const std::vector<float> tf(t.begin(), t.end()), ef(e.begin(), e.end());
+  FMMB_CUDA(cudaMemcpyToSymbolAsync(c_tabf, tf.data(), sizeof(float) * tf.size(), 0, cudaMemcpyHostToDevice, s));
+  FMMB_CUDA(cudaMemcpyToSymbolAsync(c_ef, ef.data(), sizeof(float) * ef.size(), 0, cudaMemcpyHostToDevice, s));
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -74,9 +79,11 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
   for (int i = threadIdx.x; i < 2 * TRI_MAX; i += blockDim.x) s_ab[i] = c_tab[i];
   for (int i = threadIdx.x; i < PMAX; i += blockDim.x) s_e[i] = c_e[i];
   __syncthreads();
+  // thread g: order m = g / nn of node g % nn; the lanes of a warp share the order, so the
+  // recurrence's branches on n versus m are uniform
   int g = blockIdx.x * blockDim.x + threadIdx.x;
-  int qn = g / (P + 1), m = g % (P + 1);
-  if (qn >= nn) return;
+  int m = g / nn, qn = g % nn;
+  if (m > P) return;
   int node = nodes[qn];
   int4 c = cell[node];
   double w = ldexp(geo.W0, -c.w), s = scale[c.w];
@@ -217,69 +224,6 @@ void gemm_cols(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols, i
   FMMB_LAUNCH_CHECK();
 }
 
-// ---------------------------------------------------------------- evaluation, FP64
-// one warp per group of targets in one real leaf; lanes over the targets, the sources of
-// the 27 colleagues read in lockstep (warp-uniform addresses: broadcast loads)
-template <int P, bool SELF>
-__global__ void __launch_bounds__(256) k_eval_f64(const int* __restrict__ gnode, const int* __restrict__ gstart,
-                                                  const int* __restrict__ gcount, int ngroups, const double* __restrict__ tx,
-                                                  const double* __restrict__ ty, const double* __restrict__ tz,
-                                                  const int* __restrict__ tout, const double* __restrict__ xs,
-                                                  const double* __restrict__ ys, const double* __restrict__ zs,
-                                                  const double* __restrict__ q, const int4* __restrict__ cell,
-                                                  const int* __restrict__ plo, const int* __restrict__ phi,
-                                                  const int* __restrict__ col, const double* __restrict__ Pl, int LD,
-                                                  Geometry geo, const double* __restrict__ scale, int outputs,
-                                                  double* __restrict__ pot, double* __restrict__ grad) {
-  extern __shared__ double sl[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int grp = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (grp >= ngroups) return;
-  double* L = sl + warp * LD;
-  const int leaf = gnode[grp];
-  for (int i = lane; i < LD; i += 32) L[i] = Pl[(int64_t)leaf * LD + i];
-  __syncwarp();
-  const int4 c = cell[leaf];
-  const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
-  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
-  const int t0 = gstart[grp], nt = gcount[grp];
-  for (int base = 0; base < nt; base += 32) {
-    const int k = t0 + base + lane;
-    const bool act = base + lane < nt;
-    const double x = act ? tx[k] : cx, y = act ? ty[k] : cy, z = act ? tz[k] : cz;
-    double u, gx, gy, gz;
-    l2p_f64<P>(L, (x - cx) * s, (y - cy) * s, (z - cz) * s, u, gx, gy, gz);
-    double np = 0, nx = 0, ny = 0, nz = 0;
-#pragma unroll 1
-    for (int kk = 0; kk < NCOL; ++kk) {
-      const int cn = col[(int64_t)leaf * NCOL + kk];
-      if (cn < 0) continue;
-      const int j1 = phi[cn];
-      for (int j = plo[cn]; j <= j1; ++j) {
-        const double dx = x - xs[j], dy = y - ys[j], dz = z - zs[j];
-        const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-        double ir = rsqrt(r2);
-        if (SELF && j == k) ir = 0.0;
-        const double qir = q[j] * ir;
-        const double qir3 = qir * ir * ir;
-        np += qir;
-        nx = fma(qir3, dx, nx);
-        ny = fma(qir3, dy, ny);
-        nz = fma(qir3, dz, nz);
-      }
-    }
-    if (act) {
-      const int o = tout[k];
-      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = u + KC * np;
-      if (outputs & FMMB_OUTPUT_GRADIENT) {
-        grad[3 * (int64_t)o] = gx * s - KC * nx;
-        grad[3 * (int64_t)o + 1] = gy * s - KC * ny;
-        grad[3 * (int64_t)o + 2] = gz * s - KC * nz;
-      }
-    }
-  }
-}
-
 // ---------------------------------------------------------------- locate and bucketing
 __global__ void k_locate(const double* __restrict__ tg, int64_t nt, const int4* __restrict__ cell,
                          const int* __restrict__ cf, const uint8_t* __restrict__ flags, Geometry geo,
@@ -412,18 +356,6 @@ void launch_p2m(State& S) {
   FMMB_LAUNCH_CHECK();
 }
 
-template <int P, bool SELF>
-void launch_eval_f64(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
-                     const double* ty, const double* tz, const int* tout, int outputs, double* pot, double* grad) {
-  Plan& P_ = *S.plan;
-  if (ng == 0) return;
-  const int warps = 8;
-  size_t smem = sizeof(double) * warps * P_.cache->ld;
-  k_eval_f64<P, SELF><<<(ng + warps - 1) / warps, 32 * warps, smem, P_.ctx->stream>>>(
-      gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p, S.zs.p, S.q.p, P_.cell.p, P_.plo.p, P_.phi.p, P_.col.p,
-      S.Pl.p, P_.cache->ld, geometry(P_), P_.d_scale.p, outputs, pot, grad);
-  FMMB_LAUNCH_CHECK();
-}
 
 
 }  // namespace
@@ -458,7 +390,6 @@ void gather_inputs(State& S, const double* xyz_dev, const double* tau_dev) {
   FMMB_LAUNCH_CHECK();
 }
 
-#define FMMB_P_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20)
 
 int p2m(State& S) {
   switch (S.plan->cache->p) {
@@ -525,21 +456,6 @@ void downward_pass(State& S) {
   l2l_sweep(S);
 }
 
-void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
-                     const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad) {
-  int p = S.plan->cache->p;
-  if (S.precision == FMMB_PRECISION_MIXED) {
-    eval_mixed(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, self, outputs, pot, grad);
-    return;
-  }
-  switch (p) {
-#define X(pp) case pp: if (self) launch_eval_f64<pp, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad); \
-                       else launch_eval_f64<pp, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad); break;
-    FMMB_P_CASES(X)
-#undef X
-    default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
-  }
-}
 
 void evaluate_sources(State& S, int outputs, double* pot, double* grad) {
   Plan& P = *S.plan;

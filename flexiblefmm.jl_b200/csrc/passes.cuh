@@ -1,4 +1,4 @@
-// Declarations shared by the pass kernels (passes.cu, m2l_tc.cu, eval_mixed.cu).
+// Declarations shared by the pass kernels (passes.cu, m2l_f64.cu, m2l_tc.cu, eval.cu).
 #pragma once
 #include "plan.cuh"
 
@@ -20,26 +20,35 @@ Geometry geometry(const Plan& P);
 
 extern __constant__ double c_tab[5 * TRI_MAX];
 extern __constant__ double c_e[PMAX];
+extern __constant__ float c_tabf[5 * TRI_MAX];   // the same tables in FP32 (the mixed path's L2P)
+extern __constant__ float c_ef[PMAX];
 void init_device_constants(cudaStream_t s);
 
+template <typename R> __device__ __forceinline__ R ctab(int i);
+template <> __device__ __forceinline__ double ctab<double>(int i) { return c_tab[i]; }
+template <> __device__ __forceinline__ float ctab<float>(int i) { return c_tabf[i]; }
+template <typename R> __device__ __forceinline__ R ce(int i);
+template <> __device__ __forceinline__ double ce<double>(int i) { return c_e[i]; }
+template <> __device__ __forceinline__ float ce<float>(int i) { return c_ef[i]; }
+
 // L2P at x̂ (potential and the gradient before the 1/w factor) from the local L in shared
-// memory; the orders run as a loop (a full unroll keeps too many coefficients in registers)
-template <int P>
-__device__ __forceinline__ void l2p_f64(const double* __restrict__ L, double x, double y, double z, double& u, double& gx,
-                                        double& gy, double& gz) {
-  double r2 = x * x + y * y + z * z;
-  double sr = 1.0, si = 0.0;
+// memory, in precision R (FP64 on the plain path, FP32 on the mixed path); the orders run as a
+// loop (a full unroll keeps too many coefficients in registers)
+template <int P, typename R>
+__device__ __forceinline__ void l2p(const R* __restrict__ L, R x, R y, R z, R& u, R& gx, R& gy, R& gz) {
+  R r2 = x * x + y * y + z * z;
+  R sr = 1, si = 0;
   u = 0; gx = 0; gy = 0; gz = 0;
 #pragma unroll 1
   for (int m = 0; m <= P; ++m) {
-    double pr = 0, pi = 0, cr = sr, ci = si;
+    R pr = 0, pi = 0, cr = sr, ci = si;
 #pragma unroll 2
     for (int n = m; n <= P; ++n) {
-      double vr, vi;
+      R vr, vi;
       if (n == m) { vr = sr; vi = si; }
       else {
         const int t = tri(n, m);
-        double az = c_tab[t] * z, br = c_tab[TRI_MAX + t] * r2;
+        R az = ctab<R>(t) * z, br = ctab<R>(TRI_MAX + t) * r2;
         vr = az * cr - br * pr; vi = az * ci - br * pi;
         pr = cr; pi = ci; cr = vr; ci = vi;
       }
@@ -50,21 +59,21 @@ __device__ __forceinline__ void l2p_f64(const double* __restrict__ L, double x, 
       if (n < P) {
         const int n1 = n + 1;
         if (m == 0) {
-          double cmv = c_tab[3 * TRI_MAX + tri(n1, 1)];
-          double lr = L[n1 * n1 + 1], li = L[n1 * n1 + 2];
+          R cmv = ctab<R>(3 * TRI_MAX + tri(n1, 1));
+          R lr = L[n1 * n1 + 1], li = L[n1 * n1 + 2];
           gx += -cmv * lr * vr;
           gy += -cmv * li * vr;
-          gz += c_tab[2 * TRI_MAX + tri(n1, 0)] * L[n1 * n1] * vr;
+          gz += ctab<R>(2 * TRI_MAX + tri(n1, 0)) * L[n1 * n1] * vr;
         } else {
-          double ur = L[n1 * n1 + 2 * (m + 1) - 1], ui = L[n1 * n1 + 2 * (m + 1)];
-          double dr, di;
-          if (m == 1) { dr = L[n1 * n1]; di = 0.0; }
+          R ur = L[n1 * n1 + 2 * (m + 1) - 1], ui = L[n1 * n1 + 2 * (m + 1)];
+          R dr, di;
+          if (m == 1) { dr = L[n1 * n1]; di = 0; }
           else { dr = L[n1 * n1 + 2 * (m - 1) - 1]; di = L[n1 * n1 + 2 * (m - 1)]; }
-          double cu = 0.5 * c_tab[3 * TRI_MAX + tri(n1, m + 1)], cd = 0.5 * c_tab[4 * TRI_MAX + tri(n1, m - 1)];
-          double axr = -cu * ur + cd * dr, axi = -cu * ui + cd * di;
-          double ayr = -(cu * ui + cd * di), ayi = cu * ur + cd * dr;
-          double czv = c_tab[2 * TRI_MAX + tri(n1, m)];
-          double zr = L[n1 * n1 + 2 * m - 1], zi = L[n1 * n1 + 2 * m];
+          R cu = R(0.5) * ctab<R>(3 * TRI_MAX + tri(n1, m + 1)), cd = R(0.5) * ctab<R>(4 * TRI_MAX + tri(n1, m - 1));
+          R axr = -cu * ur + cd * dr, axi = -cu * ui + cd * di;
+          R ayr = -(cu * ui + cd * di), ayi = cu * ur + cd * dr;
+          R czv = ctab<R>(2 * TRI_MAX + tri(n1, m));
+          R zr = L[n1 * n1 + 2 * m - 1], zi = L[n1 * n1 + 2 * m];
           gx += 2 * (axr * vr + axi * vi);
           gy += 2 * (ayr * vr + ayi * vi);
           gz += 2 * czv * (zr * vr + zi * vi);
@@ -72,12 +81,15 @@ __device__ __forceinline__ void l2p_f64(const double* __restrict__ L, double x, 
       }
     }
     if (m < P) {
-      double e = c_e[m];
-      double nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
+      R e = ce<R>(m);
+      R nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
       sr = nr; si = ni;
     }
   }
 }
+
+// the orders with compiled kernels
+#define FMMB_P_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20)
 
 void m2l_f64(State& S);
 int p2m(State& S);          // the stages of the passes; each returns its kernel launches
@@ -86,11 +98,9 @@ int m2l_stage(State& S);
 int l2l_sweep(State& S);
 void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
                      const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad);
-// the mixed path (m2l_tc.cu, eval_mixed.cu)
+// the mixed path (m2l_tc.cu)
 void prepare_mixed_operators(Cache& C);
 void m2l_mixed(State& S);
 int mixed_error_flag(State& S);   // 1 when a bounded wait of the tensor-core M2L gave up
-void eval_mixed(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
-                const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad);
 
 }  // namespace fmmb
