@@ -183,6 +183,10 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
       : "memory");
 }
 
+__device__ __forceinline__ void tmem_st1(uint32_t taddr, float v) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(__float_as_uint(v)) : "memory");
+}
+
 __device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
   uint32_t r;
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
@@ -232,22 +236,21 @@ struct TcCfg {
   static constexpr int B_HALF = NCHK * KP * 2;
   static constexpr int STAGE_BYTES = 2 * B_HALF;
   static constexpr int STAGES = MT == 1 ? 4 : 3;
-  // warp roles (a warp reads the tensor-memory lane quadrant warp % 4): read-back warps [0, NEPI):
-  // one tile, two per quadrant (HALVES), or two tiles (p = 11), one per quadrant plus warp 4 for the
-  // second tile's rows (quadrant 0); then one gather warp per stage from GB; the issuing warp IW
-  static constexpr int HALVES = MT == 1 ? 2 : 1;           // read-back warps per lane quadrant of the first tile
-  static constexpr int NEPI = 4 * HALVES + (MT - 1);       // read-back warps
-  static constexpr int GB = NEPI;
-  static constexpr int IW = NEPI + STAGES;
+  // warp roles (a warp reads the tensor-memory lane quadrant warp % 4): read-back warps 0-7 for the
+  // first tile (two per quadrant), for a second tile (p = 11) warps 8 and 12 (its rows lie in
+  // quadrant 0); one gather warp per stage from GB; the issuing warp IW
+  static constexpr int NEPI = 8 + 2 * (MT - 1);            // read-back warps
+  static constexpr int GB = MT == 1 ? 8 : 9;
+  static constexpr int IW = MT == 1 ? 12 : 13;
   static constexpr int THREADS = 32 * (IW + 1);
+  static_assert(GB + STAGES <= (MT == 1 ? IW : 12), "warp roles");
   static constexpr int B_OFF = (A_BYTES + 1023) / 1024 * 1024;
   static constexpr int PI_OFF = B_OFF + STAGES * STAGE_BYTES;
   static constexpr int SGN_OFF = PI_OFF + STAGES * (int)sizeof(PairInfo);
   static constexpr int D4H_OFF = SGN_OFF + 16 * KC * 16;
   static constexpr int BAR_OFF = D4H_OFF + NFAR * 4;
   static constexpr int SMEM = BAR_OFF + (1 + 3 * STAGES) * 8 + 16;
-  static constexpr int SCAN_COL = STAGES * MT * NCHK;    // per tile and half NCHK columns of run sums
-  static_assert(SCAN_COL + MT * HALVES * NCHK <= TMEM_COLS, "tensor memory");
+  static_assert(STAGES * MT * NCHK <= TMEM_COLS, "tensor memory");
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
@@ -300,12 +303,13 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
 
-  if (warp < G::NEPI) {
+  const bool reader = warp < 8 || (MT == 2 && (warp == 8 || warp == 12));
+  if (reader) {
     // ---------------- read back and scatter: thread = output row of tile `tile`
-    // with two warps per lane quadrant, one takes the columns before the chunk's split, the other
-    // the rest; the split is a run start, so every entry still has one writer per chunk
-    const int tile = warp < 4 * G::HALVES ? 0 : 1;
-    const int half = tile == 0 ? warp >> 2 : 0, quad = warp & 3;
+    // two warps per lane quadrant and tile: one takes the columns before the chunk's split, the
+    // other the rest; the split is a run start, so every entry still has one writer per chunk
+    const int tile = warp < 8 ? 0 : 1;
+    const int half = warp < 8 ? warp >> 2 : (warp == 8 ? 0 : 1), quad = warp & 3;
     const int row = 128 * tile + 32 * quad + lane;
     const bool live = row < NP;
     const double alpha = m2l_scale[b.x];
@@ -318,7 +322,6 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
       const int partner = epart == 0 ? row : (epart == 1 ? row + 1 : row - 1);
       src_lane = partner & 31;                       // pairs never straddle a 32-row boundary (p ≤ 11)
     }
-    const uint32_t scan = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(G::SCAN_COL + (tile * G::HALVES + half) * NCHK);
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
       const int a0 = co[c], a1 = co[c + 1];
@@ -333,10 +336,11 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         const PairInfo& pi = pinfo[s];
         const int nc = pi.n;
         const uint64_t starts = pi.starts;
-        const int lo = half ? pi.split : 0, hi = (G::HALVES == 2 && !half) ? pi.split : nc;
+        const int lo = half ? pi.split : 0, hi = half ? nc : pi.split;
         const uint32_t ta = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)((s * MT + tile) * NCHK);
         // phase 1 (branch-free): per column the permuted, unscaled value, and the running sum of
-        // the column's target run (reset where a run starts), parked in this tile's scan columns
+        // the column's target run (reset where a run starts), written back in place of the
+        // accumulator columns just read (only this warp's columns: the other half owns the rest)
         float acc = 0.f;
 #pragma unroll
         for (int c16 = 0; c16 < NCHK / 16; ++c16) {
@@ -363,7 +367,13 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
               a[4 * e4 + e] = acc;
             }
           }
-          tmem_st16(scan + 16 * c16, a);
+          if (16 * c16 >= lo && (16 * c16 + 16 <= hi || hi == nc)) {
+            tmem_st16(ta + 16 * c16, a);
+          } else {
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+              if (16 * c16 + e >= lo && 16 * c16 + e < hi) tmem_st1(ta + 16 * c16 + e, a[e]);   // uniform
+          }
         }
         tmem_wait_st();
         // phase 2: the sum of each run is the scan at its last column; one reduction per run
@@ -373,7 +383,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         for (int k0 = k_lo; k0 < k_hi; k0 += 4) {
           float v[4];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) v[k] = tmem_ld1(scan + (uint32_t)pi.rend[min(k0 + k, k_hi - 1)]);
+          for (int k = 0; k < 4; ++k) v[k] = tmem_ld1(ta + (uint32_t)pi.rend[min(k0 + k, k_hi - 1)]);
           tmem_wait_ld();
 #pragma unroll
           for (int k = 0; k < 4; ++k)
