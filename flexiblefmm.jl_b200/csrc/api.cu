@@ -62,7 +62,11 @@ int guard(F&& f) {
   }
 }
 
-void set_device(const Ctx& c) { FMMB_CUDA(cudaSetDevice(c.device)); }
+// every entry point: the context's device, and its stream for the thread's device allocations
+void set_device(const Ctx& c) {
+  FMMB_CUDA(cudaSetDevice(c.device));
+  g_alloc_stream = c.stream;
+}
 
 // A device-pointer argument must be memory the context's device can read and write: its own
 // device memory, managed memory, or host memory allocated or registered by CUDA. A plain host

@@ -32,40 +32,56 @@ inline void require(bool ok, int code, const std::string& msg) {
   if (!ok) throw Error(code, msg);
 }
 
-// A device allocation owned by its holder (moves only).
+// The stream the calling thread's allocations are ordered on (the context's stream, set by
+// every entry point): device buffers come from the stream-ordered allocator, so allocating and
+// freeing never synchronises the whole device (independent requests on other streams keep
+// running). Outside an entry point (no stream set) plain cudaMalloc/cudaFree are used.
+inline thread_local cudaStream_t g_alloc_stream = nullptr;
+
+// A device allocation owned by its holder (moves only); freed on the stream it was allocated on.
 template <class T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t s = nullptr;
   DBuf() = default;
   explicit DBuf(size_t count) { alloc(count); }
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
-  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
   DBuf& operator=(DBuf&& o) noexcept {
-    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) { release(); p = o.p; n = o.n; s = o.s; o.p = nullptr; o.n = 0; }
     return *this;
   }
   ~DBuf() { release(); }
+  static void raw_alloc(T** q, size_t count, cudaStream_t st) {
+    if (st) FMMB_CUDA(cudaMallocAsync((void**)q, count * sizeof(T), st));
+    else FMMB_CUDA(cudaMalloc((void**)q, count * sizeof(T)));
+  }
   void alloc(size_t count) {
     release();
     n = count;
-    if (count) FMMB_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+    s = g_alloc_stream;
+    if (count) raw_alloc(&p, count, s);
   }
   // grow to at least `count` entries, keeping the first `keep`
-  void grow(size_t count, size_t keep, cudaStream_t s) {
+  void grow(size_t count, size_t keep, cudaStream_t st) {
     if (count <= n) return;
     size_t cap = std::max(count, n * 2);
     T* q = nullptr;
-    FMMB_CUDA(cudaMalloc((void**)&q, cap * sizeof(T)));
-    if (keep && p) FMMB_CUDA(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
-    FMMB_CUDA(cudaStreamSynchronize(s));
+    raw_alloc(&q, cap, g_alloc_stream);
+    if (keep && p) FMMB_CUDA(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    FMMB_CUDA(cudaStreamSynchronize(st));
     release();
     p = q;
     n = cap;
+    s = g_alloc_stream;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (s) cudaFreeAsync(p, s);
+      else cudaFree(p);
+    }
     p = nullptr;
     n = 0;
   }

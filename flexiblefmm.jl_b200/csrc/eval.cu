@@ -62,8 +62,10 @@ __global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, cons
   }
 }
 
+// one staged source: aligned so that it is read with one 16-byte (FP32) or two 16-byte (FP64)
+// shared-memory loads
 template <typename R>
-struct R4 { R x, y, z, w; };
+struct alignas(4 * sizeof(R)) R4 { R x, y, z, w; };
 
 // the hardware reciprocal square root (PTX rsqrt.approx, relative error below 2^-22), with
 // subnormal inputs flushed: squared distances of distinct points in leaf-centred coordinates are
