@@ -54,6 +54,8 @@ def args_():
     a.add_argument("--samples", type=int, default=4096)
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--no-p10", action="store_true", help="skip the side measurement at the configured order p = 10")
+    a.add_argument("--serve-requests", type=int, default=96, help="requests of the serving measurement (0: skip it)")
+    a.add_argument("--serve-slots", type=int, default=4)
     return a.parse_args()
 
 
@@ -169,6 +171,73 @@ class Clocks:
         load = [s for s in sm if s > 0.5 * max(sm)] or sm
         return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
 
+
+
+# ---------------------------------------------------------------- the serving loop
+def serving_workload(count, seed=6):
+    """Requests as the serving configuration draws them: N log-uniform in [1e3, 5e5], points
+    uniform in the unit cube or from 4 Gaussians (σ = 0.02) with equal probability, charges
+    N(0,1), tolerance from {1e-3, 1e-6, 1e-9}. The configuration's Yukawa3D(κ=5) half runs as
+    Laplace3D: the device path provides Laplace3D only."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+        if rng.random() < 0.5:
+            pts = rng.random((n, 3))
+        else:
+            c = 0.1 + 0.8 * rng.random((4, 3))
+            pts = np.clip(c[rng.integers(0, 4, n)] + 0.02 * rng.standard_normal((n, 3)), 0.0, 1.0)
+        out.append((pts, rng.standard_normal(n), float(rng.choice([1e-3, 1e-6, 1e-9]))))
+    return out
+
+
+def serving(fmmb, device, count, slots):
+    """Throughput and latency of the request server: batched (all requests submitted at once),
+    then open-loop Poisson arrivals at 80 % of the batched request rate (p50/p99 latency), and
+    the same requests one at a time on the plain FP64 path."""
+    reqs = serving_workload(count)
+    total = sum(len(r[0]) for r in reqs)
+    srv = fmmb.Server(device, slots=slots)
+    for pts, tau, tol in reqs[:6]:                                     # warm-up: operators resident
+        srv.wait(srv.submit(pts, tau, tol=tol))
+    t0 = time.perf_counter()
+    tk = [srv.submit(pts, tau, tol=tol) for pts, tau, tol in reqs]
+    infos = [srv.wait(k)[2] for k in tk]
+    t_batch = time.perf_counter() - t0
+    rate = 0.8 * count / t_batch                                       # requests/s offered in the open loop
+    rng = np.random.default_rng(60)
+    gaps = rng.exponential(1.0 / rate, count)
+    t0 = time.perf_counter()
+    tk = []
+    due = t0
+    for (pts, tau, tol), g in zip(reqs, gaps):
+        due += g
+        while time.perf_counter() < due:
+            time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
+        tk.append(srv.submit(pts, tau, tol=tol))
+    lat = [srv.wait(k)[2]["latency_s"] for k in tk]
+    t_open = time.perf_counter() - t0
+    srv.close()
+    one = fmmb.Server(device, slots=1)
+    for pts, tau, tol in reqs[:3]:
+        one.wait(one.submit(pts, tau, tol=tol, precision="fp64"))
+    t0 = time.perf_counter()
+    seq_lat = []
+    for pts, tau, tol in reqs:
+        seq_lat.append(one.wait(one.submit(pts, tau, tol=tol, precision="fp64"))[2]["latency_s"])
+    t_seq = time.perf_counter() - t0
+    one.close()
+    q = lambda v, f: float(np.quantile(np.asarray(v) * 1e3, f))
+    return {"requests": count, "slots": slots, "points": total,
+            "workload": "N log-uniform [1e3, 5e5], uniform or 4-Gaussian (sigma 0.02) points, tol in {1e-3, 1e-6, 1e-9} "
+                        "(p and precision path chosen from tol), Laplace3D in place of the Yukawa3D half (seed 6)",
+            "batched": {"evals_per_s": total / t_batch, "requests_per_s": count / t_batch, "seconds": t_batch},
+            "open_loop": {"offered_requests_per_s": rate, "evals_per_s": total / t_open,
+                          "fraction_of_batched": (total / t_open) / (total / t_batch),
+                          "latency_ms": {"p50": q(lat, 0.5), "p99": q(lat, 0.99)}},
+            "one_at_a_time_fp64": {"evals_per_s": total / t_seq, "latency_ms": {"p50": q(seq_lat, 0.5), "p99": q(seq_lat, 0.99)}},
+            "paths": {"mixed": sum(i["precision"] == "mixed" for i in infos), "fp64": sum(i["precision"] == "fp64" for i in infos)}}
 
 # ---------------------------------------------------------------- our arm
 def run_ours(a):
@@ -335,6 +404,7 @@ def run_ours(a):
         cpu = {"value": a.n / min(r["times"]), "unit": UNIT, "cores": r["threads"], "kind": "port",
                "sample": f"full {a.n:,}-point matvec (the same points and charges), best of 2 after 1 warm-up, "
                          f"tree + operators {r['tree_s']:.2f} s untimed"}
+    serve = serving(fmmb, local, a.serve_requests, a.serve_slots) if a.serve_requests > 0 else None
     line = {
         "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -343,6 +413,7 @@ def run_ours(a):
         "config": config(a, {"precision": "mixed", "plan_s": plan_s, "levels": f.nlevels, "nodes": f.nnodes,
                              "far_pairs": f.npairs}),
         "configured_order_p10": side,
+        "serving": serve,
         "latency_ms": {"p50": pct(0.5), "p99": pct(0.99)},
         "fp64": {"value": replica_throughput(a.n, ms_fp64, world), "ms_per_step": ms_fp64},
         "mixed_vs_fp64": ms_fp64 / ms_mixed,

@@ -44,6 +44,21 @@ void free_plan_locked(fmmb_plan* x) {
 
 thread_local std::string g_last_error;
 
+}  // namespace
+
+namespace fmmb {
+// the calling thread's message (the server hands a request's error to the thread that waits)
+void set_last_error(const std::string& m) { g_last_error = m; }
+// fixes a fresh cache's base width, so that every plan's box is snapped from its own points
+// (ldexp(w, e) ⊇ the points) and not from the first box the cache saw
+void fix_cache_base_width(fmmb_cache* c, double w) {
+  std::lock_guard<std::mutex> lk(c->c.mu);
+  if (std::isnan(c->c.W0)) c->c.W0 = w;
+}
+}  // namespace fmmb
+
+namespace {
+
 template <class F>
 int guard(F&& f) {
   try {

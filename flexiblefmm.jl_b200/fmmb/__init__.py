@@ -61,6 +61,22 @@ class _TreeOpts(C.Structure):
                 ("origin", C.c_double * 3), ("width", C.c_double)]
 
 
+class _ServerOpts(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("ppl", C.c_int32), ("hbm_budget", C.c_int64)]
+
+
+class _Request(C.Structure):
+    _fields_ = [("xyz", C.c_void_p), ("tau", C.c_void_p), ("n", C.c_int64), ("tol", C.c_double), ("kernel", C.c_int32),
+                ("p", C.c_int32), ("outputs", C.c_int32), ("precision", C.c_int32), ("pot", C.c_void_p),
+                ("grad", C.c_void_p)]
+
+
+class _RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("p", C.c_int32), ("precision", C.c_int32), ("slot", C.c_int32),
+                ("queued_s", C.c_double), ("run_s", C.c_double), ("latency_s", C.c_double),
+                ("bytes_estimate", C.c_int64)]
+
+
 _lib = None
 EXPORTS = (
     "fmmb_last_error", "fmmb_version", "fmmb_ctx_create", "fmmb_ctx_destroy", "fmmb_ctx_stream", "fmmb_ctx_synchronize",
@@ -69,6 +85,7 @@ EXPORTS = (
     "fmmb_state_destroy", "fmmb_build_expansions", "fmmb_build_expansions_dev", "fmmb_evaluate_at_sources",
     "fmmb_evaluate_at_sources_dev", "fmmb_matvec", "fmmb_matvec_dev", "fmmb_evaluate", "fmmb_evaluate_dev",
     "fmmb_state_expansions", "fmmb_direct_dev", "fmmb_profile_matvec", "fmmb_direct_noalloc_dev",
+    "fmmb_server_create", "fmmb_server_submit", "fmmb_server_wait", "fmmb_server_destroy",
 )
 
 
@@ -116,6 +133,10 @@ def lib():
         "fmmb_direct_dev": [vp, dp, dp, i64, dp, dp, i64, dp, dp],
         "fmmb_profile_matvec": [vp, dp, dp, i64, i32, dp, dp, dp, i32, C.POINTER(C.c_int)],
         "fmmb_direct_noalloc_dev": [vp, dp, dp, i64, dp, dp, i64, dp, dp],
+        "fmmb_server_create": [i32, C.POINTER(_ServerOpts), C.POINTER(vp)],
+        "fmmb_server_submit": [vp, C.POINTER(_Request), C.POINTER(i64)],
+        "fmmb_server_wait": [vp, i64, C.c_double, C.POINTER(_RequestInfo)],
+        "fmmb_server_destroy": [vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -399,3 +420,59 @@ def device_matvec(fmm, state, sources, tau, output=Potential()):
     grad = np.zeros((fmm.N, 3)) if flag == OUTPUT_GRADIENT else None
     _check(lib().fmmb_matvec(state._h, _ptr(x), _ptr(t), fmm.N, flag, _ptr(pot), _ptr(grad)))
     return pot if flag == OUTPUT_POTENTIAL else grad
+
+
+# ---------------------------------------------------------------- the request server
+class Server:
+    """A continuous-batching request server on one GPU (fmmb_server): requests of different
+    sizes and tolerances are admitted in arrival order onto `slots` concurrent streams as slots
+    and device memory (hbm_budget bytes; 0 = 80 % of the free memory) free up. No counterpart in
+    the reference, which runs one FMM per call."""
+
+    def __init__(self, device=0, slots=4, ppl=64, hbm_budget=0):
+        h = C.c_void_p()
+        _check(lib().fmmb_server_create(int(device), C.byref(_ServerOpts(int(slots), int(ppl), int(hbm_budget))),
+                                        C.byref(h)))
+        self._h = h
+        self._live = {}
+
+    def submit(self, sources, tau, tol=1e-6, p=0, precision=None, gradient=True):
+        """Queue one Laplace3D FMM at the sources (potential and, optionally, gradient, self
+        excluded); returns a ticket. precision None: chosen from tol (FP64 below 1e-8)."""
+        x = _points(sources)
+        t = np.ascontiguousarray(tau, dtype=np.float64)
+        if t.shape != (x.shape[0],):
+            raise DimensionMismatch(2, "one charge per source")
+        pot = np.zeros(x.shape[0])
+        grad = np.zeros((x.shape[0], 3)) if gradient else None
+        prec = -1 if precision is None else {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}[precision]
+        flags = OUTPUT_POTENTIAL | (OUTPUT_GRADIENT if gradient else 0)
+        r = _Request(x.ctypes.data, t.ctypes.data, x.shape[0], float(tol), 1, int(p), flags, prec, pot.ctypes.data,
+                     None if grad is None else grad.ctypes.data)
+        ticket = C.c_int64()
+        _check(lib().fmmb_server_submit(self._h, C.byref(r), C.byref(ticket)))
+        self._live[ticket.value] = (x, t, pot, grad)     # the buffers stay alive until the request is waited for
+        return ticket.value
+
+    def wait(self, ticket, timeout=-1.0):
+        """(pot, grad, info) of a request; info: p, precision, slot, queued_s, run_s, latency_s."""
+        info = _RequestInfo()
+        rc = lib().fmmb_server_wait(self._h, int(ticket), float(timeout), C.byref(info))
+        if rc == 5 and info.latency_s == 0 and ticket in self._live:
+            raise TimeoutError("the request is not done yet")
+        bufs = self._live.pop(ticket)
+        _check(rc)
+        d = {k: getattr(info, k) for k, _ in _RequestInfo._fields_}
+        d["precision"] = "fp64" if info.precision == PRECISION_FP64 else "mixed"
+        return bufs[2], bufs[3], d
+
+    def close(self):
+        if self._h:
+            _check(lib().fmmb_server_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -149,6 +149,48 @@ int fmmb_direct_noalloc_dev(fmmb_ctx* ctx, const double* src_dev, const double* 
                             const double* tgt_dev, const int64_t* self_index_dev, int64_t nt, double* pot_dev,
                             double* grad_dev);
 
+/* A continuous-batching request server on one GPU (no counterpart in the reference, which runs
+ * one FMM per call: this is the serving form of FMM + build_expansions + evaluate_at_sources).
+ * Requests are admitted in arrival order onto `slots` worker threads, each with its own context
+ * (stream) and an operator cache per order that stays resident, as soon as a slot is free and
+ * the request's estimated device memory fits what the requests in flight leave of hbm_budget
+ * (the front request waits rather than being overtaken; one that exceeds the budget alone runs
+ * when nothing else does). The device work of admitted requests overlaps. Each request is
+ * computed exactly as it would be alone (its results are bitwise the same in any mix). */
+typedef struct fmmb_server fmmb_server;
+typedef struct {
+  int32_t slots;       /* concurrent requests (worker threads, one stream each), 1..64 */
+  int32_t ppl;         /* points per leaf of every request's tree */
+  int64_t hbm_budget;  /* bytes of device memory the admitted requests may hold; 0: 80 % of the free memory */
+} fmmb_server_opts;
+typedef struct {
+  const double* xyz;   /* 3×n host, original order; read while the request runs */
+  const double* tau;   /* n host */
+  int64_t n;
+  double tol;          /* requested relative accuracy: selects p (when p = 0) and the precision path */
+  int32_t kernel;      /* FMMB_KERNEL_LAPLACE3D */
+  int32_t p;           /* 0: the smallest order whose measured error is below tol */
+  int32_t outputs;     /* FMMB_OUTPUT_* bits */
+  int32_t precision;   /* -1: FP64 for tol < 1e-8 or p > 11, else the mixed path */
+  double* pot;         /* n host, written when the request completes (keep valid until then) */
+  double* grad;        /* 3×n host */
+} fmmb_request;
+typedef struct {
+  int32_t status;      /* the request's own status (FMMB_OK or an error code) */
+  int32_t p, precision, slot;
+  double queued_s;     /* submission → admission */
+  double run_s;        /* admission → results in host memory */
+  double latency_s;    /* submission → results in host memory */
+  int64_t bytes_estimate;
+} fmmb_request_info;
+int fmmb_server_create(int device, const fmmb_server_opts* opts, fmmb_server** out);
+int fmmb_server_submit(fmmb_server* server, const fmmb_request* request, int64_t* ticket);
+/* Wait for a request (timeout_s < 0: without limit; FMMB_ERR_TIMEOUT if it is not done in time,
+ * the ticket stays valid); returns the request's status. A ticket is waited for once. */
+int fmmb_server_wait(fmmb_server* server, int64_t ticket, double timeout_s, fmmb_request_info* info);
+/* Stops accepting requests, finishes the queued and running ones, then releases everything. */
+int fmmb_server_destroy(fmmb_server* server);
+
 #ifdef __cplusplus
 }
 #endif
