@@ -163,4 +163,52 @@ function evaluate(f::FMM, st::FMMState, targets::AbstractVector{SVector{3,Float6
     return out
 end
 
+# ---------------------------------------------------------------- the request server (no reference counterpart)
+struct ServerOpts; slots::Int32; ppl::Int32; hbm_budget::Int64; end
+struct Request
+    xyz::Ptr{Float64}; tau::Ptr{Float64}; n::Int64; tol::Float64; kernel::Int32; p::Int32
+    outputs::Int32; precision::Int32; pot::Ptr{Float64}; grad::Ptr{SVector{3,Float64}}
+end
+struct RequestInfo
+    status::Int32; p::Int32; precision::Int32; slot::Int32
+    queued_s::Float64; run_s::Float64; latency_s::Float64; bytes_estimate::Int64
+end
+
+"""A continuous-batching FMM request server on one GPU: `submit` queues a Laplace3D FMM at the
+sources (potential and gradient, self excluded) whose order and precision path follow `tol`;
+`wait` returns the results. Requests overlap on `slots` streams as device memory allows."""
+mutable struct Server
+    h::Ptr{Cvoid}
+    live::Dict{Int64,Any}
+    function Server(device::Integer=0; slots::Integer=4, ppl::Integer=64, hbm_budget::Integer=0)
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:fmmb_server_create, libfmmb), Cint, (Cint, Ref{ServerOpts}, Ref{Ptr{Cvoid}}),
+                    device, ServerOpts(slots, ppl, hbm_budget), r))
+        s = new(r[], Dict{Int64,Any}())
+        finalizer(x -> ccall((:fmmb_server_destroy, libfmmb), Cint, (Ptr{Cvoid},), x.h), s)
+        return s
+    end
+end
+
+function submit(s::Server, sources::AbstractVector{SVector{3,Float64}}, τ::AbstractVector{Float64}; tol::Real=1e-6)
+    length(τ) == length(sources) || throw(DimensionMismatch("one charge per source"))
+    x, t = collect(sources), collect(τ)
+    pot = Vector{Float64}(undef, length(x))
+    grad = Vector{SVector{3,Float64}}(undef, length(x))
+    req = Request(Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, x))), pointer(t), length(x), tol,
+                  1, 0, 3, -1, pointer(pot), pointer(grad))
+    ticket = Ref{Int64}(0)
+    check(ccall((:fmmb_server_submit, libfmmb), Cint, (Ptr{Cvoid}, Ref{Request}, Ref{Int64}), s.h, req, ticket))
+    s.live[ticket[]] = (x, t, pot, grad)      # rooted until the request is waited for
+    return ticket[]
+end
+
+function Base.wait(s::Server, ticket::Int64)
+    info = Ref{RequestInfo}()
+    rc = ccall((:fmmb_server_wait, libfmmb), Cint, (Ptr{Cvoid}, Int64, Float64, Ref{RequestInfo}), s.h, ticket, -1.0, info)
+    x, t, pot, grad = pop!(s.live, ticket)
+    check(rc)
+    return pot, grad, info[]
+end
+
 end # module
