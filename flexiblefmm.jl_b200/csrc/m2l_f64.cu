@@ -5,8 +5,9 @@
 //   gather  G = P_sᵀ M_src for the chunk's columns into shared memory ([column][entry], one
 //           coalesced load per lane and entry quartet, the D4h permutation computed from the
 //           offset's group element, partner entries by warp shuffles)
-//   product Y = A_class G, FP64 FMA, A streamed through shared memory in K-chunks of 16,
-//           each thread a RPT × CPT register tile
+//   product Y = A_class G on the FP64 tensor cores (mma.sync m8n8k4 f64, DMMA: there is no FP64
+//           tcgen05 kind), A streamed through shared memory in K-slabs of 16 with the next slab
+//           prefetched into registers; each warp an (LD/8 rows) × NB register tile
 //   scatter (P_t Y) summed over the consecutive pairs of each target, one update of the
 //           target's partial local per run (the block owns its targets: deterministic, no atomics)
 #include "d4h.cuh"
@@ -24,19 +25,29 @@ void upload_d4h(const HostOperators& h, cudaStream_t s) {
 
 namespace {
 
+// one FP64 tensor-core MMA, D(8×8) += A(8×4)·B(4×8): this lane holds A[g][t], B[t][g] and
+// D[g][2t], D[g][2t+1] (g = lane / 4, t = lane % 4)
+__device__ __forceinline__ void dmma(double* d, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 template <int LD, int NB>
 __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks, const int* __restrict__ cls_off,
                                                  const int2* __restrict__ pairs, const double* __restrict__ reps,
                                                  const double* __restrict__ m2l_scale, int NP, const double* __restrict__ M,
                                                  double* __restrict__ Pl) {
-  constexpr int BK = 16, RPT = LD / 16, CPT = NB / 16, GS = LD + 1;
+  // row tiles per warp, column tiles; strides ≡ 4 (mod 16) doubles keep the fragment loads free
+  // of shared-memory bank conflicts
+  constexpr int BK = 16, MT = LD / 64, NT = NB / 8, GS = LD + 4, LDA = LD + 4, AL = (BK * LD + 255) / 256;
   // entry quartets per lane (LD = 64: lanes ≥ 16 idle). A pair of entries never straddles a
   // multiple of 128 (entries 128, 256, 384 are real parts or m = 0), so the partner of a
   // lane's first and last entry is always in the neighbouring lane of the same quartet row.
   constexpr int Q = (LD + 127) / 128;
   extern __shared__ double sm[];
-  double* As = sm;                 // [BK][LD]
-  double* G = As + BK * LD;        // [NB][GS]: the gathered columns, then the product
+  double* As = sm;                 // [BK][LDA]
+  double* G = As + BK * LDA;       // [NB][GS]: the gathered columns, then the product
   int* ps = (int*)(G + NB * GS);
   int* pf = ps + NB;
   int* pt = pf + NB;
@@ -89,36 +100,53 @@ __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks
       }
       for (int j = nc + warp; j < NB; j += 8)
         for (int k = lane; k < LD; k += 32) G[j * GS + k] = 0.0;
-      double acc[RPT][CPT];
+      // product Y = A·G on the FP64 tensor cores: warp w the rows [w·LD/8, (w+1)·LD/8) (MT tiles of
+      // 8) × all NB columns (NT tiles of 8), K-steps of 4; A streamed through shared memory in
+      // slabs of BK rows of K, the next slab prefetched into registers
+      double acc[MT][NT][2];
 #pragma unroll
-      for (int r = 0; r < RPT; ++r)
+      for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
-        for (int cc = 0; cc < CPT; ++cc) acc[r][cc] = 0.0;
+        for (int nt = 0; nt < NT; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+      const int g = lane >> 2, t = lane & 3;
+      double ra[AL];
+      auto load_a = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < AL; ++u) {
+          const int e = tid + 256 * u, i = e % LD, k = e / LD;
+          ra[u] = (e < BK * LD && k0 + k < kmax) ? A[(int64_t)(k0 + k) * LD + i] : 0.0;
+        }
+      };
+      load_a(0);
       for (int k0 = 0; k0 < kmax; k0 += BK) {
         __syncthreads();
-        for (int e = tid; e < BK * LD; e += 256) {
-          const int i = e % LD, k = e / LD;
-          As[k * LD + i] = A[(int64_t)(k0 + k) * LD + i];
+#pragma unroll
+        for (int u = 0; u < AL; ++u) {
+          const int e = tid + 256 * u;
+          if (e < BK * LD) As[(e / LD) * LDA + e % LD] = ra[u];
         }
         __syncthreads();
-#pragma unroll 4
-        for (int k = 0; k < BK; ++k) {
-          double av[RPT], bv[CPT];
+        if (k0 + BK < kmax) load_a(k0 + BK);
 #pragma unroll
-          for (int r = 0; r < RPT; ++r) av[r] = As[k * LD + ty + 16 * r];
+        for (int ks = 0; ks < BK; ks += 4) {
+          double af[MT], bf[NT];
 #pragma unroll
-          for (int cc = 0; cc < CPT; ++cc) bv[cc] = G[(tx + 16 * cc) * GS + k0 + k];
+          for (int mt = 0; mt < MT; ++mt) af[mt] = As[(ks + t) * LDA + warp * (LD / 8) + 8 * mt + g];
 #pragma unroll
-          for (int r = 0; r < RPT; ++r)
+          for (int nt = 0; nt < NT; ++nt) bf[nt] = G[(8 * nt + g) * GS + k0 + ks + t];
 #pragma unroll
-            for (int cc = 0; cc < CPT; ++cc) acc[r][cc] = fma(av[r], bv[cc], acc[r][cc]);
+          for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) dmma(acc[mt][nt], af[mt], bf[nt]);
         }
       }
       __syncthreads();
 #pragma unroll
-      for (int r = 0; r < RPT; ++r)
+      for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
-        for (int cc = 0; cc < CPT; ++cc) G[(tx + 16 * cc) * GS + ty + 16 * r] = acc[r][cc];
+        for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) G[(8 * nt + 2 * t + i) * GS + warp * (LD / 8) + 8 * mt + g] = acc[mt][nt][i];
       __syncthreads();
       // scatter: thread j owns entry j of the targets' partial locals
       for (int j = tid; j < NP; j += 256) {
@@ -151,7 +179,7 @@ void launch(State& S) {
   Cache& C = *P.cache;
   const int nb = (int)P.h_blocks.size();
   if (nb == 0) return;
-  const size_t smem = sizeof(double) * (16 * LD + NB * (LD + 1)) + sizeof(int) * 3 * NB;
+  const size_t smem = sizeof(double) * (16 * (LD + 4) + NB * (LD + 4)) + sizeof(int) * 3 * NB;
   auto kern = k_m2l_f64<LD, NB>;
   FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<nb, 256, smem, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps.p, P.d_m2l_scale.p, C.np, S.M.p, S.Pl.p);
@@ -164,11 +192,11 @@ void m2l_f64(State& S) {
   switch (S.plan->cache->ld) {
     case 64: launch<64, 64>(S); break;
     case 128: launch<128, 64>(S); break;
-    case 192: launch<192, 32>(S); break;
-    case 256: launch<256, 32>(S); break;
-    case 320: launch<320, 16>(S); break;
-    case 384: launch<384, 16>(S); break;
-    case 448: launch<448, 16>(S); break;
+    case 192: launch<192, 64>(S); break;
+    case 256: launch<256, 64>(S); break;
+    case 320: launch<320, 48>(S); break;
+    case 384: launch<384, 40>(S); break;
+    case 448: launch<448, 32>(S); break;
     default: throw Error(FMMB_ERR_UNSUPPORTED, "no M2L kernel for this expansion length");
   }
 }
