@@ -136,24 +136,32 @@ struct ColMap {
   }
 };
 
+// one FP64 tensor-core MMA, D(8×8) += A(8×4)·B(4×8): this lane holds A[g][t], B[t][g] and
+// D[g][2t], D[g][2t+1] (g = lane / 4, t = lane % 4)
+__device__ __forceinline__ void dmma_gemm(double* d, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 // C(:, g) (=|+=) A · B(:, g) for mapped columns g; A column-major M × K (M a multiple of 128);
-// rows r with r mod LD ≥ NP written as 0. 128 × BN tiles, K-steps of 32 with the next step's
-// tiles prefetched into registers; each thread an RM × CN register tile.
+// rows r with r mod LD ≥ NP written as 0. 128 × BN tiles on the FP64 tensor cores (DMMA): warp w
+// the rows [16w, 16w + 16) × all BN columns; K-slabs of 32 in shared memory (row strides of 4 mod
+// 16 doubles: conflict-free fragment loads), the next slab prefetched into registers.
 template <int BN>
 __global__ void __launch_bounds__(256) k_gemm_tiles(int M, int K, const double* __restrict__ A, ColMap bm, ColMap cm,
                                                     int ncols, int LD, int NP, int accumulate) {
-  constexpr int BM = 128, BK = 32;
-  constexpr int CN = BN >= 16 ? 2 : 1, TC = BN / CN, TR = 256 / TC, RM = BM / TR;
+  constexpr int BM = 128, BK = 32, NT = BN / 8, LDA = BM + 4, LDB = BN + 4;
   constexpr int AL = BM * BK / 256, BL = (BK * BN + 255) / 256;
-  __shared__ double As[BK][BM];
-  __shared__ double Bs[BK][BN + 1];
-  const int tid = threadIdx.x, tx = tid % TC, ty = tid / TC;
+  __shared__ double As[BK * LDA];
+  __shared__ double Bs[BK * LDB];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
-  double acc[RM][CN];
+  double acc[2][NT][2];
 #pragma unroll
-  for (int r = 0; r < RM; ++r)
+  for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-    for (int c = 0; c < CN; ++c) acc[r][c] = 0.0;
+    for (int nt = 0; nt < NT; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
   double ra[AL], rb[BL];
   const double* bcol[BL];
 #pragma unroll
@@ -177,37 +185,39 @@ __global__ void __launch_bounds__(256) k_gemm_tiles(int M, int K, const double* 
   for (int k0 = 0; k0 < K; k0 += BK) {
     __syncthreads();
 #pragma unroll
-    for (int u = 0; u < AL; ++u) { const int e = tid + 256 * u; As[e / BM][e % BM] = ra[u]; }
+    for (int u = 0; u < AL; ++u) { const int e = tid + 256 * u; As[(e / BM) * LDA + e % BM] = ra[u]; }
 #pragma unroll
-    for (int u = 0; u < BL; ++u) { const int e = tid + 256 * u; if (e < BK * BN) Bs[e % BK][e / BK] = rb[u]; }
+    for (int u = 0; u < BL; ++u) { const int e = tid + 256 * u; if (e < BK * BN) Bs[(e % BK) * LDB + e / BK] = rb[u]; }
     __syncthreads();
     if (k0 + BK < K) load(k0 + BK);
-#pragma unroll 8
-    for (int k = 0; k < BK; ++k) {
-      double a[RM], b[CN];
 #pragma unroll
-      for (int r = 0; r < RM; ++r) a[r] = As[k][ty + TR * r];
+    for (int ks = 0; ks < BK; ks += 4) {
+      double af[2], bf[NT];
 #pragma unroll
-      for (int c = 0; c < CN; ++c) b[c] = Bs[k][tx + TC * c];
+      for (int mt = 0; mt < 2; ++mt) af[mt] = As[(ks + t) * LDA + 16 * warp + 8 * mt + g];
 #pragma unroll
-      for (int r = 0; r < RM; ++r)
+      for (int nt = 0; nt < NT; ++nt) bf[nt] = Bs[(ks + t) * LDB + 8 * nt + g];
 #pragma unroll
-        for (int c = 0; c < CN; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) dmma_gemm(acc[mt][nt], af[mt], bf[nt]);
     }
   }
 #pragma unroll
-  for (int c = 0; c < CN; ++c) {
-    const int g = col0 + tx + TC * c;
-    if (g >= ncols) continue;
-    double* C = cm.col(g, LD);
+  for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-    for (int r = 0; r < RM; ++r) {
-      const int row = row0 + ty + TR * r;
-      if (row >= M) continue;
-      const double v = (row % LD) < NP ? acc[r][c] : 0.0;
-      C[row] = accumulate ? C[row] + v : v;
+    for (int i = 0; i < 2; ++i) {
+      const int gc = col0 + 8 * nt + 2 * t + i;
+      if (gc >= ncols) continue;
+      double* C = cm.col(gc, LD);
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        const int row = row0 + 16 * warp + 8 * mt + g;
+        if (row >= M) continue;
+        const double v = (row % LD) < NP ? acc[mt][nt][i] : 0.0;
+        C[row] = accumulate ? C[row] + v : v;
+      }
     }
-  }
 }
 
 // the column-tile width: enough tiles to cover the SMs
