@@ -238,12 +238,14 @@ struct TcCfg {
   static constexpr int STAGES = MT == 1 ? 4 : 3;
   // warp roles (a warp reads the tensor-memory lane quadrant warp % 4): read-back warps 0-7 for the
   // first tile (two per quadrant), for a second tile (p = 11) warps 8 and 12 (its rows lie in
-  // quadrant 0); one gather warp per stage from GB; the issuing warp IW
+  // quadrant 0); the issuing warp IW = 16; the other warps gather, GPS per stage
   static constexpr int NEPI = 8 + 2 * (MT - 1);            // read-back warps
-  static constexpr int GB = MT == 1 ? 8 : 9;
-  static constexpr int IW = MT == 1 ? 12 : 13;
+  static constexpr int GPS = 2;                            // gather warps per stage
+  static constexpr int IW = 16;
   static constexpr int THREADS = 32 * (IW + 1);
-  static_assert(GB + STAGES <= (MT == 1 ? IW : 12), "warp roles");
+  static_assert(NEPI + STAGES * GPS + 1 == IW + 1, "warp roles");
+  // the gather index of warp w (not a read-back or the issuing warp)
+  __device__ static int gather_index(int w) { return MT == 1 ? w - 8 : (w < 12 ? w - 9 : w - 10); }
   static constexpr int B_OFF = (A_BYTES + 1023) / 1024 * 1024;
   static constexpr int PI_OFF = B_OFF + STAGES * STAGE_BYTES;
   static constexpr int SGN_OFF = PI_OFF + STAGES * (int)sizeof(PairInfo);
@@ -272,7 +274,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   int* s_d4h = (int*)(sm + G::D4H_OFF);
   uint64_t* bars = (uint64_t*)(sm + G::BAR_OFF);
   uint64_t* bar_a = bars;                                         // operator load
-  uint64_t* full = bars + 1;                                      // [STAGES] gathered (32 arrivals)
+  uint64_t* full = bars + 1;                                      // [STAGES] gathered (32·GPS arrivals)
   uint64_t* done = bars + 1 + G::STAGES;                          // [STAGES] MMAs complete (commit)
   uint64_t* tempty = bars + 1 + 2 * G::STAGES;                    // [STAGES] read back (NEPI·32 arrivals)
   uint32_t* tmem_slot = (uint32_t*)(bars + 1 + 3 * G::STAGES);
@@ -286,7 +288,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   if (tid == 0) {
     mbar_init(bar_a, 1);
     for (int s = 0; s < G::STAGES; ++s) {
-      mbar_init(&full[s], 32);
+      mbar_init(&full[s], 32 * G::GPS);
       mbar_init(&done[s], 1);
       mbar_init(&tempty[s], 32 * G::NEPI);
     }
@@ -393,18 +395,19 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         mbar_arrive(&tempty[s]);
       }
     }
-  } else if (warp >= G::GB && warp < G::GB + G::STAGES) {
-    // ---------------- gather: warp gw builds the chunks i ≡ gw (mod STAGES), always in stage gw;
-    // lane octet o = lane & 7 the pairs of a group of 8, cq = lane >> 3 the core column
-    const int gw = warp - G::GB, o = lane & 7, cq = lane >> 3;
-    const int s = gw;
+  } else if (warp != G::IW) {
+    // ---------------- gather: the GPS warps of stage s build the chunks i ≡ s (mod STAGES), warp h
+    // of them every GPS-th pair of groups; lane octet o = lane & 7 the pairs of a group of 8,
+    // cq = lane >> 3 the core column
+    const int gw = G::gather_index(warp), o = lane & 7, cq = lane >> 3;
+    const int s = gw / G::GPS, h = gw % G::GPS;
     unsigned char* bh = sB + s * G::STAGE_BYTES;
     PairInfo& pi = pinfo[s];
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
       const int a0 = co[c], a1 = co[c + 1];
       for (int q0 = a0; q0 < a1; q0 += NCHK, ++i) {
-        if (i % G::STAGES != gw) continue;
+        if (i % G::STAGES != s) continue;
         if (i >= G::STAGES) {
           const bool w = mbar_wait_abortable(&tempty[s], (uint32_t)(i / G::STAGES - 1) & 1, abort_flag);
           if (!__all_sync(0xffffffffu, w)) { ok = false; break; }   // the warp leaves together (shuffles below)
@@ -418,18 +421,16 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
           srcA = pr.x;
           facA = s_d4h[pr.y >> 8];
           tA = pr.y & 0xff;
-          pi.fac[2 * lane] = facA;
-          pi.tgt[2 * lane] = tA;
         }
         if (vB) {
           const int2 pr = pairs[b.w + q0 + 2 * lane + 1];
           srcB = pr.x;
           facB = s_d4h[pr.y >> 8];
           tB = pr.y & 0xff;
-          pi.fac[2 * lane + 1] = facB;
-          pi.tgt[2 * lane + 1] = tB;
         }
-        {
+        if (h == 0) {                                   // the first warp of the stage records the chunk
+          if (vA) { pi.fac[2 * lane] = facA; pi.tgt[2 * lane] = tA; }
+          if (vB) { pi.fac[2 * lane + 1] = facB; pi.tgt[2 * lane + 1] = tB; }
           // the target runs of the chunk (pairs are sorted by target within a class)
           const int tprev = __shfl_up_sync(0xffffffffu, tB, 1);
           const bool stA = vA && (lane == 0 || tA != tprev), stB = vB && tB != tA;
@@ -455,7 +456,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
           }
         }
         const float csA = srcA >= 0 ? Msc[srcA] : 0.f, csB = srcB >= 0 ? Msc[srcB] : 0.f;
-        for (int g0 = 0; g0 < ng; g0 += 2) {
+        for (int g0 = 2 * h; g0 < ng; g0 += 2 * G::GPS) {
           uint4 vh[2][G::U], vl[2][G::U];
           int facg[2];
 #pragma unroll
@@ -491,15 +492,17 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
             }
           }
         }
-        if (2 * lane < nc) pi.cs[2 * lane] = csA;
-        if (2 * lane + 1 < nc) pi.cs[2 * lane + 1] = csB;
-        if (lane == 0) pi.n = nc;
+        if (h == 0) {
+          if (2 * lane < nc) pi.cs[2 * lane] = csA;
+          if (2 * lane + 1 < nc) pi.cs[2 * lane + 1] = csB;
+          if (lane == 0) pi.n = nc;
+        }
         fence_async_smem();
         __syncwarp();
         mbar_arrive(&full[s]);
       }
     }
-  } else if (warp == G::IW && lane == 0) {
+  } else if (lane == 0) {
     // ---------------- issue: the class operator when the class changes, then the chunk's MMAs
     int i = 0, ncls = 0;
     bool a_pending = false;
