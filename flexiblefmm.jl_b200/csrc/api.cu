@@ -272,7 +272,8 @@ int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* m, fmmb_cache** out
   return guard([&] {
     require(ctx && m && out, FMMB_ERR_ARGUMENT, "null argument");
     require(m->method == FMMB_METHOD_SPHERICAL_HARMONICS, FMMB_ERR_UNSUPPORTED, "only SphericalHarmonics is provided");
-    require(m->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "only Laplace3D is provided");
+    require(m->kernel == FMMB_KERNEL_LAPLACE3D || m->kernel == FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED,
+            "the kernels provided are Laplace3D and Stokeslet3D");
     require(m->p >= 1, FMMB_ERR_ARGUMENT, "p must be at least 1");
     require(m->p <= PMAX, FMMB_ERR_UNSUPPORTED, "p above 20 is not provided");
     require(m->tol >= 0 && m->tol < 1, FMMB_ERR_ARGUMENT, "tol must lie in [0, 1)");
@@ -283,6 +284,8 @@ int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* m, fmmb_cache** out
     h->c.p = m->p;
     h->c.np = (m->p + 1) * (m->p + 1);
     h->c.ld = ld_of(m->p);
+    h->c.kernel = m->kernel;
+    h->c.nexp = m->kernel == FMMB_KERNEL_STOKESLET3D ? 4 : 1;   // StokesHarmonics: Φ₁..₃, Ψ̂
     std::lock_guard<std::mutex> lk(g_handles);
     ++ctx->deps;
     *out = h.release();
@@ -416,6 +419,8 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
     require(plan && out, FMMB_ERR_ARGUMENT, "null argument");
     require(precision == FMMB_PRECISION_FP64 || precision == FMMB_PRECISION_MIXED, FMMB_ERR_ARGUMENT, "unknown precision path");
     Plan& P = plan->p;
+    require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D || precision == FMMB_PRECISION_FP64, FMMB_ERR_UNSUPPORTED,
+            "the Stokeslet method runs on the FP64 path");
     set_device(*P.ctx);
     cudaStream_t s = P.ctx->stream;
     std::unique_ptr<fmmb_state> h(new fmmb_state());
@@ -423,7 +428,7 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
     S.plan = &P;
     S.precision = precision;
     S.xs.alloc(P.N); S.ys.alloc(P.N); S.zs.alloc(P.N); S.q.alloc(P.N);
-    size_t ne = (size_t)P.nnodes * P.cache->ld;
+    size_t ne = (size_t)P.nnodes * P.cache->ld * P.cache->nexp;
     S.M.alloc(ne);
     S.Pl.alloc(ne);
     FMMB_CUDA(cudaMemsetAsync(S.M.p, 0, S.M.bytes(), s));
@@ -647,19 +652,61 @@ int fmmb_state_expansions(const fmmb_state* state, double* multipoles, double* l
     const State& S = state->s;
     const Plan& P = *S.plan;
     set_device(*P.ctx);
-    int LD = P.cache->ld, NP = P.cache->np, n = P.nnodes;
+    // per node the nexp blocks of NP coefficients (Stokeslet states: Φ₁, Φ₂, Φ₃, Ψ̂)
+    const int LD = P.cache->ld, NP = P.cache->np, n = P.nnodes, ne = P.cache->nexp;
     cudaStream_t s = P.ctx->stream;
     if (multipoles) {
-      std::vector<double> h = to_host(S.M.p, (size_t)n * LD, s);
-      for (int i = 0; i < n; ++i) std::memcpy(multipoles + (size_t)i * NP, &h[(size_t)i * LD], sizeof(double) * NP);
+      std::vector<double> h = to_host(S.M.p, (size_t)n * ne * LD, s);
+      for (int i = 0; i < n; ++i)
+        for (int a = 0; a < ne; ++a)
+          std::memcpy(multipoles + ((size_t)i * ne + a) * NP, &h[((size_t)i * ne + a) * LD], sizeof(double) * NP);
     }
     if (locals) {
-      std::vector<double> h = to_host(S.Pl.p, (size_t)n * LD, s);
-      for (int i = 0; i < n; ++i) {
-        if (P.h_flags[i] & F_LEAF) std::memcpy(locals + (size_t)i * NP, &h[(size_t)i * LD], sizeof(double) * NP);
-        else std::memset(locals + (size_t)i * NP, 0, sizeof(double) * NP);
-      }
+      std::vector<double> h = to_host(S.Pl.p, (size_t)n * ne * LD, s);
+      for (int i = 0; i < n; ++i)
+        for (int a = 0; a < ne; ++a) {
+          double* dst = locals + ((size_t)i * ne + a) * NP;
+          if (P.h_flags[i] & F_LEAF) std::memcpy(dst, &h[((size_t)i * ne + a) * LD], sizeof(double) * NP);
+          else std::memset(dst, 0, sizeof(double) * NP);
+        }
     }
+  });
+}
+
+// stokes_fmm_eval!(velocities, plan; stokeslets) at the sources (src/stokes_api.jl:131-150):
+// build_expansions! then evaluate_at_sources!, self excluded
+int fmmb_stokes_eval_dev(fmmb_state* state, const double* xyz, const double* stokeslets, int64_t n, double* velocity) {
+  return guard([&] {
+    require(state && xyz && stokeslets && velocity, FMMB_ERR_ARGUMENT, "null argument");
+    State& S = state->s;
+    Plan& P = *S.plan;
+    require(P.cache->kernel == FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED, "the state is not a Stokeslet state");
+    require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and Stokeslets");
+    set_device(*P.ctx);
+    require_device_ptr(*P.ctx, xyz, "sources");
+    require_device_ptr(*P.ctx, stokeslets, "stokeslets");
+    require_device_ptr(*P.ctx, velocity, "velocities");
+    stokes_build(S, xyz, stokeslets);
+    stokes_evaluate_sources(S, velocity);
+  });
+}
+
+int fmmb_stokes_eval(fmmb_state* state, const double* xyz, const double* stokeslets, int64_t n, double* velocity) {
+  return guard([&] {
+    require(state && xyz && stokeslets && velocity, FMMB_ERR_ARGUMENT, "null argument");
+    State& S = state->s;
+    Plan& P = *S.plan;
+    require(P.cache->kernel == FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED, "the state is not a Stokeslet state");
+    require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and Stokeslets");
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    DBuf<double> x(3 * n), f(3 * n), v(3 * n);
+    FMMB_CUDA(cudaMemcpyAsync(x.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    FMMB_CUDA(cudaMemcpyAsync(f.p, stokeslets, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    stokes_build(S, x.p, f.p);
+    stokes_evaluate_sources(S, v.p);
+    FMMB_CUDA(cudaMemcpyAsync(velocity, v.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
   });
 }
 

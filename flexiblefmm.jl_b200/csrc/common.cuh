@@ -135,6 +135,7 @@ struct HostOperators {
   std::vector<int8_t> gsgn;   // 316 × LD
   std::vector<int16_t> sidx;  // 316 × LD: scatter source row (P_t applied as a gather)
   std::vector<int8_t> ssgn;   // 316 × LD
+  std::vector<int8_t> faroff; // 316 × 3: the far offsets (source cell − target cell), table order
   std::vector<uint8_t> d4h;   // 316: the D4h element mapping the class representative to the
                               // offset, as rotation k (bits 0-1) | εy << 2 | εz << 3
   std::vector<double> tables; // a, b, cz, cm, cp (each ntri) then e (p): the recurrences

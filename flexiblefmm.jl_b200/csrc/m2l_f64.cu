@@ -16,11 +16,15 @@
 namespace fmmb {
 
 __constant__ int c_d4h[NFAR];
+__constant__ int c_faroff[NFAR * 3];   // the far offsets, source cell − target cell
 
 void upload_d4h(const HostOperators& h, cudaStream_t s) {
   std::vector<int> fac(h.d4h.begin(), h.d4h.end());
   require(fac.size() == NFAR, FMMB_ERR_DEVICE, "the D4h factor table has the wrong size");
   FMMB_CUDA(cudaMemcpyToSymbolAsync(c_d4h, fac.data(), sizeof(int) * NFAR, 0, cudaMemcpyHostToDevice, s));
+  std::vector<int> off(h.faroff.begin(), h.faroff.end());
+  require(off.size() == 3 * NFAR, FMMB_ERR_DEVICE, "the far offset table has the wrong size");
+  FMMB_CUDA(cudaMemcpyToSymbolAsync(c_faroff, off.data(), sizeof(int) * 3 * NFAR, 0, cudaMemcpyHostToDevice, s));
 }
 
 namespace {
@@ -37,7 +41,7 @@ template <int LD, int NB>
 __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks, const int* __restrict__ cls_off,
                                                  const int2* __restrict__ pairs, const double* __restrict__ reps,
                                                  const double* __restrict__ m2l_scale, int NP, const double* __restrict__ M,
-                                                 double* __restrict__ Pl) {
+                                                 double* __restrict__ Pl, int64_t pitch, int comp, int psi) {
   // row tiles per warp, column tiles; strides ≡ 4 (mod 16) doubles keep the fragment loads free
   // of shared-memory bank conflicts
   constexpr int BK = 16, MT = LD / 64, NT = NB / 8, GS = LD + 4, LDA = LD + 4, AL = (BK * LD + 255) / 256;
@@ -72,7 +76,12 @@ __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks
       // gather: warp w the columns w, w + 8, ...; lane l the entries 4(l + 32 r) .. + 3
       for (int j = warp; j < nc; j += 8) {
         const int fac = c_d4h[pf[j]];
-        const double* src = M + (int64_t)ps[j] * LD;
+        const double* src = M + (int64_t)ps[j] * pitch + (int64_t)comp * LD;
+        // the Stokes Ψ̂ block: its source is Ψ̂ + o·Φ of the source box, o the far offset
+        // (harmonics_stokes.jl: M2L Ψ̂_B = Ψ̂_A + o·Φ, linear in the source)
+        double o3[3] = {0.0, 0.0, 0.0};
+        if (psi)
+          for (int d = 0; d < 3; ++d) o3[d] = (double)c_faroff[3 * pf[j] + d];
 #pragma unroll
         for (int r = 0; r < Q; ++r) {
           const int k0 = 4 * (lane + 32 * r);
@@ -81,6 +90,15 @@ __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks
             const double2 u = __ldg(reinterpret_cast<const double2*>(src + k0));
             const double2 w = __ldg(reinterpret_cast<const double2*>(src + k0 + 2));
             a[0] = u.x; a[1] = u.y; a[2] = w.x; a[3] = w.y;
+            if (psi) {
+              const double* base = M + (int64_t)ps[j] * pitch;
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                const double2 u2 = __ldg(reinterpret_cast<const double2*>(base + (int64_t)d * LD + k0));
+                const double2 w2 = __ldg(reinterpret_cast<const double2*>(base + (int64_t)d * LD + k0 + 2));
+                a[0] += o3[d] * u2.x; a[1] += o3[d] * u2.y; a[2] += o3[d] * w2.x; a[3] += o3[d] * w2.y;
+              }
+            }
           } else { a[0] = a[1] = a[2] = a[3] = 0.0; }
           const double nxt = __shfl_down_sync(0xffffffffu, a[0], 1);
           const double prv = __shfl_up_sync(0xffffffffu, a[3], 1);
@@ -158,7 +176,7 @@ __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks
         for (int qq = 0; qq < nc; ++qq) {
           const int t = pt[qq], fac = c_d4h[pf[qq]];
           if (t != cur) {
-            if (cur >= 0) Pl[(int64_t)(b.y + cur) * LD + j] += alpha * run;
+            if (cur >= 0) Pl[(int64_t)(b.y + cur) * pitch + (int64_t)comp * LD + j] += alpha * run;
             cur = t;
             run = 0.0;
           }
@@ -167,12 +185,14 @@ __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks
           const double y = G[qq * GS + (sw ? partner : j)];
           run += perm_sign(sw ? 3 - part : part, q, n + m, fac) < 0 ? -y : y;
         }
-        if (cur >= 0) Pl[(int64_t)(b.y + cur) * LD + j] += alpha * run;
+        if (cur >= 0) Pl[(int64_t)(b.y + cur) * pitch + (int64_t)comp * LD + j] += alpha * run;
       }
     }
   }
 }
 
+// one launch per scalar block of the method (1 for Laplace3D; 4 for the Stokeslet: Φ₁..₃ and Ψ̂,
+// the last with the coupling), the blocks nexp·LD apart per node
 template <int LD, int NB>
 void launch(State& S) {
   Plan& P = *S.plan;
@@ -182,8 +202,12 @@ void launch(State& S) {
   const size_t smem = sizeof(double) * (16 * (LD + 4) + NB * (LD + 4)) + sizeof(int) * 3 * NB;
   auto kern = k_m2l_f64<LD, NB>;
   FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<nb, 256, smem, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps.p, P.d_m2l_scale.p, C.np, S.M.p, S.Pl.p);
-  FMMB_LAUNCH_CHECK();
+  const int nexp = C.nexp;
+  for (int comp = 0; comp < nexp; ++comp) {
+    kern<<<nb, 256, smem, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps.p, P.d_m2l_scale.p, C.np, S.M.p, S.Pl.p,
+                                           (int64_t)nexp * LD, comp, nexp == 4 && comp == 3);
+    FMMB_LAUNCH_CHECK();
+  }
 }
 
 }  // namespace

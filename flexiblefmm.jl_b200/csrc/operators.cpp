@@ -192,6 +192,7 @@ HostOperators build_operators(int p, double ref_width) {
   op.ssgn.assign((size_t)NFAR * LD, 0);
   for (int f = 0; f < NFAR; ++f) {
     const auto& o = offs[f];
+    for (int d = 0; d < 3; ++d) op.faroff.push_back((int8_t)o[d]);
     int a = std::abs(o[0]), b = std::abs(o[1]);
     std::array<int, 3> r{std::max(a, b), std::min(a, b), std::abs(o[2])};
     int c = (int)(std::find(reps.begin(), reps.end(), r) - reps.begin());

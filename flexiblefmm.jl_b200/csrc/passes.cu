@@ -71,7 +71,7 @@ template <int P>
 __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restrict__ cell, const int* __restrict__ plo,
                       const int* __restrict__ phi, const double* __restrict__ xs, const double* __restrict__ ys,
                       const double* __restrict__ zs, const double* __restrict__ q, Geometry geo,
-                      const double* __restrict__ scale, int LD, double* __restrict__ M) {
+                      const double* __restrict__ scale, int64_t pitch, double* __restrict__ M) {
   // the recurrence tables in shared memory: the lanes of a warp run different orders and would
   // serialise on the constant cache
   __shared__ double s_ab[2 * TRI_MAX];
@@ -117,7 +117,7 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
       }
     }
   }
-  double* col = M + (int64_t)node * LD;
+  double* col = M + (int64_t)node * pitch;
 #pragma unroll
   for (int n = 0; n <= P; ++n) {
     if (n < m) continue;
@@ -127,14 +127,6 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
 }
 
 // ---------------------------------------------------------------- GEMM over mapped columns (M2M, L2L)
-struct ColMap {
-  double* base;
-  const int* idx;  // column g at base + (idx ? idx[g] : off + stride·g)·LD
-  int off, stride;
-  __device__ __forceinline__ double* col(int g, int LD) const {
-    return base + (int64_t)(idx ? idx[g] : off + stride * g) * LD;
-  }
-};
 
 // one FP64 tensor-core MMA, D(8×8) += A(8×4)·B(4×8): this lane holds A[g][t], B[t][g] and
 // D[g][2t], D[g][2t+1] (g = lane / 4, t = lane % 4)
@@ -357,12 +349,12 @@ __global__ void k_direct_reduce(const double* __restrict__ part, int64_t nt, int
 }
 
 template <int P>
-void launch_p2m(State& S) {
+void launch_p2m(State& S, const double* q, double* M, int64_t pitch) {
   Plan& P_ = *S.plan;
   int nth = P_.n_s2m * (P + 1);
   if (nth == 0) return;
   k_p2m<P><<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p, S.ys.p,
-                                                     S.zs.p, S.q.p, geometry(P_), P_.d_scale.p, P_.cache->ld, S.M.p);
+                                                     S.zs.p, q, geometry(P_), P_.d_scale.p, pitch, M);
   FMMB_LAUNCH_CHECK();
 }
 
@@ -396,14 +388,29 @@ void upload_operators(Cache& C) {
 
 void gather_inputs(State& S, const double* xyz_dev, const double* tau_dev) {
   Plan& P = *S.plan;
+  require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
   k_gather_inputs<<<nblk(P.N), 256, 0, P.ctx->stream>>>(xyz_dev, tau_dev, P.perm.p, P.N, S.xs.p, S.ys.p, S.zs.p, S.q.p);
   FMMB_LAUNCH_CHECK();
 }
 
 
+void p2m_block(State& S, const double* q, double* M, int64_t pitch) {
+  switch (S.plan->cache->p) {
+#define X(pp) case pp: launch_p2m<pp>(S, q, M, pitch); break;
+    FMMB_P_CASES(X)
+#undef X
+    default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
+  }
+}
+
+void gemm_columns(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols, int LD, int NP, int accumulate,
+                  int num_sms, cudaStream_t s) {
+  gemm_cols(M, K, A, bm, cm, ncols, LD, NP, accumulate, num_sms, s);
+}
+
 int p2m(State& S) {
   switch (S.plan->cache->p) {
-#define X(p) case p: launch_p2m<p>(S); break;
+#define X(pp) case pp: launch_p2m<pp>(S, S.q.p, S.M.p, (int64_t)S.plan->cache->ld); break;
     FMMB_P_CASES(X)
 #undef X
     default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
@@ -469,12 +476,14 @@ void downward_pass(State& S) {
 
 void evaluate_sources(State& S, int outputs, double* pot, double* grad) {
   Plan& P = *S.plan;
+  require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
   evaluate_groups(S, P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, S.xs.p, S.ys.p, S.zs.p, P.perm.p, true, outputs,
                   pot, grad);
 }
 
 void evaluate_targets(State& S, const double* tg, int64_t nt, int outputs, double* pot, double* grad) {
   Plan& P = *S.plan;
+  require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
   cudaStream_t s = P.ctx->stream;
   if (nt == 0) return;
   require(nt < (1ll << 31) - 1, FMMB_ERR_ARGUMENT, "too many targets");

@@ -91,6 +91,23 @@ __device__ __forceinline__ void l2p(const R* __restrict__ L, R x, R y, R z, R& u
 // the orders with compiled kernels
 #define FMMB_P_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20)
 
+// a column of a GEMM over mapped columns (M2M, L2L): column g at base + (idx ? idx[g] : off +
+// stride·g)·pitch (pitch 0: the expansion length LD)
+struct ColMap {
+  double* base;
+  const int* idx;
+  int off, stride;
+  int64_t pitch = 0;
+  __device__ __forceinline__ double* col(int g, int LD) const {
+    return base + (int64_t)(idx ? idx[g] : off + stride * g) * (pitch ? pitch : (int64_t)LD);
+  }
+};
+// C(:, g) (=|+=) A · B(:, g) on the FP64 tensor cores; rows r with r mod LD ≥ NP written as 0
+void gemm_columns(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols, int LD, int NP, int accumulate,
+                  int num_sms, cudaStream_t s);
+// P2M of the childless sourced nodes with charges q (tree order) into the block at M (node pitch)
+void p2m_block(State& S, const double* q, double* M, int64_t pitch);
+
 void m2l_f64(State& S);
 int p2m(State& S);          // the stages of the passes; each returns its kernel launches
 int m2m_sweep(State& S);

@@ -19,6 +19,8 @@ struct Ctx {
 struct Cache {
   Ctx* ctx = nullptr;
   int p = 0, np = 0, ld = 0;
+  int kernel = FMMB_KERNEL_LAPLACE3D;
+  int nexp = 1;              // scalar expansions per node: 1 (Laplace3D), 4 (Stokeslet3D: Φ₁..₃, Ψ̂)
   double W0 = NAN;           // base width, fixed by the first fitted box
   std::mutex mu;             // the cache is shared by plans; fitting and uploads are locked
   bool uploaded = false;
@@ -83,6 +85,7 @@ struct State {
   Plan* plan = nullptr;
   int precision = FMMB_PRECISION_FP64;
   DBuf<double> xs, ys, zs, q;             // sources and charges in tree order
+  DBuf<double> f3;                        // Stokeslet states: the forces in tree order (fx, fy, fz)
   DBuf<double> M, Pl;                     // nnodes × LD: multipoles, partial locals
   DBuf<uint16_t> Mh, Ml;                  // the mixed path: the multipoles scaled by a power of two
   DBuf<float> Msc;                        //   per node, as FP16 head and tail; the inverse scales
@@ -110,6 +113,9 @@ void evaluate_targets(State& S, const double* tg_dev, int64_t nt, int outputs, d
 void bounds(Ctx& ctx, const double* xyz_dev, int64_t n, double lo[3], double hi[3], int64_t* nonfinite);
 void direct(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
             int64_t nt, double* pot, double* grad);
+// stokes.cu: StokesHarmonics(Stokeslet3D()) on the FP64 path
+void stokes_build(State& S, const double* xyz_dev, const double* f_dev);
+void stokes_evaluate_sources(State& S, double* vel_dev);
 // direct_noalloc.cu: the same sums with the partials in a fixed array compiled into the library
 void direct_noalloc(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
                     int64_t nt, double* pot, double* grad);

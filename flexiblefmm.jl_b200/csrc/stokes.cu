@@ -1,0 +1,303 @@
+// StokesHarmonics(Stokeslet3D(); p) on the plain FP64 path (src/operators/harmonics_stokes.jl):
+// the Stokeslet through four Laplace potentials, Φ_k = Σ f_k/(4πr) and Ψ_c = Σ (y − c)·f/(4πr),
+// u = ½[Φ − (x − c)·∇Φ + ∇Ψ_c]. Every node holds the four scalar expansions [Φ₁; Φ₂; Φ₃; Ψ̂]
+// (Ψ̂ = Ψ_c/w in the box's own coordinates), nexp·LD apart; they use the scalar operators of
+// SphericalHarmonics with the couplings of the reference:
+//   P2M  block k: charges f_k; block 4: charges ŷ·f (ŷ = (y − c)/w)        (harmonics_stokes.jl:322-328)
+//   M2M  Ψ̂_P = ½ Ψ̂_C + δ̂·Φ_C folded into the stacked children before the product (:136-158)
+//   M2L  Ψ̂_B += T(Ψ̂_A + o·Φ_A), o the far offset (linear in the source: the gather of the fourth
+//        launch of the class-wise M2L forms it, m2l_f64.cu)                 (:77-97)
+//   L2L  children blocks 1–3 = L2L·P_a; block 4 = 2·L2L·P₄ − 2 δ̂·(L2L·P_Φ) (:159-183)
+//   L2P  u = ½[Φ − x̂·∇̂Φ + ∇̂Ψ̂] from the values and scaled gradients of the four blocks (:283-287)
+//   near c(f/r + d(d·f)/r³), c = 1/(8π), self excluded by index (src/kernels.jl:253-272)
+#include "passes.cuh"
+
+namespace fmmb {
+namespace {
+
+constexpr double KSTOKES = 0.039788735772973833942;   // 1/(8π)
+constexpr int SW = 4;                                  // warps per block of the evaluation kernels
+
+inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+// δ̂ of child slot j along d: (c_child − c_parent)/w_parent ∈ {±1/4} (bit d of j = coordinate d)
+__device__ __forceinline__ double dhat(int j, int d) { return (((j >> d) & 1) ? 0.25 : -0.25); }
+
+// points and forces in tree order (perm: sorted position → original index)
+__global__ void k_stokes_gather(const double* __restrict__ xyz, const double* __restrict__ f, const int* __restrict__ perm,
+                                int64_t n, double* __restrict__ xs, double* __restrict__ ys, double* __restrict__ zs,
+                                double* __restrict__ f3) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t j = perm[i];
+  xs[i] = xyz[3 * j];
+  ys[i] = xyz[3 * j + 1];
+  zs[i] = xyz[3 * j + 2];
+  f3[i] = f[3 * j];
+  f3[n + i] = f[3 * j + 1];
+  f3[2 * n + i] = f[3 * j + 2];
+}
+
+// the fourth P2M block's charges ŷ·f, ŷ = (y − c)·s relative to the centre c of the node whose
+// multipole the point enters, s = 1/w
+__global__ void k_stokes_q4(const int* __restrict__ nodes, int nn, const int4* __restrict__ cell,
+                            const int* __restrict__ plo, const int* __restrict__ phi, Geometry geo,
+                            const double* __restrict__ scale, int64_t n, const double* __restrict__ xs,
+                            const double* __restrict__ ys, const double* __restrict__ zs, const double* __restrict__ f3,
+                            double* __restrict__ q4) {
+  // one warp per childless node with sources (the nodes P2M runs on, ghost children of a leaf
+  // included): Ψ̂ is centred on the node whose multipole it starts
+  const int wid = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (wid >= nn) return;
+  const int node = nodes[wid];
+  const int4 c = cell[node];
+  const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
+  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  for (int i = plo[node] + lane; i <= phi[node]; i += 32) {
+    const double x = (xs[i] - cx) * s, y = (ys[i] - cy) * s, z = (zs[i] - cz) * s;
+    q4[i] = x * f3[i] + y * f3[n + i] + z * f3[2 * n + i];
+  }
+}
+
+// M2M input of block a for the ng sibling groups of children starting at c0: the eight
+// children's block a stacked (8·LD per group); block 4 with ½Ψ̂ + δ̂·Φ
+__global__ void k_stokes_m2m_in(const double* __restrict__ M, int c0, int ng, int LD, int a, double* __restrict__ X) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)ng * 8 * LD) return;
+  const int i = (int)(e % LD), j = (int)((e / LD) % 8), g = (int)(e / (8 * LD));
+  const double* ch = M + (int64_t)(c0 + 8 * g + j) * 4 * LD;
+  double v;
+  if (a < 3) v = ch[(int64_t)a * LD + i];
+  else v = 0.5 * ch[3 * (int64_t)LD + i] + dhat(j, 0) * ch[i] + dhat(j, 1) * ch[LD + i] + dhat(j, 2) * ch[2 * (int64_t)LD + i];
+  X[e] = v;
+}
+
+// L2L output: R_a = L2L·P_a (8·LD per group, a = 0..3) added to the children's partial locals,
+// block 4 as 2·R₄ − 2 δ̂·(R₁, R₂, R₃)
+__global__ void k_stokes_l2l_out(double* __restrict__ Pl, const double* __restrict__ R, int c0, int ng, int LD, int NP) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t per = (int64_t)ng * 8 * LD;
+  if (e >= per) return;
+  const int i = (int)(e % LD), j = (int)((e / LD) % 8), g = (int)(e / (8 * LD));
+  if (i >= NP) return;
+  double* ch = Pl + (int64_t)(c0 + 8 * g + j) * 4 * LD;
+  const double r1 = R[e], r2 = R[per + e], r3 = R[2 * per + e], r4 = R[3 * per + e];
+  ch[i] += r1;
+  ch[LD + i] += r2;
+  ch[2 * (int64_t)LD + i] += r3;
+  ch[3 * (int64_t)LD + i] += 2.0 * r4 - 2.0 * (dhat(j, 0) * r1 + dhat(j, 1) * r2 + dhat(j, 2) * r3);
+}
+
+// the far field at the targets of one leaf: u = ½[Φ − x̂·∇̂Φ + ∇̂Ψ̂] from the leaf's four local blocks
+// (staged in shared memory per warp), lanes over the targets; writes the velocities
+template <int P>
+__global__ void __launch_bounds__(SW * 32) k_stokes_l2p(const int* __restrict__ gnode, const int* __restrict__ gstart,
+                                                        const int* __restrict__ gcount, int ngroups,
+                                                        const double* __restrict__ tx, const double* __restrict__ ty,
+                                                        const double* __restrict__ tz, const int* __restrict__ tout,
+                                                        const int4* __restrict__ cell, const double* __restrict__ Pl, int LD,
+                                                        Geometry geo, const double* __restrict__ scale,
+                                                        double* __restrict__ vel) {
+  extern __shared__ double sl[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x * SW + warp;
+  if (grp >= ngroups) return;
+  double* L = sl + (int64_t)warp * 4 * LD;
+  const int leaf = gnode[grp];
+  for (int i = lane; i < 4 * LD; i += 32) L[i] = Pl[(int64_t)leaf * 4 * LD + i];
+  __syncwarp();
+  const int4 c = cell[leaf];
+  const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
+  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const int t0 = gstart[grp], nt = gcount[grp];
+  for (int base = 0; base < nt; base += 32) {
+    const int k = t0 + base + lane;
+    const bool act = base + lane < nt;
+    const double xh[3] = {act ? (tx[k] - cx) * s : 0.0, act ? (ty[k] - cy) * s : 0.0, act ? (tz[k] - cz) * s : 0.0};
+    double phi[3], G[3][3], gpsi[3];   // G[i][k] = ∂̂_i Φ_k
+    for (int a = 0; a < 4; ++a) {
+      double u, g[3];
+      l2p<P, double>(L + (int64_t)a * LD, xh[0], xh[1], xh[2], u, g[0], g[1], g[2]);
+      if (a < 3) {
+        phi[a] = u;
+        for (int i = 0; i < 3; ++i) G[i][a] = g[i];
+      } else {
+        for (int i = 0; i < 3; ++i) gpsi[i] = g[i];
+      }
+    }
+    if (act) {
+      const int o = tout[k];
+      for (int i = 0; i < 3; ++i)
+        vel[3 * (int64_t)o + i] = 0.5 * (phi[i] - (xh[0] * G[i][0] + xh[1] * G[i][1] + xh[2] * G[i][2]) + gpsi[i]);
+    }
+  }
+}
+
+struct alignas(16) S8 { double x, y, z, fx, fy, fz, pad0, pad1; };
+
+// the near field: the Stokeslets of the 27 colleagues, flattened into batches of 32 staged per
+// warp (the next batch's loads in flight), lanes over the targets; adds c·Σ to the velocities
+template <bool SELF>
+__global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
+                                                         const int* __restrict__ gcount, int ngroups,
+                                                         const double* __restrict__ tx, const double* __restrict__ ty,
+                                                         const double* __restrict__ tz, const int* __restrict__ tout,
+                                                         const double* __restrict__ xs, const double* __restrict__ ys,
+                                                         const double* __restrict__ zs, const double* __restrict__ f3,
+                                                         int64_t n, const int* __restrict__ plo, const int* __restrict__ phi,
+                                                         const int* __restrict__ col, double* __restrict__ vel) {
+  __shared__ S8 stg[SW][2][32];
+  __shared__ int s_lo[SW][32], s_pre[SW][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x * SW + warp;
+  if (grp >= ngroups) return;
+  const int leaf = gnode[grp];
+  const int cn = lane < NCOL ? col[(int64_t)leaf * NCOL + lane] : -1;
+  int lo = 0, len = 0;
+  if (cn >= 0) {
+    lo = plo[cn];
+    len = max(0, phi[cn] - lo + 1);
+  }
+  int incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int S = __shfl_sync(0xffffffffu, incl, 31);
+  s_lo[warp][lane] = lo;
+  s_pre[warp][lane] = incl - len;
+  const unsigned selfm = __ballot_sync(0xffffffffu, cn == leaf);
+  const int slot = selfm ? __ffs(selfm) - 1 : 0;
+  const int pself = selfm ? __shfl_sync(0xffffffffu, incl - len, slot) : -1;
+  const int loself = __shfl_sync(0xffffffffu, lo, slot), lenself = selfm ? __shfl_sync(0xffffffffu, len, slot) : 0;
+  __syncwarp();
+  auto load = [&](int b, S8& v) {
+    const int f = 32 * b + lane;
+    v = S8{0, 0, 0, 0, 0, 0, 0, 0};
+    if (f < S) {
+      int idx = 0;
+#pragma unroll
+      for (int step = 16; step; step >>= 1)
+        if (s_pre[warp][idx + step] <= f) idx += step;
+      const int64_t j = s_lo[warp][idx] + (f - s_pre[warp][idx]);
+      v = S8{xs[j], ys[j], zs[j], f3[j], f3[n + j], f3[2 * n + j], 0, 0};
+    }
+  };
+  const int t0 = gstart[grp], nt = gcount[grp];
+  for (int base = 0; base < nt; base += 32) {
+    const int k = t0 + base + lane;
+    const bool act = base + lane < nt;
+    const double x = act ? tx[k] : 0.0, y = act ? ty[k] : 0.0, z = act ? tz[k] : 0.0;
+    const int fself = SELF && act && selfm ? pself + (k - loself) : -1;
+    double ux = 0, uy = 0, uz = 0;
+    S8 nxt;
+    load(0, nxt);
+    for (int b = 0; 32 * b < S; ++b) {
+      S8* st = stg[warp][b & 1];
+      st[lane] = nxt;
+      __syncwarp();
+      if (32 * (b + 1) < S) load(b + 1, nxt);
+      const int m = min(32, S - 32 * b);
+      const bool chk = SELF && selfm && 32 * b < pself + lenself && 32 * b + 32 > pself;   // uniform
+      const int is = fself - 32 * b;
+      for (int i = 0; i < m; ++i) {
+        const S8 sv = st[i];
+        const double dx = x - sv.x, dy = y - sv.y, dz = z - sv.z;
+        const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+        double ir = rsqrt(r2);
+        if (chk && i == is) ir = 0.0;
+        const double df = (dx * sv.fx + dy * sv.fy + dz * sv.fz) * ir * ir * ir;
+        ux += sv.fx * ir + dx * df;
+        uy += sv.fy * ir + dy * df;
+        uz += sv.fz * ir + dz * df;
+      }
+    }
+    if (act) {
+      const int o = tout[k];
+      vel[3 * (int64_t)o] += KSTOKES * ux;
+      vel[3 * (int64_t)o + 1] += KSTOKES * uy;
+      vel[3 * (int64_t)o + 2] += KSTOKES * uz;
+    }
+    __syncwarp();
+  }
+}
+
+template <int P>
+void launch_stokes_l2p(State& S, double* vel) {
+  Plan& P_ = *S.plan;
+  const int LD = P_.cache->ld;
+  const size_t smem = sizeof(double) * SW * 4 * LD;
+  FMMB_CUDA(cudaFuncSetAttribute(k_stokes_l2p<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_stokes_l2p<P><<<(P_.n_leaves + SW - 1) / SW, SW * 32, smem, P_.ctx->stream>>>(
+      P_.leaves.p, P_.leaf_start.p, P_.leaf_count.p, P_.n_leaves, S.xs.p, S.ys.p, S.zs.p, P_.perm.p, P_.cell.p, S.Pl.p, LD,
+      geometry(P_), P_.d_scale.p, vel);
+  FMMB_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+// build_expansions! of a Stokes state from Stokeslets f (3×n, original order, device)
+void stokes_build(State& S, const double* xyz_dev, const double* f_dev) {
+  Plan& P = *S.plan;
+  Cache& C = *P.cache;
+  cudaStream_t s = P.ctx->stream;
+  const int LD = C.ld;
+  const int64_t n = P.N, pitch = 4 * (int64_t)LD;
+  if (S.f3.n < (size_t)(3 * n)) S.f3.alloc(3 * n);
+  if (S.q.n < (size_t)n) S.q.alloc(n);
+  k_stokes_gather<<<nblk(n), 256, 0, s>>>(xyz_dev, f_dev, P.perm.p, n, S.xs.p, S.ys.p, S.zs.p, S.f3.p);
+  FMMB_LAUNCH_CHECK();
+  if (P.n_s2m > 0) {
+    k_stokes_q4<<<nblk((int64_t)P.n_s2m * 32), 256, 0, s>>>(P.s2m_nodes.p, P.n_s2m, P.cell.p, P.plo.p, P.phi.p, geometry(P),
+                                                           P.d_scale.p, n, S.xs.p, S.ys.p, S.zs.p, S.f3.p, S.q.p);
+    FMMB_LAUNCH_CHECK();
+  }
+  // P2M, one block at a time
+  for (int a = 0; a < 3; ++a) p2m_block(S, S.f3.p + a * n, S.M.p + (int64_t)a * LD, pitch);
+  p2m_block(S, S.q.p, S.M.p + 3 * (int64_t)LD, pitch);
+  // M2M, level by level: the stacked children of each block (Ψ̂ with the coupling), one product each
+  for (int l = P.L - 2; l >= 2; --l) {
+    const int c0 = P.level_start[l + 1], ng = (P.level_start[l + 2] - c0) / NCH;
+    if (ng == 0) continue;
+    DBuf<double> X((size_t)ng * NCH * LD);
+    for (int a = 0; a < 4; ++a) {
+      k_stokes_m2m_in<<<nblk((int64_t)ng * NCH * LD), 256, 0, s>>>(S.M.p, c0, ng, LD, a, X.p);
+      FMMB_LAUNCH_CHECK();
+      ColMap bm{X.p, nullptr, 0, NCH}, cm{S.M.p + (int64_t)a * LD, P.group_parent[l + 1].p, 0, 0, pitch};
+      gemm_columns(LD, NCH * LD, C.m2m.p, bm, cm, ng, LD, C.np, 0, P.ctx->num_sms, s);
+    }
+  }
+  // M2L of every block (the Ψ̂ launch with the coupling), then L2L level by level
+  m2l_stage(S);
+  for (int l = 3; l < P.L; ++l) {
+    const int c0 = P.level_start[l], ng = (P.level_start[l + 1] - c0) / NCH;
+    if (ng == 0) continue;
+    const int64_t per = (int64_t)ng * NCH * LD;
+    DBuf<double> R(4 * per);
+    for (int a = 0; a < 4; ++a) {
+      ColMap bm{S.Pl.p + (int64_t)a * LD, P.group_parent[l].p, 0, 0, pitch}, cm{R.p + a * per, nullptr, 0, NCH};
+      gemm_columns(NCH * LD, LD, C.l2l.p, bm, cm, ng, LD, C.np, 0, P.ctx->num_sms, s);
+    }
+    k_stokes_l2l_out<<<nblk(per), 256, 0, s>>>(S.Pl.p, R.p, c0, ng, LD, C.np);
+    FMMB_LAUNCH_CHECK();
+  }
+  S.built = true;
+}
+
+// evaluate_at_sources! of a Stokes state: velocities (3×n, original order, device), self excluded
+void stokes_evaluate_sources(State& S, double* vel_dev) {
+  Plan& P = *S.plan;
+  switch (P.cache->p) {
+#define X(pp) case pp: launch_stokes_l2p<pp>(S, vel_dev); break;
+    FMMB_P_CASES(X)
+#undef X
+    default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
+  }
+  k_stokes_near<true><<<(P.n_leaves + SW - 1) / SW, SW * 32, 0, P.ctx->stream>>>(
+      P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, S.xs.p, S.ys.p, S.zs.p, P.perm.p, S.xs.p, S.ys.p, S.zs.p,
+      S.f3.p, P.N, P.plo.p, P.phi.p, P.col.p, vel_dev);
+  FMMB_LAUNCH_CHECK();
+}
+
+}  // namespace fmmb

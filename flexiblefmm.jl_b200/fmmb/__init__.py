@@ -85,7 +85,8 @@ EXPORTS = (
     "fmmb_state_destroy", "fmmb_build_expansions", "fmmb_build_expansions_dev", "fmmb_evaluate_at_sources",
     "fmmb_evaluate_at_sources_dev", "fmmb_matvec", "fmmb_matvec_dev", "fmmb_evaluate", "fmmb_evaluate_dev",
     "fmmb_state_expansions", "fmmb_direct_dev", "fmmb_profile_matvec", "fmmb_direct_noalloc_dev",
-    "fmmb_server_create", "fmmb_server_submit", "fmmb_server_wait", "fmmb_server_destroy",
+    "fmmb_server_create", "fmmb_server_submit", "fmmb_server_wait", "fmmb_server_destroy", "fmmb_stokes_eval",
+    "fmmb_stokes_eval_dev",
 )
 
 
@@ -137,6 +138,8 @@ def lib():
         "fmmb_server_submit": [vp, C.POINTER(_Request), C.POINTER(i64)],
         "fmmb_server_wait": [vp, i64, C.c_double, C.POINTER(_RequestInfo)],
         "fmmb_server_destroy": [vp],
+        "fmmb_stokes_eval": [vp, dp, dp, i64, dp],
+        "fmmb_stokes_eval_dev": [vp, dp, dp, i64, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -169,6 +172,25 @@ def _points(x):
 class Laplace3D:
     """Free-space Laplace Green's function 1/(4π|t − s|) (src/kernels.jl:179-200)."""
     c = 1.0 / (4.0 * np.pi)
+
+
+class Stokeslet3D:
+    """The 3D Stokeslet (1/8π)(f/r + d(d·f)/r³) (src/kernels.jl:253-272)."""
+    c = 1.0 / (8.0 * np.pi)
+
+
+class StokesHarmonics:
+    """StokesHarmonics(Stokeslet3D(); p=16) (src/operators/harmonics_stokes.jl:34-45): four
+    solid-harmonic expansions per box; Stokeslet densities, velocity output, FP64 path."""
+
+    def __init__(self, kernel, p=16, tol=0.0):
+        if not isinstance(kernel, Stokeslet3D):
+            raise ArgumentError(1, "StokesHarmonics takes Stokeslet3D")
+        if p < 1:
+            raise ArgumentError(1, "p must be at least 1")
+        if tol != 0:
+            raise Unsupported(6, "low-rank translations (tol > 0) are not provided")
+        self.kernel, self.p, self.tol = kernel, int(p), 0.0
 
 
 class SphericalHarmonics:
@@ -240,7 +262,7 @@ class OperatorCache:
     def __init__(self, method, ctx=None):
         self.method = method
         self.ctx = ctx or default_context()
-        d = _MethodDesc(1, 1, method.p, 0, method.tol)
+        d = _MethodDesc(1, 3 if isinstance(method, StokesHarmonics) else 1, method.p, 0, method.tol)
         h = C.c_void_p()
         _check(lib().fmmb_cache_create(self.ctx._h, C.byref(d), C.byref(h)))
         self._h = h
@@ -337,9 +359,12 @@ class FMMState:
         self._h = h
 
     def expansions(self):
+        """(multipoles, locals): nnodes × (p+1)² for Laplace3D, nnodes × 4 × (p+1)² for the
+        Stokeslet (blocks Φ₁, Φ₂, Φ₃, Ψ̂)."""
         n, np_ = self.fmm.nnodes, (self.fmm.method.p + 1) ** 2
-        M = np.zeros((n, np_))
-        Lc = np.zeros((n, np_))
+        shape = (n, 4, np_) if isinstance(self.fmm.method, StokesHarmonics) else (n, np_)
+        M = np.zeros(shape)
+        Lc = np.zeros(shape)
         _check(lib().fmmb_state_expansions(self._h, _ptr(M), _ptr(Lc)))
         return M, Lc
 
@@ -476,3 +501,38 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- the Stokes plan API
+class StokesFMMPlan:
+    """StokesFMMPlan(sources; method=:harmonics, p=16, ppl, bbox) (src/stokes_api.jl:20-71) for a
+    self plan (targets = nothing): the tree and operators of StokesHarmonics(Stokeslet3D(); p) for
+    a fixed geometry, reused by every stokes_fmm_eval. The device path provides the :harmonics
+    method with Stokeslet densities and velocity output."""
+
+    def __init__(self, sources, method="harmonics", p=16, ppl=200, bbox=None, targets=None):
+        if method != "harmonics":
+            raise Unsupported(6, "the device path provides method=:harmonics")
+        if targets is not None:
+            raise Unsupported(6, "the device path evaluates Stokes plans at their sources")
+        self.sources = _points(sources)
+        if bbox is None:
+            lo, hi = self.sources.min(axis=0), self.sources.max(axis=0)
+            w = float(np.max(hi - lo)) or 1.0
+            c = (lo + hi) / 2
+            bbox = (tuple(c - w / 2 * (1 + 1e-12)), w * (1 + 2e-12))
+        self.method = StokesHarmonics(Stokeslet3D(), p=p)
+        self.fmm = FMM(self.method, self.sources, ppl=ppl, bbox=bbox)
+        self.state = FMMState(self.fmm, "fp64")
+
+
+def stokes_fmm_eval(plan, stokeslets, sources=None):
+    """stokes_fmm_eval!(velocities, plan; stokeslets) (src/stokes_api.jl:131-150): velocities at the
+    sources of a self plan, the i = j term skipped; stokeslets (N, 3)."""
+    x = plan.sources if sources is None else _points(sources)
+    f = np.ascontiguousarray(stokeslets, dtype=np.float64)
+    if f.shape != x.shape:
+        raise DimensionMismatch(2, f"stokeslets has shape {f.shape}, expected {x.shape}")
+    vel = np.zeros_like(f)
+    _check(lib().fmmb_stokes_eval(plan.state._h, _ptr(x), _ptr(f), x.shape[0], _ptr(vel)))
+    return vel

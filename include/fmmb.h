@@ -33,6 +33,7 @@ extern "C" {
 #define FMMB_ERR_UNSUPPORTED 6 /* a method, kernel, density or output this build does not provide */
 
 #define FMMB_KERNEL_LAPLACE3D 1
+#define FMMB_KERNEL_STOKESLET3D 3 /* StokesHarmonics(Stokeslet3D(); p): FP64 path, Stokeslet densities, velocities */
 #define FMMB_METHOD_SPHERICAL_HARMONICS 1
 
 #define FMMB_PRECISION_FP64 0  /* the plain path: FP64 everywhere (the drop-in) */
@@ -46,7 +47,8 @@ typedef struct fmmb_cache fmmb_cache;
 typedef struct fmmb_plan fmmb_plan;
 typedef struct fmmb_state fmmb_state;
 
-/* The method: SphericalHarmonics(Laplace3D(); p) (src/operators/harmonics.jl:303-308). */
+/* The method: SphericalHarmonics(Laplace3D(); p) (src/operators/harmonics.jl:303-308), or with kernel
+ * FMMB_KERNEL_STOKESLET3D StokesHarmonics(Stokeslet3D(); p) (src/operators/harmonics_stokes.jl:34-45). */
 typedef struct {
   int32_t method;  /* FMMB_METHOD_SPHERICAL_HARMONICS */
   int32_t kernel;  /* FMMB_KERNEL_LAPLACE3D */
@@ -126,9 +128,18 @@ int fmmb_evaluate_dev(fmmb_state* state, const double* targets_dev, int64_t nt, 
  * *launches = the kernels launched (the reference times the same phases: bench/bench.jl:44-56). */
 int fmmb_profile_matvec(fmmb_state* state, const double* xyz_dev, const double* tau_dev, int64_t n, int outputs,
                         double* pot_dev, double* grad_dev, double* stage_ms, int cap, int* launches);
-/* The multipoles and locals of the last build (nnodes × (p+1)² each, node order, the real
- * storage of src/operators/harmonics.jl:20-27; locals are zero outside the real leaves). */
+/* The multipoles and locals of the last build (nnodes × nexp × (p+1)² each, node order, the real
+ * storage of src/operators/harmonics.jl:20-27, nexp = 1 for Laplace3D and 4 (Φ₁, Φ₂, Φ₃, Ψ̂) for
+ * the Stokeslet; locals are zero outside the real leaves). */
 int fmmb_state_expansions(const fmmb_state* state, double* multipoles, double* locals);
+
+/* stokes_fmm_eval!(velocities, plan; stokeslets) with a self plan (src/stokes_api.jl:131-150) on a
+ * state of a Stokeslet cache (FP64 path): build_expansions! then evaluate_at_sources!, the i = j
+ * term skipped. xyz 3×n, stokeslets 3×n (Vector{SVector{3,Float64}}), velocity 3×n out, all in
+ * the original order. The Laplace entry points reject Stokeslet states (FMMB_ERR_UNSUPPORTED). */
+int fmmb_stokes_eval(fmmb_state* state, const double* xyz, const double* stokeslets, int64_t n, double* velocity);
+int fmmb_stokes_eval_dev(fmmb_state* state, const double* xyz_dev, const double* stokeslets_dev, int64_t n,
+                         double* velocity_dev);
 
 /* direct!(out, K, sources, τ, targets) / direct_self! (src/kernels.jl:463-487) for Laplace3D on
  * the device in FP64, device pointers: sources 3×ns, targets 3×nt. self_index (device, may be
