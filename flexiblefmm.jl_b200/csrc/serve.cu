@@ -44,24 +44,31 @@ struct Job {
   std::string error;
 };
 
-// the order for a requested tolerance: the smallest p whose relative L2 error of the potential
-// against direct sums stays below it, measured with the CPU oracle (ppl = 64, uniform and
-// 4-cluster points of 2·10⁵, uniform points of 10⁶ for p = 10..13; the worst of them)
-int order_for_tol(double tol) {
-  static const double err[PMAX + 1] = {1, 1, 9.5e-3, 3.1e-3, 1.0e-3, 3.6e-4, 1.3e-4, 5.6e-5, 2.4e-5, 7.6e-6, 3.8e-6,
+// the order for a requested tolerance: the smallest p whose relative L2 error against direct sums
+// stays below it. Laplace3D potential: measured with the CPU oracle (ppl = 64, uniform and
+// 4-cluster points of 2·10⁵, uniform points of 10⁶ for p = 10..13; the worst of them).
+// Stokeslet3D velocity: measured on the device path (ppl = 64 and 200, 2·10⁵ points uniform in
+// the cube and on the jittered unit sphere; the worst of them).
+int order_for_tol(double tol, int kernel) {
+  static const double lap[PMAX + 1] = {1, 1, 9.5e-3, 3.1e-3, 1.0e-3, 3.6e-4, 1.3e-4, 5.6e-5, 2.4e-5, 7.6e-6, 3.8e-6,
                                        7.3e-7, 3.8e-7, 1.8e-7, 1.6e-7, 8.5e-8, 4.5e-8, 2.0e-8, 8.4e-9, 5.0e-9, 2.7e-9};
+  static const double sto[PMAX + 1] = {1, 1, 3.7e-2, 1.3e-2, 4.8e-3, 1.9e-3, 7.5e-4, 3.4e-4, 1.4e-4, 6.9e-5, 3.1e-5,
+                                       1.6e-5, 7.8e-6, 4.1e-6, 2.2e-6, 9.6e-7, 5.9e-7, 2.7e-7, 2.2e-7, 1.4e-7, 8.1e-8};
+  const double* err = kernel == FMMB_KERNEL_STOKESLET3D ? sto : lap;
   for (int p = 2; p <= PMAX; ++p)
     if (err[p] <= tol) return p;
   return PMAX;
 }
 
-// an upper estimate of the device memory one request holds (tree, lists, expansions, staging)
-int64_t bytes_estimate(int64_t n, int p, int ppl, int precision) {
+// an upper estimate of the device memory one request holds (tree, lists, expansions, staging);
+// a Stokeslet request holds four expansions per node and three densities per point
+int64_t bytes_estimate(int64_t n, int p, int ppl, int precision, int kernel) {
   const int64_t ld = ld_of(p), kp = (int64_t)((p + 1) * (p + 1) + 15) / 16 * 16;
-  const int64_t nodes = 4 * n / std::max(ppl, 1) + 4096;
-  int64_t b = n * 256;                                   // points in and sorted, keys, perm, outputs
-  b += nodes * (2 * ld * 8 + 27 * 4 + 64);               // multipoles, partial locals, colleagues, node arrays
+  const int64_t nodes = 4 * n / std::max(ppl, 1) + 4096, nexp = kernel == FMMB_KERNEL_STOKESLET3D ? 4 : 1;
+  int64_t b = n * (nexp == 4 ? 448 : 256);               // points in and sorted, keys, perm, densities, outputs
+  b += nodes * (2 * nexp * ld * 8 + 27 * 4 + 64);        // multipoles, partial locals, colleagues, node arrays
   b += nodes * 190 * 8;                                  // far pairs
+  if (nexp == 4) b += nodes / 8 * 4 * 8 * ld * 8;        // M2M / L2L staging of the largest level
   if (precision == FMMB_PRECISION_MIXED) b += nodes * kp * 8 + nodes * 4;   // FP16 copies, scales
   return b + (16 << 20);
 }
@@ -92,30 +99,35 @@ namespace {
 // one request on a slot: plan, state, matvec through the host-pointer entry points of the
 // slot's context, then release; returns the status
 int run_job(fmmb_server& S, int slot, Job& j, std::string& err) {
+  const int kernel = j.r.kernel;
   fmmb_cache* cache = nullptr;
   {
     auto& cs = S.caches[slot];
-    auto it = cs.find(j.p);
+    const int key = kernel * 64 + j.p;
+    auto it = cs.find(key);
     if (it == cs.end()) {
-      fmmb_method_desc m{FMMB_METHOD_SPHERICAL_HARMONICS, FMMB_KERNEL_LAPLACE3D, j.p, 0, 0.0};
+      fmmb_method_desc m{FMMB_METHOD_SPHERICAL_HARMONICS, kernel, j.p, 0, 0.0};
       int rc = fmmb_cache_create(S.ctx[slot], &m, &cache);
       if (rc) { err = fmmb_last_error(); return rc; }
       // a request's box depends on its own points only (not on which request the slot's cache
       // saw first), so its results are the same on any slot
       fix_cache_base_width(cache, 1.0);
-      cs[j.p] = cache;
+      cs[key] = cache;
     } else {
       cache = it->second;
     }
   }
   fmmb_tree_opts o{};
-  o.ppl = S.ppl;
+  o.ppl = j.r.ppl > 0 ? j.r.ppl : S.ppl;
   o.max_levels = 30;
   fmmb_plan* plan = nullptr;
   fmmb_state* st = nullptr;
   int rc = fmmb_plan_create(cache, j.r.xyz, j.r.n, &o, &plan);
   if (!rc) rc = fmmb_state_create(plan, j.precision, &st);
-  if (!rc) rc = fmmb_matvec(st, j.r.xyz, j.r.tau, j.r.n, j.r.outputs, j.r.pot, j.r.grad);
+  if (!rc) {
+    if (kernel == FMMB_KERNEL_STOKESLET3D) rc = fmmb_stokes_eval(st, j.r.xyz, j.r.tau, j.r.n, j.r.pot);
+    else rc = fmmb_matvec(st, j.r.xyz, j.r.tau, j.r.n, j.r.outputs, j.r.pot, j.r.grad);
+  }
   if (rc) err = fmmb_last_error();
   if (st) fmmb_state_destroy(st);
   if (plan) fmmb_plan_destroy(plan);
@@ -189,19 +201,29 @@ int fmmb_server_create(int device, const fmmb_server_opts* opts, fmmb_server** o
 
 int fmmb_server_submit(fmmb_server* S, const fmmb_request* r, int64_t* ticket) {
   if (!S || !r || !ticket) return FMMB_ERR_ARGUMENT;
-  if (r->kernel != FMMB_KERNEL_LAPLACE3D) return FMMB_ERR_UNSUPPORTED;
-  if (!r->xyz || !r->tau || r->n <= 0 || r->outputs < 1 || r->outputs > 3) return FMMB_ERR_ARGUMENT;
-  if (((r->outputs & FMMB_OUTPUT_POTENTIAL) && !r->pot) || ((r->outputs & FMMB_OUTPUT_GRADIENT) && !r->grad))
-    return FMMB_ERR_ARGUMENT;
+  const bool stokes = r->kernel == FMMB_KERNEL_STOKESLET3D;
+  if (r->kernel != FMMB_KERNEL_LAPLACE3D && !stokes) return FMMB_ERR_UNSUPPORTED;
+  if (!r->xyz || !r->tau || r->n <= 0 || r->ppl < 0) return FMMB_ERR_ARGUMENT;
+  if (stokes) {
+    // Stokeslets in tau (3×n), velocities in pot (3×n), on the FP64 path
+    if (!r->pot) return FMMB_ERR_ARGUMENT;
+    if (r->precision == FMMB_PRECISION_MIXED) return FMMB_ERR_UNSUPPORTED;
+  } else {
+    if (r->outputs < 1 || r->outputs > 3) return FMMB_ERR_ARGUMENT;
+    if (((r->outputs & FMMB_OUTPUT_POTENTIAL) && !r->pot) || ((r->outputs & FMMB_OUTPUT_GRADIENT) && !r->grad))
+      return FMMB_ERR_ARGUMENT;
+  }
   if (!(r->tol > 0 && r->tol < 1) && r->p == 0) return FMMB_ERR_ARGUMENT;
   std::unique_ptr<Job> j(new Job());
   j->r = *r;
-  j->p = r->p > 0 ? r->p : order_for_tol(r->tol);
+  j->p = r->p > 0 ? r->p : order_for_tol(r->tol, r->kernel);
   if (j->p < 1 || j->p > PMAX) return FMMB_ERR_ARGUMENT;
   // the precision path: FP64 below 1e-8 (or where the mixed path has no kernel), mixed above
-  j->precision = r->precision >= 0 ? r->precision
-                                   : ((r->tol < 1e-8 || (j->p + 1) * (j->p + 1) > 144) ? FMMB_PRECISION_FP64 : FMMB_PRECISION_MIXED);
-  j->bytes = bytes_estimate(r->n, j->p, S->ppl, j->precision);
+  if (stokes) j->precision = FMMB_PRECISION_FP64;
+  else
+    j->precision = r->precision >= 0 ? r->precision
+                                     : ((r->tol < 1e-8 || (j->p + 1) * (j->p + 1) > 144) ? FMMB_PRECISION_FP64 : FMMB_PRECISION_MIXED);
+  j->bytes = bytes_estimate(r->n, j->p, r->ppl > 0 ? r->ppl : S->ppl, j->precision, r->kernel);
   j->t_submit = clk::now();
   std::lock_guard<std::mutex> lk(S->mu);
   if (S->stop) return FMMB_ERR_ARGUMENT;

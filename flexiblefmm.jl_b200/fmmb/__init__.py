@@ -29,6 +29,8 @@ PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 OUTPUT_POTENTIAL = 1
 OUTPUT_GRADIENT = 2
+KERNEL_LAPLACE3D = 1
+KERNEL_STOKESLET3D = 3
 
 
 class FMMBError(RuntimeError):
@@ -67,8 +69,8 @@ class _ServerOpts(C.Structure):
 
 class _Request(C.Structure):
     _fields_ = [("xyz", C.c_void_p), ("tau", C.c_void_p), ("n", C.c_int64), ("tol", C.c_double), ("kernel", C.c_int32),
-                ("p", C.c_int32), ("outputs", C.c_int32), ("precision", C.c_int32), ("pot", C.c_void_p),
-                ("grad", C.c_void_p)]
+                ("p", C.c_int32), ("outputs", C.c_int32), ("precision", C.c_int32), ("ppl", C.c_int32),
+                ("pot", C.c_void_p), ("grad", C.c_void_p)]
 
 
 class _RequestInfo(C.Structure):
@@ -461,9 +463,10 @@ class Server:
         self._h = h
         self._live = {}
 
-    def submit(self, sources, tau, tol=1e-6, p=0, precision=None, gradient=True):
+    def submit(self, sources, tau, tol=1e-6, p=0, precision=None, gradient=True, ppl=0):
         """Queue one Laplace3D FMM at the sources (potential and, optionally, gradient, self
-        excluded); returns a ticket. precision None: chosen from tol (FP64 below 1e-8)."""
+        excluded); returns a ticket. precision None: chosen from tol (FP64 below 1e-8); ppl 0:
+        the server's."""
         x = _points(sources)
         t = np.ascontiguousarray(tau, dtype=np.float64)
         if t.shape != (x.shape[0],):
@@ -472,11 +475,26 @@ class Server:
         grad = np.zeros((x.shape[0], 3)) if gradient else None
         prec = -1 if precision is None else {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}[precision]
         flags = OUTPUT_POTENTIAL | (OUTPUT_GRADIENT if gradient else 0)
-        r = _Request(x.ctypes.data, t.ctypes.data, x.shape[0], float(tol), 1, int(p), flags, prec, pot.ctypes.data,
-                     None if grad is None else grad.ctypes.data)
+        r = _Request(x.ctypes.data, t.ctypes.data, x.shape[0], float(tol), KERNEL_LAPLACE3D, int(p), flags, prec,
+                     int(ppl), pot.ctypes.data, None if grad is None else grad.ctypes.data)
+        return self._submit(r, (x, t, pot, grad))
+
+    def submit_stokes(self, sources, stokeslets, tol=1e-6, p=0, ppl=0):
+        """Queue one StokesHarmonics(Stokeslet3D()) FMM (velocities at the sources, self
+        excluded, FP64); p 0: chosen from tol. wait() returns (velocities, None, info)."""
+        x = _points(sources)
+        f = np.ascontiguousarray(stokeslets, dtype=np.float64)
+        if f.shape != x.shape:
+            raise DimensionMismatch(2, f"stokeslets has shape {f.shape}, expected {x.shape}")
+        vel = np.zeros_like(f)
+        r = _Request(x.ctypes.data, f.ctypes.data, x.shape[0], float(tol), KERNEL_STOKESLET3D, int(p), 0, -1,
+                     int(ppl), vel.ctypes.data, None)
+        return self._submit(r, (x, f, vel, None))
+
+    def _submit(self, r, bufs):
         ticket = C.c_int64()
         _check(lib().fmmb_server_submit(self._h, C.byref(r), C.byref(ticket)))
-        self._live[ticket.value] = (x, t, pot, grad)     # the buffers stay alive until the request is waited for
+        self._live[ticket.value] = bufs     # the buffers stay alive until the request is waited for
         return ticket.value
 
     def wait(self, ticket, timeout=-1.0):
@@ -504,6 +522,30 @@ class Server:
 
 
 # ---------------------------------------------------------------- the Stokes plan API
+def square_bbox(points):
+    """square_bbox(points) (src/tree/tree.jl:97-113): the cube of the points' largest extent
+    about their midpoint, widened by 4 ulps at a time until every point is inside."""
+    x = _points(points)
+    if x.shape[0] == 0:
+        raise ArgumentError(1, "no points")
+    if not np.all(np.isfinite(x)):
+        raise ArgumentError(1, "the points must be finite")
+    lo, hi = x.min(axis=0), x.max(axis=0)
+    w0 = float(np.max(hi - lo))
+    if not np.isfinite(w0):
+        raise ArgumentError(1, "the points' extent overflows")
+    if not w0 > 0:
+        w0 = 1.0
+    c = lo + (hi - lo) / 2
+    origin = c - w0 / 2
+    for _ in range(64):
+        if np.all(origin <= lo) and np.all(origin + w0 >= hi):
+            return tuple(float(v) for v in origin), w0
+        w0 *= 1 + 4 * np.finfo(np.float64).eps
+        origin = c - w0 / 2
+    raise ArgumentError(1, "could not fit a box around the points")
+
+
 class StokesFMMPlan:
     """StokesFMMPlan(sources; method=:harmonics, p=16, ppl, bbox) (src/stokes_api.jl:20-71) for a
     self plan (targets = nothing): the tree and operators of StokesHarmonics(Stokeslet3D(); p) for
@@ -517,10 +559,7 @@ class StokesFMMPlan:
             raise Unsupported(6, "the device path evaluates Stokes plans at their sources")
         self.sources = _points(sources)
         if bbox is None:
-            lo, hi = self.sources.min(axis=0), self.sources.max(axis=0)
-            w = float(np.max(hi - lo)) or 1.0
-            c = (lo + hi) / 2
-            bbox = (tuple(c - w / 2 * (1 + 1e-12)), w * (1 + 2e-12))
+            bbox = square_bbox(self.sources)
         self.method = StokesHarmonics(Stokeslet3D(), p=p)
         self.fmm = FMM(self.method, self.sources, ppl=ppl, bbox=bbox)
         self.state = FMMState(self.fmm, "fp64")

@@ -13,7 +13,7 @@
 # interleaved array the ABI takes); outputs come back in the original order.
 module FlexibleFMMB200
 
-using FlexibleFMM: FlexibleFMM, SphericalHarmonics, Laplace3D, Potential, Gradient
+using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, Laplace3D, Stokeslet3D, Potential, Gradient
 using StaticArrays: SVector
 
 const libfmmb = get(ENV, "FMMB_LIB", joinpath(@__DIR__, "..", "libfmmb.so"))
@@ -63,13 +63,18 @@ default_context() = something(DEFAULT_CONTEXT[], (DEFAULT_CONTEXT[] = Context(0)
 """
     OperatorCache(method)  (src/operators/cache.jl:19-22)
 """
+const DeviceMethod = Union{SphericalHarmonics,StokesHarmonics}
+_kernel_id(m::SphericalHarmonics) = m.kernel isa Laplace3D ? Int32(1) :
+    throw(ArgumentError("the device method is written for Laplace3D"))
+_kernel_id(m::StokesHarmonics) = m.kernel isa Stokeslet3D ? Int32(3) :
+    throw(ArgumentError("the device Stokes method is written for Stokeslet3D"))
+
 mutable struct OperatorCache
-    method::SphericalHarmonics
+    method::DeviceMethod
     ctx::Context
     h::Ptr{Cvoid}
-    function OperatorCache(m::SphericalHarmonics; ctx::Context=default_context())
-        m.kernel isa Laplace3D || throw(ArgumentError("the device method is written for Laplace3D"))
-        d = Ref(MethodDesc(1, 1, Int32(m.p), 0, m.tol))
+    function OperatorCache(m::DeviceMethod; ctx::Context=default_context())
+        d = Ref(MethodDesc(1, _kernel_id(m), Int32(m.p), 0, m isa SphericalHarmonics ? m.tol : 0.0))
         r = Ref{Ptr{Cvoid}}(C_NULL)
         check(ccall((:fmmb_cache_create, libfmmb), Cint, (Ptr{Cvoid}, Ref{MethodDesc}, Ref{Ptr{Cvoid}}), ctx.h, d, r))
         c = new(m, ctx, r[])
@@ -81,12 +86,12 @@ end
     FMM(method, sources; ppl=50, bbox=nothing, cache=OperatorCache(method), max_levels=30)  (src/fmm.jl:31-49)
 """
 mutable struct FMM
-    method::SphericalHarmonics
+    method::DeviceMethod
     cache::OperatorCache
     h::Ptr{Cvoid}
     n::Int
 end
-function FMM(m::SphericalHarmonics, sources::AbstractVector{SVector{3,Float64}}; ppl::Integer=50, bbox=nothing,
+function FMM(m::DeviceMethod, sources::AbstractVector{SVector{3,Float64}}; ppl::Integer=50, bbox=nothing,
              cache::OperatorCache=OperatorCache(m), max_levels::Integer=30)
     cache.method === m || throw(ArgumentError("the cache was built for a different method"))
     pts = collect(sources)
@@ -167,7 +172,7 @@ end
 struct ServerOpts; slots::Int32; ppl::Int32; hbm_budget::Int64; end
 struct Request
     xyz::Ptr{Float64}; tau::Ptr{Float64}; n::Int64; tol::Float64; kernel::Int32; p::Int32
-    outputs::Int32; precision::Int32; pot::Ptr{Float64}; grad::Ptr{SVector{3,Float64}}
+    outputs::Int32; precision::Int32; ppl::Int32; pot::Ptr{Float64}; grad::Ptr{SVector{3,Float64}}
 end
 struct RequestInfo
     status::Int32; p::Int32; precision::Int32; slot::Int32
@@ -196,10 +201,27 @@ function submit(s::Server, sources::AbstractVector{SVector{3,Float64}}, τ::Abst
     pot = Vector{Float64}(undef, length(x))
     grad = Vector{SVector{3,Float64}}(undef, length(x))
     req = Request(Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, x))), pointer(t), length(x), tol,
-                  1, 0, 3, -1, pointer(pot), pointer(grad))
+                  1, 0, 3, -1, 0, pointer(pot), pointer(grad))
+    return _submit(s, req, (x, t, pot, grad))
+end
+
+"""`submit_stokes(server, sources, stokeslets; tol, p=0, ppl=0)`: a StokesHarmonics(Stokeslet3D())
+FMM (velocities at the sources, self excluded, FP64); `wait` returns (velocities, nothing, info)."""
+function submit_stokes(s::Server, sources::AbstractVector{SVector{3,Float64}}, f::AbstractVector{SVector{3,Float64}};
+                       tol::Real=1e-6, p::Integer=0, ppl::Integer=0)
+    length(f) == length(sources) || throw(DimensionMismatch("one Stokeslet per source"))
+    x, fs = collect(sources), collect(f)
+    vel = Vector{SVector{3,Float64}}(undef, length(x))
+    req = Request(Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, x))),
+                  Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, fs))), length(x), tol, 3, p, 0, -1, ppl,
+                  Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, vel))), C_NULL)
+    return _submit(s, req, (x, fs, vel, nothing))
+end
+
+function _submit(s::Server, req::Request, bufs)
     ticket = Ref{Int64}(0)
     check(ccall((:fmmb_server_submit, libfmmb), Cint, (Ptr{Cvoid}, Ref{Request}, Ref{Int64}), s.h, req, ticket))
-    s.live[ticket[]] = (x, t, pot, grad)      # rooted until the request is waited for
+    s.live[ticket[]] = bufs      # rooted until the request is waited for
     return ticket[]
 end
 
@@ -209,6 +231,47 @@ function Base.wait(s::Server, ticket::Int64)
     x, t, pot, grad = pop!(s.live, ticket)
     check(rc)
     return pot, grad, info[]
+end
+
+# ---------------------------------------------------------------- the Stokes plan API (src/stokes_api.jl)
+"""
+    StokesFMMPlan(sources; method=:harmonics, p=16, ppl=200, bbox=nothing)  (src/stokes_api.jl:20-62)
+
+A self plan (targets = nothing) of StokesHarmonics(Stokeslet3D(); p) on the device: the tree and
+operators for a fixed geometry, reused by every `stokes_fmm_eval!`.
+"""
+struct StokesFMMPlan
+    fmm::FMM
+    state::FMMState
+    sources::Vector{SVector{3,Float64}}
+end
+function StokesFMMPlan(sources::AbstractVector{SVector{3,Float64}}; method::Symbol=:harmonics, p::Integer=16,
+                       ppl::Integer=200, bbox=nothing, targets=nothing)
+    method === :harmonics || throw(ArgumentError("the device path provides method=:harmonics"))
+    targets === nothing || throw(ArgumentError("the device path evaluates Stokes plans at their sources"))
+    pts = collect(sources)
+    bbox === nothing && (bbox = FlexibleFMM.square_bbox(pts))     # as the reference plan does
+    f = FMM(StokesHarmonics(Stokeslet3D(); p=p), pts; ppl, bbox)
+    return StokesFMMPlan(f, FMMState(f), pts)
+end
+
+"""
+    stokes_fmm_eval!(velocities, plan; stokeslets)  (src/stokes_api.jl:107-123)
+
+Velocities at the plan's sources, the i = j term skipped.
+"""
+function stokes_fmm_eval!(vel::AbstractVector{SVector{3,Float64}}, plan::StokesFMMPlan;
+                          stokeslets::AbstractVector{SVector{3,Float64}})
+    n = length(plan.sources)
+    length(stokeslets) == n || throw(DimensionMismatch("expected $n stokeslets"))
+    length(vel) == n || throw(DimensionMismatch("expected $n velocities"))
+    fs = collect(stokeslets)
+    out = Vector{SVector{3,Float64}}(undef, n)
+    check(ccall((:fmmb_stokes_eval, libfmmb), Cint,
+                (Ptr{Cvoid}, Ptr{SVector{3,Float64}}, Ptr{SVector{3,Float64}}, Int64, Ptr{SVector{3,Float64}}),
+                plan.state.h, plan.sources, fs, n, out))
+    copyto!(vel, out)
+    return vel
 end
 
 end # module

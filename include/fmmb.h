@@ -176,14 +176,16 @@ typedef struct {
 } fmmb_server_opts;
 typedef struct {
   const double* xyz;   /* 3×n host, original order; read while the request runs */
-  const double* tau;   /* n host */
+  const double* tau;   /* n host charges (Laplace3D); 3×n Stokeslets (Stokeslet3D) */
   int64_t n;
   double tol;          /* requested relative accuracy: selects p (when p = 0) and the precision path */
-  int32_t kernel;      /* FMMB_KERNEL_LAPLACE3D */
+  int32_t kernel;      /* FMMB_KERNEL_LAPLACE3D, or FMMB_KERNEL_STOKESLET3D (velocities at the sources) */
   int32_t p;           /* 0: the smallest order whose measured error is below tol */
-  int32_t outputs;     /* FMMB_OUTPUT_* bits */
-  int32_t precision;   /* -1: FP64 for tol < 1e-8 or p > 11, else the mixed path */
-  double* pot;         /* n host, written when the request completes (keep valid until then) */
+  int32_t outputs;     /* FMMB_OUTPUT_* bits (Laplace3D) */
+  int32_t precision;   /* -1: FP64 for tol < 1e-8 or p > 11, else the mixed path (Stokeslet3D: FP64) */
+  int32_t ppl;         /* points per leaf of this request's tree; 0: the server's */
+  double* pot;         /* n host potentials, or 3×n velocities; written when the request completes
+                          (keep valid until then) */
   double* grad;        /* 3×n host */
 } fmmb_request;
 typedef struct {

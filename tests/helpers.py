@@ -157,3 +157,24 @@ def same_structure(a, b, keys=("cell", "level", "parent", "child_first", "plo", 
 def oracle_tree_dict(T):
     return {k: getattr(T, k) for k in ("cell", "level", "parent", "child_first", "plo", "phi", "leaf", "ghost", "xlist",
                                        "has_source", "colleagues", "perm", "point_node")}
+
+
+# ---------------------------------------------------------------- Stokes (src/kernels.jl:253-272)
+def sphere_points(rng, n):
+    """Points on the unit sphere jittered by U(−0.01, 0.01)³ (the batched Stokes workload)."""
+    v = rng.standard_normal((n, 3))
+    return v / np.linalg.norm(v, axis=1)[:, None] + rng.uniform(-0.01, 0.01, (n, 3))
+
+
+def stokes_direct(src, f, sel):
+    """FP64 Stokeslet velocities (1/8π)Σ_{j≠i}[f_j/r + d(d·f_j)/r³] at the sources `sel`."""
+    out = np.zeros((len(sel), 3))
+    for a in range(0, len(sel), 64):
+        idx = sel[a:a + 64]
+        d = src[idx, None, :] - src[None, :, :]                     # (t, s, 3)
+        r2 = np.einsum("tsk,tsk->ts", d, d)
+        r2[np.arange(len(idx)), idx] = np.inf                         # the i = j term
+        ir = 1.0 / np.sqrt(r2)
+        df = np.einsum("tsk,sk->ts", d, f) * ir ** 3
+        out[a:a + 64] = (np.einsum("ts,sk->tk", ir, f) + np.einsum("ts,tsk->tk", df, d)) / (8 * np.pi)
+    return out

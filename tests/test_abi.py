@@ -3,6 +3,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -52,3 +53,43 @@ def test_julia_shim_binds_declared_symbols():
 def test_struct_layouts(fmmb):
     import ctypes as C
     assert C.sizeof(fmmb._MethodDesc) == 24 and C.sizeof(fmmb._TreeOpts) == 48
+
+
+def test_struct_layouts_match_the_header(fmmb, tmp_path):
+    """Every ctypes mirror of a header struct has the C compiler's size and field offsets."""
+    import ctypes as C
+    mirrors = {"fmmb_method_desc": fmmb._MethodDesc, "fmmb_tree_opts": fmmb._TreeOpts,
+               "fmmb_server_opts": fmmb._ServerOpts, "fmmb_request": fmmb._Request,
+               "fmmb_request_info": fmmb._RequestInfo}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "fmmb.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def test_square_bbox_contains_the_points(fmmb):
+    """square_bbox (src/tree/tree.jl:97-113): the largest extent about the midpoint, every point
+    inside; a single point gets width 1; non-finite points are an ArgumentError."""
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((1000, 3)) * [1.0, 3.0, 0.5] + 7.0
+    o, w = fmmb.square_bbox(x)
+    assert np.all(np.array(o) <= x.min(0)) and np.all(np.array(o) + w >= x.max(0))
+    assert abs(w - float((x.max(0) - x.min(0)).max())) <= 1e-12 * w
+    o1, w1 = fmmb.square_bbox(np.full((1, 3), 2.0))
+    assert w1 == 1.0 and o1 == (1.5, 1.5, 1.5)
+    bad = x.copy()
+    bad[5, 2] = np.inf
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.square_bbox(bad)

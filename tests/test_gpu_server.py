@@ -74,3 +74,31 @@ def test_server_errors(fmmb):
     u, g, info = srv.wait(srv.submit(good, np.ones(3000), tol=1e-3))    # the server keeps serving
     assert info["status"] == 0 and np.all(np.isfinite(u))
     srv.close()
+
+
+def test_server_stokes_requests_mixed_with_laplace(fmmb):
+    """Stokeslet requests (the batched Stokes workload: jittered unit-sphere points, N(0,1)³
+    forces) submitted among Laplace requests: each velocity field is bitwise the same as the
+    request alone, and within 3·tol of FP64 direct Stokeslet sums (p from the Stokes table)."""
+    from helpers import sphere_points, stokes_direct
+    rng = np.random.default_rng(9)
+    stokes = []
+    for i, tol in enumerate((1e-3, 1e-5, 1e-6)):
+        n = int(rng.integers(20000, 60000))
+        stokes.append((sphere_points(rng, n), rng.standard_normal((n, 3)), tol))
+    lap = _requests(10, 3)
+    srv = fmmb.Server(0, slots=4)
+    tickets = []
+    for (x, f, tol), (px, pt, ptol) in zip(stokes, lap):
+        tickets.append(("s", srv.submit_stokes(x, f, tol=tol, ppl=200)))
+        tickets.append(("l", srv.submit(px, pt, tol=ptol)))
+    mixed = [srv.wait(k) for _, k in tickets]
+    alone = [srv.wait(srv.submit_stokes(x, f, tol=tol, ppl=200)) for x, f, tol in stokes]
+    srv.close()
+    res = [m for (kind, _), m in zip(tickets, mixed) if kind == "s"]
+    for (x, f, tol), (v, g, info), (va, _, _) in zip(stokes, res, alone):
+        assert g is None and info["precision"] == "fp64" and info["status"] == 0
+        assert np.array_equal(v, va), info
+        sel = np.sort(rng.choice(len(x), 200, replace=False))
+        err = rel_l2(v[sel], stokes_direct(x, f, sel))
+        assert err < 3 * tol, (len(x), tol, info["p"], err)
