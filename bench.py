@@ -56,6 +56,7 @@ def args_():
     a.add_argument("--no-p10", action="store_true", help="skip the side measurement at the configured order p = 10")
     a.add_argument("--serve-requests", type=int, default=96, help="requests of the serving measurement (0: skip it)")
     a.add_argument("--serve-slots", type=int, default=4)
+    a.add_argument("--stokes-instances", type=int, default=64, help="instances of the batched Stokes measurement (0: skip it)")
     return a.parse_args()
 
 
@@ -239,6 +240,70 @@ def serving(fmmb, device, count, slots):
             "one_at_a_time_fp64": {"evals_per_s": total / t_seq, "latency_ms": {"p50": q(seq_lat, 0.5), "p99": q(seq_lat, 0.99)}},
             "paths": {"mixed": sum(i["precision"] == "mixed" for i in infos), "fp64": sum(i["precision"] == "fp64" for i in infos)}}
 
+# ---------------------------------------------------------------- batched Stokes
+def stokes_workload(count, seed=5):
+    """The batched Stokes configuration: N log-uniform in [2e4, 2e5] points on the unit sphere
+    jittered by U(-0.01, 0.01)^3, Stokeslets N(0,1)^3."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(np.exp(rng.uniform(np.log(2e4), np.log(2e5))))
+        v = rng.standard_normal((n, 3))
+        pts = v / np.linalg.norm(v, axis=1)[:, None] + rng.uniform(-0.01, 0.01, (n, 3))
+        out.append((pts, rng.standard_normal((n, 3))))
+    return out
+
+
+def stokes_direct(src, f, sel):
+    """FP64 Stokeslet velocities (1/8pi) sum_{j != i} [f_j/r + d(d.f_j)/r^3] at the sources sel."""
+    out = np.zeros((len(sel), 3))
+    for a in range(0, len(sel), 16):
+        idx = sel[a:a + 16]
+        d = src[idx, None, :] - src[None, :, :]
+        r2 = np.einsum("tsk,tsk->ts", d, d)
+        r2[np.arange(len(idx)), idx] = np.inf
+        ir = 1.0 / np.sqrt(r2)
+        df = np.einsum("tsk,sk->ts", d, f) * ir ** 3
+        out[a:a + 16] = (np.einsum("ts,sk->tk", ir, f) + np.einsum("ts,tsk->tk", df, d)) / (8 * np.pi)
+    return out
+
+
+def stokes_batched(fmmb, device, count, slots, p=16, ppl=200, samples=32):
+    """StokesHarmonics(Stokeslet3D(); p = 16) instances through the request server: all submitted
+    at once over `slots` streams (aggregate velocity evaluations/s), then one at a time on one
+    slot; per-instance relative L2 error of the velocities against FP64 direct sums at `samples`
+    sampled sources."""
+    reqs = stokes_workload(count)
+    total = sum(len(x) for x, _ in reqs)
+    srv = fmmb.Server(device, slots=slots)
+    for x, f in reqs[:2]:                                              # warm-up: operators resident
+        srv.wait(srv.submit_stokes(x, f, p=p, ppl=ppl))
+    t0 = time.perf_counter()
+    tk = [srv.submit_stokes(x, f, p=p, ppl=ppl) for x, f in reqs]
+    res = [srv.wait(k) for k in tk]
+    t_batch = time.perf_counter() - t0
+    srv.close()
+    one = fmmb.Server(device, slots=1)
+    one.wait(one.submit_stokes(*reqs[0], p=p, ppl=ppl))
+    t0 = time.perf_counter()
+    for x, f in reqs:
+        one.wait(one.submit_stokes(x, f, p=p, ppl=ppl))
+    t_seq = time.perf_counter() - t0
+    one.close()
+    rng = np.random.default_rng(50)
+    errs = []
+    for (x, f), (v, _, _) in zip(reqs, res):
+        sel = np.sort(rng.choice(len(x), samples, replace=False))
+        ud = stokes_direct(x, f, sel)
+        errs.append(float(np.linalg.norm(v[sel] - ud) / np.linalg.norm(ud)))
+    return {"instances": count, "points": total, "p": p, "ppl": ppl, "slots": slots, "precision": "fp64",
+            "workload": "N log-uniform [2e4, 2e5] jittered unit-sphere points, N(0,1)^3 Stokeslets (seed 5); each "
+                        "instance's box fitted to its own points and snapped to a power-of-two width",
+            "batched": {"evals_per_s": total / t_batch, "seconds": t_batch},
+            "one_at_a_time": {"evals_per_s": total / t_seq, "seconds": t_seq},
+            "error": {"samples_per_instance": samples, "max": max(errs), "median": float(np.median(errs))}}
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(a):
     import torch
@@ -405,6 +470,7 @@ def run_ours(a):
                "sample": f"full {a.n:,}-point matvec (the same points and charges), best of 2 after 1 warm-up, "
                          f"tree + operators {r['tree_s']:.2f} s untimed"}
     serve = serving(fmmb, local, a.serve_requests, a.serve_slots) if a.serve_requests > 0 else None
+    stokes = stokes_batched(fmmb, local, a.stokes_instances, a.serve_slots) if a.stokes_instances > 0 else None
     line = {
         "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -414,6 +480,7 @@ def run_ours(a):
                              "far_pairs": f.npairs}),
         "configured_order_p10": side,
         "serving": serve,
+        "stokes_batched": stokes,
         "latency_ms": {"p50": pct(0.5), "p99": pct(0.99)},
         "fp64": {"value": replica_throughput(a.n, ms_fp64, world), "ms_per_step": ms_fp64},
         "mixed_vs_fp64": ms_fp64 / ms_mixed,

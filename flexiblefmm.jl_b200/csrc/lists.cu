@@ -60,14 +60,15 @@ __global__ void k_pair_count(const int4* __restrict__ cell, const int* __restric
 // offsets, and the fill
 __global__ void k_block_fill(const int4* __restrict__ blocks, const int4* __restrict__ cell, const int* __restrict__ parent,
                              const int* __restrict__ cf, const int* __restrict__ col, const uint8_t* __restrict__ flags,
-                             int* __restrict__ cls_off, int2* __restrict__ pairs) {
+                             int* __restrict__ cls_off, int2* __restrict__ pairs, int TB) {
+  // blockDim.x = max(TB, 64) threads: the class scans below take one thread per class
   extern __shared__ int sm[];
-  const int TB = blockDim.x;
   int* cnt = sm;                 // [NCLASS][TB]
   int* tot = sm + NCLASS * TB;   // [NCLASS + 1]
   int4 b = blocks[blockIdx.x];
   int t = threadIdx.x;
-  for (int c = 0; c < NCLASS; ++c) cnt[c * TB + t] = 0;
+  if (t < TB)
+    for (int c = 0; c < NCLASS; ++c) cnt[c * TB + t] = 0;
   if (t < b.z)
     for_far_pairs(b.y + t, cell, parent, cf, col, flags, [&](int, int f) { cnt[c_class[f] * TB + t]++; });
   __syncthreads();
@@ -159,6 +160,14 @@ void build_lists(Plan& P) {
     FMMB_LAUNCH_CHECK();
   }
   std::vector<int> hc = to_host(cnt.p, n, s);
+  // targets per block: 128, halved (down to 16) while the targets with far pairs fill fewer
+  // blocks than the device has SMs, so that small trees still spread over the whole GPU
+  {
+    int64_t nt = 0;
+    for (int g = P.level_start[std::min(2, L)]; g < P.level_start[L]; ++g) nt += hc[g] > 0;
+    P.TB = 128;
+    while (P.TB > 16 && nt / P.TB < P.ctx->num_sms) P.TB /= 2;
+  }
   P.h_blocks.clear();
   P.level_pairs.assign(L, 0);
   int64_t base = 0;
@@ -183,7 +192,8 @@ void build_lists(Plan& P) {
   P.pairs.alloc(std::max<int64_t>(base, 1));
   if (nb) {
     size_t smem = sizeof(int) * (NCLASS * P.TB + NCLASS + 1);
-    k_block_fill<<<nb, P.TB, smem, s>>>(P.blocks.p, P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p, P.cls_off.p, P.pairs.p);
+    k_block_fill<<<nb, std::max(P.TB, 64), smem, s>>>(P.blocks.p, P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p,
+                                                    P.cls_off.p, P.pairs.p, P.TB);
     FMMB_LAUNCH_CHECK();
   }
   // per level factors

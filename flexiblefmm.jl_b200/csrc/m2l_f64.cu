@@ -41,7 +41,9 @@ template <int LD, int NB>
 __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks, const int* __restrict__ cls_off,
                                                  const int2* __restrict__ pairs, const double* __restrict__ reps,
                                                  const double* __restrict__ m2l_scale, int NP, const double* __restrict__ M,
-                                                 double* __restrict__ Pl, int64_t pitch, int comp, int psi) {
+                                                 double* __restrict__ Pl, int64_t pitch, int stokes) {
+  // the expansion block of this CTA; the Stokes Ψ̂ block (the fourth) adds the coupling
+  const int comp = blockIdx.y, psi = stokes && comp == 3;
   // row tiles per warp, column tiles; strides ≡ 4 (mod 16) doubles keep the fragment loads free
   // of shared-memory bank conflicts
   constexpr int BK = 16, MT = LD / 64, NT = NB / 8, GS = LD + 4, LDA = LD + 4, AL = (BK * LD + 255) / 256;
@@ -191,8 +193,8 @@ __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks
   }
 }
 
-// one launch per scalar block of the method (1 for Laplace3D; 4 for the Stokeslet: Φ₁..₃ and Ψ̂,
-// the last with the coupling), the blocks nexp·LD apart per node
+// the scalar blocks of the method (1 for Laplace3D; 4 for the Stokeslet: Φ₁..₃ and Ψ̂, the last
+// with the coupling), nexp·LD apart per node
 template <int LD, int NB>
 void launch(State& S) {
   Plan& P = *S.plan;
@@ -202,12 +204,12 @@ void launch(State& S) {
   const size_t smem = sizeof(double) * (16 * (LD + 4) + NB * (LD + 4)) + sizeof(int) * 3 * NB;
   auto kern = k_m2l_f64<LD, NB>;
   FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // one launch: blockIdx.x the target block, blockIdx.y the expansion block (the CTAs of different
+  // expansion blocks write disjoint slices of the targets' locals)
   const int nexp = C.nexp;
-  for (int comp = 0; comp < nexp; ++comp) {
-    kern<<<nb, 256, smem, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps.p, P.d_m2l_scale.p, C.np, S.M.p, S.Pl.p,
-                                           (int64_t)nexp * LD, comp, nexp == 4 && comp == 3);
-    FMMB_LAUNCH_CHECK();
-  }
+  kern<<<dim3(nb, nexp), 256, smem, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps.p, P.d_m2l_scale.p, C.np,
+                                                     S.M.p, S.Pl.p, (int64_t)nexp * LD, nexp == 4);
+  FMMB_LAUNCH_CHECK();
 }
 
 }  // namespace
