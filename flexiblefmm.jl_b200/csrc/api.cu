@@ -191,7 +191,19 @@ void plan_from_device_points(fmmb_cache* cache, const double* xyz, int64_t n, co
     int e = P.e0 - l;                       // the level's width is ldexp(cache W0, e)
     double lam = std::ldexp(1.0, e);        // w / W_ref (src/operators/harmonics.jl:414-418)
     P.scale[l] = e == 0 ? 1.0 / C.W0 : (1.0 / C.W0) / lam;
-    P.m2l_scale[l] = e == 0 ? 1.0 : 1.0 / lam;
+    // Yukawa3D is not homogeneous: its operators carry their width's c_K / w themselves
+    P.m2l_scale[l] = C.kernel == FMMB_KERNEL_YUKAWA3D ? 1.0 : (e == 0 ? 1.0 : 1.0 / lam);
+  }
+  // the translation operators of every level: the cache's (homogeneous kernels), or the
+  // level width's own (Yukawa3D, built on first use)
+  P.lv_reps.assign(P.L, C.reps.p);
+  P.lv_m2m.assign(P.L, C.m2m.p);
+  P.lv_l2l.assign(P.L, C.l2l.p);
+  if (C.kernel == FMMB_KERNEL_YUKAWA3D) yukawa_prepare(P);
+  {
+    std::vector<uint64_t> t(P.L);
+    for (int l = 0; l < P.L; ++l) t[l] = (uint64_t)(uintptr_t)P.lv_reps[l];
+    to_device(P.d_lv_reps, t, ctx.stream);
   }
   build_lists(P);
   h->parent = cache;
@@ -272,8 +284,10 @@ int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* m, fmmb_cache** out
   return guard([&] {
     require(ctx && m && out, FMMB_ERR_ARGUMENT, "null argument");
     require(m->method == FMMB_METHOD_SPHERICAL_HARMONICS, FMMB_ERR_UNSUPPORTED, "only SphericalHarmonics is provided");
-    require(m->kernel == FMMB_KERNEL_LAPLACE3D || m->kernel == FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED,
-            "the kernels provided are Laplace3D and Stokeslet3D");
+    require(m->kernel == FMMB_KERNEL_LAPLACE3D || m->kernel == FMMB_KERNEL_YUKAWA3D || m->kernel == FMMB_KERNEL_STOKESLET3D,
+            FMMB_ERR_UNSUPPORTED, "the kernels provided are Laplace3D, Yukawa3D and Stokeslet3D");
+    if (m->kernel == FMMB_KERNEL_YUKAWA3D)
+      require(std::isfinite(m->kappa) && m->kappa > 0, FMMB_ERR_ARGUMENT, "the Yukawa κ must be positive and finite");
     require(m->p >= 1, FMMB_ERR_ARGUMENT, "p must be at least 1");
     require(m->p <= PMAX, FMMB_ERR_UNSUPPORTED, "p above 20 is not provided");
     require(m->tol >= 0 && m->tol < 1, FMMB_ERR_ARGUMENT, "tol must lie in [0, 1)");
@@ -286,6 +300,7 @@ int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* m, fmmb_cache** out
     h->c.ld = ld_of(m->p);
     h->c.kernel = m->kernel;
     h->c.nexp = m->kernel == FMMB_KERNEL_STOKESLET3D ? 4 : 1;   // StokesHarmonics: Φ₁..₃, Ψ̂
+    h->c.kappa = m->kernel == FMMB_KERNEL_YUKAWA3D ? m->kappa : 0.0;
     std::lock_guard<std::mutex> lk(g_handles);
     ++ctx->deps;
     *out = h.release();
@@ -420,7 +435,7 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
     require(precision == FMMB_PRECISION_FP64 || precision == FMMB_PRECISION_MIXED, FMMB_ERR_ARGUMENT, "unknown precision path");
     Plan& P = plan->p;
     require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D || precision == FMMB_PRECISION_FP64, FMMB_ERR_UNSUPPORTED,
-            "the Stokeslet method runs on the FP64 path");
+            "the Stokeslet and Yukawa methods run on the FP64 path");
     set_device(*P.ctx);
     cudaStream_t s = P.ctx->stream;
     std::unique_ptr<fmmb_state> h(new fmmb_state());

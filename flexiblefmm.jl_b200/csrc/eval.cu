@@ -24,14 +24,15 @@ namespace {
 
 constexpr int NEAR_WARPS = 4;
 
-template <int P, typename R>
+// YK: Yukawa3D's weighted L2P (FP64), κ̂² = kh2[level]
+template <int P, typename R, bool YK>
 __global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, const int* __restrict__ gstart,
                                              const int* __restrict__ gcount, int ngroups, const double* __restrict__ tx,
                                              const double* __restrict__ ty, const double* __restrict__ tz,
                                              const int* __restrict__ tout, const int4* __restrict__ cell,
                                              const double* __restrict__ Pl, int LD, Geometry geo,
                                              const double* __restrict__ scale, int outputs, double* __restrict__ pot,
-                                             double* __restrict__ grad) {
+                                             double* __restrict__ grad, const double* __restrict__ kh2) {
   extern __shared__ __align__(16) unsigned char sl_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -49,7 +50,8 @@ __global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, cons
     const bool act = base + lane < nt;
     const double x = act ? tx[k] : cx, y = act ? ty[k] : cy, z = act ? tz[k] : cz;
     R u, gx, gy, gz;
-    l2p<P, R>(L, (R)((x - cx) * s), (R)((y - cy) * s), (R)((z - cz) * s), u, gx, gy, gz);
+    if constexpr (YK) l2p_yukawa<P>(L, kh2[c.w], (x - cx) * s, (y - cy) * s, (z - cz) * s, u, gx, gy, gz);
+    else l2p<P, R>(L, (R)((x - cx) * s), (R)((y - cy) * s), (R)((z - cz) * s), u, gx, gy, gz);
     if (act) {
       const int o = tout[k];
       if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = (double)u;
@@ -103,10 +105,12 @@ __device__ __forceinline__ void load_batch(const NearWarp<R>& sw, int b, int lan
   }
 }
 
-// one batch of m staged sources against this lane's target; CHECK skips flat index `is`
-template <typename R, bool CHECK>
+// one batch of m staged sources against this lane's target; CHECK skips flat index `is`.
+// YK (FP64): the Yukawa pair e^{−κr}/r and its radial derivative −e^{−κr}(1 + κr)/r²
+// (src/kernels.jl:235-242)
+template <typename R, bool CHECK, bool YK = false>
 __device__ __forceinline__ void near_batch(const R4<R>* __restrict__ stg, int m, int is, R fx, R fy, R fz, R& bp, R& bx,
-                                           R& by, R& bz) {
+                                           R& by, R& bz, double kappa = 0) {
   auto body = [&](int i) {
     const R4<R> sv = stg[i];
     const R dx = fx - sv.x, dy = fy - sv.y, dz = fz - sv.z;
@@ -119,8 +123,15 @@ __device__ __forceinline__ void near_batch(const R4<R>* __restrict__ stg, int m,
       ir = rsqrt_ftz(r2);
     }
     if (CHECK && i == is) ir = R(0);
-    const R qir = sv.w * ir;
-    const R qir3 = qir * ir * ir;
+    R qir, qir3;
+    if constexpr (YK) {
+      const double r = r2 * ir, e = exp(-kappa * r);
+      qir = sv.w * e * ir;
+      qir3 = qir * (1 + kappa * r) * ir * ir;
+    } else {
+      qir = sv.w * ir;
+      qir3 = qir * ir * ir;
+    }
     bp += qir;
     bx = fma(qir3, dx, bx);
     by = fma(qir3, dy, by);
@@ -135,7 +146,7 @@ __device__ __forceinline__ void near_batch(const R4<R>* __restrict__ stg, int m,
   }
 }
 
-template <typename R, bool SELF>
+template <typename R, bool SELF, bool YK>
 __global__ void __launch_bounds__(NEAR_WARPS * 32) k_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
                                                          const int* __restrict__ gcount, int ngroups,
                                                          const double* __restrict__ tx, const double* __restrict__ ty,
@@ -145,7 +156,7 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32) k_near(const int* __restrict_
                                                          const int4* __restrict__ cell, const int* __restrict__ plo,
                                                          const int* __restrict__ phi, const int* __restrict__ col,
                                                          Geometry geo, int outputs, double* __restrict__ pot,
-                                                         double* __restrict__ grad) {
+                                                         double* __restrict__ grad, double kappa) {
   constexpr bool REL = sizeof(R) == 4;   // the mixed path works relative to the leaf's centre
   __shared__ NearWarp<R> sws[NEAR_WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -202,8 +213,8 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32) k_near(const int* __restrict_
       const bool chk = SELF && selfm && 32 * b < pself + lenself && 32 * b + 32 > pself;   // uniform
       if constexpr (sizeof(R) == 8) {
         // the plain path sums straight into the FP64 totals, in the reference's order
-        if (chk) near_batch<R, true>(stg, m, fself - 32 * b, fx, fy, fz, np, nx, ny, nz);
-        else near_batch<R, false>(stg, m, 0, fx, fy, fz, np, nx, ny, nz);
+        if (chk) near_batch<R, true, YK>(stg, m, fself - 32 * b, fx, fy, fz, np, nx, ny, nz, kappa);
+        else near_batch<R, false, YK>(stg, m, 0, fx, fy, fz, np, nx, ny, nz, kappa);
       } else {
         R bp = 0, bx = 0, by = 0, bz = 0;
         if (chk) near_batch<R, true>(stg, m, fself - 32 * b, fx, fy, fz, bp, bx, by, bz);
@@ -234,20 +245,21 @@ void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount
   const int warps = 8;
   const bool mixed = S.precision == FMMB_PRECISION_MIXED;
   const size_t smem = (mixed ? sizeof(float) : sizeof(double)) * warps * P_.cache->ld;
-  auto kern = mixed ? k_l2p<P, float> : k_l2p<P, double>;
+  auto kern = mixed ? k_l2p<P, float, false>
+                    : (P_.cache->kernel == FMMB_KERNEL_YUKAWA3D ? k_l2p<P, double, true> : k_l2p<P, double, false>);
   kern<<<(ng + warps - 1) / warps, 32 * warps, smem, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, P_.cell.p,
                                                                       S.Pl.p, P_.cache->ld, geometry(P_), P_.d_scale.p,
-                                                                      outputs, pot, grad);
+                                                                      outputs, pot, grad, P_.d_kh2.p);
   FMMB_LAUNCH_CHECK();
 }
 
-template <typename R, bool SELF>
+template <typename R, bool SELF, bool YK = false>
 void launch_near(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
                  const double* tz, const int* tout, int outputs, double* pot, double* grad) {
   Plan& P_ = *S.plan;
-  k_near<R, SELF><<<(ng + NEAR_WARPS - 1) / NEAR_WARPS, 32 * NEAR_WARPS, 0, P_.ctx->stream>>>(
+  k_near<R, SELF, YK><<<(ng + NEAR_WARPS - 1) / NEAR_WARPS, 32 * NEAR_WARPS, 0, P_.ctx->stream>>>(
       gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p, S.zs.p, S.q.p, P_.cell.p, P_.plo.p, P_.phi.p, P_.col.p,
-      geometry(P_), outputs, pot, grad);
+      geometry(P_), outputs, pot, grad, P_.cache->kappa);
   FMMB_LAUNCH_CHECK();
 }
 
@@ -263,6 +275,12 @@ void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* g
     default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
   }
   const bool mixed = S.precision == FMMB_PRECISION_MIXED;
+  if (S.plan->cache->kernel == FMMB_KERNEL_YUKAWA3D) {
+    require(!mixed, FMMB_ERR_UNSUPPORTED, "Yukawa3D runs on the FP64 path");
+    if (self) launch_near<double, true, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+    else launch_near<double, false, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+    return;
+  }
   if (mixed && self) launch_near<float, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
   else if (mixed) launch_near<float, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
   else if (self) launch_near<double, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);

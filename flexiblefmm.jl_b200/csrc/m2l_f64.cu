@@ -39,7 +39,7 @@ __device__ __forceinline__ void dmma(double* d, double a, double b) {
 
 template <int LD, int NB>
 __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks, const int* __restrict__ cls_off,
-                                                 const int2* __restrict__ pairs, const double* __restrict__ reps,
+                                                 const int2* __restrict__ pairs, const uint64_t* __restrict__ reps_lv,
                                                  const double* __restrict__ m2l_scale, int NP, const double* __restrict__ M,
                                                  double* __restrict__ Pl, int64_t pitch, int stokes) {
   // the expansion block of this CTA; the Stokes Ψ̂ block (the fourth) adds the coupling
@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks
   const int kmax = (NP + BK - 1) / BK * BK;
   for (int c = 0; c < NCLASS; ++c) {
     const int a0 = co[c], a1 = co[c + 1];
-    const double* A = reps + (int64_t)c * LD * LD;
+    const double* A = reinterpret_cast<const double*>(reps_lv[b.x]) + (int64_t)c * LD * LD;   // the level's representatives
     for (int q0 = a0; q0 < a1; q0 += NB) {
       const int nc = min(NB, a1 - q0);
       __syncthreads();
@@ -207,7 +207,7 @@ void launch(State& S) {
   // one launch: blockIdx.x the target block, blockIdx.y the expansion block (the CTAs of different
   // expansion blocks write disjoint slices of the targets' locals)
   const int nexp = C.nexp;
-  kern<<<dim3(nb, nexp), 256, smem, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps.p, P.d_m2l_scale.p, C.np,
+  kern<<<dim3(nb, nexp), 256, smem, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, P.d_lv_reps.p, P.d_m2l_scale.p, C.np,
                                                      S.M.p, S.Pl.p, (int64_t)nexp * LD, nexp == 4);
   FMMB_LAUNCH_CHECK();
 }

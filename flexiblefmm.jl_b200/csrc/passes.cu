@@ -67,11 +67,14 @@ __global__ void k_gather_inputs(const double* __restrict__ xyz, const double* __
 // ---------------------------------------------------------------- P2M
 // one thread per (node, order m): M_n^m += τ conj Υ̃_n^m((y − c)/w) over the node's sources,
 // n = m..P, the chain of order m started from its own sectoral value (harmonics.jl:682-743)
-template <int P>
+// Yukawa3D (YK): the degree-n terms weighted by u_n(κ̂|x̂|), κ̂² = kh2[level]
+// (harmonics_yukawa.jl:281-296)
+template <int P, bool YK>
 __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restrict__ cell, const int* __restrict__ plo,
                       const int* __restrict__ phi, const double* __restrict__ xs, const double* __restrict__ ys,
                       const double* __restrict__ zs, const double* __restrict__ q, Geometry geo,
-                      const double* __restrict__ scale, int64_t pitch, double* __restrict__ M) {
+                      const double* __restrict__ scale, int64_t pitch, double* __restrict__ M,
+                      const double* __restrict__ kh2) {
   // the recurrence tables in shared memory: the lanes of a warp run different orders and would
   // serialise on the constant cache
   __shared__ double s_ab[2 * TRI_MAX];
@@ -88,6 +91,7 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
   int4 c = cell[node];
   double w = ldexp(geo.W0, -c.w), s = scale[c.w];
   double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const double k2 = YK ? kh2[c.w] : 0.0;
   double ar[P + 1], ai[P + 1];
 #pragma unroll
   for (int n = 0; n <= P; ++n) { ar[n] = 0; ai[n] = 0; }
@@ -102,18 +106,21 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
       sr = nr; si = ni;
     }
     double tau = q[j];
+    double u[P + 1];
+    if constexpr (YK) yukawa_u<P>(k2 * r2, u);
     double pr = 0, pi = 0, cr = 0, ci = 0;
 #pragma unroll
     for (int n = 0; n <= P; ++n) {
+      const double tn = YK ? tau * u[n] : tau;
       if (n == m) {
         cr = sr; ci = si; pr = 0; pi = 0;
-        ar[n] += tau * cr; ai[n] -= tau * ci;
+        ar[n] += tn * cr; ai[n] -= tn * ci;
       } else if (n > m) {
         int t = tri(n, m);
         double az = s_ab[t] * z, br = s_ab[TRI_MAX + t] * r2;
         double nr = az * cr - br * pr, ni = az * ci - br * pi;
         pr = cr; pi = ci; cr = nr; ci = ni;
-        ar[n] += tau * nr; ai[n] -= tau * ni;
+        ar[n] += tn * nr; ai[n] -= tn * ni;
       }
     }
   }
@@ -353,8 +360,9 @@ void launch_p2m(State& S, const double* q, double* M, int64_t pitch) {
   Plan& P_ = *S.plan;
   int nth = P_.n_s2m * (P + 1);
   if (nth == 0) return;
-  k_p2m<P><<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p, S.ys.p,
-                                                     S.zs.p, q, geometry(P_), P_.d_scale.p, pitch, M);
+  auto kern = P_.cache->kernel == FMMB_KERNEL_YUKAWA3D ? k_p2m<P, true> : k_p2m<P, false>;
+  kern<<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p, S.ys.p,
+                                                 S.zs.p, q, geometry(P_), P_.d_scale.p, pitch, M, P_.d_kh2.p);
   FMMB_LAUNCH_CHECK();
 }
 
@@ -388,7 +396,7 @@ void upload_operators(Cache& C) {
 
 void gather_inputs(State& S, const double* xyz_dev, const double* tau_dev) {
   Plan& P = *S.plan;
-  require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
+  require(P.cache->kernel != FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
   k_gather_inputs<<<nblk(P.N), 256, 0, P.ctx->stream>>>(xyz_dev, tau_dev, P.perm.p, P.N, S.xs.p, S.ys.p, S.zs.p, S.q.p);
   FMMB_LAUNCH_CHECK();
 }
@@ -427,7 +435,7 @@ int m2m_sweep(State& S) {
     int c0 = P.level_start[l + 1], ng = (P.level_start[l + 2] - c0) / NCH;
     if (ng == 0) continue;
     ColMap bm{S.M.p, nullptr, c0, NCH}, cm{S.M.p, P.group_parent[l + 1].p, 0, 0};
-    gemm_cols(C.ld, NCH * C.ld, C.m2m.p, bm, cm, ng, C.ld, C.np, 0, P.ctx->num_sms, s);
+    gemm_cols(C.ld, NCH * C.ld, P.lv_m2m[l], bm, cm, ng, C.ld, C.np, 0, P.ctx->num_sms, s);
     ++launches;
   }
   return launches;
@@ -448,7 +456,7 @@ int l2l_sweep(State& S) {
     int c0 = P.level_start[l], ng = (P.level_start[l + 1] - c0) / NCH;
     if (ng == 0) continue;
     ColMap bm{S.Pl.p, P.group_parent[l].p, 0, 0}, cm{S.Pl.p, nullptr, c0, NCH};
-    gemm_cols(NCH * C.ld, C.ld, C.l2l.p, bm, cm, ng, C.ld, C.np, 1, P.ctx->num_sms, s);
+    gemm_cols(NCH * C.ld, C.ld, P.lv_l2l[l - 1], bm, cm, ng, C.ld, C.np, 1, P.ctx->num_sms, s);
     ++launches;
   }
   return launches;
@@ -476,14 +484,14 @@ void downward_pass(State& S) {
 
 void evaluate_sources(State& S, int outputs, double* pot, double* grad) {
   Plan& P = *S.plan;
-  require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
+  require(P.cache->kernel != FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
   evaluate_groups(S, P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, S.xs.p, S.ys.p, S.zs.p, P.perm.p, true, outputs,
                   pot, grad);
 }
 
 void evaluate_targets(State& S, const double* tg, int64_t nt, int outputs, double* pot, double* grad) {
   Plan& P = *S.plan;
-  require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
+  require(P.cache->kernel != FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
   cudaStream_t s = P.ctx->stream;
   if (nt == 0) return;
   require(nt < (1ll << 31) - 1, FMMB_ERR_ARGUMENT, "too many targets");

@@ -88,6 +88,99 @@ __device__ __forceinline__ void l2p(const R* __restrict__ L, R x, R y, R z, R& u
   }
 }
 
+// Yukawa3D's radial factors u_n(z), n = 0..NM, from z² (harmonics_yukawa.jl:224-245): Miller's
+// backward recurrence u_n = u_{n+1} + z² u_{n+2}/((2n+3)(2n+5)) started at max(NM, ⌈z⌉) + 25 and
+// normalised with u_0 = sinh z / z; 1 + z²/(2(2n+3)) for z² < 1e-8
+template <int NM>
+__device__ __forceinline__ void yukawa_u(double z2, double (&u)[NM + 1]) {
+  if (z2 < 1e-8) {
+#pragma unroll
+    for (int n = 0; n <= NM; ++n) u[n] = 1 + z2 / (2 * (2 * n + 3));
+    return;
+  }
+  const double z = sqrt(z2);
+  const int N = max(NM, (int)ceil(z)) + 25;
+  double a = 0, b = 1;
+  for (int n = N - 1; n > NM; --n) {
+    const double c = b + z2 * a / (double)((2 * n + 3) * (2 * n + 5));
+    a = b;
+    b = c;
+  }
+#pragma unroll
+  for (int n = NM; n >= 0; --n) {
+    const double c = b + z2 * a / (double)((2 * n + 3) * (2 * n + 5));
+    u[n] = c;
+    a = b;
+    b = c;
+  }
+  const double s = (sinh(z) / z) / b;
+#pragma unroll
+  for (int n = 0; n <= NM; ++n) u[n] *= s;
+}
+
+// Yukawa3D's L2P at x̂ (harmonics_yukawa.jl:298-313): the potential Σ u_n(κ̂|x̂|) L_n^m conj Υ̃_n^m;
+// the gradient (before the 1/w factor) the Laplace identities weighted by u_n of the local's
+// degree, plus x̂ Σ κ̂² u_{n+1}/(2n+3) L_n^m conj Υ̃_n^m (from u_n'(z) = z u_{n+1}(z)/(2n+3))
+template <int P>
+__device__ __forceinline__ void l2p_yukawa(const double* __restrict__ L, double kh2, double x, double y, double z, double& u,
+                                           double& gx, double& gy, double& gz) {
+  const double r2 = x * x + y * y + z * z;
+  double w[P + 2];
+  yukawa_u<P + 1>(kh2 * r2, w);
+  double sr = 1, si = 0, rad = 0;
+  u = 0; gx = 0; gy = 0; gz = 0;
+#pragma unroll 1
+  for (int m = 0; m <= P; ++m) {
+    double pr = 0, pi = 0, cr = sr, ci = si;
+#pragma unroll
+    for (int n = 0; n <= P; ++n) {
+      if (n < m) continue;
+      double vr, vi;
+      if (n == m) { vr = sr; vi = si; }
+      else {
+        const int t = tri(n, m);
+        const double az = c_tab[t] * z, br = c_tab[TRI_MAX + t] * r2;
+        vr = az * cr - br * pr; vi = az * ci - br * pi;
+        pr = cr; pi = ci; cr = vr; ci = vi;
+      }
+      const double term = m == 0 ? L[n * n] * vr : 2 * (L[n * n + 2 * m - 1] * vr + L[n * n + 2 * m] * vi);
+      u += w[n] * term;
+      rad += kh2 * w[n + 1] / (2 * n + 3) * term;
+      if (n < P) {
+        const int n1 = n + 1;
+        const double wn = w[n1];
+        if (m == 0) {
+          const double cmv = c_tab[3 * TRI_MAX + tri(n1, 1)];
+          gx += wn * (-cmv * L[n1 * n1 + 1] * vr);
+          gy += wn * (-cmv * L[n1 * n1 + 2] * vr);
+          gz += wn * (c_tab[2 * TRI_MAX + tri(n1, 0)] * L[n1 * n1] * vr);
+        } else {
+          const double ur = L[n1 * n1 + 2 * (m + 1) - 1], ui = L[n1 * n1 + 2 * (m + 1)];
+          double dr, di;
+          if (m == 1) { dr = L[n1 * n1]; di = 0; }
+          else { dr = L[n1 * n1 + 2 * (m - 1) - 1]; di = L[n1 * n1 + 2 * (m - 1)]; }
+          const double cu = 0.5 * c_tab[3 * TRI_MAX + tri(n1, m + 1)], cd = 0.5 * c_tab[4 * TRI_MAX + tri(n1, m - 1)];
+          const double axr = -cu * ur + cd * dr, axi = -cu * ui + cd * di;
+          const double ayr = -(cu * ui + cd * di), ayi = cu * ur + cd * dr;
+          const double czv = c_tab[2 * TRI_MAX + tri(n1, m)];
+          const double zr = L[n1 * n1 + 2 * m - 1], zi = L[n1 * n1 + 2 * m];
+          gx += 2 * wn * (axr * vr + axi * vi);
+          gy += 2 * wn * (ayr * vr + ayi * vi);
+          gz += 2 * wn * czv * (zr * vr + zi * vi);
+        }
+      }
+    }
+    if (m < P) {
+      const double e = c_e[m];
+      const double nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
+      sr = nr; si = ni;
+    }
+  }
+  gx += x * rad;
+  gy += y * rad;
+  gz += z * rad;
+}
+
 // the orders with compiled kernels
 #define FMMB_P_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20)
 

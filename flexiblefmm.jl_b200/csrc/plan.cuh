@@ -1,5 +1,6 @@
 // The context, operator cache, plan (tree + lists) and state (expansions) of the library.
 #pragma once
+#include <map>
 #include <memory>
 #include <mutex>
 
@@ -12,6 +13,13 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int num_sms = 148;
+};
+
+// The Yukawa operators of one box width (src/operators/harmonics_yukawa.jl:164-207): the 34
+// class representatives with c_K / w folded in, M2M (children of width w/2 into the parent) and
+// L2L (the parent into its children), in the Laplace layouts.
+struct YukawaLevel {
+  DBuf<double> reps, m2m, l2l;
 };
 
 // OperatorCache (src/operators/cache.jl:5-83): the base width, the host operators at the base
@@ -36,6 +44,12 @@ struct Cache {
   DBuf<float> row_scale;
   DBuf<uint32_t> perm16;
   bool split_ready = false;
+  // Yukawa3D: κ, the operators per width (keyed by the exponent e of w = ldexp(W0, e), built
+  // on first use), and the sphere quadrature of the projections
+  double kappa = 0;
+  std::map<int, std::unique_ptr<YukawaLevel>> yk_levels;
+  DBuf<double> yk_xq, yk_wq;
+  int yk_nq = 0;
 };
 
 // One M2L work block: TB consecutive nodes of one level (the targets), their far pairs
@@ -79,6 +93,12 @@ struct Plan {
   int64_t npairs = 0;
   std::vector<int64_t> level_pairs;       // far pairs per level
   DBuf<double> d_scale, d_m2l_scale;      // per level
+  // the translation operators of each level (the cache's for the homogeneous kernels; the
+  // level's own width for Yukawa3D): M2L representatives, M2M into and L2L out of the level's
+  // nodes; the representatives' table on the device for the M2L kernel; Yukawa3D's κ̂² per level
+  std::vector<const double*> lv_reps, lv_m2m, lv_l2l;
+  DBuf<uint64_t> d_lv_reps;
+  DBuf<double> d_kh2;
 };
 
 struct State {
@@ -113,6 +133,9 @@ void evaluate_targets(State& S, const double* tg_dev, int64_t nt, int outputs, d
 void bounds(Ctx& ctx, const double* xyz_dev, int64_t n, double lo[3], double hi[3], int64_t* nonfinite);
 void direct(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
             int64_t nt, double* pot, double* grad);
+// yukawa.cu: SphericalHarmonics(Yukawa3D(κ)) — the operators of the plan's widths (built on the
+// device by projection when a width is first used) and the per-level factors
+void yukawa_prepare(Plan& P);
 // stokes.cu: StokesHarmonics(Stokeslet3D()) on the FP64 path
 void stokes_build(State& S, const double* xyz_dev, const double* f_dev);
 void stokes_evaluate_sources(State& S, double* vel_dev);

@@ -13,12 +13,14 @@
 // deterministic (its box is snapped from its own points to a power-of-two width), so its results
 // are the same alone and in any mix, on any slot.
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 
 #include "passes.cuh"
@@ -48,7 +50,8 @@ struct Job {
 // stays below it. Laplace3D potential: measured with the CPU oracle (ppl = 64, uniform and
 // 4-cluster points of 2·10⁵, uniform points of 10⁶ for p = 10..13; the worst of them).
 // Stokeslet3D velocity: measured on the device path (ppl = 64 and 200, 2·10⁵ points uniform in
-// the cube and on the jittered unit sphere; the worst of them).
+// the cube and on the jittered unit sphere; the worst of them). Yukawa3D takes the Laplace3D
+// table (the screening only lowers the far field's share of the error).
 int order_for_tol(double tol, int kernel) {
   static const double lap[PMAX + 1] = {1, 1, 9.5e-3, 3.1e-3, 1.0e-3, 3.6e-4, 1.3e-4, 5.6e-5, 2.4e-5, 7.6e-6, 3.8e-6,
                                        7.3e-7, 3.8e-7, 1.8e-7, 1.6e-7, 8.5e-8, 4.5e-8, 2.0e-8, 8.4e-9, 5.0e-9, 2.7e-9};
@@ -90,7 +93,7 @@ struct fmmb_server {
   bool stop = false;      // no new submissions
   bool stop_now = false;  // the workers leave
   std::vector<fmmb_ctx*> ctx;
-  std::vector<std::map<int, fmmb_cache*>> caches;
+  std::vector<std::map<std::tuple<int, int, double>, fmmb_cache*>> caches;   // per slot, by (kernel, p, κ)
   std::vector<std::thread> workers;
 };
 
@@ -103,10 +106,11 @@ int run_job(fmmb_server& S, int slot, Job& j, std::string& err) {
   fmmb_cache* cache = nullptr;
   {
     auto& cs = S.caches[slot];
-    const int key = kernel * 64 + j.p;
+    const double kappa = kernel == FMMB_KERNEL_YUKAWA3D ? j.r.kappa : 0.0;
+    const auto key = std::make_tuple(kernel, j.p, kappa);
     auto it = cs.find(key);
     if (it == cs.end()) {
-      fmmb_method_desc m{FMMB_METHOD_SPHERICAL_HARMONICS, kernel, j.p, 0, 0.0};
+      fmmb_method_desc m{FMMB_METHOD_SPHERICAL_HARMONICS, kernel, j.p, 0, 0.0, kappa};
       int rc = fmmb_cache_create(S.ctx[slot], &m, &cache);
       if (rc) { err = fmmb_last_error(); return rc; }
       // a request's box depends on its own points only (not on which request the slot's cache
@@ -201,8 +205,10 @@ int fmmb_server_create(int device, const fmmb_server_opts* opts, fmmb_server** o
 
 int fmmb_server_submit(fmmb_server* S, const fmmb_request* r, int64_t* ticket) {
   if (!S || !r || !ticket) return FMMB_ERR_ARGUMENT;
-  const bool stokes = r->kernel == FMMB_KERNEL_STOKESLET3D;
-  if (r->kernel != FMMB_KERNEL_LAPLACE3D && !stokes) return FMMB_ERR_UNSUPPORTED;
+  const bool stokes = r->kernel == FMMB_KERNEL_STOKESLET3D, yukawa = r->kernel == FMMB_KERNEL_YUKAWA3D;
+  if (r->kernel != FMMB_KERNEL_LAPLACE3D && !stokes && !yukawa) return FMMB_ERR_UNSUPPORTED;
+  if (yukawa && !(std::isfinite(r->kappa) && r->kappa > 0)) return FMMB_ERR_ARGUMENT;
+  if (yukawa && r->precision == FMMB_PRECISION_MIXED) return FMMB_ERR_UNSUPPORTED;
   if (!r->xyz || !r->tau || r->n <= 0 || r->ppl < 0) return FMMB_ERR_ARGUMENT;
   if (stokes) {
     // Stokeslets in tau (3×n), velocities in pot (3×n), on the FP64 path
@@ -219,7 +225,7 @@ int fmmb_server_submit(fmmb_server* S, const fmmb_request* r, int64_t* ticket) {
   j->p = r->p > 0 ? r->p : order_for_tol(r->tol, r->kernel);
   if (j->p < 1 || j->p > PMAX) return FMMB_ERR_ARGUMENT;
   // the precision path: FP64 below 1e-8 (or where the mixed path has no kernel), mixed above
-  if (stokes) j->precision = FMMB_PRECISION_FP64;
+  if (stokes || yukawa) j->precision = FMMB_PRECISION_FP64;   // the paths these kernels have
   else
     j->precision = r->precision >= 0 ? r->precision
                                      : ((r->tol < 1e-8 || (j->p + 1) * (j->p + 1) > 144) ? FMMB_PRECISION_FP64 : FMMB_PRECISION_MIXED);

@@ -30,6 +30,7 @@ PRECISION_MIXED = 1
 OUTPUT_POTENTIAL = 1
 OUTPUT_GRADIENT = 2
 KERNEL_LAPLACE3D = 1
+KERNEL_YUKAWA3D = 2
 KERNEL_STOKESLET3D = 3
 
 
@@ -55,7 +56,7 @@ class Unsupported(FMMBError, NotImplementedError):
 
 class _MethodDesc(C.Structure):
     _fields_ = [("method", C.c_int32), ("kernel", C.c_int32), ("p", C.c_int32), ("reserved", C.c_int32),
-                ("tol", C.c_double)]
+                ("tol", C.c_double), ("kappa", C.c_double)]
 
 
 class _TreeOpts(C.Structure):
@@ -70,7 +71,7 @@ class _ServerOpts(C.Structure):
 class _Request(C.Structure):
     _fields_ = [("xyz", C.c_void_p), ("tau", C.c_void_p), ("n", C.c_int64), ("tol", C.c_double), ("kernel", C.c_int32),
                 ("p", C.c_int32), ("outputs", C.c_int32), ("precision", C.c_int32), ("ppl", C.c_int32),
-                ("pot", C.c_void_p), ("grad", C.c_void_p)]
+                ("pot", C.c_void_p), ("grad", C.c_void_p), ("kappa", C.c_double)]
 
 
 class _RequestInfo(C.Structure):
@@ -176,6 +177,14 @@ class Laplace3D:
     c = 1.0 / (4.0 * np.pi)
 
 
+class Yukawa3D:
+    """Modified Helmholtz (Yukawa) Green's function e^{−k|t − s|}/(4π|t − s|) (src/kernels.jl:224-242)."""
+    c = 1.0 / (4.0 * np.pi)
+
+    def __init__(self, k):
+        self.k = float(k)
+
+
 class Stokeslet3D:
     """The 3D Stokeslet (1/8π)(f/r + d(d·f)/r³) (src/kernels.jl:253-272)."""
     c = 1.0 / (8.0 * np.pi)
@@ -199,8 +208,8 @@ class SphericalHarmonics:
     """SphericalHarmonics(kernel; p=16, tol=0) (src/operators/harmonics.jl:303-308)."""
 
     def __init__(self, kernel, p=16, tol=0.0):
-        if not isinstance(kernel, Laplace3D):
-            raise ArgumentError(1, "the device method is written for Laplace3D")
+        if not isinstance(kernel, (Laplace3D, Yukawa3D)):
+            raise ArgumentError(1, "the device method is written for Laplace3D and Yukawa3D")
         if p < 1:
             raise ArgumentError(1, "p must be at least 1")
         if not (0 <= tol < 1):
@@ -264,7 +273,13 @@ class OperatorCache:
     def __init__(self, method, ctx=None):
         self.method = method
         self.ctx = ctx or default_context()
-        d = _MethodDesc(1, 3 if isinstance(method, StokesHarmonics) else 1, method.p, 0, method.tol)
+        if isinstance(method, StokesHarmonics):
+            kernel, kappa = KERNEL_STOKESLET3D, 0.0
+        elif isinstance(method.kernel, Yukawa3D):
+            kernel, kappa = KERNEL_YUKAWA3D, method.kernel.k
+        else:
+            kernel, kappa = KERNEL_LAPLACE3D, 0.0
+        d = _MethodDesc(1, kernel, method.p, 0, method.tol, kappa)
         h = C.c_void_p()
         _check(lib().fmmb_cache_create(self.ctx._h, C.byref(d), C.byref(h)))
         self._h = h
@@ -463,10 +478,10 @@ class Server:
         self._h = h
         self._live = {}
 
-    def submit(self, sources, tau, tol=1e-6, p=0, precision=None, gradient=True, ppl=0):
-        """Queue one Laplace3D FMM at the sources (potential and, optionally, gradient, self
-        excluded); returns a ticket. precision None: chosen from tol (FP64 below 1e-8); ppl 0:
-        the server's."""
+    def submit(self, sources, tau, tol=1e-6, p=0, precision=None, gradient=True, ppl=0, kappa=None):
+        """Queue one Laplace3D FMM (or Yukawa3D(kappa), FP64) at the sources (potential and,
+        optionally, gradient, self excluded); returns a ticket. precision None: chosen from tol
+        (FP64 below 1e-8); ppl 0: the server's."""
         x = _points(sources)
         t = np.ascontiguousarray(tau, dtype=np.float64)
         if t.shape != (x.shape[0],):
@@ -475,8 +490,10 @@ class Server:
         grad = np.zeros((x.shape[0], 3)) if gradient else None
         prec = -1 if precision is None else {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}[precision]
         flags = OUTPUT_POTENTIAL | (OUTPUT_GRADIENT if gradient else 0)
-        r = _Request(x.ctypes.data, t.ctypes.data, x.shape[0], float(tol), KERNEL_LAPLACE3D, int(p), flags, prec,
-                     int(ppl), pot.ctypes.data, None if grad is None else grad.ctypes.data)
+        kernel = KERNEL_LAPLACE3D if kappa is None else KERNEL_YUKAWA3D
+        r = _Request(x.ctypes.data, t.ctypes.data, x.shape[0], float(tol), kernel, int(p), flags, prec,
+                     int(ppl), pot.ctypes.data, None if grad is None else grad.ctypes.data,
+                     0.0 if kappa is None else float(kappa))
         return self._submit(r, (x, t, pot, grad))
 
     def submit_stokes(self, sources, stokeslets, tol=1e-6, p=0, ppl=0):

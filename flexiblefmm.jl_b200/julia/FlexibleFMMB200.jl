@@ -13,7 +13,7 @@
 # interleaved array the ABI takes); outputs come back in the original order.
 module FlexibleFMMB200
 
-using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, Laplace3D, Stokeslet3D, Potential, Gradient
+using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, Laplace3D, Yukawa3D, Stokeslet3D, Potential, Gradient
 using StaticArrays: SVector
 
 const libfmmb = get(ENV, "FMMB_LIB", joinpath(@__DIR__, "..", "libfmmb.so"))
@@ -29,6 +29,7 @@ struct MethodDesc
     p::Int32
     reserved::Int32
     tol::Float64
+    kappa::Float64
 end
 
 struct TreeOpts
@@ -64,8 +65,10 @@ default_context() = something(DEFAULT_CONTEXT[], (DEFAULT_CONTEXT[] = Context(0)
     OperatorCache(method)  (src/operators/cache.jl:19-22)
 """
 const DeviceMethod = Union{SphericalHarmonics,StokesHarmonics}
-_kernel_id(m::SphericalHarmonics) = m.kernel isa Laplace3D ? Int32(1) :
-    throw(ArgumentError("the device method is written for Laplace3D"))
+_kernel_id(m::SphericalHarmonics) = m.kernel isa Laplace3D ? Int32(1) : m.kernel isa Yukawa3D ? Int32(2) :
+    throw(ArgumentError("the device method is written for Laplace3D and Yukawa3D"))
+_kappa(m::SphericalHarmonics) = m.kernel isa Yukawa3D ? Float64(m.kernel.k) : 0.0
+_kappa(m::StokesHarmonics) = 0.0
 _kernel_id(m::StokesHarmonics) = m.kernel isa Stokeslet3D ? Int32(3) :
     throw(ArgumentError("the device Stokes method is written for Stokeslet3D"))
 
@@ -74,7 +77,7 @@ mutable struct OperatorCache
     ctx::Context
     h::Ptr{Cvoid}
     function OperatorCache(m::DeviceMethod; ctx::Context=default_context())
-        d = Ref(MethodDesc(1, _kernel_id(m), Int32(m.p), 0, m isa SphericalHarmonics ? m.tol : 0.0))
+        d = Ref(MethodDesc(1, _kernel_id(m), Int32(m.p), 0, m isa SphericalHarmonics ? m.tol : 0.0, _kappa(m)))
         r = Ref{Ptr{Cvoid}}(C_NULL)
         check(ccall((:fmmb_cache_create, libfmmb), Cint, (Ptr{Cvoid}, Ref{MethodDesc}, Ref{Ptr{Cvoid}}), ctx.h, d, r))
         c = new(m, ctx, r[])
@@ -173,6 +176,7 @@ struct ServerOpts; slots::Int32; ppl::Int32; hbm_budget::Int64; end
 struct Request
     xyz::Ptr{Float64}; tau::Ptr{Float64}; n::Int64; tol::Float64; kernel::Int32; p::Int32
     outputs::Int32; precision::Int32; ppl::Int32; pot::Ptr{Float64}; grad::Ptr{SVector{3,Float64}}
+    kappa::Float64
 end
 struct RequestInfo
     status::Int32; p::Int32; precision::Int32; slot::Int32
@@ -195,13 +199,17 @@ mutable struct Server
     end
 end
 
-function submit(s::Server, sources::AbstractVector{SVector{3,Float64}}, τ::AbstractVector{Float64}; tol::Real=1e-6)
+"""`submit(server, sources, τ; tol, kappa=nothing)`: a Laplace3D FMM, or Yukawa3D(kappa) on the FP64
+path, at the sources (potential and gradient, self excluded)."""
+function submit(s::Server, sources::AbstractVector{SVector{3,Float64}}, τ::AbstractVector{Float64}; tol::Real=1e-6,
+                kappa::Union{Nothing,Real}=nothing)
     length(τ) == length(sources) || throw(DimensionMismatch("one charge per source"))
     x, t = collect(sources), collect(τ)
     pot = Vector{Float64}(undef, length(x))
     grad = Vector{SVector{3,Float64}}(undef, length(x))
     req = Request(Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, x))), pointer(t), length(x), tol,
-                  1, 0, 3, -1, 0, pointer(pot), pointer(grad))
+                  kappa === nothing ? 1 : 2, 0, 3, -1, 0, pointer(pot), pointer(grad),
+                  kappa === nothing ? 0.0 : Float64(kappa))
     return _submit(s, req, (x, t, pot, grad))
 end
 
@@ -214,7 +222,7 @@ function submit_stokes(s::Server, sources::AbstractVector{SVector{3,Float64}}, f
     vel = Vector{SVector{3,Float64}}(undef, length(x))
     req = Request(Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, x))),
                   Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, fs))), length(x), tol, 3, p, 0, -1, ppl,
-                  Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, vel))), C_NULL)
+                  Base.unsafe_convert(Ptr{Float64}, pointer(reinterpret(Float64, vel))), C_NULL, 0.0)
     return _submit(s, req, (x, fs, vel, nothing))
 end
 

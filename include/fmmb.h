@@ -33,6 +33,7 @@ extern "C" {
 #define FMMB_ERR_UNSUPPORTED 6 /* a method, kernel, density or output this build does not provide */
 
 #define FMMB_KERNEL_LAPLACE3D 1
+#define FMMB_KERNEL_YUKAWA3D 2    /* e^{−κr}/(4πr), SphericalHarmonics(Yukawa3D(κ); p): FP64 path, operators per width */
 #define FMMB_KERNEL_STOKESLET3D 3 /* StokesHarmonics(Stokeslet3D(); p): FP64 path, Stokeslet densities, velocities */
 #define FMMB_METHOD_SPHERICAL_HARMONICS 1
 
@@ -47,14 +48,16 @@ typedef struct fmmb_cache fmmb_cache;
 typedef struct fmmb_plan fmmb_plan;
 typedef struct fmmb_state fmmb_state;
 
-/* The method: SphericalHarmonics(Laplace3D(); p) (src/operators/harmonics.jl:303-308), or with kernel
- * FMMB_KERNEL_STOKESLET3D StokesHarmonics(Stokeslet3D(); p) (src/operators/harmonics_stokes.jl:34-45). */
+/* The method: SphericalHarmonics(Laplace3D(); p) (src/operators/harmonics.jl:303-308); with kernel
+ * FMMB_KERNEL_YUKAWA3D SphericalHarmonics(Yukawa3D(kappa); p) (src/operators/harmonics_yukawa.jl:27-32);
+ * with FMMB_KERNEL_STOKESLET3D StokesHarmonics(Stokeslet3D(); p) (src/operators/harmonics_stokes.jl:34-45). */
 typedef struct {
   int32_t method;  /* FMMB_METHOD_SPHERICAL_HARMONICS */
-  int32_t kernel;  /* FMMB_KERNEL_LAPLACE3D */
+  int32_t kernel;  /* FMMB_KERNEL_* */
   int32_t p;       /* expansion degree, 1..20 */
   int32_t reserved;
   double tol;      /* 0: dense class operators (the only form this build provides) */
+  double kappa;    /* the Yukawa screening κ > 0 (FMMB_KERNEL_YUKAWA3D); ignored otherwise */
 } fmmb_method_desc;
 
 /* Tree options: FMM(m, sources; ppl, bbox, max_levels) (src/fmm.jl:31-49). */
@@ -179,7 +182,8 @@ typedef struct {
   const double* tau;   /* n host charges (Laplace3D); 3×n Stokeslets (Stokeslet3D) */
   int64_t n;
   double tol;          /* requested relative accuracy: selects p (when p = 0) and the precision path */
-  int32_t kernel;      /* FMMB_KERNEL_LAPLACE3D, or FMMB_KERNEL_STOKESLET3D (velocities at the sources) */
+  int32_t kernel;      /* FMMB_KERNEL_LAPLACE3D, FMMB_KERNEL_YUKAWA3D (FP64), or FMMB_KERNEL_STOKESLET3D
+                          (velocities at the sources) */
   int32_t p;           /* 0: the smallest order whose measured error is below tol */
   int32_t outputs;     /* FMMB_OUTPUT_* bits (Laplace3D) */
   int32_t precision;   /* -1: FP64 for tol < 1e-8 or p > 11, else the mixed path (Stokeslet3D: FP64) */
@@ -187,6 +191,7 @@ typedef struct {
   double* pot;         /* n host potentials, or 3×n velocities; written when the request completes
                           (keep valid until then) */
   double* grad;        /* 3×n host */
+  double kappa;        /* the Yukawa screening κ (FMMB_KERNEL_YUKAWA3D) */
 } fmmb_request;
 typedef struct {
   int32_t status;      /* the request's own status (FMMB_OK or an error code) */

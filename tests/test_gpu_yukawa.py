@@ -1,0 +1,93 @@
+"""SphericalHarmonics(Yukawa3D(κ); p) on the device (FP64 path), as the reference's Yukawa
+tests check it (test/test_harmonics_yukawa.jl): the FMM end to end against FP64 direct sums of
+e^{−κr}/(4πr) (κ = 4, p = 16, ppl = 40, N = 5000 in the unit box: potential at the sources and
+at targets within 1e-5, gradient at targets within 1e-4, max-norm relative), and the Laplace
+limit (a tiny κ reproduces the Laplace3D FMM, whose path is pinned to the oracle)."""
+import numpy as np
+import pytest
+
+from helpers import clustered3, helix3, mrd, uniform3
+
+pytestmark = pytest.mark.gpu
+
+
+def yukawa_direct(src, tau, tgt, kappa, self_excluded=False, gradient=False):
+    """FP64 Σ_j τ_j e^{−κr}/(4πr) (and its gradient in the target) at tgt, in chunks."""
+    pot = np.zeros(len(tgt))
+    grad = np.zeros((len(tgt), 3))
+    for a in range(0, len(tgt), 256):
+        d = tgt[a:a + 256, None, :] - src[None, :, :]
+        r = np.sqrt(np.einsum("tsk,tsk->ts", d, d))
+        if self_excluded:
+            r[np.arange(len(r)), np.arange(a, a + len(r))] = np.inf
+        e = np.exp(-kappa * r) / r
+        pot[a:a + 256] = e @ tau / (4 * np.pi)
+        if gradient:
+            g = -(e * (1 + kappa * r) / r ** 2) * tau[None, :]
+            grad[a:a + 256] = np.einsum("ts,tsk->tk", g, d) / (4 * np.pi)
+    return (pot, grad) if gradient else pot
+
+
+@pytest.mark.parametrize("gen", [uniform3, helix3, clustered3])
+def test_yukawa_fmm_against_direct(fmmb, gen):
+    rng = np.random.default_rng(52)
+    n, kappa = 5000, 4.0
+    pts = gen(rng, n)
+    tau = rng.standard_normal(n)
+    tg = rng.random((400, 3))
+    m = fmmb.SphericalHarmonics(fmmb.Yukawa3D(kappa), p=16)
+    f = fmmb.FMM(m, pts, ppl=40, bbox=((0.0, 0.0, 0.0), 1.0))
+    assert f.nlevels >= 3
+    st = fmmb.build_expansions(f, pts, tau)
+    u = fmmb.evaluate_at_sources(f, st)
+    assert mrd(u, yukawa_direct(pts, tau, pts, kappa, self_excluded=True)) < 1e-5
+    ut = fmmb.evaluate(f, st, tg)
+    gt = fmmb.evaluate(f, st, tg, output=fmmb.Gradient())
+    dp, dg = yukawa_direct(pts, tau, tg, kappa, gradient=True)
+    assert mrd(ut, dp) < 1e-5
+    assert mrd(gt, dg) < 1e-4
+
+
+def test_yukawa_gradient_at_sources(fmmb):
+    rng = np.random.default_rng(4)
+    n, kappa = 20000, 5.0                                               # p = 12: the order of tol 1e-6
+    pts = uniform3(rng, n)
+    tau = rng.standard_normal(n)
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Yukawa3D(kappa), p=12), pts, ppl=64, bbox=((0.0, 0.0, 0.0), 1.0))
+    st = fmmb.build_expansions(f, pts, tau)
+    u, g = fmmb.evaluate_at_sources_both(f, st)
+    sel = np.sort(rng.choice(n, 200, replace=False))
+    d = pts[sel, None, :] - pts[None, :, :]
+    r = np.sqrt(np.einsum("tsk,tsk->ts", d, d))
+    r[np.arange(len(sel)), sel] = 1.0                                  # the self terms, dropped below
+    e = np.exp(-kappa * r) / r
+    e[np.arange(len(sel)), sel] = 0.0
+    du = e @ tau / (4 * np.pi)
+    dg = np.einsum("ts,tsk->tk", -(e * (1 + kappa * r) / r ** 2) * tau[None, :], d) / (4 * np.pi)
+    assert mrd(u[sel], du) < 5e-6
+    assert mrd(g[sel], dg) < 5e-5
+
+
+def test_yukawa_laplace_limit(fmmb):
+    """κ = 1e-10: the Yukawa operators (built by projection on the device) and radial weights
+    reduce to the exact Laplace ones; the FMMs agree to the kernels' own difference."""
+    rng = np.random.default_rng(3)
+    n = 20000
+    pts = uniform3(rng, n)
+    tau = rng.standard_normal(n)
+    out = []
+    for k in (fmmb.Yukawa3D(1e-10), fmmb.Laplace3D()):
+        f = fmmb.FMM(fmmb.SphericalHarmonics(k, p=8), pts, ppl=64, bbox=((0.0, 0.0, 0.0), 1.0))
+        assert f.nlevels >= 4
+        out.append(fmmb.evaluate_at_sources_both(f, fmmb.build_expansions(f, pts, tau)))
+    assert mrd(out[0][0], out[1][0]) < 1e-9
+    assert mrd(out[0][1], out[1][1]) < 1e-9
+
+
+def test_yukawa_errors(fmmb):
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.OperatorCache(fmmb.SphericalHarmonics(fmmb.Yukawa3D(-1.0), p=6))
+    pts = np.random.default_rng(1).random((3000, 3))
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Yukawa3D(2.0), p=6), pts, ppl=64)
+    with pytest.raises(fmmb.Unsupported):
+        fmmb.FMMState(f, "mixed")
