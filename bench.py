@@ -176,20 +176,21 @@ class Clocks:
 
 # ---------------------------------------------------------------- the serving loop
 def serving_workload(count, seed=6):
-    """Requests as the serving configuration draws them: N log-uniform in [1e3, 5e5], points
-    uniform in the unit cube or from 4 Gaussians (σ = 0.02) with equal probability, charges
-    N(0,1), tolerance from {1e-3, 1e-6, 1e-9}. The configuration's Yukawa3D(κ=5) half runs as
-    Laplace3D: the device path provides Laplace3D only."""
+    """Requests as the serving configuration draws them: Laplace3D or Yukawa3D(kappa = 5) with
+    equal probability, N log-uniform in [1e3, 5e5], points uniform in the unit cube or from 4
+    Gaussians (sigma = 0.02) with equal probability, charges N(0,1), tolerance from
+    {1e-3, 1e-6, 1e-9}. Each request is (points, charges, tol, kappa or None)."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
+        kappa = 5.0 if rng.random() < 0.5 else None
         n = int(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
         if rng.random() < 0.5:
             pts = rng.random((n, 3))
         else:
             c = 0.1 + 0.8 * rng.random((4, 3))
             pts = np.clip(c[rng.integers(0, 4, n)] + 0.02 * rng.standard_normal((n, 3)), 0.0, 1.0)
-        out.append((pts, rng.standard_normal(n), float(rng.choice([1e-3, 1e-6, 1e-9]))))
+        out.append((pts, rng.standard_normal(n), float(rng.choice([1e-3, 1e-6, 1e-9])), kappa))
     return out
 
 
@@ -200,10 +201,10 @@ def serving(fmmb, device, count, slots):
     reqs = serving_workload(count)
     total = sum(len(r[0]) for r in reqs)
     srv = fmmb.Server(device, slots=slots)
-    for pts, tau, tol in reqs[:6]:                                     # warm-up: operators resident
-        srv.wait(srv.submit(pts, tau, tol=tol))
+    for pts, tau, tol, kappa in reqs[:6]:                              # warm-up: operators resident
+        srv.wait(srv.submit(pts, tau, tol=tol, kappa=kappa))
     t0 = time.perf_counter()
-    tk = [srv.submit(pts, tau, tol=tol) for pts, tau, tol in reqs]
+    tk = [srv.submit(pts, tau, tol=tol, kappa=kappa) for pts, tau, tol, kappa in reqs]
     infos = [srv.wait(k)[2] for k in tk]
     t_batch = time.perf_counter() - t0
     rate = 0.8 * count / t_batch                                       # requests/s offered in the open loop
@@ -212,33 +213,35 @@ def serving(fmmb, device, count, slots):
     t0 = time.perf_counter()
     tk = []
     due = t0
-    for (pts, tau, tol), g in zip(reqs, gaps):
+    for (pts, tau, tol, kappa), g in zip(reqs, gaps):
         due += g
         while time.perf_counter() < due:
             time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
-        tk.append(srv.submit(pts, tau, tol=tol))
+        tk.append(srv.submit(pts, tau, tol=tol, kappa=kappa))
     lat = [srv.wait(k)[2]["latency_s"] for k in tk]
     t_open = time.perf_counter() - t0
     srv.close()
     one = fmmb.Server(device, slots=1)
-    for pts, tau, tol in reqs[:3]:
-        one.wait(one.submit(pts, tau, tol=tol, precision="fp64"))
+    for pts, tau, tol, kappa in reqs[:3]:
+        one.wait(one.submit(pts, tau, tol=tol, precision="fp64", kappa=kappa))
     t0 = time.perf_counter()
     seq_lat = []
-    for pts, tau, tol in reqs:
-        seq_lat.append(one.wait(one.submit(pts, tau, tol=tol, precision="fp64"))[2]["latency_s"])
+    for pts, tau, tol, kappa in reqs:
+        seq_lat.append(one.wait(one.submit(pts, tau, tol=tol, precision="fp64", kappa=kappa))[2]["latency_s"])
     t_seq = time.perf_counter() - t0
     one.close()
     q = lambda v, f: float(np.quantile(np.asarray(v) * 1e3, f))
     return {"requests": count, "slots": slots, "points": total,
-            "workload": "N log-uniform [1e3, 5e5], uniform or 4-Gaussian (sigma 0.02) points, tol in {1e-3, 1e-6, 1e-9} "
-                        "(p and precision path chosen from tol), Laplace3D in place of the Yukawa3D half (seed 6)",
+            "workload": "Laplace3D or Yukawa3D(kappa=5) 50/50, N log-uniform [1e3, 5e5], uniform or 4-Gaussian (sigma 0.02) "
+                        "points, tol in {1e-3, 1e-6, 1e-9} (p and precision path chosen from tol; Yukawa on the FP64 "
+                        "path) (seed 6)",
             "batched": {"evals_per_s": total / t_batch, "requests_per_s": count / t_batch, "seconds": t_batch},
             "open_loop": {"offered_requests_per_s": rate, "evals_per_s": total / t_open,
                           "fraction_of_batched": (total / t_open) / (total / t_batch),
                           "latency_ms": {"p50": q(lat, 0.5), "p99": q(lat, 0.99)}},
             "one_at_a_time_fp64": {"evals_per_s": total / t_seq, "latency_ms": {"p50": q(seq_lat, 0.5), "p99": q(seq_lat, 0.99)}},
-            "paths": {"mixed": sum(i["precision"] == "mixed" for i in infos), "fp64": sum(i["precision"] == "fp64" for i in infos)}}
+            "paths": {"mixed": sum(i["precision"] == "mixed" for i in infos), "fp64": sum(i["precision"] == "fp64" for i in infos),
+                      "yukawa": sum(r[3] is not None for r in reqs)}}
 
 # ---------------------------------------------------------------- batched Stokes
 def stokes_workload(count, seed=5):

@@ -44,10 +44,11 @@ struct Cache {
   DBuf<float> row_scale;
   DBuf<uint32_t> perm16;
   bool split_ready = false;
-  // Yukawa3D: κ, the operators per width (keyed by the exponent e of w = ldexp(W0, e), built
-  // on first use), and the sphere quadrature of the projections
+  // Yukawa3D: κ, the operators per width (keyed by the exponent e of w = ldexp(W0, e); built on
+  // first use and shared by every cache of the same device, order, κ and width), and the sphere
+  // quadrature of the projections
   double kappa = 0;
-  std::map<int, std::unique_ptr<YukawaLevel>> yk_levels;
+  std::map<int, std::shared_ptr<YukawaLevel>> yk_levels;
   DBuf<double> yk_xq, yk_wq;
   int yk_nq = 0;
 };

@@ -13,9 +13,12 @@
 // computed on the host and everything else on the device in FP64: the basis of each translated
 // sphere (one thread per quadrature point) and the projections, which are GEMMs of
 // (p+1)² × (2p+10)(4p+20) by (2p+10)(4p+20) × (p+1)² on the FP64 tensor cores (the same DMMA
-// GEMM as M2M and L2L). Each width's operators are built once per operator cache, when a plan
-// first needs that width.
+// GEMM as M2M and L2L). Each width's operators are built once, when a plan first needs that
+// width, and kept in a process-wide store shared by the operator caches of the same device,
+// order and κ.
 #include <cmath>
+#include <map>
+#include <tuple>
 
 #include "passes.cuh"
 
@@ -243,6 +246,56 @@ void build_level(Cache& C, int e, YukawaLevel& out, cudaStream_t s) {
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
 
+// the operators of every width built so far, by (device, p, κ, width): caches on different
+// contexts (the request server's slots, successive servers) share them rather than rebuilding.
+// The store keeps them after their last cache is gone, up to STORE_BYTES; beyond that the
+// oldest that no cache holds are released.
+constexpr size_t STORE_BYTES = size_t(4) << 30;
+std::mutex g_store_mu;
+std::map<std::tuple<int, int, double, double>, std::shared_ptr<YukawaLevel>> g_store;
+std::vector<std::tuple<int, int, double, double>> g_store_order;   // insertion order
+size_t g_store_bytes = 0;
+
+size_t level_bytes(const YukawaLevel& lv) { return lv.reps.bytes() + lv.m2m.bytes() + lv.l2l.bytes(); }
+
+void store_trim() {
+  for (size_t i = 0; i < g_store_order.size() && g_store_bytes > STORE_BYTES;) {
+    auto it = g_store.find(g_store_order[i]);
+    if (it != g_store.end() && it->second.use_count() == 1) {
+      g_store_bytes -= level_bytes(*it->second);
+      g_store.erase(it);
+      g_store_order.erase(g_store_order.begin() + i);
+    } else {
+      ++i;
+    }
+  }
+}
+
+std::shared_ptr<YukawaLevel> level_operators(Cache& C, int e, cudaStream_t s) {
+  const auto key = std::make_tuple(C.ctx->device, C.p, C.kappa, std::ldexp(C.W0, e));
+  std::lock_guard<std::mutex> lk(g_store_mu);
+  auto it = g_store.find(key);
+  if (it != g_store.end()) return it->second;
+  // allocated outside the stream-ordered pool (freed by whichever cache releases it last)
+  const cudaStream_t keep = g_alloc_stream;
+  g_alloc_stream = nullptr;
+  std::shared_ptr<YukawaLevel> lv;
+  try {
+    lv = std::make_shared<YukawaLevel>();
+    build_level(C, e, *lv, s);
+  } catch (...) {
+    lv.reset();
+    g_alloc_stream = keep;
+    throw;
+  }
+  g_alloc_stream = keep;
+  g_store[key] = lv;
+  g_store_order.push_back(key);
+  g_store_bytes += level_bytes(*lv);
+  store_trim();
+  return lv;
+}
+
 }  // namespace
 
 void yukawa_prepare(Plan& P) {
@@ -258,11 +311,7 @@ void yukawa_prepare(Plan& P) {
       kh2[l] = kh * kh;
       if (l < 2) continue;                          // no translations touch levels 0 and 1
       auto it = C.yk_levels.find(e);
-      if (it == C.yk_levels.end()) {
-        std::unique_ptr<YukawaLevel> lv(new YukawaLevel());
-        build_level(C, e, *lv, s);
-        it = C.yk_levels.emplace(e, std::move(lv)).first;
-      }
+      if (it == C.yk_levels.end()) it = C.yk_levels.emplace(e, level_operators(C, e, s)).first;
       P.lv_reps[l] = it->second->reps.p;
       P.lv_m2m[l] = it->second->m2m.p;
       P.lv_l2l[l] = it->second->l2l.p;

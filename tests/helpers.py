@@ -178,3 +178,21 @@ def stokes_direct(src, f, sel):
         df = np.einsum("tsk,sk->ts", d, f) * ir ** 3
         out[a:a + 64] = (np.einsum("ts,sk->tk", ir, f) + np.einsum("ts,tsk->tk", df, d)) / (8 * np.pi)
     return out
+
+
+# ---------------------------------------------------------------- Yukawa (src/kernels.jl:224-242)
+def yukawa_direct(src, tau, tgt, kappa, self_excluded=False, gradient=False):
+    """FP64 Σ_j τ_j e^{−κr}/(4πr) (and its gradient in the target) at tgt, in chunks."""
+    pot = np.zeros(len(tgt))
+    grad = np.zeros((len(tgt), 3))
+    for a in range(0, len(tgt), 256):
+        d = tgt[a:a + 256, None, :] - src[None, :, :]
+        r = np.sqrt(np.einsum("tsk,tsk->ts", d, d))
+        if self_excluded:
+            r[np.arange(len(r)), np.arange(a, a + len(r))] = np.inf
+        e = np.exp(-kappa * r) / r
+        pot[a:a + 256] = e @ tau / (4 * np.pi)
+        if gradient:
+            g = -(e * (1 + kappa * r) / r ** 2) * tau[None, :]
+            grad[a:a + 256] = np.einsum("ts,tsk->tk", g, d) / (4 * np.pi)
+    return (pot, grad) if gradient else pot

@@ -102,3 +102,27 @@ def test_server_stokes_requests_mixed_with_laplace(fmmb):
         sel = np.sort(rng.choice(len(x), 200, replace=False))
         err = rel_l2(v[sel], stokes_direct(x, f, sel))
         assert err < 3 * tol, (len(x), tol, info["p"], err)
+
+
+def test_server_yukawa_requests(fmmb):
+    """Yukawa3D(κ = 5) requests among Laplace ones (the serving workload's other half): FP64
+    path, each result bitwise the same alone, within 3·tol of FP64 direct sums."""
+    from helpers import yukawa_direct
+    reqs = _requests(12, 6, 2000, 40000)
+    srv = fmmb.Server(0, slots=4)
+    tickets = [srv.submit(p, t, tol=tol, kappa=5.0 if i % 2 == 0 else None) for i, (p, t, tol) in enumerate(reqs)]
+    mixed = [srv.wait(k) for k in tickets]
+    alone = [srv.wait(srv.submit(p, t, tol=tol, kappa=5.0)) for i, (p, t, tol) in enumerate(reqs) if i % 2 == 0]
+    srv.close()
+    rng = np.random.default_rng(1)
+    for (pts, tau, tol), (u, g, info), (ua, ga, _) in zip(reqs[::2], mixed[::2], alone):
+        assert info["precision"] == "fp64" and info["status"] == 0
+        assert np.array_equal(u, ua) and np.array_equal(g, ga)
+        sel = np.sort(rng.choice(len(pts), 300, replace=False))
+        du = np.zeros(len(sel))
+        for k, i in enumerate(sel):                      # self excluded
+            m = np.ones(len(pts), bool)
+            m[i] = False
+            du[k] = yukawa_direct(pts[m], tau[m], pts[i:i + 1], 5.0)[0]
+        err = rel_l2(u[sel], du)
+        assert err < (1e-8 if tol < 1e-8 else 3 * tol), (len(pts), tol, info["p"], err)
