@@ -206,6 +206,7 @@ void plan_from_device_points(fmmb_cache* cache, const double* xyz, int64_t n, co
     to_device(P.d_lv_reps, t, ctx.stream);
   }
   build_lists(P);
+  if (C.method == FMMB_METHOD_CUBE_KI) ki_prepare(P);   // its operators, its target-major pairs
   h->parent = cache;
   std::lock_guard<std::mutex> lk(g_handles);
   ++cache->deps;
@@ -283,7 +284,37 @@ int fmmb_ctx_synchronize(fmmb_ctx* ctx) {  // state errors surface at the next h
 int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* m, fmmb_cache** out) {
   return guard([&] {
     require(ctx && m && out, FMMB_ERR_ARGUMENT, "null argument");
-    require(m->method == FMMB_METHOD_SPHERICAL_HARMONICS, FMMB_ERR_UNSUPPORTED, "only SphericalHarmonics is provided");
+    require(m->method == FMMB_METHOD_SPHERICAL_HARMONICS || m->method == FMMB_METHOD_CUBE_KI, FMMB_ERR_UNSUPPORTED,
+            "the methods provided are SphericalHarmonics, StokesHarmonics and CubeKernelIndependent{3}");
+    if (m->method == FMMB_METHOD_CUBE_KI) {
+      // CubeKernelIndependent{3}(Laplace3D(); p, pc = 2p, d = 0.1, pinv_rtol) (src/operators/cubeki.jl:35-42)
+      require(m->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "the cube KI method is provided for Laplace3D");
+      require(m->p >= 2, FMMB_ERR_ARGUMENT, "p must be at least 2");
+      require(m->p <= KI_PMAX, FMMB_ERR_UNSUPPORTED, "p above 12 is not provided for the cube KI method");
+      const int pc = m->pc ? m->pc : 2 * m->p;
+      const double d = m->d != 0 ? m->d : 0.1;
+      require(pc >= m->p, FMMB_ERR_ARGUMENT, "pc must be at least p");
+      require(pc <= 2 * KI_PMAX, FMMB_ERR_UNSUPPORTED, "pc above 24 is not provided");
+      require(d > 0 && d < 2.0 / 3.0, FMMB_ERR_ARGUMENT,
+              "d must lie in (0, 2/3): the large surface, at (3 − 2d)w/2, must lie outside the small one, at (1 + d)w/2");
+      require(m->pinv_rtol >= 0 && m->pinv_rtol < 1, FMMB_ERR_ARGUMENT, "pinv_rtol must lie in [0, 1)");
+      std::unique_ptr<fmmb_cache> h(new fmmb_cache());
+      h->c.ctx = &ctx->c;
+      h->parent = ctx;
+      h->c.method = FMMB_METHOD_CUBE_KI;
+      h->c.p = m->p;
+      h->c.np = 6 * m->p * m->p - 12 * m->p + 8;   // p³ − (p−2)³ small-surface points
+      h->c.ld = (h->c.np + 63) / 64 * 64;
+      h->c.kernel = FMMB_KERNEL_LAPLACE3D;
+      h->c.nexp = 1;
+      h->c.ki_pc = pc;
+      h->c.ki_d = d;
+      h->c.ki_rtol = m->pinv_rtol > 0 ? m->pinv_rtol : 50 * 1.1920928955078125e-7;
+      std::lock_guard<std::mutex> lk(g_handles);
+      ++ctx->deps;
+      *out = h.release();
+      return;
+    }
     require(m->kernel == FMMB_KERNEL_LAPLACE3D || m->kernel == FMMB_KERNEL_YUKAWA3D || m->kernel == FMMB_KERNEL_STOKESLET3D,
             FMMB_ERR_UNSUPPORTED, "the kernels provided are Laplace3D, Yukawa3D and Stokeslet3D");
     if (m->kernel == FMMB_KERNEL_YUKAWA3D)
@@ -448,7 +479,9 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
     S.Pl.alloc(ne);
     FMMB_CUDA(cudaMemsetAsync(S.M.p, 0, S.M.bytes(), s));
     FMMB_CUDA(cudaMemsetAsync(S.Pl.p, 0, S.Pl.bytes(), s));
-    if (precision == FMMB_PRECISION_MIXED) {
+    if (P.cache->method == FMMB_METHOD_CUBE_KI) {
+      ki_state(S);   // its spectra, check and local buffers; the precision selects the far field's and P2P's
+    } else if (precision == FMMB_PRECISION_MIXED) {
       std::lock_guard<std::mutex> lk(P.cache->mu);
       prepare_mixed_operators(*P.cache);
     }

@@ -238,6 +238,69 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32) k_near(const int* __restrict_
   }
 }
 
+// The kernel-independent far field (l2t, src/operators/ki_common.jl:293-327): at each target
+// Σ_k G(x − y_k) L_k over the leaf's large surface y_k = c + w·ŷ_k (ŷ at width 1), the local
+// density L staged per warp in shared memory, times w (the pseudo-inverse's scale). R = float:
+// leaf-centred FP32 terms summed in FP32 per 32 surface points, the partial sums in FP64;
+// R = double: FP64 throughout. Writes the outputs (the near field adds to them).
+template <typename R>
+__global__ void __launch_bounds__(128) k_ki_l2t(const int* __restrict__ gnode, const int* __restrict__ gstart,
+                                                const int* __restrict__ gcount, int ngroups, const double* __restrict__ tx,
+                                                const double* __restrict__ ty, const double* __restrict__ tz,
+                                                const int* __restrict__ tout, const int4* __restrict__ cell,
+                                                const double* __restrict__ Ll, int nl, int nld,
+                                                const double* __restrict__ large, Geometry geo, int outputs,
+                                                double* __restrict__ pot, double* __restrict__ grad) {
+  extern __shared__ __align__(16) unsigned char sk_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (grp >= ngroups) return;
+  R* L = reinterpret_cast<R*>(sk_raw) + (size_t)warp * 4 * nl;   // [nl] densities, then [3·nl] points
+  R* Y = L + nl;
+  const int leaf = gnode[grp];
+  const int4 c = cell[leaf];
+  const double w = ldexp(geo.W0, -c.w);
+  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  for (int k = lane; k < nl; k += 32) {
+    L[k] = (R)Ll[(int64_t)leaf * nld + k];
+    Y[3 * k] = (R)(w * large[3 * k]);
+    Y[3 * k + 1] = (R)(w * large[3 * k + 1]);
+    Y[3 * k + 2] = (R)(w * large[3 * k + 2]);
+  }
+  __syncwarp();
+  const int t0 = gstart[grp], nt = gcount[grp];
+  for (int base = 0; base < nt; base += 32) {
+    const int k = t0 + base + lane;
+    const bool act = base + lane < nt;
+    const R x = act ? (R)(tx[k] - cx) : R(0), y = act ? (R)(ty[k] - cy) : R(0), z = act ? (R)(tz[k] - cz) : R(0);
+    double u = 0, gx = 0, gy = 0, gz = 0;
+    for (int k0 = 0; k0 < nl; k0 += 32) {
+      R bu = 0, bx = 0, by = 0, bz = 0;
+      const int k1 = min(nl, k0 + 32);
+      for (int q = k0; q < k1; ++q) {
+        const R dx = x - Y[3 * q], dy = y - Y[3 * q + 1], dz = z - Y[3 * q + 2];
+        const R ir = rsqrt(dx * dx + dy * dy + dz * dz);
+        const R li = L[q] * ir;
+        bu += li;
+        const R li3 = li * ir * ir;
+        bx += li3 * dx;
+        by += li3 * dy;
+        bz += li3 * dz;
+      }
+      u += bu; gx += bx; gy += by; gz += bz;
+    }
+    if (act) {
+      const int o = tout[k];
+      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = KC * w * u;
+      if (outputs & FMMB_OUTPUT_GRADIENT) {
+        grad[3 * (int64_t)o] = -KC * w * gx;
+        grad[3 * (int64_t)o + 1] = -KC * w * gy;
+        grad[3 * (int64_t)o + 2] = -KC * w * gz;
+      }
+    }
+  }
+}
+
 template <int P>
 void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
                 const double* tz, const int* tout, int outputs, double* pot, double* grad) {
@@ -268,6 +331,25 @@ void launch_near(State& S, const int* gnode, const int* gstart, const int* gcoun
 void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
                      const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad) {
   if (ng == 0) return;
+  if (S.plan->cache->method == FMMB_METHOD_CUBE_KI) {
+    Plan& P_ = *S.plan;
+    Cache& C = *P_.cache;
+    const bool mixed = S.precision == FMMB_PRECISION_MIXED;
+    const size_t per_warp = (mixed ? sizeof(float) : sizeof(double)) * 4 * C.ki_nl;
+    const int warps = (int)std::max<size_t>(1, std::min<size_t>(4, (200u << 10) / per_warp));
+    const size_t smem = per_warp * warps;
+    auto kern = mixed ? k_ki_l2t<float> : k_ki_l2t<double>;
+    FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(ng + warps - 1) / warps, 32 * warps, smem, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout,
+                                                                       P_.cell.p, S.ki_ll.p, C.ki_nl, C.ki_nld,
+                                                                       C.ki_large.p, geometry(P_), outputs, pot, grad);
+    FMMB_LAUNCH_CHECK();
+    if (mixed && self) launch_near<float, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+    else if (mixed) launch_near<float, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+    else if (self) launch_near<double, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+    else launch_near<double, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+    return;
+  }
   switch (S.plan->cache->p) {
 #define X(pp) case pp: launch_l2p<pp>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad); break;
     FMMB_P_CASES(X)

@@ -56,6 +56,17 @@ __global__ void k_pair_count(const int4* __restrict__ cell, const int* __restric
   cnt[first + q] = c;
 }
 
+// the target-major list of the kernel-independent M2L: target g's pairs (source, far index)
+// at tp[ptr[g]..], in the enumeration order
+__global__ void k_target_fill(const int4* __restrict__ cell, const int* __restrict__ parent, const int* __restrict__ cf,
+                              const int* __restrict__ col, const uint8_t* __restrict__ flags, int first, int n,
+                              const int* __restrict__ ptr, int2* __restrict__ tp) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  int k = ptr[first + q];
+  for_far_pairs(first + q, cell, parent, cf, col, flags, [&](int s, int f) { tp[k++] = make_int2(s, f); });
+}
+
 // one CTA per block, one thread per target: counts per (target, class), the class-major
 // offsets, and the fill
 __global__ void k_block_fill(const int4* __restrict__ blocks, const int4* __restrict__ cell, const int* __restrict__ parent,
@@ -201,6 +212,31 @@ void build_lists(Plan& P) {
   for (int l = 0; l < L; ++l) { sc[l] = P.scale[l]; ms[l] = P.m2l_scale[l]; }
   to_device(P.d_scale, sc, s);
   to_device(P.d_m2l_scale, ms, s);
+  FMMB_CUDA(cudaStreamSynchronize(s));
+}
+
+// the far pairs of every target as one target-major list (the kernel-independent method's
+// spectral M2L pulls each target's sources; ptr has nnodes + 1 entries)
+void build_target_pairs(Plan& P) {
+  cudaStream_t s = P.ctx->stream;
+  const int n = P.nnodes, L = P.L;
+  DBuf<int> cnt(n + 1);
+  FMMB_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (n + 1), s));
+  for (int l = 2; l < L; ++l) {
+    int first = P.level_start[l], nl = P.level_start[l + 1] - first;
+    if (nl) k_pair_count<<<(nl + 127) / 128, 128, 0, s>>>(P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p, first, nl, cnt.p);
+    FMMB_LAUNCH_CHECK();
+  }
+  P.tp_ptr.alloc(n + 1);
+  const int64_t total = scan_exclusive_total(cnt.p, P.tp_ptr.p, n + 1, s);
+  require(total < (1ll << 31), FMMB_ERR_ARGUMENT, "too many far pairs for 32-bit offsets");
+  P.tp.alloc(std::max<int64_t>(total, 1));
+  for (int l = 2; l < L; ++l) {
+    int first = P.level_start[l], nl = P.level_start[l + 1] - first;
+    if (nl) k_target_fill<<<(nl + 127) / 128, 128, 0, s>>>(P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p, first, nl,
+                                                        P.tp_ptr.p, P.tp.p);
+    FMMB_LAUNCH_CHECK();
+  }
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
 

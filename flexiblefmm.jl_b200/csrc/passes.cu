@@ -417,6 +417,7 @@ void gemm_columns(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols
 }
 
 int p2m(State& S) {
+  if (S.plan->cache->method == FMMB_METHOD_CUBE_KI) return ki_p2m(S);
   switch (S.plan->cache->p) {
 #define X(pp) case pp: launch_p2m<pp>(S, S.q.p, S.M.p, (int64_t)S.plan->cache->ld); break;
     FMMB_P_CASES(X)
@@ -459,6 +460,8 @@ int l2l_sweep(State& S) {
     gemm_cols(NCH * C.ld, C.ld, P.lv_l2l[l - 1], bm, cm, ng, C.ld, C.np, 1, P.ctx->num_sms, s);
     ++launches;
   }
+  // the kernel-independent method: the leaves' local densities from their check potentials
+  if (C.method == FMMB_METHOD_CUBE_KI) launches += ki_leaf_locals(S);
   return launches;
 }
 
@@ -467,6 +470,7 @@ int l2l_sweep(State& S) {
 int m2l_stage(State& S) {
   Plan& P = *S.plan;
   FMMB_CUDA(cudaMemsetAsync(S.Pl.p, 0, S.Pl.bytes(), P.ctx->stream));
+  if (P.cache->method == FMMB_METHOD_CUBE_KI) return ki_m2l(S);
   if (P.h_blocks.empty()) return 0;
   if (S.precision == FMMB_PRECISION_MIXED) {
     m2l_mixed(S);

@@ -5,6 +5,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "ki.h"
 
 namespace fmmb {
 
@@ -51,6 +52,18 @@ struct Cache {
   std::map<int, std::shared_ptr<YukawaLevel>> yk_levels;
   DBuf<double> yk_xq, yk_wq;
   int yk_nq = 0;
+  // CubeKernelIndependent{3}: the method, its parameters, the host operators at width 1 (shared
+  // by caches with the same parameters) and their device copies at width 1 (surfaces, factored
+  // pseudo-inverses padded to RU/RD/NLD rows, M2M/L2L in the Laplace layouts, spectral tables
+  // as float2 over nfp = nfreq rounded up to 64 frequencies)
+  int method = FMMB_METHOD_SPHERICAL_HARMONICS;
+  int ki_pc = 0;
+  double ki_d = 0, ki_rtol = 0;
+  std::shared_ptr<const KIHost> ki;
+  int ki_nl = 0, ki_nld = 0, ki_ru = 0, ki_rd = 0, ki_nfp = 0;
+  DBuf<double> ki_large, ki_upv, ki_upsu, ki_downv, ki_downsu, ki_m2m, ki_l2l;
+  DBuf<int> ki_embed;
+  DBuf<float2> ki_tab, ki_tw;
 };
 
 // One M2L work block: TB consecutive nodes of one level (the targets), their far pairs
@@ -100,6 +113,11 @@ struct Plan {
   std::vector<const double*> lv_reps, lv_m2m, lv_l2l;
   DBuf<uint64_t> d_lv_reps;
   DBuf<double> d_kh2;
+  // the kernel-independent method: every target's far pairs (source, far index), target-major
+  DBuf<int> tp_ptr;
+  DBuf<int2> tp;
+  DBuf<int> ki_leaves;                    // every real leaf (with sources or not)
+  int n_ki_leaves = 0;
 };
 
 struct State {
@@ -111,6 +129,11 @@ struct State {
   DBuf<uint16_t> Mh, Ml;                  // the mixed path: the multipoles scaled by a power of two
   DBuf<float> Msc;                        //   per node, as FP16 head and tail; the inverse scales
   DBuf<int> err;                          // the mixed path: the bounded-wait error flag
+  // the kernel-independent method: check potentials of the childless nodes on their large
+  // surfaces, the pseudo-inverses' middle products, the leaves' local densities on their large
+  // surfaces (nnodes × NLD), the spectra of the multipoles and of the M2L sums (nnodes × nfp)
+  DBuf<double> ki_pm, ki_y, ki_ll;
+  DBuf<float2> ki_spec, ki_u;
   bool built = false;
   // staging of the host-pointer entry points and the evaluation at targets
   DBuf<double> h_in_xyz, h_in_tau, d_pot, d_grad;
@@ -124,6 +147,7 @@ struct State {
 void build_tree(Plan& P, const double* xyz_dev, int ppl, int max_levels);
 // lists.cu
 void build_lists(Plan& P);
+void build_target_pairs(Plan& P);
 // passes.cu
 void upload_operators(Cache& C);
 void gather_inputs(State& S, const double* xyz_dev, const double* tau_dev);
@@ -134,6 +158,12 @@ void evaluate_targets(State& S, const double* tg_dev, int64_t nt, int outputs, d
 void bounds(Ctx& ctx, const double* xyz_dev, int64_t n, double lo[3], double hi[3], int64_t* nonfinite);
 void direct(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
             int64_t nt, double* pot, double* grad);
+// ki.cu: CubeKernelIndependent{3}(Laplace3D()): cache and plan setup, the passes
+void ki_prepare(Plan& P);
+void ki_state(State& S);
+int ki_p2m(State& S);
+int ki_m2l(State& S);
+int ki_leaf_locals(State& S);
 // yukawa.cu: SphericalHarmonics(Yukawa3D(κ)) — the operators of the plan's widths (built on the
 // device by projection when a width is first used) and the per-level factors
 void yukawa_prepare(Plan& P);

@@ -56,7 +56,8 @@ class Unsupported(FMMBError, NotImplementedError):
 
 class _MethodDesc(C.Structure):
     _fields_ = [("method", C.c_int32), ("kernel", C.c_int32), ("p", C.c_int32), ("reserved", C.c_int32),
-                ("tol", C.c_double), ("kappa", C.c_double)]
+                ("tol", C.c_double), ("kappa", C.c_double), ("pc", C.c_int32), ("reserved2", C.c_int32),
+                ("d", C.c_double), ("pinv_rtol", C.c_double)]
 
 
 class _TreeOpts(C.Structure):
@@ -204,6 +205,32 @@ class StokesHarmonics:
         self.kernel, self.p, self.tol = kernel, int(p), 0.0
 
 
+class CubeKernelIndependent:
+    """CubeKernelIndependent{3}(kernel; p=8, pc=2p, d=0.1, pinv_rtol=50·eps(Float32))
+    (src/operators/cubeki.jl:35-42): the kernel-independent method on cube surfaces with p
+    points per edge on the small surface (p³ − (p−2)³ points), pc on the large one, margin d;
+    the M2L by FFT. Laplace3D only; the far field and the near field in FP32 on the "mixed"
+    precision path, in FP64 on the "fp64" path (the spectra are FP32 on both)."""
+
+    def __init__(self, kernel, p=8, pc=None, d=0.1, pinv_rtol=None):
+        if not isinstance(kernel, Laplace3D):
+            raise ArgumentError(1, "the device cube KI method is written for Laplace3D")
+        pc = 2 * p if pc is None else pc
+        if p < 2:
+            raise ArgumentError(1, "p must be at least 2")
+        if pc < p:
+            raise ArgumentError(1, "pc must be at least p")
+        if not (0 < d < 2 / 3):
+            raise ArgumentError(1, "d must lie in (0, 2/3)")
+        self.kernel, self.p, self.pc, self.d = kernel, int(p), int(pc), float(d)
+        self.pinv_rtol = 50 * float(np.finfo(np.float32).eps) if pinv_rtol is None else float(pinv_rtol)
+        self.tol = 0.0
+
+    @property
+    def nsurface(self):
+        return self.p ** 3 - (self.p - 2) ** 3
+
+
 class SphericalHarmonics:
     """SphericalHarmonics(kernel; p=16, tol=0) (src/operators/harmonics.jl:303-308)."""
 
@@ -273,13 +300,16 @@ class OperatorCache:
     def __init__(self, method, ctx=None):
         self.method = method
         self.ctx = ctx or default_context()
-        if isinstance(method, StokesHarmonics):
-            kernel, kappa = KERNEL_STOKESLET3D, 0.0
-        elif isinstance(method.kernel, Yukawa3D):
-            kernel, kappa = KERNEL_YUKAWA3D, method.kernel.k
+        if isinstance(method, CubeKernelIndependent):
+            d = _MethodDesc(2, KERNEL_LAPLACE3D, method.p, 0, 0.0, 0.0, method.pc, 0, method.d, method.pinv_rtol)
         else:
-            kernel, kappa = KERNEL_LAPLACE3D, 0.0
-        d = _MethodDesc(1, kernel, method.p, 0, method.tol, kappa)
+            if isinstance(method, StokesHarmonics):
+                kernel, kappa = KERNEL_STOKESLET3D, 0.0
+            elif isinstance(method.kernel, Yukawa3D):
+                kernel, kappa = KERNEL_YUKAWA3D, method.kernel.k
+            else:
+                kernel, kappa = KERNEL_LAPLACE3D, 0.0
+            d = _MethodDesc(1, kernel, method.p, 0, method.tol, kappa)
         h = C.c_void_p()
         _check(lib().fmmb_cache_create(self.ctx._h, C.byref(d), C.byref(h)))
         self._h = h
@@ -378,8 +408,9 @@ class FMMState:
     def expansions(self):
         """(multipoles, locals): nnodes × (p+1)² for Laplace3D, nnodes × 4 × (p+1)² for the
         Stokeslet (blocks Φ₁, Φ₂, Φ₃, Ψ̂)."""
-        n, np_ = self.fmm.nnodes, (self.fmm.method.p + 1) ** 2
-        shape = (n, 4, np_) if isinstance(self.fmm.method, StokesHarmonics) else (n, np_)
+        m = self.fmm.method
+        n, np_ = self.fmm.nnodes, (m.nsurface if isinstance(m, CubeKernelIndependent) else (m.p + 1) ** 2)
+        shape = (n, 4, np_) if isinstance(m, StokesHarmonics) else (n, np_)
         M = np.zeros(shape)
         Lc = np.zeros(shape)
         _check(lib().fmmb_state_expansions(self._h, _ptr(M), _ptr(Lc)))

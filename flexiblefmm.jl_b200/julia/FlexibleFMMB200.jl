@@ -13,7 +13,8 @@
 # interleaved array the ABI takes); outputs come back in the original order.
 module FlexibleFMMB200
 
-using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, Laplace3D, Yukawa3D, Stokeslet3D, Potential, Gradient
+using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, CubeKernelIndependent, Laplace3D, Yukawa3D,
+    Stokeslet3D, Potential, Gradient
 using StaticArrays: SVector
 
 const libfmmb = get(ENV, "FMMB_LIB", joinpath(@__DIR__, "..", "libfmmb.so"))
@@ -30,6 +31,10 @@ struct MethodDesc
     reserved::Int32
     tol::Float64
     kappa::Float64
+    pc::Int32
+    reserved2::Int32
+    d::Float64
+    pinv_rtol::Float64
 end
 
 struct TreeOpts
@@ -64,7 +69,7 @@ default_context() = something(DEFAULT_CONTEXT[], (DEFAULT_CONTEXT[] = Context(0)
 """
     OperatorCache(method)  (src/operators/cache.jl:19-22)
 """
-const DeviceMethod = Union{SphericalHarmonics,StokesHarmonics}
+const DeviceMethod = Union{SphericalHarmonics,StokesHarmonics,CubeKernelIndependent{3}}
 _kernel_id(m::SphericalHarmonics) = m.kernel isa Laplace3D ? Int32(1) : m.kernel isa Yukawa3D ? Int32(2) :
     throw(ArgumentError("the device method is written for Laplace3D and Yukawa3D"))
 _kappa(m::SphericalHarmonics) = m.kernel isa Yukawa3D ? Float64(m.kernel.k) : 0.0
@@ -72,12 +77,19 @@ _kappa(m::StokesHarmonics) = 0.0
 _kernel_id(m::StokesHarmonics) = m.kernel isa Stokeslet3D ? Int32(3) :
     throw(ArgumentError("the device Stokes method is written for Stokeslet3D"))
 
+_method_desc(m::Union{SphericalHarmonics,StokesHarmonics}) =
+    MethodDesc(1, _kernel_id(m), Int32(m.p), 0, m isa SphericalHarmonics ? m.tol : 0.0, _kappa(m), 0, 0, 0.0, 0.0)
+# CubeKernelIndependent{3}(Laplace3D(); p, pc, d, pinv_rtol): the spectral-M2L method on cube surfaces
+_method_desc(m::CubeKernelIndependent{3}) = m.kernel isa Laplace3D ?
+    MethodDesc(2, 1, Int32(m.p), 0, 0.0, 0.0, Int32(m.pc), 0, Float64(m.d), Float64(m.pinv_rtol)) :
+    throw(ArgumentError("the device cube KI method is written for Laplace3D"))
+
 mutable struct OperatorCache
     method::DeviceMethod
     ctx::Context
     h::Ptr{Cvoid}
     function OperatorCache(m::DeviceMethod; ctx::Context=default_context())
-        d = Ref(MethodDesc(1, _kernel_id(m), Int32(m.p), 0, m isa SphericalHarmonics ? m.tol : 0.0, _kappa(m)))
+        d = Ref(_method_desc(m))
         r = Ref{Ptr{Cvoid}}(C_NULL)
         check(ccall((:fmmb_cache_create, libfmmb), Cint, (Ptr{Cvoid}, Ref{MethodDesc}, Ref{Ptr{Cvoid}}), ctx.h, d, r))
         c = new(m, ctx, r[])

@@ -36,6 +36,7 @@ extern "C" {
 #define FMMB_KERNEL_YUKAWA3D 2    /* e^{−κr}/(4πr), SphericalHarmonics(Yukawa3D(κ); p): FP64 path, operators per width */
 #define FMMB_KERNEL_STOKESLET3D 3 /* StokesHarmonics(Stokeslet3D(); p): FP64 path, Stokeslet densities, velocities */
 #define FMMB_METHOD_SPHERICAL_HARMONICS 1
+#define FMMB_METHOD_CUBE_KI 2 /* CubeKernelIndependent{3}(Laplace3D(); p, pc, d): spectral (FFT) M2L */
 
 #define FMMB_PRECISION_FP64 0  /* the plain path: FP64 everywhere (the drop-in) */
 #define FMMB_PRECISION_MIXED 1 /* split-precision tensor-core M2L, FP32 compensated near field */
@@ -50,14 +51,21 @@ typedef struct fmmb_state fmmb_state;
 
 /* The method: SphericalHarmonics(Laplace3D(); p) (src/operators/harmonics.jl:303-308); with kernel
  * FMMB_KERNEL_YUKAWA3D SphericalHarmonics(Yukawa3D(kappa); p) (src/operators/harmonics_yukawa.jl:27-32);
- * with FMMB_KERNEL_STOKESLET3D StokesHarmonics(Stokeslet3D(); p) (src/operators/harmonics_stokes.jl:34-45). */
+ * with FMMB_KERNEL_STOKESLET3D StokesHarmonics(Stokeslet3D(); p) (src/operators/harmonics_stokes.jl:34-45);
+ * with method FMMB_METHOD_CUBE_KI CubeKernelIndependent{3}(Laplace3D(); p, pc, d, pinv_rtol)
+ * (src/operators/cubeki.jl:18-48). */
 typedef struct {
-  int32_t method;  /* FMMB_METHOD_SPHERICAL_HARMONICS */
-  int32_t kernel;  /* FMMB_KERNEL_* */
-  int32_t p;       /* expansion degree, 1..20 */
+  int32_t method;  /* FMMB_METHOD_SPHERICAL_HARMONICS or FMMB_METHOD_CUBE_KI */
+  int32_t kernel;  /* FMMB_KERNEL_* (the cube KI method: FMMB_KERNEL_LAPLACE3D) */
+  int32_t p;       /* harmonics: expansion degree, 1..20; cube KI: points per edge, 2..12 */
   int32_t reserved;
   double tol;      /* 0: dense class operators (the only form this build provides) */
   double kappa;    /* the Yukawa screening κ > 0 (FMMB_KERNEL_YUKAWA3D); ignored otherwise */
+  int32_t pc;      /* cube KI: points per edge of the large surface; 0: 2p */
+  int32_t reserved2;
+  double d;        /* cube KI: the surfaces' margin, in (0, 2/3); 0: 0.1 */
+  double pinv_rtol; /* cube KI: the pseudo-inverses' truncation; 0: 50·eps(Float32), the reference's default
+                       for Laplace3D(Float32) */
 } fmmb_method_desc;
 
 /* Tree options: FMM(m, sources; ppl, bbox, max_levels) (src/fmm.jl:31-49). */

@@ -52,7 +52,7 @@ def test_julia_shim_binds_declared_symbols():
 
 def test_struct_layouts(fmmb):
     import ctypes as C
-    assert C.sizeof(fmmb._MethodDesc) == 32 and C.sizeof(fmmb._TreeOpts) == 48
+    assert C.sizeof(fmmb._MethodDesc) == 56 and C.sizeof(fmmb._TreeOpts) == 48
 
 
 def test_struct_layouts_match_the_header(fmmb, tmp_path):

@@ -1,0 +1,113 @@
+"""CubeKernelIndependent{3}(Laplace3D(); p = 8, pc = 16, d = 0.1) on the device: the P2M's
+multipoles reproduce their sources' far field, the spectral M2L equals the dense kernel-matrix
+product on every far pair of a level (the reference's check, test/test_cubeki.jl:43-69), and the
+FMM matches FP64 direct sums (the reference's cube p = 8 reaches ~3e-8 in FP64 and its Float32
+floor is ~2e-5, docs/kifmm.md: the FP32 spectra put this path between them)."""
+import numpy as np
+import pytest
+
+from helpers import clustered3, rel_l2, uniform3
+
+pytestmark = pytest.mark.gpu
+KC = 1 / (4 * np.pi)
+
+
+def cube_boundary_points(p, a):
+    """The boundary points of the p³ lattice on [−a, a]³, coordinate 1 fastest
+    (src/operators/spectral_m2l.jl:159-172)."""
+    c = -a + 2 * a * np.arange(p) / (p - 1)
+    out = []
+    for i3 in range(p):
+        for i2 in range(p):
+            for i1 in range(p):
+                if min(i1, i2, i3) == 0 or max(i1, i2, i3) == p - 1:
+                    out.append((c[i1], c[i2], c[i3]))
+    return np.array(out)
+
+
+def centres(f, t):
+    w = f.width / 2.0 ** t["level"]
+    return f.origin[None, :] + (t["cell"] + 0.5) * w[:, None], w
+
+
+def test_ki_multipoles_reproduce_the_far_field(fmmb):
+    rng = np.random.default_rng(1)
+    pts = uniform3(rng, 20000)
+    tau = rng.standard_normal(20000)
+    m = fmmb.CubeKernelIndependent(fmmb.Laplace3D(), p=8)
+    f = fmmb.FMM(m, pts, ppl=64, bbox=((0.0, 0.0, 0.0), 1.0))
+    st = fmmb.build_expansions(f, pts, tau)
+    M, _ = st.expansions()
+    t = f.tree()
+    cen, w = centres(f, t)
+    small = cube_boundary_points(8, 1.1 / 2)
+    leaves = np.where(t["leaf"].astype(bool) & (t["phi"] >= t["plo"]))[0]
+    perm = t["perm"]
+    worst = 0.0
+    for g in rng.choice(leaves, 20, replace=False):
+        src = perm[t["plo"][g]:t["phi"][g] + 1]
+        far = cen[g] + 2.5 * w[g] * rng.standard_normal((30, 3)) / 1.0
+        far = cen[g] + 2.5 * w[g] * (far - cen[g]) / np.linalg.norm(far - cen[g], axis=1)[:, None]
+        direct = KC * (tau[src][None, :] / np.linalg.norm(far[:, None, :] - pts[src][None, :, :], axis=2)).sum(1)
+        eq = cen[g] + w[g] * small
+        field = KC * (M[g][None, :] / np.linalg.norm(far[:, None, :] - eq[None, :, :], axis=2)).sum(1)
+        worst = max(worst, np.max(np.abs(field - direct)) / np.max(np.abs(direct)))
+    assert worst < 1e-5, worst
+
+
+def test_ki_spectral_m2l_equals_the_dense_product(fmmb):
+    """A three-level tree: the level-2 leaves' check potentials are their M2L sums alone."""
+    rng = np.random.default_rng(2)
+    pts = uniform3(rng, 2500)
+    tau = rng.standard_normal(2500)
+    m = fmmb.CubeKernelIndependent(fmmb.Laplace3D(), p=8)
+    f = fmmb.FMM(m, pts, ppl=64, bbox=((0.0, 0.0, 0.0), 1.0))
+    assert f.nlevels == 3
+    st = fmmb.build_expansions(f, pts, tau)
+    M, Lc = st.expansions()
+    t = f.tree()
+    cen, w = centres(f, t)
+    small = cube_boundary_points(8, 1.1 / 2)
+    tg, src, _ = f.pairs(2)
+    ref = np.zeros_like(Lc)
+    for a, b in zip(tg, src):
+        x = cen[a] + w[a] * small
+        y = cen[b] + w[b] * small
+        ref[a] += KC * (M[b][None, :] / np.linalg.norm(x[:, None, :] - y[None, :, :], axis=2)).sum(1)
+    sel = np.unique(tg)
+    assert len(sel) == 64
+    err = np.max(np.abs(Lc[sel] - ref[sel])) / np.max(np.abs(ref[sel]))
+    assert err < 2e-6, err
+
+
+@pytest.mark.parametrize("gen", [uniform3, clustered3])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ki_fmm_against_direct(fmmb, oracle, gen, precision):
+    rng = np.random.default_rng(3)
+    n = 60000
+    pts = gen(rng, n)
+    tau = rng.standard_normal(n)
+    m = fmmb.CubeKernelIndependent(fmmb.Laplace3D(), p=8)
+    f = fmmb.FMM(m, pts, ppl=64, bbox=((0.0, 0.0, 0.0), 1.0))
+    assert f.nlevels >= 4
+    st = fmmb.build_expansions(f, pts, tau, precision=precision)
+    u, g = fmmb.evaluate_at_sources_both(f, st)
+    sel = np.sort(rng.choice(n, 400, replace=False))
+    du, dg = oracle.direct_sample(pts, tau, sel)
+    eu, eg = rel_l2(u[sel], du), rel_l2(g[sel], dg)
+    assert eu < (5e-6 if precision == "fp64" else 2e-5), (gen.__name__, precision, eu)
+    assert eg < (5e-5 if precision == "fp64" else 2e-4), (gen.__name__, precision, eg)
+    tgt = rng.random((300, 3))
+    ut = fmmb.evaluate(f, st, tgt)
+    d = tgt[:, None, :] - pts[None, :, :]
+    dt = KC * (tau[None, :] / np.linalg.norm(d, axis=2)).sum(1)
+    assert rel_l2(ut, dt) < (5e-6 if precision == "fp64" else 2e-5)
+
+
+def test_ki_errors(fmmb):
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.CubeKernelIndependent(fmmb.Laplace3D(), p=8, pc=6)
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.CubeKernelIndependent(fmmb.Laplace3D(), d=0.7)
+    with pytest.raises(fmmb.Unsupported):
+        fmmb.OperatorCache(fmmb.CubeKernelIndependent(fmmb.Laplace3D(), p=14))
