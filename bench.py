@@ -57,6 +57,7 @@ def args_():
     a.add_argument("--serve-requests", type=int, default=96, help="requests of the serving measurement (0: skip it)")
     a.add_argument("--serve-slots", type=int, default=4)
     a.add_argument("--stokes-instances", type=int, default=64, help="instances of the batched Stokes measurement (0: skip it)")
+    a.add_argument("--ki-points", type=int, default=2_000_000, help="points of the cube KI measurement (0: skip it)")
     return a.parse_args()
 
 
@@ -307,6 +308,93 @@ def stokes_batched(fmmb, device, count, slots, p=16, ppl=200, samples=32):
             "error": {"samples_per_instance": samples, "max": max(errs), "median": float(np.median(errs))}}
 
 
+# ---------------------------------------------------------------- the cube KI method
+def cube_ki_workload(n, seed=4):
+    """The adaptive configuration: n points from 16 isotropic Gaussians (centres uniform in
+    [0.1, 0.9]^3, sigma = 0.01), points outside the unit box redrawn; charges U(-1, 1) rounded to
+    FP32 values (the configuration's Float32 densities)."""
+    rng = np.random.default_rng(seed)
+    c = 0.1 + 0.8 * rng.random((16, 3))
+    pts = c[rng.integers(0, 16, n)] + 0.01 * rng.standard_normal((n, 3))
+    bad = np.any((pts < 0) | (pts >= 1), axis=1)
+    while bad.any():
+        pts[bad] = c[rng.integers(0, 16, int(bad.sum()))] + 0.01 * rng.standard_normal((int(bad.sum()), 3))
+        bad = np.any((pts < 0) | (pts >= 1), axis=1)
+    tau = rng.uniform(-1, 1, n).astype(np.float32).astype(np.float64)
+    return pts, tau
+
+
+def cube_ki(fmmb, torch, ctx, n, steps, warmup, samples=4096):
+    """CubeKernelIndependent{3}(Laplace3D(); p = 8, pc = 16, d = 0.1), ppl = 64, spectral M2L: the
+    matvec (potential + gradient at the sources, inputs resident on the device, CUDA events on the
+    library's stream) on the FP32 far/near-field path, its relative L2 error against FP64 direct
+    sums, the stage times, and the spectral M2L stage's bytes per second."""
+    import ctypes as C
+    L = fmmb.lib()
+    pts, tau = cube_ki_workload(n)
+    P = lambda t: C.c_void_p(t.data_ptr())
+    xyz_d = torch.from_numpy(pts).cuda()
+    tau_d = torch.from_numpy(tau).cuda()
+    pot_d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    grad_d = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    m = fmmb.CubeKernelIndependent(fmmb.Laplace3D(), p=8)
+    t0 = time.perf_counter()
+    f = fmmb.FMM(m, pts, ppl=64, bbox=((0.0, 0.0, 0.0), 1.0))
+    plan_s = time.perf_counter() - t0
+    st = fmmb.FMMState(f, "mixed")
+    step = lambda: fmmb._check(L.fmmb_matvec_dev(st._h, P(xyz_d), P(tau_d), n, 3, P(pot_d), P(grad_d)))
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+    names = ("gather", "p2m", "m2m", "m2l", "l2l", "eval")
+    runs = []
+    for _ in range(3):
+        msa = (C.c_double * 6)()
+        nl = C.c_int()
+        fmmb._check(L.fmmb_profile_matvec(st._h, P(xyz_d), P(tau_d), n, 3, P(pot_d), P(grad_d), msa, 6, C.byref(nl)))
+        runs.append(list(msa))
+    stages = {k: statistics.median(r[i] for r in runs) for i, k in enumerate(names)}
+    step()
+    torch.cuda.synchronize()
+    u, g = pot_d.cpu().numpy(), grad_d.cpu().numpy()
+    rng = np.random.default_rng(8)
+    sel = np.sort(rng.choice(n, size=min(samples, n), replace=False)).astype(np.int64)
+    sel_d = torch.from_numpy(sel).cuda()
+    tg_d = xyz_d[sel_d].contiguous()
+    dp = torch.zeros(len(sel), dtype=torch.float64, device="cuda")
+    dg = torch.zeros((len(sel), 3), dtype=torch.float64, device="cuda")
+    fmmb._check(L.fmmb_direct_dev(ctx._h, P(xyz_d), P(tau_d), n, P(tg_d), P(sel_d), len(sel), P(dp), P(dg)))
+    dp_h, dg_h = dp.cpu().numpy(), dg.cpu().numpy()
+    err = {"pot_rel_l2": float(np.linalg.norm(u[sel] - dp_h) / np.linalg.norm(dp_h)),
+           "grad_rel_l2": float(np.linalg.norm(g[sel] - dg_h) / np.linalg.norm(dg_h))}
+    nfreq = 9 * 16 * 16
+    ntarget = f.nnodes - int(f.level_start[2])
+    # the spectral stage streams each far pair's source spectrum (FP32 complex) once and writes
+    # one spectrum per box twice (the transform and the target sums)
+    fft_bytes = 8.0 * nfreq * (f.npairs + 2 * ntarget)
+    return {"workload": f"{n:,} points from 16 Gaussians (sigma 0.01, centres U[0.1, 0.9]^3, seed 4), charges U(-1,1) "
+                        "as FP32 values; CubeKernelIndependent{3}(Laplace3D; p=8, pc=16, d=0.1), ppl=64, bbox (0,1); "
+                        "potential + gradient at the sources",
+            "precision": "FP32 spectra, far field (surface sums) and near field; FP64 dense translations",
+            "evals_per_s": n / (ms / 1e3), "ms_per_step": ms, "plan_s": plan_s, "levels": f.nlevels, "nodes": f.nnodes,
+            "far_pairs": f.npairs, "stages_ms": stages, "error": {"samples": len(sel), **err},
+            "spectral_m2l": {"bytes": fft_bytes, "GB_per_s": fft_bytes / (stages["m2l"] / 1e3) / 1e9,
+                             "note": "source spectra per far pair + spectra and target sums per box, / the m2l stage"}}
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(a):
     import torch
@@ -474,6 +562,7 @@ def run_ours(a):
                          f"tree + operators {r['tree_s']:.2f} s untimed"}
     serve = serving(fmmb, local, a.serve_requests, a.serve_slots) if a.serve_requests > 0 else None
     stokes = stokes_batched(fmmb, local, a.stokes_instances, a.serve_slots) if a.stokes_instances > 0 else None
+    ki = cube_ki(fmmb, torch, ctx, a.ki_points, 5, 3) if a.ki_points > 0 else None
     line = {
         "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -484,6 +573,7 @@ def run_ours(a):
         "configured_order_p10": side,
         "serving": serve,
         "stokes_batched": stokes,
+        "cube_ki": ki,
         "latency_ms": {"p50": pct(0.5), "p99": pct(0.99)},
         "fp64": {"value": replica_throughput(a.n, ms_fp64, world), "ms_per_step": ms_fp64},
         "mixed_vs_fp64": ms_fp64 / ms_mixed,
