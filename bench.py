@@ -54,7 +54,7 @@ def args_():
     a.add_argument("--samples", type=int, default=4096)
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--no-p10", action="store_true", help="skip the side measurement at the configured order p = 10")
-    a.add_argument("--serve-requests", type=int, default=96, help="requests of the serving measurement (0: skip it)")
+    a.add_argument("--serve-requests", type=int, default=384, help="requests of the serving measurement (0: skip it)")
     a.add_argument("--serve-slots", type=int, default=4)
     a.add_argument("--stokes-instances", type=int, default=64, help="instances of the batched Stokes measurement (0: skip it)")
     a.add_argument("--ki-points", type=int, default=2_000_000, help="points of the cube KI measurement (0: skip it)")

@@ -9,7 +9,7 @@
 //               transformed (k_ki_forward, half spectrum, FP32); per target the Hadamard sums
 //               Σ κ̂_o ⊙ σ̂_s over its far pairs (k_ki_hadamard: one frequency block of 64 per
 //               CTA, the block of the 316 kernel tables in shared memory, a warp per target,
-//               float4 loads of the sources' spectra); the inverse transform at the target's
+//               float4 loads of the sources' spectra, 8 pairs in flight); the inverse transform at the target's
 //               small-surface points added to its check potentials (k_ki_inverse)
 //   locals      the leaves' densities on their large surfaces, V·(S⁺Uᴴ·check) (DMMA GEMMs)
 //   L2T (a22)   the surface sums of the leaves' local densities (eval.cu) and the near field
@@ -32,6 +32,7 @@ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 constexpr int FB = 64;             // frequencies per block of the Hadamard stage
 constexpr int HAD_THREADS = 512;   // 16 warps, one target at a time each
+constexpr int HAD_UNROLL = 8;
 constexpr int SIDE = 2 * KI_PMAX;
 
 
@@ -179,16 +180,17 @@ __global__ void __launch_bounds__(HAD_THREADS) k_ki_hadamard(int first, int last
     if (k0 == k1) continue;
     float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
     int k = k0;
-    for (; k + 4 <= k1; k += 4) {
-      int2 pr[4];
-      float4 sv[4];
+    // HAD_UNROLL pairs' loads in flight per warp: the kernel is bound by their latency
+    for (; k + HAD_UNROLL <= k1; k += HAD_UNROLL) {
+      int2 pr[HAD_UNROLL];
+      float4 sv[HAD_UNROLL];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) pr[u] = tp[k + u];
+      for (int u = 0; u < HAD_UNROLL; ++u) pr[u] = tp[k + u];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < HAD_UNROLL; ++u)
         sv[u] = __ldg(reinterpret_cast<const float4*>(spec + (int64_t)pr[u].x * nfp + fb * FB) + lane);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < HAD_UNROLL; ++u) {
         const float4 tv = st[pr[u].y * (FB / 2) + lane];
         ar = fmaf(tv.x, sv[u].x, fmaf(-tv.y, sv[u].y, ar));
         ai = fmaf(tv.x, sv[u].y, fmaf(tv.y, sv[u].x, ai));
