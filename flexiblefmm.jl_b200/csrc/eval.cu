@@ -13,8 +13,8 @@
 //           (src/kernels.jl:20-24) and its summation order (colleagues in order, points in order)
 //   float   the mixed path: coordinates relative to the target leaf's centre, converted from FP64
 //           when staged (the FP32 differences carry an absolute error of ~2⁻²⁴·w instead of
-//           2⁻²⁴·|x|, so close pairs keep their accuracy); each batch summed in FP32, the batch
-//           sums accumulated in FP64
+//           2⁻²⁴·|x|, so close pairs keep their accuracy); two sources per packed f32x2
+//           instruction; each batch summed in FP32, the batch sums accumulated in FP64
 // Splitting the two keeps the near-field loop at a low register count (high occupancy); the
 // outputs are u then u + KC·near, the same arithmetic as one fused pass.
 #include "passes.cuh"
@@ -146,8 +146,88 @@ __device__ __forceinline__ void near_batch(const R4<R>* __restrict__ stg, int m,
   }
 }
 
+// packed FP32 pairs (the f32x2 instructions of sm_100: two lanes of arithmetic per instruction)
+__device__ __forceinline__ uint64_t pk2(float a, float b) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void upk2(uint64_t v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// The FP32 batch with two sources per instruction: the batch staged as 16 source pairs
+// {x₀ x₁ y₀ y₁}{z₀ z₁ w₀ w₁}; each pair's arithmetic in packed f32x2 (the same operations and
+// per-element rounding as near_batch), the two running sums of every quantity added at the end;
+// an odd last source takes the scalar body. CHECK skips flat index `is`.
+template <bool CHECK>
+__device__ __forceinline__ void near_batch_f32x2(const float4* __restrict__ pr, int m, int is, float fx, float fy,
+                                                 float fz, float& bp, float& bx, float& by, float& bz) {
+  const uint64_t fx2 = pk2(fx, fx), fy2 = pk2(fy, fy), fz2 = pk2(fz, fz);
+  uint64_t p2 = pk2(0.f, 0.f), x2 = p2, y2 = p2, z2 = p2;
+  const int np = m >> 1;
+  auto body = [&](int k) {
+    const float4 a = pr[2 * k], b = pr[2 * k + 1];
+    const uint64_t dx = sub2(fx2, pk2(a.x, a.y)), dy = sub2(fy2, pk2(a.z, a.w)), dz = sub2(fz2, pk2(b.x, b.y));
+    const uint64_t r2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+    float ra, rb;
+    upk2(r2, ra, rb);
+    float ia = rsqrt_ftz(ra), ib = rsqrt_ftz(rb);
+    if (CHECK && 2 * k == is) ia = 0.f;
+    if (CHECK && 2 * k + 1 == is) ib = 0.f;
+    const uint64_t ir = pk2(ia, ib);
+    const uint64_t qir = mul2(pk2(b.z, b.w), ir);
+    const uint64_t qir3 = mul2(mul2(qir, ir), ir);
+    p2 = add2(p2, qir);
+    x2 = fma2(qir3, dx, x2);
+    y2 = fma2(qir3, dy, y2);
+    z2 = fma2(qir3, dz, z2);
+  };
+  if (np == 16) {
+#pragma unroll 8
+    for (int k = 0; k < 16; ++k) body(k);
+  } else {
+#pragma unroll 2
+    for (int k = 0; k < np; ++k) body(k);
+  }
+  float a0, a1;
+  upk2(p2, a0, a1); bp += a0 + a1;
+  upk2(x2, a0, a1); bx += a0 + a1;
+  upk2(y2, a0, a1); by += a0 + a1;
+  upk2(z2, a0, a1); bz += a0 + a1;
+  if (m & 1) {                                   // the odd last source
+    const float* f = reinterpret_cast<const float*>(pr + 2 * np);
+    const float dx = fx - f[0], dy = fy - f[2], dz = fz - f[4];
+    float ir = rsqrt_ftz(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+    if (CHECK && m - 1 == is) ir = 0.f;
+    const float qir = f[6] * ir, qir3 = qir * ir * ir;
+    bp += qir;
+    bx = fmaf(qir3, dx, bx);
+    by = fmaf(qir3, dy, by);
+    bz = fmaf(qir3, dz, bz);
+  }
+}
+
 template <typename R, bool SELF, bool YK>
-__global__ void __launch_bounds__(NEAR_WARPS * 32) k_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
+__global__ void __launch_bounds__(NEAR_WARPS * 32, 5) k_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
                                                          const int* __restrict__ gcount, int ngroups,
                                                          const double* __restrict__ tx, const double* __restrict__ ty,
                                                          const double* __restrict__ tz, const int* __restrict__ tout,
@@ -206,7 +286,16 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32) k_near(const int* __restrict_
     load_batch(sw, 0, lane, S, xs, ys, zs, q, sx, sy, sz, sq);
     for (int b = 0; 32 * b < S; ++b) {
       R4<R>* stg = sw.stg[b & 1];
-      stg[lane] = R4<R>{(R)(sx - cx), (R)(sy - cy), (R)(sz - cz), (R)sq};
+      if constexpr (sizeof(R) == 4) {
+        // the FP32 path stages source pairs: lane l into pair l/2, slot l%2
+        float* f = reinterpret_cast<float*>(stg) + 8 * (lane >> 1) + (lane & 1);
+        f[0] = (float)(sx - cx);
+        f[2] = (float)(sy - cy);
+        f[4] = (float)(sz - cz);
+        f[6] = (float)sq;
+      } else {
+        stg[lane] = R4<R>{(R)(sx - cx), (R)(sy - cy), (R)(sz - cz), (R)sq};
+      }
       __syncwarp();
       if (32 * (b + 1) < S) load_batch(sw, b + 1, lane, S, xs, ys, zs, q, sx, sy, sz, sq);
       const int m = min(32, S - 32 * b);
@@ -216,9 +305,10 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32) k_near(const int* __restrict_
         if (chk) near_batch<R, true, YK>(stg, m, fself - 32 * b, fx, fy, fz, np, nx, ny, nz, kappa);
         else near_batch<R, false, YK>(stg, m, 0, fx, fy, fz, np, nx, ny, nz, kappa);
       } else {
-        R bp = 0, bx = 0, by = 0, bz = 0;
-        if (chk) near_batch<R, true>(stg, m, fself - 32 * b, fx, fy, fz, bp, bx, by, bz);
-        else near_batch<R, false>(stg, m, 0, fx, fy, fz, bp, bx, by, bz);
+        float bp = 0, bx = 0, by = 0, bz = 0;
+        const float4* pr = reinterpret_cast<const float4*>(stg);
+        if (chk) near_batch_f32x2<true>(pr, m, fself - 32 * b, fx, fy, fz, bp, bx, by, bz);
+        else near_batch_f32x2<false>(pr, m, 0, fx, fy, fz, bp, bx, by, bz);
         np += bp;
         nx += bx;
         ny += by;
