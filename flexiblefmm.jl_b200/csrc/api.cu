@@ -180,7 +180,8 @@ void plan_from_device_points(fmmb_cache* cache, const double* xyz, int64_t n, co
   {
     std::lock_guard<std::mutex> lk(C.mu);
     if (!C.uploaded) {
-      C.host = build_operators(C.p, C.W0);
+      // the harmonic tables and the symmetry classes the lists use (the KI methods take order 2)
+      C.host = build_operators(C.method == FMMB_METHOD_SPHERICAL_HARMONICS ? C.p : 2, C.W0);
       upload_operators(C);
     }
   }
@@ -207,6 +208,7 @@ void plan_from_device_points(fmmb_cache* cache, const double* xyz, int64_t n, co
   }
   build_lists(P);
   if (C.method == FMMB_METHOD_CUBE_KI) ki_prepare(P);   // its operators, its target-major pairs
+  if (C.method == FMMB_METHOD_KI_CIRCLE) kic_prepare(P);
   h->parent = cache;
   std::lock_guard<std::mutex> lk(g_handles);
   ++cache->deps;
@@ -284,8 +286,31 @@ int fmmb_ctx_synchronize(fmmb_ctx* ctx) {  // state errors surface at the next h
 int fmmb_cache_create(fmmb_ctx* ctx, const fmmb_method_desc* m, fmmb_cache** out) {
   return guard([&] {
     require(ctx && m && out, FMMB_ERR_ARGUMENT, "null argument");
-    require(m->method == FMMB_METHOD_SPHERICAL_HARMONICS || m->method == FMMB_METHOD_CUBE_KI, FMMB_ERR_UNSUPPORTED,
-            "the methods provided are SphericalHarmonics, StokesHarmonics and CubeKernelIndependent{3}");
+    require(m->method == FMMB_METHOD_SPHERICAL_HARMONICS || m->method == FMMB_METHOD_CUBE_KI ||
+                m->method == FMMB_METHOD_KI_CIRCLE,
+            FMMB_ERR_UNSUPPORTED,
+            "the methods provided are SphericalHarmonics, StokesHarmonics, CubeKernelIndependent{3} and KernelIndependent");
+    if (m->method == FMMB_METHOD_KI_CIRCLE) {
+      // KernelIndependent(Laplace2D(); nequiv = p, pinv_rtol) (src/operators/kifmm.jl:17-33), FP64
+      require(m->kernel == FMMB_KERNEL_LAPLACE2D, FMMB_ERR_UNSUPPORTED, "the circle KI method is provided for Laplace2D");
+      require(m->p >= 4, FMMB_ERR_ARGUMENT, "nequiv must be at least 4");
+      require(m->p <= 64, FMMB_ERR_UNSUPPORTED, "nequiv above 64 is not provided");
+      require(m->pinv_rtol >= 0 && m->pinv_rtol < 1, FMMB_ERR_ARGUMENT, "pinv_rtol must lie in [0, 1)");
+      std::unique_ptr<fmmb_cache> h(new fmmb_cache());
+      h->c.ctx = &ctx->c;
+      h->parent = ctx;
+      h->c.method = FMMB_METHOD_KI_CIRCLE;
+      h->c.p = m->p;
+      h->c.np = m->p;
+      h->c.ld = 64;
+      h->c.kernel = FMMB_KERNEL_LAPLACE2D;
+      h->c.nexp = 1;
+      h->c.ki_rtol = m->pinv_rtol > 0 ? m->pinv_rtol : 50 * 2.220446049250313e-16;
+      std::lock_guard<std::mutex> lk(g_handles);
+      ++ctx->deps;
+      *out = h.release();
+      return;
+    }
     if (m->method == FMMB_METHOD_CUBE_KI) {
       // CubeKernelIndependent{3}(Laplace3D(); p, pc = 2p, d = 0.1, pinv_rtol) (src/operators/cubeki.jl:35-42)
       require(m->kernel == FMMB_KERNEL_LAPLACE3D, FMMB_ERR_UNSUPPORTED, "the cube KI method is provided for Laplace3D");
@@ -481,6 +506,8 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
     FMMB_CUDA(cudaMemsetAsync(S.Pl.p, 0, S.Pl.bytes(), s));
     if (P.cache->method == FMMB_METHOD_CUBE_KI) {
       ki_state(S);   // its spectra, check and local buffers; the precision selects the far field's and P2P's
+    } else if (P.cache->method == FMMB_METHOD_KI_CIRCLE) {
+      kic_state(S);
     } else if (precision == FMMB_PRECISION_MIXED) {
       std::lock_guard<std::mutex> lk(P.cache->mu);
       prepare_mixed_operators(*P.cache);

@@ -108,7 +108,9 @@ __device__ __forceinline__ void load_batch(const NearWarp<R>& sw, int b, int lan
 // one batch of m staged sources against this lane's target; CHECK skips flat index `is`.
 // YK (FP64): the Yukawa pair e^{−κr}/r and its radial derivative −e^{−κr}(1 + κr)/r²
 // (src/kernels.jl:235-242)
-template <typename R, bool CHECK, bool YK = false>
+// KIND 2 (FP64): the Laplace2D pair c·log r², c = −1/(4π), as KC·(−τ log r²) and gradient
+// −KC·(2τ/r²)·d (src/kernels.jl:58-66; the points share z, so r² is the planar distance)
+template <typename R, bool CHECK, int YK = 0>
 __device__ __forceinline__ void near_batch(const R4<R>* __restrict__ stg, int m, int is, R fx, R fy, R fz, R& bp, R& bx,
                                            R& by, R& bz, double kappa = 0) {
   auto body = [&](int i) {
@@ -124,7 +126,11 @@ __device__ __forceinline__ void near_batch(const R4<R>* __restrict__ stg, int m,
     }
     if (CHECK && i == is) ir = R(0);
     R qir, qir3;
-    if constexpr (YK) {
+    if constexpr (YK == 2) {
+      const bool self = CHECK && i == is;
+      qir = self ? R(0) : -sv.w * log(r2);
+      qir3 = self ? R(0) : 2 * sv.w / r2;
+    } else if constexpr (YK == 1) {
       const double r = r2 * ir, e = exp(-kappa * r);
       qir = sv.w * e * ir;
       qir3 = qir * (1 + kappa * r) * ir * ir;
@@ -226,7 +232,7 @@ __device__ __forceinline__ void near_batch_f32x2(const float4* __restrict__ pr, 
   }
 }
 
-template <typename R, bool SELF, bool YK>
+template <typename R, bool SELF, int YK>
 __global__ void __launch_bounds__(NEAR_WARPS * 32, 5) k_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
                                                          const int* __restrict__ gcount, int ngroups,
                                                          const double* __restrict__ tx, const double* __restrict__ ty,
@@ -391,6 +397,57 @@ __global__ void __launch_bounds__(128) k_ki_l2t(const int* __restrict__ gnode, c
   }
 }
 
+// The circle method's far field (l2t over the large circle, src/operators/ki_common.jl:293-327):
+// Σ_k c·log|x − y_k|² L_k and its gradient Σ_k 2c (x − y_k)/|x − y_k|² L_k, y_k on the leaf's
+// circle of radius (4 − √2)/2·w, FP64; writes the outputs (the near field adds to them)
+__global__ void __launch_bounds__(128) k_kic_l2t(const int* __restrict__ gnode, const int* __restrict__ gstart,
+                                                 const int* __restrict__ gcount, int ngroups, const double* __restrict__ tx,
+                                                 const double* __restrict__ ty, const int* __restrict__ tout,
+                                                 const int4* __restrict__ cell, const double* __restrict__ Ll, int N,
+                                                 Geometry geo, int outputs, double* __restrict__ pot,
+                                                 double* __restrict__ grad) {
+  __shared__ double sL[4][64], sx[4][64], sy[4][64];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x * 4 + warp;
+  if (grp >= ngroups) return;
+  const int leaf = gnode[grp];
+  const int4 c = cell[leaf];
+  const double w = ldexp(geo.W0, -c.w);
+  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w);
+  for (int k = lane; k < N; k += 32) {
+    double sn, cs;
+    sincospi(2.0 * k / N, &sn, &cs);
+    sL[warp][k] = Ll[(int64_t)leaf * 64 + k];
+    sx[warp][k] = cx + KIC_LARGE * w * cs;
+    sy[warp][k] = cy + KIC_LARGE * w * sn;
+  }
+  __syncwarp();
+  const int t0 = gstart[grp], nt = gcount[grp];
+  for (int base = 0; base < nt; base += 32) {
+    const int k = t0 + base + lane;
+    const bool act = base + lane < nt;
+    const double x = act ? tx[k] : cx, y = act ? ty[k] : cy;
+    double u = 0, gx = 0, gy = 0;
+    for (int q = 0; q < N; ++q) {
+      const double dx = x - sx[warp][q], dy = y - sy[warp][q];
+      const double r2 = fma(dy, dy, dx * dx);
+      u = fma(sL[warp][q], log(r2), u);
+      const double g = sL[warp][q] / r2;
+      gx = fma(g, dx, gx);
+      gy = fma(g, dy, gy);
+    }
+    if (act) {
+      const int o = tout[k];
+      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = -KC * u;
+      if (outputs & FMMB_OUTPUT_GRADIENT) {
+        grad[3 * (int64_t)o] = -2 * KC * gx;
+        grad[3 * (int64_t)o + 1] = -2 * KC * gy;
+        grad[3 * (int64_t)o + 2] = 0.0;
+      }
+    }
+  }
+}
+
 template <int P>
 void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
                 const double* tz, const int* tout, int outputs, double* pot, double* grad) {
@@ -406,7 +463,7 @@ void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount
   FMMB_LAUNCH_CHECK();
 }
 
-template <typename R, bool SELF, bool YK = false>
+template <typename R, bool SELF, int YK = 0>
 void launch_near(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
                  const double* tz, const int* tout, int outputs, double* pot, double* grad) {
   Plan& P_ = *S.plan;
@@ -421,6 +478,15 @@ void launch_near(State& S, const int* gnode, const int* gstart, const int* gcoun
 void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
                      const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad) {
   if (ng == 0) return;
+  if (S.plan->cache->method == FMMB_METHOD_KI_CIRCLE) {
+    Plan& P_ = *S.plan;
+    k_kic_l2t<<<(ng + 3) / 4, 128, 0, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tout, P_.cell.p, S.ki_ll.p,
+                                                        P_.cache->np, geometry(P_), outputs, pot, grad);
+    FMMB_LAUNCH_CHECK();
+    if (self) launch_near<double, true, 2>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+    else launch_near<double, false, 2>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+    return;
+  }
   if (S.plan->cache->method == FMMB_METHOD_CUBE_KI) {
     Plan& P_ = *S.plan;
     Cache& C = *P_.cache;

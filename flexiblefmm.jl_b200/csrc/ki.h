@@ -26,4 +26,19 @@ struct KIHost {
 };
 KIHost build_ki_operators(int p, int pc, double d, double rtol, double w);
 
+// KernelIndependent(Laplace2D(); nequiv) (src/operators/kifmm.jl): circles of N equispaced
+// points, radius √2/2·w (small: upward equivalent, downward check) and (4 − √2)/2·w (large),
+// the operators of one width (the log kernel is not homogeneous), column-major and zero-padded
+// to CLD = roundup(N, 64): the factored pseudo-inverses (V, S⁺Uᴴ each CLD × CLD), M2M
+// (CLD × 8·CLD) and L2L (8·CLD × CLD) over the eight child slots of the embedding octree (a slot's
+// circle centre is its (x, y) offset; both z halves map alike), and the M2L check maps of the 316
+// far offsets (CLD × CLD each; only the in-plane offsets, oz = 0, are filled)
+struct KICircleLevel {
+  int n = 0, ld = 0, rank_up = 0, rank_down = 0;
+  std::vector<double> up_v, up_su, down_v, down_su, m2m, l2l, m2l;
+};
+KICircleLevel build_ki_circle_level(int n, double rtol, double w);
+constexpr double KIC_SMALL = 0.70710678118654752440;   // √2/2
+constexpr double KIC_LARGE = 1.29289321881345247560;   // (4 − √2)/2
+
 }  // namespace fmmb

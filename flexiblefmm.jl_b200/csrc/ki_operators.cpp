@@ -225,7 +225,93 @@ void pinv_factors(int m, int n, const std::vector<double>& A, double rtol, std::
   }
 }
 
+// the 2D Laplace kernel c·log(r²), c = −1/(4π) (src/kernels.jl:58-66), between points in the plane
+inline double lap2(const double* x, const double* y) {
+  const double dx = x[0] - y[0], dy = x[1] - y[1];
+  return -KCL * std::log(dx * dx + dy * dy);
+}
+
+// N equispaced points on the circle of radius r about (cx, cy), angle 2πk/N (kifmm.jl:69-71)
+std::vector<double> circle(int N, double r, double cx = 0, double cy = 0) {
+  std::vector<double> p(2 * N);
+  for (int k = 0; k < N; ++k) {
+    const double t = 2 * M_PI / N * k;
+    p[2 * k] = cx + r * std::cos(t);
+    p[2 * k + 1] = cy + r * std::sin(t);
+  }
+  return p;
+}
+
+// targets × sources, column-major, of the 2D kernel
+std::vector<double> kernel_matrix2(const std::vector<double>& src, const std::vector<double>& tgt) {
+  const int ns = (int)src.size() / 2, nt = (int)tgt.size() / 2;
+  std::vector<double> K((size_t)nt * ns);
+  for (int j = 0; j < ns; ++j)
+    for (int i = 0; i < nt; ++i) K[(size_t)j * nt + i] = lap2(&tgt[2 * i], &src[2 * j]);
+  return K;
+}
+
 }  // namespace
+
+KICircleLevel build_ki_circle_level(int n, double rtol, double w) {
+  require(n >= 4 && n <= 64, FMMB_ERR_ARGUMENT, "nequiv must lie in 4..64");
+  KICircleLevel c;
+  c.n = n;
+  c.ld = 64;
+  const int L = c.ld;
+  const std::vector<double> small = circle(n, KIC_SMALL * w), large = circle(n, KIC_LARGE * w);
+  std::vector<double> uv, usu, dv, dsu;
+  pinv_factors(n, n, kernel_matrix2(small, large), rtol, uv, usu, c.rank_up);
+  pinv_factors(n, n, kernel_matrix2(large, small), rtol, dv, dsu, c.rank_down);
+  // M2Mc: each child slot's small circle (centre (δx − ½, δy − ½)·w/2) seen on the large one;
+  // L2Lc: the large circle seen on each child's small one
+  std::vector<double> M2Mc((size_t)n * NCH * n), L2Lc((size_t)NCH * n * n);
+  for (int k = 0; k < NCH; ++k) {
+    const double cx = ((k & 1) - 0.5) * (w / 2), cy = (((k >> 1) & 1) - 0.5) * (w / 2);
+    const std::vector<double> ch = circle(n, KIC_SMALL * w / 2, cx, cy);
+    const std::vector<double> a = kernel_matrix2(ch, large), b = kernel_matrix2(large, ch);
+    std::copy(a.begin(), a.end(), M2Mc.begin() + (size_t)k * n * n);
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) L2Lc[(size_t)j * NCH * n + k * n + i] = b[(size_t)j * n + i];
+  }
+  const int ru = c.rank_up, rd = c.rank_down;
+  const std::vector<double> m2m = matmul(n, ru, NCH * n, uv, matmul(ru, n, NCH * n, usu, M2Mc));
+  const std::vector<double> l2l = matmul(NCH * n, rd, n, matmul(NCH * n, n, rd, L2Lc, dv), dsu);
+  // zero-padded copies
+  auto padm = [](const std::vector<double>& a, int rows, int cols, int R, int C) {
+    std::vector<double> o((size_t)R * C, 0.0);
+    for (int j = 0; j < cols; ++j)
+      for (int i = 0; i < rows; ++i) o[(size_t)j * R + i] = a[(size_t)j * rows + i];
+    return o;
+  };
+  c.up_v = padm(uv, n, ru, L, L);
+  c.up_su = padm(usu, ru, n, L, L);
+  c.down_v = padm(dv, n, rd, L, L);
+  c.down_su = padm(dsu, rd, n, L, L);
+  c.m2m.assign((size_t)L * NCH * L, 0.0);
+  c.l2l.assign((size_t)NCH * L * L, 0.0);
+  for (int k = 0; k < NCH; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        c.m2m[(size_t)(k * L + j) * L + i] = m2m[(size_t)(k * n + j) * n + i];
+        c.l2l[(size_t)j * NCH * L + k * L + i] = l2l[(size_t)j * NCH * n + k * n + i];
+      }
+  // M2L: the source's small circle at offset o·w seen on the target's small circle
+  c.m2l.assign((size_t)NFAR * L * L, 0.0);
+  int f = 0;
+  for (int t = 0; t < 343; ++t) {
+    const int o[3] = {t % 7 - 3, (t / 7) % 7 - 3, (t / 49) % 7 - 3};
+    if (std::max({std::abs(o[0]), std::abs(o[1]), std::abs(o[2])}) < 2) continue;
+    if (o[2] == 0) {
+      const std::vector<double> src = circle(n, KIC_SMALL * w, o[0] * w, o[1] * w);
+      const std::vector<double> A = kernel_matrix2(src, small);
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) c.m2l[(size_t)f * L * L + (size_t)j * L + i] = A[(size_t)j * n + i];
+    }
+    ++f;
+  }
+  return c;
+}
 
 KIHost build_ki_operators(int p, int pc, double d, double rtol, double w) {
   require(p >= 2 && p <= KI_PMAX, FMMB_ERR_ARGUMENT, "the cube KI method takes 2 ≤ p ≤ " + std::to_string(KI_PMAX));

@@ -418,6 +418,7 @@ void gemm_columns(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols
 
 int p2m(State& S) {
   if (S.plan->cache->method == FMMB_METHOD_CUBE_KI) return ki_p2m(S);
+  if (S.plan->cache->method == FMMB_METHOD_KI_CIRCLE) return kic_p2m(S);
   switch (S.plan->cache->p) {
 #define X(pp) case pp: launch_p2m<pp>(S, S.q.p, S.M.p, (int64_t)S.plan->cache->ld); break;
     FMMB_P_CASES(X)
@@ -462,6 +463,7 @@ int l2l_sweep(State& S) {
   }
   // the kernel-independent method: the leaves' local densities from their check potentials
   if (C.method == FMMB_METHOD_CUBE_KI) launches += ki_leaf_locals(S);
+  if (C.method == FMMB_METHOD_KI_CIRCLE) launches += kic_leaf_locals(S);
   return launches;
 }
 
@@ -471,6 +473,7 @@ int m2l_stage(State& S) {
   Plan& P = *S.plan;
   FMMB_CUDA(cudaMemsetAsync(S.Pl.p, 0, S.Pl.bytes(), P.ctx->stream));
   if (P.cache->method == FMMB_METHOD_CUBE_KI) return ki_m2l(S);
+  if (P.cache->method == FMMB_METHOD_KI_CIRCLE) return kic_m2l(S);
   if (P.h_blocks.empty()) return 0;
   if (S.precision == FMMB_PRECISION_MIXED) {
     m2l_mixed(S);

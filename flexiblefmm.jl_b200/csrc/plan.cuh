@@ -64,6 +64,10 @@ struct Cache {
   DBuf<double> ki_large, ki_upv, ki_upsu, ki_downv, ki_downsu, ki_m2m, ki_l2l;
   DBuf<int> ki_embed;
   DBuf<float2> ki_tab, ki_tw;
+  // KernelIndependent(Laplace2D()): circle operators per width (keyed by the exponent e of
+  // w = ldexp(W0, e)), built on the host when a plan first needs that width
+  struct CircleLevel { DBuf<double> upv, upsu, downv, downsu, m2m, l2l, m2l; };
+  std::map<int, std::unique_ptr<CircleLevel>> kic_levels;
 };
 
 // One M2L work block: TB consecutive nodes of one level (the targets), their far pairs
@@ -118,6 +122,10 @@ struct Plan {
   DBuf<int2> tp;
   DBuf<int> ki_leaves;                    // every real leaf (with sources or not)
   int n_ki_leaves = 0;
+  // the circle method: per level its pseudo-inverse factors, and the level ranges of the
+  // childless nodes with sources and of the real leaves (both lists are in node order)
+  std::vector<const double*> kic_upv, kic_upsu, kic_downv, kic_downsu;
+  std::vector<int> s2m_level_start, ki_leaf_level_start;
 };
 
 struct State {
@@ -164,6 +172,12 @@ void ki_state(State& S);
 int ki_p2m(State& S);
 int ki_m2l(State& S);
 int ki_leaf_locals(State& S);
+// kic.cu: KernelIndependent(Laplace2D()) on circles, the points in the plane z = 0 of the octree
+void kic_prepare(Plan& P);
+void kic_state(State& S);
+int kic_p2m(State& S);
+int kic_m2l(State& S);
+int kic_leaf_locals(State& S);
 // yukawa.cu: SphericalHarmonics(Yukawa3D(κ)) — the operators of the plan's widths (built on the
 // device by projection when a width is first used) and the per-level factors
 void yukawa_prepare(Plan& P);

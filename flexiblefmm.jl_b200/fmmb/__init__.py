@@ -32,6 +32,7 @@ OUTPUT_GRADIENT = 2
 KERNEL_LAPLACE3D = 1
 KERNEL_YUKAWA3D = 2
 KERNEL_STOKESLET3D = 3
+KERNEL_LAPLACE2D = 4
 
 
 class FMMBError(RuntimeError):
@@ -172,6 +173,23 @@ def _points(x):
     return x
 
 
+def _points2(x):
+    """(N, 2) points of a 2D method, embedded as (N, 3) in the plane z = 0."""
+    x = np.asarray(x, dtype=np.float64)
+    if x.ndim != 2 or x.shape[1] != 2:
+        raise DimensionMismatch(2, f"expected an (N, 2) array of points, got {x.shape}")
+    return np.ascontiguousarray(np.concatenate([x, np.zeros((x.shape[0], 1))], axis=1))
+
+
+def _pts(fmm_or_method, x):
+    m = getattr(fmm_or_method, "method", fmm_or_method)
+    return _points2(x) if getattr(m, "dimension", 3) == 2 else _points(x)
+
+
+def _grad_out(fmm, g):
+    return g[:, :2].copy() if getattr(fmm.method, "dimension", 3) == 2 else g
+
+
 # ---------------------------------------------------------------- kernels, methods, outputs
 class Laplace3D:
     """Free-space Laplace Green's function 1/(4π|t − s|) (src/kernels.jl:179-200)."""
@@ -203,6 +221,32 @@ class StokesHarmonics:
         if tol != 0:
             raise Unsupported(6, "low-rank translations (tol > 0) are not provided")
         self.kernel, self.p, self.tol = kernel, int(p), 0.0
+
+
+class Laplace2D:
+    """Free-space Laplace Green's function −log|t − s|/2π = c·log r², c = −1/(4π)
+    (src/kernels.jl:53-66)."""
+    c = -1.0 / (4.0 * np.pi)
+
+
+class KernelIndependent:
+    """KernelIndependent(kernel; nequiv=50, pinv_rtol=50·eps(Float64)) (src/operators/kifmm.jl:17-33):
+    the 2D kernel-independent method on circles of nequiv equispaced points. Laplace2D; points
+    (N, 2), gradients (N, 2); FP64."""
+    dimension = 2
+
+    def __init__(self, kernel, nequiv=50, pinv_rtol=None):
+        if not isinstance(kernel, Laplace2D):
+            raise ArgumentError(1, "the device circle KI method is written for Laplace2D")
+        if nequiv < 4:
+            raise ArgumentError(1, "nequiv must be at least 4")
+        self.kernel, self.nequiv, self.p = kernel, int(nequiv), int(nequiv)
+        self.pinv_rtol = 50 * float(np.finfo(np.float64).eps) if pinv_rtol is None else float(pinv_rtol)
+        self.tol = 0.0
+
+    @property
+    def nsurface(self):
+        return self.nequiv
 
 
 class CubeKernelIndependent:
@@ -302,6 +346,8 @@ class OperatorCache:
         self.ctx = ctx or default_context()
         if isinstance(method, CubeKernelIndependent):
             d = _MethodDesc(2, KERNEL_LAPLACE3D, method.p, 0, 0.0, 0.0, method.pc, 0, method.d, method.pinv_rtol)
+        elif isinstance(method, KernelIndependent):
+            d = _MethodDesc(3, KERNEL_LAPLACE2D, method.nequiv, 0, 0.0, 0.0, 0, 0, 0.0, method.pinv_rtol)
         else:
             if isinstance(method, StokesHarmonics):
                 kernel, kappa = KERNEL_STOKESLET3D, 0.0
@@ -337,10 +383,17 @@ class FMM:
         self.method, self.cache = method, cache
         opts = _TreeOpts()
         opts.ppl, opts.max_levels = int(ppl), int(max_levels)
+        two_d = getattr(method, "dimension", 3) == 2
+        if two_d and bbox is None:
+            bbox = square_bbox2(sources)
         if bbox is not None:
             opts.has_bbox = 1
-            for d in range(3):
-                opts.origin[d] = float(bbox[0][d])
+            if two_d:                            # the square as the cube's mid-plane z = 0
+                opts.origin[0], opts.origin[1] = float(bbox[0][0]), float(bbox[0][1])
+                opts.origin[2] = -float(bbox[1]) / 2
+            else:
+                for d in range(3):
+                    opts.origin[d] = float(bbox[0][d])
             opts.width = float(bbox[1])
         h = C.c_void_p()
         if device_points is not None:           # (pointer, n) of a 3×n device array
@@ -348,7 +401,7 @@ class FMM:
             _check(lib().fmmb_plan_create_dev(cache._h, C.c_void_p(ptr), int(n), C.byref(opts), C.byref(h)))
             self.N = int(n)
         else:
-            x = _points(sources)
+            x = _pts(method, sources)
             if x.shape[0] == 0:
                 raise ArgumentError(1, "no points")
             _check(lib().fmmb_plan_create(cache._h, _ptr(x), x.shape[0], C.byref(opts), C.byref(h)))
@@ -434,7 +487,7 @@ def _densities(tau, n):
 
 def build_expansions_(state, fmm, sources, tau):
     """build_expansions!(state, fmm, sources, τ) (src/fmm.jl:270-298)."""
-    x = _points(sources)
+    x = _pts(fmm, sources)
     if x.shape[0] != fmm.N:
         raise DimensionMismatch(2, f"expected {fmm.N} sources in group 1")
     t = _densities(tau, fmm.N)
@@ -458,6 +511,7 @@ def evaluate_at_sources(fmm, state, g=1, output=Potential()):
     else:
         out = np.zeros((fmm.N, 3))
         _check(lib().fmmb_evaluate_at_sources(state._h, flag, None, _ptr(out)))
+        out = _grad_out(fmm, out)
     return out
 
 
@@ -465,13 +519,13 @@ def evaluate_at_sources_both(fmm, state):
     """Potential and gradient at the sources in one pass."""
     pot, grad = np.zeros(fmm.N), np.zeros((fmm.N, 3))
     _check(lib().fmmb_evaluate_at_sources(state._h, 3, _ptr(pot), _ptr(grad)))
-    return pot, grad
+    return pot, _grad_out(fmm, grad)
 
 
 def evaluate(fmm, state, targets, output=Potential()):
     """evaluate(fmm, state, targets; output) (src/evaluate.jl:81-102)."""
     flag = _output_flag(output)
-    tg = _points(targets)
+    tg = _pts(fmm, targets)
     nt = tg.shape[0]
     if flag == OUTPUT_POTENTIAL:
         out = np.zeros(nt)
@@ -479,20 +533,21 @@ def evaluate(fmm, state, targets, output=Potential()):
     else:
         out = np.zeros((nt, 3))
         _check(lib().fmmb_evaluate(state._h, _ptr(tg), nt, flag, None, _ptr(out)))
+        out = _grad_out(fmm, out)
     return out
 
 
 def device_matvec(fmm, state, sources, tau, output=Potential()):
     """device_matvec!(out, plan, (sources, τ)) (src/device_passes.jl:619-640)."""
     flag = _output_flag(output)
-    x = _points(sources)
+    x = _pts(fmm, sources)
     t = _densities(tau, fmm.N)
     if x.shape[0] != fmm.N:
         raise DimensionMismatch(2, f"expected {fmm.N} sources")
     pot = np.zeros(fmm.N) if flag == OUTPUT_POTENTIAL else None
     grad = np.zeros((fmm.N, 3)) if flag == OUTPUT_GRADIENT else None
     _check(lib().fmmb_matvec(state._h, _ptr(x), _ptr(t), fmm.N, flag, _ptr(pot), _ptr(grad)))
-    return pot if flag == OUTPUT_POTENTIAL else grad
+    return pot if flag == OUTPUT_POTENTIAL else _grad_out(fmm, grad)
 
 
 # ---------------------------------------------------------------- the request server
@@ -570,6 +625,15 @@ class Server:
 
 
 # ---------------------------------------------------------------- the Stokes plan API
+def square_bbox2(points):
+    """square_bbox of 2D points (src/tree/tree.jl:97-113): the square of their largest extent."""
+    x = np.asarray(points, dtype=np.float64)
+    if x.ndim != 2 or x.shape[1] != 2:
+        raise DimensionMismatch(2, f"expected an (N, 2) array of points, got {x.shape}")
+    o, w = square_bbox(np.concatenate([x, np.zeros((x.shape[0], 1))], axis=1))
+    return (o[0], o[1]), w
+
+
 def square_bbox(points):
     """square_bbox(points) (src/tree/tree.jl:97-113): the cube of the points' largest extent
     about their midpoint, widened by 4 ulps at a time until every point is inside."""

@@ -35,8 +35,12 @@ extern "C" {
 #define FMMB_KERNEL_LAPLACE3D 1
 #define FMMB_KERNEL_YUKAWA3D 2    /* e^{−κr}/(4πr), SphericalHarmonics(Yukawa3D(κ); p): FP64 path, operators per width */
 #define FMMB_KERNEL_STOKESLET3D 3 /* StokesHarmonics(Stokeslet3D(); p): FP64 path, Stokeslet densities, velocities */
+#define FMMB_KERNEL_LAPLACE2D 4   /* c·log r², c = −1/(4π): the circle KI method, points in the plane z = 0 */
 #define FMMB_METHOD_SPHERICAL_HARMONICS 1
 #define FMMB_METHOD_CUBE_KI 2 /* CubeKernelIndependent{3}(Laplace3D(); p, pc, d): spectral (FFT) M2L */
+#define FMMB_METHOD_KI_CIRCLE 3 /* KernelIndependent(Laplace2D(); nequiv = p) (src/operators/kifmm.jl:17-33): 2D
+                                   points given as 3×n with z = 0 (the binding embeds them), bbox origin
+                                   z = −width/2; gradients come back with a zero z component */
 
 #define FMMB_PRECISION_FP64 0  /* the plain path: FP64 everywhere (the drop-in) */
 #define FMMB_PRECISION_MIXED 1 /* split-precision tensor-core M2L, FP32 compensated near field */
@@ -57,15 +61,15 @@ typedef struct fmmb_state fmmb_state;
 typedef struct {
   int32_t method;  /* FMMB_METHOD_SPHERICAL_HARMONICS or FMMB_METHOD_CUBE_KI */
   int32_t kernel;  /* FMMB_KERNEL_* (the cube KI method: FMMB_KERNEL_LAPLACE3D) */
-  int32_t p;       /* harmonics: expansion degree, 1..20; cube KI: points per edge, 2..12 */
+  int32_t p;       /* harmonics: expansion degree, 1..20; cube KI: points per edge, 2..12; circle KI: nequiv, 4..64 */
   int32_t reserved;
   double tol;      /* 0: dense class operators (the only form this build provides) */
   double kappa;    /* the Yukawa screening κ > 0 (FMMB_KERNEL_YUKAWA3D); ignored otherwise */
   int32_t pc;      /* cube KI: points per edge of the large surface; 0: 2p */
   int32_t reserved2;
   double d;        /* cube KI: the surfaces' margin, in (0, 2/3); 0: 0.1 */
-  double pinv_rtol; /* cube KI: the pseudo-inverses' truncation; 0: 50·eps(Float32), the reference's default
-                       for Laplace3D(Float32) */
+  double pinv_rtol; /* KI: the pseudo-inverses' truncation; 0: the reference's default, 50·eps(Float32) for
+                       the cube method (Laplace3D(Float32)), 50·eps(Float64) for the circle method */
 } fmmb_method_desc;
 
 /* Tree options: FMM(m, sources; ppl, bbox, max_levels) (src/fmm.jl:31-49). */
