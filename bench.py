@@ -58,6 +58,7 @@ def args_():
     a.add_argument("--serve-slots", type=int, default=4)
     a.add_argument("--stokes-instances", type=int, default=64, help="instances of the batched Stokes measurement (0: skip it)")
     a.add_argument("--ki-points", type=int, default=2_000_000, help="points of the cube KI measurement (0: skip it)")
+    a.add_argument("--no-circle-ki", action="store_true", help="skip the 2D circle KI measurement")
     return a.parse_args()
 
 
@@ -395,6 +396,53 @@ def cube_ki(fmmb, torch, ctx, n, steps, warmup, samples=4096):
                              "note": "source spectra per far pair + spectra and target sums per box, / the m2l stage"}}
 
 
+# ---------------------------------------------------------------- the 2D circle KI method
+def circle_ki(fmmb, n=100_000, nt=50_000, samples=2000, reps=5):
+    """The CPU-runnable configuration on the device: KernelIndependent(Laplace2D(); nequiv = 60),
+    ppl = 50, bbox ((0,0), 1), n sources uniform in the unit square with N(0,1) charges (seed 1)
+    and nt uniform targets (seed 2): evaluate_at_sources and evaluate at the targets (potentials,
+    host arrays in and out, the build of the expansions included), best of `reps`; relative L2
+    error against FP64 direct sums (numpy) at `samples` sampled sources and targets."""
+    pts = np.random.default_rng(1).random((n, 2))
+    tau = np.random.default_rng(1).standard_normal(n)
+    tg = np.random.default_rng(2).random((nt, 2))
+    m = fmmb.KernelIndependent(fmmb.Laplace2D(), nequiv=60)
+    t0 = time.perf_counter()
+    f = fmmb.FMM(m, pts, ppl=50, bbox=((0.0, 0.0), 1.0))
+    plan_s = time.perf_counter() - t0
+    st = fmmb.FMMState(f, "fp64")
+    best = None
+    for _ in range(reps + 1):
+        t0 = time.perf_counter()
+        fmmb.build_expansions_(st, f, pts, tau)
+        u = fmmb.evaluate_at_sources(f, st)
+        ut = fmmb.evaluate(f, st, tg)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    rng = np.random.default_rng(3)
+    ss = np.sort(rng.choice(n, samples, replace=False))
+    st_ = np.sort(rng.choice(nt, samples, replace=False))
+    c = -1 / (4 * np.pi)
+
+    def direct(x, excl=None):
+        out = np.zeros(len(x))
+        for a in range(0, len(x), 256):
+            r2 = ((x[a:a + 256, None, :] - pts[None, :, :]) ** 2).sum(-1)
+            if excl is not None:
+                r2[np.arange(len(r2)), excl[a:a + 256]] = 1.0
+            out[a:a + 256] = c * np.log(r2) @ tau
+        return out
+
+    du, dt_ = direct(pts[ss], ss), direct(tg[st_])
+    return {"workload": f"KernelIndependent(Laplace2D; nequiv=60), ppl=50, bbox ((0,0),1); {n:,} sources uniform in the "
+                        f"unit square, N(0,1) charges (seed 1); {nt:,} uniform targets (seed 2); potentials at the sources and "
+                        "at the targets, host arrays in and out, FP64",
+            "seconds": best, "evals_per_s": (n + nt) / best, "plan_s": plan_s, "levels": f.nlevels, "nodes": f.nnodes,
+            "far_pairs": f.npairs,
+            "error": {"samples": samples, "sources_rel_l2": float(np.linalg.norm(u[ss] - du) / np.linalg.norm(du)),
+                      "targets_rel_l2": float(np.linalg.norm(ut[st_] - dt_) / np.linalg.norm(dt_))}}
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(a):
     import torch
@@ -563,6 +611,7 @@ def run_ours(a):
     serve = serving(fmmb, local, a.serve_requests, a.serve_slots) if a.serve_requests > 0 else None
     stokes = stokes_batched(fmmb, local, a.stokes_instances, a.serve_slots) if a.stokes_instances > 0 else None
     ki = cube_ki(fmmb, torch, ctx, a.ki_points, 5, 3) if a.ki_points > 0 else None
+    kic = None if a.no_circle_ki else circle_ki(fmmb)
     line = {
         "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -574,6 +623,7 @@ def run_ours(a):
         "serving": serve,
         "stokes_batched": stokes,
         "cube_ki": ki,
+        "circle_ki": kic,
         "latency_ms": {"p50": pct(0.5), "p99": pct(0.99)},
         "fp64": {"value": replica_throughput(a.n, ms_fp64, world), "ms_per_step": ms_fp64},
         "mixed_vs_fp64": ms_fp64 / ms_mixed,

@@ -13,8 +13,8 @@
 # interleaved array the ABI takes); outputs come back in the original order.
 module FlexibleFMMB200
 
-using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, CubeKernelIndependent, Laplace3D, Yukawa3D,
-    Stokeslet3D, Potential, Gradient
+using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, CubeKernelIndependent, KernelIndependent,
+    Laplace3D, Laplace2D, Yukawa3D, Stokeslet3D, Potential, Gradient
 using StaticArrays: SVector
 
 const libfmmb = get(ENV, "FMMB_LIB", joinpath(@__DIR__, "..", "libfmmb.so"))
@@ -69,7 +69,7 @@ default_context() = something(DEFAULT_CONTEXT[], (DEFAULT_CONTEXT[] = Context(0)
 """
     OperatorCache(method)  (src/operators/cache.jl:19-22)
 """
-const DeviceMethod = Union{SphericalHarmonics,StokesHarmonics,CubeKernelIndependent{3}}
+const DeviceMethod = Union{SphericalHarmonics,StokesHarmonics,CubeKernelIndependent{3},KernelIndependent}
 _kernel_id(m::SphericalHarmonics) = m.kernel isa Laplace3D ? Int32(1) : m.kernel isa Yukawa3D ? Int32(2) :
     throw(ArgumentError("the device method is written for Laplace3D and Yukawa3D"))
 _kappa(m::SphericalHarmonics) = m.kernel isa Yukawa3D ? Float64(m.kernel.k) : 0.0
@@ -83,6 +83,13 @@ _method_desc(m::Union{SphericalHarmonics,StokesHarmonics}) =
 _method_desc(m::CubeKernelIndependent{3}) = m.kernel isa Laplace3D ?
     MethodDesc(2, 1, Int32(m.p), 0, 0.0, 0.0, Int32(m.pc), 0, Float64(m.d), Float64(m.pinv_rtol)) :
     throw(ArgumentError("the device cube KI method is written for Laplace3D"))
+
+# KernelIndependent(Laplace2D(); nequiv, pinv_rtol): the 2D circle method; the ABI takes its points as
+# 3 × N with z = 0 (`embed2`) and a bbox whose z origin is −width/2
+_method_desc(m::KernelIndependent) = m.kernel isa Laplace2D ?
+    MethodDesc(3, 4, Int32(m.nequiv), 0, 0.0, 0.0, 0, 0, 0.0, Float64(m.pinv_rtol)) :
+    throw(ArgumentError("the device circle KI method is written for Laplace2D"))
+embed2(pts::AbstractVector{SVector{2,Float64}}) = [SVector(p[1], p[2], 0.0) for p in pts]
 
 mutable struct OperatorCache
     method::DeviceMethod
@@ -117,6 +124,15 @@ function FMM(m::DeviceMethod, sources::AbstractVector{SVector{3,Float64}}; ppl::
                 cache.h, pts, length(pts), Ref(o), r))
     f = FMM(m, cache, r[], length(pts))
     finalizer(x -> ccall((:fmmb_plan_destroy, libfmmb), Cint, (Ptr{Cvoid},), x.h), f)
+end
+# the circle method's 2D points and square: the plane z = 0 of the cube (the gradients it returns
+# are 3-vectors with a zero z component)
+function FMM(m::KernelIndependent, sources::AbstractVector{SVector{2,Float64}}; ppl::Integer=50, bbox=nothing,
+             cache::OperatorCache=OperatorCache(m), max_levels::Integer=30)
+    pts = collect(sources)
+    bbox === nothing && (bbox = FlexibleFMM.square_bbox(pts))
+    b3 = ((Float64(bbox[1][1]), Float64(bbox[1][2]), -Float64(bbox[2]) / 2), Float64(bbox[2]))
+    return FMM(m, embed2(pts); ppl, bbox=b3, cache, max_levels)
 end
 
 """
