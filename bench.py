@@ -57,6 +57,7 @@ def args_():
     a.add_argument("--serve-requests", type=int, default=384, help="requests of the serving measurement (0: skip it)")
     a.add_argument("--serve-slots", type=int, default=4)
     a.add_argument("--stokes-instances", type=int, default=64, help="instances of the batched Stokes measurement (0: skip it)")
+    a.add_argument("--stokes-slots", type=int, default=4, help="server slots of the batched Stokes measurement")
     a.add_argument("--ki-points", type=int, default=2_000_000, help="points of the cube KI measurement (0: skip it)")
     a.add_argument("--no-circle-ki", action="store_true", help="skip the 2D circle KI measurement")
     return a.parse_args()
@@ -281,8 +282,9 @@ def stokes_batched(fmmb, device, count, slots, p=16, ppl=200, samples=32):
     reqs = stokes_workload(count)
     total = sum(len(x) for x, _ in reqs)
     srv = fmmb.Server(device, slots=slots)
-    for x, f in reqs[:2]:                                              # warm-up: operators resident
-        srv.wait(srv.submit_stokes(x, f, p=p, ppl=ppl))
+    for _ in range(2):                                                 # warm-up: every slot's operators resident
+        for k in [srv.submit_stokes(x, f, p=p, ppl=ppl) for x, f in reqs[:slots]]:
+            srv.wait(k)
     t0 = time.perf_counter()
     tk = [srv.submit_stokes(x, f, p=p, ppl=ppl) for x, f in reqs]
     res = [srv.wait(k) for k in tk]
@@ -609,7 +611,7 @@ def run_ours(a):
                "sample": f"full {a.n:,}-point matvec (the same points and charges), best of 2 after 1 warm-up, "
                          f"tree + operators {r['tree_s']:.2f} s untimed"}
     serve = serving(fmmb, local, a.serve_requests, a.serve_slots) if a.serve_requests > 0 else None
-    stokes = stokes_batched(fmmb, local, a.stokes_instances, a.serve_slots) if a.stokes_instances > 0 else None
+    stokes = stokes_batched(fmmb, local, a.stokes_instances, a.stokes_slots) if a.stokes_instances > 0 else None
     ki = cube_ki(fmmb, torch, ctx, a.ki_points, 5, 3) if a.ki_points > 0 else None
     kic = None if a.no_circle_ki else circle_ki(fmmb)
     line = {
