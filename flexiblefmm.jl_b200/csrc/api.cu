@@ -562,6 +562,44 @@ int fmmb_build_expansions(fmmb_state* state, const double* xyz, const double* ta
   });
 }
 
+int fmmb_build_expansions_dipoles_dev(fmmb_state* state, const double* xyz, const double* tau, const double* dipoles,
+                                      int64_t n) {
+  return guard([&] {
+    require(state && xyz && (tau || dipoles), FMMB_ERR_ARGUMENT, "null argument");
+    State& S = state->s;
+    require(n == S.plan->N, FMMB_ERR_DIMENSION, "expected " + std::to_string(S.plan->N) + " sources and densities");
+    set_device(*S.plan->ctx);
+    require_device_ptr(*S.plan->ctx, xyz, "points");
+    if (tau) require_device_ptr(*S.plan->ctx, tau, "charges");
+    if (dipoles) require_device_ptr(*S.plan->ctx, dipoles, "dipoles");
+    gather_inputs_dipoles(S, xyz, tau, dipoles);
+    upward_pass(S);
+    downward_pass(S);
+    S.built = true;
+  });
+}
+
+int fmmb_build_expansions_dipoles(fmmb_state* state, const double* xyz, const double* tau, const double* dipoles, int64_t n) {
+  return guard([&] {
+    require(state && xyz && (tau || dipoles), FMMB_ERR_ARGUMENT, "null argument");
+    State& S = state->s;
+    Plan& P = *S.plan;
+    require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and densities");
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    DBuf<double> d_xyz(3 * n), d_tau(tau ? n : 0), d_dip(dipoles ? 3 * n : 0);
+    FMMB_CUDA(cudaMemcpyAsync(d_xyz.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    if (tau) FMMB_CUDA(cudaMemcpyAsync(d_tau.p, tau, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    if (dipoles) FMMB_CUDA(cudaMemcpyAsync(d_dip.p, dipoles, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    gather_inputs_dipoles(S, d_xyz.p, tau ? d_tau.p : nullptr, dipoles ? d_dip.p : nullptr);
+    upward_pass(S);
+    downward_pass(S);
+    S.built = true;
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    check_state_errors(S);
+  });
+}
+
 int fmmb_evaluate_at_sources_dev(fmmb_state* state, int outputs, double* pot, double* grad) {
   return guard([&] {
     require(state != nullptr, FMMB_ERR_ARGUMENT, "null argument");

@@ -448,6 +448,111 @@ __global__ void __launch_bounds__(128) k_kic_l2t(const int* __restrict__ gnode, 
   }
 }
 
+// The near field of charges and dipoles (source_field / target_field of src/sources.jl:137-155 with
+// Laplace3D): per source q/r + (d·v)/r³ and the gradient −q v/r³ + d/r³ − 3 v (d·v)/r⁵, v = t − s,
+// as KC times the sums below (pot += KC·Σ, grad −= KC·Σ). Same flattening of the colleagues'
+// ranges as k_near, one batch of 32 staged sources (positions and moments) at a time; R as there
+// (FP32 relative to the leaf's centre with FP64 batch sums, or FP64).
+template <typename R, bool SELF>
+__global__ void __launch_bounds__(NEAR_WARPS * 32) k_near_dip(const int* __restrict__ gnode, const int* __restrict__ gstart,
+                                                             const int* __restrict__ gcount, int ngroups,
+                                                             const double* __restrict__ tx, const double* __restrict__ ty,
+                                                             const double* __restrict__ tz, const int* __restrict__ tout,
+                                                             const double* __restrict__ xs, const double* __restrict__ ys,
+                                                             const double* __restrict__ zs, const double* __restrict__ q,
+                                                             const double* __restrict__ d3, int64_t npts,
+                                                             const int4* __restrict__ cell, const int* __restrict__ plo,
+                                                             const int* __restrict__ phi, const int* __restrict__ col,
+                                                             Geometry geo, int outputs, double* __restrict__ pot,
+                                                             double* __restrict__ grad) {
+  constexpr bool REL = sizeof(R) == 4;
+  __shared__ R4<R> sp[NEAR_WARPS][32], sd[NEAR_WARPS][32];
+  __shared__ int slo[NEAR_WARPS][32], spre[NEAR_WARPS][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x * NEAR_WARPS + warp;
+  if (grp >= ngroups) return;
+  const int leaf = gnode[grp];
+  double cx = 0, cy = 0, cz = 0;
+  if (REL) {
+    const int4 c = cell[leaf];
+    const double w = ldexp(geo.W0, -c.w);
+    cx = geo.center(0, c.x, w);
+    cy = geo.center(1, c.y, w);
+    cz = geo.center(2, c.z, w);
+  }
+  const int cn = lane < NCOL ? col[(int64_t)leaf * NCOL + lane] : -1;
+  int lo = 0, len = 0;
+  if (cn >= 0) {
+    lo = plo[cn];
+    len = max(0, phi[cn] - lo + 1);
+  }
+  int incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int S = __shfl_sync(0xffffffffu, incl, 31);
+  slo[warp][lane] = lo;
+  spre[warp][lane] = incl - len;
+  __syncwarp();
+  const int t0 = gstart[grp], nt = gcount[grp];
+  for (int base = 0; base < nt; base += 32) {
+    const int k = t0 + base + lane;
+    const bool act = base + lane < nt;
+    const double x = act ? tx[k] : cx, y = act ? ty[k] : cy, z = act ? tz[k] : cz;
+    const R fx = (R)(x - cx), fy = (R)(y - cy), fz = (R)(z - cz);
+    double np = 0, nx = 0, ny = 0, nz = 0;
+    for (int b = 0; 32 * b < S; ++b) {
+      const int f = 32 * b + lane;
+      int src = -1;
+      if (f < S) {
+        int idx = 0;
+#pragma unroll
+        for (int step = 16; step; step >>= 1)
+          if (spre[warp][idx + step] <= f) idx += step;
+        src = slo[warp][idx] + (f - spre[warp][idx]);
+      }
+      __syncwarp();
+      if (src >= 0) {
+        sp[warp][lane] = R4<R>{(R)(xs[src] - cx), (R)(ys[src] - cy), (R)(zs[src] - cz), (R)q[src]};
+        sd[warp][lane] = R4<R>{(R)d3[src], (R)d3[npts + src], (R)d3[2 * npts + src], (R)0};
+      }
+      // the source index of each staged slot, for the self check
+      const int sidx = src;
+      __syncwarp();
+      const int m = min(32, S - 32 * b);
+      R bp = 0, bx = 0, by = 0, bz = 0;
+      for (int i = 0; i < m; ++i) {
+        const R4<R> sv = sp[warp][i], dv = sd[warp][i];
+        const int si = __shfl_sync(0xffffffffu, sidx, i);
+        const R vx = fx - sv.x, vy = fy - sv.y, vz = fz - sv.z;
+        const R r2 = vx * vx + vy * vy + vz * vz;
+        R ir = r2 > R(0) ? R(1) / sqrt(r2) : R(0);
+        if (SELF && act && si == k) ir = R(0);     // the target's own source: k is its tree index
+        const R ir2 = ir * ir, ir3 = ir2 * ir;
+        const R dd = dv.x * vx + dv.y * vy + dv.z * vz;
+        bp += sv.w * ir + dd * ir3;
+        const R cv = sv.w * ir3 + 3 * dd * ir3 * ir2;
+        bx += cv * vx - dv.x * ir3;
+        by += cv * vy - dv.y * ir3;
+        bz += cv * vz - dv.z * ir3;
+      }
+      np += bp; nx += bx; ny += by; nz += bz;
+    }
+    if (act) {
+      const int o = tout[k];
+      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = pot[o] + KC * np;
+      if (outputs & FMMB_OUTPUT_GRADIENT) {
+        grad[3 * (int64_t)o] = grad[3 * (int64_t)o] - KC * nx;
+        grad[3 * (int64_t)o + 1] = grad[3 * (int64_t)o + 1] - KC * ny;
+        grad[3 * (int64_t)o + 2] = grad[3 * (int64_t)o + 2] - KC * nz;
+      }
+    }
+    __syncwarp();
+  }
+}
+
 template <int P>
 void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
                 const double* tz, const int* tout, int outputs, double* pot, double* grad) {
@@ -513,6 +618,22 @@ void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* g
     default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
   }
   const bool mixed = S.precision == FMMB_PRECISION_MIXED;
+  if (S.has_dip) {
+    Plan& P_ = *S.plan;
+    const unsigned nb = (ng + NEAR_WARPS - 1) / NEAR_WARPS;
+#define FMMB_NEAR_DIP(R, SELF)                                                                                  \
+  k_near_dip<R, SELF><<<nb, 32 * NEAR_WARPS, 0, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, \
+                                                                  S.ys.p, S.zs.p, S.q.p, S.dip.p, P_.N, P_.cell.p,     \
+                                                                  P_.plo.p, P_.phi.p, P_.col.p, geometry(P_), outputs, \
+                                                                  pot, grad)
+    if (mixed && self) FMMB_NEAR_DIP(float, true);
+    else if (mixed) FMMB_NEAR_DIP(float, false);
+    else if (self) FMMB_NEAR_DIP(double, true);
+    else FMMB_NEAR_DIP(double, false);
+#undef FMMB_NEAR_DIP
+    FMMB_LAUNCH_CHECK();
+    return;
+  }
   if (S.plan->cache->kernel == FMMB_KERNEL_YUKAWA3D) {
     require(!mixed, FMMB_ERR_UNSUPPORTED, "Yukawa3D runs on the FP64 path");
     if (self) launch_near<double, true, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);

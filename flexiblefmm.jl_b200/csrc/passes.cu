@@ -64,6 +64,116 @@ __global__ void k_gather_inputs(const double* __restrict__ xyz, const double* __
   q[k] = tau[j];
 }
 
+// charges (or zeros) and dipole moments into tree order
+__global__ void k_gather_dipoles(const double* __restrict__ xyz, const double* __restrict__ tau,
+                                 const double* __restrict__ dip, const int* __restrict__ perm, int64_t n,
+                                 double* __restrict__ xs, double* __restrict__ ys, double* __restrict__ zs,
+                                 double* __restrict__ q, double* __restrict__ d3) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t j = perm[k];
+  xs[k] = xyz[3 * j];
+  ys[k] = xyz[3 * j + 1];
+  zs[k] = xyz[3 * j + 2];
+  q[k] = tau ? tau[j] : 0.0;
+  d3[k] = dip ? dip[3 * j] : 0.0;
+  d3[n + k] = dip ? dip[3 * j + 1] : 0.0;
+  d3[2 * n + k] = dip ? dip[3 * j + 2] : 0.0;
+}
+
+// P2M of charges and dipoles d (src/operators/harmonics.jl:708-738): one thread per (node, order
+// m); per source the charge's chain of order m, and the dipole's three terms from the chains of
+// orders m − 1, m, m + 1 of degree n′ = n − 1 (the derivative identities, with the moment in box
+// units d·s, harmonics.jl:436):
+//   chain m − 1: (n, m) += ½ cm(n, m) · (−(dx ur − dy ui), dx ui + dy ur)
+//   chain m:     (n, m) += cz(n, m) dz · (ur, −ui)
+//   chain m + 1: (n, m) += ½ cp(n, m) · (dx ur + dy ui, dy ur − dx ui)   (m = 0: cp(n, 0) (dx ur + dy ui), 0)
+template <int P>
+__global__ void k_p2m_dip(const int* __restrict__ nodes, int nn, const int4* __restrict__ cell, const int* __restrict__ plo,
+                          const int* __restrict__ phi, const double* __restrict__ xs, const double* __restrict__ ys,
+                          const double* __restrict__ zs, const double* __restrict__ q, const double* __restrict__ d3,
+                          int64_t npts, Geometry geo, const double* __restrict__ scale, int64_t pitch,
+                          double* __restrict__ M) {
+  __shared__ double s_t[5 * TRI_MAX];   // a, b, cz, cm, cp
+  __shared__ double s_e[PMAX];
+  for (int i = threadIdx.x; i < 5 * TRI_MAX; i += blockDim.x) s_t[i] = c_tab[i];
+  for (int i = threadIdx.x; i < PMAX; i += blockDim.x) s_e[i] = c_e[i];
+  __syncthreads();
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = g / nn, qn = g % nn;
+  if (m > P) return;
+  const int node = nodes[qn];
+  const int4 c = cell[node];
+  const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
+  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  double ar[P + 1], ai[P + 1];
+#pragma unroll
+  for (int n = 0; n <= P; ++n) { ar[n] = 0; ai[n] = 0; }
+  for (int j = plo[node]; j <= phi[node]; ++j) {
+    const double x = (xs[j] - cx) * s, y = (ys[j] - cy) * s, z = (zs[j] - cz) * s;
+    const double r2 = x * x + y * y + z * z;
+    const double tau = q[j], dx = d3[j] * s, dy = d3[npts + j] * s, dz = d3[2 * npts + j] * s;
+    // sectoral values of orders m − 1, m, m + 1
+    double sr = 1.0, si = 0.0, lr = 0, li = 0, mr = 1.0, mi = 0.0, hr = 0, hi = 0;
+    for (int k = 1; k <= m + 1; ++k) {
+      const double e = s_e[k - 1];
+      const double nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
+      if (k == m) { lr = sr; li = si; }
+      sr = nr; si = ni;
+      if (k == m) { mr = sr; mi = si; }
+      if (k == m + 1) { hr = sr; hi = si; }
+    }
+    if (m == 0) { mr = 1.0; mi = 0.0; }
+    // the chain of order k from its sectoral value (vr, vi), calling f(n′, ur, ui) for n′ = k..nmax
+    auto chain = [&](int k, double vr, double vi, int nmax, auto&& f) {
+      double pr = 0, pi = 0, cr = vr, ci = vi;
+#pragma unroll
+      for (int n = 0; n <= P; ++n) {
+        if (n < k || n > nmax) continue;
+        if (n > k) {
+          const int t = tri(n, k);
+          const double az = s_t[t] * z, br = s_t[TRI_MAX + t] * r2;
+          const double nr = az * cr - br * pr, ni = az * ci - br * pi;
+          pr = cr; pi = ci; cr = nr; ci = ni;
+        }
+        f(n, cr, ci);
+      }
+    };
+    chain(m, mr, mi, P, [&](int n, double ur, double ui) {
+      ar[n] += tau * ur;
+      ai[n] -= tau * ui;
+      if (n < P) {
+        const double cc = s_t[2 * TRI_MAX + tri(n + 1, m)] * dz;
+        ar[n + 1] += cc * ur;
+        ai[n + 1] -= cc * ui;
+      }
+    });
+    if (m >= 1)
+      chain(m - 1, lr, li, P - 1, [&](int n, double ur, double ui) {
+        const double cc = 0.5 * s_t[3 * TRI_MAX + tri(n + 1, m)];
+        ar[n + 1] += -cc * (dx * ur - dy * ui);
+        ai[n + 1] += cc * (dx * ui + dy * ur);
+      });
+    if (m + 1 <= P - 1)
+      chain(m + 1, hr, hi, P - 1, [&](int n, double ur, double ui) {
+        if (m >= 1) {
+          const double cc = 0.5 * s_t[4 * TRI_MAX + tri(n + 1, m)];
+          ar[n + 1] += cc * (dx * ur + dy * ui);
+          ai[n + 1] += cc * (dy * ur - dx * ui);
+        } else {
+          ar[n + 1] += s_t[4 * TRI_MAX + tri(n + 1, 0)] * (dx * ur + dy * ui);
+        }
+      });
+  }
+  double* col = M + (int64_t)node * pitch;
+#pragma unroll
+  for (int n = 0; n <= P; ++n) {
+    if (n < m) continue;
+    if (m == 0) col[n * n] = ar[n];
+    else { col[n * n + 2 * m - 1] = ar[n]; col[n * n + 2 * m] = ai[n]; }
+  }
+}
+
 // ---------------------------------------------------------------- P2M
 // one thread per (node, order m): M_n^m += τ conj Υ̃_n^m((y − c)/w) over the node's sources,
 // n = m..P, the chain of order m started from its own sectoral value (harmonics.jl:682-743)
@@ -360,6 +470,13 @@ void launch_p2m(State& S, const double* q, double* M, int64_t pitch) {
   Plan& P_ = *S.plan;
   int nth = P_.n_s2m * (P + 1);
   if (nth == 0) return;
+  if (S.has_dip) {
+    k_p2m_dip<P><<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p,
+                                                           S.ys.p, S.zs.p, q, S.dip.p, P_.N, geometry(P_), P_.d_scale.p,
+                                                           pitch, M);
+    FMMB_LAUNCH_CHECK();
+    return;
+  }
   auto kern = P_.cache->kernel == FMMB_KERNEL_YUKAWA3D ? k_p2m<P, true> : k_p2m<P, false>;
   kern<<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p, S.ys.p,
                                                  S.zs.p, q, geometry(P_), P_.d_scale.p, pitch, M, P_.d_kh2.p);
@@ -399,6 +516,18 @@ void gather_inputs(State& S, const double* xyz_dev, const double* tau_dev) {
   require(P.cache->kernel != FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
   k_gather_inputs<<<nblk(P.N), 256, 0, P.ctx->stream>>>(xyz_dev, tau_dev, P.perm.p, P.N, S.xs.p, S.ys.p, S.zs.p, S.q.p);
   FMMB_LAUNCH_CHECK();
+  S.has_dip = false;
+}
+
+void gather_inputs_dipoles(State& S, const double* xyz_dev, const double* tau_dev, const double* dip_dev) {
+  Plan& P = *S.plan;
+  require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D && P.cache->method == FMMB_METHOD_SPHERICAL_HARMONICS,
+          FMMB_ERR_UNSUPPORTED, "dipole densities are provided for SphericalHarmonics(Laplace3D)");
+  if (S.dip.n < (size_t)(3 * P.N)) S.dip.alloc(3 * P.N);
+  k_gather_dipoles<<<nblk(P.N), 256, 0, P.ctx->stream>>>(xyz_dev, tau_dev, dip_dev, P.perm.p, P.N, S.xs.p, S.ys.p, S.zs.p,
+                                                         S.q.p, S.dip.p);
+  FMMB_LAUNCH_CHECK();
+  S.has_dip = dip_dev != nullptr;
 }
 
 

@@ -133,6 +133,8 @@ struct State {
   int precision = FMMB_PRECISION_FP64;
   DBuf<double> xs, ys, zs, q;             // sources and charges in tree order
   DBuf<double> f3;                        // Stokeslet states: the forces in tree order (fx, fy, fz)
+  DBuf<double> dip;                       // dipole densities in tree order (dx, dy, dz: 3 × N planar)
+  bool has_dip = false;                   // the last build had dipoles (the P2M and near field take them)
   DBuf<double> M, Pl;                     // nnodes × LD: multipoles, partial locals
   DBuf<uint16_t> Mh, Ml;                  // the mixed path: the multipoles scaled by a power of two
   DBuf<float> Msc;                        //   per node, as FP16 head and tail; the inverse scales
@@ -159,6 +161,8 @@ void build_target_pairs(Plan& P);
 // passes.cu
 void upload_operators(Cache& C);
 void gather_inputs(State& S, const double* xyz_dev, const double* tau_dev);
+// charges (tau, or none) and dipole moments (3 × n interleaved, or none) in original order
+void gather_inputs_dipoles(State& S, const double* xyz_dev, const double* tau_dev, const double* dip_dev);
 void upward_pass(State& S);
 void downward_pass(State& S);
 void evaluate_sources(State& S, int outputs, double* pot_dev, double* grad_dev);

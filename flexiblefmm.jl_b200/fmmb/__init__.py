@@ -91,7 +91,7 @@ EXPORTS = (
     "fmmb_evaluate_at_sources_dev", "fmmb_matvec", "fmmb_matvec_dev", "fmmb_evaluate", "fmmb_evaluate_dev",
     "fmmb_state_expansions", "fmmb_direct_dev", "fmmb_profile_matvec", "fmmb_direct_noalloc_dev",
     "fmmb_server_create", "fmmb_server_submit", "fmmb_server_wait", "fmmb_server_destroy", "fmmb_stokes_eval",
-    "fmmb_stokes_eval_dev",
+    "fmmb_stokes_eval_dev", "fmmb_build_expansions_dipoles", "fmmb_build_expansions_dipoles_dev",
 )
 
 
@@ -144,6 +144,8 @@ def lib():
         "fmmb_server_wait": [vp, i64, C.c_double, C.POINTER(_RequestInfo)],
         "fmmb_server_destroy": [vp],
         "fmmb_stokes_eval": [vp, dp, dp, i64, dp],
+        "fmmb_build_expansions_dipoles": [vp, dp, dp, dp, i64],
+        "fmmb_build_expansions_dipoles_dev": [vp, dp, dp, dp, i64],
         "fmmb_stokes_eval_dev": [vp, dp, dp, i64, dp],
     }
     for name, args in sig.items():
@@ -485,13 +487,35 @@ def _densities(tau, n):
     return t
 
 
+class Dipoles:
+    """Dipole densities Dipole(d) per source (src/sources.jl:16-31): moments d (N, 3), field
+    d·∇ₛG. As build_expansions' τ alone, or with charges as the tuple (charges, Dipoles(d))."""
+
+    def __init__(self, d):
+        self.d = np.ascontiguousarray(d, dtype=np.float64)
+
+
 def build_expansions_(state, fmm, sources, tau):
-    """build_expansions!(state, fmm, sources, τ) (src/fmm.jl:270-298)."""
+    """build_expansions!(state, fmm, sources, τ) (src/fmm.jl:270-298); τ: charges (N,),
+    Dipoles(d), or the tuple (charges, Dipoles(d))."""
     x = _pts(fmm, sources)
     if x.shape[0] != fmm.N:
         raise DimensionMismatch(2, f"expected {fmm.N} sources in group 1")
-    t = _densities(tau, fmm.N)
-    _check(lib().fmmb_build_expansions(state._h, _ptr(x), _ptr(t), fmm.N))
+    charges, dip = tau, None
+    if isinstance(tau, Dipoles):
+        charges, dip = None, tau
+    elif isinstance(tau, tuple):
+        if len(tau) != 2 or not isinstance(tau[1], Dipoles):
+            raise ArgumentError(1, "densities as a tuple: (charges, Dipoles(d))")
+        charges, dip = tau
+    if dip is None:
+        t = _densities(charges, fmm.N)
+        _check(lib().fmmb_build_expansions(state._h, _ptr(x), _ptr(t), fmm.N))
+        return state
+    if dip.d.shape != (fmm.N, 3):
+        raise DimensionMismatch(2, f"expected {fmm.N} dipole moments (N, 3), got {dip.d.shape}")
+    t = None if charges is None else _densities(charges, fmm.N)
+    _check(lib().fmmb_build_expansions_dipoles(state._h, _ptr(x), _ptr(t), _ptr(dip.d), fmm.N))
     return state
 
 

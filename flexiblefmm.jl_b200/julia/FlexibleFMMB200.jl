@@ -14,7 +14,7 @@
 module FlexibleFMMB200
 
 using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, CubeKernelIndependent, KernelIndependent,
-    Laplace3D, Laplace2D, Yukawa3D, Stokeslet3D, Potential, Gradient
+    Laplace3D, Laplace2D, Yukawa3D, Stokeslet3D, Potential, Gradient, Dipole
 using StaticArrays: SVector
 
 const libfmmb = get(ENV, "FMMB_LIB", joinpath(@__DIR__, "..", "libfmmb.so"))
@@ -157,6 +157,19 @@ function build_expansions!(st::FMMState, f::FMM, sources::AbstractVector{SVector
     tau = Vector{Float64}(τ)
     check(ccall((:fmmb_build_expansions, libfmmb), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64),
                 st.h, pts, tau, f.n))
+    return st
+end
+# Dipole densities, alone or as (charge, Dipole) tuples per source (src/sources.jl:16-31)
+function build_expansions!(st::FMMState, f::FMM, sources::AbstractVector{SVector{3,Float64}},
+                           τ::AbstractVector{<:Union{Dipole{3,Float64},Tuple{Float64,Dipole{3,Float64}}}})
+    length(sources) == f.n || throw(DimensionMismatch("expected $(f.n) sources in group 1"))
+    length(τ) == f.n || throw(DimensionMismatch("expected $(f.n) densities in group 1"))
+    pts = collect(sources)
+    dip = [t isa Dipole ? t.d : t[2].d for t in τ]
+    q = eltype(τ) <: Dipole ? nothing : Float64[t[1] for t in τ]
+    check(ccall((:fmmb_build_expansions_dipoles, libfmmb), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{SVector{3,Float64}}, Int64),
+                st.h, pts, q === nothing ? C_NULL : pointer(q), dip, f.n))
     return st
 end
 build_expansions!(st::FMMState, f::FMM, sources, τ) =

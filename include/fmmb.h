@@ -125,6 +125,13 @@ int fmmb_state_destroy(fmmb_state* state);
 /* build_expansions!(state, fmm, sources, τ) (src/fmm.jl:270-298) with charges τ. */
 int fmmb_build_expansions(fmmb_state* state, const double* xyz, const double* tau, int64_t n);
 int fmmb_build_expansions_dev(fmmb_state* state, const double* xyz_dev, const double* tau_dev, int64_t n);
+/* build_expansions! with Dipole densities, alone or with charges (τ as a tuple of a charge and a
+ * Dipole per source, src/sources.jl:16-31, src/operators/harmonics.jl:708-738): tau n charges or
+ * NULL, dipoles 3×n moments d (field d·∇ₛG) or NULL; SphericalHarmonics(Laplace3D) on either
+ * precision path. The evaluation of a state built this way takes the dipoles' near field. */
+int fmmb_build_expansions_dipoles(fmmb_state* state, const double* xyz, const double* tau, const double* dipoles, int64_t n);
+int fmmb_build_expansions_dipoles_dev(fmmb_state* state, const double* xyz_dev, const double* tau_dev,
+                                      const double* dipoles_dev, int64_t n);
 /* evaluate_at_sources!(out, fmm, state; output) (src/evaluate.jl:111-127): pot (n) and/or
  * grad (3×n) in the original order, self excluded. */
 int fmmb_evaluate_at_sources(fmmb_state* state, int outputs, double* pot, double* grad);
