@@ -37,8 +37,12 @@ __device__ __forceinline__ void dmma(double* d, double a, double b) {
                : "d"(a), "d"(b));
 }
 
+// two CTAs per SM where their shared memory fits (the registers are then capped at 128)
 template <int LD, int NB>
-__global__ void __launch_bounds__(256) k_m2l_f64(const int4* __restrict__ blocks, const int* __restrict__ cls_off,
+constexpr int m2l_f64_ctas() { return (16 + NB) * (LD + 4) * 8 + 12 * NB <= 113 * 1024 ? 2 : 1; }
+
+template <int LD, int NB>
+__global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const int4* __restrict__ blocks, const int* __restrict__ cls_off,
                                                  const int2* __restrict__ pairs, const uint64_t* __restrict__ reps_lv,
                                                  const double* __restrict__ m2l_scale, int NP, const double* __restrict__ M,
                                                  double* __restrict__ Pl, int64_t pitch, int stokes) {
@@ -218,8 +222,8 @@ void m2l_f64(State& S) {
   switch (S.plan->cache->ld) {
     case 64: launch<64, 64>(S); break;
     case 128: launch<128, 64>(S); break;
-    case 192: launch<192, 64>(S); break;
-    case 256: launch<256, 64>(S); break;
+    case 192: launch<192, 32>(S); break;
+    case 256: launch<256, 32>(S); break;
     case 320: launch<320, 48>(S); break;
     case 384: launch<384, 40>(S); break;
     case 448: launch<448, 32>(S); break;
