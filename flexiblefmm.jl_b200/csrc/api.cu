@@ -799,8 +799,10 @@ int fmmb_stokes_eval_dev(fmmb_state* state, const double* xyz, const double* sto
     require_device_ptr(*P.ctx, xyz, "sources");
     require_device_ptr(*P.ctx, stokeslets, "stokeslets");
     require_device_ptr(*P.ctx, velocity, "velocities");
-    stokes_build(S, xyz, stokeslets);
-    stokes_evaluate_sources(S, velocity);
+    StokesDensities d;
+    d.stokeslets = stokeslets;
+    stokes_build(S, xyz, d);
+    stokes_evaluate_sources(S, FMMB_STOKES_VELOCITY, velocity);
   });
 }
 
@@ -816,9 +818,87 @@ int fmmb_stokes_eval(fmmb_state* state, const double* xyz, const double* stokesl
     DBuf<double> x(3 * n), f(3 * n), v(3 * n);
     FMMB_CUDA(cudaMemcpyAsync(x.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
     FMMB_CUDA(cudaMemcpyAsync(f.p, stokeslets, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-    stokes_build(S, x.p, f.p);
-    stokes_evaluate_sources(S, v.p);
+    StokesDensities d;
+    d.stokeslets = f.p;
+    stokes_build(S, x.p, d);
+    stokes_evaluate_sources(S, FMMB_STOKES_VELOCITY, v.p);
     FMMB_CUDA(cudaMemcpyAsync(velocity, v.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+namespace {
+
+// the checks of stokes_densities (src/stokes_api.jl:72-83) and of the state
+void check_stokes_call(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n, int output,
+                       double* out) {
+  require(state && xyz && dens && out, FMMB_ERR_ARGUMENT, "null argument");
+  require((dens->stresslets == nullptr) == (dens->stressvecs == nullptr), FMMB_ERR_ARGUMENT,
+          "stresslets and stressvecs must be given together");
+  require(dens->stokeslets || dens->stresslets || dens->doublets, FMMB_ERR_ARGUMENT,
+          "provide at least one of stokeslets, stresslets, doublets");
+  require(output == FMMB_STOKES_VELOCITY || output == FMMB_STOKES_PRESSURE, FMMB_ERR_UNSUPPORTED,
+          "Stokes outputs are the velocity and the pressure");
+  Plan& P = *state->s.plan;
+  require(P.cache->kernel == FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED, "the state is not a Stokeslet state");
+  require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and densities");
+}
+
+}  // namespace
+
+int fmmb_stokes_eval_densities_dev(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
+                                   int output, double* out) {
+  return guard([&] {
+    check_stokes_call(state, xyz, dens, n, output, out);
+    State& S = state->s;
+    Plan& P = *S.plan;
+    set_device(*P.ctx);
+    require_device_ptr(*P.ctx, xyz, "sources");
+    const double* arrays[5] = {dens->stokeslets, dens->stresslets, dens->stressvecs, dens->doublets, dens->weights};
+    for (const double* a : arrays)
+      if (a) require_device_ptr(*P.ctx, a, "densities");
+    require_device_ptr(*P.ctx, out, "outputs");
+    StokesDensities d;
+    d.stokeslets = dens->stokeslets;
+    d.stresslets = dens->stresslets;
+    d.stressvecs = dens->stressvecs;
+    d.doublets = dens->doublets;
+    d.weights = dens->weights;
+    stokes_build(S, xyz, d);
+    stokes_evaluate_sources(S, output, out);
+  });
+}
+
+int fmmb_stokes_eval_densities(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
+                               int output, double* out) {
+  return guard([&] {
+    check_stokes_call(state, xyz, dens, n, output, out);
+    State& S = state->s;
+    Plan& P = *S.plan;
+    set_device(*P.ctx);
+    cudaStream_t s = P.ctx->stream;
+    const int64_t no = output == FMMB_STOKES_PRESSURE ? n : 3 * n;
+    DBuf<double> x(3 * n), o(no);
+    DBuf<double> a[5];
+    const double* src[5] = {dens->stokeslets, dens->stresslets, dens->stressvecs, dens->doublets, dens->weights};
+    const double* dev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    FMMB_CUDA(cudaMemcpyAsync(x.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    for (int k = 0; k < 5; ++k) {
+      if (!src[k]) continue;
+      const int64_t len = k == 4 ? n : 3 * n;
+      a[k].alloc(len);
+      FMMB_CUDA(cudaMemcpyAsync(a[k].p, src[k], sizeof(double) * len, cudaMemcpyHostToDevice, s));
+      dev[k] = a[k].p;
+    }
+    StokesDensities d;
+    d.stokeslets = dev[0];
+    d.stresslets = dev[1];
+    d.stressvecs = dev[2];
+    d.doublets = dev[3];
+    d.weights = dev[4];
+    stokes_build(S, x.p, d);
+    stokes_evaluate_sources(S, output, o.p);
+    FMMB_CUDA(cudaMemcpyAsync(out, o.p, sizeof(double) * no, cudaMemcpyDeviceToHost, s));
     FMMB_CUDA(cudaStreamSynchronize(s));
   });
 }

@@ -465,14 +465,15 @@ __global__ void k_direct_reduce(const double* __restrict__ part, int64_t nt, int
   if (grad) { grad[3 * t] = -KC * gx; grad[3 * t + 1] = -KC * gy; grad[3 * t + 2] = -KC * gz; }
 }
 
+// P2M of charges q (and, when d3 is given, dipoles d3: 3 × N planar) into M (pitch per node)
 template <int P>
-void launch_p2m(State& S, const double* q, double* M, int64_t pitch) {
+void launch_p2m(State& S, const double* q, const double* d3, double* M, int64_t pitch) {
   Plan& P_ = *S.plan;
   int nth = P_.n_s2m * (P + 1);
   if (nth == 0) return;
-  if (S.has_dip) {
+  if (d3) {
     k_p2m_dip<P><<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p,
-                                                           S.ys.p, S.zs.p, q, S.dip.p, P_.N, geometry(P_), P_.d_scale.p,
+                                                           S.ys.p, S.zs.p, q, d3, P_.N, geometry(P_), P_.d_scale.p,
                                                            pitch, M);
     FMMB_LAUNCH_CHECK();
     return;
@@ -531,9 +532,9 @@ void gather_inputs_dipoles(State& S, const double* xyz_dev, const double* tau_de
 }
 
 
-void p2m_block(State& S, const double* q, double* M, int64_t pitch) {
+void p2m_block(State& S, const double* q, const double* d3, double* M, int64_t pitch) {
   switch (S.plan->cache->p) {
-#define X(pp) case pp: launch_p2m<pp>(S, q, M, pitch); break;
+#define X(pp) case pp: launch_p2m<pp>(S, q, d3, M, pitch); break;
     FMMB_P_CASES(X)
 #undef X
     default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
@@ -549,7 +550,7 @@ int p2m(State& S) {
   if (S.plan->cache->method == FMMB_METHOD_CUBE_KI) return ki_p2m(S);
   if (S.plan->cache->method == FMMB_METHOD_KI_CIRCLE) return kic_p2m(S);
   switch (S.plan->cache->p) {
-#define X(pp) case pp: launch_p2m<pp>(S, S.q.p, S.M.p, (int64_t)S.plan->cache->ld); break;
+#define X(pp) case pp: launch_p2m<pp>(S, S.q.p, S.has_dip ? S.dip.p : nullptr, S.M.p, (int64_t)S.plan->cache->ld); break;
     FMMB_P_CASES(X)
 #undef X
     default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");

@@ -199,7 +199,8 @@ struct ColMap {
 void gemm_columns(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols, int LD, int NP, int accumulate,
                   int num_sms, cudaStream_t s);
 // P2M of the childless sourced nodes with charges q (tree order) into the block at M (node pitch)
-void p2m_block(State& S, const double* q, double* M, int64_t pitch);
+// P2M of charges q and, when d3 (3 × N planar) is given, dipoles into M (pitch doubles per node)
+void p2m_block(State& S, const double* q, const double* d3, double* M, int64_t pitch);
 
 void m2l_f64(State& S);
 int p2m(State& S);          // the stages of the passes; each returns its kernel launches

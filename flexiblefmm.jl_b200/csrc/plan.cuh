@@ -133,6 +133,9 @@ struct State {
   int precision = FMMB_PRECISION_FP64;
   DBuf<double> xs, ys, zs, q;             // sources and charges in tree order
   DBuf<double> f3;                        // Stokeslet states: the forces in tree order (fx, fy, fz)
+  DBuf<double> sd;                        //   stresslet strengths, stressvecs, doublets (3 × N planar each)
+  DBuf<double> dip4;                      //   the four blocks' dipole densities (3 × N planar each)
+  bool stokes_dens = false;               //   the last build had stresslets or doublets
   DBuf<double> dip;                       // dipole densities in tree order (dx, dy, dz: 3 × N planar)
   bool has_dip = false;                   // the last build had dipoles (the P2M and near field take them)
   DBuf<double> M, Pl;                     // nnodes × LD: multipoles, partial locals
@@ -186,8 +189,15 @@ int kic_leaf_locals(State& S);
 // device by projection when a width is first used) and the per-level factors
 void yukawa_prepare(Plan& P);
 // stokes.cu: StokesHarmonics(Stokeslet3D()) on the FP64 path
-void stokes_build(State& S, const double* xyz_dev, const double* f_dev);
-void stokes_evaluate_sources(State& S, double* vel_dev);
+// the densities of stokes_fmm_eval! (device, original order; each may be null, stresslets and
+// stressvecs together): 3 × n each, weights n
+struct StokesDensities {
+  const double *stokeslets = nullptr, *stresslets = nullptr, *stressvecs = nullptr, *doublets = nullptr,
+               *weights = nullptr;
+};
+void stokes_build(State& S, const double* xyz_dev, const StokesDensities& d);
+// output FMMB_STOKES_VELOCITY (3 × n) or FMMB_STOKES_PRESSURE (n), original order, device
+void stokes_evaluate_sources(State& S, int output, double* out_dev);
 // direct_noalloc.cu: the same sums with the partials in a fixed array compiled into the library
 void direct_noalloc(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
                     int64_t nt, double* pot, double* grad);

@@ -10,6 +10,13 @@
 //   L2L  children blocks 1–3 = L2L·P_a; block 4 = 2·L2L·P₄ − 2 δ̂·(L2L·P_Φ) (:159-183)
 //   L2P  u = ½[Φ − x̂·∇̂Φ + ∇̂Ψ̂] from the values and scaled gradients of the four blocks (:283-287)
 //   near c(f/r + d(d·f)/r³), c = 1/(8π), self excluded by index (src/kernels.jl:253-272)
+// Stresslets (f, ν) and doublets g (src/sources.jl:203-281) enter as dipole densities
+// (harmonics_stokes.jl:205-216,382-393): block k takes the dipole −(f_k ν + ν_k f), block 4 the
+// dipole −((ν·ŷ) f + (f·ŷ) ν) + g/w; the translations and L2P are the same. The pressure is
+// −∇·Φ (−s·tr of the scaled gradients of blocks 1–3, :343-346) plus the near-field pressures
+// 2c(d·f)/r³ and 4c[(f·ν)/r³ − 3(d·f)(d·ν)/r⁵] (a doublet has none).
+#include <type_traits>
+
 #include "passes.cuh"
 
 namespace fmmb {
@@ -23,28 +30,41 @@ inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t
 // δ̂ of child slot j along d: (c_child − c_parent)/w_parent ∈ {±1/4} (bit d of j = coordinate d)
 __device__ __forceinline__ double dhat(int j, int d) { return (((j >> d) & 1) ? 0.25 : -0.25); }
 
-// points and forces in tree order (perm: sorted position → original index)
-__global__ void k_stokes_gather(const double* __restrict__ xyz, const double* __restrict__ f, const int* __restrict__ perm,
+// points and densities in tree order (perm: sorted position → original index), weighted: the
+// Stokeslets into f3 (zeros when absent), the stresslet strengths, stressvecs and doublets into
+// sd (3 × n planar each, zeros when absent) when sd is given
+__global__ void k_stokes_gather(const double* __restrict__ xyz, StokesDensities d, const int* __restrict__ perm,
                                 int64_t n, double* __restrict__ xs, double* __restrict__ ys, double* __restrict__ zs,
-                                double* __restrict__ f3) {
+                                double* __restrict__ f3, double* __restrict__ sd) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int64_t j = perm[i];
   xs[i] = xyz[3 * j];
   ys[i] = xyz[3 * j + 1];
   zs[i] = xyz[3 * j + 2];
-  f3[i] = f[3 * j];
-  f3[n + i] = f[3 * j + 1];
-  f3[2 * n + i] = f[3 * j + 2];
+  const double wt = d.weights ? d.weights[j] : 1.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) f3[k * n + i] = d.stokeslets ? wt * d.stokeslets[3 * j + k] : 0.0;
+  if (sd) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      sd[k * n + i] = d.stresslets ? wt * d.stresslets[3 * j + k] : 0.0;
+      sd[(3 + k) * n + i] = d.stresslets ? d.stressvecs[3 * j + k] : 0.0;
+      sd[(6 + k) * n + i] = d.doublets ? wt * d.doublets[3 * j + k] : 0.0;
+    }
+  }
 }
 
 // the fourth P2M block's charges ŷ·f, ŷ = (y − c)·s relative to the centre c of the node whose
-// multipole the point enters, s = 1/w
+// multipole the point enters, s = 1/w; with DENS also the four blocks' dipoles (3 × n planar per
+// block, in physical units: the P2M scales them by s): −(f_k ν + ν_k f) for block k and
+// −((ν·ŷ) f + (f·ŷ) ν) + g·s for block 4 (f, ν the stresslet, g the doublet)
+template <bool DENS>
 __global__ void k_stokes_q4(const int* __restrict__ nodes, int nn, const int4* __restrict__ cell,
                             const int* __restrict__ plo, const int* __restrict__ phi, Geometry geo,
                             const double* __restrict__ scale, int64_t n, const double* __restrict__ xs,
                             const double* __restrict__ ys, const double* __restrict__ zs, const double* __restrict__ f3,
-                            double* __restrict__ q4) {
+                            const double* __restrict__ sd, double* __restrict__ q4, double* __restrict__ dip4) {
   // one warp per childless node with sources (the nodes P2M runs on, ghost children of a leaf
   // included): Ψ̂ is centred on the node whose multipole it starts
   const int wid = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
@@ -54,8 +74,24 @@ __global__ void k_stokes_q4(const int* __restrict__ nodes, int nn, const int4* _
   const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
   const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
   for (int i = plo[node] + lane; i <= phi[node]; i += 32) {
-    const double x = (xs[i] - cx) * s, y = (ys[i] - cy) * s, z = (zs[i] - cz) * s;
-    q4[i] = x * f3[i] + y * f3[n + i] + z * f3[2 * n + i];
+    const double y[3] = {(xs[i] - cx) * s, (ys[i] - cy) * s, (zs[i] - cz) * s};
+    q4[i] = y[0] * f3[i] + y[1] * f3[n + i] + y[2] * f3[2 * n + i];
+    if (DENS) {
+      double f[3], nu[3], g[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        f[k] = sd[k * n + i];
+        nu[k] = sd[(3 + k) * n + i];
+        g[k] = sd[(6 + k) * n + i];
+      }
+      const double ny = nu[0] * y[0] + nu[1] * y[1] + nu[2] * y[2], fy = f[0] * y[0] + f[1] * y[1] + f[2] * y[2];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int e = 0; e < 3; ++e) dip4[(3 * k + e) * n + i] = -(f[k] * nu[e] + nu[k] * f[e]);
+        dip4[(9 + k) * n + i] = -(ny * f[k] + fy * nu[k]) + g[k] * s;
+      }
+    }
   }
 }
 
@@ -89,8 +125,9 @@ __global__ void k_stokes_l2l_out(double* __restrict__ Pl, const double* __restri
 }
 
 // the far field at the targets of one leaf: u = ½[Φ − x̂·∇̂Φ + ∇̂Ψ̂] from the leaf's four local blocks
-// (staged in shared memory per warp), lanes over the targets; writes the velocities
-template <int P>
+// (staged in shared memory per warp), lanes over the targets; writes the velocities, or with PRES
+// the pressures −s·tr(∇̂Φ) (blocks 1–3 only)
+template <int P, bool PRES>
 __global__ void __launch_bounds__(SW * 32) k_stokes_l2p(const int* __restrict__ gnode, const int* __restrict__ gstart,
                                                         const int* __restrict__ gcount, int ngroups,
                                                         const double* __restrict__ tx, const double* __restrict__ ty,
@@ -115,7 +152,7 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_l2p(const int* __restrict__ 
     const bool act = base + lane < nt;
     const double xh[3] = {act ? (tx[k] - cx) * s : 0.0, act ? (ty[k] - cy) * s : 0.0, act ? (tz[k] - cz) * s : 0.0};
     double phi[3], G[3][3], gpsi[3];   // G[i][k] = ∂̂_i Φ_k
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < (PRES ? 3 : 4); ++a) {
       double u, g[3];
       l2p<P, double>(L + (int64_t)a * LD, xh[0], xh[1], xh[2], u, g[0], g[1], g[2]);
       if (a < 3) {
@@ -127,26 +164,35 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_l2p(const int* __restrict__ 
     }
     if (act) {
       const int o = tout[k];
-      for (int i = 0; i < 3; ++i)
-        vel[3 * (int64_t)o + i] = 0.5 * (phi[i] - (xh[0] * G[i][0] + xh[1] * G[i][1] + xh[2] * G[i][2]) + gpsi[i]);
+      if (PRES)
+        vel[o] = -s * (G[0][0] + G[1][1] + G[2][2]);
+      else
+        for (int i = 0; i < 3; ++i)
+          vel[3 * (int64_t)o + i] = 0.5 * (phi[i] - (xh[0] * G[i][0] + xh[1] * G[i][1] + xh[2] * G[i][2]) + gpsi[i]);
     }
   }
 }
 
 struct alignas(16) S8 { double x, y, z, fx, fy, fz, pad0, pad1; };
+struct alignas(16) S16 { double x, y, z, fx, fy, fz, sx, sy, sz, nx, ny, nz, gx, gy, gz, pad; };
 
-// the near field: the Stokeslets of the 27 colleagues, flattened into batches of 32 staged per
-// warp (the next batch's loads in flight), lanes over the targets; adds c·Σ to the velocities
-template <bool SELF>
+// the near field: the sources of the 27 colleagues, flattened into batches of 32 staged per warp
+// (the next batch's loads in flight), lanes over the targets; adds c·Σ to the velocities (or with
+// PRES to the pressures). DENS adds the stresslets and doublets of sd (3 × n planar: strengths,
+// stressvecs, doublets) to the Stokeslets:
+//   u = c[f/r + g/r³ + d((d·f)/r³ − 3(d·g)/r⁵ − 6(d·f_s)(d·ν)/r⁵)],  p = c[2(d·f)/r³ + 4(f_s·ν)/r³ − 12(d·f_s)(d·ν)/r⁵]
+template <bool SELF, bool DENS, bool PRES>
 __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
                                                          const int* __restrict__ gcount, int ngroups,
                                                          const double* __restrict__ tx, const double* __restrict__ ty,
                                                          const double* __restrict__ tz, const int* __restrict__ tout,
                                                          const double* __restrict__ xs, const double* __restrict__ ys,
                                                          const double* __restrict__ zs, const double* __restrict__ f3,
-                                                         int64_t n, const int* __restrict__ plo, const int* __restrict__ phi,
-                                                         const int* __restrict__ col, double* __restrict__ vel) {
-  __shared__ S8 stg[SW][2][32];
+                                                         const double* __restrict__ sd, int64_t n,
+                                                         const int* __restrict__ plo, const int* __restrict__ phi,
+                                                         const int* __restrict__ col, double* __restrict__ out) {
+  using SV = std::conditional_t<DENS, S16, S8>;
+  __shared__ SV stg[SW][2][32];
   __shared__ int s_lo[SW][32], s_pre[SW][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = blockIdx.x * SW + warp;
@@ -172,16 +218,21 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__
   const int pself = selfm ? __shfl_sync(0xffffffffu, incl - len, slot) : -1;
   const int loself = __shfl_sync(0xffffffffu, lo, slot), lenself = selfm ? __shfl_sync(0xffffffffu, len, slot) : 0;
   __syncwarp();
-  auto load = [&](int b, S8& v) {
+  auto load = [&](int b, SV& v) {
     const int f = 32 * b + lane;
-    v = S8{0, 0, 0, 0, 0, 0, 0, 0};
+    v = SV{};
     if (f < S) {
       int idx = 0;
 #pragma unroll
       for (int step = 16; step; step >>= 1)
         if (s_pre[warp][idx + step] <= f) idx += step;
       const int64_t j = s_lo[warp][idx] + (f - s_pre[warp][idx]);
-      v = S8{xs[j], ys[j], zs[j], f3[j], f3[n + j], f3[2 * n + j], 0, 0};
+      if constexpr (DENS)
+        v = SV{xs[j],         ys[j],         zs[j],         f3[j],         f3[n + j],     f3[2 * n + j],
+               sd[j],         sd[n + j],     sd[2 * n + j], sd[3 * n + j], sd[4 * n + j], sd[5 * n + j],
+               sd[6 * n + j], sd[7 * n + j], sd[8 * n + j], 0};
+      else
+        v = SV{xs[j], ys[j], zs[j], f3[j], f3[n + j], f3[2 * n + j], 0, 0};
     }
   };
   const int t0 = gstart[grp], nt = gcount[grp];
@@ -191,10 +242,10 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__
     const double x = act ? tx[k] : 0.0, y = act ? ty[k] : 0.0, z = act ? tz[k] : 0.0;
     const int fself = SELF && act && selfm ? pself + (k - loself) : -1;
     double ux = 0, uy = 0, uz = 0;
-    S8 nxt;
+    SV nxt;
     load(0, nxt);
     for (int b = 0; 32 * b < S; ++b) {
-      S8* st = stg[warp][b & 1];
+      SV* st = stg[warp][b & 1];
       st[lane] = nxt;
       __syncwarp();
       if (32 * (b + 1) < S) load(b + 1, nxt);
@@ -202,60 +253,93 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__
       const bool chk = SELF && selfm && 32 * b < pself + lenself && 32 * b + 32 > pself;   // uniform
       const int is = fself - 32 * b;
       for (int i = 0; i < m; ++i) {
-        const S8 sv = st[i];
+        const SV sv = st[i];
         const double dx = x - sv.x, dy = y - sv.y, dz = z - sv.z;
         const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
         double ir = rsqrt(r2);
         if (chk && i == is) ir = 0.0;
-        const double df = (dx * sv.fx + dy * sv.fy + dz * sv.fz) * ir * ir * ir;
-        ux += sv.fx * ir + dx * df;
-        uy += sv.fy * ir + dy * df;
-        uz += sv.fz * ir + dz * df;
+        const double ir3 = ir * ir * ir;
+        const double df = dx * sv.fx + dy * sv.fy + dz * sv.fz;
+        if constexpr (DENS) {
+          const double ir5 = ir3 * ir * ir;
+          const double ds = dx * sv.sx + dy * sv.sy + dz * sv.sz, dn = dx * sv.nx + dy * sv.ny + dz * sv.nz;
+          if constexpr (PRES) {
+            const double sn = sv.sx * sv.nx + sv.sy * sv.ny + sv.sz * sv.nz;
+            ux += 2.0 * df * ir3 + 4.0 * sn * ir3 - 12.0 * ds * dn * ir5;
+          } else {
+            const double dg = dx * sv.gx + dy * sv.gy + dz * sv.gz;
+            const double c = df * ir3 - (3.0 * dg + 6.0 * ds * dn) * ir5;
+            ux += sv.fx * ir + sv.gx * ir3 + dx * c;
+            uy += sv.fy * ir + sv.gy * ir3 + dy * c;
+            uz += sv.fz * ir + sv.gz * ir3 + dz * c;
+          }
+        } else if constexpr (PRES) {
+          ux += 2.0 * df * ir3;
+        } else {
+          const double c = df * ir3;
+          ux += sv.fx * ir + dx * c;
+          uy += sv.fy * ir + dy * c;
+          uz += sv.fz * ir + dz * c;
+        }
       }
     }
     if (act) {
       const int o = tout[k];
-      vel[3 * (int64_t)o] += KSTOKES * ux;
-      vel[3 * (int64_t)o + 1] += KSTOKES * uy;
-      vel[3 * (int64_t)o + 2] += KSTOKES * uz;
+      if (PRES) {
+        out[o] += KSTOKES * ux;
+      } else {
+        out[3 * (int64_t)o] += KSTOKES * ux;
+        out[3 * (int64_t)o + 1] += KSTOKES * uy;
+        out[3 * (int64_t)o + 2] += KSTOKES * uz;
+      }
     }
     __syncwarp();
   }
 }
 
 template <int P>
-void launch_stokes_l2p(State& S, double* vel) {
+void launch_stokes_l2p(State& S, bool pres, double* out) {
   Plan& P_ = *S.plan;
   const int LD = P_.cache->ld;
   const size_t smem = sizeof(double) * SW * 4 * LD;
-  FMMB_CUDA(cudaFuncSetAttribute(k_stokes_l2p<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_stokes_l2p<P><<<(P_.n_leaves + SW - 1) / SW, SW * 32, smem, P_.ctx->stream>>>(
+  auto kern = pres ? k_stokes_l2p<P, true> : k_stokes_l2p<P, false>;
+  FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(P_.n_leaves + SW - 1) / SW, SW * 32, smem, P_.ctx->stream>>>(
       P_.leaves.p, P_.leaf_start.p, P_.leaf_count.p, P_.n_leaves, S.xs.p, S.ys.p, S.zs.p, P_.perm.p, P_.cell.p, S.Pl.p, LD,
-      geometry(P_), P_.d_scale.p, vel);
+      geometry(P_), P_.d_scale.p, out);
   FMMB_LAUNCH_CHECK();
 }
 
 }  // namespace
 
-// build_expansions! of a Stokes state from Stokeslets f (3×n, original order, device)
-void stokes_build(State& S, const double* xyz_dev, const double* f_dev) {
+// build_expansions! of a Stokes state from the densities of stokes_fmm_eval! (device, original
+// order)
+void stokes_build(State& S, const double* xyz_dev, const StokesDensities& d) {
   Plan& P = *S.plan;
   Cache& C = *P.cache;
   cudaStream_t s = P.ctx->stream;
   const int LD = C.ld;
   const int64_t n = P.N, pitch = 4 * (int64_t)LD;
+  const bool dens = d.stresslets || d.doublets;
   if (S.f3.n < (size_t)(3 * n)) S.f3.alloc(3 * n);
   if (S.q.n < (size_t)n) S.q.alloc(n);
-  k_stokes_gather<<<nblk(n), 256, 0, s>>>(xyz_dev, f_dev, P.perm.p, n, S.xs.p, S.ys.p, S.zs.p, S.f3.p);
+  if (dens && S.sd.n < (size_t)(9 * n)) S.sd.alloc(9 * n);
+  if (dens && S.dip4.n < (size_t)(12 * n)) S.dip4.alloc(12 * n);
+  k_stokes_gather<<<nblk(n), 256, 0, s>>>(xyz_dev, d, P.perm.p, n, S.xs.p, S.ys.p, S.zs.p, S.f3.p,
+                                          dens ? S.sd.p : nullptr);
   FMMB_LAUNCH_CHECK();
+  S.stokes_dens = dens;
   if (P.n_s2m > 0) {
-    k_stokes_q4<<<nblk((int64_t)P.n_s2m * 32), 256, 0, s>>>(P.s2m_nodes.p, P.n_s2m, P.cell.p, P.plo.p, P.phi.p, geometry(P),
-                                                           P.d_scale.p, n, S.xs.p, S.ys.p, S.zs.p, S.f3.p, S.q.p);
+    auto kern = dens ? k_stokes_q4<true> : k_stokes_q4<false>;
+    kern<<<nblk((int64_t)P.n_s2m * 32), 256, 0, s>>>(P.s2m_nodes.p, P.n_s2m, P.cell.p, P.plo.p, P.phi.p, geometry(P),
+                                                     P.d_scale.p, n, S.xs.p, S.ys.p, S.zs.p, S.f3.p,
+                                                     dens ? S.sd.p : nullptr, S.q.p, dens ? S.dip4.p : nullptr);
     FMMB_LAUNCH_CHECK();
   }
-  // P2M, one block at a time
-  for (int a = 0; a < 3; ++a) p2m_block(S, S.f3.p + a * n, S.M.p + (int64_t)a * LD, pitch);
-  p2m_block(S, S.q.p, S.M.p + 3 * (int64_t)LD, pitch);
+  // P2M, one block at a time (charges, and the dipoles of the stresslets and doublets)
+  for (int a = 0; a < 3; ++a)
+    p2m_block(S, S.f3.p + a * n, dens ? S.dip4.p + 3 * a * n : nullptr, S.M.p + (int64_t)a * LD, pitch);
+  p2m_block(S, S.q.p, dens ? S.dip4.p + 9 * n : nullptr, S.M.p + 3 * (int64_t)LD, pitch);
   // M2M, level by level: the stacked children of each block (Ψ̂ with the coupling), one product each
   for (int l = P.L - 2; l >= 2; --l) {
     const int c0 = P.level_start[l + 1], ng = (P.level_start[l + 2] - c0) / NCH;
@@ -285,18 +369,24 @@ void stokes_build(State& S, const double* xyz_dev, const double* f_dev) {
   S.built = true;
 }
 
-// evaluate_at_sources! of a Stokes state: velocities (3×n, original order, device), self excluded
-void stokes_evaluate_sources(State& S, double* vel_dev) {
+// evaluate_at_sources! of a Stokes state: velocities (3 × n) or pressures (n), original order,
+// device, self excluded
+void stokes_evaluate_sources(State& S, int output, double* out_dev) {
   Plan& P = *S.plan;
+  const bool pres = output == FMMB_STOKES_PRESSURE;
+  require(output == FMMB_STOKES_VELOCITY || pres, FMMB_ERR_UNSUPPORTED,
+          "Stokes outputs are the velocity and the pressure");
   switch (P.cache->p) {
-#define X(pp) case pp: launch_stokes_l2p<pp>(S, vel_dev); break;
+#define X(pp) case pp: launch_stokes_l2p<pp>(S, pres, out_dev); break;
     FMMB_P_CASES(X)
 #undef X
     default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
   }
-  k_stokes_near<true><<<(P.n_leaves + SW - 1) / SW, SW * 32, 0, P.ctx->stream>>>(
+  auto kern = S.stokes_dens ? (pres ? k_stokes_near<true, true, true> : k_stokes_near<true, true, false>)
+                            : (pres ? k_stokes_near<true, false, true> : k_stokes_near<true, false, false>);
+  kern<<<(P.n_leaves + SW - 1) / SW, SW * 32, 0, P.ctx->stream>>>(
       P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, S.xs.p, S.ys.p, S.zs.p, P.perm.p, S.xs.p, S.ys.p, S.zs.p,
-      S.f3.p, P.N, P.plo.p, P.phi.p, P.col.p, vel_dev);
+      S.f3.p, S.stokes_dens ? S.sd.p : nullptr, P.N, P.plo.p, P.phi.p, P.col.p, out_dev);
   FMMB_LAUNCH_CHECK();
 }
 

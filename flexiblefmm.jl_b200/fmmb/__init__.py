@@ -76,6 +76,11 @@ class _Request(C.Structure):
                 ("pot", C.c_void_p), ("grad", C.c_void_p), ("kappa", C.c_double)]
 
 
+class _StokesDensities(C.Structure):
+    _fields_ = [("stokeslets", C.c_void_p), ("stresslets", C.c_void_p), ("stressvecs", C.c_void_p),
+                ("doublets", C.c_void_p), ("weights", C.c_void_p)]
+
+
 class _RequestInfo(C.Structure):
     _fields_ = [("status", C.c_int32), ("p", C.c_int32), ("precision", C.c_int32), ("slot", C.c_int32),
                 ("queued_s", C.c_double), ("run_s", C.c_double), ("latency_s", C.c_double),
@@ -92,6 +97,7 @@ EXPORTS = (
     "fmmb_state_expansions", "fmmb_direct_dev", "fmmb_profile_matvec", "fmmb_direct_noalloc_dev",
     "fmmb_server_create", "fmmb_server_submit", "fmmb_server_wait", "fmmb_server_destroy", "fmmb_stokes_eval",
     "fmmb_stokes_eval_dev", "fmmb_build_expansions_dipoles", "fmmb_build_expansions_dipoles_dev",
+    "fmmb_stokes_eval_densities", "fmmb_stokes_eval_densities_dev",
 )
 
 
@@ -147,6 +153,8 @@ def lib():
         "fmmb_build_expansions_dipoles": [vp, dp, dp, dp, i64],
         "fmmb_build_expansions_dipoles_dev": [vp, dp, dp, dp, i64],
         "fmmb_stokes_eval_dev": [vp, dp, dp, i64, dp],
+        "fmmb_stokes_eval_densities": [vp, dp, C.POINTER(_StokesDensities), i64, i32, dp],
+        "fmmb_stokes_eval_densities_dev": [vp, dp, C.POINTER(_StokesDensities), i64, i32, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -213,7 +221,8 @@ class Stokeslet3D:
 
 class StokesHarmonics:
     """StokesHarmonics(Stokeslet3D(); p=16) (src/operators/harmonics_stokes.jl:34-45): four
-    solid-harmonic expansions per box; Stokeslet densities, velocity output, FP64 path."""
+    solid-harmonic expansions per box; Stokeslet, stresslet and doublet densities, velocity and
+    pressure outputs, FP64 path."""
 
     def __init__(self, kernel, p=16, tol=0.0):
         if not isinstance(kernel, Stokeslet3D):
@@ -686,7 +695,7 @@ class StokesFMMPlan:
     """StokesFMMPlan(sources; method=:harmonics, p=16, ppl, bbox) (src/stokes_api.jl:20-71) for a
     self plan (targets = nothing): the tree and operators of StokesHarmonics(Stokeslet3D(); p) for
     a fixed geometry, reused by every stokes_fmm_eval. The device path provides the :harmonics
-    method with Stokeslet densities and velocity output."""
+    method with Stokeslet, stresslet and doublet densities and velocity and pressure outputs."""
 
     def __init__(self, sources, method="harmonics", p=16, ppl=200, bbox=None, targets=None):
         if method != "harmonics":
@@ -701,13 +710,53 @@ class StokesFMMPlan:
         self.state = FMMState(self.fmm, "fp64")
 
 
-def stokes_fmm_eval(plan, stokeslets, sources=None):
-    """stokes_fmm_eval!(velocities, plan; stokeslets) (src/stokes_api.jl:131-150): velocities at the
-    sources of a self plan, the i = j term skipped; stokeslets (N, 3)."""
+STOKES_VELOCITY = 0
+STOKES_PRESSURE = 1
+
+
+def stokes_densities(n, weights=None, stokeslets=None, stresslets=None, stressvecs=None, doublets=None):
+    """stokes_densities (src/stokes_api.jl:72-83): the checks of the density arrays, as float64
+    arrays in C order ((n, 3) each, weights (n,)); returns them in the order of the C struct."""
+    if (stresslets is None) != (stressvecs is None):
+        raise ArgumentError(1, "stresslets and stressvecs must be given together")
+    out = []
+    for name, a in (("stokeslets", stokeslets), ("stresslets", stresslets), ("stressvecs", stressvecs),
+                    ("doublets", doublets), ("weights", weights)):
+        if a is None:
+            out.append(None)
+            continue
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape[0] != n:
+            raise DimensionMismatch(2, f"{name} has length {a.shape[0]}, expected {n}")
+        if name != "weights" and a.shape != (n, 3):
+            raise DimensionMismatch(2, f"{name} has shape {a.shape}, expected ({n}, 3)")
+        if name == "weights" and a.shape != (n,):
+            raise DimensionMismatch(2, f"weights has shape {a.shape}, expected ({n},)")
+        out.append(a)
+    if out[0] is None and out[1] is None and out[3] is None:
+        raise ArgumentError(1, "provide at least one of stokeslets, stresslets, doublets")
+    return out
+
+
+def stokes_fmm_eval(plan, stokeslets=None, sources=None, stresslets=None, stressvecs=None, doublets=None,
+                    weights=None, output="velocity"):
+    """stokes_fmm_eval!(out, plan; stokeslets, stresslets, stressvecs, doublets, weights, output)
+    (src/stokes_api.jl:107-123) with a self plan: the velocities ((N, 3), output="velocity") or
+    pressures ((N,), output="pressure") at the sources, the i = j term skipped. Stokeslets,
+    stresslet strengths with their stressvecs, and doublets are (N, 3); weights (N,) multiply the
+    stokeslets, stresslet strengths and doublets."""
     x = plan.sources if sources is None else _points(sources)
-    f = np.ascontiguousarray(stokeslets, dtype=np.float64)
-    if f.shape != x.shape:
-        raise DimensionMismatch(2, f"stokeslets has shape {f.shape}, expected {x.shape}")
-    vel = np.zeros_like(f)
-    _check(lib().fmmb_stokes_eval(plan.state._h, _ptr(x), _ptr(f), x.shape[0], _ptr(vel)))
-    return vel
+    n = x.shape[0]
+    outs = {"velocity": STOKES_VELOCITY, "pressure": STOKES_PRESSURE}
+    if output not in outs:
+        raise Unsupported(6, "Stokes outputs are 'velocity' and 'pressure'")
+    arrs = stokes_densities(n, weights=weights, stokeslets=stokeslets, stresslets=stresslets,
+                            stressvecs=stressvecs, doublets=doublets)
+    if stresslets is None and doublets is None and weights is None and output == "velocity":
+        vel = np.zeros((n, 3))
+        _check(lib().fmmb_stokes_eval(plan.state._h, _ptr(x), _ptr(arrs[0]), n, _ptr(vel)))
+        return vel
+    d = _StokesDensities(*[None if a is None else a.ctypes.data for a in arrs])
+    out = np.zeros((n, 3) if output == "velocity" else (n,))
+    _check(lib().fmmb_stokes_eval_densities(plan.state._h, _ptr(x), C.byref(d), n, outs[output], _ptr(out)))
+    return out

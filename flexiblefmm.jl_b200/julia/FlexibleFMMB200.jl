@@ -14,7 +14,7 @@
 module FlexibleFMMB200
 
 using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, CubeKernelIndependent, KernelIndependent,
-    Laplace3D, Laplace2D, Yukawa3D, Stokeslet3D, Potential, Gradient, Dipole
+    Laplace3D, Laplace2D, Yukawa3D, Stokeslet3D, Potential, Gradient, Pressure, Dipole
 using StaticArrays: SVector
 
 const libfmmb = get(ENV, "FMMB_LIB", joinpath(@__DIR__, "..", "libfmmb.so"))
@@ -304,23 +304,53 @@ function StokesFMMPlan(sources::AbstractVector{SVector{3,Float64}}; method::Symb
     return StokesFMMPlan(f, FMMState(f), pts)
 end
 
-"""
-    stokes_fmm_eval!(velocities, plan; stokeslets)  (src/stokes_api.jl:107-123)
+# fmmb_stokes_densities
+struct StokesDensitiesC
+    stokeslets::Ptr{Cvoid}
+    stresslets::Ptr{Cvoid}
+    stressvecs::Ptr{Cvoid}
+    doublets::Ptr{Cvoid}
+    weights::Ptr{Cvoid}
+end
+_dptr(::Nothing) = C_NULL
+_dptr(a::Vector) = Ptr{Cvoid}(pointer(a))
+_dcollect(::Nothing, n, name) = nothing
+function _dcollect(a::AbstractVector, n, name)
+    length(a) == n || throw(DimensionMismatch("$name has length $(length(a)), expected $n"))
+    return collect(a)
+end
 
-Velocities at the plan's sources, the i = j term skipped.
 """
-function stokes_fmm_eval!(vel::AbstractVector{SVector{3,Float64}}, plan::StokesFMMPlan;
-                          stokeslets::AbstractVector{SVector{3,Float64}})
+    stokes_fmm_eval!(out, plan; stokeslets=nothing, stresslets=nothing, stressvecs=nothing,
+                     doublets=nothing, weights=nothing, output=Velocity())  (src/stokes_api.jl:72-123)
+
+Velocities (`Vector{SVector{3,Float64}}`) or, with `output=Pressure()`, pressures (`Vector{Float64}`)
+at the plan's sources, the i = j term skipped. Stokeslets, stresslet strengths with their stressvecs,
+and doublets are `SVector{3,Float64}` per source; weights multiply the stokeslets, the stresslet
+strengths and the doublets.
+"""
+function stokes_fmm_eval!(out::AbstractVector, plan::StokesFMMPlan; stokeslets=nothing, stresslets=nothing,
+                          stressvecs=nothing, doublets=nothing, weights=nothing, output=Potential())
     n = length(plan.sources)
-    length(stokeslets) == n || throw(DimensionMismatch("expected $n stokeslets"))
-    length(vel) == n || throw(DimensionMismatch("expected $n velocities"))
-    fs = collect(stokeslets)
-    out = Vector{SVector{3,Float64}}(undef, n)
-    check(ccall((:fmmb_stokes_eval, libfmmb), Cint,
-                (Ptr{Cvoid}, Ptr{SVector{3,Float64}}, Ptr{SVector{3,Float64}}, Int64, Ptr{SVector{3,Float64}}),
-                plan.state.h, plan.sources, fs, n, out))
-    copyto!(vel, out)
-    return vel
+    (stresslets === nothing) == (stressvecs === nothing) ||
+        throw(ArgumentError("stresslets and stressvecs must be given together"))
+    (stokeslets !== nothing || stresslets !== nothing || doublets !== nothing) ||
+        throw(ArgumentError("provide at least one of stokeslets, stresslets, doublets"))
+    length(out) == n || throw(DimensionMismatch("expected $n outputs"))
+    pres = output isa Pressure
+    pres || output isa Potential || throw(ArgumentError("Stokes outputs are Velocity() and Pressure()"))
+    arrs = (_dcollect(stokeslets, n, "stokeslets"), _dcollect(stresslets, n, "stresslets"),
+            _dcollect(stressvecs, n, "stressvecs"), _dcollect(doublets, n, "doublets"),
+            _dcollect(weights, n, "weights"))
+    res = pres ? Vector{Float64}(undef, n) : Vector{SVector{3,Float64}}(undef, n)
+    GC.@preserve arrs begin
+        d = Ref(StokesDensitiesC(map(_dptr, arrs)...))
+        check(ccall((:fmmb_stokes_eval_densities, libfmmb), Cint,
+                    (Ptr{Cvoid}, Ptr{SVector{3,Float64}}, Ref{StokesDensitiesC}, Int64, Cint, Ptr{Cvoid}),
+                    plan.state.h, plan.sources, d, n, pres ? Cint(1) : Cint(0), res))
+    end
+    copyto!(out, res)
+    return out
 end
 
 end # module

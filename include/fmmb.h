@@ -34,7 +34,7 @@ extern "C" {
 
 #define FMMB_KERNEL_LAPLACE3D 1
 #define FMMB_KERNEL_YUKAWA3D 2    /* e^{−κr}/(4πr), SphericalHarmonics(Yukawa3D(κ); p): FP64 path, operators per width */
-#define FMMB_KERNEL_STOKESLET3D 3 /* StokesHarmonics(Stokeslet3D(); p): FP64 path, Stokeslet densities, velocities */
+#define FMMB_KERNEL_STOKESLET3D 3 /* StokesHarmonics(Stokeslet3D(); p): FP64 path; stokeslets, stresslets, doublets; velocity, pressure */
 #define FMMB_KERNEL_LAPLACE2D 4   /* c·log r², c = −1/(4π): the circle KI method, points in the plane z = 0 */
 #define FMMB_METHOD_SPHERICAL_HARMONICS 1
 #define FMMB_METHOD_CUBE_KI 2 /* CubeKernelIndependent{3}(Laplace3D(); p, pc, d): spectral (FFT) M2L */
@@ -162,6 +162,33 @@ int fmmb_state_expansions(const fmmb_state* state, double* multipoles, double* l
 int fmmb_stokes_eval(fmmb_state* state, const double* xyz, const double* stokeslets, int64_t n, double* velocity);
 int fmmb_stokes_eval_dev(fmmb_state* state, const double* xyz_dev, const double* stokeslets_dev, int64_t n,
                          double* velocity_dev);
+
+/* The densities of stokes_fmm_eval! (src/stokes_api.jl:72-83,107-123): any of stokeslets,
+ * stresslets with stressvecs (both or neither), doublets, each 3×n in the original order or NULL,
+ * at least one given; weights (n or NULL) multiply the stokeslets, the stresslet strengths and the
+ * doublets. Fields (src/sources.jl:203-281, c = 1/8π, d = t − s): stokeslet c(f/r + d(d·f)/r³),
+ * Stresslet(f, ν) −6c d(d·f)(d·ν)/r⁵, Doublet(g) c(g/r³ − 3d(d·g)/r⁵); pressures 2c(d·f)/r³,
+ * 4c[(f·ν)/r³ − 3(d·f)(d·ν)/r⁵] and 0. */
+typedef struct fmmb_stokes_densities {
+  const double* stokeslets;
+  const double* stresslets;
+  const double* stressvecs;
+  const double* doublets;
+  const double* weights;
+} fmmb_stokes_densities;
+
+#define FMMB_STOKES_VELOCITY 0 /* Velocity(): 3×n out */
+#define FMMB_STOKES_PRESSURE 1 /* Pressure(): n out */
+
+/* stokes_fmm_eval!(out, plan; stokeslets, stresslets, stressvecs, doublets, weights, output) with
+ * a self plan (src/stokes_api.jl:107-123) on a Stokeslet state: the velocities or pressures at the
+ * sources, the i = j term skipped. Host pointers (the densities' pointers too); the _dev form
+ * takes device pointers for xyz, every density array and out (dens itself is a host struct).
+ * ArgumentError for no density or a stresslet without its stressvecs. */
+int fmmb_stokes_eval_densities(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
+                               int output, double* out);
+int fmmb_stokes_eval_densities_dev(fmmb_state* state, const double* xyz_dev, const fmmb_stokes_densities* dens,
+                                   int64_t n, int output, double* out_dev);
 
 /* direct!(out, K, sources, τ, targets) / direct_self! (src/kernels.jl:463-487) for Laplace3D on
  * the device in FP64, device pointers: sources 3×ns, targets 3×nt. self_index (device, may be

@@ -180,6 +180,40 @@ def stokes_direct(src, f, sel):
     return out
 
 
+def stokes_direct_all(src, sel, f=None, fs=None, nu=None, g=None, w=None, output="velocity"):
+    """FP64 direct sums at the sources `sel` (i = j skipped) of weighted Stokeslets f, stresslets
+    (fs, ν) and doublets g (src/sources.jl:203-251, c = 1/8π, d = t − s): velocities
+    c[f/r + d(d·f)/r³] − 6c d(d·f_s)(d·ν)/r⁵ + c(g/r³ − 3d(d·g)/r⁵), or pressures
+    2c(d·f)/r³ + 4c[(f_s·ν)/r³ − 3(d·f_s)(d·ν)/r⁵]."""
+    n = src.shape[0]
+    wt = np.ones(n) if w is None else w
+    z = np.zeros((n, 3))
+    f = z if f is None else f * wt[:, None]
+    fs = z if fs is None else fs * wt[:, None]
+    nu = z if nu is None else nu
+    g = z if g is None else g * wt[:, None]
+    c = 1 / (8 * np.pi)
+    out = np.zeros((len(sel), 3) if output == "velocity" else len(sel))
+    for a in range(0, len(sel), 64):
+        idx = sel[a:a + 64]
+        d = src[idx, None, :] - src[None, :, :]
+        r2 = np.einsum("tsk,tsk->ts", d, d)
+        r2[np.arange(len(idx)), idx] = np.inf
+        ir = 1.0 / np.sqrt(r2)
+        ir3, ir5 = ir ** 3, ir ** 5
+        df = np.einsum("tsk,sk->ts", d, f)
+        ds = np.einsum("tsk,sk->ts", d, fs)
+        dn = np.einsum("tsk,sk->ts", d, nu)
+        if output == "velocity":
+            dg = np.einsum("tsk,sk->ts", d, g)
+            coef = df * ir3 - (3 * dg + 6 * ds * dn) * ir5
+            out[a:a + 64] = c * (ir @ f + ir3 @ g + np.einsum("ts,tsk->tk", coef, d))
+        else:
+            sn = np.einsum("sk,sk->s", fs, nu)
+            out[a:a + 64] = c * np.sum(2 * df * ir3 + 4 * sn[None, :] * ir3 - 12 * ds * dn * ir5, axis=1)
+    return out
+
+
 # ---------------------------------------------------------------- Yukawa (src/kernels.jl:224-242)
 def yukawa_direct(src, tau, tgt, kappa, self_excluded=False, gradient=False):
     """FP64 Σ_j τ_j e^{−κr}/(4πr) (and its gradient in the target) at tgt, in chunks."""

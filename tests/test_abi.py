@@ -60,7 +60,7 @@ def test_struct_layouts_match_the_header(fmmb, tmp_path):
     import ctypes as C
     mirrors = {"fmmb_method_desc": fmmb._MethodDesc, "fmmb_tree_opts": fmmb._TreeOpts,
                "fmmb_server_opts": fmmb._ServerOpts, "fmmb_request": fmmb._Request,
-               "fmmb_request_info": fmmb._RequestInfo}
+               "fmmb_request_info": fmmb._RequestInfo, "fmmb_stokes_densities": fmmb._StokesDensities}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "fmmb.h"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
@@ -77,6 +77,24 @@ def test_struct_layouts_match_the_header(fmmb, tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def test_stokes_density_checks(fmmb):
+    """stokes_densities (src/stokes_api.jl:72-83) rejects a stresslet without its stressvecs, no
+    density at all, and arrays of the wrong length, before any device work."""
+    n = 10
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.stokes_densities(n, stresslets=np.ones((n, 3)))
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.stokes_densities(n, stressvecs=np.ones((n, 3)))
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.stokes_densities(n, weights=np.ones(n))
+    with pytest.raises(fmmb.DimensionMismatch):
+        fmmb.stokes_densities(n, doublets=np.ones((n - 1, 3)))
+    with pytest.raises(fmmb.DimensionMismatch):
+        fmmb.stokes_densities(n, stokeslets=np.ones((n, 3)), weights=np.ones(n + 1))
+    a = fmmb.stokes_densities(n, stokeslets=np.ones((n, 3)), doublets=np.zeros((n, 3)))
+    assert a[0].shape == (n, 3) and a[1] is None and a[2] is None and a[3].shape == (n, 3) and a[4] is None
 
 
 def test_square_bbox_contains_the_points(fmmb):

@@ -7,7 +7,7 @@ and the error falling with p."""
 import numpy as np
 import pytest
 
-from helpers import rel_l2, sphere_points, stokes_direct
+from helpers import mrd, rel_l2, sphere_points, stokes_direct, stokes_direct_all
 
 pytestmark = pytest.mark.gpu
 
@@ -85,3 +85,92 @@ def test_stokes_blocks_are_laplace_expansions(fmmb, dist):
         ref = (E0[i] - sum(cen[:, k:k + 1] * E[k][i] for k in range(3))) / wl[:, None]
         got = (SM if i == 0 else SL)[:, 3]
         assert np.max(np.abs(got[sel] - ref[sel])) < 1e-12 * np.max(np.abs(ref[sel])), (dist, i)
+
+
+# ---------------------------------------------------------------- stresslets, doublets, pressure
+def _mixed(rng, n):
+    """Stokeslets, unit stressvecs with their strengths, doublets and weights (the densities of
+    test/test_harmonics_stokes.jl:10-12)."""
+    nu = rng.standard_normal((n, 3))
+    nu /= np.linalg.norm(nu, axis=1)[:, None]
+    return dict(stokeslets=rng.standard_normal((n, 3)), stresslets=rng.standard_normal((n, 3)), stressvecs=nu,
+                doublets=rng.standard_normal((n, 3)), weights=rng.random(n) + 0.5)
+
+
+def _direct(pts, sel, d, output):
+    return stokes_direct_all(pts, sel, f=d.get("stokeslets"), fs=d.get("stresslets"), nu=d.get("stressvecs"),
+                             g=d.get("doublets"), w=d.get("weights"), output=output)
+
+
+def test_single_leaf_densities_are_the_direct_sum(fmmb):
+    rng = np.random.default_rng(11)
+    pts = rng.random((150, 3))
+    d = _mixed(rng, 150)
+    plan = fmmb.StokesFMMPlan(pts, p=6, ppl=200)
+    for output in ("velocity", "pressure"):
+        u = fmmb.stokes_fmm_eval(plan, output=output, **d)
+        assert rel_l2(u, _direct(pts, np.arange(150), d, output)) < 1e-13, output
+
+
+@pytest.mark.parametrize("dist", ["uniform", "sphere"])
+def test_stresslets_doublets_against_direct(fmmb, dist):
+    """test/test_harmonics_stokes.jl:48-60: mixed densities at p = 16 within 1e-4 (max-norm
+    relative, velocity) and 1e-3 (pressure) of direct sums; here each kind alone as well."""
+    rng = np.random.default_rng(12)
+    n = 20000
+    pts = rng.random((n, 3)) if dist == "uniform" else sphere_points(rng, n)
+    d = _mixed(rng, n)
+    sel = np.sort(rng.choice(n, 300, replace=False))
+    plan = fmmb.StokesFMMPlan(pts, p=16, ppl=40)
+    for output, tol in (("velocity", 1e-4), ("pressure", 1e-3)):
+        u = fmmb.stokes_fmm_eval(plan, output=output, **d)
+        assert mrd(u[sel], _direct(pts, sel, d, output)) < tol, (dist, output)
+    for kind in ({"stresslets": d["stresslets"], "stressvecs": d["stressvecs"]}, {"doublets": d["doublets"]}):
+        u = fmmb.stokes_fmm_eval(plan, **kind)
+        assert mrd(u[sel], _direct(pts, sel, kind, "velocity")) < 1e-4, (dist, list(kind))
+
+
+def test_densities_are_linear(fmmb):
+    """The evaluation is linear in the densities: the sum of the three kinds evaluated apart is
+    the evaluation of all three (up to rounding), and the weights scale each source."""
+    rng = np.random.default_rng(13)
+    n = 20000
+    pts = sphere_points(rng, n)
+    d = _mixed(rng, n)
+    plan = fmmb.StokesFMMPlan(pts, p=12, ppl=64)
+    w = d.pop("weights")
+    for output in ("velocity", "pressure"):
+        whole = fmmb.stokes_fmm_eval(plan, output=output, **d)
+        parts = (fmmb.stokes_fmm_eval(plan, output=output, stokeslets=d["stokeslets"])
+                 + fmmb.stokes_fmm_eval(plan, output=output, stresslets=d["stresslets"], stressvecs=d["stressvecs"])
+                 + fmmb.stokes_fmm_eval(plan, output=output, doublets=d["doublets"]))
+        assert rel_l2(parts, whole) < 1e-12, output
+        pre = {k: (v * w[:, None] if k != "stressvecs" else v) for k, v in d.items()}
+        assert rel_l2(fmmb.stokes_fmm_eval(plan, output=output, weights=w, **d),
+                      fmmb.stokes_fmm_eval(plan, output=output, **pre)) < 1e-13, output
+
+
+def test_stokeslets_with_small_doublets(fmmb):
+    """test/test_harmonics_stokes.jl:72-77: the Stokes plan with stokeslets and doublets 0.01·g
+    on a helix-like curve within 1e-5 of direct sums (here at the sources)."""
+    rng = np.random.default_rng(14)
+    n = 3000
+    t = np.sort(rng.random(n)) * 8 * np.pi
+    pts = np.stack([0.5 + 0.3 * np.cos(t), 0.5 + 0.3 * np.sin(t), 0.1 + 0.8 * t / t[-1]], axis=1)
+    pts += 1e-3 * rng.standard_normal(pts.shape)
+    d = dict(stokeslets=rng.standard_normal((n, 3)), doublets=0.01 * rng.standard_normal((n, 3)))
+    plan = fmmb.StokesFMMPlan(pts, p=16, ppl=30)
+    u = fmmb.stokes_fmm_eval(plan, **d)
+    assert mrd(u, _direct(pts, np.arange(n), d, "velocity")) < 1e-5
+
+
+def test_density_errors(fmmb):
+    rng = np.random.default_rng(15)
+    pts = rng.random((2000, 3))
+    plan = fmmb.StokesFMMPlan(pts, p=8, ppl=64)
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.stokes_fmm_eval(plan, stresslets=np.ones((2000, 3)))
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.stokes_fmm_eval(plan)
+    with pytest.raises(fmmb.Unsupported):
+        fmmb.stokes_fmm_eval(plan, stokeslets=np.ones((2000, 3)), output="gradient")
