@@ -232,6 +232,32 @@ void state_build(State& S, const double* xyz, const double* tau) {
   S.built = true;
 }
 
+// build_expansions! + evaluate_at_sources! in one call: the near field (it needs the sources and
+// charges only) runs on the state's side stream beside the upward and downward passes, and the
+// far field adds to it after both; the outputs equal those of the two calls bit for bit
+void matvec_sources(State& S, const double* xyz, const double* tau, int outputs, double* pot, double* grad) {
+  Plan& P = *S.plan;
+  gather_inputs(S, xyz, tau);
+  if (!split_evaluation(S)) {
+    upward_pass(S);
+    downward_pass(S);
+    S.built = true;
+    evaluate_sources(S, outputs, pot, grad);
+    return;
+  }
+  cudaStream_t s = P.ctx->stream;
+  S.side.ensure();
+  FMMB_CUDA(cudaEventRecord(S.side.fork, s));
+  FMMB_CUDA(cudaStreamWaitEvent(S.side.s, S.side.fork, 0));
+  near_sources(S, outputs, pot, grad, S.side.s);
+  FMMB_CUDA(cudaEventRecord(S.side.join, S.side.s));
+  upward_pass(S);
+  downward_pass(S);
+  S.built = true;
+  FMMB_CUDA(cudaStreamWaitEvent(s, S.side.join, 0));
+  far_sources(S, outputs, pot, grad);
+}
+
 }  // namespace
 
 extern "C" {
@@ -252,7 +278,11 @@ int fmmb_ctx_create(int device, fmmb_ctx** out) {
     FMMB_CUDA(cudaGetDeviceProperties(&prop, device));
     require(prop.major == 10, FMMB_ERR_UNSUPPORTED, "this build targets sm_100a (B200)");
     h->c.num_sms = prop.multiProcessorCount;
-    FMMB_CUDA(cudaStreamCreateWithFlags(&h->c.stream, cudaStreamNonBlocking));
+    // the highest priority: the split matvec's near field (on a lowest-priority side stream)
+    // fills what the passes leave of the SMs
+    int lo = 0, hi = 0;
+    FMMB_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    FMMB_CUDA(cudaStreamCreateWithPriority(&h->c.stream, cudaStreamNonBlocking, hi));
     h->c.own_stream = true;
     init_device_constants(h->c.stream);
     *out = h.release();
@@ -638,8 +668,20 @@ int fmmb_evaluate_at_sources(fmmb_state* state, int outputs, double* pot, double
 }
 
 int fmmb_matvec_dev(fmmb_state* state, const double* xyz, const double* tau, int64_t n, int outputs, double* pot, double* grad) {
-  int rc = fmmb_build_expansions_dev(state, xyz, tau, n);
-  return rc != FMMB_OK ? rc : fmmb_evaluate_at_sources_dev(state, outputs, pot, grad);
+  return guard([&] {
+    require(state && xyz && tau, FMMB_ERR_ARGUMENT, "null argument");
+    check_outputs(outputs);
+    State& S = state->s;
+    require(n == S.plan->N, FMMB_ERR_DIMENSION, "expected " + std::to_string(S.plan->N) + " sources and densities");
+    require(!(outputs & FMMB_OUTPUT_POTENTIAL) || pot, FMMB_ERR_ARGUMENT, "null potential output");
+    require(!(outputs & FMMB_OUTPUT_GRADIENT) || grad, FMMB_ERR_ARGUMENT, "null gradient output");
+    set_device(*S.plan->ctx);
+    require_device_ptr(*S.plan->ctx, xyz, "points");
+    require_device_ptr(*S.plan->ctx, tau, "densities");
+    if (outputs & FMMB_OUTPUT_POTENTIAL) require_device_ptr(*S.plan->ctx, pot, "potential output");
+    if (outputs & FMMB_OUTPUT_GRADIENT) require_device_ptr(*S.plan->ctx, grad, "gradient output");
+    matvec_sources(S, xyz, tau, outputs, pot, grad);
+  });
 }
 
 int fmmb_matvec(fmmb_state* state, const double* xyz, const double* tau, int64_t n, int outputs, double* pot, double* grad) {
@@ -657,8 +699,7 @@ int fmmb_matvec(fmmb_state* state, const double* xyz, const double* tau, int64_t
     if (S.d_pot.n < (size_t)P.N) { S.d_pot.alloc(P.N); S.d_grad.alloc(3 * P.N); }
     FMMB_CUDA(cudaMemcpyAsync(S.h_in_xyz.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
     FMMB_CUDA(cudaMemcpyAsync(S.h_in_tau.p, tau, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    state_build(S, S.h_in_xyz.p, S.h_in_tau.p);
-    evaluate_sources(S, outputs, S.d_pot.p, S.d_grad.p);
+    matvec_sources(S, S.h_in_xyz.p, S.h_in_tau.p, outputs, S.d_pot.p, S.d_grad.p);
     if (outputs & FMMB_OUTPUT_POTENTIAL)
       FMMB_CUDA(cudaMemcpyAsync(pot, S.d_pot.p, sizeof(double) * P.N, cudaMemcpyDeviceToHost, s));
     if (outputs & FMMB_OUTPUT_GRADIENT)

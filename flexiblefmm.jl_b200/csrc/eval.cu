@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, cons
                                              const int* __restrict__ tout, const int4* __restrict__ cell,
                                              const double* __restrict__ Pl, int LD, Geometry geo,
                                              const double* __restrict__ scale, int outputs, double* __restrict__ pot,
-                                             double* __restrict__ grad, const double* __restrict__ kh2) {
+                                             double* __restrict__ grad, const double* __restrict__ kh2, int acc) {
   extern __shared__ __align__(16) unsigned char sl_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -54,11 +54,13 @@ __global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, cons
     else l2p<P, R>(L, (R)((x - cx) * s), (R)((y - cy) * s), (R)((z - cz) * s), u, gx, gy, gz);
     if (act) {
       const int o = tout[k];
-      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = (double)u;
+      // acc: the near field is already in the outputs (x + y = y + x: the same sums either way)
+      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = (acc ? pot[o] : 0.0) + (double)u;
       if (outputs & FMMB_OUTPUT_GRADIENT) {
-        grad[3 * (int64_t)o] = (double)gx * s;
-        grad[3 * (int64_t)o + 1] = (double)gy * s;
-        grad[3 * (int64_t)o + 2] = (double)gz * s;
+        const int64_t o3 = 3 * (int64_t)o;
+        grad[o3] = (acc ? grad[o3] : 0.0) + (double)gx * s;
+        grad[o3 + 1] = (acc ? grad[o3 + 1] : 0.0) + (double)gy * s;
+        grad[o3 + 2] = (acc ? grad[o3 + 2] : 0.0) + (double)gz * s;
       }
     }
   }
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32, 5) k_near(const int* __restri
                                                          const int4* __restrict__ cell, const int* __restrict__ plo,
                                                          const int* __restrict__ phi, const int* __restrict__ col,
                                                          Geometry geo, int outputs, double* __restrict__ pot,
-                                                         double* __restrict__ grad, double kappa) {
+                                                         double* __restrict__ grad, double kappa, int first) {
   constexpr bool REL = sizeof(R) == 4;   // the mixed path works relative to the leaf's centre
   __shared__ NearWarp<R> sws[NEAR_WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -323,11 +325,13 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32, 5) k_near(const int* __restri
     }
     if (act) {
       const int o = tout[k];
-      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = pot[o] + KC * np;
+      // first: the far field comes after (and adds to) these
+      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = (first ? 0.0 : pot[o]) + KC * np;
       if (outputs & FMMB_OUTPUT_GRADIENT) {
-        grad[3 * (int64_t)o] = grad[3 * (int64_t)o] - KC * nx;
-        grad[3 * (int64_t)o + 1] = grad[3 * (int64_t)o + 1] - KC * ny;
-        grad[3 * (int64_t)o + 2] = grad[3 * (int64_t)o + 2] - KC * nz;
+        const int64_t o3 = 3 * (int64_t)o;
+        grad[o3] = (first ? 0.0 : grad[o3]) - KC * nx;
+        grad[o3 + 1] = (first ? 0.0 : grad[o3 + 1]) - KC * ny;
+        grad[o3 + 2] = (first ? 0.0 : grad[o3 + 2]) - KC * nz;
       }
     }
     __syncwarp();   // the staging buffers are reused by the next group of targets
@@ -555,7 +559,7 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32) k_near_dip(const int* __restr
 
 template <int P>
 void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
-                const double* tz, const int* tout, int outputs, double* pot, double* grad) {
+                const double* tz, const int* tout, int outputs, double* pot, double* grad, int acc = 0) {
   Plan& P_ = *S.plan;
   const int warps = 8;
   const bool mixed = S.precision == FMMB_PRECISION_MIXED;
@@ -564,17 +568,18 @@ void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount
                     : (P_.cache->kernel == FMMB_KERNEL_YUKAWA3D ? k_l2p<P, double, true> : k_l2p<P, double, false>);
   kern<<<(ng + warps - 1) / warps, 32 * warps, smem, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, P_.cell.p,
                                                                       S.Pl.p, P_.cache->ld, geometry(P_), P_.d_scale.p,
-                                                                      outputs, pot, grad, P_.d_kh2.p);
+                                                                      outputs, pot, grad, P_.d_kh2.p, acc);
   FMMB_LAUNCH_CHECK();
 }
 
 template <typename R, bool SELF, int YK = 0>
 void launch_near(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
-                 const double* tz, const int* tout, int outputs, double* pot, double* grad) {
+                 const double* tz, const int* tout, int outputs, double* pot, double* grad, int first = 0,
+                 cudaStream_t st = nullptr) {
   Plan& P_ = *S.plan;
-  k_near<R, SELF, YK><<<(ng + NEAR_WARPS - 1) / NEAR_WARPS, 32 * NEAR_WARPS, 0, P_.ctx->stream>>>(
+  k_near<R, SELF, YK><<<(ng + NEAR_WARPS - 1) / NEAR_WARPS, 32 * NEAR_WARPS, 0, st ? st : P_.ctx->stream>>>(
       gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p, S.zs.p, S.q.p, P_.cell.p, P_.plo.p, P_.phi.p, P_.col.p,
-      geometry(P_), outputs, pot, grad, P_.cache->kappa);
+      geometry(P_), outputs, pot, grad, P_.cache->kappa, first);
   FMMB_LAUNCH_CHECK();
 }
 
@@ -644,6 +649,45 @@ void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* g
   else if (mixed) launch_near<float, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
   else if (self) launch_near<double, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
   else launch_near<double, false>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
+}
+
+// the harmonic method's evaluation at the sources in two halves: the near field on stream st
+// (writing the outputs) and, after it, the far field (adding to them); charges only
+bool split_evaluation(const State& S) {
+  const Cache& C = *S.plan->cache;
+  return C.method == FMMB_METHOD_SPHERICAL_HARMONICS && !S.has_dip &&
+         (C.kernel == FMMB_KERNEL_LAPLACE3D || C.kernel == FMMB_KERNEL_YUKAWA3D);
+}
+
+void near_sources(State& S, int outputs, double* pot, double* grad, cudaStream_t st) {
+  Plan& P = *S.plan;
+  if (P.n_leaves == 0) return;
+  const bool mixed = S.precision == FMMB_PRECISION_MIXED;
+  const double *tx = S.xs.p, *ty = S.ys.p, *tz = S.zs.p;
+  if (P.cache->kernel == FMMB_KERNEL_YUKAWA3D)
+    launch_near<double, true, 1>(S, P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, tx, ty, tz, P.perm.p, outputs,
+                                 pot, grad, 1, st);
+  else if (mixed)
+    launch_near<float, true>(S, P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, tx, ty, tz, P.perm.p, outputs, pot,
+                             grad, 1, st);
+  else
+    launch_near<double, true>(S, P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, tx, ty, tz, P.perm.p, outputs, pot,
+                              grad, 1, st);
+}
+
+void far_sources(State& S, int outputs, double* pot, double* grad) {
+  Plan& P = *S.plan;
+  if (P.n_leaves == 0) return;
+  switch (P.cache->p) {
+#define X(pp)                                                                                                    \
+  case pp:                                                                                                       \
+    launch_l2p<pp>(S, P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, S.xs.p, S.ys.p, S.zs.p, P.perm.p, outputs, \
+                   pot, grad, 1);                                                                                \
+    break;
+    FMMB_P_CASES(X)
+#undef X
+    default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
+  }
 }
 
 }  // namespace fmmb

@@ -573,6 +573,24 @@ int m2m_sweep(State& S) {
   return launches;
 }
 
+void State::Side::ensure() {
+  if (s) return;
+  int lo = 0, hi = 0;
+  FMMB_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  FMMB_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, lo));   // the lowest priority
+  FMMB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  FMMB_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+}
+
+State::Side::~Side() {
+  if (s) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
+}
+
 void upward_pass(State& S) {
   p2m(S);
   m2m_sweep(S);

@@ -148,6 +148,14 @@ struct State {
   DBuf<double> ki_pm, ki_y, ki_ll;
   DBuf<float2> ki_spec, ki_u;
   bool built = false;
+  // the side stream of the split matvec (the near field beside the passes) and its two events,
+  // created on first use
+  struct Side {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    void ensure();
+    ~Side();
+  } side;
   // staging of the host-pointer entry points and the evaluation at targets
   DBuf<double> h_in_xyz, h_in_tau, d_pot, d_grad;
   DBuf<double> t_x, t_y, t_z;
@@ -170,6 +178,11 @@ void upward_pass(State& S);
 void downward_pass(State& S);
 void evaluate_sources(State& S, int outputs, double* pot_dev, double* grad_dev);
 void evaluate_targets(State& S, const double* tg_dev, int64_t nt, int outputs, double* pot_dev, double* grad_dev);
+// eval.cu: the evaluation at the sources split in two (harmonic methods with charges): the near
+// field on stream st writes the outputs, the far field (on the state's stream, after it) adds
+bool split_evaluation(const State& S);
+void near_sources(State& S, int outputs, double* pot_dev, double* grad_dev, cudaStream_t st);
+void far_sources(State& S, int outputs, double* pot_dev, double* grad_dev);
 void bounds(Ctx& ctx, const double* xyz_dev, int64_t n, double lo[3], double hi[3], int64_t* nonfinite);
 void direct(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
             int64_t nt, double* pot, double* grad);
