@@ -872,8 +872,11 @@ namespace {
 
 // the checks of stokes_densities (src/stokes_api.jl:72-83) and of the state
 void check_stokes_call(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n, int output,
-                       double* out) {
-  require(state && xyz && dens && out, FMMB_ERR_ARGUMENT, "null argument");
+                       const double* targets, int64_t nt, const double* out_src, const double* out_trg) {
+  require(state && xyz && dens, FMMB_ERR_ARGUMENT, "null argument");
+  require(out_src || out_trg, FMMB_ERR_ARGUMENT, "no output");
+  require(nt >= 0, FMMB_ERR_DIMENSION, "negative target count");
+  require(!out_trg || nt == 0 || targets, FMMB_ERR_ARGUMENT, "null targets");
   require((dens->stresslets == nullptr) == (dens->stressvecs == nullptr), FMMB_ERR_ARGUMENT,
           "stresslets and stressvecs must be given together");
   require(dens->stokeslets || dens->stresslets || dens->doublets, FMMB_ERR_ARGUMENT,
@@ -885,12 +888,18 @@ void check_stokes_call(fmmb_state* state, const double* xyz, const fmmb_stokes_d
   require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and densities");
 }
 
-}  // namespace
+// build_expansions! then the evaluations asked for (device pointers)
+void stokes_run(State& S, const double* xyz, const StokesDensities& d, const double* tg, int64_t nt, int output,
+                double* out_src, double* out_trg) {
+  stokes_build(S, xyz, d);
+  if (out_src) stokes_evaluate_sources(S, output, out_src);
+  if (out_trg && nt > 0) stokes_evaluate_targets(S, tg, nt, output, out_trg);
+}
 
-int fmmb_stokes_eval_densities_dev(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
-                                   int output, double* out) {
+int stokes_dev(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n, const double* tg,
+               int64_t nt, int output, double* out_src, double* out_trg) {
   return guard([&] {
-    check_stokes_call(state, xyz, dens, n, output, out);
+    check_stokes_call(state, xyz, dens, n, output, tg, nt, out_src, out_trg);
     State& S = state->s;
     Plan& P = *S.plan;
     set_device(*P.ctx);
@@ -898,32 +907,37 @@ int fmmb_stokes_eval_densities_dev(fmmb_state* state, const double* xyz, const f
     const double* arrays[5] = {dens->stokeslets, dens->stresslets, dens->stressvecs, dens->doublets, dens->weights};
     for (const double* a : arrays)
       if (a) require_device_ptr(*P.ctx, a, "densities");
-    require_device_ptr(*P.ctx, out, "outputs");
+    if (out_src) require_device_ptr(*P.ctx, out_src, "outputs");
+    if (out_trg && nt > 0) {
+      require_device_ptr(*P.ctx, tg, "targets");
+      require_device_ptr(*P.ctx, out_trg, "outputs");
+    }
     StokesDensities d;
     d.stokeslets = dens->stokeslets;
     d.stresslets = dens->stresslets;
     d.stressvecs = dens->stressvecs;
     d.doublets = dens->doublets;
     d.weights = dens->weights;
-    stokes_build(S, xyz, d);
-    stokes_evaluate_sources(S, output, out);
+    stokes_run(S, xyz, d, tg, nt, output, out_src, out_trg);
   });
 }
 
-int fmmb_stokes_eval_densities(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
-                               int output, double* out) {
+int stokes_host(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n, const double* tg,
+                int64_t nt, int output, double* out_src, double* out_trg) {
   return guard([&] {
-    check_stokes_call(state, xyz, dens, n, output, out);
+    check_stokes_call(state, xyz, dens, n, output, tg, nt, out_src, out_trg);
     State& S = state->s;
     Plan& P = *S.plan;
     set_device(*P.ctx);
     cudaStream_t s = P.ctx->stream;
-    const int64_t no = output == FMMB_STOKES_PRESSURE ? n : 3 * n;
-    DBuf<double> x(3 * n), o(no);
+    const int w = output == FMMB_STOKES_PRESSURE ? 1 : 3;
+    const bool trg = out_trg && nt > 0;
+    DBuf<double> x(3 * n), os(out_src ? w * n : 0), t(trg ? 3 * nt : 0), ot(trg ? w * nt : 0);
     DBuf<double> a[5];
     const double* src[5] = {dens->stokeslets, dens->stresslets, dens->stressvecs, dens->doublets, dens->weights};
     const double* dev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     FMMB_CUDA(cudaMemcpyAsync(x.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    if (trg) FMMB_CUDA(cudaMemcpyAsync(t.p, tg, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
     for (int k = 0; k < 5; ++k) {
       if (!src[k]) continue;
       const int64_t len = k == 4 ? n : 3 * n;
@@ -937,11 +951,33 @@ int fmmb_stokes_eval_densities(fmmb_state* state, const double* xyz, const fmmb_
     d.stressvecs = dev[2];
     d.doublets = dev[3];
     d.weights = dev[4];
-    stokes_build(S, x.p, d);
-    stokes_evaluate_sources(S, output, o.p);
-    FMMB_CUDA(cudaMemcpyAsync(out, o.p, sizeof(double) * no, cudaMemcpyDeviceToHost, s));
+    stokes_run(S, x.p, d, t.p, trg ? nt : 0, output, out_src ? os.p : nullptr, trg ? ot.p : nullptr);
+    if (out_src) FMMB_CUDA(cudaMemcpyAsync(out_src, os.p, sizeof(double) * w * n, cudaMemcpyDeviceToHost, s));
+    if (trg) FMMB_CUDA(cudaMemcpyAsync(out_trg, ot.p, sizeof(double) * w * nt, cudaMemcpyDeviceToHost, s));
     FMMB_CUDA(cudaStreamSynchronize(s));
   });
+}
+
+}  // namespace
+
+int fmmb_stokes_eval_densities_dev(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
+                                   int output, double* out) {
+  return stokes_dev(state, xyz, dens, n, nullptr, 0, output, out, nullptr);
+}
+
+int fmmb_stokes_eval_densities(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
+                               int output, double* out) {
+  return stokes_host(state, xyz, dens, n, nullptr, 0, output, out, nullptr);
+}
+
+int fmmb_stokes_eval_src_trg_dev(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
+                                 const double* targets, int64_t nt, int output, double* out_src, double* out_trg) {
+  return stokes_dev(state, xyz, dens, n, targets, nt, output, out_src, out_trg);
+}
+
+int fmmb_stokes_eval_src_trg(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
+                             const double* targets, int64_t nt, int output, double* out_src, double* out_trg) {
+  return stokes_host(state, xyz, dens, n, targets, nt, output, out_src, out_trg);
 }
 
 int fmmb_direct_dev(fmmb_ctx* ctx, const double* src, const double* tau, int64_t ns, const double* tgt,

@@ -647,8 +647,16 @@ void evaluate_sources(State& S, int outputs, double* pot, double* grad) {
 void evaluate_targets(State& S, const double* tg, int64_t nt, int outputs, double* pot, double* grad) {
   Plan& P = *S.plan;
   require(P.cache->kernel != FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED, "a Stokeslet state takes fmmb_stokes_eval");
-  cudaStream_t s = P.ctx->stream;
   if (nt == 0) return;
+  const int ng = group_targets(S, tg, nt);
+  const int* gnode = S.t_groups.p;
+  evaluate_groups(S, gnode, gnode + ng, gnode + 2 * ng, ng, S.t_x.p, S.t_y.p, S.t_z.p, S.t_out.p, false, outputs, pot, grad);
+  FMMB_CUDA(cudaStreamSynchronize(P.ctx->stream));
+}
+
+int group_targets(State& S, const double* tg, int64_t nt) {
+  Plan& P = *S.plan;
+  cudaStream_t s = P.ctx->stream;
   require(nt < (1ll << 31) - 1, FMMB_ERR_ARGUMENT, "too many targets");
   if ((int64_t)S.t_x.n < nt) {
     S.t_x.alloc(nt); S.t_y.alloc(nt); S.t_z.alloc(nt); S.t_out.alloc(nt); S.t_node.alloc(nt);
@@ -670,8 +678,7 @@ void evaluate_targets(State& S, const double* tg, int64_t nt, int outputs, doubl
   int* gcount = gstart + ng;
   k_groups<<<nblk(nt), 256, 0, s>>>(S.t_keys.p, S.t_node.p, pos.p, nt, ng, gnode, gstart, gcount);
   FMMB_LAUNCH_CHECK();
-  evaluate_groups(S, gnode, gstart, gcount, ng, S.t_x.p, S.t_y.p, S.t_z.p, S.t_out.p, false, outputs, pot, grad);
-  FMMB_CUDA(cudaStreamSynchronize(s));
+  return ng;   // pos and the flag are freed in stream order
 }
 
 void bounds(Ctx& ctx, const double* xyz, int64_t n, double lo[3], double hi[3], int64_t* nonfinite) {

@@ -178,6 +178,10 @@ void upward_pass(State& S);
 void downward_pass(State& S);
 void evaluate_sources(State& S, int outputs, double* pot_dev, double* grad_dev);
 void evaluate_targets(State& S, const double* tg_dev, int64_t nt, int outputs, double* pot_dev, double* grad_dev);
+// locate nt > 0 targets (device, 3 × nt) in the tree's leaves (FMMB_ERR_ARGUMENT outside the box)
+// and group them per leaf: S.t_x/t_y/t_z in leaf order, S.t_out their original indices, and the ng
+// groups (returned) as S.t_groups = [node; first; count] (ng each)
+int group_targets(State& S, const double* tg_dev, int64_t nt);
 // eval.cu: the evaluation at the sources split in two (harmonic methods with charges): the near
 // field on stream st writes the outputs, the far field (on the state's stream, after it) adds
 bool split_evaluation(const State& S);
@@ -211,6 +215,8 @@ struct StokesDensities {
 void stokes_build(State& S, const double* xyz_dev, const StokesDensities& d);
 // output FMMB_STOKES_VELOCITY (3 × n) or FMMB_STOKES_PRESSURE (n), original order, device
 void stokes_evaluate_sources(State& S, int output, double* out_dev);
+// the same at nt targets (device, 3 × nt) inside the tree's box, in the targets' order
+void stokes_evaluate_targets(State& S, const double* tg_dev, int64_t nt, int output, double* out_dev);
 // direct_noalloc.cu: the same sums with the partials in a fixed array compiled into the library
 void direct_noalloc(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
                     int64_t nt, double* pot, double* grad);

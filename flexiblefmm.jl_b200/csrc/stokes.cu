@@ -298,15 +298,15 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__
 }
 
 template <int P>
-void launch_stokes_l2p(State& S, bool pres, double* out) {
+void launch_stokes_l2p(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
+                       const double* ty, const double* tz, const int* tout, bool pres, double* out) {
   Plan& P_ = *S.plan;
   const int LD = P_.cache->ld;
   const size_t smem = sizeof(double) * SW * 4 * LD;
   auto kern = pres ? k_stokes_l2p<P, true> : k_stokes_l2p<P, false>;
   FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(P_.n_leaves + SW - 1) / SW, SW * 32, smem, P_.ctx->stream>>>(
-      P_.leaves.p, P_.leaf_start.p, P_.leaf_count.p, P_.n_leaves, S.xs.p, S.ys.p, S.zs.p, P_.perm.p, P_.cell.p, S.Pl.p, LD,
-      geometry(P_), P_.d_scale.p, out);
+  kern<<<(ng + SW - 1) / SW, SW * 32, smem, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, P_.cell.p, S.Pl.p,
+                                                              LD, geometry(P_), P_.d_scale.p, out);
   FMMB_LAUNCH_CHECK();
 }
 
@@ -369,25 +369,51 @@ void stokes_build(State& S, const double* xyz_dev, const StokesDensities& d) {
   S.built = true;
 }
 
-// evaluate_at_sources! of a Stokes state: velocities (3 × n) or pressures (n), original order,
-// device, self excluded
-void stokes_evaluate_sources(State& S, int output, double* out_dev) {
+namespace {
+
+// the far and near fields at ng groups of targets (per leaf: node, first, count), targets in
+// group order with their output indices tout; self: the targets are the sources (i = j skipped)
+void stokes_evaluate_groups(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
+                            const double* ty, const double* tz, const int* tout, bool self, int output, double* out) {
   Plan& P = *S.plan;
   const bool pres = output == FMMB_STOKES_PRESSURE;
   require(output == FMMB_STOKES_VELOCITY || pres, FMMB_ERR_UNSUPPORTED,
           "Stokes outputs are the velocity and the pressure");
+  if (ng == 0) return;
   switch (P.cache->p) {
-#define X(pp) case pp: launch_stokes_l2p<pp>(S, pres, out_dev); break;
+#define X(pp) case pp: launch_stokes_l2p<pp>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, pres, out); break;
     FMMB_P_CASES(X)
 #undef X
     default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
   }
-  auto kern = S.stokes_dens ? (pres ? k_stokes_near<true, true, true> : k_stokes_near<true, true, false>)
-                            : (pres ? k_stokes_near<true, false, true> : k_stokes_near<true, false, false>);
-  kern<<<(P.n_leaves + SW - 1) / SW, SW * 32, 0, P.ctx->stream>>>(
-      P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, S.xs.p, S.ys.p, S.zs.p, P.perm.p, S.xs.p, S.ys.p, S.zs.p,
-      S.f3.p, S.stokes_dens ? S.sd.p : nullptr, P.N, P.plo.p, P.phi.p, P.col.p, out_dev);
+  const bool d = S.stokes_dens;
+  auto kern = self ? (d ? (pres ? k_stokes_near<true, true, true> : k_stokes_near<true, true, false>)
+                        : (pres ? k_stokes_near<true, false, true> : k_stokes_near<true, false, false>))
+                   : (d ? (pres ? k_stokes_near<false, true, true> : k_stokes_near<false, true, false>)
+                        : (pres ? k_stokes_near<false, false, true> : k_stokes_near<false, false, false>));
+  kern<<<(ng + SW - 1) / SW, SW * 32, 0, P.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p,
+                                                          S.zs.p, S.f3.p, d ? S.sd.p : nullptr, P.N, P.plo.p, P.phi.p,
+                                                          P.col.p, out);
   FMMB_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+// evaluate_at_sources! of a Stokes state: velocities (3 × n) or pressures (n), original order,
+// device, self excluded
+void stokes_evaluate_sources(State& S, int output, double* out_dev) {
+  Plan& P = *S.plan;
+  stokes_evaluate_groups(S, P.leaves.p, P.leaf_start.p, P.leaf_count.p, P.n_leaves, S.xs.p, S.ys.p, S.zs.p, P.perm.p, true,
+                         output, out_dev);
+}
+
+// evaluate! of a Stokes state at nt targets (device, 3 × nt): velocities (3 × nt) or pressures
+// (nt) in the targets' order, device
+void stokes_evaluate_targets(State& S, const double* tg_dev, int64_t nt, int output, double* out_dev) {
+  if (nt == 0) return;
+  const int ng = group_targets(S, tg_dev, nt);
+  const int* g = S.t_groups.p;
+  stokes_evaluate_groups(S, g, g + ng, g + 2 * ng, ng, S.t_x.p, S.t_y.p, S.t_z.p, S.t_out.p, false, output, out_dev);
 }
 
 }  // namespace fmmb

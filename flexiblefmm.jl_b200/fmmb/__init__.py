@@ -97,7 +97,8 @@ EXPORTS = (
     "fmmb_state_expansions", "fmmb_direct_dev", "fmmb_profile_matvec", "fmmb_direct_noalloc_dev",
     "fmmb_server_create", "fmmb_server_submit", "fmmb_server_wait", "fmmb_server_destroy", "fmmb_stokes_eval",
     "fmmb_stokes_eval_dev", "fmmb_build_expansions_dipoles", "fmmb_build_expansions_dipoles_dev",
-    "fmmb_stokes_eval_densities", "fmmb_stokes_eval_densities_dev",
+    "fmmb_stokes_eval_densities", "fmmb_stokes_eval_densities_dev", "fmmb_stokes_eval_src_trg",
+    "fmmb_stokes_eval_src_trg_dev",
 )
 
 
@@ -155,6 +156,8 @@ def lib():
         "fmmb_stokes_eval_dev": [vp, dp, dp, i64, dp],
         "fmmb_stokes_eval_densities": [vp, dp, C.POINTER(_StokesDensities), i64, i32, dp],
         "fmmb_stokes_eval_densities_dev": [vp, dp, C.POINTER(_StokesDensities), i64, i32, dp],
+        "fmmb_stokes_eval_src_trg": [vp, dp, C.POINTER(_StokesDensities), i64, dp, i64, i32, dp, dp],
+        "fmmb_stokes_eval_src_trg_dev": [vp, dp, C.POINTER(_StokesDensities), i64, dp, i64, i32, dp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -692,19 +695,21 @@ def square_bbox(points):
 
 
 class StokesFMMPlan:
-    """StokesFMMPlan(sources; method=:harmonics, p=16, ppl, bbox) (src/stokes_api.jl:20-71) for a
-    self plan (targets = nothing): the tree and operators of StokesHarmonics(Stokeslet3D(); p) for
-    a fixed geometry, reused by every stokes_fmm_eval. The device path provides the :harmonics
-    method with Stokeslet, stresslet and doublet densities and velocity and pressure outputs."""
+    """StokesFMMPlan(sources; targets, method=:harmonics, p=16, ppl, bbox) (src/stokes_api.jl:20-62):
+    the tree and operators of StokesHarmonics(Stokeslet3D(); p) for a fixed geometry, reused by
+    every stokes_fmm_eval; with targets, the box covers the sources and the targets (square_bbox of
+    both, as the reference plan fits it) and stokes_fmm_eval evaluates there. The device path
+    provides the :harmonics method with Stokeslet, stresslet and doublet densities and velocity and
+    pressure outputs."""
 
     def __init__(self, sources, method="harmonics", p=16, ppl=200, bbox=None, targets=None):
         if method != "harmonics":
             raise Unsupported(6, "the device path provides method=:harmonics")
-        if targets is not None:
-            raise Unsupported(6, "the device path evaluates Stokes plans at their sources")
         self.sources = _points(sources)
+        self.targets = None if targets is None else _points(targets)
         if bbox is None:
-            bbox = square_bbox(self.sources)
+            bbox = square_bbox(self.sources if self.targets is None
+                               else np.concatenate([self.sources, self.targets]))
         self.method = StokesHarmonics(Stokeslet3D(), p=p)
         self.fmm = FMM(self.method, self.sources, ppl=ppl, bbox=bbox)
         self.state = FMMState(self.fmm, "fp64")
@@ -738,25 +743,49 @@ def stokes_densities(n, weights=None, stokeslets=None, stresslets=None, stressve
     return out
 
 
-def stokes_fmm_eval(plan, stokeslets=None, sources=None, stresslets=None, stressvecs=None, doublets=None,
-                    weights=None, output="velocity"):
-    """stokes_fmm_eval!(out, plan; stokeslets, stresslets, stressvecs, doublets, weights, output)
-    (src/stokes_api.jl:107-123) with a self plan: the velocities ((N, 3), output="velocity") or
-    pressures ((N,), output="pressure") at the sources, the i = j term skipped. Stokeslets,
-    stresslet strengths with their stressvecs, and doublets are (N, 3); weights (N,) multiply the
-    stokeslets, stresslet strengths and doublets."""
+def _stokes_call(plan, sources, targets, at_sources, output, dens):
     x = plan.sources if sources is None else _points(sources)
     n = x.shape[0]
     outs = {"velocity": STOKES_VELOCITY, "pressure": STOKES_PRESSURE}
     if output not in outs:
         raise Unsupported(6, "Stokes outputs are 'velocity' and 'pressure'")
-    arrs = stokes_densities(n, weights=weights, stokeslets=stokeslets, stresslets=stresslets,
-                            stressvecs=stressvecs, doublets=doublets)
-    if stresslets is None and doublets is None and weights is None and output == "velocity":
-        vel = np.zeros((n, 3))
-        _check(lib().fmmb_stokes_eval(plan.state._h, _ptr(x), _ptr(arrs[0]), n, _ptr(vel)))
-        return vel
+    arrs = stokes_densities(n, **dens)
+    tg = plan.targets if targets is None else _points(targets)
+    shape = (lambda m: (m, 3)) if output == "velocity" else (lambda m: (m,))
+    src = np.zeros(shape(n)) if at_sources else None
+    trg = None if tg is None else np.zeros(shape(tg.shape[0]))
+    if src is not None and trg is None and arrs[1] is None and arrs[3] is None and arrs[4] is None \
+            and output == "velocity":
+        _check(lib().fmmb_stokes_eval(plan.state._h, _ptr(x), _ptr(arrs[0]), n, _ptr(src)))
+        return src, None
     d = _StokesDensities(*[None if a is None else a.ctypes.data for a in arrs])
-    out = np.zeros((n, 3) if output == "velocity" else (n,))
-    _check(lib().fmmb_stokes_eval_densities(plan.state._h, _ptr(x), C.byref(d), n, outs[output], _ptr(out)))
-    return out
+    _check(lib().fmmb_stokes_eval_src_trg(plan.state._h, _ptr(x), C.byref(d), n, _ptr(tg),
+                                          0 if tg is None else tg.shape[0], outs[output], _ptr(src), _ptr(trg)))
+    return src, trg
+
+
+def stokes_fmm_eval(plan, stokeslets=None, sources=None, stresslets=None, stressvecs=None, doublets=None,
+                    weights=None, targets=None, output="velocity"):
+    """stokes_fmm_eval!(out, plan; stokeslets, stresslets, stressvecs, doublets, weights, sources,
+    targets, output) (src/stokes_api.jl:107-123): the velocities ((M, 3), output="velocity") or
+    pressures ((M,), output="pressure") at the plan's targets (or `targets`, inside the plan's
+    box), or at the sources of a self plan with the i = j term skipped. Stokeslets, stresslet
+    strengths with their stressvecs, and doublets are (N, 3); weights (N,) multiply the
+    stokeslets, stresslet strengths and doublets."""
+    dens = dict(weights=weights, stokeslets=stokeslets, stresslets=stresslets, stressvecs=stressvecs,
+                doublets=doublets)
+    self_plan = plan.targets is None and targets is None
+    src, trg = _stokes_call(plan, sources, targets, self_plan, output, dens)
+    return src if self_plan else trg
+
+
+def stokes_fmm_eval_src_trg(plan, stokeslets=None, sources=None, stresslets=None, stressvecs=None, doublets=None,
+                            weights=None, targets=None, output="velocity"):
+    """stokes_fmm_eval_src_trg!(vel_src, vel_trg, plan; ...) (src/stokes_api.jl:125-146): one
+    expansion build, the outputs at the sources (i = j skipped) and at the plan's targets (or
+    `targets`); returns (at the sources, at the targets)."""
+    if plan.targets is None and targets is None:
+        raise ArgumentError(1, "the plan has no targets")
+    dens = dict(weights=weights, stokeslets=stokeslets, stresslets=stresslets, stressvecs=stressvecs,
+                doublets=doublets)
+    return _stokes_call(plan, sources, targets, True, output, dens)

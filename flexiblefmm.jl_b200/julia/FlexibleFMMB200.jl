@@ -284,24 +284,26 @@ end
 
 # ---------------------------------------------------------------- the Stokes plan API (src/stokes_api.jl)
 """
-    StokesFMMPlan(sources; method=:harmonics, p=16, ppl=200, bbox=nothing)  (src/stokes_api.jl:20-62)
+    StokesFMMPlan(sources; targets=nothing, method=:harmonics, p=16, ppl=200, bbox=nothing)  (src/stokes_api.jl:20-62)
 
-A self plan (targets = nothing) of StokesHarmonics(Stokeslet3D(); p) on the device: the tree and
-operators for a fixed geometry, reused by every `stokes_fmm_eval!`.
+A plan of StokesHarmonics(Stokeslet3D(); p) on the device: the tree and operators for a fixed
+geometry, reused by every `stokes_fmm_eval!`. With targets, the box covers the sources and the
+targets (`square_bbox` of both, as the reference plan fits it) and the evaluation is there.
 """
 struct StokesFMMPlan
     fmm::FMM
     state::FMMState
     sources::Vector{SVector{3,Float64}}
+    targets::Union{Nothing,Vector{SVector{3,Float64}}}
 end
 function StokesFMMPlan(sources::AbstractVector{SVector{3,Float64}}; method::Symbol=:harmonics, p::Integer=16,
                        ppl::Integer=200, bbox=nothing, targets=nothing)
     method === :harmonics || throw(ArgumentError("the device path provides method=:harmonics"))
-    targets === nothing || throw(ArgumentError("the device path evaluates Stokes plans at their sources"))
     pts = collect(sources)
-    bbox === nothing && (bbox = FlexibleFMM.square_bbox(pts))     # as the reference plan does
+    tgs = targets === nothing ? nothing : collect(SVector{3,Float64}, targets)
+    bbox === nothing && (bbox = FlexibleFMM.square_bbox(tgs === nothing ? pts : vcat(pts, tgs)))
     f = FMM(StokesHarmonics(Stokeslet3D(); p=p), pts; ppl, bbox)
-    return StokesFMMPlan(f, FMMState(f), pts)
+    return StokesFMMPlan(f, FMMState(f), pts, tgs)
 end
 
 # fmmb_stokes_densities
@@ -320,37 +322,69 @@ function _dcollect(a::AbstractVector, n, name)
     return collect(a)
 end
 
-"""
-    stokes_fmm_eval!(out, plan; stokeslets=nothing, stresslets=nothing, stressvecs=nothing,
-                     doublets=nothing, weights=nothing, output=Velocity())  (src/stokes_api.jl:72-123)
-
-Velocities (`Vector{SVector{3,Float64}}`) or, with `output=Pressure()`, pressures (`Vector{Float64}`)
-at the plan's sources, the i = j term skipped. Stokeslets, stresslet strengths with their stressvecs,
-and doublets are `SVector{3,Float64}` per source; weights multiply the stokeslets, the stresslet
-strengths and the doublets.
-"""
-function stokes_fmm_eval!(out::AbstractVector, plan::StokesFMMPlan; stokeslets=nothing, stresslets=nothing,
-                          stressvecs=nothing, doublets=nothing, weights=nothing, output=Potential())
+function _stokes_call!(out_src, out_trg, plan::StokesFMMPlan, tg, stokeslets, stresslets, stressvecs, doublets,
+                       weights, output)
     n = length(plan.sources)
     (stresslets === nothing) == (stressvecs === nothing) ||
         throw(ArgumentError("stresslets and stressvecs must be given together"))
     (stokeslets !== nothing || stresslets !== nothing || doublets !== nothing) ||
         throw(ArgumentError("provide at least one of stokeslets, stresslets, doublets"))
-    length(out) == n || throw(DimensionMismatch("expected $n outputs"))
     pres = output isa Pressure
     pres || output isa Potential || throw(ArgumentError("Stokes outputs are Velocity() and Pressure()"))
+    out_src === nothing || length(out_src) == n || throw(DimensionMismatch("expected $n outputs at the sources"))
+    nt = tg === nothing ? 0 : length(tg)
+    out_trg === nothing || length(out_trg) == nt || throw(DimensionMismatch("expected $nt outputs at the targets"))
     arrs = (_dcollect(stokeslets, n, "stokeslets"), _dcollect(stresslets, n, "stresslets"),
             _dcollect(stressvecs, n, "stressvecs"), _dcollect(doublets, n, "doublets"),
             _dcollect(weights, n, "weights"))
-    res = pres ? Vector{Float64}(undef, n) : Vector{SVector{3,Float64}}(undef, n)
-    GC.@preserve arrs begin
+    T = pres ? Float64 : SVector{3,Float64}
+    rs = out_src === nothing ? nothing : Vector{T}(undef, n)
+    rt = out_trg === nothing ? nothing : Vector{T}(undef, nt)
+    tgv = tg === nothing ? nothing : collect(SVector{3,Float64}, tg)
+    GC.@preserve arrs rs rt tgv begin
         d = Ref(StokesDensitiesC(map(_dptr, arrs)...))
-        check(ccall((:fmmb_stokes_eval_densities, libfmmb), Cint,
-                    (Ptr{Cvoid}, Ptr{SVector{3,Float64}}, Ref{StokesDensitiesC}, Int64, Cint, Ptr{Cvoid}),
-                    plan.state.h, plan.sources, d, n, pres ? Cint(1) : Cint(0), res))
+        check(ccall((:fmmb_stokes_eval_src_trg, libfmmb), Cint,
+                    (Ptr{Cvoid}, Ptr{SVector{3,Float64}}, Ref{StokesDensitiesC}, Int64, Ptr{Cvoid}, Int64, Cint,
+                     Ptr{Cvoid}, Ptr{Cvoid}),
+                    plan.state.h, plan.sources, d, n, _dptr(tgv), nt, pres ? Cint(1) : Cint(0), _dptr(rs), _dptr(rt)))
     end
-    copyto!(out, res)
+    out_src === nothing || copyto!(out_src, rs)
+    out_trg === nothing || copyto!(out_trg, rt)
+    return nothing
+end
+
+"""
+    stokes_fmm_eval!(out, plan; stokeslets=nothing, stresslets=nothing, stressvecs=nothing,
+                     doublets=nothing, weights=nothing, targets=nothing, output=Velocity())  (src/stokes_api.jl:72-123)
+
+Velocities (`Vector{SVector{3,Float64}}`) or, with `output=Pressure()`, pressures (`Vector{Float64}`)
+at the plan's targets (or `targets`), or at the sources of a self plan with the i = j term skipped.
+Stokeslets, stresslet strengths with their stressvecs, and doublets are `SVector{3,Float64}` per
+source; weights multiply the stokeslets, the stresslet strengths and the doublets.
+"""
+function stokes_fmm_eval!(out::AbstractVector, plan::StokesFMMPlan; stokeslets=nothing, stresslets=nothing,
+                          stressvecs=nothing, doublets=nothing, weights=nothing, targets=nothing, output=Potential())
+    tg = targets === nothing ? plan.targets : targets
+    if tg === nothing
+        _stokes_call!(out, nothing, plan, nothing, stokeslets, stresslets, stressvecs, doublets, weights, output)
+    else
+        _stokes_call!(nothing, out, plan, tg, stokeslets, stresslets, stressvecs, doublets, weights, output)
+    end
     return out
+end
+
+"""
+    stokes_fmm_eval_src_trg!(out_src, out_trg, plan; ...)  (src/stokes_api.jl:125-146)
+
+One expansion build, two evaluations: at the sources (i = j skipped) and at the plan's targets.
+"""
+function stokes_fmm_eval_src_trg!(out_src::AbstractVector, out_trg::AbstractVector, plan::StokesFMMPlan;
+                                  stokeslets=nothing, stresslets=nothing, stressvecs=nothing, doublets=nothing,
+                                  weights=nothing, targets=nothing, output=Potential())
+    tg = targets === nothing ? plan.targets : targets
+    tg === nothing && throw(ArgumentError("the plan has no targets"))
+    _stokes_call!(out_src, out_trg, plan, tg, stokeslets, stresslets, stressvecs, doublets, weights, output)
+    return out_src, out_trg
 end
 
 end # module

@@ -190,6 +190,16 @@ int fmmb_stokes_eval_densities(fmmb_state* state, const double* xyz, const fmmb_
 int fmmb_stokes_eval_densities_dev(fmmb_state* state, const double* xyz_dev, const fmmb_stokes_densities* dens,
                                    int64_t n, int output, double* out_dev);
 
+/* stokes_fmm_eval! with a plan that has targets, and stokes_fmm_eval_src_trg! (src/stokes_api.jl:
+ * 107-146): one build_expansions!, then the outputs at the sources (out_src, i = j skipped; NULL to
+ * skip) and at nt targets (3×nt, inside the plan's box, else ArgumentError; out_trg, NULL to
+ * skip), velocities 3 per point or pressures 1 per point, in the original orders. */
+int fmmb_stokes_eval_src_trg(fmmb_state* state, const double* xyz, const fmmb_stokes_densities* dens, int64_t n,
+                             const double* targets, int64_t nt, int output, double* out_src, double* out_trg);
+int fmmb_stokes_eval_src_trg_dev(fmmb_state* state, const double* xyz_dev, const fmmb_stokes_densities* dens,
+                                 int64_t n, const double* targets_dev, int64_t nt, int output, double* out_src_dev,
+                                 double* out_trg_dev);
+
 /* direct!(out, K, sources, τ, targets) / direct_self! (src/kernels.jl:463-487) for Laplace3D on
  * the device in FP64, device pointers: sources 3×ns, targets 3×nt. self_index (device, may be
  * NULL): per target, the source index it excludes (-1 for none). */

@@ -180,8 +180,9 @@ def stokes_direct(src, f, sel):
     return out
 
 
-def stokes_direct_all(src, sel, f=None, fs=None, nu=None, g=None, w=None, output="velocity"):
-    """FP64 direct sums at the sources `sel` (i = j skipped) of weighted Stokeslets f, stresslets
+def stokes_direct_all(src, sel, f=None, fs=None, nu=None, g=None, w=None, output="velocity", tgt=None):
+    """FP64 direct sums at the sources `sel` (i = j skipped), or at the points `tgt` (sel None),
+    of weighted Stokeslets f, stresslets
     (fs, ν) and doublets g (src/sources.jl:203-251, c = 1/8π, d = t − s): velocities
     c[f/r + d(d·f)/r³] − 6c d(d·f_s)(d·ν)/r⁵ + c(g/r³ − 3d(d·g)/r⁵), or pressures
     2c(d·f)/r³ + 4c[(f_s·ν)/r³ − 3(d·f_s)(d·ν)/r⁵]."""
@@ -193,12 +194,17 @@ def stokes_direct_all(src, sel, f=None, fs=None, nu=None, g=None, w=None, output
     nu = z if nu is None else nu
     g = z if g is None else g * wt[:, None]
     c = 1 / (8 * np.pi)
-    out = np.zeros((len(sel), 3) if output == "velocity" else len(sel))
-    for a in range(0, len(sel), 64):
-        idx = sel[a:a + 64]
-        d = src[idx, None, :] - src[None, :, :]
-        r2 = np.einsum("tsk,tsk->ts", d, d)
-        r2[np.arange(len(idx)), idx] = np.inf
+    m = len(sel) if tgt is None else len(tgt)
+    out = np.zeros((m, 3) if output == "velocity" else m)
+    for a in range(0, m, 64):
+        if tgt is None:
+            idx = sel[a:a + 64]
+            d = src[idx, None, :] - src[None, :, :]
+            r2 = np.einsum("tsk,tsk->ts", d, d)
+            r2[np.arange(len(idx)), idx] = np.inf
+        else:
+            d = tgt[a:a + 64, None, :] - src[None, :, :]
+            r2 = np.einsum("tsk,tsk->ts", d, d)
         ir = 1.0 / np.sqrt(r2)
         ir3, ir5 = ir ** 3, ir ** 5
         df = np.einsum("tsk,sk->ts", d, f)

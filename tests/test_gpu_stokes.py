@@ -174,3 +174,49 @@ def test_density_errors(fmmb):
         fmmb.stokes_fmm_eval(plan)
     with pytest.raises(fmmb.Unsupported):
         fmmb.stokes_fmm_eval(plan, stokeslets=np.ones((2000, 3)), output="gradient")
+
+
+# ---------------------------------------------------------------- targets
+@pytest.mark.parametrize("dist", ["uniform", "helix"])
+def test_stokes_at_targets(fmmb, dist):
+    """test/test_harmonics_stokes.jl:48-60 at targets: a plan with targets (its box covers both),
+    Stokeslets within 1e-5 and mixed densities within 1e-4 (velocity) / 1e-3 (pressure) max-norm
+    relative of direct sums at 400 uniform targets; stokes_fmm_eval_src_trg gives the same values
+    at the sources and at the targets as the two separate evaluations."""
+    rng = np.random.default_rng(16)
+    n = 5000
+    if dist == "uniform":
+        pts = rng.random((n, 3))
+    else:
+        t = np.sort(rng.random(n)) * 6 * np.pi
+        pts = np.stack([0.5 + 0.3 * np.cos(t), 0.5 + 0.3 * np.sin(t), 0.1 + 0.8 * t / t[-1]], axis=1)
+    tg = rng.random((400, 3)) * 1.2 - 0.1                     # some outside the sources' cube
+    d = _mixed(rng, n)
+    plan = fmmb.StokesFMMPlan(pts, targets=tg, p=16, ppl=40)
+    f = {"stokeslets": d["stokeslets"]}
+    ref = stokes_direct_all(pts, None, f=d["stokeslets"], tgt=tg)
+    assert mrd(fmmb.stokes_fmm_eval(plan, **f), ref) < 1e-5
+    for output, tol in (("velocity", 1e-4), ("pressure", 1e-3)):
+        u = fmmb.stokes_fmm_eval(plan, output=output, **d)
+        ref = stokes_direct_all(pts, None, f=d["stokeslets"], fs=d["stresslets"], nu=d["stressvecs"],
+                                g=d["doublets"], w=d["weights"], output=output, tgt=tg)
+        assert mrd(u, ref) < tol, (dist, output)
+        us, ut = fmmb.stokes_fmm_eval_src_trg(plan, output=output, **d)
+        assert np.array_equal(ut, u)
+        self_plan = fmmb.StokesFMMPlan(pts, p=16, ppl=40, bbox=fmmb.square_bbox(np.concatenate([pts, tg])))
+        assert np.array_equal(us, fmmb.stokes_fmm_eval(self_plan, output=output, **d))
+
+
+def test_stokes_target_errors(fmmb):
+    rng = np.random.default_rng(17)
+    pts = rng.random((2000, 3))
+    plan = fmmb.StokesFMMPlan(pts, p=8, ppl=64)
+    f = rng.standard_normal((2000, 3))
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.stokes_fmm_eval_src_trg(plan, stokeslets=f)                  # no targets
+    with pytest.raises(fmmb.ArgumentError):
+        fmmb.stokes_fmm_eval(plan, stokeslets=f, targets=np.array([[2.0, 0.5, 0.5]]))   # outside the box
+    tg = pts[:50] * 0.99 + 0.005                                      # near the sources, inside the box
+    u = fmmb.stokes_fmm_eval(plan, stokeslets=f, targets=tg)
+    ref = stokes_direct_all(pts, None, f=f, tgt=tg)
+    assert mrd(u, ref) < 3e-3
