@@ -881,8 +881,8 @@ void check_stokes_call(fmmb_state* state, const double* xyz, const fmmb_stokes_d
           "stresslets and stressvecs must be given together");
   require(dens->stokeslets || dens->stresslets || dens->doublets, FMMB_ERR_ARGUMENT,
           "provide at least one of stokeslets, stresslets, doublets");
-  require(output == FMMB_STOKES_VELOCITY || output == FMMB_STOKES_PRESSURE, FMMB_ERR_UNSUPPORTED,
-          "Stokes outputs are the velocity and the pressure");
+  require(output == FMMB_STOKES_VELOCITY || output == FMMB_STOKES_PRESSURE || output == FMMB_STOKES_GRADIENT,
+          FMMB_ERR_UNSUPPORTED, "Stokes outputs are the velocity, the pressure and the velocity gradient");
   Plan& P = *state->s.plan;
   require(P.cache->kernel == FMMB_KERNEL_STOKESLET3D, FMMB_ERR_UNSUPPORTED, "the state is not a Stokeslet state");
   require(n == P.N, FMMB_ERR_DIMENSION, "expected " + std::to_string(P.N) + " sources and densities");
@@ -930,7 +930,7 @@ int stokes_host(fmmb_state* state, const double* xyz, const fmmb_stokes_densitie
     Plan& P = *S.plan;
     set_device(*P.ctx);
     cudaStream_t s = P.ctx->stream;
-    const int w = output == FMMB_STOKES_PRESSURE ? 1 : 3;
+    const int w = output == FMMB_STOKES_PRESSURE ? 1 : output == FMMB_STOKES_GRADIENT ? 9 : 3;
     const bool trg = out_trg && nt > 0;
     DBuf<double> x(3 * n), os(out_src ? w * n : 0), t(trg ? 3 * nt : 0), ot(trg ? w * nt : 0);
     DBuf<double> a[5];

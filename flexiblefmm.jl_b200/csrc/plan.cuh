@@ -213,7 +213,8 @@ struct StokesDensities {
                *weights = nullptr;
 };
 void stokes_build(State& S, const double* xyz_dev, const StokesDensities& d);
-// output FMMB_STOKES_VELOCITY (3 × n) or FMMB_STOKES_PRESSURE (n), original order, device
+// output FMMB_STOKES_VELOCITY (3 × n), FMMB_STOKES_PRESSURE (n) or FMMB_STOKES_GRADIENT (9 × n),
+// original order, device
 void stokes_evaluate_sources(State& S, int output, double* out_dev);
 // the same at nt targets (device, 3 × nt) inside the tree's box, in the targets' order
 void stokes_evaluate_targets(State& S, const double* tg_dev, int64_t nt, int output, double* out_dev);

@@ -173,15 +173,106 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_l2p(const int* __restrict__ 
   }
 }
 
+// the scaled gradient of a local expansion L of degree P as three expansions of degree P − 1 in
+// the real storage (n², and re/im of order m at n² + 2m − 1, n² + 2m), from the derivative
+// identities (harmonics_stokes.jl:231-240, harmonics.jl:465-486): (D₋L)_n^m = −cm(n+1, m+1) L_{n+1}^{m+1},
+// (D₊L)_n^m = cp(n+1, m−1) L_{n+1}^{m−1}, (D_zL)_n^m = cz(n+1, m) L_{n+1}^m, ∂̂_x = ½(D₋ + D₊),
+// ∂̂_y = (i/2)(D₊ − D₋), ∂̂_z = D_z; the lanes of a warp share the P² entries
+template <int P>
+__device__ void grad_sets(const double* __restrict__ L, double* __restrict__ Ax, double* __restrict__ Ay,
+                          double* __restrict__ Az, int lane) {
+  for (int e = lane; e < P * P; e += 32) {
+    int n = (int)sqrtf((float)e);
+    while (n * n > e) --n;
+    while ((n + 1) * (n + 1) <= e) ++n;
+    const int k = e - n * n, m = (k + 1) / 2, n1 = n + 1, b = n1 * n1;
+    const bool im = k > 0 && (k & 1) == 0;
+    if (m == 0) {
+      const double cmv = c_tab[3 * TRI_MAX + tri(n1, 1)];
+      Ax[e] = -cmv * L[b + 1];
+      Ay[e] = -cmv * L[b + 2];
+      Az[e] = c_tab[2 * TRI_MAX + tri(n1, 0)] * L[b];
+    } else {
+      const double ur = L[b + 2 * (m + 1) - 1], ui = L[b + 2 * (m + 1)];
+      const double dr = m == 1 ? L[b] : L[b + 2 * (m - 1) - 1], di = m == 1 ? 0.0 : L[b + 2 * (m - 1)];
+      const double cu = 0.5 * c_tab[3 * TRI_MAX + tri(n1, m + 1)], cd = 0.5 * c_tab[4 * TRI_MAX + tri(n1, m - 1)];
+      const double czv = c_tab[2 * TRI_MAX + tri(n1, m)];
+      Ax[e] = im ? -cu * ui + cd * di : -cu * ur + cd * dr;
+      Ay[e] = im ? cu * ur + cd * dr : -(cu * ui + cd * di);
+      Az[e] = czv * (im ? L[b + 2 * m] : L[b + 2 * m - 1]);
+    }
+  }
+}
+
+constexpr int GW = 2;   // warps per block of the velocity-gradient L2P
+
+// the far-field velocity gradient at the targets of one leaf (harmonics_stokes.jl:347-350):
+// ∂u_i/∂t_j = (s/2)[∂̂_jΦ_i − ∂̂_iΦ_j − Σ_k x̂_k ∂̂_i∂̂_jΦ_k + ∂̂_i∂̂_jΨ̂], written at 9·o + 3i + j. Per
+// warp the leaf's four blocks and their twelve gradient expansions sit in shared memory; per target
+// twelve degree-(P−1) L2Ps give the first and second derivatives.
+template <int P>
+__global__ void __launch_bounds__(GW * 32) k_stokes_l2p_grad(const int* __restrict__ gnode, const int* __restrict__ gstart,
+                                                             const int* __restrict__ gcount, int ngroups,
+                                                             const double* __restrict__ tx, const double* __restrict__ ty,
+                                                             const double* __restrict__ tz, const int* __restrict__ tout,
+                                                             const int4* __restrict__ cell, const double* __restrict__ Pl,
+                                                             int LD, Geometry geo, const double* __restrict__ scale,
+                                                             double* __restrict__ out) {
+  extern __shared__ double sg[];
+  constexpr int NG = P * P;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x * GW + warp;
+  if (grp >= ngroups) return;
+  double* L = sg + (int64_t)warp * (4 * LD + 12 * NG);
+  double* A = L + 4 * LD;   // block a, direction j at A + (3a + j)·NG
+  const int leaf = gnode[grp];
+  for (int i = lane; i < 4 * LD; i += 32) L[i] = Pl[(int64_t)leaf * 4 * LD + i];
+  __syncwarp();
+  for (int a = 0; a < 4; ++a) grad_sets<P>(L + a * LD, A + 3 * a * NG, A + (3 * a + 1) * NG, A + (3 * a + 2) * NG, lane);
+  __syncwarp();
+  const int4 c = cell[leaf];
+  const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
+  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const int t0 = gstart[grp], nt = gcount[grp];
+  for (int base = 0; base < nt; base += 32) {
+    const int k = t0 + base + lane;
+    const bool act = base + lane < nt;
+    const double xh[3] = {act ? (tx[k] - cx) * s : 0.0, act ? (ty[k] - cy) * s : 0.0, act ? (tz[k] - cz) * s : 0.0};
+    double gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int a = 0; a < 4; ++a) {
+      const double coef = a < 3 ? -xh[a] : 1.0;
+      for (int j = 0; j < 3; ++j) {
+        double v, h[3];
+        l2p<P - 1, double>(A + (3 * a + j) * NG, xh[0], xh[1], xh[2], v, h[0], h[1], h[2]);
+        if (a < 3) {   // v = ∂̂_jΦ_a: +v at (a, j), −v at (j, a)
+          gr[a][j] += v;
+          gr[j][a] -= v;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) gr[i][j] += coef * h[i];   // h_i = ∂̂_i∂̂_j of block a
+      }
+    }
+    if (act) {
+      const int o = tout[k];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) out[9 * (int64_t)o + e] = 0.5 * s * gr[e / 3][e % 3];
+    }
+  }
+}
+
 struct alignas(16) S8 { double x, y, z, fx, fy, fz, pad0, pad1; };
 struct alignas(16) S16 { double x, y, z, fx, fy, fz, sx, sy, sz, nx, ny, nz, gx, gy, gz, pad; };
 
 // the near field: the sources of the 27 colleagues, flattened into batches of 32 staged per warp
-// (the next batch's loads in flight), lanes over the targets; adds c·Σ to the velocities (or with
-// PRES to the pressures). DENS adds the stresslets and doublets of sd (3 × n planar: strengths,
-// stressvecs, doublets) to the Stokeslets:
+// (the next batch's loads in flight), lanes over the targets; adds c·Σ to the velocities (OUT 0),
+// the pressures (OUT 1) or the velocity gradients (OUT 2, ∂u_i/∂t_j at 9·o + 3i + j). DENS adds
+// the stresslets and doublets of sd (3 × n planar: strengths, stressvecs, doublets) to the
+// Stokeslets (src/sources.jl:203-281):
 //   u = c[f/r + g/r³ + d((d·f)/r³ − 3(d·g)/r⁵ − 6(d·f_s)(d·ν)/r⁵)],  p = c[2(d·f)/r³ + 4(f_s·ν)/r³ − 12(d·f_s)(d·ν)/r⁵]
-template <bool SELF, bool DENS, bool PRES>
+//   ∂u_i/∂t_j = c[d_i(A d_j + v_j) + w_i d_j + B δ_ij] with A = −3(d·f)/r⁵ + (30(d·f_s)(d·ν) + 15(d·g))/r⁷,
+//   B = (d·f)/r³ − (6(d·f_s)(d·ν) + 3(d·g))/r⁵, v = f/r³ − 6((d·ν) f_s + (d·f_s) ν)/r⁵ − 3g/r⁵,
+//   w = −f/r³ − 3g/r⁵ (the closed forms of the three gradients, summed)
+template <bool SELF, bool DENS, int OUT>
 __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
                                                          const int* __restrict__ gcount, int ngroups,
                                                          const double* __restrict__ tx, const double* __restrict__ ty,
@@ -242,6 +333,7 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__
     const double x = act ? tx[k] : 0.0, y = act ? ty[k] : 0.0, z = act ? tz[k] : 0.0;
     const int fself = SELF && act && selfm ? pself + (k - loself) : -1;
     double ux = 0, uy = 0, uz = 0;
+    double gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     SV nxt;
     load(0, nxt);
     for (int b = 0; 32 * b < S; ++b) {
@@ -260,10 +352,32 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__
         if (chk && i == is) ir = 0.0;
         const double ir3 = ir * ir * ir;
         const double df = dx * sv.fx + dy * sv.fy + dz * sv.fz;
-        if constexpr (DENS) {
+        if constexpr (OUT == 2) {
+          const double ir2 = ir * ir, ir5 = ir3 * ir2;
+          const double d[3] = {dx, dy, dz};
+          double A = -3.0 * df * ir5, B = df * ir3;
+          double v[3] = {sv.fx * ir3, sv.fy * ir3, sv.fz * ir3}, w[3] = {-v[0], -v[1], -v[2]};
+          if constexpr (DENS) {
+            const double ds = dx * sv.sx + dy * sv.sy + dz * sv.sz, dn = dx * sv.nx + dy * sv.ny + dz * sv.nz;
+            const double dg = dx * sv.gx + dy * sv.gy + dz * sv.gz;
+            A += (30.0 * ds * dn + 15.0 * dg) * ir5 * ir2;
+            B -= (6.0 * ds * dn + 3.0 * dg) * ir5;
+            const double fs[3] = {sv.sx, sv.sy, sv.sz}, nu[3] = {sv.nx, sv.ny, sv.nz}, g[3] = {sv.gx, sv.gy, sv.gz};
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+              v[e] -= (6.0 * (dn * fs[e] + ds * nu[e]) + 3.0 * g[e]) * ir5;
+              w[e] -= 3.0 * g[e] * ir5;
+            }
+          }
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int b = 0; b < 3; ++b) gr[a][b] += d[a] * (A * d[b] + v[b]) + w[a] * d[b] + (a == b ? B : 0.0);
+          }
+        } else if constexpr (DENS) {
           const double ir5 = ir3 * ir * ir;
           const double ds = dx * sv.sx + dy * sv.sy + dz * sv.sz, dn = dx * sv.nx + dy * sv.ny + dz * sv.nz;
-          if constexpr (PRES) {
+          if constexpr (OUT == 1) {
             const double sn = sv.sx * sv.nx + sv.sy * sv.ny + sv.sz * sv.nz;
             ux += 2.0 * df * ir3 + 4.0 * sn * ir3 - 12.0 * ds * dn * ir5;
           } else {
@@ -273,7 +387,7 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__
             uy += sv.fy * ir + sv.gy * ir3 + dy * c;
             uz += sv.fz * ir + sv.gz * ir3 + dz * c;
           }
-        } else if constexpr (PRES) {
+        } else if constexpr (OUT == 1) {
           ux += 2.0 * df * ir3;
         } else {
           const double c = df * ir3;
@@ -285,7 +399,10 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__
     }
     if (act) {
       const int o = tout[k];
-      if (PRES) {
+      if (OUT == 2) {
+#pragma unroll
+        for (int e = 0; e < 9; ++e) out[9 * (int64_t)o + e] += KSTOKES * gr[e / 3][e % 3];
+      } else if (OUT == 1) {
         out[o] += KSTOKES * ux;
       } else {
         out[3 * (int64_t)o] += KSTOKES * ux;
@@ -299,9 +416,18 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_near(const int* __restrict__
 
 template <int P>
 void launch_stokes_l2p(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
-                       const double* ty, const double* tz, const int* tout, bool pres, double* out) {
+                       const double* ty, const double* tz, const int* tout, int output, double* out) {
   Plan& P_ = *S.plan;
   const int LD = P_.cache->ld;
+  if (output == FMMB_STOKES_GRADIENT) {
+    const size_t smem = sizeof(double) * GW * (4 * LD + 12 * P * P);
+    FMMB_CUDA(cudaFuncSetAttribute(k_stokes_l2p_grad<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_stokes_l2p_grad<P><<<(ng + GW - 1) / GW, GW * 32, smem, P_.ctx->stream>>>(
+        gnode, gstart, gcount, ng, tx, ty, tz, tout, P_.cell.p, S.Pl.p, LD, geometry(P_), P_.d_scale.p, out);
+    FMMB_LAUNCH_CHECK();
+    return;
+  }
+  const bool pres = output == FMMB_STOKES_PRESSURE;
   const size_t smem = sizeof(double) * SW * 4 * LD;
   auto kern = pres ? k_stokes_l2p<P, true> : k_stokes_l2p<P, false>;
   FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -376,21 +502,22 @@ namespace {
 void stokes_evaluate_groups(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx,
                             const double* ty, const double* tz, const int* tout, bool self, int output, double* out) {
   Plan& P = *S.plan;
-  const bool pres = output == FMMB_STOKES_PRESSURE;
-  require(output == FMMB_STOKES_VELOCITY || pres, FMMB_ERR_UNSUPPORTED,
-          "Stokes outputs are the velocity and the pressure");
+  require(output == FMMB_STOKES_VELOCITY || output == FMMB_STOKES_PRESSURE || output == FMMB_STOKES_GRADIENT,
+          FMMB_ERR_UNSUPPORTED, "Stokes outputs are the velocity, the pressure and the velocity gradient");
   if (ng == 0) return;
   switch (P.cache->p) {
-#define X(pp) case pp: launch_stokes_l2p<pp>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, pres, out); break;
+#define X(pp) case pp: launch_stokes_l2p<pp>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, output, out); break;
     FMMB_P_CASES(X)
 #undef X
     default: throw Error(FMMB_ERR_UNSUPPORTED, "p out of range");
   }
   const bool d = S.stokes_dens;
-  auto kern = self ? (d ? (pres ? k_stokes_near<true, true, true> : k_stokes_near<true, true, false>)
-                        : (pres ? k_stokes_near<true, false, true> : k_stokes_near<true, false, false>))
-                   : (d ? (pres ? k_stokes_near<false, true, true> : k_stokes_near<false, true, false>)
-                        : (pres ? k_stokes_near<false, false, true> : k_stokes_near<false, false, false>));
+  using K = decltype(&k_stokes_near<true, true, 0>);
+  const K table[2][2][3] = {{{k_stokes_near<false, false, 0>, k_stokes_near<false, false, 1>, k_stokes_near<false, false, 2>},
+                             {k_stokes_near<false, true, 0>, k_stokes_near<false, true, 1>, k_stokes_near<false, true, 2>}},
+                            {{k_stokes_near<true, false, 0>, k_stokes_near<true, false, 1>, k_stokes_near<true, false, 2>},
+                             {k_stokes_near<true, true, 0>, k_stokes_near<true, true, 1>, k_stokes_near<true, true, 2>}}};
+  const K kern = table[self][d][output];
   kern<<<(ng + SW - 1) / SW, SW * 32, 0, P.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p,
                                                           S.zs.p, S.f3.p, d ? S.sd.p : nullptr, P.N, P.plo.p, P.phi.p,
                                                           P.col.p, out);

@@ -224,8 +224,8 @@ class Stokeslet3D:
 
 class StokesHarmonics:
     """StokesHarmonics(Stokeslet3D(); p=16) (src/operators/harmonics_stokes.jl:34-45): four
-    solid-harmonic expansions per box; Stokeslet, stresslet and doublet densities, velocity and
-    pressure outputs, FP64 path."""
+    solid-harmonic expansions per box; Stokeslet, stresslet and doublet densities, velocity,
+    pressure and velocity-gradient outputs, FP64 path."""
 
     def __init__(self, kernel, p=16, tol=0.0):
         if not isinstance(kernel, Stokeslet3D):
@@ -717,6 +717,7 @@ class StokesFMMPlan:
 
 STOKES_VELOCITY = 0
 STOKES_PRESSURE = 1
+STOKES_GRADIENT = 2
 
 
 def stokes_densities(n, weights=None, stokeslets=None, stresslets=None, stressvecs=None, doublets=None):
@@ -746,12 +747,12 @@ def stokes_densities(n, weights=None, stokeslets=None, stresslets=None, stressve
 def _stokes_call(plan, sources, targets, at_sources, output, dens):
     x = plan.sources if sources is None else _points(sources)
     n = x.shape[0]
-    outs = {"velocity": STOKES_VELOCITY, "pressure": STOKES_PRESSURE}
+    outs = {"velocity": STOKES_VELOCITY, "pressure": STOKES_PRESSURE, "gradient": STOKES_GRADIENT}
     if output not in outs:
-        raise Unsupported(6, "Stokes outputs are 'velocity' and 'pressure'")
+        raise Unsupported(6, "Stokes outputs are 'velocity', 'pressure' and 'gradient'")
     arrs = stokes_densities(n, **dens)
     tg = plan.targets if targets is None else _points(targets)
-    shape = (lambda m: (m, 3)) if output == "velocity" else (lambda m: (m,))
+    shape = {"velocity": lambda m: (m, 3), "pressure": lambda m: (m,), "gradient": lambda m: (m, 3, 3)}[output]
     src = np.zeros(shape(n)) if at_sources else None
     trg = None if tg is None else np.zeros(shape(tg.shape[0]))
     if src is not None and trg is None and arrs[1] is None and arrs[3] is None and arrs[4] is None \
@@ -767,9 +768,10 @@ def _stokes_call(plan, sources, targets, at_sources, output, dens):
 def stokes_fmm_eval(plan, stokeslets=None, sources=None, stresslets=None, stressvecs=None, doublets=None,
                     weights=None, targets=None, output="velocity"):
     """stokes_fmm_eval!(out, plan; stokeslets, stresslets, stressvecs, doublets, weights, sources,
-    targets, output) (src/stokes_api.jl:107-123): the velocities ((M, 3), output="velocity") or
-    pressures ((M,), output="pressure") at the plan's targets (or `targets`, inside the plan's
-    box), or at the sources of a self plan with the i = j term skipped. Stokeslets, stresslet
+    targets, output) (src/stokes_api.jl:107-123): the velocities ((M, 3), output="velocity"),
+    pressures ((M,), output="pressure") or velocity gradients ((M, 3, 3), [k, i, j] = ∂u_i/∂t_j,
+    output="gradient") at the plan's targets (or `targets`, inside the plan's box), or at the
+    sources of a self plan with the i = j term skipped. Stokeslets, stresslet
     strengths with their stressvecs, and doublets are (N, 3); weights (N,) multiply the
     stokeslets, stresslet strengths and doublets."""
     dens = dict(weights=weights, stokeslets=stokeslets, stresslets=stresslets, stressvecs=stressvecs,

@@ -15,7 +15,7 @@ module FlexibleFMMB200
 
 using FlexibleFMM: FlexibleFMM, SphericalHarmonics, StokesHarmonics, CubeKernelIndependent, KernelIndependent,
     Laplace3D, Laplace2D, Yukawa3D, Stokeslet3D, Potential, Gradient, Pressure, Dipole
-using StaticArrays: SVector
+using StaticArrays: SVector, SMatrix
 
 const libfmmb = get(ENV, "FMMB_LIB", joinpath(@__DIR__, "..", "libfmmb.so"))
 
@@ -329,15 +329,16 @@ function _stokes_call!(out_src, out_trg, plan::StokesFMMPlan, tg, stokeslets, st
         throw(ArgumentError("stresslets and stressvecs must be given together"))
     (stokeslets !== nothing || stresslets !== nothing || doublets !== nothing) ||
         throw(ArgumentError("provide at least one of stokeslets, stresslets, doublets"))
-    pres = output isa Pressure
-    pres || output isa Potential || throw(ArgumentError("Stokes outputs are Velocity() and Pressure()"))
+    code = output isa Pressure ? Cint(1) : output isa Gradient ? Cint(2) : output isa Potential ? Cint(0) :
+        throw(ArgumentError("Stokes outputs are Velocity(), Pressure() and Gradient()"))
     out_src === nothing || length(out_src) == n || throw(DimensionMismatch("expected $n outputs at the sources"))
     nt = tg === nothing ? 0 : length(tg)
     out_trg === nothing || length(out_trg) == nt || throw(DimensionMismatch("expected $nt outputs at the targets"))
     arrs = (_dcollect(stokeslets, n, "stokeslets"), _dcollect(stresslets, n, "stresslets"),
             _dcollect(stressvecs, n, "stressvecs"), _dcollect(doublets, n, "doublets"),
             _dcollect(weights, n, "weights"))
-    T = pres ? Float64 : SVector{3,Float64}
+    # the library writes ∂u_i/∂t_j at 9k + 3i + j: read as an SMatrix that is the transpose
+    T = code == 1 ? Float64 : code == 2 ? SMatrix{3,3,Float64,9} : SVector{3,Float64}
     rs = out_src === nothing ? nothing : Vector{T}(undef, n)
     rt = out_trg === nothing ? nothing : Vector{T}(undef, nt)
     tgv = tg === nothing ? nothing : collect(SVector{3,Float64}, tg)
@@ -346,10 +347,11 @@ function _stokes_call!(out_src, out_trg, plan::StokesFMMPlan, tg, stokeslets, st
         check(ccall((:fmmb_stokes_eval_src_trg, libfmmb), Cint,
                     (Ptr{Cvoid}, Ptr{SVector{3,Float64}}, Ref{StokesDensitiesC}, Int64, Ptr{Cvoid}, Int64, Cint,
                      Ptr{Cvoid}, Ptr{Cvoid}),
-                    plan.state.h, plan.sources, d, n, _dptr(tgv), nt, pres ? Cint(1) : Cint(0), _dptr(rs), _dptr(rt)))
+                    plan.state.h, plan.sources, d, n, _dptr(tgv), nt, code, _dptr(rs), _dptr(rt)))
     end
-    out_src === nothing || copyto!(out_src, rs)
-    out_trg === nothing || copyto!(out_trg, rt)
+    fix(r) = code == 2 ? map(transpose, r) : r
+    out_src === nothing || copyto!(out_src, fix(rs))
+    out_trg === nothing || copyto!(out_trg, fix(rt))
     return nothing
 end
 
@@ -357,7 +359,8 @@ end
     stokes_fmm_eval!(out, plan; stokeslets=nothing, stresslets=nothing, stressvecs=nothing,
                      doublets=nothing, weights=nothing, targets=nothing, output=Velocity())  (src/stokes_api.jl:72-123)
 
-Velocities (`Vector{SVector{3,Float64}}`) or, with `output=Pressure()`, pressures (`Vector{Float64}`)
+Velocities (`Vector{SVector{3,Float64}}`), with `output=Pressure()` pressures (`Vector{Float64}`), or
+with `output=Gradient()` velocity gradients (`Vector{SMatrix{3,3,Float64,9}}`, [i, j] = ∂u_i/∂t_j)
 at the plan's targets (or `targets`), or at the sources of a self plan with the i = j term skipped.
 Stokeslets, stresslet strengths with their stressvecs, and doublets are `SVector{3,Float64}` per
 source; weights multiply the stokeslets, the stresslet strengths and the doublets.

@@ -179,6 +179,7 @@ typedef struct fmmb_stokes_densities {
 
 #define FMMB_STOKES_VELOCITY 0 /* Velocity(): 3×n out */
 #define FMMB_STOKES_PRESSURE 1 /* Pressure(): n out */
+#define FMMB_STOKES_GRADIENT 2 /* Gradient(): 9×n out, ∂u_i/∂t_j at 9·k + 3·i + j (row-major per point) */
 
 /* stokes_fmm_eval!(out, plan; stokeslets, stresslets, stressvecs, doublets, weights, output) with
  * a self plan (src/stokes_api.jl:107-123) on a Stokeslet state: the velocities or pressures at the

@@ -195,7 +195,7 @@ def stokes_direct_all(src, sel, f=None, fs=None, nu=None, g=None, w=None, output
     g = z if g is None else g * wt[:, None]
     c = 1 / (8 * np.pi)
     m = len(sel) if tgt is None else len(tgt)
-    out = np.zeros((m, 3) if output == "velocity" else m)
+    out = np.zeros({"velocity": (m, 3), "pressure": (m,), "gradient": (m, 3, 3)}[output])
     for a in range(0, m, 64):
         if tgt is None:
             idx = sel[a:a + 64]
@@ -214,6 +214,22 @@ def stokes_direct_all(src, sel, f=None, fs=None, nu=None, g=None, w=None, output
             dg = np.einsum("tsk,sk->ts", d, g)
             coef = df * ir3 - (3 * dg + 6 * ds * dn) * ir5
             out[a:a + 64] = c * (ir @ f + ir3 @ g + np.einsum("ts,tsk->tk", coef, d))
+        elif output == "gradient":
+            # ∂u_i/∂t_j of each kind in closed form (src/sources.jl:242-276), summed
+            dg = np.einsum("tsk,sk->ts", d, g)
+            ir7 = ir5 * ir * ir
+            eye = np.eye(3)
+            ddt = np.einsum("tsi,tsj->tsij", d, d)
+            gr = np.einsum("ts,tsij->tij", ir3 * df, eye[None, None] * np.ones_like(ir)[..., None, None])
+            gr += np.einsum("ts,tsi,sj->tij", ir3, d, f) - np.einsum("ts,si,tsj->tij", ir3, f, d)
+            gr -= np.einsum("ts,tsij->tij", 3 * ir5 * df, ddt)
+            gr -= np.einsum("ts,ij->tij", 6 * ir5 * ds * dn, eye)
+            gr -= np.einsum("ts,tsi,sj->tij", 6 * ir5 * dn, d, fs) + np.einsum("ts,tsi,sj->tij", 6 * ir5 * ds, d, nu)
+            gr += np.einsum("ts,tsij->tij", 30 * ir7 * ds * dn, ddt)
+            gr -= np.einsum("ts,si,tsj->tij", 3 * ir5, g, d) + np.einsum("ts,ij->tij", 3 * ir5 * dg, eye)
+            gr -= np.einsum("ts,tsi,sj->tij", 3 * ir5, d, g)
+            gr += np.einsum("ts,tsij->tij", 15 * ir7 * dg, ddt)
+            out[a:a + 64] = c * gr
         else:
             sn = np.einsum("sk,sk->s", fs, nu)
             out[a:a + 64] = c * np.sum(2 * df * ir3 + 4 * sn[None, :] * ir3 - 12 * ds * dn * ir5, axis=1)

@@ -107,7 +107,7 @@ def test_single_leaf_densities_are_the_direct_sum(fmmb):
     pts = rng.random((150, 3))
     d = _mixed(rng, 150)
     plan = fmmb.StokesFMMPlan(pts, p=6, ppl=200)
-    for output in ("velocity", "pressure"):
+    for output in ("velocity", "pressure", "gradient"):
         u = fmmb.stokes_fmm_eval(plan, output=output, **d)
         assert rel_l2(u, _direct(pts, np.arange(150), d, output)) < 1e-13, output
 
@@ -173,7 +173,7 @@ def test_density_errors(fmmb):
     with pytest.raises(fmmb.ArgumentError):
         fmmb.stokes_fmm_eval(plan)
     with pytest.raises(fmmb.Unsupported):
-        fmmb.stokes_fmm_eval(plan, stokeslets=np.ones((2000, 3)), output="gradient")
+        fmmb.stokes_fmm_eval(plan, stokeslets=np.ones((2000, 3)), output="hessian")
 
 
 # ---------------------------------------------------------------- targets
@@ -220,3 +220,31 @@ def test_stokes_target_errors(fmmb):
     u = fmmb.stokes_fmm_eval(plan, stokeslets=f, targets=tg)
     ref = stokes_direct_all(pts, None, f=f, tgt=tg)
     assert mrd(u, ref) < 3e-3
+
+
+@pytest.mark.parametrize("dist", ["uniform", "sphere"])
+def test_velocity_gradient(fmmb, dist):
+    """test/test_harmonics_stokes.jl:48-60's Gradient() bars (10·tol: 1e-4 for Stokeslets, 1e-3
+    for mixed densities, max-norm relative of the 3 × 3 matrices) at the sources and at targets,
+    p = 16; the far-field gradient is the Hessians of the four local blocks (degree-(p−1) L2Ps of
+    their gradient expansions). The trace of a Stokeslet velocity gradient vanishes (∇·u = 0)."""
+    rng = np.random.default_rng(18)
+    n = 20000
+    pts = rng.random((n, 3)) if dist == "uniform" else sphere_points(rng, n)
+    tg = rng.random((300, 3))
+    d = _mixed(rng, n)
+    plan = fmmb.StokesFMMPlan(pts, targets=tg, p=16, ppl=40)
+    sel = np.sort(rng.choice(n, 200, replace=False))
+    f = {"stokeslets": d["stokeslets"]}
+    for dens, tol in ((f, 1e-4), (d, 1e-3)):
+        gs, gt = fmmb.stokes_fmm_eval_src_trg(plan, output="gradient", **dens)
+        kw = dict(f=dens.get("stokeslets"), fs=dens.get("stresslets"), nu=dens.get("stressvecs"),
+                  g=dens.get("doublets"), w=dens.get("weights"), output="gradient")
+        es = np.max(np.linalg.norm(gs[sel] - stokes_direct_all(pts, sel, **kw), axis=(1, 2)))
+        rs = np.max(np.linalg.norm(stokes_direct_all(pts, sel, **kw), axis=(1, 2)))
+        ref_t = stokes_direct_all(pts, None, tgt=tg, **kw)
+        et = np.max(np.linalg.norm(gt - ref_t, axis=(1, 2))) / np.max(np.linalg.norm(ref_t, axis=(1, 2)))
+        assert es / rs < tol and et < tol, (dist, list(dens), es / rs, et)
+        if dens is f:
+            tr = np.abs(np.trace(gt, axis1=1, axis2=2))
+            assert np.max(tr) < 1e-4 * np.max(np.linalg.norm(gt, axis=(1, 2)))
