@@ -80,9 +80,9 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo) {
   return d;                                             // base offset 0, no swizzle
 }
 
-// instruction descriptor: D f32, A/B f16, both K-major, M = 128, N = n
-__device__ __forceinline__ uint32_t instr_desc(int n) {
-  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+// instruction descriptor: D f32, A/B f16, both K-major, M = m (128 or 64), N = n
+__device__ __forceinline__ uint32_t instr_desc(int n, int m = 128) {
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
@@ -526,7 +526,9 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         if (i >= G::STAGES && !mbar_wait_abortable(&tempty[s], ph ^ 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
         const int nn = (pinfo[s].n + 15) & ~15;
-        const uint32_t id = instr_desc(nn);
+        // the second tile holds rows 128..(p+1)²-1 (16 at p = 11): M = 64 halves its tensor time;
+        // its rows 0-15 sit in lanes 0-15 of the first lane quadrant, as with M = 128
+        const uint32_t id = instr_desc(nn), id1 = instr_desc(nn, 64);
         const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB + s * G::STAGE_BYTES);
 #pragma unroll 2
         for (int ks = 0; ks < KP / 16; ++ks) {
@@ -537,9 +539,10 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
             const uint32_t ah = a_base + (uint32_t)(t * 16 * G::SBO) + ko;
             const uint64_t dah = umma_desc(ah, G::SBO), dal = umma_desc(ah + (uint32_t)lo_off, G::SBO);
             const uint32_t td = tmem + (uint32_t)((s * MT + t) * NCHK);
-            mma_f16(td, dah, dbh, id, ks > 0 ? 1u : 0u);
-            mma_f16(td, dah, dbl, id, 1u);
-            mma_f16(td, dal, dbh, id, 1u);
+            const uint32_t it = t == 0 ? id : id1;
+            mma_f16(td, dah, dbh, it, ks > 0 ? 1u : 0u);
+            mma_f16(td, dah, dbl, it, 1u);
+            mma_f16(td, dal, dbh, it, 1u);
           }
         }
         mma_commit(&done[s]);
