@@ -8,6 +8,7 @@
 // targets grouped by symmetry class, and inside a class by target, then by the enumeration
 // order. A block is the unit of the M2L kernels: it owns its targets' partial locals, so
 // the scatter is deterministic and needs no atomics, and one launch covers all levels.
+#include <algorithm>
 #include <numeric>
 
 #include "plan.cuh"
@@ -196,8 +197,19 @@ void build_lists(Plan& P) {
   require(base < (1ll << 31), FMMB_ERR_ARGUMENT, "too many far pairs for 32-bit offsets");
   P.npairs = base;
   int nb = (int)P.h_blocks.size();
+  // the M2L kernels take the blocks in launch order heaviest first (most far pairs): the CTA
+  // scheduler hands out blocks in index order, so the light ones fill the last wave (longest
+  // processing time first); every block owns its targets, so the order changes no sum
+  std::vector<int64_t> bp(nb);
+  for (int b = 0; b < nb; ++b) bp[b] = (b + 1 < nb ? P.h_blocks[b + 1].pair_base : base) - P.h_blocks[b].pair_base;
+  std::vector<int> order(nb);
+  for (int b = 0; b < nb; ++b) order[b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return bp[a] > bp[b]; });
   std::vector<int4> hb(nb);
-  for (int b = 0; b < nb; ++b) hb[b] = make_int4(P.h_blocks[b].level, P.h_blocks[b].first, P.h_blocks[b].count, P.h_blocks[b].pair_base);
+  for (int i = 0; i < nb; ++i) {
+    const M2LBlock& B = P.h_blocks[order[i]];
+    hb[i] = make_int4(B.level, B.first, B.count, B.pair_base);
+  }
   to_device(P.blocks, hb, s);
   P.cls_off.alloc((size_t)std::max(nb, 1) * (NCLASS + 1));
   P.pairs.alloc(std::max<int64_t>(base, 1));
