@@ -251,8 +251,13 @@ void matvec_sources(State& S, const double* xyz, const double* tau, int outputs,
   FMMB_CUDA(cudaStreamWaitEvent(S.side.s, S.side.fork, 0));
   near_sources(S, outputs, pot, grad, S.side.s);
   FMMB_CUDA(cudaEventRecord(S.side.join, S.side.s));
-  upward_pass(S);
-  downward_pass(S);
+  try {
+    upward_pass(S);
+    downward_pass(S);
+  } catch (...) {
+    cudaStreamWaitEvent(s, S.side.join, 0);   // later work on the stream stays ordered after the near field
+    throw;
+  }
   S.built = true;
   FMMB_CUDA(cudaStreamWaitEvent(s, S.side.join, 0));
   far_sources(S, outputs, pot, grad);

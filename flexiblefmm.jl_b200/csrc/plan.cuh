@@ -156,6 +156,11 @@ struct State {
     void ensure();
     ~Side();
   } side;
+  // the side stream's work reads the state's buffers and writes the outputs: it ends before any
+  // member is freed (an exception between the fork and the join leaves it unjoined)
+  ~State() {
+    if (side.s) cudaStreamSynchronize(side.s);
+  }
   // staging of the host-pointer entry points and the evaluation at targets
   DBuf<double> h_in_xyz, h_in_tau, d_pot, d_grad;
   DBuf<double> t_x, t_y, t_z;
