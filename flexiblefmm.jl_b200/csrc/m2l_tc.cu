@@ -219,7 +219,7 @@ __host__ __device__ __forceinline__ uint32_t perm_mask(int k, bool target) {
 // of `starts` set where column q begins a run; per run its last column and its target)
 struct __align__(16) PairInfo {
   float cs[NCHK];
-  int fac[NCHK];
+  int fac[NCHK];     // twice the D4h element (the shift of its code in a row's mask)
   int tgt[NCHK];
   int rend[NCHK];
   int rtgt[NCHK];
@@ -362,7 +362,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
               const int q = 16 * c16 + 4 * e4 + e;
               const float v = d[4 * e4 + e];
               const float other = __shfl_sync(0xffffffffu, v, src_lane);
-              const uint32_t code = emask >> (2 * ff[e]);
+              const uint32_t code = emask >> ff[e];   // ff = 2·(D4h element): its 2-bit code
               float y = ((code & 1) ? other : v) * cc[e];
               y = (code & 2) ? -y : y;
               acc = ((starts >> q) & 1) ? y : acc + y;
@@ -429,8 +429,8 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
           tB = pr.y & 0xff;
         }
         if (h == 0) {                                   // the first warp of the stage records the chunk
-          if (vA) { pi.fac[2 * lane] = facA; pi.tgt[2 * lane] = tA; }
-          if (vB) { pi.fac[2 * lane + 1] = facB; pi.tgt[2 * lane + 1] = tB; }
+          if (vA) { pi.fac[2 * lane] = 2 * facA; pi.tgt[2 * lane] = tA; }
+          if (vB) { pi.fac[2 * lane + 1] = 2 * facB; pi.tgt[2 * lane + 1] = tB; }
           // the target runs of the chunk (pairs are sorted by target within a class)
           const int tprev = __shfl_up_sync(0xffffffffu, tB, 1);
           const bool stA = vA && (lane == 0 || tA != tprev), stB = vB && tB != tA;
