@@ -219,6 +219,7 @@ __host__ __device__ __forceinline__ uint32_t perm_mask(int k, bool target) {
 // of `starts` set where column q begins a run; per run its last column and its target)
 struct __align__(16) PairInfo {
   float cs[NCHK];
+  float keep[NCHK];  // 0 where the column starts a target run, else 1 (the running sum's factor)
   int fac[NCHK];     // twice the D4h element (the shift of its code in a row's mask)
   int tgt[NCHK];
   int rend[NCHK];
@@ -355,17 +356,18 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
           for (int e4 = 0; e4 < 4; ++e4) {
             const int4 f4 = reinterpret_cast<const int4*>(pi.fac)[4 * c16 + e4];
             const float4 c4 = reinterpret_cast<const float4*>(pi.cs)[4 * c16 + e4];
+            const float4 k4 = reinterpret_cast<const float4*>(pi.keep)[4 * c16 + e4];
+            const float kk[4] = {k4.x, k4.y, k4.z, k4.w};
             const int ff[4] = {f4.x, f4.y, f4.z, f4.w};
             const float cc[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-              const int q = 16 * c16 + 4 * e4 + e;
               const float v = d[4 * e4 + e];
               const float other = __shfl_sync(0xffffffffu, v, src_lane);
               const uint32_t code = emask >> ff[e];   // ff = 2·(D4h element): its 2-bit code
               float y = ((code & 1) ? other : v) * cc[e];
               y = (code & 2) ? -y : y;
-              acc = ((starts >> q) & 1) ? y : acc + y;
+              acc = fmaf(acc, kk[e], y);   // y where a run starts (0·acc + y), else acc + y
               a[4 * e4 + e] = acc;
             }
           }
@@ -434,6 +436,8 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
           // the target runs of the chunk (pairs are sorted by target within a class)
           const int tprev = __shfl_up_sync(0xffffffffu, tB, 1);
           const bool stA = vA && (lane == 0 || tA != tprev), stB = vB && tB != tA;
+          if (vA) pi.keep[2 * lane] = stA ? 0.f : 1.f;
+          if (vB) pi.keep[2 * lane + 1] = stB ? 0.f : 1.f;
           const uint64_t starts = spread_bits(__ballot_sync(0xffffffffu, stA)) | (spread_bits(__ballot_sync(0xffffffffu, stB)) << 1);
           const bool endA = vA && (2 * lane + 1 == nc || stB);
           const bool endB = vB && (2 * lane + 2 == nc || ((starts >> (2 * lane + 2)) & 1));
