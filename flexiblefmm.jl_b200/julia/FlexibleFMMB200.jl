@@ -316,10 +316,11 @@ struct StokesDensitiesC
 end
 _dptr(::Nothing) = C_NULL
 _dptr(a::Vector) = Ptr{Cvoid}(pointer(a))
-_dcollect(::Nothing, n, name) = nothing
-function _dcollect(a::AbstractVector, n, name)
+# a density array as the library reads it: Float64 (weights) or SVector{3,Float64} per source
+_dcollect(::Nothing, n, name, ::Type) = nothing
+function _dcollect(a::AbstractVector, n, name, ::Type{T}) where {T}
     length(a) == n || throw(DimensionMismatch("$name has length $(length(a)), expected $n"))
-    return collect(a)
+    return collect(T, a)
 end
 
 function _stokes_call!(out_src, out_trg, plan::StokesFMMPlan, tg, stokeslets, stresslets, stressvecs, doublets,
@@ -334,9 +335,10 @@ function _stokes_call!(out_src, out_trg, plan::StokesFMMPlan, tg, stokeslets, st
     out_src === nothing || length(out_src) == n || throw(DimensionMismatch("expected $n outputs at the sources"))
     nt = tg === nothing ? 0 : length(tg)
     out_trg === nothing || length(out_trg) == nt || throw(DimensionMismatch("expected $nt outputs at the targets"))
-    arrs = (_dcollect(stokeslets, n, "stokeslets"), _dcollect(stresslets, n, "stresslets"),
-            _dcollect(stressvecs, n, "stressvecs"), _dcollect(doublets, n, "doublets"),
-            _dcollect(weights, n, "weights"))
+    V = SVector{3,Float64}
+    arrs = (_dcollect(stokeslets, n, "stokeslets", V), _dcollect(stresslets, n, "stresslets", V),
+            _dcollect(stressvecs, n, "stressvecs", V), _dcollect(doublets, n, "doublets", V),
+            _dcollect(weights, n, "weights", Float64))
     # the library writes ∂u_i/∂t_j at 9k + 3i + j: read as an SMatrix that is the transpose
     T = code == 1 ? Float64 : code == 2 ? SMatrix{3,3,Float64,9} : SVector{3,Float64}
     rs = out_src === nothing ? nothing : Vector{T}(undef, n)
