@@ -18,6 +18,13 @@ sums; p = 11 gives 7.3e-7). The configured order is measured beside it (configur
              sources (computed on the device, fmmb_direct_dev)
   roofline   the dominant kernel of the mixed path (the M2L) against the measured peak
   cpu_baseline  the CPU oracle (C++ restatement of the reference CPU path) on this host
+  parity     the oracle's outputs of that baseline run, and of one more at p = 10, against the
+             device's at all 10^6 points: tree field by field (perm included) and far pairs per
+             level, FP64 path max-norm relative (1e-12 potential, 1e-11 gradient), mixed path
+             relative L2 (1e-6 potential)
+
+Every figure goes on a "bench_detail" line first; the headline line after it carries the
+contract's keys and a compact copy of the rest.
 
 --impl reference times that CPU path alone (all host threads) as the reference arm.
 --gpus N: N independent replicas (the single FMM is not sharded: replicas only), one
@@ -81,7 +88,9 @@ def config(a, extra=None):
 
 
 # ---------------------------------------------------------------- the CPU oracle (baseline / reference arm)
-def cpu_oracle(pts, tau, p, ppl, reps, warmup=1):
+def cpu_oracle(pts, tau, p, ppl, reps, warmup=1, keep=False):
+    """The oracle's matvec on all host threads: step times; with keep, the oracle FMM (its tree)
+    and the outputs of the last step too."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     threads = oracle.set_threads(0)
@@ -89,14 +98,61 @@ def cpu_oracle(pts, tau, p, ppl, reps, warmup=1):
     f = oracle.FMM(p, pts, ppl)
     t_tree = time.perf_counter() - t0
     times = []
+    out = None
     for r in range(warmup + reps):
         t0 = time.perf_counter()
         f.build_expansions(pts, tau)
-        f.evaluate_at_sources()
+        out = f.evaluate_at_sources()
         dt = time.perf_counter() - t0
         if r >= warmup:
             times.append(dt)
-    return dict(times=times, threads=threads, tree_s=t_tree)
+    res = dict(times=times, threads=threads, tree_s=t_tree)
+    if keep:
+        res.update(fmm=f, pot=out[0], grad=out[1])
+    return res
+
+
+def _mrd(a, b):
+    """max-norm relative difference; rows of a 2-D array are vectors"""
+    if a.ndim == 2:
+        return float(np.max(np.linalg.norm(a - b, axis=1)) / np.max(np.linalg.norm(b, axis=1)))
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def _rl2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+TREE_FIELDS = ("cell", "level", "parent", "child_first", "plo", "phi", "leaf", "ghost", "xlist", "has_source", "colleagues",
+               "point_node", "perm")
+
+
+def parity(dev, orc):
+    """The device results of one order against the oracle's on the same points and charges:
+    the tree field by field (perm included) and the far pairs of every level as sets; the FP64
+    path's potential and gradient by max-norm relative difference (bars 1e-12 / 1e-11, the
+    reference's CPU-vs-device tolerances); the mixed path's by relative L2 (bar 1e-6 on the
+    potential, the metric's tolerance, 1e-5 on the gradient)."""
+    T = orc["fmm"].tree
+    t = dev["tree"]
+    bad = [k for k in TREE_FIELDS if t[k].shape != getattr(T, k).shape or not np.array_equal(t[k], getattr(T, k))]
+    pairs_ok, npairs = len(dev["pairs"]) == T.L, 0
+    for l in range(min(T.L, len(dev["pairs"]))):
+        a, b = np.stack(dev["pairs"][l]), np.stack(T.pairs(l))
+        npairs += b.shape[1]
+        if a.shape != b.shape or not np.array_equal(a[:, np.lexsort(a)], b[:, np.lexsort(b)]):
+            pairs_ok = False
+    ou, og = orc["pot"], orc["grad"]
+    fu, fg = dev["fp64"]
+    mu, mg = dev["mixed"]
+    r = {"tree_equal": not bad and dev["nnodes"] == T.n, "mismatched_fields": bad, "nodes": int(T.n), "levels": int(T.L),
+         "far_pairs_equal": pairs_ok, "far_pairs": int(npairs),
+         "fp64_vs_oracle_maxrel": {"pot": _mrd(fu, ou), "grad": _mrd(fg, og)},
+         "mixed_vs_oracle_rel_l2": {"pot": _rl2(mu, ou), "grad": _rl2(mg, og)}}
+    r["pass"] = bool(r["tree_equal"] and pairs_ok and r["fp64_vs_oracle_maxrel"]["pot"] < 1e-12
+                     and r["fp64_vs_oracle_maxrel"]["grad"] < 1e-11 and r["mixed_vs_oracle_rel_l2"]["pot"] < 1e-6
+                     and r["mixed_vs_oracle_rel_l2"]["grad"] < 1e-5)
+    return r
 
 
 def run_reference(a):
@@ -527,14 +583,15 @@ def run_ours(a):
              "ms_mixed": max_over_ranks(statistics.mean(t_mixed), dist, "cuda"),
              "ms_fp64": max_over_ranks(statistics.mean(t_fp64), dist, "cuda")}
         err = {}
+        dev = {"tree": f.tree(), "pairs": [f.pairs(l) for l in range(f.nlevels)], "nnodes": f.nnodes}
         for name in ("mixed", "fp64"):
             step(states[name])
             torch.cuda.synchronize()
-            u = pot_d.cpu().numpy()[sel]
-            g = grad_d.cpu().numpy()[sel]
+            dev[name] = (pot_d.cpu().numpy().copy(), grad_d.cpu().numpy().copy())
+            u, g = dev[name][0][sel], dev[name][1][sel]
             err[name] = {"pot_rel_l2": float(np.linalg.norm(u - dp_h) / np.linalg.norm(dp_h)),
                          "grad_rel_l2": float(np.linalg.norm(g - dg_h) / np.linalg.norm(dg_h))}
-        r["error"] = err
+        r["error"], r["dev"] = err, dev
         # stage times of one matvec per path (median of 3, CUDA events on the library's stream)
         stages, launches = {}, {}
         names = ("gather", "p2m", "m2m", "m2l", "l2l", "eval")
@@ -554,13 +611,14 @@ def run_ours(a):
         return r
 
     # the configured order (p = 10) first, then the headline order
-    side = None
+    side, dev10 = None, None
     if a.p != 10 and not a.no_p10:
         r10 = measure(10, False)
         side = {"p": 10, "value": replica_throughput(a.n, r10["ms_mixed"], world), "ms_per_step": r10["ms_mixed"],
                 "fp64": {"value": replica_throughput(a.n, r10["ms_fp64"], world), "ms_per_step": r10["ms_fp64"]},
                 "mixed_vs_fp64": r10["ms_fp64"] / r10["ms_mixed"], "error": {"samples": len(sel), **r10["error"]},
                 "stages_ms": r10["stages"]}
+        dev10 = r10["dev"]
         del r10
     R = measure(a.p, True)
     f, states, t_mixed = R["f"], R["states"], R["t_mixed"]
@@ -604,33 +662,34 @@ def run_ours(a):
         traffic = tj.get("dram_bytes_per_launch_full") or tj.get("dram_bytes_per_launch")
     lat = sorted(t_mixed)
     pct = lambda q: lat[min(len(lat) - 1, int(round(q * (len(lat) - 1))))]
-    cpu = None
+    cpu, par = None, {}
     if world == 1 and not a.no_cpu_baseline:
-        r = cpu_oracle(pts, tau, a.p, a.ppl, reps=2, warmup=1)
+        r = cpu_oracle(pts, tau, a.p, a.ppl, reps=2, warmup=1, keep=True)
         cpu = {"value": a.n / min(r["times"]), "unit": UNIT, "cores": r["threads"], "kind": "port",
                "sample": f"full {a.n:,}-point matvec (the same points and charges), best of 2 after 1 warm-up, "
                          f"tree + operators {r['tree_s']:.2f} s untimed"}
+        par[f"p{a.p}"] = parity(R["dev"], r)
+        del r
+        if dev10 is not None:
+            r = cpu_oracle(pts, tau, 10, a.ppl, reps=1, warmup=0, keep=True)
+            par["p10"] = parity(dev10, r)
+            del r
+    del dev10
+    R.pop("dev", None)
     serve = serving(fmmb, local, a.serve_requests, a.serve_slots) if a.serve_requests > 0 else None
     stokes = stokes_batched(fmmb, local, a.stokes_instances, a.stokes_slots) if a.stokes_instances > 0 else None
     ki = cube_ki(fmmb, torch, ctx, a.ki_points, 5, 3) if a.ki_points > 0 else None
     kic = None if a.no_circle_ki else circle_ki(fmmb)
+    # every figure, on a line of its own before the headline
+    detail = {"configured_order_p10": side, "serving": serve, "stokes_batched": stokes, "cube_ki": ki, "circle_ki": kic,
+              "parity": par, "stages_ms": stages, "error": {"samples": len(sel), **err}}
+    print(json.dumps({"bench_detail": detail}), flush=True)
     line = {
         "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp16x3 M2L (tcgen05 kind::f16, FP32 accumulation) + f32 near field (FP64 batch sums), f64 elsewhere",
         "data": "synthetic (seeded uniform points, N(0,1) charges)",
-        "config": config(a, {"precision": "mixed", "plan_s": plan_s, "levels": f.nlevels, "nodes": f.nnodes,
-                             "far_pairs": f.npairs}),
-        "configured_order_p10": side,
-        "serving": serve,
-        "stokes_batched": stokes,
-        "cube_ki": ki,
-        "circle_ki": kic,
-        "latency_ms": {"p50": pct(0.5), "p99": pct(0.99)},
-        "fp64": {"value": replica_throughput(a.n, ms_fp64, world), "ms_per_step": ms_fp64},
-        "mixed_vs_fp64": ms_fp64 / ms_mixed,
-        "error": {"samples": len(sel), **{k: v for k, v in err.items()}},
-        "stages_ms": stages,
+        "config": config(a, {"precision": "mixed", "levels": f.nlevels, "nodes": f.nnodes, "far_pairs": f.npairs}),
         "roofline": {"bound": "tensor", "kernel": "k_m2l_tc (M2L, all levels, one launch)", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if "bf16_tflops" in peaks else "fallback",
@@ -639,11 +698,61 @@ def run_ours(a):
         "gpu_launches": launches["mixed"] * a.steps,
         "clocks": clk,
         "cpu_baseline": cpu,
+        # the rest is a compact copy of the detail line's figures
+        "latency_ms": {"p50": _sig(pct(0.5)), "p99": _sig(pct(0.99))},
+        "fp64": {"value": _sig(replica_throughput(a.n, ms_fp64, world)), "ms_per_step": _sig(ms_fp64)},
+        "mixed_vs_fp64": _sig(ms_fp64 / ms_mixed),
+        "error": {"samples": len(sel), **_sig(err)},
+        "stages_ms": {"plan_s": _sig(plan_s), **_sig(stages)},
+        "parity": compact_parity(par),
+        "side": compact_side(side, serve, stokes, ki, kic),
     }
     print(json.dumps(line), flush=True)
     del states, f
     if dist:
         dist.destroy_process_group()
+
+
+def _sig(x, d=4):
+    """x with floats rounded to d significant digits (nested dicts and lists too)"""
+    if isinstance(x, dict):
+        return {k: _sig(v, d) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [_sig(v, d) for v in x]
+    if isinstance(x, float):
+        return float(f"{x:.{d}g}")
+    return x
+
+
+def compact_parity(par):
+    out = {}
+    for k, r in par.items():
+        out[k] = {"pass": r["pass"], "tree_equal": r["tree_equal"], "far_pairs_equal": r["far_pairs_equal"],
+                  "fp64_maxrel": _sig(r["fp64_vs_oracle_maxrel"], 3), "mixed_rel_l2": _sig(r["mixed_vs_oracle_rel_l2"], 3)}
+    return out
+
+
+def compact_side(p10, serve, stokes, ki, kic):
+    s = {}
+    if p10:
+        s["p10"] = {"value": _sig(p10["value"]), "fp64": _sig(p10["fp64"]["value"]),
+                    "err_mixed": _sig(p10["error"]["mixed"]["pot_rel_l2"], 3), "err_fp64": _sig(p10["error"]["fp64"]["pot_rel_l2"], 3)}
+    if serve:
+        s["serving"] = {"requests": serve["requests"], "batched": _sig(serve["batched"]["evals_per_s"]),
+                        "open_frac": _sig(serve["open_loop"]["fraction_of_batched"], 3),
+                        "p50_ms": _sig(serve["open_loop"]["latency_ms"]["p50"], 3), "p99_ms": _sig(serve["open_loop"]["latency_ms"]["p99"], 3),
+                        "fp64_one": _sig(serve["one_at_a_time_fp64"]["evals_per_s"])}
+        if "host_device_s" in serve:
+            s["serving"]["host_device_s"] = _sig(serve["host_device_s"], 3)
+    if stokes:
+        s["stokes"] = {"instances": stokes["instances"], "batched": _sig(stokes["batched"]["evals_per_s"]),
+                       "one": _sig(stokes["one_at_a_time"]["evals_per_s"]), "err_max": _sig(stokes["error"]["max"], 3)}
+    if ki:
+        s["cube_ki"] = {"value": _sig(ki["evals_per_s"]), "ms": _sig(ki["ms_per_step"]), "m2l_ms": _sig(ki["stages_ms"]["m2l"]),
+                        "err": _sig(ki["error"]["pot_rel_l2"], 3)}
+    if kic:
+        s["circle_ki"] = {"value": _sig(kic["evals_per_s"]), "err": _sig(kic["error"]["sources_rel_l2"], 3)}
+    return s
 
 
 def main():

@@ -145,6 +145,80 @@ def check_tree_invariants(t, pts, origin=(0.0, 0.0, 0.0), W0=1.0):
         assert leaf[p] and t["plo"][p] <= j <= t["phi"][p]
 
 
+def vlists(t):
+    """V(y) of every node (test/test_coverage.jl:16-29): the children of the colleagues of
+    parent(y) that are not colleagues of y (0-based, -1 for none)."""
+    cf, par, col = t["child_first"], t["parent"], t["colleagues"]
+    out = []
+    for y in range(len(cf)):
+        p = par[y]
+        if p < 0:
+            out.append(np.zeros(0, np.int64))
+            continue
+        c = col[p][col[p] >= 0]
+        c = c[cf[c] >= 0]
+        ch = (cf[c][:, None] + np.arange(8)[None, :]).ravel()
+        out.append(np.setdiff1d(ch, col[y][col[y] >= 0]))
+    return out
+
+
+def check_coverage(t, pairs, far):
+    """The kernel-free invariant of the FMM structure (test/test_coverage.jl:31-84), on a tree
+    `t` (dict of arrays, 0-based) and its far pairs `pairs[l] = (target, source, far index)`:
+    every (source terminal, target leaf) pair is covered exactly once, by the near field or by
+    exactly one V-list interaction between an ancestor-or-self of each; the pairs are exactly
+    the V lists restricted to sourced sources and non-ghost targets; offsets and levels agree
+    with `far`; a target appears at most once per offset; levels 0 and 1 have no pairs.
+    Terminals are childless, so "X is an ancestor-or-self of terminal T" is "T's points lie in
+    X's point range": the count runs over points, one difference array per leaf."""
+    n = len(t["level"])
+    N = len(t["perm"])
+    cf, par, col = t["child_first"], t["parent"], t["colleagues"]
+    plo, phi = t["plo"].astype(np.int64), t["phi"].astype(np.int64)
+    hs, leaf, ghost = (t[k].astype(bool) for k in ("has_source", "leaf", "ghost"))
+    V = vlists(t)
+    anc = []
+    for i in range(n):
+        a, j = [], i
+        while j >= 0:
+            a.append(j)
+            j = par[j]
+        anc.append(a)
+    term = np.nonzero((cf < 0) & hs)[0]
+    bad = 0
+    for B in np.nonzero(leaf)[0]:
+        near = np.zeros(N + 1, np.int64)
+        c = col[B][col[B] >= 0]
+        c = c[hs[c]]
+        np.add.at(near, plo[c], 1)
+        np.add.at(near, phi[c] + 1, -1)
+        X = np.concatenate([V[Y] for Y in anc[B]]) if anc[B] else np.zeros(0, np.int64)
+        X = X[hs[X]]
+        cnt = np.zeros(N + 1, np.int64)
+        np.add.at(cnt, plo[X], 1)
+        np.add.at(cnt, phi[X] + 1, -1)
+        nr, ct = np.cumsum(near)[plo[term]], np.cumsum(cnt)[plo[term]]
+        ok = ((nr > 0) & (ct == 0)) | ((nr == 0) & (ct == 1))
+        bad += int(np.count_nonzero(~ok))
+    assert bad == 0, f"{bad} (terminal, leaf) pairs not covered exactly once"
+    # the pairs are exactly V restricted to sourced sources and non-ghost targets
+    got = np.concatenate([np.stack([pt[0], pt[1]]).astype(np.int64) for pt in pairs], axis=1) if pairs else np.zeros((2, 0), np.int64)
+    key = got[0] * n + got[1]
+    assert len(np.unique(key)) == len(key), "a pair listed twice"
+    exp = [y * n + x for y in range(n) if not ghost[y] for x in V[y] if hs[x]]
+    assert np.array_equal(np.sort(key), np.sort(np.asarray(exp, np.int64))), "pairs differ from the V lists"
+    # offsets and levels; each target at most once per offset; nothing at levels 0 and 1
+    for l, (tg, sc, f) in enumerate(pairs):
+        if l < 2:
+            assert len(tg) == 0
+        if len(tg) == 0:
+            continue
+        assert np.all(t["level"][tg] == l) and np.all(t["level"][sc] == l)
+        assert np.array_equal(t["cell"][sc] - t["cell"][tg], far[f])
+        k = f.astype(np.int64) * n + tg
+        assert len(np.unique(k)) == len(k), "a target twice for one offset"
+
+
 def same_structure(a, b, keys=("cell", "level", "parent", "child_first", "plo", "phi", "leaf", "ghost", "xlist",
                                 "has_source", "colleagues", "point_node")):
     """test/test_device_tree.jl:110-112: every structural field equal."""
@@ -252,3 +326,23 @@ def yukawa_direct(src, tau, tgt, kappa, self_excluded=False, gradient=False):
             g = -(e * (1 + kappa * r) / r ** 2) * tau[None, :]
             grad[a:a + 256] = np.einsum("ts,tsk->tk", g, d) / (4 * np.pi)
     return (pot, grad) if gradient else pot
+
+
+# ---------------------------------------------------------------- the adaptive cloud (16 Gaussians, sigma 0.01)
+def gaussian_cloud(n, seed=4, ncentres=16, sigma=0.01):
+    """n points from `ncentres` isotropic Gaussians with centres uniform in [0.1, 0.9]^3, points
+    outside the unit box redrawn (the adaptive cube-KI configuration's point cloud)."""
+    rng = np.random.default_rng(seed)
+    c = 0.1 + 0.8 * rng.random((ncentres, 3))
+    pts = c[rng.integers(0, ncentres, n)] + sigma * rng.standard_normal((n, 3))
+    bad = np.any((pts < 0) | (pts >= 1), axis=1)
+    while bad.any():
+        pts[bad] = c[rng.integers(0, ncentres, int(bad.sum()))] + sigma * rng.standard_normal((int(bad.sum()), 3))
+        bad = np.any((pts < 0) | (pts >= 1), axis=1)
+    return pts
+
+
+def pairs_equal_as_sets(a, b):
+    """(target, source, far index) arrays of one level equal as sets of triples."""
+    a, b = np.stack(a), np.stack(b)
+    return a.shape == b.shape and np.array_equal(a[:, np.lexsort(a)], b[:, np.lexsort(b)])

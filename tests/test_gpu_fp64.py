@@ -9,7 +9,8 @@ on potentials.
 import numpy as np
 import pytest
 
-from helpers import DISTRIBUTIONS3, check_tree_invariants, mrd, oracle_tree_dict, same_structure
+from helpers import (DISTRIBUTIONS3, check_coverage, check_tree_invariants, gaussian_cloud, mrd, oracle_tree_dict,
+                     pairs_equal_as_sets, same_structure)
 
 pytestmark = pytest.mark.gpu
 BOX = ((0.0, 0.0, 0.0), 1.0)
@@ -39,6 +40,39 @@ def test_device_tree_equals_host_tree(oracle, fmmb, name, n, ppl, seed):
         a = sorted(zip(*[x.tolist() for x in f.pairs(l)]))
         b = sorted(zip(*[x.tolist() for x in T.pairs(l)]))
         assert a == b, f"level {l}"
+
+
+def test_device_tree_equals_host_tree_adaptive_cloud(oracle, fmmb):
+    """The adaptive configuration's point cloud (16 Gaussians, sigma 0.01) at 5e5 points and
+    ppl = 64: 10 levels, ghosts and 2:1 restriction at scale; every field, perm and the far
+    pairs of every level equal the oracle's."""
+    pts = gaussian_cloud(500_000)
+    T = oracle.Tree.build(pts, 64)
+    f = fmmb.FMM(_method(fmmb, 4), pts, ppl=64, bbox=BOX)
+    assert T.L >= 10 and f.nlevels == T.L and f.nnodes == T.n and T.ghost.sum() > 0
+    t = f.tree()
+    ref = oracle_tree_dict(T)
+    assert same_structure(t, ref) is None, same_structure(t, ref)
+    assert np.array_equal(t["perm"], ref["perm"])
+    for l in range(T.L):
+        assert pairs_equal_as_sets(f.pairs(l), T.pairs(l)), f"level {l}"
+
+
+@pytest.mark.parametrize("name", sorted(DISTRIBUTIONS3))
+def test_device_lists_coverage(oracle, fmmb, name):
+    """test/test_coverage.jl:86-96 on the device tree and the device far pairs."""
+    rng = np.random.default_rng(4)
+    pts = DISTRIBUTIONS3[name](rng, 400)
+    f = fmmb.FMM(_method(fmmb, 4), pts, ppl=4, bbox=BOX)
+    check_coverage(f.tree(), [f.pairs(l) for l in range(f.nlevels)], oracle.far_offsets())
+
+
+def test_device_lists_coverage_larger(oracle, fmmb):
+    rng = np.random.default_rng(5)
+    for pts, ppl in ((DISTRIBUTIONS3["mixed"](rng, 800), 3), (DISTRIBUTIONS3["uniform"](rng, 12), 12),
+                     (DISTRIBUTIONS3["clustered"](rng, 10000), 30), (DISTRIBUTIONS3["sphere"](rng, 10000), 16)):
+        f = fmmb.FMM(_method(fmmb, 4), pts, ppl=ppl, bbox=BOX)
+        check_coverage(f.tree(), [f.pairs(l) for l in range(f.nlevels)], oracle.far_offsets())
 
 
 def test_device_tree_invariants(fmmb):
