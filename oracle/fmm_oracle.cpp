@@ -522,8 +522,19 @@ static void dgemm(int m, int n, int k, double alpha, const double* A, int lda, c
 // ---------------------------------------------------------------- the FMM (src/fmm.jl, src/evaluate.jl)
 static const double KC = 1.0 / (4.0 * M_PI);   // Laplace3D c (src/kernels.jl:182)
 
+// the operators of one box width (Yukawa3D: src/operators/harmonics_yukawa.jl:164-218)
+struct LevelOps { std::vector<double> M2M, L2L; std::vector<std::vector<double>> reps; };
+
+// the kernel of the harmonic method: Laplace3D (harmonics.jl), Yukawa3D (harmonics_yukawa.jl),
+// Stokeslet3D through four Laplace expansions (harmonics_stokes.jl)
+enum Kind { LAPLACE = 0, YUKAWA = 1, STOKES = 2 };
+
 struct FMM {
   int p, NP;
+  int kind = LAPLACE;
+  int nb = 1;                                   // scalar expansions per node (4 for Stokes)
+  double kappa = 0;                             // Yukawa3D's κ
+  std::vector<LevelOps> yk;                     // Yukawa3D: the operators of each level's width
   Tree t;
   double W0ref;                                 // the operator cache's reference width
   std::vector<double> M2M, L2L;                 // NP × 8NP and 8NP × NP, column-major
@@ -570,6 +581,147 @@ static void level_operators(FMM& f) {
   f.tb = harmonic_tables(p);
 }
 
+// ---------------------------------------------------------------- Yukawa3D (src/operators/harmonics_yukawa.jl)
+// u_n(z) from z², n = 0..nmax: Miller's backward recurrence u_n = u_{n+1} + z² u_{n+2}/((2n+3)(2n+5))
+// from above max(nmax, z), normalised with u_0 = sinh z / z; two series terms for z² < 1e-8
+// (harmonics_yukawa.jl:44-59; _radial_weights, :232-253, is the same recurrence)
+static void yukawa_u(double z2, int nmax, double* u) {
+  if (z2 < 1e-8) {
+    for (int n = 0; n <= nmax; ++n) u[n] = 1 + z2 / (2 * (2 * n + 3));
+    return;
+  }
+  double z = std::sqrt(z2);
+  int N = std::max(nmax, (int)std::ceil(z)) + 25;
+  double a = 0, b = 1;
+  for (int n = N - 1; n >= 0; --n) {
+    double c = b + z2 * a / (double)((2 * n + 3) * (2 * n + 5));
+    if (n <= nmax) u[n] = c;
+    a = b; b = c;
+  }
+  double s = (std::sinh(z) / z) / b;
+  for (int n = 0; n <= nmax; ++n) u[n] *= s;
+}
+// v_n(z): v_0 = e^{−z}, v_1 = e^{−z}(1 + z), v_{n+1} = v_n + z² v_{n−1}/((2n−1)(2n+1)) (:61-73)
+static void yukawa_v(double z, int nmax, double* v) {
+  double e = std::exp(-z), z2 = z * z;
+  v[0] = e;
+  if (nmax >= 1) v[1] = e * (1 + z);
+  for (int n = 1; n <= nmax - 1; ++n) v[n + 1] = v[n] + z2 * v[n - 1] / (double)((2 * n - 1) * (2 * n + 1));
+}
+static double norm3(const double* y) { return std::sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]); }
+
+// the product rule on the unit sphere (:94-110): Gauss–Legendre nodes t (ascending) × 4p+20
+// equispaced angles; the nodes and weights come from the caller (the Golub–Welsch eigenvalues)
+struct SphereRule { std::vector<double> x, w; int nq; };
+static SphereRule sphere_quadrature(int p, const double* gt, const double* gw, int nt) {
+  SphereRule S;
+  int nphi = 4 * p + 20;
+  for (int i = 0; i < nt; ++i)
+    for (int k = 0; k < nphi; ++k) {
+      double phi = 2 * M_PI * k / nphi, s = std::sqrt(std::max(0.0, 1 - gt[i] * gt[i]));
+      S.x.push_back(s * std::cos(phi)); S.x.push_back(s * std::sin(phi)); S.x.push_back(gt[i]);
+      S.w.push_back(gw[i] * 2 * M_PI / nphi);
+    }
+  S.nq = nt * nphi;
+  return S;
+}
+// u_n(κ̂|y|) [Υ̃_n^0 | 2 Re Υ̃ | 2 Im Υ̃](y) (:111-125) into b[0..N)
+static void yukawa_regular(double* b, const double* y, double kh, int p, const Tables& tb) {
+  std::vector<double> u(p + 1);
+  double r = norm3(y);
+  yukawa_u((kh * r) * (kh * r), p, u.data());
+  fold_regular([&](int n, int m, double vr, double vi) {
+    double w = u[n];
+    if (m == 0) b[n * n] = w * vr;
+    else { b[rre(n, m)] = 2 * w * vr; b[rim(n, m)] = 2 * w * vi; }
+  }, y, p, tb);
+}
+// v_n(κ̂|y|) |y|^{−(2n+1)} [Υ̃_n^0 | 2 Re Υ̃ | −2 Im Υ̃](y) (:126-142)
+static void yukawa_irregular(double* b, const double* y, double kh, int p, const Tables& tb) {
+  std::vector<double> v(p + 1);
+  double r = norm3(y);
+  yukawa_v(kh * r, p, v.data());
+  double ir = 1 / r;
+  fold_regular([&](int n, int m, double vr, double vi) {
+    double w = v[n] * std::pow(ir, 2 * n + 1);
+    if (m == 0) b[n * n] = w * vr;
+    else { b[rre(n, m)] = 2 * w * vr; b[rim(n, m)] = -2 * w * vi; }
+  }, y, p, tb);
+}
+// the projection onto the regular or irregular basis on the sphere of radius ρ (:143-163):
+// N × nq column-major
+static std::vector<double> yukawa_projection(int p, double kh, double rho, bool irregular, const SphereRule& S, const Tables& tb) {
+  int N = (p + 1) * (p + 1);
+  std::vector<double> B((size_t)N * S.nq);
+  for (int q = 0; q < S.nq; ++q) {
+    double* col = &B[(size_t)q * N];
+    fold_regular([&](int n, int m, double vr, double vi) {
+      if (m == 0) col[n * n] = vr;
+      else { col[rre(n, m)] = 2 * vr; col[rim(n, m)] = 2 * vi; }
+    }, &S.x[3 * q], p, tb);
+    for (int i = 0; i < N; ++i) col[i] *= S.w[q];
+  }
+  std::vector<double> rad(p + 1);
+  if (irregular) yukawa_v(kh * rho, p, rad.data());
+  else yukawa_u((kh * rho) * (kh * rho), p, rad.data());
+  for (int n = 0; n <= p; ++n) {
+    double f = irregular ? rad[n] * std::pow(rho, -n - 1) : rad[n] * std::pow(rho, n);
+    double g0 = 4 * M_PI / (2 * n + 1);
+    for (int i = n * n; i < (n + 1) * (n + 1); ++i) {
+      int k = i - n * n + 1;                    // 1-based position in the degree's block
+      double g = k == 1 ? g0 : 2 * g0;
+      double sg = (irregular && k > 1 && (k & 1)) ? -1.0 : 1.0;
+      double fac = sg / (g * f);
+      for (int q = 0; q < S.nq; ++q) B[(size_t)q * N + i] *= fac;
+    }
+  }
+  return B;
+}
+// the operators of one width in box coordinates, κ̂ = κ w, the M2L carrying c/w (:164-207):
+// projection spheres of radius ½ about the target, 2 about the parent, 1 about the child
+static LevelOps yukawa_operators(int p, double kh, double cw, const Classes& sc, const Tables& tb, const SphereRule& S) {
+  int N = (p + 1) * (p + 1), nq = S.nq;
+  std::vector<double> Preg = yukawa_projection(p, kh, 0.5, false, S, tb);
+  std::vector<double> Pirr = yukawa_projection(p, kh, 2.0, true, S, tb);
+  std::vector<double> Pregc = yukawa_projection(p, kh / 2, 1.0, false, S, tb);
+  for (double& x : Preg) x *= cw;                // (cw * Preg) * transpose(F)
+  std::vector<double> FT((size_t)nq * N), col(N);   // FT[i·nq + q] = F[i, q]
+  auto fill = [&](auto&& body) {
+    for (int q = 0; q < nq; ++q) {
+      body(&S.x[3 * q], col.data());
+      for (int i = 0; i < N; ++i) FT[(size_t)i * nq + q] = col[i];
+    }
+  };
+  LevelOps ops;
+  for (const I3& o : sc.reps) {
+    fill([&](const double* x, double* c) {
+      double y[3] = {0.5 * x[0] - o.v[0], 0.5 * x[1] - o.v[1], 0.5 * x[2] - o.v[2]};
+      yukawa_irregular(c, y, kh, p, tb);
+    });
+    std::vector<double> R((size_t)N * N);
+    dgemm(N, N, nq, 1.0, Preg.data(), N, FT.data(), nq, R.data(), N);
+    ops.reps.push_back(R);
+  }
+  ops.M2M.assign((size_t)N * 8 * N, 0.0);
+  ops.L2L.assign((size_t)8 * N * N, 0.0);
+  for (int k = 0; k < NCH; ++k) {
+    I3 d = child_off(k);
+    double dh[3] = {(d.v[0] - 0.5) / 2, (d.v[1] - 0.5) / 2, (d.v[2] - 0.5) / 2};
+    fill([&](const double* x, double* c) {
+      double y[3] = {2 * (2.0 * x[0] - dh[0]), 2 * (2.0 * x[1] - dh[1]), 2 * (2.0 * x[2] - dh[2])};
+      yukawa_irregular(c, y, kh / 2, p, tb);
+      for (int i = 0; i < N; ++i) c[i] *= 2;
+    });
+    dgemm(N, N, nq, 1.0, Pirr.data(), N, FT.data(), nq, &ops.M2M[(size_t)k * N * N], N);
+    fill([&](const double* x, double* c) {
+      double y[3] = {dh[0] + 1.0 * x[0] / 2, dh[1] + 1.0 * x[1] / 2, dh[2] + 1.0 * x[2] / 2};
+      yukawa_regular(c, y, kh, p, tb);
+    });
+    dgemm(N, N, nq, 1.0, Pregc.data(), N, FT.data(), nq, &ops.L2L[(size_t)k * N], 8 * N);
+  }
+  return ops;
+}
+
 // S2M of one childless node (harmonics.jl:425-434, 242-250)
 static void s2m_node(FMM& f, int node, double* col) {
   const Tree& t = f.t;
@@ -577,37 +729,76 @@ static void s2m_node(FMM& f, int node, double* col) {
   double w = std::ldexp(t.W0, -l), c[3];
   cell_center(t.origin, &t.cell[3 * node], w, c);
   double s = f.scale[l];
-  for (int i = 0; i < f.NP; ++i) col[i] = 0;
+  const int N = f.NP;
+  for (int i = 0; i < f.nb * N; ++i) col[i] = 0;
+  // M_n^m += w(n) τ conj Υ̃_n^m(x̂) (harmonics.jl:243-252); the weight is 1, or u_n(κ̂|x̂|) for Yukawa
+  auto charge = [&](double* b, const double* xh, double tau, const double* wt) {
+    fold_regular([&](int n, int m, double vr, double vi) {
+      double tw = wt ? tau * wt[n] : tau;
+      if (m == 0) b[n * n] += tw * vr;
+      else { b[rre(n, m)] += tw * vr; b[rim(n, m)] += -tw * vi; }
+    }, xh, f.p, f.tb);
+  };
+  std::vector<double> u(f.p + 2);
+  double kh = f.kappa * w;
   for (int j = t.plo[node]; j <= t.phi[node]; ++j) {
     double xh[3] = {(f.xs[3 * j] - c[0]) * s, (f.xs[3 * j + 1] - c[1]) * s, (f.xs[3 * j + 2] - c[2]) * s};
-    double tau = f.tau[j];
-    fold_regular([&](int n, int m, double vr, double vi) {
-      if (m == 0) col[n * n] += tau * vr;
-      else { col[rre(n, m)] += tau * vr; col[rim(n, m)] += -tau * vi; }
-    }, xh, f.p, f.tb);
+    if (f.kind == LAPLACE) {
+      charge(col, xh, f.tau[j], nullptr);
+    } else if (f.kind == YUKAWA) {                 // harmonics_yukawa.jl:290-302
+      yukawa_u(kh * kh * ((xh[0] * xh[0] + xh[1] * xh[1]) + xh[2] * xh[2]), f.p + 1, u.data());
+      charge(col, xh, f.tau[j], u.data());
+    } else {                                       // the four blocks of a Stokeslet (harmonics_stokes.jl:197-204)
+      const double* fk = &f.tau[3 * j];
+      for (int k = 0; k < 3; ++k) charge(col + k * N, xh, fk[k], nullptr);
+      charge(col + 3 * N, xh, (xh[0] * fk[0] + xh[1] * fk[1]) + xh[2] * fk[2], nullptr);
+    }
   }
 }
 
 static void upward(FMM& f) {   // fmm.jl:170-205
   const Tree& t = f.t;
-  int N = f.NP, L = t.L;
+  int N = f.NP, L = t.L, NB = f.nb * N;
   std::fill(f.Mp.begin(), f.Mp.end(), 0.0);
   for (int l = L - 1; l >= 2; --l) {
     const std::vector<int>& nodes = f.s2m_nodes[l];
 #pragma omp parallel for schedule(dynamic, 16)
-    for (int q = 0; q < (int)nodes.size(); ++q) s2m_node(f, nodes[q], &f.Mp[(size_t)nodes[q] * N]);
+    for (int q = 0; q < (int)nodes.size(); ++q) s2m_node(f, nodes[q], &f.Mp[(size_t)nodes[q] * NB]);
     if (l < L - 1) {
       int c0 = t.level_start[l + 1], ng = (t.level_start[l + 2] - c0) / NCH;
-      std::vector<double> tmp((size_t)N * ng);
+      std::vector<double> tmp((size_t)NB * ng);
+      // the parent level's operator (Yukawa: its width's; harmonics_yukawa.jl:209-218)
+      const double* M2M = f.kind == YUKAWA ? f.yk[l].M2M.data() : f.M2M.data();
       int nth = omp_get_max_threads();
 #pragma omp parallel for schedule(static)
       for (int ch = 0; ch < nth; ++ch) {
         int g0 = (int)((i64)ch * ng / nth), g1 = (int)((i64)(ch + 1) * ng / nth);
-        if (g1 > g0) dgemm(N, g1 - g0, 8 * N, 1.0, f.M2M.data(), N, &f.Mp[(size_t)(c0 + NCH * g0) * N], 8 * N, &tmp[(size_t)g0 * N], N);
+        if (g1 <= g0) continue;
+        if (f.kind != STOKES) {
+          dgemm(N, g1 - g0, 8 * N, 1.0, M2M, N, &f.Mp[(size_t)(c0 + NCH * g0) * N], 8 * N, &tmp[(size_t)g0 * N], N);
+          continue;
+        }
+        // Stokes (harmonics_stokes.jl:157-179): block a of the parent is M2M on the children's
+        // block a stacked; the fourth with the coupling folded in, ½Ψ̂ + δ̂·Φ
+        int nc = g1 - g0;
+        std::vector<double> X((size_t)8 * N * nc), R((size_t)N * nc);
+        for (int a = 0; a < 4; ++a) {
+          for (int g = 0; g < nc; ++g)
+            for (int j = 0; j < NCH; ++j) {
+              const double* B = &f.Mp[(size_t)(c0 + NCH * (g0 + g) + j) * NB];
+              double* x = &X[(size_t)g * 8 * N + (size_t)j * N];
+              I3 d = child_off(j);
+              double dh[3] = {(d.v[0] - 0.5) / 2, (d.v[1] - 0.5) / 2, (d.v[2] - 0.5) / 2};
+              for (int i = 0; i < N; ++i)
+                x[i] = a < 3 ? B[a * N + i] : B[3 * N + i] / 2 + dh[0] * B[i] + dh[1] * B[N + i] + dh[2] * B[2 * N + i];
+            }
+          dgemm(N, nc, 8 * N, 1.0, M2M, N, X.data(), 8 * N, R.data(), N);
+          for (int g = 0; g < nc; ++g) std::copy(&R[(size_t)g * N], &R[(size_t)(g + 1) * N], &tmp[(size_t)(g0 + g) * NB + a * N]);
+        }
       }
       for (int g = 0; g < ng; ++g) {
         int par = t.parent[c0 + NCH * g];
-        std::copy(&tmp[(size_t)g * N], &tmp[(size_t)(g + 1) * N], &f.Mp[(size_t)par * N]);
+        std::copy(&tmp[(size_t)g * NB], &tmp[(size_t)(g + 1) * NB], &f.Mp[(size_t)par * NB]);
       }
     }
   }
@@ -615,18 +806,22 @@ static void upward(FMM& f) {   // fmm.jl:170-205
 
 static void m2l_level(FMM& f, int l) {   // harmonics.jl:531-645, symmetry.jl:207-240
   const Tree& t = f.t;
-  int N = f.NP, lo = t.level_start[l];
+  int N = f.NP, lo = t.level_start[l], nb = f.nb, NB = nb * N;
   const std::vector<int>& ptr = t.ptr[l]; const std::vector<int>& src = t.src[l]; const std::vector<int>& far = t.far[l];
   const std::vector<int>& ord = f.torder[l];
   int nt = (int)ord.size();
   if (nt == 0) return;
-  int nclass = (int)f.reps.size();
+  // Laplace and Stokes: the reference width's representatives and the level's factor;
+  // Yukawa: the level width's representatives (harmonics_yukawa.jl:209-218)
+  const std::vector<std::vector<double>>& reps = f.kind == YUKAWA ? f.yk[l].reps : f.reps;
+  int nclass = (int)reps.size();
   const int TB = 32;                              // _TARGET_BLOCK
   int nblocks = (nt + TB - 1) / TB;
-  double alpha = f.m2l_scale[l];
+  double alpha = f.kind == YUKAWA ? 1.0 : f.m2l_scale[l];
+  static const std::vector<I3> offs = far_offsets();
 #pragma omp parallel
   {
-    std::vector<double> G((size_t)N * 512), R((size_t)N * 512);
+    std::vector<double> G((size_t)N * 512 * nb), R((size_t)N * 512 * nb);
     std::vector<int> qs; qs.reserve(512);
     std::vector<int> qt; qt.reserve(512);
 #pragma omp for schedule(dynamic, 1)
@@ -640,20 +835,33 @@ static void m2l_level(FMM& f, int l) {   // harmonics.jl:531-645, symmetry.jl:20
         }
         int nc = (int)qs.size();
         if (nc == 0) continue;
+        if ((size_t)nc * nb * N > G.size()) { G.resize((size_t)nc * nb * N); R.resize((size_t)nc * nb * N); }
+        // one column per pair and scalar expansion, the blocks of a pair consecutive (_gather_column!)
         for (int j = 0; j < nc; ++j) {
           int e = qs[j], fo = far[e];
-          const double* m = &f.Mp[(size_t)src[e] * N];
           const int* idx = f.sc.idx[fo].data(); const int8_t* sg = f.sc.sgn[fo].data();
-          double* gcol = &G[(size_t)j * N];
-          for (int i = 0; i < N; ++i) gcol[i] = sg[i] * m[idx[i]];
+          for (int a = 0; a < nb; ++a) {
+            const double* m = &f.Mp[(size_t)src[e] * NB + (size_t)a * N];
+            double* gcol = &G[(size_t)(j * nb + a) * N];
+            for (int i = 0; i < N; ++i) gcol[i] = sg[i] * m[idx[i]];
+          }
         }
-        dgemm(N, nc, N, alpha, f.reps[c].data(), N, G.data(), N, R.data(), N);
+        dgemm(N, nc * nb, N, alpha, reps[c].data(), N, G.data(), N, R.data(), N);
+        // _scatter_target!: the target permutation, and for Stokes Ψ̂ += o·Φ with the pair's offset
         for (int j = 0; j < nc; ++j) {
           int fo = far[qs[j]];
-          double* pl = &f.Pl[(size_t)qt[j] * N];
           const int* it = f.sc.idx_t[fo].data(); const int8_t* st = f.sc.sgn_t[fo].data();
-          const double* r = &R[(size_t)j * N];
-          for (int i = 0; i < N; ++i) pl[it[i]] += st[i] * r[i];
+          for (int a = 0; a < nb; ++a) {
+            double* pl = &f.Pl[(size_t)qt[j] * NB + (size_t)a * N];
+            const double* r = &R[(size_t)(j * nb + a) * N];
+            if (nb == 4 && a == 3) {
+              const double *r1 = &R[(size_t)(j * nb) * N], *r2 = r1 + N, *r3 = r2 + N;
+              const I3& o = offs[fo];
+              for (int i = 0; i < N; ++i) pl[it[i]] += st[i] * (r[i] + o.v[0] * r1[i] + o.v[1] * r2[i] + o.v[2] * r3[i]);
+            } else {
+              for (int i = 0; i < N; ++i) pl[it[i]] += st[i] * r[i];
+            }
+          }
         }
       }
     }
@@ -662,31 +870,59 @@ static void m2l_level(FMM& f, int l) {   // harmonics.jl:531-645, symmetry.jl:20
 
 static void downward(FMM& f) {   // fmm.jl:207-262
   const Tree& t = f.t;
-  int N = f.NP, L = t.L;
+  int N = f.NP, L = t.L, NB = f.nb * N;
   std::fill(f.Pl.begin(), f.Pl.end(), 0.0);
   std::fill(f.Lc.begin(), f.Lc.end(), 0.0);
   for (int l = 2; l < L; ++l) {
     int lo = t.level_start[l], nl = t.level_start[l + 1] - lo;
     if (l > 2) {
       int ng = nl / NCH;
-      std::vector<double> G((size_t)N * ng);
+      std::vector<double> G((size_t)NB * ng);
       for (int g = 0; g < ng; ++g) {
         int par = t.parent[lo + NCH * g];
-        std::copy(&f.Pl[(size_t)par * N], &f.Pl[(size_t)(par + 1) * N], &G[(size_t)g * N]);
+        std::copy(&f.Pl[(size_t)par * NB], &f.Pl[(size_t)(par + 1) * NB], &G[(size_t)g * NB]);
       }
+      // the parent level's operator (Yukawa: its width's)
+      const double* L2L = f.kind == YUKAWA ? f.yk[l - 1].L2L.data() : f.L2L.data();
       int nth = omp_get_max_threads();
 #pragma omp parallel for schedule(static)
       for (int ch = 0; ch < nth; ++ch) {
         int g0 = (int)((i64)ch * ng / nth), g1 = (int)((i64)(ch + 1) * ng / nth);
-        if (g1 > g0) dgemm(8 * N, g1 - g0, N, 1.0, f.L2L.data(), 8 * N, &G[(size_t)g0 * N], N, &f.Pl[(size_t)(lo + NCH * g0) * N], 8 * N);
+        if (g1 <= g0) continue;
+        if (f.kind != STOKES) {
+          dgemm(8 * N, g1 - g0, N, 1.0, L2L, 8 * N, &G[(size_t)g0 * N], N, &f.Pl[(size_t)(lo + NCH * g0) * N], 8 * N);
+          continue;
+        }
+        // Stokes (harmonics_stokes.jl:180-203): R_a = L2L · G_a per block; child blocks 1-3 are
+        // R_a, the fourth 2·R_4 − 2 δ̂·(R_1, R_2, R_3)
+        int nc = g1 - g0;
+        std::vector<double> X((size_t)N * nc), R((size_t)4 * 8 * N * nc);
+        for (int a = 0; a < 4; ++a) {
+          for (int g = 0; g < nc; ++g) std::copy(&G[(size_t)(g0 + g) * NB + a * N], &G[(size_t)(g0 + g) * NB + (a + 1) * N], &X[(size_t)g * N]);
+          dgemm(8 * N, nc, N, 1.0, L2L, 8 * N, X.data(), N, &R[(size_t)a * 8 * N * nc], 8 * N);
+        }
+        for (int g = 0; g < nc; ++g)
+          for (int j = 0; j < NCH; ++j) {
+            I3 d = child_off(j);
+            double dh[3] = {(d.v[0] - 0.5) / 2, (d.v[1] - 0.5) / 2, (d.v[2] - 0.5) / 2};
+            double* out = &f.Pl[(size_t)(lo + NCH * (g0 + g) + j) * NB];
+            for (int i = 0; i < N; ++i) {
+              size_t x0 = (size_t)g * 8 * N + (size_t)j * N + i, bs = (size_t)8 * N * nc;
+              double r1 = R[x0], r2 = R[bs + x0], r3 = R[2 * bs + x0];
+              out[i] = r1; out[N + i] = r2; out[2 * N + i] = r3;
+              out[3 * N + i] = 2 * R[3 * bs + x0] - 2 * (dh[0] * r1 + dh[1] * r2 + dh[2] * r3);
+            }
+          }
       }
     }
     m2l_level(f, l);
-    for (int i : f.leaf_nodes[l]) std::copy(&f.Pl[(size_t)i * N], &f.Pl[(size_t)(i + 1) * N], &f.Lc[(size_t)i * N]);
+    for (int i : f.leaf_nodes[l]) std::copy(&f.Pl[(size_t)i * NB], &f.Pl[(size_t)(i + 1) * NB], &f.Lc[(size_t)i * NB]);
   }
 }
 
-// evaluate_target (evaluate.jl:33-48) for potential and gradient at once; skip = tree index or -1
+// evaluate_target (evaluate.jl:33-48) for potential and gradient at once; skip = tree index or -1.
+// Laplace3D (harmonics.jl:447-486) and Yukawa3D, whose far field weighs degree n by u_n(κ̂|x̂|) and
+// adds x̂ times the potential weighted by κ̂² u_{n+1}/(2n+3) to the gradient (harmonics_yukawa.jl:304-317)
 static void evaluate_target(const FMM& f, const double* x, int i, int skip, double* pot, double* grad) {
   const Tree& t = f.t;
   int l = t.level[i];
@@ -695,20 +931,33 @@ static void evaluate_target(const FMM& f, const double* x, int i, int skip, doub
   double s = f.scale[l];
   double xh[3] = {(x[0] - c[0]) * s, (x[1] - c[1]) * s, (x[2] - c[2]) * s};
   const double* Lc = &f.Lc[(size_t)i * f.NP];
-  double u = 0;
-  fold_regular([&](int n, int m, double vr, double vi) {
-    double lr, li; get_coef(Lc, n, m, lr, li);
-    u = m == 0 ? u + lr * vr : u + 2 * (lr * vr + li * vi);
-  }, xh, f.p, f.tb);
+  const bool yk = f.kind == YUKAWA;
+  double kh = f.kappa * w, kh2 = kh * kh, r2h = (xh[0] * xh[0] + xh[1] * xh[1]) + xh[2] * xh[2];
+  std::vector<double> up(f.p + 2), ug(f.p + 2);
+  if (yk) { yukawa_u(kh * kh * r2h, f.p, up.data()); yukawa_u(kh * kh * r2h, f.p + 1, ug.data()); }
+  // Σ w(n) L conj Υ̃ (_harmonic_potential) with the weights wt (null: 1) or the radial ones
+  auto potential = [&](const double* wt, bool radial) {
+    double u = 0;
+    fold_regular([&](int n, int m, double vr, double vi) {
+      double lr, li; get_coef(Lc, n, m, lr, li);
+      double wn = radial ? kh2 * wt[n + 1] / (2 * n + 3) : (wt ? wt[n] : 1.0);
+      if (!wt) u = m == 0 ? u + lr * vr : u + 2 * (lr * vr + li * vi);
+      else u = m == 0 ? u + wn * (lr * vr) : u + wn * (2 * (lr * vr + li * vi));
+    }, xh, f.p, f.tb);
+    return u;
+  };
+  double u = potential(yk ? up.data() : nullptr, false);
   double gx = 0, gy = 0, gz = 0;
   const Tables& tb = f.tb;
   fold_regular([&](int n1, int m1, double vr, double vi) {
     int n = n1 + 1;
+    double wn = yk ? ug[n] : 1.0;
     if (m1 == 0) {
       double lr, li; get_coef(Lc, n, 1, lr, li);
       double cc = tb.cm[tidx(n, 1)];
       double ax = -cc * lr, ay = -cc * li, az = tb.cz[tidx(n, 0)] * Lc[n * n];
-      gx += ax * vr; gy += ay * vr; gz += az * vr;
+      if (yk) { gx += wn * (ax * vr); gy += wn * (ay * vr); gz += wn * (az * vr); }
+      else { gx += ax * vr; gy += ay * vr; gz += az * vr; }
     } else {
       double ur, ui, dr, di, zr, zi;
       get_coef(Lc, n, m1 + 1, ur, ui); get_coef(Lc, n, m1 - 1, dr, di);
@@ -717,11 +966,17 @@ static void evaluate_target(const FMM& f, const double* x, int i, int skip, doub
       double ayr = -(cu * ui + cd * di), ayi = cu * ur + cd * dr;
       double czv = tb.cz[tidx(n, m1)];
       get_coef(Lc, n, m1, zr, zi);
-      gx += 2 * (axr * vr + axi * vi); gy += 2 * (ayr * vr + ayi * vi); gz += 2 * (czv * (zr * vr + zi * vi));
+      double w2 = 2 * wn;
+      gx += w2 * (axr * vr + axi * vi); gy += w2 * (ayr * vr + ayi * vi); gz += w2 * (czv * (zr * vr + zi * vi));
     }
   }, xh, f.p - 1, tb);
+  if (yk) {
+    double pr = potential(ug.data(), true);
+    gx += xh[0] * pr; gy += xh[1] * pr; gz += xh[2] * pr;
+  }
   gx *= s; gy *= s; gz *= s;
-  // near field over the 27 colleagues, the excluded source masked (evaluate.jl:12-25, kernels.jl:179-193)
+  // near field over the 27 colleagues, the excluded source masked (evaluate.jl:12-25, kernels.jl:179-193;
+  // Yukawa: the radial kernel c e^{−κr}/r and its gradient (c f′/r) d, kernels.jl:33-41,228-242)
   for (int k = 0; k < NCOL; ++k) {
     int cn = t.col[(size_t)NCOL * i + k];
     if (cn < 0) continue;
@@ -729,14 +984,92 @@ static void evaluate_target(const FMM& f, const double* x, int i, int skip, doub
       if (j == skip) continue;
       double d0 = x[0] - f.xs[3 * j], d1 = x[1] - f.xs[3 * j + 1], d2 = x[2] - f.xs[3 * j + 2];
       double r2 = std::fma(d2, d2, std::fma(d1, d1, d0 * d0));
-      double ir = 1.0 / std::sqrt(r2);
       double tj = f.tau[j];
+      if (yk) {
+        double r = std::sqrt(r2), ir = 1 / r, e = std::exp(-f.kappa * r);
+        u += (KC * (e * ir)) * tj;
+        double fp = -e * (f.kappa * ir + ir * ir);
+        double a = KC * fp / r;
+        gx += (a * d0) * tj; gy += (a * d1) * tj; gz += (a * d2) * tj;
+        continue;
+      }
+      double ir = 1.0 / std::sqrt(r2);
       u += (KC * ir) * tj;
       double a = -KC * ir * ir * ir;
       gx += (a * d0) * tj; gy += (a * d1) * tj; gz += (a * d2) * tj;
     }
   }
   *pot = u; grad[0] = gx; grad[1] = gy; grad[2] = gz;
+}
+
+// ---------------------------------------------------------------- Stokes outputs (harmonics_stokes.jl:236-343)
+// the (n, m) coefficient of block `o` as a complex number, zero outside the triangle; negative m
+// by conjugate symmetry (_cget)
+static cplx cget(const double* L, int p, int n, int m) {
+  if (n > p || std::abs(m) > n) return cplx(0, 0);
+  if (m == 0) return cplx(L[n * n], 0);
+  if (m > 0) return cplx(L[rre(n, m)], L[rim(n, m)]);
+  return (double)((-m) % 2 == 0 ? 1 : -1) * cplx(L[rre(n, -m)], -L[rim(n, -m)]);
+}
+static double tcz(const Tables& tb, int n, int m) { return std::abs(m) > n ? 0.0 : tb.cz[tidx(n, std::abs(m))]; }
+static double tcm(const Tables& tb, int n, int m) { return std::abs(m) > n ? 0.0 : m >= 0 ? tb.cm[tidx(n, m)] : tb.cp[tidx(n, -m)]; }
+static double tcp(const Tables& tb, int n, int m) { return std::abs(m) > n ? 0.0 : m >= 0 ? tb.cp[tidx(n, m)] : tb.cm[tidx(n, -m)]; }
+// the (n′, m′) coefficients of the scaled gradient of one block (_dcoef)
+static void dcoef(const double* L, int p, const Tables& tb, int n1, int m1, cplx* a) {
+  int n = n1 + 1;
+  cplx dm = -tcm(tb, n, m1 + 1) * cget(L, p, n, m1 + 1);
+  cplx dp = tcp(tb, n, m1 - 1) * cget(L, p, n, m1 - 1);
+  cplx dz = tcz(tb, n, m1) * cget(L, p, n, m1);
+  a[0] = (dm + dp) / 2.0; a[1] = cplx(0, 1) * (dp - dm) / 2.0; a[2] = dz;
+}
+static double re_conj(cplx c, cplx v) { return (c * std::conj(v)).real(); }
+
+// velocity ½[Φ − x̂·∇̂Φ + ∇̂Ψ̂] and pressure −s·tr ∇̂Φ of the leaf's four local expansions
+// (_stokes_fold1, _stokes_output), plus the Stokeslet near field c[f/r + d(d·f)/r³] and its
+// pressure 2c(d·f)/r³ (kernels.jl:253-272); skip = tree index or -1
+static void stokes_evaluate_target(const FMM& f, const double* x, int i, int skip, double* vel, double* pres) {
+  const Tree& t = f.t;
+  int l = t.level[i], N = f.NP, p = f.p;
+  double w = std::ldexp(t.W0, -l), c[3];
+  cell_center(t.origin, &t.cell[3 * i], w, c);
+  double s = f.scale[l];
+  double xh[3] = {(x[0] - c[0]) * s, (x[1] - c[1]) * s, (x[2] - c[2]) * s};
+  const double* Lc = &f.Lc[(size_t)i * 4 * N];
+  double Phi[3] = {0, 0, 0}, G[3][3] = {{0}}, gP[3] = {0, 0, 0};   // G[i][k] = ∂̂_iΦ_k
+  fold_regular([&](int n, int m, double vr, double vi) {
+    cplx v(vr, vi);
+    double wt = m == 0 ? 1 : 2;
+    for (int k = 0; k < 3; ++k) Phi[k] += wt * re_conj(cget(Lc + k * N, p, n, m), v);
+    if (n < p) {
+      cplx a[3];
+      for (int k = 0; k < 3; ++k) {
+        dcoef(Lc + k * N, p, f.tb, n, m, a);
+        for (int d = 0; d < 3; ++d) G[d][k] += wt * re_conj(a[d], v);
+      }
+      dcoef(Lc + 3 * N, p, f.tb, n, m, a);
+      for (int d = 0; d < 3; ++d) gP[d] += wt * re_conj(a[d], v);
+    }
+  }, xh, p, f.tb);
+  double u[3], pr = -s * ((G[0][0] + G[1][1]) + G[2][2]);
+  for (int d = 0; d < 3; ++d) u[d] = (Phi[d] - ((G[d][0] * xh[0] + G[d][1] * xh[1]) + G[d][2] * xh[2]) + gP[d]) / 2;
+  const double KS = 1.0 / (8.0 * M_PI);
+  for (int k = 0; k < NCOL; ++k) {
+    int cn = t.col[(size_t)NCOL * i + k];
+    if (cn < 0) continue;
+    for (int j = t.plo[cn]; j <= t.phi[cn]; ++j) {
+      if (j == skip) continue;
+      double d[3] = {x[0] - f.xs[3 * j], x[1] - f.xs[3 * j + 1], x[2] - f.xs[3 * j + 2]};
+      double r2 = std::fma(d[2], d[2], std::fma(d[1], d[1], d[0] * d[0]));
+      double ir = 1.0 / std::sqrt(r2);
+      double a = KS * ir, b = a * ir * ir;
+      const double* fj = &f.tau[3 * j];
+      double df = (d[0] * fj[0] + d[1] * fj[1]) + d[2] * fj[2];
+      for (int e = 0; e < 3; ++e) u[e] += a * fj[e] + b * d[e] * df;
+      pr += (2 * KS * ir * ir * ir) * df;
+    }
+  }
+  if (vel) { vel[0] = u[0]; vel[1] = u[1]; vel[2] = u[2]; }
+  if (pres) *pres = pr;
 }
 
 static int locate(const Tree& t, const double* x) {   // locate.jl:10-22
@@ -749,19 +1082,32 @@ static int locate(const Tree& t, const double* x) {   // locate.jl:10-22
   return i;
 }
 
-static FMM* make_fmm(int p, const double* xyz, int N, int ppl, const double* origin, double W0, int max_levels, double W0ref) {
+// kind: LAPLACE, YUKAWA (κ = kappa; gt/gw: the Gauss–Legendre rule of 2p+10 points) or STOKES
+static FMM* make_fmm(int p, const double* xyz, int N, int ppl, const double* origin, double W0, int max_levels, double W0ref,
+                     int kind = LAPLACE, double kappa = 0, const double* gt = nullptr, const double* gw = nullptr, int ngl = 0) {
   FMM* f = new FMM();
   try {
     f->p = p; f->NP = (p + 1) * (p + 1);
+    f->kind = kind; f->kappa = kappa; f->nb = kind == STOKES ? 4 : 1;
     f->t = build_tree(xyz, N, ppl, origin, W0, max_levels);
     f->W0ref = W0ref > 0 ? W0ref : W0;
     level_operators(*f);
     const Tree& t = f->t;
     int L = t.L;
+    if (kind == YUKAWA) {
+      if (ngl != 2 * p + 10) throw Error(1, "the Yukawa sphere rule needs 2p+10 Gauss-Legendre nodes");
+      SphereRule S = sphere_quadrature(p, gt, gw, ngl);
+      f->yk.resize(L);
+      for (int l = 2; l < L; ++l) {
+        double w = std::ldexp(t.W0, -l);
+        f->yk[l] = yukawa_operators(p, kappa * w, KC / w, f->sc, f->tb, S);
+      }
+    }
     f->scale.resize(L); f->m2l_scale.resize(L);
     for (int l = 0; l < L; ++l) {
       double w = std::ldexp(t.W0, -l), lam = w / f->W0ref;
       f->scale[l] = (1.0 / f->W0ref) / lam;       // _rescaled (harmonics.jl:362)
+      if (kind == YUKAWA) f->scale[l] = 1 / w;      // built per width (harmonics_yukawa.jl:209-218)
       f->m2l_scale[l] = 1.0 / lam;                 // rescale (harmonics.jl:414-418)
     }
     f->s2m_nodes.resize(L); f->leaf_nodes.resize(L); f->torder.resize(L);
@@ -778,8 +1124,9 @@ static FMM* make_fmm(int p, const double* xyz, int N, int ppl, const double* ori
       std::stable_sort(ks.begin(), ks.end(), [](const std::pair<uint64_t, int>& a, const std::pair<uint64_t, int>& b) { return a.first < b.first; });
       for (auto& kq : ks) f->torder[l].push_back(kq.second);
     }
-    f->Mp.assign((size_t)f->NP * t.n, 0.0); f->Pl.assign((size_t)f->NP * t.n, 0.0); f->Lc.assign((size_t)f->NP * t.n, 0.0);
-    f->xs.resize(3 * (size_t)N); f->tau.resize(N);
+    size_t ne = (size_t)f->nb * f->NP * t.n;
+    f->Mp.assign(ne, 0.0); f->Pl.assign(ne, 0.0); f->Lc.assign(ne, 0.0);
+    f->xs.resize(3 * (size_t)N); f->tau.resize((kind == STOKES ? 3 : 1) * (size_t)N);
   } catch (...) { delete f; throw; }
   return f;
 }
@@ -843,6 +1190,12 @@ void orc_tree_pairs(void* h, int l, int32_t* tgt, int32_t* src, int32_t* far) {
 int orc_fmm_create(int p, const double* xyz, i64 n, int ppl, const double* origin, double W0, int max_levels, double W0ref, void** out) {
   GUARD({ *out = make_fmm(p, xyz, (int)n, ppl, origin, W0, max_levels, W0ref); return 0; })
 }
+// the harmonic method of another kernel: kind 1 Yukawa3D(κ) (gt/gw: the Gauss–Legendre rule of
+// 2p+10 points on [−1, 1], ascending), kind 2 Stokeslet3D (four expansions per node)
+int orc_fmm_create_kind(int kind, int p, double kappa, const double* gt, const double* gw, int ngl, const double* xyz, i64 n,
+                        int ppl, const double* origin, double W0, int max_levels, double W0ref, void** out) {
+  GUARD({ *out = make_fmm(p, xyz, (int)n, ppl, origin, W0, max_levels, W0ref, kind, kappa, gt, gw, ngl); return 0; })
+}
 void orc_fmm_free(void* h) { delete (FMM*)h; }
 void* orc_fmm_tree(void* h) { return &((FMM*)h)->t; }
 // build_expansions! (fmm.jl:271-298): inputs in the original order
@@ -851,7 +1204,9 @@ int orc_fmm_build(void* h, const double* xyz, const double* tau) {
   GUARD({
     for (int k = 0; k < f.t.N; ++k) {
       int j = f.t.perm[k];
-      f.xs[3 * k] = xyz[3 * j]; f.xs[3 * k + 1] = xyz[3 * j + 1]; f.xs[3 * k + 2] = xyz[3 * j + 2]; f.tau[k] = tau[j];
+      f.xs[3 * k] = xyz[3 * j]; f.xs[3 * k + 1] = xyz[3 * j + 1]; f.xs[3 * k + 2] = xyz[3 * j + 2];
+      if (f.kind == STOKES) for (int d = 0; d < 3; ++d) f.tau[3 * k + d] = tau[3 * j + d];
+      else f.tau[k] = tau[j];
     }
     upward(f); downward(f); return 0;
   })
@@ -860,6 +1215,7 @@ int orc_fmm_upward(void* h) { FMM& f = *(FMM*)h; upward(f); return 0; }
 // evaluate_at_sources! (evaluate.jl:111-127): outputs in the original order
 int orc_fmm_eval_sources(void* h, double* pot, double* grad) {
   FMM& f = *(FMM*)h;
+  if (f.kind == STOKES) { g_err = "a Stokes FMM: use the Stokes outputs"; return 1; }
   int N = f.t.N;
 #pragma omp parallel for schedule(dynamic, 256)
   for (int k = 0; k < N; ++k) {
@@ -874,6 +1230,7 @@ int orc_fmm_eval_sources(void* h, double* pot, double* grad) {
 // evaluate! (evaluate.jl:81-96)
 int orc_fmm_eval_targets(void* h, const double* tg, i64 nt, double* pot, double* grad) {
   FMM& f = *(FMM*)h;
+  if (f.kind == STOKES) { g_err = "a Stokes FMM: use the Stokes outputs"; return 1; }
   std::vector<int> node(nt);
   GUARD({ for (i64 q = 0; q < nt; ++q) node[q] = locate(f.t, &tg[3 * q]); })
 #pragma omp parallel for schedule(dynamic, 256)
@@ -885,6 +1242,36 @@ int orc_fmm_eval_targets(void* h, const double* tg, i64 nt, double* pot, double*
   }
   return 0;
 }
+// the Stokes outputs (velocity N × 3, pressure N) at the sources, self excluded, original order
+int orc_fmm_eval_sources_stokes(void* h, double* vel, double* pres) {
+  FMM& f = *(FMM*)h;
+  if (f.kind != STOKES) { g_err = "not a Stokes FMM"; return 1; }
+  int N = f.t.N;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int k = 0; k < N; ++k) {
+    double u[3], pr;
+    stokes_evaluate_target(f, &f.xs[3 * k], f.t.point_node[k], k, u, &pr);
+    int j = f.t.perm[k];
+    if (vel) { vel[3 * j] = u[0]; vel[3 * j + 1] = u[1]; vel[3 * j + 2] = u[2]; }
+    if (pres) pres[j] = pr;
+  }
+  return 0;
+}
+int orc_fmm_eval_targets_stokes(void* h, const double* tg, i64 nt, double* vel, double* pres) {
+  FMM& f = *(FMM*)h;
+  if (f.kind != STOKES) { g_err = "not a Stokes FMM"; return 1; }
+  std::vector<int> node(nt);
+  GUARD({ for (i64 q = 0; q < nt; ++q) node[q] = locate(f.t, &tg[3 * q]); })
+#pragma omp parallel for schedule(dynamic, 256)
+  for (i64 q = 0; q < nt; ++q) {
+    double u[3], pr;
+    stokes_evaluate_target(f, &tg[3 * q], node[q], -1, u, &pr);
+    if (vel) { vel[3 * q] = u[0]; vel[3 * q + 1] = u[1]; vel[3 * q + 2] = u[2]; }
+    if (pres) pres[q] = pr;
+  }
+  return 0;
+}
+int orc_fmm_nblocks(void* h) { return ((FMM*)h)->nb; }
 int orc_fmm_locate(void* h, const double* tg, i64 nt, int32_t* node) {
   FMM& f = *(FMM*)h;
   GUARD({ for (i64 q = 0; q < nt; ++q) node[q] = locate(f.t, &tg[3 * q]); return 0; })
@@ -939,6 +1326,14 @@ int orc_harmonic_classes(int p, int32_t* cls, int32_t* reps, int32_t* idx, int8_
   return (int)sc.reps.size();
 }
 void orc_far_offsets(int32_t* out) { std::vector<I3> o = far_offsets(); for (int f = 0; f < NFAR; ++f) for (int d = 0; d < 3; ++d) out[3 * f + d] = o[f].v[d]; }
+
+// ---- Yukawa pieces (for the known-answer tests of harmonics_yukawa.jl)
+void orc_yukawa_uv(double z, int nmax, double* u, double* v) { yukawa_u(z * z, nmax, u); yukawa_v(z, nmax, v); }
+void orc_yukawa_bases(const double* y, const double* x, double kappa, int p, double* br, double* bi) {
+  Tables tb = harmonic_tables(p);
+  yukawa_regular(br, y, kappa, p, tb);
+  yukawa_irregular(bi, x, kappa, p, tb);
+}
 
 // ---- direct sums (kernels.jl:442-487): self excludes the target's own index
 void orc_direct(const double* src, const double* tau, i64 ns, const double* tg, i64 nt, int self, double* pot, double* grad) {

@@ -1,8 +1,9 @@
 """ctypes binding of the CPU oracle (test infrastructure only).
 
-The oracle restates the reference CPU path of FlexibleFMM.jl for Laplace3D
-`SphericalHarmonics` (src/tree/*.jl, src/operators/harmonics.jl, symmetry.jl,
-src/fmm.jl, src/evaluate.jl, src/kernels.jl). Only the tests, the smoke check and
+The oracle restates the reference CPU path of FlexibleFMM.jl for the harmonic methods:
+`SphericalHarmonics` of Laplace3D (src/tree/*.jl, src/operators/harmonics.jl, symmetry.jl,
+src/fmm.jl, src/evaluate.jl, src/kernels.jl) and of Yukawa3D (harmonics_yukawa.jl), and
+`StokesHarmonics` of Stokeslet3D (harmonics_stokes.jl). Only the tests, the smoke check and
 the CPU baseline of the benchmark import this module; the product never does.
 Node and point indices here are 0-based (-1 for "none"), levels 0-based (root 0).
 """
@@ -56,6 +57,11 @@ def lib():
     L.orc_tree_npairs.restype = C.c_int64
     L.orc_tree_pairs.argtypes = [C.c_void_p, C.c_int, i32p, i32p, i32p]
     L.orc_fmm_create.argtypes = [C.c_int, f64p, C.c_int64, C.c_int, f64p, C.c_double, C.c_int, C.c_double, C.POINTER(C.c_void_p)]
+    L.orc_fmm_create_kind.argtypes = [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, f64p, C.c_int64, C.c_int,
+                                      f64p, C.c_double, C.c_int, C.c_double, C.POINTER(C.c_void_p)]
+    L.orc_fmm_eval_sources_stokes.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_fmm_eval_targets_stokes.argtypes = [C.c_void_p, f64p, C.c_int64, C.c_void_p, C.c_void_p]
+    L.orc_fmm_nblocks.argtypes = [C.c_void_p]
     L.orc_fmm_free.argtypes = [C.c_void_p]
     L.orc_fmm_tree.argtypes = [C.c_void_p]
     L.orc_fmm_tree.restype = C.c_void_p
@@ -73,6 +79,8 @@ def lib():
     L.orc_harmonic_m2l.argtypes = [i32p, C.c_int, C.c_double, f64p]
     L.orc_harmonic_classes.argtypes = [C.c_int, i32p, i32p, i32p, i8p, i32p, i8p]
     L.orc_far_offsets.argtypes = [i32p]
+    L.orc_yukawa_uv.argtypes = [C.c_double, C.c_int, f64p, f64p]
+    L.orc_yukawa_bases.argtypes = [f64p, f64p, C.c_double, C.c_int, f64p, f64p]
     L.orc_direct.argtypes = [f64p, f64p, C.c_int64, f64p, C.c_int64, C.c_int, C.c_void_p, C.c_void_p]
     L.orc_direct_sample.argtypes = [f64p, f64p, C.c_int64, i64p, C.c_int64, C.c_void_p, C.c_void_p]
     _lib = L
@@ -164,24 +172,63 @@ class Tree:
 
 
 # ---------------------------------------------------------------- FMM
-class FMM:
-    """FMM(SphericalHarmonics(Laplace3D(); p), sources; ppl, bbox) with build_expansions and evaluation."""
+def gauss_legendre(n):
+    """The Gauss–Legendre rule on [−1, 1] by the Golub–Welsch eigenvalues of the Jacobi matrix,
+    as src/operators/harmonics_yukawa.jl:89-93 computes it (LAPACK through numpy): nodes
+    ascending, weights 2 v₁²."""
+    k = np.arange(1, n)
+    beta = k / np.sqrt(4.0 * k * k - 1)
+    J = np.diag(beta, 1) + np.diag(beta, -1)
+    t, V = np.linalg.eigh(J)
+    return np.ascontiguousarray(t), np.ascontiguousarray(2 * V[0, :] ** 2)
 
-    def __init__(self, p, xyz, ppl, origin=(0.0, 0.0, 0.0), width=1.0, max_levels=30, ref_width=0.0):
+
+KINDS = {"laplace": 0, "yukawa": 1, "stokes": 2}
+
+
+class FMM:
+    """FMM(method, sources; ppl, bbox) with build_expansions and evaluation, for the harmonic
+    methods: kernel "laplace" (SphericalHarmonics(Laplace3D())), "yukawa" (SphericalHarmonics(
+    Yukawa3D(kappa))) or "stokes" (StokesHarmonics(Stokeslet3D()): forces (N, 3), velocity and
+    pressure outputs)."""
+
+    def __init__(self, p, xyz, ppl, origin=(0.0, 0.0, 0.0), width=1.0, max_levels=30, ref_width=0.0, kernel="laplace",
+                 kappa=0.0):
         x = _pts(xyz)
         h = C.c_void_p()
-        _check(lib().orc_fmm_create(int(p), x, x.shape[0], int(ppl), np.asarray(origin, np.float64), float(width),
-                                    int(max_levels), float(ref_width), C.byref(h)))
+        self.kernel = kernel
+        if kernel == "laplace":
+            _check(lib().orc_fmm_create(int(p), x, x.shape[0], int(ppl), np.asarray(origin, np.float64), float(width),
+                                        int(max_levels), float(ref_width), C.byref(h)))
+        else:
+            gt, gw = gauss_legendre(2 * p + 10)
+            _check(lib().orc_fmm_create_kind(KINDS[kernel], int(p), float(kappa), _ptr(gt), _ptr(gw), len(gt), x,
+                                             x.shape[0], int(ppl), np.asarray(origin, np.float64), float(width),
+                                             int(max_levels), float(ref_width), C.byref(h)))
         self._h = h
         self.p = p
         self.np_ = lib().orc_fmm_np(self._h)
+        self.nb = lib().orc_fmm_nblocks(self._h)
         self.tree = Tree(C.c_void_p(lib().orc_fmm_tree(self._h)), owner=False)
         self.N = x.shape[0]
 
     def build_expansions(self, xyz, tau):
         x = _pts(xyz)
         t = np.ascontiguousarray(tau, dtype=np.float64)
+        assert t.shape == ((self.N, 3) if self.kernel == "stokes" else (self.N,))
         _check(lib().orc_fmm_build(self._h, x, t))
+
+    def evaluate_at_sources_stokes(self):
+        """(velocity (N, 3), pressure (N,)) at the sources, each source's own term excluded."""
+        vel, pres = np.zeros((self.N, 3)), np.zeros(self.N)
+        _check(lib().orc_fmm_eval_sources_stokes(self._h, _ptr(vel), _ptr(pres)))
+        return vel, pres
+
+    def evaluate_stokes(self, targets):
+        tg = _pts(targets)
+        vel, pres = np.zeros((tg.shape[0], 3)), np.zeros(tg.shape[0])
+        _check(lib().orc_fmm_eval_targets_stokes(self._h, tg, tg.shape[0], _ptr(vel), _ptr(pres)))
+        return vel, pres
 
     def evaluate_at_sources(self, potential=True, gradient=True):
         pot = np.zeros(self.N) if potential else None
@@ -204,10 +251,11 @@ class FMM:
         return out
 
     def expansions(self):
-        """(multipoles, locals) as (nnodes, (p+1)^2) arrays in node order."""
+        """(multipoles, locals) as (nnodes, nblocks·(p+1)^2) arrays in node order (Stokes: the blocks
+        Φ₁, Φ₂, Φ₃, Ψ̂ one after the other)."""
         n = self.tree.n
-        M = np.zeros((n, self.np_))
-        Lc = np.zeros((n, self.np_))
+        M = np.zeros((n, self.nb * self.np_))
+        Lc = np.zeros((n, self.nb * self.np_))
         lib().orc_fmm_expansions(self._h, _ptr(M), _ptr(Lc))
         return M, Lc
 
@@ -298,3 +346,18 @@ def direct_sample(src, tau, sel, potential=True, gradient=True):
     grad = np.zeros((len(sel), 3)) if gradient else None
     lib().orc_direct_sample(s, t, s.shape[0], sel, len(sel), _ptr(pot), _ptr(grad))
     return pot, grad
+
+
+def yukawa_radial(z, nmax):
+    """(u_n(z), v_n(z)) for n = 0..nmax (src/operators/harmonics_yukawa.jl:44-73)."""
+    u, v = np.zeros(nmax + 1), np.zeros(nmax + 1)
+    lib().orc_yukawa_uv(float(z), int(nmax), u, v)
+    return u, v
+
+
+def yukawa_bases(y, x, kappa, p):
+    """The real regular basis at y and the real irregular basis at x (harmonics_yukawa.jl:111-142)."""
+    N = (p + 1) ** 2
+    br, bi = np.zeros(N), np.zeros(N)
+    lib().orc_yukawa_bases(np.asarray(y, np.float64), np.asarray(x, np.float64), float(kappa), int(p), br, bi)
+    return br, bi

@@ -248,3 +248,36 @@ def test_velocity_gradient(fmmb, dist):
         if dens is f:
             tr = np.abs(np.trace(gt, axis1=1, axis2=2))
             assert np.max(tr) < 1e-4 * np.max(np.linalg.norm(gt, axis=(1, 2)))
+
+
+ST_PARITY = [("uniform", 20000, 64, 12, 71), ("sphere", 20000, 64, 16, 72), ("helix", 8000, 30, 8, 73)]
+
+
+@pytest.mark.parametrize("name,n,ppl,p,seed", ST_PARITY)
+def test_stokes_fp64_path_matches_oracle(oracle, fmmb, name, n, ppl, p, seed):
+    """The device's Stokes harmonics against the oracle's restatement of harmonics_stokes.jl
+    on the same box and tree: the four expansion blocks of every node (multipoles and leaf
+    locals), the velocities and pressures at the sources and at targets, max-norm relative."""
+    from helpers import DISTRIBUTIONS3
+    rng = np.random.default_rng(seed)
+    pts = sphere_points(rng, n) if name == "sphere" else DISTRIBUTIONS3[name](rng, n)
+    f = rng.standard_normal((n, 3))
+    plan = fmmb.StokesFMMPlan(pts, p=p, ppl=ppl)
+    lo = plan.fmm.origin
+    O = oracle.FMM(p, pts, ppl, origin=tuple(lo), width=plan.fmm.width, kernel="stokes")
+    assert plan.fmm.nnodes == O.tree.n and plan.fmm.nlevels >= 4
+    O.build_expansions(pts, f)
+    ov, op = O.evaluate_at_sources_stokes()
+    u = fmmb.stokes_fmm_eval(plan, f)
+    pr = fmmb.stokes_fmm_eval(plan, f, output="pressure")
+    M, Lc = plan.state.expansions()
+    OM, OL = O.expansions()
+    M, Lc = M.reshape(OM.shape), Lc.reshape(OL.shape)
+    assert np.max(np.abs(M - OM)) < 1e-12 * np.max(np.abs(OM))
+    assert np.max(np.abs(Lc - OL)) < 1e-11 * np.max(np.abs(OL))
+    assert mrd(u, ov) < 1e-12 and mrd(pr, op) < 1e-11
+    tg = pts[rng.choice(n, 300, replace=False)] + 1e-3 * rng.standard_normal((300, 3))
+    tg = np.clip(tg, lo + 1e-9, lo + plan.fmm.width - 1e-9)
+    tv, tp = O.evaluate_stokes(tg)
+    assert mrd(fmmb.stokes_fmm_eval(plan, f, targets=tg), tv) < 1e-12
+    assert mrd(fmmb.stokes_fmm_eval(plan, f, targets=tg, output="pressure"), tp) < 1e-11
