@@ -219,7 +219,7 @@ void check_outputs(int outputs) {
   require(outputs >= 1 && outputs <= 3, FMMB_ERR_ARGUMENT, "outputs must be POTENTIAL, GRADIENT or both");
 }
 
-// after a synchronisation: a bounded device wait that gave up is reported as a timeout
+// after a synchronisation: a bounded device wait that gave up is reported (once) as a timeout
 void check_state_errors(State& S) {
   if (S.precision == FMMB_PRECISION_MIXED && mixed_error_flag(S))
     throw Error(FMMB_ERR_TIMEOUT, "a bounded wait of the tensor-core M2L gave up; the expansions are incomplete");
@@ -687,6 +687,21 @@ int fmmb_matvec_dev(fmmb_state* state, const double* xyz, const double* tau, int
     if (outputs & FMMB_OUTPUT_GRADIENT) require_device_ptr(*S.plan->ctx, grad, "gradient output");
     matvec_sources(S, xyz, tau, outputs, pot, grad);
   });
+}
+
+int fmmb_state_synchronize(fmmb_state* state) {
+  return guard([&] {
+    require(state != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    State& S = state->s;
+    set_device(*S.plan->ctx);
+    if (S.side.s) FMMB_CUDA(cudaStreamSynchronize(S.side.s));
+    FMMB_CUDA(cudaStreamSynchronize(S.plan->ctx->stream));
+    check_state_errors(S);
+  });
+}
+
+int fmmb_test_m2l_stall(int64_t slab, double wait_seconds) {
+  return guard([&] { set_m2l_stall((long long)slab, wait_seconds); });
 }
 
 int fmmb_matvec(fmmb_state* state, const double* xyz, const double* tau, int64_t n, int outputs, double* pot, double* grad) {

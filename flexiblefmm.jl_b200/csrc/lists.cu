@@ -69,10 +69,13 @@ __global__ void k_target_fill(const int4* __restrict__ cell, const int* __restri
 }
 
 // one CTA per block, one thread per target: counts per (target, class), the class-major
-// offsets, and the fill
+// offsets, and the fill; for the tensor-core M2L the round table: per class and target its
+// pair count << 16 | its first pair's offset in the class, and per class the largest count
+// (the class's rounds: round r gathers every target's r-th pair of the class)
 __global__ void k_block_fill(const int4* __restrict__ blocks, const int4* __restrict__ cell, const int* __restrict__ parent,
                              const int* __restrict__ cf, const int* __restrict__ col, const uint8_t* __restrict__ flags,
-                             int* __restrict__ cls_off, int2* __restrict__ pairs, int TB) {
+                             int* __restrict__ cls_off, int2* __restrict__ pairs, int TB, int* __restrict__ rtab,
+                             int* __restrict__ rounds) {
   // blockDim.x = max(TB, 64) threads: the class scans below take one thread per class
   extern __shared__ int sm[];
   int* cnt = sm;                 // [NCLASS][TB]
@@ -84,10 +87,14 @@ __global__ void k_block_fill(const int4* __restrict__ blocks, const int4* __rest
   if (t < b.z)
     for_far_pairs(b.y + t, cell, parent, cf, col, flags, [&](int, int f) { cnt[c_class[f] * TB + t]++; });
   __syncthreads();
-  if (t < NCLASS) {        // exclusive scan down each class column
-    int run = 0;
-    for (int q = 0; q < TB; ++q) { int v = cnt[t * TB + q]; cnt[t * TB + q] = run; run += v; }
+  if (t < TB)
+    for (int c = 0; c < NCLASS; ++c) rtab[((int64_t)blockIdx.x * NCLASS + c) * TB + t] = cnt[c * TB + t] << 16;
+  __syncthreads();         // the counts are read above before the scans below overwrite them
+  if (t < NCLASS) {        // exclusive scan down each class column, and the class's largest count
+    int run = 0, mx = 0;
+    for (int q = 0; q < TB; ++q) { int v = cnt[t * TB + q]; cnt[t * TB + q] = run; run += v; mx = max(mx, v); }
     tot[t] = run;
+    rounds[(int64_t)blockIdx.x * NCLASS + t] = mx;
   }
   __syncthreads();
   if (t == 0) {
@@ -97,6 +104,8 @@ __global__ void k_block_fill(const int4* __restrict__ blocks, const int4* __rest
   }
   __syncthreads();
   if (t <= NCLASS) cls_off[(int64_t)blockIdx.x * (NCLASS + 1) + t] = tot[t];
+  if (t < TB)
+    for (int c = 0; c < NCLASS; ++c) rtab[((int64_t)blockIdx.x * NCLASS + c) * TB + t] |= cnt[c * TB + t];
   if (t < b.z) {
     int cur[NCLASS];
 #pragma unroll
@@ -213,10 +222,12 @@ void build_lists(Plan& P) {
   to_device(P.blocks, hb, s);
   P.cls_off.alloc((size_t)std::max(nb, 1) * (NCLASS + 1));
   P.pairs.alloc(std::max<int64_t>(base, 1));
+  P.rtab.alloc((size_t)std::max(nb, 1) * NCLASS * P.TB);
+  P.rounds.alloc((size_t)std::max(nb, 1) * NCLASS);
   if (nb) {
     size_t smem = sizeof(int) * (NCLASS * P.TB + NCLASS + 1);
     k_block_fill<<<nb, std::max(P.TB, 64), smem, s>>>(P.blocks.p, P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p,
-                                                    P.cls_off.p, P.pairs.p, P.TB);
+                                                    P.cls_off.p, P.pairs.p, P.TB, P.rtab.p, P.rounds.p);
     FMMB_LAUNCH_CHECK();
   }
   // per level factors

@@ -1,37 +1,43 @@
 // The mixed path's M2L on the 5th-generation tensor cores (tcgen05, kind::f16).
 //
-// Same work decomposition as the FP64 kernel (one CTA per block of targets, the block's far
-// pairs grouped by symmetry class; src/device_passes.jl:565-580, harmonics.jl:589-645), with
-// the class product on the tensor cores in three-term split precision over FP16:
+// The block decomposition of the FP64 kernel (one CTA per block of ≤ 128 targets, the block's far
+// pairs grouped by symmetry class; src/device_passes.jl:565-580, harmonics.jl:589-645), with the
+// class product on the tensor cores in three-term split precision over FP16:
 //   - every multipole column is scaled by a power of two (per node, so that its largest entry
 //     lies in [2^13, 2^14)) and split into an FP16 head and tail, x·2^e ≈ hi + lo (22
 //     significant bits over FP16's range; the scale keeps every column inside it);
 //   - every row of a class operator is scaled the same way (per class and (n, m) pair of rows);
 //   - A·B ≈ hi(A)·hi(B) + hi(A)·lo(B) + lo(A)·hi(B), accumulated in FP32 in tensor memory;
 //     FP16 products are exact in FP32. The read-back removes both scales (exact powers of two).
-// Orders with (p+1)² ≤ 128 use one 128-row tile of outputs; up to (p+1)² = 144 (p = 11) a
-// second tile covers rows 128..(p+1)²-1.
 //
-// Per CTA, three roles connected by mbarriers over a ring of STAGES (warp specialisation):
-//   - one gather warp per stage builds chunk i (≤ 64 pairs of one class) in B stage i mod
-//     STAGES, so STAGES chunks are gathered at once; in the UMMA K-major canonical layout
-//     (8-row × 16-byte core matrices, no swizzle): 8 consecutive lanes write the 8 pairs of one
-//     core matrix (one 128-byte row of banks), 4 lanes read 64 contiguous bytes of one source
-//     column, and the loads of two groups of 8 pairs are in flight together. The source-side
-//     signed permutation P_sᵀ costs one XOR per word: odd quarter-turn rotations read a second
-//     copy of the multipoles in which the two entries of every odd-order pair are swapped;
+// The product is oriented so that one MMA serves every target of the block: M = 128 is the
+// block's targets (one TMEM lane each), N = (p+1)² rounded to 16 is the output rows, K likewise.
+// A class runs in rounds; round r gathers each target's r-th pair of the class (a zero row where
+// it has fewer), so a target's pairs all land in its own lane and its class sum is a running sum
+// in one thread: D = A·Bᵀ with A = the gathered source multipoles (source-side signed
+// permutation applied) and B = the class operator, resident in shared memory for the class.
+//
+// Per CTA, four roles connected by mbarriers (warp specialisation):
+//   - two setup warps write, per round (alternately), each target's pair (source node, D4h
+//     element, source scale) into a ring of round records;
+//   - gather warps build K-step slabs of A (128 rows × 16 FP16, head and tail, in the UMMA
+//     K-major canonical layout) into a ring: 8 lanes write the 8 rows of one 128-byte core
+//     matrix; odd quarter-turn rotations read a second copy of the multipoles in which the two
+//     entries of every odd-order pair are swapped, and the source-side signs cost one XOR;
 //   - one thread loads the class operator (head and tail, laid out on the host) with one bulk
 //     copy (cp.async.bulk, no tensor map, no multicast) when the class changes, after the
-//     previous class's MMAs completed; then per chunk issues (p+1)²/16 K-steps × tiles × 3 MMAs
-//     (M = 128, N = chunk rounded to 16, K = 16) into accumulator stage s and commits them;
-//   - the read-back warps (thread = output row) load the stage from tensor memory, apply the
-//     target-side permutation P_t (one shuffle), sum the consecutive pairs of each target in
-//     FP32 and add the sum, with both scales and the level factor W_ref/w applied, to the FP64
-//     partial local with a reduction (the block owns its targets and each entry has one
-//     writing thread, so the additions apply in program order: deterministic).
+//     previous class's MMAs completed; then per K-step issues three MMAs (M = 128, N, K = 16)
+//     into one of two accumulator stages in tensor memory;
+//   - read-back warps (thread = target; two warps per TMEM lane quadrant, each half of the
+//     columns) apply the target-side permutation of the pair's element (odd-m entries take their
+//     partner's value for odd rotations, signs by XOR) and the source scale, and add the row into
+//     the target's class sums, kept in tensor memory; at the class's last round they add the sums,
+//     with the row scales and the level factor W_ref/w, to the FP64 partial locals with
+//     reductions, transposed through shared memory so that each covers consecutive rows.
 // Every wait on an mbarrier is bounded and also gives up when another role has given up; the
 // CTA then waits (bounded) for the copies and MMAs it issued, records an error in a device
 // flag, frees its tensor memory and returns; the host turns the flag into FMMB_ERR_TIMEOUT.
+#include <atomic>
 #include <cstring>
 
 #include <cuda_fp16.h>
@@ -42,10 +48,8 @@
 namespace fmmb {
 namespace {
 
-constexpr int NCHK = 64;          // pairs per MMA chunk (the N of the MMA)
 constexpr int CORE = 128;         // bytes of one 8 × 16 B core matrix
 constexpr int NPMAX = 144;        // (p+1)² supported: p ≤ 11
-constexpr int GROUP = 32;         // entries one gather lane octet covers per instruction (4 core columns)
 constexpr unsigned long long SPIN_LIMIT = 1ull << 26;
 constexpr uint64_t WAIT_NS = 1000000000ull;  // one second: a wait in a working pipeline takes microseconds
 constexpr int TMEM_COLS = 512;
@@ -56,17 +60,6 @@ __host__ __device__ constexpr int rows_of(int np) { return np > 128 ? 128 + (np 
 // canonical K-major offset (bytes) of FP16 element (row, k) in a tile with kp columns
 __host__ __device__ __forceinline__ uint32_t canon16(int row, int k, int kp) {
   return (uint32_t)((row >> 3) * (kp / 8) * CORE + (k >> 3) * CORE + (row & 7) * 16 + (k & 7) * 2);
-}
-
-// bit i of x moved to bit 2i
-__device__ __forceinline__ uint64_t spread_bits(uint32_t x32) {
-  uint64_t x = x32;
-  x = (x | (x << 16)) & 0x0000ffff0000ffffull;
-  x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
-  x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
-  x = (x | (x << 2)) & 0x3333333333333333ull;
-  x = (x | (x << 1)) & 0x5555555555555555ull;
-  return x;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -107,8 +100,8 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
   return ok != 0;
 }
 
-// a wait bounded in time (WAIT_NS of the global timer) and in polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// a wait bounded in time (wait_ns of the global timer) and in polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t wait_ns) {
   const uint32_t a = smem_u32(bar);
   uint64_t t0 = 0;
   for (unsigned long long it = 0; it < SPIN_LIMIT; ++it) {
@@ -116,14 +109,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if ((it & 63) == 63) {
       const uint64_t t = global_ns();
       if (t0 == 0) t0 = t;
-      else if (t - t0 > WAIT_NS) return false;
+      else if (t - t0 > wait_ns) return false;
     }
   }
   return false;
 }
 
 // a bounded wait that also gives up when another role aborted
-__device__ __forceinline__ bool mbar_wait_abortable(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+__device__ __forceinline__ bool mbar_wait_abortable(uint64_t* bar, uint32_t parity, volatile int* abort_flag, uint64_t wait_ns) {
   const uint32_t a = smem_u32(bar);
   uint64_t t0 = 0;
   for (unsigned long long it = 0; it < SPIN_LIMIT; ++it) {
@@ -132,7 +125,7 @@ __device__ __forceinline__ bool mbar_wait_abortable(uint64_t* bar, uint32_t pari
       if (*abort_flag) return false;
       const uint64_t t = global_ns();
       if (t0 == 0) t0 = t;
-      else if (t - t0 > WAIT_NS) break;
+      else if (t - t0 > wait_ns) break;
     }
   }
   *abort_flag = 1;
@@ -148,6 +141,11 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
+}
+
+// a reduction without a returned value (an atomicAdd whose result is unused may still wait for one)
+__device__ __forceinline__ void red_add_f64(double* p, double v) {
+  asm volatile("red.global.add.f64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "d"(v) : "memory");
 }
 
 __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
@@ -183,16 +181,6 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
       : "memory");
 }
 
-__device__ __forceinline__ void tmem_st1(uint32_t taddr, float v) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(__float_as_uint(v)) : "memory");
-}
-
-__device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
-  uint32_t r;
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
-  return __uint_as_float(r);
-}
-
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -215,84 +203,215 @@ __host__ __device__ __forceinline__ uint32_t perm_mask(int k, bool target) {
   return mask;
 }
 
-// per chunk: the source scale, D4h element and target of every column; the target runs (bit q
-// of `starts` set where column q begins a run; per run its last column and its target)
-struct __align__(16) PairInfo {
-  float cs[NCHK];
-  float keep[NCHK];  // 0 where the column starts a target run, else 1 (the running sum's factor)
-  int fac[NCHK];     // twice the D4h element (the shift of its code in a row's mask)
-  int tgt[NCHK];
-  int rend[NCHK];
-  int rtgt[NCHK];
-  unsigned long long starts;
-  int n, nruns, split;      // split: the first run start at or after column n/2 (n if none)
+// ---------------------------------------------------------------- the kernel
+// One CTA per block of ≤ 128 targets, one TMEM lane (one row of the MMA's M = 128) per target.
+// The block's far pairs are taken class by class; a class runs in rounds, round r gathering every
+// target's r-th pair of the class (a zero row where a target has fewer), so that each target's
+// pairs land in its own lane and its sum over the class is a per-thread running sum: no sums
+// across lanes, no runs. Per round the product is D = A·Bᵀ with A = the gathered multipoles
+// (128 × K, the pairs' source-side permutation applied) and B = the class operator (N = (p+1)²
+// rounded to 16 rows × K, resident in shared memory for the whole class): one MMA per K-step
+// and split term covers all 128 targets and every output row.
+constexpr int LANES = 128;                 // targets per block tile: the MMA's M
+constexpr int NSLAB = 12;                  // K-step slabs (A operand, 128 rows × 16 FP16, head and tail) in the ring
+constexpr int GW = 8;                      // gather warps
+constexpr int RBQ = 2;                     // read-back warps per TMEM lane quadrant
+constexpr int RBW = 4 * RBQ;               // read-back warps 0..7 (warp w reads lanes 32·(w % 4)..)
+constexpr int W_GATHER = RBW;              // gather warps 8..15
+constexpr int SW = 2;                      // round setup warps (alternate rounds)
+constexpr int W_SETUP = RBW + GW;          // round setup warps 16, 17
+constexpr int W_ISSUE = RBW + GW + SW;     // MMA issuing warp 18
+constexpr int THREADS = 32 * (W_ISSUE + 1);
+
+// one round: per target (lane) the source node of its pair (-1: none), the pair's D4h element
+// and the source's inverse power-of-two scale
+struct __align__(16) RoundRec {
+  int src[LANES];
+  int fac[LANES];
+  float cs[LANES];
 };
 
-template <int KP, int MT>
-struct TcCfg {
+// per 16-row group g of the real storage: the rows whose target-side permutation may swap them
+// with their partner (Re/Im entries of odd order m), and of those the Re rows (partner below them
+// at +1; Im rows take theirs at −1). Odd-m pairs never straddle a multiple of 4, so a row and
+// its partner always share a group.
+__host__ __device__ constexpr int row_n(int k) {
+  int n = 0;
+  while ((n + 1) * (n + 1) <= k) ++n;
+  return n;
+}
+__host__ __device__ constexpr uint32_t swap16(int g) {
+  uint32_t m = 0;
+  for (int e = 0; e < 16; ++e) {
+    const int k = 16 * g + e, r = k - row_n(k) * row_n(k), mm = (r + 1) >> 1;
+    if (r != 0 && (mm & 1)) m |= 1u << e;
+  }
+  return m;
+}
+__host__ __device__ constexpr uint32_t re16(int g) {
+  uint32_t m = 0;
+  for (int e = 0; e < 16; ++e) {
+    const int k = 16 * g + e, r = k - row_n(k) * row_n(k);
+    if (r != 0 && (r & 1)) m |= 1u << e;
+  }
+  return m;
+}
+
+template <int KP>
+struct Cfg {
   static constexpr int KC = KP / 8;                        // 16-byte core columns along K
-  static constexpr int SBO = KC * CORE;                    // bytes between 8-row groups
-  static constexpr int U = (KC + 3) / 4;                   // gather instructions per column and half
-  static constexpr int A_BYTES = 2 * (MT == 1 ? 128 : NPMAX) * KP * 2;   // head + tail of one class
-  static constexpr int B_HALF = NCHK * KP * 2;
-  static constexpr int STAGE_BYTES = 2 * B_HALF;
-  static constexpr int STAGES = MT == 1 ? 4 : 3;
-  // warp roles (a warp reads the tensor-memory lane quadrant warp % 4): read-back warps 0-7 for the
-  // first tile (two per quadrant), for a second tile (p = 11) warps 8 and 12 (its rows lie in
-  // quadrant 0); the issuing warp IW = 16; the other warps gather, GPS per stage
-  static constexpr int NEPI = 8 + 2 * (MT - 1);            // read-back warps
-  static constexpr int GPS = 2;                            // gather warps per stage
-  static constexpr int IW = 16;
-  static constexpr int THREADS = 32 * (IW + 1);
-  static_assert(NEPI + STAGES * GPS + 1 == IW + 1, "warp roles");
-  // the gather index of warp w (not a read-back or the issuing warp)
-  __device__ static int gather_index(int w) { return MT == 1 ? w - 8 : (w < 12 ? w - 9 : w - 10); }
-  static constexpr int B_OFF = (A_BYTES + 1023) / 1024 * 1024;
-  static constexpr int PI_OFF = B_OFF + STAGES * STAGE_BYTES;
-  static constexpr int SGN_OFF = PI_OFF + STAGES * (int)sizeof(PairInfo);
+  static constexpr int KS = KP / 16;                       // K-steps of 16
+  // round records in the ring. A gather warp may work up to (NSLAB + KS − 2) / KS rounds ahead
+  // of the oldest unconsumed slab's round; the ring must be longer than that, or a wait on a
+  // record's phase parity could see the record's previous-but-one phase as complete
+  static constexpr int NREC_MIN = (NSLAB + KS - 2) / KS + 2;
+  static constexpr int NREC = NREC_MIN > 8 ? NREC_MIN : 8;
+  static constexpr int NG = KP / 16;                       // 16-column groups of an accumulator
+  static constexpr int NW = (KP + 31) / 32;                // 32-row words of the sign masks
+  static constexpr int OPR = KP > 128 ? KP : 128;          // operator rows stored (rows_of)
+  static constexpr int OP_BYTES = 2 * OPR * KP * 2;        // head and tail of one class
+  static constexpr int SLAB_HALF = LANES * 16 * 2;         // one K-step of 128 rows, FP16
+  static constexpr int SLAB = 2 * SLAB_HALF;
+  // TMEM columns: accumulator stage 0 at 0, the class sums at SCOL, stage 1 at D1 (64-aligned)
+  static constexpr int SCOL = (KP + 31) / 32 * 32;
+  static constexpr int D1 = (SCOL + KP + 63) / 64 * 64;
+  static_assert(D1 + KP <= TMEM_COLS, "tensor memory");
+  static constexpr int SLAB_OFF = (OP_BYTES + 1023) / 1024 * 1024;
+  static constexpr int REC_OFF = SLAB_OFF + NSLAB * SLAB;
+  static constexpr int XP_OFF = REC_OFF + NREC * (int)sizeof(RoundRec);   // per read-back warp 32 × 17 floats
+  static constexpr int SGN_OFF = XP_OFF + RBW * 32 * 17 * 4;
   static constexpr int D4H_OFF = SGN_OFF + 16 * KC * 16;
-  static constexpr int BAR_OFF = D4H_OFF + NFAR * 4;
-  static constexpr int SMEM = BAR_OFF + (1 + 3 * STAGES) * 8 + 16;
-  static_assert(STAGES * MT * NCHK <= TMEM_COLS, "tensor memory");
+  static constexpr int NEG_OFF = D4H_OFF + NFAR * 4;
+  static constexpr int MSK_OFF = NEG_OFF + NW * 16 * 4;      // swap16, re16 per group
+  static constexpr int BAR_OFF = (MSK_OFF + 2 * NG * 4 + 7) / 8 * 8;
+  // slab full/empty, record full/empty, accumulator full/empty, operator loaded/free
+  static constexpr int NBAR = 2 * NSLAB + 2 * NREC + 4 + 2;
+  static constexpr int SMEM = BAR_OFF + NBAR * 8 + 16;
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
-// perm16 (global): KC × 16 × 4 sign words of the source-side permutation (0x8000 in each FP16
-// half that is negated); Mh/Ml: two copies of the split multipoles vstride apart, the second
-// with the two entries of every odd-order pair swapped (what odd quarter-turns read)
-template <int KP, int MT>
-__global__ void __launch_bounds__(TcCfg<KP, MT>::THREADS, 1)
+// the read-back of one round for column groups [g0, g1) of lane quadrant q: the accumulator row
+// of this lane's pair, the target-side permutation of its D4h element (rot: odd-m entries take
+// their partner's value; s_neg: the negated rows per element), times the source scale, into the
+// class sums;
+// sw/re: per group the swappable rows and the Re rows among them (swap16, re16)
+template <int KP>
+__device__ __forceinline__ void rb_round(uint32_t tq, int g0, int g1, int d, bool first, bool rot, const uint32_t* s_neg, int fac,
+                                         float cs, const uint32_t* sw, const uint32_t* re) {
+  using G = Cfg<KP>;
+#pragma unroll 1
+  for (int g = g0; g < g1; ++g) {
+    const uint32_t SW = rot ? sw[g] : 0u, RE = re[g];
+    float dv[16], sv[16];
+    tmem_ld16(tq + (uint32_t)((d ? G::D1 : 0) + 16 * g), dv);
+    if (!first) tmem_ld16(tq + (uint32_t)(G::SCOL + 16 * g), sv);
+    tmem_wait_ld();
+    const uint32_t nw = s_neg[(g >> 1) * 16 + fac] >> (16 * (g & 1));   // this group's 16 negation bits
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      const float yp = ((RE >> e) & 1u) ? dv[e < 15 ? e + 1 : e] : dv[e > 0 ? e - 1 : e];
+      float y = ((SW >> e) & 1u) ? yp : dv[e];
+      y = __uint_as_float(__float_as_uint(y) ^ ((nw << (31 - e)) & 0x80000000u));
+      sv[e] = first ? y * cs : fmaf(y, cs, sv[e]);
+    }
+    tmem_st16(tq + (uint32_t)(G::SCOL + 16 * g), sv);
+  }
+}
+
+// the class sums of lane quadrant q, column groups [g0, g1): times the row scales and the level
+// factor, added to the targets' FP64 partial locals, transposed through xp so that each
+// reduction covers 16 consecutive rows of two targets
+template <int KP>
+__device__ __forceinline__ void rb_write(uint32_t tq, int g0, int g1, float* xp, int lane, int q, unsigned anymask, int nodes0,
+                                         int count, int NP, int LD, const float* __restrict__ rsc, double alpha,
+                                         double* __restrict__ Pl) {
+  using G = Cfg<KP>;
+#pragma unroll 1
+  for (int g = g0; g < g1; ++g) {
+    float sv[16];
+    tmem_ld16(tq + (uint32_t)(G::SCOL + 16 * g), sv);
+    tmem_wait_ld();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) xp[lane * 17 + e] = sv[e];
+    __syncwarp();
+    const int e = lane & 15, r = 16 * g + e;
+    const double rs = r < NP ? alpha * (double)rsc[r] : 0.0;
+#pragma unroll 4
+    for (int it = 0; it < 16; ++it) {
+      const int t = 2 * it + (lane >> 4), tgt = 32 * q + t;
+      if (!((anymask >> (2 * it)) & 3u)) continue;                 // uniform: neither target had a pair
+      if (((anymask >> t) & 1u) && tgt < count && r < NP)
+        red_add_f64(&Pl[(int64_t)(nodes0 + tgt) * LD + r], rs * (double)xp[t * 17 + e]);
+    }
+    __syncwarp();
+  }
+}
+
+// The launch's control: the bounded waits' time limit, and (tests only) one K-step slab whose
+// gather never reports it full, so that the waits run out and the kernel reports the abort
+struct TcCtl {
+  uint64_t wait_ns;
+  long long stall_slab;     // -1: none
+};
+
+// blocks: (level, first node, count, pair base); cls_off: per block the class offsets of its
+// pairs; rtab/rounds: the round table (per class and target count << 16 | offset; per class the
+// rounds); reps16/row_scale: the class operators (head, tail) and their inverse row scales;
+// perm16: the source-side sign words; Mh/Ml/Msc: the split multipoles (two copies vstride
+// apart) and their inverse scales
+template <int KP>
+__global__ void __launch_bounds__(THREADS, 1)
 k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const int2* __restrict__ pairs,
-         const uint16_t* __restrict__ reps16, const float* __restrict__ row_scale, const uint32_t* __restrict__ perm16,
-         const double* __restrict__ m2l_scale, int NP, int LD, int lo_off, int64_t vstride, const uint16_t* __restrict__ Mh,
-         const uint16_t* __restrict__ Ml, const float* __restrict__ Msc, double* __restrict__ Pl, int* __restrict__ err) {
-  using G = TcCfg<KP, MT>;
+         const int* __restrict__ rtab, const int* __restrict__ rounds, int TB, const uint16_t* __restrict__ reps16,
+         const float* __restrict__ row_scale, const uint32_t* __restrict__ perm16, const double* __restrict__ m2l_scale,
+         int NP, int LD, int lo_off, int64_t vstride, const uint16_t* __restrict__ Mh, const uint16_t* __restrict__ Ml,
+         const float* __restrict__ Msc, double* __restrict__ Pl, int* __restrict__ err, TcCtl ctl) {
+  using G = Cfg<KP>;
   extern __shared__ __align__(1024) unsigned char sm[];
-  unsigned char* sA = sm;                                         // head rows, then the tail at lo_off
-  unsigned char* sB = sm + G::B_OFF;                              // stage s: head at s·STAGE_BYTES, tail after it
-  PairInfo* pinfo = (PairInfo*)(sm + G::PI_OFF);                  // per stage
-  uint4* s_sgn = (uint4*)(sm + G::SGN_OFF);                       // [KC][16]
+  unsigned char* sOp = sm;                                     // class operator: head rows, then the tail at lo_off
+  unsigned char* sSlab = sm + G::SLAB_OFF;                     // slab s: head at s·SLAB, tail after it
+  RoundRec* recs = (RoundRec*)(sm + G::REC_OFF);
+  float* xps = (float*)(sm + G::XP_OFF);
+  uint4* s_sgn = (uint4*)(sm + G::SGN_OFF);                    // [KC][16]
   int* s_d4h = (int*)(sm + G::D4H_OFF);
+  uint32_t* s_neg = (uint32_t*)(sm + G::NEG_OFF);              // [NW][16]: bit r & 31 of word r >> 5, per element
+  uint32_t* s_sw = (uint32_t*)(sm + G::MSK_OFF);               // [NG] swappable rows of each 16-row group
+  uint32_t* s_re = s_sw + G::NG;                               // [NG] their Re rows
   uint64_t* bars = (uint64_t*)(sm + G::BAR_OFF);
-  uint64_t* bar_a = bars;                                         // operator load
-  uint64_t* full = bars + 1;                                      // [STAGES] gathered (32·GPS arrivals)
-  uint64_t* done = bars + 1 + G::STAGES;                          // [STAGES] MMAs complete (commit)
-  uint64_t* tempty = bars + 1 + 2 * G::STAGES;                    // [STAGES] read back (NEPI·32 arrivals)
-  uint32_t* tmem_slot = (uint32_t*)(bars + 1 + 3 * G::STAGES);
+  uint64_t* sfull = bars;                                      // [NSLAB] gathered (1 arrival)
+  uint64_t* sempty = bars + NSLAB;                             // [NSLAB] consumed by the MMAs (commit)
+  uint64_t* rfull = bars + 2 * NSLAB;                          // [G::NREC] written by the setup warp
+  uint64_t* rempty = bars + 2 * NSLAB + G::NREC;                  // [G::NREC] released by the read-back (RBW arrivals)
+  uint64_t* dfull = bars + 2 * NSLAB + 2 * G::NREC;               // [2] accumulator ready (commit)
+  uint64_t* dempty = dfull + 2;                                // [2] accumulator read (RBW arrivals)
+  uint64_t* opfull = dempty + 2;                               // operator loaded (bulk copy)
+  uint64_t* opfree = opfull + 1;                               // the class's MMAs complete (commit)
+  uint32_t* tmem_slot = (uint32_t*)(bars + G::NBAR);
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int4 b = blocks[blockIdx.x];
   const int* co = cls_off + (int64_t)blockIdx.x * (NCLASS + 1);
+  const int* nr = rounds + (int64_t)blockIdx.x * NCLASS;
+  const int* rt = rtab + (int64_t)blockIdx.x * NCLASS * TB;
+  const uint64_t wns = ctl.wait_ns;
 
-  for (int f = tid; f < NFAR; f += G::THREADS) s_d4h[f] = c_d4h[f];
-  for (int e = tid; e < 16 * G::KC; e += G::THREADS) s_sgn[e] = reinterpret_cast<const uint4*>(perm16)[e];
-  if (tid == 0) {
-    mbar_init(bar_a, 1);
-    for (int s = 0; s < G::STAGES; ++s) {
-      mbar_init(&full[s], 32 * G::GPS);
-      mbar_init(&done[s], 1);
-      mbar_init(&tempty[s], 32 * G::NEPI);
+  for (int f = tid; f < NFAR; f += THREADS) s_d4h[f] = c_d4h[f];
+  for (int e = tid; e < 16 * G::KC; e += THREADS) s_sgn[e] = reinterpret_cast<const uint4*>(perm16)[e];
+  for (int g = tid; g < G::NG; g += THREADS) { s_sw[g] = swap16(g); s_re[g] = re16(g); }
+  if (warp < G::NW) {                                          // the target-side negations, one ballot per element
+    const int r = 32 * warp + lane;
+    const uint32_t mask = r < NP ? perm_mask(r, true) : 0u;
+    for (int fac = 0; fac < 16; ++fac) {
+      const unsigned bal = __ballot_sync(0xffffffffu, (mask >> (2 * fac + 1)) & 1u);
+      if (lane == 0) s_neg[warp * 16 + fac] = bal;
     }
+  }
+  if (tid == 0) {
+    for (int s = 0; s < NSLAB; ++s) { mbar_init(&sfull[s], 1); mbar_init(&sempty[s], 1); }
+    for (int s = 0; s < G::NREC; ++s) { mbar_init(&rfull[s], 1); mbar_init(&rempty[s], RBW); }
+    for (int s = 0; s < 2; ++s) { mbar_init(&dfull[s], 1); mbar_init(&dempty[s], RBW); }
+    mbar_init(opfull, 1);
+    mbar_init(opfree, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -306,256 +425,167 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
 
-  const bool reader = warp < 8 || (MT == 2 && (warp == 8 || warp == 12));
-  if (reader) {
-    // ---------------- read back and scatter: thread = output row of tile `tile`
-    // two warps per lane quadrant and tile: one takes the columns before the chunk's split, the
-    // other the rest; the split is a run start, so every entry still has one writer per chunk
-    const int tile = warp < 8 ? 0 : 1;
-    const int half = warp < 8 ? warp >> 2 : (warp == 8 ? 0 : 1), quad = warp & 3;
-    const int row = 128 * tile + 32 * quad + lane;
-    const bool live = row < NP;
+  if (warp < RBW) {
+    // ---------------- read-back: lane quadrant q, one of RBQ ranges of the column groups
+    const int q = warp & 3, part = warp >> 2, j = 32 * q + lane;
+    const int g0 = part * G::NG / RBQ, g1 = (part + 1) * G::NG / RBQ;
+    const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
+    float* xp = xps + warp * 32 * 17;
     const double alpha = m2l_scale[b.x];
-    uint32_t emask = 0;
-    int src_lane = lane;
-    if (live) {
-      int en, em, epart;
-      coef_nmp(row, en, em, epart);
-      emask = perm_mask(row, true);
-      const int partner = epart == 0 ? row : (epart == 1 ? row + 1 : row - 1);
-      src_lane = partner & 31;                       // pairs never straddle a 32-row boundary (p ≤ 11)
-    }
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
-      const int a0 = co[c], a1 = co[c + 1];
-      if (a0 == a1) continue;
-      const double rs = live ? alpha * (double)row_scale[c * NP + row] : 0.0;
-      for (int q0 = a0; q0 < a1; q0 += NCHK, ++i) {
-        const int s = i % G::STAGES;
-        const uint32_t ph = (uint32_t)(i / G::STAGES) & 1;
-        const bool w = mbar_wait_abortable(&full[s], ph, abort_flag) && mbar_wait_abortable(&done[s], ph, abort_flag);
+      const int R = nr[c];
+      bool any = false;
+      for (int r = 0; r < R; ++r, ++i) {
+        const int d = i & 1, rc = i % G::NREC;
+        const bool w = mbar_wait_abortable(&rfull[rc], (uint32_t)(i / G::NREC) & 1, abort_flag, wns) &&
+                       mbar_wait_abortable(&dfull[d], (uint32_t)(i >> 1) & 1, abort_flag, wns);
         if (!__all_sync(0xffffffffu, w)) { ok = false; break; }   // the warp leaves together (tcgen05.ld is warp-wide)
         tc_fence_after();
-        const PairInfo& pi = pinfo[s];
-        const int nc = pi.n;
-        const uint64_t starts = pi.starts;
-        const int lo = half ? pi.split : 0, hi = half ? nc : pi.split;
-        const uint32_t ta = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)((s * MT + tile) * NCHK);
-        // phase 1 (branch-free): per column the permuted, unscaled value, and the running sum of
-        // the column's target run (reset where a run starts), written back in place of the
-        // accumulator columns just read (only this warp's columns: the other half owns the rest)
-        float acc = 0.f;
-#pragma unroll
-        for (int c16 = 0; c16 < NCHK / 16; ++c16) {
-          if (16 * c16 >= hi) break;                      // uniform across the warp
-          if (16 * c16 + 16 <= lo) continue;
-          float d[16], a[16];
-          tmem_ld16(ta + 16 * c16, d);
-          tmem_wait_ld();
-#pragma unroll
-          for (int e4 = 0; e4 < 4; ++e4) {
-            const int4 f4 = reinterpret_cast<const int4*>(pi.fac)[4 * c16 + e4];
-            const float4 c4 = reinterpret_cast<const float4*>(pi.cs)[4 * c16 + e4];
-            const float4 k4 = reinterpret_cast<const float4*>(pi.keep)[4 * c16 + e4];
-            const float kk[4] = {k4.x, k4.y, k4.z, k4.w};
-            const int ff[4] = {f4.x, f4.y, f4.z, f4.w};
-            const float cc[4] = {c4.x, c4.y, c4.z, c4.w};
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const float v = d[4 * e4 + e];
-              const float other = __shfl_sync(0xffffffffu, v, src_lane);
-              const uint32_t code = emask >> ff[e];   // ff = 2·(D4h element): its 2-bit code
-              float y = ((code & 1) ? other : v) * cc[e];
-              y = (code & 2) ? -y : y;
-              acc = fmaf(acc, kk[e], y);   // y where a run starts (0·acc + y), else acc + y
-              a[4 * e4 + e] = acc;
-            }
-          }
-          if (16 * c16 >= lo && (16 * c16 + 16 <= hi || hi == nc)) {
-            tmem_st16(ta + 16 * c16, a);
-          } else {
-#pragma unroll
-            for (int e = 0; e < 16; ++e)
-              if (16 * c16 + e >= lo && 16 * c16 + e < hi) tmem_st1(ta + 16 * c16 + e, a[e]);   // uniform
-          }
-        }
+        const RoundRec& rec = recs[rc];
+        const int fac = rec.fac[j];
+        const float cs = rec.cs[j];
+        any |= rec.src[j] >= 0;
+        rb_round<KP>(tq, g0, g1, d, r == 0, (fac & 1) != 0, s_neg, fac, cs, s_sw, s_re);
         tmem_wait_st();
-        // phase 2: the sum of each run is the scan at its last column; one reduction per run
-        // (the only writer of these entries: the reductions apply in program order)
-        const int k_lo = lo >= 64 ? __popcll(starts) : __popcll(starts & ((1ull << lo) - 1));
-        const int k_hi = hi >= 64 ? __popcll(starts) : __popcll(starts & ((1ull << hi) - 1));
-        for (int k0 = k_lo; k0 < k_hi; k0 += 4) {
-          float v[4];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) v[k] = tmem_ld1(ta + (uint32_t)pi.rend[min(k0 + k, k_hi - 1)]);
-          tmem_wait_ld();
-#pragma unroll
-          for (int k = 0; k < 4; ++k)
-            if (live && k0 + k < k_hi) atomicAdd(&Pl[(int64_t)(b.y + pi.rtgt[k0 + k]) * LD + row], rs * (double)v[k]);
-        }
         tc_fence_before();
-        mbar_arrive(&tempty[s]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&dempty[d]);
+        if (r == R - 1)
+          rb_write<KP>(tq, g0, g1, xp, lane, q, __ballot_sync(0xffffffffu, any), b.y, b.z, NP, LD, row_scale + (size_t)c * NP,
+                       alpha, Pl);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&rempty[rc]);
       }
     }
-  } else if (warp != G::IW) {
-    // ---------------- gather: the GPS warps of stage s build the chunks i ≡ s (mod STAGES), warp h
-    // of them every GPS-th pair of groups; lane octet o = lane & 7 the pairs of a group of 8,
-    // cq = lane >> 3 the core column
-    const int gw = G::gather_index(warp), o = lane & 7, cq = lane >> 3;
-    const int s = gw / G::GPS, h = gw % G::GPS;
-    unsigned char* bh = sB + s * G::STAGE_BYTES;
-    PairInfo& pi = pinfo[s];
+  } else if (warp < W_SETUP) {
+    // ---------------- gather: warp gw builds slabs gw, gw + GW, ...: lane (o = lane & 7, sub = lane >> 3)
+    // writes row o of every 8-row group for core column sub & 1 of the K-step, head (sub < 2) or tail
+    const int gw = warp - W_GATHER, o = lane & 7, kc = (lane >> 3) & 1, half = lane >> 4;
+    const uint16_t* Mx = half ? Ml : Mh;
+    int total = 0;
+    for (int c = 0; c < NCLASS; ++c) total += nr[c];
+    const long long nslabs = (long long)total * G::KS;
+    for (long long k = gw; k < nslabs && ok; k += GW) {
+      const int i = (int)(k / G::KS), ks = (int)(k % G::KS), rc = i % G::NREC, s = (int)(k % NSLAB);
+      bool w = mbar_wait_abortable(&rfull[rc], (uint32_t)(i / G::NREC) & 1, abort_flag, wns);
+      if (w && k >= NSLAB) w = mbar_wait_abortable(&sempty[s], (uint32_t)(k / NSLAB - 1) & 1, abort_flag, wns);
+      if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+      const RoundRec& rec = recs[rc];
+      const int kcg = 2 * ks + kc;
+      unsigned char* dst = sSlab + s * G::SLAB + half * G::SLAB_HALF + kc * CORE + o * 16;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        uint4 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int row = 8 * (8 * h + u) + o, src = rec.src[row], fac = rec.fac[row];
+          v[u] = make_uint4(0, 0, 0, 0);
+          if (src >= 0) {
+            // odd quarter-turns read the copy with the odd-order pairs swapped
+            v[u] = __ldcg(reinterpret_cast<const uint4*>(Mx + (int64_t)(fac & 1) * vstride + (int64_t)src * KP) + kcg);
+            const uint4 sg = s_sgn[kcg * 16 + fac];
+            v[u] = make_uint4(v[u].x ^ sg.x, v[u].y ^ sg.y, v[u].z ^ sg.z, v[u].w ^ sg.w);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) *(uint4*)(dst + (8 * h + u) * 256) = v[u];
+      }
+      fence_async_smem();
+      __syncwarp();
+      if (lane == 0 && k != ctl.stall_slab) mbar_arrive(&sfull[s]);
+    }
+  } else if (warp < W_ISSUE) {
+    // ---------------- round setup (warp sw of SW takes rounds i ≡ sw mod SW): per target its r-th
+    // pair of the class, its element and scale
+    const int sw = warp - W_SETUP;
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
-      const int a0 = co[c], a1 = co[c + 1];
-      for (int q0 = a0; q0 < a1; q0 += NCHK, ++i) {
-        if (i % G::STAGES != s) continue;
-        if (i >= G::STAGES) {
-          const bool w = mbar_wait_abortable(&tempty[s], (uint32_t)(i / G::STAGES - 1) & 1, abort_flag);
-          if (!__all_sync(0xffffffffu, w)) { ok = false; break; }   // the warp leaves together (shuffles below)
-        }
-        const int nc = min(NCHK, a1 - q0), ng = (nc + 15) / 16 * 2;   // groups of 8 up to N = nc rounded to 16
-        // the chunk's pairs: lane l holds columns 2l and 2l + 1
-        int srcA = -1, srcB = -1, facA = 0, facB = 0, tA = -1, tB = -1;
-        const bool vA = 2 * lane < nc, vB = 2 * lane + 1 < nc;
-        if (vA) {
-          const int2 pr = pairs[b.w + q0 + 2 * lane];
-          srcA = pr.x;
-          facA = s_d4h[pr.y >> 8];
-          tA = pr.y & 0xff;
-        }
-        if (vB) {
-          const int2 pr = pairs[b.w + q0 + 2 * lane + 1];
-          srcB = pr.x;
-          facB = s_d4h[pr.y >> 8];
-          tB = pr.y & 0xff;
-        }
-        if (h == 0) {                                   // the first warp of the stage records the chunk
-          if (vA) { pi.fac[2 * lane] = 2 * facA; pi.tgt[2 * lane] = tA; }
-          if (vB) { pi.fac[2 * lane + 1] = 2 * facB; pi.tgt[2 * lane + 1] = tB; }
-          // the target runs of the chunk (pairs are sorted by target within a class)
-          const int tprev = __shfl_up_sync(0xffffffffu, tB, 1);
-          const bool stA = vA && (lane == 0 || tA != tprev), stB = vB && tB != tA;
-          if (vA) pi.keep[2 * lane] = stA ? 0.f : 1.f;
-          if (vB) pi.keep[2 * lane + 1] = stB ? 0.f : 1.f;
-          const uint64_t starts = spread_bits(__ballot_sync(0xffffffffu, stA)) | (spread_bits(__ballot_sync(0xffffffffu, stB)) << 1);
-          const bool endA = vA && (2 * lane + 1 == nc || stB);
-          const bool endB = vB && (2 * lane + 2 == nc || ((starts >> (2 * lane + 2)) & 1));
-          if (endA) {
-            const int k = __popcll(starts & ((2ull << (2 * lane)) - 1)) - 1;
-            pi.rend[k] = 2 * lane;
-            pi.rtgt[k] = tA;
-          }
-          if (endB) {
-            const int k = __popcll(starts & ((2ull << (2 * lane + 1)) - 1)) - 1;
-            pi.rend[k] = 2 * lane + 1;
-            pi.rtgt[k] = tB;
-          }
-          if (lane == 0) {
-            const int h = (nc + 1) / 2;
-            const uint64_t later = h >= 64 ? 0ull : starts & (~0ull << h);
-            pi.starts = starts;
-            pi.nruns = __popcll(starts);
-            pi.split = later ? __ffsll((long long)later) - 1 : nc;
-          }
-        }
-        const float csA = srcA >= 0 ? Msc[srcA] : 0.f, csB = srcB >= 0 ? Msc[srcB] : 0.f;
-        for (int g0 = 2 * h; g0 < ng; g0 += 2 * G::GPS) {
-          uint4 vh[2][G::U], vl[2][G::U];
-          int facg[2];
+      const int R = nr[c];
+      int ent[4];
 #pragma unroll
-          for (int gg = 0; gg < 2; ++gg) {
-            const int j = 8 * (g0 + gg) + o;
-            const int s1 = __shfl_sync(0xffffffffu, srcA, j >> 1), s2 = __shfl_sync(0xffffffffu, srcB, j >> 1);
-            const int f1 = __shfl_sync(0xffffffffu, facA, j >> 1), f2 = __shfl_sync(0xffffffffu, facB, j >> 1);
-            const int src = (j & 1) ? s2 : s1;
-            facg[gg] = (j & 1) ? f2 : f1;
-            // odd quarter-turns read the copy with the odd-order pairs swapped
-            const int64_t base = src >= 0 ? (int64_t)(facg[gg] & 1) * vstride + (int64_t)src * KP : 0;
+      for (int u = 0; u < 4; ++u) {
+        const int j = lane + 32 * u;
+        ent[u] = (j < TB && j < b.z) ? rt[c * TB + j] : 0;
+      }
+      for (int r = 0; r < R; ++r, ++i) {
+        if (i % SW != sw) continue;
+        const int rc = i % G::NREC;
+        const bool w = i < G::NREC || mbar_wait_abortable(&rempty[rc], (uint32_t)(i / G::NREC - 1) & 1, abort_flag, wns);
+        if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+        RoundRec& rec = recs[rc];
 #pragma unroll
-            for (int u = 0; u < G::U; ++u) {
-              const int kc = 4 * u + cq;
-              vh[gg][u] = vl[gg][u] = make_uint4(0, 0, 0, 0);
-              if (src >= 0 && kc < G::KC) {
-                vh[gg][u] = __ldg(reinterpret_cast<const uint4*>(Mh + base) + kc);
-                vl[gg][u] = __ldg(reinterpret_cast<const uint4*>(Ml + base) + kc);
-              }
-            }
+        for (int u = 0; u < 4; ++u) {
+          const int j = lane + 32 * u;
+          int src = -1, fac = 0;
+          float cs = 0.f;
+          if (r < (ent[u] >> 16)) {
+            const int2 pr = pairs[b.w + co[c] + (ent[u] & 0xffff) + r];
+            src = pr.x;
+            fac = s_d4h[pr.y >> 8];
+            cs = Msc[src];
           }
-#pragma unroll
-          for (int gg = 0; gg < 2; ++gg) {
-            const int j = 8 * (g0 + gg) + o;
-#pragma unroll
-            for (int u = 0; u < G::U; ++u) {
-              const int kc = 4 * u + cq;
-              if (kc >= G::KC) continue;
-              const uint4 sg = s_sgn[kc * 16 + facg[gg]];
-              const uint32_t off = canon16(j, 8 * kc, KP);
-              *(uint4*)(bh + off) = make_uint4(vh[gg][u].x ^ sg.x, vh[gg][u].y ^ sg.y, vh[gg][u].z ^ sg.z, vh[gg][u].w ^ sg.w);
-              *(uint4*)(bh + G::B_HALF + off) = make_uint4(vl[gg][u].x ^ sg.x, vl[gg][u].y ^ sg.y, vl[gg][u].z ^ sg.z, vl[gg][u].w ^ sg.w);
-            }
-          }
+          rec.src[j] = src;
+          rec.fac[j] = fac;
+          rec.cs[j] = cs;
         }
-        if (h == 0) {
-          if (2 * lane < nc) pi.cs[2 * lane] = csA;
-          if (2 * lane + 1 < nc) pi.cs[2 * lane + 1] = csB;
-          if (lane == 0) pi.n = nc;
-        }
-        fence_async_smem();
         __syncwarp();
-        mbar_arrive(&full[s]);
+        if (lane == 0) mbar_arrive(&rfull[rc]);
       }
     }
   } else if (lane == 0) {
-    // ---------------- issue: the class operator when the class changes, then the chunk's MMAs
+    // ---------------- issue: the class operator when the class changes, then per round and K-step
+    // three MMAs (head·head, head·tail, tail·head) of M = 128 targets, N = KP rows, K = 16
     int i = 0, ncls = 0;
+    long long k = 0;
     bool a_pending = false;
+    uint64_t* last_bar = nullptr;                              // the barrier of the last commit, and its parity
+    uint32_t last_par = 0;
+    const uint32_t idesc = instr_desc(KP, 128);
     for (int c = 0; c < NCLASS && ok; ++c) {
-      const int a0 = co[c], a1 = co[c + 1];
-      if (a0 == a1) continue;
+      const int R = nr[c];
+      if (R == 0) continue;
       // the previous class's MMAs must have completed before its operator is replaced
-      if (i > 0 && !mbar_wait_abortable(&done[(i - 1) % G::STAGES], (uint32_t)((i - 1) / G::STAGES) & 1, abort_flag)) {
-        ok = false;
-        break;
-      }
-      bulk_load(sA, reps16 + (size_t)c * lo_off, 2u * (uint32_t)lo_off, bar_a);   // lo_off bytes = lo_off/2 elements per half
+      if (ncls > 0 && !mbar_wait_abortable(opfree, (uint32_t)(ncls - 1) & 1, abort_flag, wns)) { ok = false; break; }
+      bulk_load(sOp, reps16 + (size_t)c * lo_off, 2u * (uint32_t)lo_off, opfull);   // lo_off bytes = lo_off/2 elements per half
       a_pending = true;
-      if (!mbar_wait_abortable(bar_a, (uint32_t)ncls & 1, abort_flag)) { ok = false; break; }
+      if (!mbar_wait_abortable(opfull, (uint32_t)ncls & 1, abort_flag, wns)) { ok = false; break; }
       a_pending = false;
-      ++ncls;
-      for (int q0 = a0; q0 < a1; q0 += NCHK, ++i) {
-        const int s = i % G::STAGES;
-        const uint32_t ph = (uint32_t)(i / G::STAGES) & 1;
-        if (!mbar_wait_abortable(&full[s], ph, abort_flag)) { ok = false; break; }
-        if (i >= G::STAGES && !mbar_wait_abortable(&tempty[s], ph ^ 1, abort_flag)) { ok = false; break; }
-        tc_fence_after();
-        const int nn = (pinfo[s].n + 15) & ~15;
-        // the second tile holds rows 128..(p+1)²-1 (16 at p = 11): M = 64 halves its tensor time;
-        // its rows 0-15 sit in lanes 0-15 of the first lane quadrant, as with M = 128
-        const uint32_t id = instr_desc(nn), id1 = instr_desc(nn, 64);
-        const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB + s * G::STAGE_BYTES);
-#pragma unroll 2
-        for (int ks = 0; ks < KP / 16; ++ks) {
-          const uint32_t ko = (uint32_t)ks * 2 * CORE;   // 16 FP16 along K: two core matrices
-          const uint64_t dbh = umma_desc(b_base + ko, G::SBO), dbl = umma_desc(b_base + G::B_HALF + ko, G::SBO);
-#pragma unroll
-          for (int t = 0; t < MT; ++t) {
-            const uint32_t ah = a_base + (uint32_t)(t * 16 * G::SBO) + ko;
-            const uint64_t dah = umma_desc(ah, G::SBO), dal = umma_desc(ah + (uint32_t)lo_off, G::SBO);
-            const uint32_t td = tmem + (uint32_t)((s * MT + t) * NCHK);
-            const uint32_t it = t == 0 ? id : id1;
-            mma_f16(td, dah, dbh, it, ks > 0 ? 1u : 0u);
-            mma_f16(td, dah, dbl, it, 1u);
-            mma_f16(td, dal, dbh, it, 1u);
-          }
+      const uint32_t ob = smem_u32(sOp);
+      for (int r = 0; r < R && ok; ++r, ++i) {
+        const int d = i & 1;
+        if (i >= 2 && !mbar_wait_abortable(&dempty[d], (uint32_t)((i >> 1) - 1) & 1, abort_flag, wns)) { ok = false; break; }
+        const uint32_t td = tmem + (uint32_t)(d ? G::D1 : 0);
+        for (int ks = 0; ks < G::KS; ++ks, ++k) {
+          const int s = (int)(k % NSLAB);
+          if (!mbar_wait_abortable(&sfull[s], (uint32_t)(k / NSLAB) & 1, abort_flag, wns)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t ab = smem_u32(sSlab + s * G::SLAB);
+          const uint64_t dah = umma_desc(ab, 256), dal = umma_desc(ab + G::SLAB_HALF, 256);
+          const uint32_t bo = ob + (uint32_t)ks * 2 * CORE;   // 16 FP16 along K: two core matrices
+          const uint64_t dbh = umma_desc(bo, G::KC * CORE), dbl = umma_desc(bo + (uint32_t)lo_off, G::KC * CORE);
+          mma_f16(td, dah, dbh, idesc, ks > 0 ? 1u : 0u);
+          mma_f16(td, dah, dbl, idesc, 1u);
+          mma_f16(td, dal, dbh, idesc, 1u);
+          mma_commit(&sempty[s]);
+          last_bar = &sempty[s];
+          last_par = (uint32_t)(k / NSLAB) & 1;
         }
-        mma_commit(&done[s]);
+        if (!ok) break;
+        mma_commit(&dfull[d]);
+        last_bar = &dfull[d];
+        last_par = (uint32_t)(i >> 1) & 1;
       }
+      if (!ok) break;
+      mma_commit(opfree);
+      last_bar = opfree;
+      last_par = (uint32_t)ncls & 1;
+      ++ncls;
     }
     if (!ok) {
       // give the work already issued a bounded time to finish before the memory is released
-      if (a_pending) mbar_wait(bar_a, (uint32_t)ncls & 1);
-      if (i > 0) mbar_wait(&done[(i - 1) % G::STAGES], (uint32_t)((i - 1) / G::STAGES) & 1);
+      if (a_pending) mbar_wait(opfull, (uint32_t)ncls & 1, wns);
+      if (last_bar) mbar_wait(last_bar, last_par, wns);
     }
   }
   if (!ok) *abort_flag = 1;
@@ -660,12 +690,6 @@ void prepare_mixed_operators(Cache& C) {
   if (C.split_ready) return;
   const int np = C.np;
   require(np <= NPMAX, FMMB_ERR_UNSUPPORTED, "the mixed path is built for p ≤ 11");
-  // the gather's lane octets and the read-back warps exchange partners inside 32 entries
-  for (int k = GROUP; k < np; k += GROUP) {
-    int n, m, part;
-    coef_nmp(k, n, m, part);
-    require(part != 2, FMMB_ERR_UNSUPPORTED, "the mixed path does not support this order");
-  }
   std::vector<uint16_t> h;
   std::vector<float> rsc;
   build_reps16(C.host, h, rsc);
@@ -677,17 +701,29 @@ void prepare_mixed_operators(Cache& C) {
   C.split_ready = true;
 }
 
+// the bounded waits' limit and the test hook's stalled slab, for the next launches
+// (fmmb_test_m2l_stall); process-wide
+static std::atomic<long long> g_stall_slab{-1};
+static std::atomic<uint64_t> g_wait_ns{WAIT_NS};
+
+void set_m2l_stall(long long slab, double wait_s) {
+  g_stall_slab = slab;
+  g_wait_ns = wait_s > 0 ? (uint64_t)(wait_s * 1e9) : WAIT_NS;
+}
+
 namespace {
-template <int KP, int MT>
+template <int KP>
 void launch_tc(State& S, int nb) {
-  using G = TcCfg<KP, MT>;
+  using G = Cfg<KP>;
   Plan& P = *S.plan;
   Cache& C = *P.cache;
   const int lo_off = rows_of(C.np) * KP * 2;
-  FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc<KP, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
-  k_m2l_tc<KP, MT><<<nb, G::THREADS, G::SMEM, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, C.reps16.p, C.row_scale.p,
-                                                               C.perm16.p, P.d_m2l_scale.p, C.np, C.ld, lo_off, (int64_t)P.nnodes * KP, S.Mh.p,
-                                                               S.Ml.p, S.Msc.p, S.Pl.p, S.err.p);
+  require(P.TB <= LANES, FMMB_ERR_UNSUPPORTED, "M2L blocks hold at most 128 targets");
+  FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
+  const TcCtl ctl{g_wait_ns.load(), g_stall_slab.load()};
+  k_m2l_tc<KP><<<nb, THREADS, G::SMEM, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, P.rtab.p, P.rounds.p, P.TB, C.reps16.p,
+                                                        C.row_scale.p, C.perm16.p, P.d_m2l_scale.p, C.np, C.ld, lo_off,
+                                                        (int64_t)P.nnodes * KP, S.Mh.p, S.Ml.p, S.Msc.p, S.Pl.p, S.err.p, ctl);
   FMMB_LAUNCH_CHECK();
 }
 }  // namespace
@@ -702,27 +738,34 @@ void m2l_mixed(State& S) {
   const size_t ne = (size_t)P.nnodes * KP;
   if (S.Mh.n < 2 * ne) { S.Mh.alloc(2 * ne); S.Ml.alloc(2 * ne); }
   if (S.Msc.n < (size_t)P.nnodes) S.Msc.alloc(P.nnodes);
-  if (!S.err.p) S.err.alloc(1);
+  if (!S.err.p) {                                  // sticky until reported (mixed_error_flag clears it)
+    S.err.alloc(1);
+    FMMB_CUDA(cudaMemsetAsync(S.err.p, 0, sizeof(int), s));
+  }
   k_split16<<<(unsigned)(((int64_t)P.nnodes * 32 + 255) / 256), 256, 0, s>>>(S.M.p, P.nnodes, C.np, C.ld, KP, (int64_t)ne, S.Mh.p, S.Ml.p,
                                                                               S.Msc.p);
   FMMB_LAUNCH_CHECK();
-  FMMB_CUDA(cudaMemsetAsync(S.err.p, 0, sizeof(int), s));
   switch (KP) {
-    case 16: launch_tc<16, 1>(S, nb); break;
-    case 32: launch_tc<32, 1>(S, nb); break;
-    case 48: launch_tc<48, 1>(S, nb); break;
-    case 64: launch_tc<64, 1>(S, nb); break;
-    case 96: launch_tc<96, 1>(S, nb); break;
-    case 112: launch_tc<112, 1>(S, nb); break;
-    case 128: launch_tc<128, 1>(S, nb); break;
-    case 144: launch_tc<144, 2>(S, nb); break;
+    case 16: launch_tc<16>(S, nb); break;
+    case 32: launch_tc<32>(S, nb); break;
+    case 48: launch_tc<48>(S, nb); break;
+    case 64: launch_tc<64>(S, nb); break;
+    case 96: launch_tc<96>(S, nb); break;
+    case 112: launch_tc<112>(S, nb); break;
+    case 128: launch_tc<128>(S, nb); break;
+    case 144: launch_tc<144>(S, nb); break;
     default: throw Error(FMMB_ERR_UNSUPPORTED, "the mixed path does not support this order");
   }
 }
 
 int mixed_error_flag(State& S) {
   if (!S.err.p) return 0;
-  return read_one(S.err.p, S.plan->ctx->stream);
+  const int f = read_one(S.err.p, S.plan->ctx->stream);
+  if (f) {
+    FMMB_CUDA(cudaMemsetAsync(S.err.p, 0, sizeof(int), S.plan->ctx->stream));
+    FMMB_CUDA(cudaStreamSynchronize(S.plan->ctx->stream));
+  }
+  return f;
 }
 
 }  // namespace fmmb

@@ -108,6 +108,8 @@ struct Plan {
   DBuf<int4> blocks;
   DBuf<int> cls_off;                      // nblocks × 35, relative to the block's pair_base
   DBuf<int2> pairs;
+  DBuf<int> rtab;                         // nblocks × 34 × TB: per class and target, count << 16 | offset in the class
+  DBuf<int> rounds;                       // nblocks × 34: per class the largest count of a target
   int64_t npairs = 0;
   std::vector<int64_t> level_pairs;       // far pairs per level
   DBuf<double> d_scale, d_m2l_scale;      // per level

@@ -98,7 +98,7 @@ EXPORTS = (
     "fmmb_server_create", "fmmb_server_submit", "fmmb_server_wait", "fmmb_server_destroy", "fmmb_stokes_eval",
     "fmmb_stokes_eval_dev", "fmmb_build_expansions_dipoles", "fmmb_build_expansions_dipoles_dev",
     "fmmb_stokes_eval_densities", "fmmb_stokes_eval_densities_dev", "fmmb_stokes_eval_src_trg",
-    "fmmb_stokes_eval_src_trg_dev",
+    "fmmb_stokes_eval_src_trg_dev", "fmmb_state_synchronize", "fmmb_test_m2l_stall",
 )
 
 
@@ -134,6 +134,8 @@ def lib():
         "fmmb_plan_pairs": [vp, i32, dp, dp, dp, i64, C.POINTER(i64)],
         "fmmb_state_create": [vp, i32, C.POINTER(vp)],
         "fmmb_state_destroy": [vp],
+        "fmmb_state_synchronize": [vp],
+        "fmmb_test_m2l_stall": [i64, C.c_double],
         "fmmb_build_expansions": [vp, dp, dp, i64],
         "fmmb_build_expansions_dev": [vp, dp, dp, i64],
         "fmmb_evaluate_at_sources": [vp, i32, dp, dp],
@@ -483,6 +485,11 @@ class FMMState:
         _check(lib().fmmb_state_expansions(self._h, _ptr(M), _ptr(Lc)))
         return M, Lc
 
+    def synchronize(self):
+        """Wait for the state's device work; raises FMMBError (Timeout) when a bounded wait of
+        the tensor-core M2L gave up since the last report (fmmb_state_synchronize)."""
+        _check(lib().fmmb_state_synchronize(self._h))
+
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.fmmb_state_destroy(self._h)
@@ -791,3 +798,9 @@ def stokes_fmm_eval_src_trg(plan, stokeslets=None, sources=None, stresslets=None
     dens = dict(weights=weights, stokeslets=stokeslets, stresslets=stresslets, stressvecs=stressvecs,
                 doublets=doublets)
     return _stokes_call(plan, sources, targets, True, output, dens)
+
+def _test_m2l_stall(slab, wait_seconds=0.0):
+    """Test hook of the bounded waits (fmmb_test_m2l_stall): the tensor-core M2L launches stop
+    reporting K-step slab `slab` of every block as gathered (-1: back to normal) and wait at most
+    `wait_seconds` (≤ 0: one second) on each barrier."""
+    _check(lib().fmmb_test_m2l_stall(int(slab), float(wait_seconds)))

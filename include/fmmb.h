@@ -144,6 +144,12 @@ int fmmb_matvec_dev(fmmb_state* state, const double* xyz_dev, const double* tau_
  * on the device (src/tree/locate.jl:10-22). */
 int fmmb_evaluate(fmmb_state* state, const double* targets, int64_t nt, int outputs, double* pot, double* grad);
 int fmmb_evaluate_dev(fmmb_state* state, const double* targets_dev, int64_t nt, int outputs, double* pot_dev, double* grad_dev);
+/* Waits for the state's work on the context's stream and reports what its kernels flagged:
+ * FMMB_ERR_TIMEOUT when a bounded wait of the tensor-core M2L gave up since the last report
+ * (the expansions of that build are incomplete). The host-pointer entry points report it
+ * themselves; callers of the _dev entry points call this where they synchronise. No
+ * counterpart in the reference (its calls are synchronous). */
+int fmmb_state_synchronize(fmmb_state* state);
 /* One device matvec (fmmb_matvec_dev) with CUDA events between its stages, on the context's
  * stream, synchronised: stage_ms[0..5] = gather, P2M, M2M, M2L (with the zeroing of the partial
  * locals and, on the mixed path, the FP32 copy of the multipoles), L2L, evaluation (L2P + P2P).
@@ -265,6 +271,13 @@ int fmmb_server_submit(fmmb_server* server, const fmmb_request* request, int64_t
 int fmmb_server_wait(fmmb_server* server, int64_t ticket, double timeout_s, fmmb_request_info* info);
 /* Stops accepting requests, finishes the queued and running ones, then releases everything. */
 int fmmb_server_destroy(fmmb_server* server);
+
+/* Test hook of the bounded waits (no counterpart in the reference): until called again with
+ * slab = -1, the tensor-core M2L launches stop reporting K-step slab number `slab` of every
+ * block as gathered and give each wait `wait_seconds` (default one second when ≤ 0), so that
+ * the waits run out, every role gives up, the kernel frees its tensor memory and returns, and
+ * the next synchronising call reports FMMB_ERR_TIMEOUT. Process-wide; for tests only. */
+int fmmb_test_m2l_stall(int64_t slab, double wait_seconds);
 
 #ifdef __cplusplus
 }

@@ -105,3 +105,41 @@ def test_matvec_equals_build_then_evaluate(fmmb, kernel, precision):
     pot = np.zeros(n)
     fmmb._check(L.fmmb_matvec(st._h, fmmb._ptr(pts), fmmb._ptr(tau), n, 1, fmmb._ptr(pot), None))
     assert np.array_equal(pot, u_ref)
+
+
+def test_bounded_wait_gives_up_and_recovers(fmmb):
+    """The tensor-core M2L's waits are bounded: with the test hook one K-step slab of every block
+    is never reported gathered, so the MMA issuer's wait runs out (20 ms here), every role gives
+    up, the kernel frees its tensor memory and returns, and the call reports a timeout; the same
+    state then recomputes the same result. No fault, trap or endless wait is involved."""
+    import ctypes as C
+    import torch
+    rng = np.random.default_rng(31)
+    n = 30000
+    pts = rng.random((n, 3))
+    tau = rng.standard_normal(n)
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Laplace3D(), p=10), pts, ppl=64, bbox=BOX)
+    st = fmmb.FMMState(f, "mixed")
+    u0 = fmmb.device_matvec(f, st, pts, tau)
+    L = fmmb.lib()
+    try:
+        fmmb._test_m2l_stall(3, 0.02)
+        with pytest.raises(fmmb.FMMBError) as e:                       # host-pointer call: reported at once
+            fmmb.device_matvec(f, st, pts, tau)
+        assert e.value.code == 5
+        # device-pointer call: enqueued without error, reported at the state's synchronisation
+        P = lambda t: C.c_void_p(t.data_ptr())
+        xd, td = torch.from_numpy(pts).cuda(), torch.from_numpy(tau).cuda()
+        pd, gd = torch.zeros(n, dtype=torch.float64, device="cuda"), torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        fmmb._check(L.fmmb_matvec_dev(st._h, P(xd), P(td), n, 3, P(pd), P(gd)))
+        with pytest.raises(fmmb.FMMBError) as e:
+            st.synchronize()
+        assert e.value.code == 5
+        st.synchronize()                                               # reported once
+    finally:
+        fmmb._test_m2l_stall(-1)
+    assert np.array_equal(fmmb.device_matvec(f, st, pts, tau), u0)
+    fmmb._check(L.fmmb_matvec_dev(st._h, P(xd), P(td), n, 1, P(pd), None))
+    st.synchronize()
+    assert np.array_equal(pd.cpu().numpy(), u0)
