@@ -3,9 +3,9 @@
 // The block decomposition of the FP64 kernel (one CTA per block of ≤ 128 targets, the block's far
 // pairs grouped by symmetry class; src/device_passes.jl:565-580, harmonics.jl:589-645), with the
 // class product on the tensor cores in three-term split precision over FP16:
-//   - every multipole column is scaled by a power of two (per node, so that its largest entry
-//     lies in [2^13, 2^14)) and split into an FP16 head and tail, x·2^e ≈ hi + lo (22
-//     significant bits over FP16's range; the scale keeps every column inside it);
+//   - the multipoles of each level are scaled by a power of two (so that the level's largest
+//     entry lies in [2^13, 2^14)) and split into an FP16 head and tail, x·2^e ≈ hi + lo (22
+//     significant bits over FP16's range);
 //   - every row of a class operator is scaled the same way (per class and (n, m) pair of rows);
 //   - A·B ≈ hi(A)·hi(B) + hi(A)·lo(B) + lo(A)·hi(B), accumulated in FP32 in tensor memory;
 //     FP16 products are exact in FP32. The read-back removes both scales (exact powers of two).
@@ -143,6 +143,15 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                : "memory");
 }
 
+// 16 bytes from global memory into shared memory, asynchronously (L2 only); the bytes past
+// src_bytes (0 or 16) are zero-filled
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // a reduction without a returned value (an atomicAdd whose result is unused may still wait for one)
 __device__ __forceinline__ void red_add_f64(double* p, double v) {
   asm volatile("red.global.add.f64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "d"(v) : "memory");
@@ -213,22 +222,20 @@ __host__ __device__ __forceinline__ uint32_t perm_mask(int k, bool target) {
 // rounded to 16 rows × K, resident in shared memory for the whole class): one MMA per K-step
 // and split term covers all 128 targets and every output row.
 constexpr int LANES = 128;                 // targets per block tile: the MMA's M
-constexpr int NSLAB = 12;                  // K-step slabs (A operand, 128 rows × 16 FP16, head and tail) in the ring
+constexpr int RING_KSTEPS = 12;            // K-steps of A staged in the ring (12 × 8 KB)
 constexpr int GW = 8;                      // gather warps
-constexpr int RBQ = 2;                     // read-back warps per TMEM lane quadrant
-constexpr int RBW = 4 * RBQ;               // read-back warps 0..7 (warp w reads lanes 32·(w % 4)..)
-constexpr int W_GATHER = RBW;              // gather warps 8..15
+constexpr int RBQ = 4;                     // read-back warps per TMEM lane quadrant
+constexpr int RBW = 4 * RBQ;               // read-back warps 0..15 (warp w reads lanes 32·(w % 4)..)
+constexpr int W_GATHER = RBW;              // gather warps 16..23
 constexpr int SW = 2;                      // round setup warps (alternate rounds)
-constexpr int W_SETUP = RBW + GW;          // round setup warps 16, 17
-constexpr int W_ISSUE = RBW + GW + SW;     // MMA issuing warp 18
+constexpr int W_SETUP = RBW + GW;          // round setup warps 24, 25
+constexpr int W_ISSUE = RBW + GW + SW;     // MMA issuing warp 26
 constexpr int THREADS = 32 * (W_ISSUE + 1);
 
-// one round: per target (lane) the source node of its pair (-1: none), the pair's D4h element
-// and the source's inverse power-of-two scale
+// one round: per target (lane) the source node of its pair (-1: none) and the pair's D4h element
 struct __align__(16) RoundRec {
   int src[LANES];
   int fac[LANES];
-  float cs[LANES];
 };
 
 // per 16-row group g of the real storage: the rows whose target-side permutation may swap them
@@ -261,17 +268,27 @@ template <int KP>
 struct Cfg {
   static constexpr int KC = KP / 8;                        // 16-byte core columns along K
   static constexpr int KS = KP / 16;                       // K-steps of 16
-  // round records in the ring. A gather warp may work up to (NSLAB + KS − 2) / KS rounds ahead
+  // a slab holds SK K-steps of A (a barrier wait, a fence and a commit per slab cost about as
+  // much as three MMAs, so slabs span up to three K-steps); KS / SK slabs per round
+  static constexpr int SK = KS % 3 == 0 ? 3 : (KS % 2 == 0 ? 2 : 1);
+  static constexpr int SPR = KS / SK;
+  static constexpr int NSLAB = RING_KSTEPS / SK;
+  // gather warps in use: a warp that waits for slab k's buffer (consumed fill k − NSLAB) must
+  // already have seen fill k − 2·NSLAB consumed, or the wait on that barrier's phase parity could
+  // pass a phase early; its previous slab k − NGW waited for k − NGW − NSLAB, so NGW ≤ NSLAB
+  static constexpr int NGW = GW < NSLAB ? GW : NSLAB;
+  // round records in the ring. A gather warp may work up to (RING_KSTEPS + KS − 2) / KS rounds ahead
   // of the oldest unconsumed slab's round; the ring must be longer than that, or a wait on a
   // record's phase parity could see the record's previous-but-one phase as complete
-  static constexpr int NREC_MIN = (NSLAB + KS - 2) / KS + 2;
-  static constexpr int NREC = NREC_MIN > 8 ? NREC_MIN : 8;
+  static constexpr int NREC_MIN = (RING_KSTEPS + KS - 2) / KS + 2;
+  static constexpr int NREC = NREC_MIN > 6 ? NREC_MIN : 6;
   static constexpr int NG = KP / 16;                       // 16-column groups of an accumulator
   static constexpr int NW = (KP + 31) / 32;                // 32-row words of the sign masks
   static constexpr int OPR = KP > 128 ? KP : 128;          // operator rows stored (rows_of)
   static constexpr int OP_BYTES = 2 * OPR * KP * 2;        // head and tail of one class
-  static constexpr int SLAB_HALF = LANES * 16 * 2;         // one K-step of 128 rows, FP16
+  static constexpr int SLAB_HALF = LANES * 16 * 2 * SK;    // SK K-steps of 128 rows, FP16
   static constexpr int SLAB = 2 * SLAB_HALF;
+  static constexpr int SBO_A = 2 * SK * CORE;                // bytes between 8-row groups of a slab
   // TMEM columns: accumulator stage 0 at 0, the class sums at SCOL, stage 1 at D1 (64-aligned)
   static constexpr int SCOL = (KP + 31) / 32 * 32;
   static constexpr int D1 = (SCOL + KP + 63) / 64 * 64;
@@ -295,9 +312,13 @@ struct Cfg {
 // their partner's value; s_neg: the negated rows per element), times the source scale, into the
 // class sums;
 // sw/re: per group the swappable rows and the Re rows among them (swap16, re16)
+// the read-back of one round for column groups [g0, g1) of lane quadrant q: the accumulator row
+// of this lane's pair, the target-side permutation of its D4h element (rot: odd-m entries take
+// their partner's value; s_neg: the negated rows per element), into the class sums; sw/re: per
+// group the swappable rows and the Re rows among them (swap16, re16)
 template <int KP>
 __device__ __forceinline__ void rb_round(uint32_t tq, int g0, int g1, int d, bool first, bool rot, const uint32_t* s_neg, int fac,
-                                         float cs, const uint32_t* sw, const uint32_t* re) {
+                                         const uint32_t* sw, const uint32_t* re) {
   using G = Cfg<KP>;
 #pragma unroll 1
   for (int g = g0; g < g1; ++g) {
@@ -312,7 +333,7 @@ __device__ __forceinline__ void rb_round(uint32_t tq, int g0, int g1, int d, boo
       const float yp = ((RE >> e) & 1u) ? dv[e < 15 ? e + 1 : e] : dv[e > 0 ? e - 1 : e];
       float y = ((SW >> e) & 1u) ? yp : dv[e];
       y = __uint_as_float(__float_as_uint(y) ^ ((nw << (31 - e)) & 0x80000000u));
-      sv[e] = first ? y * cs : fmaf(y, cs, sv[e]);
+      sv[e] = first ? y : sv[e] + y;
     }
     tmem_st16(tq + (uint32_t)(G::SCOL + 16 * g), sv);
   }
@@ -357,15 +378,15 @@ struct TcCtl {
 // blocks: (level, first node, count, pair base); cls_off: per block the class offsets of its
 // pairs; rtab/rounds: the round table (per class and target count << 16 | offset; per class the
 // rounds); reps16/row_scale: the class operators (head, tail) and their inverse row scales;
-// perm16: the source-side sign words; Mh/Ml/Msc: the split multipoles (two copies vstride
-// apart) and their inverse scales
+// perm16: the source-side sign words; Mh/Ml/lsc: the split multipoles (two copies vstride
+// apart) and the inverse scale of each level
 template <int KP>
 __global__ void __launch_bounds__(THREADS, 1)
 k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const int2* __restrict__ pairs,
          const int* __restrict__ rtab, const int* __restrict__ rounds, int TB, const uint16_t* __restrict__ reps16,
          const float* __restrict__ row_scale, const uint32_t* __restrict__ perm16, const double* __restrict__ m2l_scale,
          int NP, int LD, int lo_off, int64_t vstride, const uint16_t* __restrict__ Mh, const uint16_t* __restrict__ Ml,
-         const float* __restrict__ Msc, double* __restrict__ Pl, int* __restrict__ err, TcCtl ctl) {
+         const float* __restrict__ lsc, double* __restrict__ Pl, int* __restrict__ err, TcCtl ctl) {
   using G = Cfg<KP>;
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char* sOp = sm;                                     // class operator: head rows, then the tail at lo_off
@@ -379,10 +400,10 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   uint32_t* s_re = s_sw + G::NG;                               // [NG] their Re rows
   uint64_t* bars = (uint64_t*)(sm + G::BAR_OFF);
   uint64_t* sfull = bars;                                      // [NSLAB] gathered (1 arrival)
-  uint64_t* sempty = bars + NSLAB;                             // [NSLAB] consumed by the MMAs (commit)
-  uint64_t* rfull = bars + 2 * NSLAB;                          // [G::NREC] written by the setup warp
-  uint64_t* rempty = bars + 2 * NSLAB + G::NREC;                  // [G::NREC] released by the read-back (RBW arrivals)
-  uint64_t* dfull = bars + 2 * NSLAB + 2 * G::NREC;               // [2] accumulator ready (commit)
+  uint64_t* sempty = bars + G::NSLAB;                          // [NSLAB] consumed by the MMAs (commit)
+  uint64_t* rfull = sempty + G::NSLAB;                         // [NREC] written by a setup warp
+  uint64_t* rempty = rfull + G::NREC;                          // [NREC] released by the read-back (RBW arrivals)
+  uint64_t* dfull = rempty + G::NREC;                          // [2] accumulator ready (commit)
   uint64_t* dempty = dfull + 2;                                // [2] accumulator read (RBW arrivals)
   uint64_t* opfull = dempty + 2;                               // operator loaded (bulk copy)
   uint64_t* opfree = opfull + 1;                               // the class's MMAs complete (commit)
@@ -407,7 +428,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
     }
   }
   if (tid == 0) {
-    for (int s = 0; s < NSLAB; ++s) { mbar_init(&sfull[s], 1); mbar_init(&sempty[s], 1); }
+    for (int s = 0; s < G::NSLAB; ++s) { mbar_init(&sfull[s], 1); mbar_init(&sempty[s], 1); }
     for (int s = 0; s < G::NREC; ++s) { mbar_init(&rfull[s], 1); mbar_init(&rempty[s], RBW); }
     for (int s = 0; s < 2; ++s) { mbar_init(&dfull[s], 1); mbar_init(&dempty[s], RBW); }
     mbar_init(opfull, 1);
@@ -431,7 +452,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
     const int g0 = part * G::NG / RBQ, g1 = (part + 1) * G::NG / RBQ;
     const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
     float* xp = xps + warp * 32 * 17;
-    const double alpha = m2l_scale[b.x];
+    const double alpha = m2l_scale[b.x] * (double)lsc[b.x];     // the level factor and the multipoles' scale
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
       const int R = nr[c];
@@ -444,9 +465,8 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         tc_fence_after();
         const RoundRec& rec = recs[rc];
         const int fac = rec.fac[j];
-        const float cs = rec.cs[j];
         any |= rec.src[j] >= 0;
-        rb_round<KP>(tq, g0, g1, d, r == 0, (fac & 1) != 0, s_neg, fac, cs, s_sw, s_re);
+        rb_round<KP>(tq, g0, g1, d, r == 0, (fac & 1) != 0, s_neg, fac, s_sw, s_re);
         tmem_wait_st();
         tc_fence_before();
         __syncwarp();
@@ -459,37 +479,46 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
       }
     }
   } else if (warp < W_SETUP) {
-    // ---------------- gather: warp gw builds slabs gw, gw + GW, ...: lane (o = lane & 7, sub = lane >> 3)
+    // ---------------- gather: warp gw builds slabs gw, gw + NGW, ...: lane (o = lane & 7, sub = lane >> 3)
     // writes row o of every 8-row group for core column sub & 1 of the K-step, head (sub < 2) or tail
     const int gw = warp - W_GATHER, o = lane & 7, kc = (lane >> 3) & 1, half = lane >> 4;
     const uint16_t* Mx = half ? Ml : Mh;
     int total = 0;
     for (int c = 0; c < NCLASS; ++c) total += nr[c];
-    const long long nslabs = (long long)total * G::KS;
-    for (long long k = gw; k < nslabs && ok; k += GW) {
-      const int i = (int)(k / G::KS), ks = (int)(k % G::KS), rc = i % G::NREC, s = (int)(k % NSLAB);
+    const long long nslabs = (long long)total * G::SPR;
+    for (long long k = gw; gw < G::NGW && k < nslabs && ok; k += G::NGW) {
+      const int i = (int)(k / G::SPR), ks0 = (int)(k % G::SPR) * G::SK, rc = i % G::NREC, s = (int)(k % G::NSLAB);
       bool w = mbar_wait_abortable(&rfull[rc], (uint32_t)(i / G::NREC) & 1, abort_flag, wns);
-      if (w && k >= NSLAB) w = mbar_wait_abortable(&sempty[s], (uint32_t)(k / NSLAB - 1) & 1, abort_flag, wns);
+      if (w && k >= G::NSLAB) w = mbar_wait_abortable(&sempty[s], (uint32_t)(k / G::NSLAB - 1) & 1, abort_flag, wns);
       if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
       const RoundRec& rec = recs[rc];
-      const int kcg = 2 * ks + kc;
-      unsigned char* dst = sSlab + s * G::SLAB + half * G::SLAB_HALF + kc * CORE + o * 16;
+      unsigned char* dst0 = sSlab + s * G::SLAB + half * G::SLAB_HALF + kc * CORE + o * 16;
+      // the 16 rows' chunks of the slab's K-steps copied asynchronously (zero rows where a target
+      // has no pair), then the source-side signs applied in place; odd quarter-turns read the copy
+      // with the odd-order pairs swapped
+      uint64_t facs = 0;
+      uint32_t valid = 0;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        uint4 v[8];
+      for (int u = 0; u < 16; ++u) {
+        const int row = 8 * u + o, src = rec.src[row], fac = rec.fac[row];
+        facs |= (uint64_t)fac << (4 * u);
+        valid |= (src >= 0 ? 1u : 0u) << u;
+        const uint16_t* g = src >= 0 ? Mx + (int64_t)(fac & 1) * vstride + (int64_t)src * KP + 8 * (2 * ks0 + kc) : Mx;
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int row = 8 * (8 * h + u) + o, src = rec.src[row], fac = rec.fac[row];
-          v[u] = make_uint4(0, 0, 0, 0);
-          if (src >= 0) {
-            // odd quarter-turns read the copy with the odd-order pairs swapped
-            v[u] = __ldcg(reinterpret_cast<const uint4*>(Mx + (int64_t)(fac & 1) * vstride + (int64_t)src * KP) + kcg);
-            const uint4 sg = s_sgn[kcg * 16 + fac];
-            v[u] = make_uint4(v[u].x ^ sg.x, v[u].y ^ sg.y, v[u].z ^ sg.z, v[u].w ^ sg.w);
-          }
+        for (int j = 0; j < G::SK; ++j) cp_async16(dst0 + u * G::SBO_A + j * 2 * CORE, g + (src >= 0 ? 16 * j : 0), src >= 0 ? 16u : 0u);
+      }
+      cp_async_wait_all();
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        if (!((valid >> u) & 1u)) continue;
+        const int fac = (int)((facs >> (4 * u)) & 15);
+#pragma unroll
+        for (int j = 0; j < G::SK; ++j) {
+          uint4* pv = (uint4*)(dst0 + u * G::SBO_A + j * 2 * CORE);
+          const uint4 sg = s_sgn[(2 * (ks0 + j) + kc) * 16 + fac];
+          const uint4 v = *pv;
+          *pv = make_uint4(v.x ^ sg.x, v.y ^ sg.y, v.z ^ sg.z, v.w ^ sg.w);
         }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) *(uint4*)(dst + (8 * h + u) * 256) = v[u];
       }
       fence_async_smem();
       __syncwarp();
@@ -518,16 +547,13 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         for (int u = 0; u < 4; ++u) {
           const int j = lane + 32 * u;
           int src = -1, fac = 0;
-          float cs = 0.f;
           if (r < (ent[u] >> 16)) {
             const int2 pr = pairs[b.w + co[c] + (ent[u] & 0xffff) + r];
             src = pr.x;
             fac = s_d4h[pr.y >> 8];
-            cs = Msc[src];
           }
           rec.src[j] = src;
           rec.fac[j] = fac;
-          rec.cs[j] = cs;
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&rfull[rc]);
@@ -556,20 +582,25 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
         const int d = i & 1;
         if (i >= 2 && !mbar_wait_abortable(&dempty[d], (uint32_t)((i >> 1) - 1) & 1, abort_flag, wns)) { ok = false; break; }
         const uint32_t td = tmem + (uint32_t)(d ? G::D1 : 0);
-        for (int ks = 0; ks < G::KS; ++ks, ++k) {
-          const int s = (int)(k % NSLAB);
-          if (!mbar_wait_abortable(&sfull[s], (uint32_t)(k / NSLAB) & 1, abort_flag, wns)) { ok = false; break; }
+        for (int sl = 0; sl < G::SPR; ++sl, ++k) {
+          const int s = (int)(k % G::NSLAB);
+          if (!mbar_wait_abortable(&sfull[s], (uint32_t)(k / G::NSLAB) & 1, abort_flag, wns)) { ok = false; break; }
           tc_fence_after();
           const uint32_t ab = smem_u32(sSlab + s * G::SLAB);
-          const uint64_t dah = umma_desc(ab, 256), dal = umma_desc(ab + G::SLAB_HALF, 256);
-          const uint32_t bo = ob + (uint32_t)ks * 2 * CORE;   // 16 FP16 along K: two core matrices
-          const uint64_t dbh = umma_desc(bo, G::KC * CORE), dbl = umma_desc(bo + (uint32_t)lo_off, G::KC * CORE);
-          mma_f16(td, dah, dbh, idesc, ks > 0 ? 1u : 0u);
-          mma_f16(td, dah, dbl, idesc, 1u);
-          mma_f16(td, dal, dbh, idesc, 1u);
+#pragma unroll
+          for (int j = 0; j < G::SK; ++j) {
+            const int ks = sl * G::SK + j;
+            const uint32_t aj = ab + (uint32_t)j * 2 * CORE;     // 16 FP16 along K: two core matrices
+            const uint64_t dah = umma_desc(aj, G::SBO_A), dal = umma_desc(aj + G::SLAB_HALF, G::SBO_A);
+            const uint32_t bo = ob + (uint32_t)ks * 2 * CORE;
+            const uint64_t dbh = umma_desc(bo, G::KC * CORE), dbl = umma_desc(bo + (uint32_t)lo_off, G::KC * CORE);
+            mma_f16(td, dah, dbh, idesc, ks > 0 ? 1u : 0u);
+            mma_f16(td, dah, dbl, idesc, 1u);
+            mma_f16(td, dal, dbh, idesc, 1u);
+          }
           mma_commit(&sempty[s]);
           last_bar = &sempty[s];
-          last_par = (uint32_t)(k / NSLAB) & 1;
+          last_par = (uint32_t)(k / G::NSLAB) & 1;
         }
         if (!ok) break;
         mma_commit(&dfull[d]);
@@ -595,24 +626,45 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
-// the multipoles of every node, scaled by a power of two so that the largest entry of the
-// column lies in [2^13, 2^14), as FP16 head and tail (one warp per node), twice: as they are and
-// with the two entries of every odd-order pair swapped (vstride further); Msc = the inverse scale
-__global__ void k_split16(const double* __restrict__ M, int nnodes, int NP, int LD, int KP, int64_t vstride,
-                          uint16_t* __restrict__ Mh, uint16_t* __restrict__ Ml, float* __restrict__ Msc) {
+// the largest |entry| of the multipoles of each level (one warp per node): the bit patterns of
+// non-negative doubles order as integers (a non-finite entry makes its level's maximum
+// non-finite, and the level is then split unscaled)
+__global__ void k_level_absmax(const double* __restrict__ M, const int4* __restrict__ cell, int nnodes, int NP, int LD,
+                               unsigned long long* __restrict__ lvmax) {
   const int node = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (node >= nnodes) return;
   const double* m = M + (int64_t)node * LD;
   double mx = 0.0;
   for (int k = lane; k < NP; k += 32) mx = fmax(mx, fabs(m[k]));
   for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  int e = 0;
-  if (mx > 0.0 && mx <= 1.7e308) {                 // finite and nonzero; otherwise unscaled (0 or non-finite)
-    int ex;
-    frexp(mx, &ex);                                // mx = f·2^ex, f ∈ [0.5, 1)
-    e = 14 - ex;                                   // mx·2^e ∈ [2^13, 2^14)
-    e = max(-100, min(100, e));                    // keeps the inverse scale inside FP32's range
-  }
+  if (lane == 0 && mx != 0.0) atomicMax(&lvmax[cell[node].w], (unsigned long long)__double_as_longlong(mx));
+}
+
+// the exponent e of each level: its largest entry times 2^e lies in [2^13, 2^14); lsc = 2^-e
+__device__ __forceinline__ int level_exponent(unsigned long long bits) {
+  const double mx = __longlong_as_double((long long)bits);
+  if (!(mx > 0.0 && mx <= 1.7e308)) return 0;     // finite and nonzero; otherwise unscaled (0 or non-finite)
+  int ex;
+  frexp(mx, &ex);                                  // mx = f·2^ex, f ∈ [0.5, 1)
+  return max(-100, min(100, 14 - ex));             // keeps the inverse scale inside FP32's range
+}
+__global__ void k_level_scale(const unsigned long long* __restrict__ lvmax, int L, float* __restrict__ lsc) {
+  const int l = threadIdx.x;
+  if (l < L) lsc[l] = (float)ldexp(1.0, -level_exponent(lvmax[l]));
+}
+
+// the multipoles of every node, scaled by its level's power of two, as FP16 head and tail (one
+// warp per node), twice: as they are and with the two entries of every odd-order pair swapped
+// (vstride further). One scale per level keeps the sums of a target's pairs in one scale (no
+// per-pair factor in the read-back); an entry 2^-k of its level's largest keeps 22 significant
+// bits down to k ≈ 17 and an absolute error below 2^-38 of the level's largest entry beyond.
+__global__ void k_split16(const double* __restrict__ M, const int4* __restrict__ cell, int nnodes, int NP, int LD, int KP,
+                          int64_t vstride, const unsigned long long* __restrict__ lvmax, uint16_t* __restrict__ Mh,
+                          uint16_t* __restrict__ Ml) {
+  const int node = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (node >= nnodes) return;
+  const double* m = M + (int64_t)node * LD;
+  const int e = level_exponent(lvmax[cell[node].w]);
   for (int k = lane; k < KP; k += 32) {
     int n, mm, part;
     coef_nmp(k, n, mm, part);
@@ -627,7 +679,6 @@ __global__ void k_split16(const double* __restrict__ M, int nnodes, int NP, int 
       Ml[v * vstride + (int64_t)node * KP + k] = __half_as_ushort(l);
     }
   }
-  if (lane == 0) Msc[node] = (float)ldexp(1.0, -e);
 }
 
 }  // namespace
@@ -723,7 +774,7 @@ void launch_tc(State& S, int nb) {
   const TcCtl ctl{g_wait_ns.load(), g_stall_slab.load()};
   k_m2l_tc<KP><<<nb, THREADS, G::SMEM, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, P.rtab.p, P.rounds.p, P.TB, C.reps16.p,
                                                         C.row_scale.p, C.perm16.p, P.d_m2l_scale.p, C.np, C.ld, lo_off,
-                                                        (int64_t)P.nnodes * KP, S.Mh.p, S.Ml.p, S.Msc.p, S.Pl.p, S.err.p, ctl);
+                                                        (int64_t)P.nnodes * KP, S.Mh.p, S.Ml.p, S.Lsc.p, S.Pl.p, S.err.p, ctl);
   FMMB_LAUNCH_CHECK();
 }
 }  // namespace
@@ -737,13 +788,18 @@ void m2l_mixed(State& S) {
   const int KP = kp_of(C.np);
   const size_t ne = (size_t)P.nnodes * KP;
   if (S.Mh.n < 2 * ne) { S.Mh.alloc(2 * ne); S.Ml.alloc(2 * ne); }
-  if (S.Msc.n < (size_t)P.nnodes) S.Msc.alloc(P.nnodes);
+  if (S.Lsc.n < (size_t)P.L) { S.Lsc.alloc(P.L); S.Lmax.alloc(P.L); }
   if (!S.err.p) {                                  // sticky until reported (mixed_error_flag clears it)
     S.err.alloc(1);
     FMMB_CUDA(cudaMemsetAsync(S.err.p, 0, sizeof(int), s));
   }
-  k_split16<<<(unsigned)(((int64_t)P.nnodes * 32 + 255) / 256), 256, 0, s>>>(S.M.p, P.nnodes, C.np, C.ld, KP, (int64_t)ne, S.Mh.p, S.Ml.p,
-                                                                              S.Msc.p);
+  const unsigned nbk = (unsigned)(((int64_t)P.nnodes * 32 + 255) / 256);
+  FMMB_CUDA(cudaMemsetAsync(S.Lmax.p, 0, sizeof(unsigned long long) * P.L, s));
+  k_level_absmax<<<nbk, 256, 0, s>>>(S.M.p, P.cell.p, P.nnodes, C.np, C.ld, S.Lmax.p);
+  FMMB_LAUNCH_CHECK();
+  k_level_scale<<<1, 64, 0, s>>>(S.Lmax.p, P.L, S.Lsc.p);
+  FMMB_LAUNCH_CHECK();
+  k_split16<<<nbk, 256, 0, s>>>(S.M.p, P.cell.p, P.nnodes, C.np, C.ld, KP, (int64_t)ne, S.Lmax.p, S.Mh.p, S.Ml.p);
   FMMB_LAUNCH_CHECK();
   switch (KP) {
     case 16: launch_tc<16>(S, nb); break;

@@ -625,7 +625,7 @@ int m2l_stage(State& S) {
   if (P.h_blocks.empty()) return 0;
   if (S.precision == FMMB_PRECISION_MIXED) {
     m2l_mixed(S);
-    return 2;
+    return 4;
   }
   m2l_f64(S);
   return 1;

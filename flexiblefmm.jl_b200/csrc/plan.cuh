@@ -142,7 +142,8 @@ struct State {
   bool has_dip = false;                   // the last build had dipoles (the P2M and near field take them)
   DBuf<double> M, Pl;                     // nnodes × LD: multipoles, partial locals
   DBuf<uint16_t> Mh, Ml;                  // the mixed path: the multipoles scaled by a power of two
-  DBuf<float> Msc;                        //   per node, as FP16 head and tail; the inverse scales
+  DBuf<float> Lsc;                        //   per level, as FP16 head and tail; the inverse scales
+  DBuf<unsigned long long> Lmax;          //   and the levels' largest entries
   DBuf<int> err;                          // the mixed path: the bounded-wait error flag
   // the kernel-independent method: check potentials of the childless nodes on their large
   // surfaces, the pseudo-inverses' middle products, the leaves' local densities on their large
