@@ -290,6 +290,7 @@ int fmmb_ctx_create(int device, fmmb_ctx** out) {
     FMMB_CUDA(cudaStreamCreateWithPriority(&h->c.stream, cudaStreamNonBlocking, hi));
     h->c.own_stream = true;
     init_device_constants(h->c.stream);
+    direct_noalloc_prepare();                       // the no-allocation scratch's address, at set-up
     *out = h.release();
   });
 }

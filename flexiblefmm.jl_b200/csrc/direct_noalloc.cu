@@ -15,10 +15,16 @@
 // array: calls that overlap on the GPU (several streams, several host threads) race on it.
 //
 // Host code cannot use the array's name as a device address (it names a host-side
-// stand-in); the device address comes from cudaGetSymbolAddress, taken once per device on
-// the first call made with that device current. Make that first call before any stream
-// capture begins.
+// stand-in); the device address comes from cudaGetSymbolAddress. The library takes it when a
+// context is created (fmmb_ctx_create, with its device current), so the module holding the
+// array is loaded at set-up rather than inside the first call; it is kept per CUDA context, so
+// a reset device (a new primary context) resolves it again on its next call. Create the context
+// before any stream capture begins.
+#include <cuda.h>
+
 #include <mutex>
+#include <utility>
+#include <vector>
 
 #include "passes.cuh"
 
@@ -27,76 +33,48 @@ namespace {
 
 constexpr int64_t SCRATCH_DOUBLES = 1 << 19;   // 4 MiB
 constexpr int MAX_SPLIT = 32;
-constexpr int NT = 128;                        // targets per CTA and sources per staged tile
 
 static __device__ __align__(256) double g_direct_scratch[SCRATCH_DOUBLES];
 
-constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
-double* g_scratch_ptr[MAX_DEVICES] = {};
+std::vector<std::pair<CUcontext, double*>> g_scratch;   // per CUDA context: the array's address
 
-// the scratch array's device address on the current device (set up once per device)
+// the current CUDA context (the driver's cuCtxGetCurrent, through the runtime's entry-point query)
+CUcontext current_context() {
+  using Fn = CUresult (*)(CUcontext*);
+  static Fn fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    FMMB_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q));
+    require(f != nullptr && q == cudaDriverEntryPointSuccess, FMMB_ERR_DEVICE, "cuCtxGetCurrent is not available");
+    fn = (Fn)f;
+  }
+  CUcontext c = nullptr;
+  require(fn(&c) == CUDA_SUCCESS && c != nullptr, FMMB_ERR_DEVICE, "no current CUDA context");
+  return c;
+}
+
+// the scratch array's device address in the current context (resolved once per context)
 double* scratch_address() {
-  int dev = 0;
-  FMMB_CUDA(cudaGetDevice(&dev));
-  require(dev >= 0 && dev < MAX_DEVICES, FMMB_ERR_ARGUMENT, "device index out of range");
+  FMMB_CUDA(cudaFree(nullptr));                     // makes the device's primary context current
+  const CUcontext c = current_context();
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    FMMB_CUDA(cudaGetSymbolAddress(&p, g_direct_scratch));
-    g_scratch_ptr[dev] = (double*)p;
-  }
-  return g_scratch_ptr[dev];
-}
-
-__global__ void __launch_bounds__(NT) k_direct_partial(const double* __restrict__ src, const double* __restrict__ tau,
-                                                       int64_t ns, const double* __restrict__ tgt,
-                                                       const int64_t* __restrict__ self_idx, int64_t nt, int nsplit,
-                                                       double* __restrict__ part) {
-  __shared__ double sx[NT], sy[NT], sz[NT], sq[NT];
-  const int64_t t = (int64_t)blockIdx.x * NT + threadIdx.x;
-  const int sp = blockIdx.y;
-  const int64_t s0 = ns * sp / nsplit, s1 = ns * (sp + 1) / nsplit;
-  const bool act = t < nt;
-  const double x = act ? tgt[3 * t] : 0, y = act ? tgt[3 * t + 1] : 0, z = act ? tgt[3 * t + 2] : 0;
-  const int64_t me = (act && self_idx) ? self_idx[t] : -1;
-  double u = 0, gx = 0, gy = 0, gz = 0;
-  for (int64_t b = s0; b < s1; b += NT) {
-    __syncthreads();
-    const int64_t j = b + threadIdx.x;
-    if (j < s1) { sx[threadIdx.x] = src[3 * j]; sy[threadIdx.x] = src[3 * j + 1]; sz[threadIdx.x] = src[3 * j + 2]; sq[threadIdx.x] = tau[j]; }
-    __syncthreads();
-    const int m = (int)min((int64_t)NT, s1 - b);
-    for (int i = 0; i < m; ++i) {
-      const double dx = x - sx[i], dy = y - sy[i], dz = z - sz[i];
-      const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-      const double ir = (b + i == me) ? 0.0 : 1.0 / sqrt(r2);
-      const double qi = sq[i] * ir, qi3 = qi * ir * ir;
-      u += qi; gx += qi3 * dx; gy += qi3 * dy; gz += qi3 * dz;
-    }
-  }
-  if (act) {
-    double* o = part + ((int64_t)sp * nt + t) * 4;
-    o[0] = u; o[1] = gx; o[2] = gy; o[3] = gz;
-  }
-}
-
-__global__ void k_direct_sum(const double* __restrict__ part, int64_t nt, int nsplit, double* __restrict__ pot,
-                             double* __restrict__ grad) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nt) return;
-  double u = 0, gx = 0, gy = 0, gz = 0;
-  for (int sp = 0; sp < nsplit; ++sp) {
-    const double* o = part + ((int64_t)sp * nt + t) * 4;
-    u += o[0]; gx += o[1]; gy += o[2]; gz += o[3];
-  }
-  if (pot) pot[t] = KC * u;
-  if (grad) { grad[3 * t] = -KC * gx; grad[3 * t + 1] = -KC * gy; grad[3 * t + 2] = -KC * gz; }
+  for (auto& e : g_scratch)
+    if (e.first == c) return e.second;
+  void* p = nullptr;
+  FMMB_CUDA(cudaGetSymbolAddress(&p, g_direct_scratch));
+  g_scratch.emplace_back(c, (double*)p);
+  return (double*)p;
 }
 
 }  // namespace
 
-// enqueues on the context's stream; no allocation, no synchronisation
+void direct_noalloc_prepare() { scratch_address(); }
+
+// enqueues on the context's stream; no allocation, no synchronisation. The partial sums use the
+// kernels of fmmb_direct_dev; only the split of the sources differs (at most MAX_SPLIT ranges,
+// and as many as the scratch holds for nt targets)
 void direct_noalloc(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
                     int64_t nt, double* pot, double* grad) {
   require(nt * 4 <= SCRATCH_DOUBLES, FMMB_ERR_ARGUMENT,
@@ -104,12 +82,12 @@ void direct_noalloc(Ctx& ctx, const double* src, const double* tau, int64_t ns, 
               std::to_string(SCRATCH_DOUBLES * 8 >> 20) + " MiB); got " + std::to_string(nt));
   if (nt == 0) return;
   double* part = scratch_address();
-  const int tb = (int)((nt + NT - 1) / NT);
+  const int tb = (int)((nt + DT - 1) / DT);
   int nsplit = std::max(1, std::min<int>(MAX_SPLIT, (4 * ctx.num_sms + tb - 1) / tb));
   nsplit = (int)std::max<int64_t>(1, std::min<int64_t>(nsplit, SCRATCH_DOUBLES / (4 * nt)));
-  k_direct_partial<<<dim3(tb, nsplit), NT, 0, ctx.stream>>>(src, tau, ns, tgt, self_idx, nt, nsplit, part);
+  k_direct<<<dim3(tb, nsplit), DT, 0, ctx.stream>>>(src, tau, ns, tgt, self_idx, nt, nsplit, part);
   FMMB_LAUNCH_CHECK();
-  k_direct_sum<<<(unsigned)((nt + 255) / 256), 256, 0, ctx.stream>>>(part, nt, nsplit, pot, grad);
+  k_direct_reduce<<<(unsigned)((nt + 255) / 256), 256, 0, ctx.stream>>>(part, nt, nsplit, pot, grad);
   FMMB_LAUNCH_CHECK();
 }
 

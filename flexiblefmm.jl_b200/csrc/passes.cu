@@ -419,8 +419,31 @@ __global__ void k_bounds(const double* __restrict__ xyz, int64_t n, double* __re
   if (threadIdx.x < 6) out[blockIdx.x * 6 + threadIdx.x] = s[threadIdx.x][0];
 }
 
+// P2M of charges q (and, when d3 is given, dipoles d3: 3 × N planar) into M (pitch per node)
+template <int P>
+void launch_p2m(State& S, const double* q, const double* d3, double* M, int64_t pitch) {
+  Plan& P_ = *S.plan;
+  int nth = P_.n_s2m * (P + 1);
+  if (nth == 0) return;
+  if (d3) {
+    k_p2m_dip<P><<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p,
+                                                           S.ys.p, S.zs.p, q, d3, P_.N, geometry(P_), P_.d_scale.p,
+                                                           pitch, M);
+    FMMB_LAUNCH_CHECK();
+    return;
+  }
+  auto kern = P_.cache->kernel == FMMB_KERNEL_YUKAWA3D ? k_p2m<P, true> : k_p2m<P, false>;
+  kern<<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p, S.ys.p,
+                                                 S.zs.p, q, geometry(P_), P_.d_scale.p, pitch, M, P_.d_kh2.p);
+  FMMB_LAUNCH_CHECK();
+}
+
+
+
+}  // namespace
+
 // ---------------------------------------------------------------- direct sums, FP64
-constexpr int DT = 128;  // targets per CTA and sources per shared-memory tile
+// (shared by fmmb_direct_dev and fmmb_direct_noalloc_dev; declared in passes.cuh)
 __global__ void __launch_bounds__(DT) k_direct(const double* __restrict__ src, const double* __restrict__ tau, int64_t ns,
                                                const double* __restrict__ tgt, const int64_t* __restrict__ self_idx,
                                                int64_t nt, int nsplit, double* __restrict__ part) {
@@ -465,28 +488,6 @@ __global__ void k_direct_reduce(const double* __restrict__ part, int64_t nt, int
   if (grad) { grad[3 * t] = -KC * gx; grad[3 * t + 1] = -KC * gy; grad[3 * t + 2] = -KC * gz; }
 }
 
-// P2M of charges q (and, when d3 is given, dipoles d3: 3 × N planar) into M (pitch per node)
-template <int P>
-void launch_p2m(State& S, const double* q, const double* d3, double* M, int64_t pitch) {
-  Plan& P_ = *S.plan;
-  int nth = P_.n_s2m * (P + 1);
-  if (nth == 0) return;
-  if (d3) {
-    k_p2m_dip<P><<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p,
-                                                           S.ys.p, S.zs.p, q, d3, P_.N, geometry(P_), P_.d_scale.p,
-                                                           pitch, M);
-    FMMB_LAUNCH_CHECK();
-    return;
-  }
-  auto kern = P_.cache->kernel == FMMB_KERNEL_YUKAWA3D ? k_p2m<P, true> : k_p2m<P, false>;
-  kern<<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p, S.ys.p,
-                                                 S.zs.p, q, geometry(P_), P_.d_scale.p, pitch, M, P_.d_kh2.p);
-  FMMB_LAUNCH_CHECK();
-}
-
-
-
-}  // namespace
 
 Geometry geometry(const Plan& P) {
   Geometry g;

@@ -215,4 +215,16 @@ void m2l_mixed(State& S);
 int mixed_error_flag(State& S);   // 1 when a bounded wait of the tensor-core M2L gave up since the last call (then cleared)
 void set_m2l_stall(long long slab, double wait_s);   // the test hook of fmmb_test_m2l_stall
 
+// FP64 direct sums at nt targets (passes.cu): per (source range sp of nsplit, target) the partial
+// potential and gradient sums into part[(sp·nt + t)·4 ..], then their reduction; DT targets per CTA
+constexpr int DT = 128;
+__global__ void k_direct(const double* __restrict__ src, const double* __restrict__ tau, int64_t ns,
+                         const double* __restrict__ tgt, const int64_t* __restrict__ self_idx, int64_t nt, int nsplit,
+                         double* __restrict__ part);
+__global__ void k_direct_reduce(const double* __restrict__ part, int64_t nt, int nsplit, double* __restrict__ pot,
+                                double* __restrict__ grad);
+// resolves the no-allocation scratch array's device address for the current device and context
+// (direct_noalloc.cu; called when a context is created)
+void direct_noalloc_prepare();
+
 }  // namespace fmmb

@@ -220,8 +220,10 @@ int fmmb_direct_dev(fmmb_ctx* ctx, const double* src_dev, const double* tau_dev,
  * the context's stream and returns without synchronising. The partial sums live in a 4 MiB
  * array compiled into the library (held by every GPU that loads it until exit), so nt is
  * limited to 131,072 targets (FMMB_ERR_ARGUMENT above). All calls share that array: calls that
- * overlap on the GPU race. The first call on a device looks up the array's device address;
- * make it before any stream capture. */
+ * overlap on the GPU race. The array's device address is looked up when the context is created
+ * (fmmb_ctx_create), which loads the library's device code then rather than inside a call, and
+ * again in a new CUDA context (after a device reset); create the context before any stream
+ * capture. */
 int fmmb_direct_noalloc_dev(fmmb_ctx* ctx, const double* src_dev, const double* tau_dev, int64_t ns,
                             const double* tgt_dev, const int64_t* self_index_dev, int64_t nt, double* pot_dev,
                             double* grad_dev);
