@@ -64,7 +64,6 @@ def args_():
     a.add_argument("--serve-requests", type=int, default=384, help="requests of the serving measurement (0: skip it)")
     a.add_argument("--serve-slots", type=int, default=4)
     a.add_argument("--stokes-instances", type=int, default=64, help="instances of the batched Stokes measurement (0: skip it)")
-    a.add_argument("--stokes-slots", type=int, default=4, help="server slots of the batched Stokes measurement")
     a.add_argument("--ki-points", type=int, default=2_000_000, help="points of the cube KI measurement (0: skip it)")
     a.add_argument("--no-circle-ki", action="store_true", help="skip the 2D circle KI measurement")
     return a.parse_args()
@@ -330,41 +329,89 @@ def stokes_direct(src, f, sel):
     return out
 
 
-def stokes_batched(fmmb, device, count, slots, p=16, ppl=200, samples=32):
-    """StokesHarmonics(Stokeslet3D(); p = 16) instances through the request server: all submitted
-    at once over `slots` streams (aggregate velocity evaluations/s), then one at a time on one
-    slot; per-instance relative L2 error of the velocities against FP64 direct sums at `samples`
-    sampled sources."""
+def stokes_batch(fmmb, torch, ctx, count, p=16, ppl=200, samples=32, steps=3):
+    """The batched Stokes configuration as ONE batch plan (fmmb_batch_plan_create):
+    StokesHarmonics(Stokeslet3D(); p = 16) self plans of `count` jittered unit-sphere point sets in
+    the common box [-1.02, 1.02]^3, all trees built in one tree build and all instances evaluated
+    by one call (one launch per pass and level). Timed: the plan (every tree, list and operator
+    table) followed by one evaluation through host arrays (a call with new geometry), the
+    evaluation alone with the inputs resident on the device (CUDA events on the library's stream,
+    L2 flushed between steps), and the instances one at a time (each its own plan and evaluation,
+    one operator cache). Every instance's velocities are compared bitwise with its own plan's, and
+    their relative L2 error against FP64 direct sums at `samples` sampled sources is reported."""
+    import ctypes as C
+    L = fmmb.lib()
     reqs = stokes_workload(count)
-    total = sum(len(x) for x, _ in reqs)
-    srv = fmmb.Server(device, slots=slots)
-    for _ in range(2):                                                 # warm-up: every slot's operators resident
-        for k in [srv.submit_stokes(x, f, p=p, ppl=ppl) for x, f in reqs[:slots]]:
-            srv.wait(k)
+    xs, fs = [x for x, _ in reqs], [f for _, f in reqs]
+    total = sum(len(x) for x in xs)
+    box = ((-1.02, -1.02, -1.02), 2.04)
+    cache = fmmb.OperatorCache(fmmb.StokesHarmonics(fmmb.Stokeslet3D(), p=p))
+    w = fmmb.BatchStokesFMMPlan(xs[:2], ppl=ppl, bbox=box, cache=cache)      # warm-up: operators resident
+    fmmb.stokes_fmm_eval(w, stokeslets=w.fmm.concat(fs[:2]))
+    del w
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    tk = [srv.submit_stokes(x, f, p=p, ppl=ppl) for x, f in reqs]
-    res = [srv.wait(k) for k in tk]
-    t_batch = time.perf_counter() - t0
-    srv.close()
-    one = fmmb.Server(device, slots=1)
-    one.wait(one.submit_stokes(*reqs[0], p=p, ppl=ppl))
+    bp = fmmb.BatchStokesFMMPlan(xs, ppl=ppl, bbox=box, cache=cache)
+    t_plan = time.perf_counter() - t0
+    F = bp.fmm.concat(fs)
     t0 = time.perf_counter()
-    for x, f in reqs:
-        one.wait(one.submit_stokes(x, f, p=p, ppl=ppl))
+    vel = fmmb.stokes_fmm_eval(bp, stokeslets=F)
+    t_eval_host = time.perf_counter() - t0
+    P = lambda t: C.c_void_p(t.data_ptr())
+    xd, fd = torch.from_numpy(bp.sources).cuda(), torch.from_numpy(F).cuda()
+    vd = torch.zeros((total, 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    step = lambda: fmmb._check(L.fmmb_stokes_eval_dev(bp.state._h, P(xd), P(fd), total, P(vd)))
+    step()
+    torch.cuda.synchronize()
+    ev = []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    ms_dev = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+    same_dev = bool(np.array_equal(vd.cpu().numpy(), vel))
+    del xd, fd, vd, flush
+    # one at a time: each instance its own plan and evaluation (the same cache, so the same box)
+    one = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for x, f in zip(xs, fs):
+        sp = fmmb.StokesFMMPlan(x, ppl=ppl, bbox=box, cache=cache)
+        one.append(fmmb.stokes_fmm_eval(sp, stokeslets=f))
+        del sp
     t_seq = time.perf_counter() - t0
-    one.close()
+    parts = bp.fmm.split(vel)
+    bitwise = sum(bool(np.array_equal(a, b)) for a, b in zip(parts, one))
     rng = np.random.default_rng(50)
     errs = []
-    for (x, f), (v, _, _) in zip(reqs, res):
+    for x, f, v in zip(xs, fs, parts):
         sel = np.sort(rng.choice(len(x), samples, replace=False))
         ud = stokes_direct(x, f, sel)
         errs.append(float(np.linalg.norm(v[sel] - ud) / np.linalg.norm(ud)))
-    return {"instances": count, "points": total, "p": p, "ppl": ppl, "slots": slots, "precision": "fp64",
-            "workload": "N log-uniform [2e4, 2e5] jittered unit-sphere points, N(0,1)^3 Stokeslets (seed 5); each "
-                        "instance's box fitted to its own points and snapped to a power-of-two width",
-            "batched": {"evals_per_s": total / t_batch, "seconds": t_batch},
-            "one_at_a_time": {"evals_per_s": total / t_seq, "seconds": t_seq},
-            "error": {"samples_per_instance": samples, "max": max(errs), "median": float(np.median(errs))}}
+    fm = bp.fmm
+    out = {"instances": count, "points": total, "p": p, "ppl": ppl, "precision": "fp64",
+           "workload": "N log-uniform [2e4, 2e5] jittered unit-sphere points, N(0,1)^3 Stokeslets (seed 5), one batch "
+                       "plan over all instances in the common box [-1.02, 1.02]^3",
+           "plan": {"levels": fm.nlevels, "nodes": fm.nnodes, "far_pairs": fm.npairs, "seconds": t_plan},
+           "batched": {"evals_per_s": total / (t_plan + t_eval_host), "seconds": t_plan + t_eval_host,
+                       "what": "batch plan + one evaluation, host arrays"},
+           "eval_device": {"evals_per_s": total / (ms_dev / 1e3), "ms": ms_dev, "steps": steps,
+                           "what": "one evaluation of all instances, inputs resident, CUDA events",
+                           "equals_host_path": same_dev},
+           "eval_host": {"evals_per_s": total / t_eval_host, "seconds": t_eval_host},
+           "one_at_a_time": {"evals_per_s": total / t_seq, "seconds": t_seq},
+           "bitwise_equal_instances": bitwise,
+           "error": {"samples_per_instance": samples, "max": max(errs), "median": float(np.median(errs)),
+                     "per_instance": [float(f"{e:.3g}") for e in errs]}}
+    del bp, one
+    return out
 
 
 # ---------------------------------------------------------------- the cube KI method
@@ -677,7 +724,7 @@ def run_ours(a):
     del dev10
     R.pop("dev", None)
     serve = serving(fmmb, local, a.serve_requests, a.serve_slots) if a.serve_requests > 0 else None
-    stokes = stokes_batched(fmmb, local, a.stokes_instances, a.stokes_slots) if a.stokes_instances > 0 else None
+    stokes = stokes_batch(fmmb, torch, ctx, a.stokes_instances) if a.stokes_instances > 0 else None
     ki = cube_ki(fmmb, torch, ctx, a.ki_points, 5, 3) if a.ki_points > 0 else None
     kic = None if a.no_circle_ki else circle_ki(fmmb)
     # every figure, on a line of its own before the headline
@@ -746,7 +793,8 @@ def compact_side(p10, serve, stokes, ki, kic):
             s["serving"]["host_device_s"] = _sig(serve["host_device_s"], 3)
     if stokes:
         s["stokes"] = {"instances": stokes["instances"], "batched": _sig(stokes["batched"]["evals_per_s"]),
-                       "one": _sig(stokes["one_at_a_time"]["evals_per_s"]), "err_max": _sig(stokes["error"]["max"], 3)}
+                       "eval_dev": _sig(stokes["eval_device"]["evals_per_s"]), "one": _sig(stokes["one_at_a_time"]["evals_per_s"]),
+                       "bitwise": stokes["bitwise_equal_instances"], "err_max": _sig(stokes["error"]["max"], 3)}
     if ki:
         s["cube_ki"] = {"value": _sig(ki["evals_per_s"]), "ms": _sig(ki["ms_per_step"]), "m2l_ms": _sig(ki["stages_ms"]["m2l"]),
                         "err": _sig(ki["error"]["pot_rel_l2"], 3)}

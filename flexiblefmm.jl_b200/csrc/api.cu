@@ -1,5 +1,6 @@
 // The C ABI of fmmb (include/fmmb.h): handles, validation with the reference's error
 // semantics, host↔device staging, and the order of the passes.
+#include <algorithm>
 #include <cstring>
 
 #include "passes.cuh"
@@ -152,6 +153,9 @@ void fit_box(Cache& C, const double lo[3], const double hi[3], const double bo[3
   throw Error(FMMB_ERR_ARGUMENT, "could not fit a box");
 }
 
+void finish_plan(fmmb_cache* cache, std::unique_ptr<fmmb_plan>& h, const double* xyz, const fmmb_tree_opts* opts,
+                 fmmb_plan** out);
+
 void plan_from_device_points(fmmb_cache* cache, const double* xyz, int64_t n, const fmmb_tree_opts* opts, fmmb_plan** out) {
   require(cache && opts && out, FMMB_ERR_ARGUMENT, "null argument");
   Cache& C = cache->c;
@@ -177,6 +181,15 @@ void plan_from_device_points(fmmb_cache* cache, const double* xyz, int64_t n, co
   P.ctx = &ctx;
   P.N = n;
   fit_box(C, lo, hi, bo, bw, P.origin, P.W0, P.e0);
+  finish_plan(cache, h, xyz, opts, out);
+}
+
+// the tree, scales, operators and lists of a plan whose box (or a batch's boxes) is fitted
+void finish_plan(fmmb_cache* cache, std::unique_ptr<fmmb_plan>& h, const double* xyz, const fmmb_tree_opts* opts,
+                 fmmb_plan** out) {
+  Cache& C = cache->c;
+  Ctx& ctx = *C.ctx;
+  Plan& P = h->p;
   {
     std::lock_guard<std::mutex> lk(C.mu);
     if (!C.uploaded) {
@@ -213,6 +226,62 @@ void plan_from_device_points(fmmb_cache* cache, const double* xyz, int64_t n, co
   std::lock_guard<std::mutex> lk(g_handles);
   ++cache->deps;
   *out = h.release();
+}
+
+// a batch: ninst point sets (counts[i] points each, consecutive in xyz), each with its own box
+// (boxes: 4 per instance, origin and width, or null for each set's square_bbox) fitted by
+// fit_box! in instance order, as plans built one after another with the same cache would be
+void batch_plan_from_device_points(fmmb_cache* cache, const double* xyz, const int64_t* counts, int64_t ninst,
+                                   const fmmb_tree_opts* opts, const double* boxes, fmmb_plan** out) {
+  require(cache && counts && opts && out, FMMB_ERR_ARGUMENT, "null argument");
+  Cache& C = cache->c;
+  Ctx& ctx = *C.ctx;
+  set_device(ctx);
+  require(ninst >= 1 && ninst < (1 << 24), FMMB_ERR_ARGUMENT, "the instance count must be in 1 .. 2^24 - 1");
+  require(C.method == FMMB_METHOD_SPHERICAL_HARMONICS, FMMB_ERR_UNSUPPORTED,
+          "batch plans take the harmonic methods (Laplace3D, Yukawa3D, Stokeslet3D)");
+  require(opts->ppl >= 1, FMMB_ERR_ARGUMENT, "ppl must be positive");
+  require(opts->max_levels >= 1, FMMB_ERR_ARGUMENT, "max_levels must be positive");
+  std::vector<int64_t> off(ninst + 1, 0);
+  for (int64_t i = 0; i < ninst; ++i) {
+    require(counts[i] > 0, FMMB_ERR_ARGUMENT, "instance " + std::to_string(i) + " has no points");
+    off[i + 1] = off[i] + counts[i];
+    require(off[i + 1] < (1ll << 31) - 1, FMMB_ERR_ARGUMENT, "too many points for 32-bit indices");
+  }
+  std::vector<double> lo, hi;
+  int64_t bad = 0;
+  bounds_batch(ctx, xyz, off, lo, hi, &bad);
+  require(bad == 0, FMMB_ERR_ARGUMENT, "the points must be finite");
+  std::unique_ptr<fmmb_plan> h(new fmmb_plan());
+  Plan& P = h->p;
+  P.cache = &C;
+  P.ctx = &ctx;
+  P.N = off[ninst];
+  P.ninst = (int)ninst;
+  P.inst_off = off;
+  P.inst_box.resize(4 * ninst);
+  P.inst_e.resize(ninst);
+  for (int64_t i = 0; i < ninst; ++i) {
+    double bo[3], bw;
+    if (boxes) {
+      for (int d = 0; d < 3; ++d) bo[d] = boxes[4 * i + d];
+      bw = boxes[4 * i + 3];
+    } else {
+      square_bbox(&lo[3 * i], &hi[3 * i], bo, bw);
+    }
+    double o[3], W;
+    fit_box(C, &lo[3 * i], &hi[3 * i], bo, bw, o, W, P.inst_e[i]);
+    for (int d = 0; d < 3; ++d) P.inst_box[4 * i + d] = o[d];
+    P.inst_box[4 * i + 3] = W;
+  }
+  // the global levels: the widest root on level 0, every root on the level of its width
+  const int64_t iw = std::max_element(P.inst_e.begin(), P.inst_e.end()) - P.inst_e.begin();
+  P.e0 = P.inst_e[iw];
+  P.W0 = P.inst_box[4 * iw + 3];
+  for (int d = 0; d < 3; ++d) P.origin[d] = P.inst_box[4 * iw + d];
+  P.inst_root.resize(ninst);
+  for (int64_t i = 0; i < ninst; ++i) P.inst_root[i] = P.e0 - P.inst_e[i];
+  finish_plan(cache, h, xyz, opts, out);
 }
 
 void check_outputs(int outputs) {
@@ -433,6 +502,54 @@ int fmmb_plan_create_dev(fmmb_cache* cache, const double* xyz_dev, int64_t n, co
     set_device(cache->parent->c);
     require_device_ptr(cache->parent->c, xyz_dev, "points");
     plan_from_device_points(cache, xyz_dev, n, opts, out);
+  });
+}
+
+int fmmb_batch_plan_create(fmmb_cache* cache, const double* xyz, const int64_t* counts, int64_t ninst,
+                           const fmmb_tree_opts* opts, const double* boxes, fmmb_plan** out) {
+  return guard([&] {
+    require(cache && xyz && counts && opts && out, FMMB_ERR_ARGUMENT, "null argument");
+    require(ninst >= 1, FMMB_ERR_ARGUMENT, "no instances");
+    int64_t n = 0;
+    for (int64_t i = 0; i < ninst; ++i) {
+      require(counts[i] > 0, FMMB_ERR_ARGUMENT, "instance " + std::to_string(i) + " has no points");
+      n += counts[i];
+    }
+    Ctx& ctx = *cache->c.ctx;
+    set_device(ctx);
+    DBuf<double> d(3 * n);
+    FMMB_CUDA(cudaMemcpyAsync(d.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx.stream));
+    batch_plan_from_device_points(cache, d.p, counts, ninst, opts, boxes, out);
+  });
+}
+
+int fmmb_batch_plan_create_dev(fmmb_cache* cache, const double* xyz_dev, const int64_t* counts, int64_t ninst,
+                               const fmmb_tree_opts* opts, const double* boxes, fmmb_plan** out) {
+  return guard([&] {
+    require(cache && xyz_dev != nullptr, FMMB_ERR_ARGUMENT, "null argument");
+    set_device(cache->parent->c);
+    require_device_ptr(cache->parent->c, xyz_dev, "points");
+    batch_plan_from_device_points(cache, xyz_dev, counts, ninst, opts, boxes, out);
+  });
+}
+
+int fmmb_batch_plan_instances(const fmmb_plan* plan, int64_t* ninst, int64_t* offsets, double* boxes, int32_t* root_level,
+                              int32_t* node_instance) {
+  return guard([&] {
+    require(plan && ninst, FMMB_ERR_ARGUMENT, "null argument");
+    const Plan& P = plan->p;
+    *ninst = P.ninst;
+    for (int i = 0; i < P.ninst; ++i) {
+      if (offsets) offsets[i] = P.inst_off[i];
+      if (boxes)
+        for (int d = 0; d < 4; ++d) boxes[4 * i + d] = P.inst_box[4 * i + d];
+      if (root_level) root_level[i] = P.inst_root[i];
+    }
+    if (offsets) offsets[P.ninst] = P.inst_off[P.ninst];
+    if (node_instance) {
+      if (P.ninst > 1) std::copy(P.h_inst.begin(), P.h_inst.end(), node_instance);
+      else std::fill(node_instance, node_instance + P.nnodes, 0);
+    }
   });
 }
 

@@ -42,8 +42,9 @@ __global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, cons
   for (int i = lane; i < LD; i += 32) L[i] = (R)Pl[(int64_t)leaf * LD + i];
   __syncwarp();
   const int4 c = cell[leaf];
+  const Geometry gn = geo.at(leaf);
   const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
-  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w), cz = gn.center(2, c.z, w);
   const int t0 = gstart[grp], nt = gcount[grp];
   for (int base = 0; base < nt; base += 32) {
     const int k = t0 + base + lane;
@@ -255,10 +256,11 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32, 5) k_near(const int* __restri
   double cx = 0, cy = 0, cz = 0;
   if (REL) {
     const int4 c = cell[leaf];
+    const Geometry gn = geo.at(leaf);
     const double w = ldexp(geo.W0, -c.w);
-    cx = geo.center(0, c.x, w);
-    cy = geo.center(1, c.y, w);
-    cz = geo.center(2, c.z, w);
+    cx = gn.center(0, c.x, w);
+    cy = gn.center(1, c.y, w);
+    cz = gn.center(2, c.z, w);
   }
   // the colleagues' point ranges, flattened in colleague order
   const int cn = lane < NCOL ? col[(int64_t)leaf * NCOL + lane] : -1;
@@ -359,8 +361,9 @@ __global__ void __launch_bounds__(128) k_ki_l2t(const int* __restrict__ gnode, c
   R* Y = L + nl;
   const int leaf = gnode[grp];
   const int4 c = cell[leaf];
+  const Geometry gn = geo.at(leaf);
   const double w = ldexp(geo.W0, -c.w);
-  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w), cz = gn.center(2, c.z, w);
   for (int k = lane; k < nl; k += 32) {
     L[k] = (R)Ll[(int64_t)leaf * nld + k];
     Y[3 * k] = (R)(w * large[3 * k]);
@@ -416,8 +419,9 @@ __global__ void __launch_bounds__(128) k_kic_l2t(const int* __restrict__ gnode, 
   if (grp >= ngroups) return;
   const int leaf = gnode[grp];
   const int4 c = cell[leaf];
+  const Geometry gn = geo.at(leaf);
   const double w = ldexp(geo.W0, -c.w);
-  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w);
+  const double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w);
   for (int k = lane; k < N; k += 32) {
     double sn, cs;
     sincospi(2.0 * k / N, &sn, &cs);
@@ -479,10 +483,11 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32) k_near_dip(const int* __restr
   double cx = 0, cy = 0, cz = 0;
   if (REL) {
     const int4 c = cell[leaf];
+    const Geometry gn = geo.at(leaf);
     const double w = ldexp(geo.W0, -c.w);
-    cx = geo.center(0, c.x, w);
-    cy = geo.center(1, c.y, w);
-    cz = geo.center(2, c.z, w);
+    cx = gn.center(0, c.x, w);
+    cy = gn.center(1, c.y, w);
+    cz = gn.center(2, c.z, w);
   }
   const int cn = lane < NCOL ? col[(int64_t)leaf * NCOL + lane] : -1;
   int lo = 0, len = 0;

@@ -33,6 +33,7 @@ __device__ __forceinline__ void for_far_pairs(int t, const int4* __restrict__ ce
                                               const uint8_t* __restrict__ flags, F&& fn) {
   if (flags[t] & F_GHOST) return;
   int p = parent[t];
+  if (p < 0) return;               // a root (a batch's roots sit on any level)
   int4 ct = cell[t];
   for (int k = 0; k < NCOL; ++k) {
     int pc = col[(int64_t)p * NCOL + k];
@@ -133,12 +134,15 @@ void build_lists(Plan& P) {
   P.h_phi = to_host(P.phi.p, n, s);
   P.h_flags = to_host(P.flags.p, n, s);
 
-  // childless nodes with sources on levels ≥ 2 (src/fmm.jl:45-46), real leaves with points
+  // childless nodes with sources on levels ≥ 2 of their own tree (src/fmm.jl:45-46), real
+  // leaves with points
+  const bool batch = P.ninst > 1;
   std::vector<int> s2m, leaves, lstart, lcount;
   for (int l = 0; l < L; ++l)
     for (int g = P.level_start[l]; g < P.level_start[l + 1]; ++g) {
       bool src = (P.h_flags[g] & F_SOURCE) != 0;
-      if (l >= 2 && P.h_cf[g] < 0 && src) s2m.push_back(g);
+      const int lr = batch ? l - P.inst_root[P.h_inst[g]] : l;
+      if (lr >= 2 && P.h_cf[g] < 0 && src) s2m.push_back(g);
       if ((P.h_flags[g] & F_LEAF) && src) {
         leaves.push_back(g);
         lstart.push_back(P.h_plo[g]);
@@ -154,10 +158,29 @@ void build_lists(Plan& P) {
   P.group_parent.clear();
   P.group_parent.resize(L);
   for (int l = 1; l < L; ++l) {
-    int nl = P.level_start[l + 1] - P.level_start[l];
-    std::vector<int> gp(nl / NCH);
-    for (int g = 0; g < nl / NCH; ++g) gp[g] = P.h_parent[P.level_start[l] + NCH * g];
+    const int ng = P.level_groups[l];
+    std::vector<int> gp(ng);
+    for (int g = 0; g < ng; ++g) gp[g] = P.h_parent[P.level_start[l] + NCH * g];
     to_device(P.group_parent[l], gp, s);
+  }
+  // the segments: per level, the runs of one instance's nodes (one per level for one point set)
+  P.seg_start.clear(); P.seg_level.clear(); P.seg_inst.clear();
+  for (int l = 0; l < L; ++l)
+    for (int g = P.level_start[l]; g < P.level_start[l + 1]; ++g)
+      if (g == P.level_start[l] || (batch && P.h_inst[g] != P.h_inst[g - 1])) {
+        P.seg_start.push_back(g);
+        P.seg_level.push_back(l);
+        P.seg_inst.push_back(batch ? P.h_inst[g] : 0);
+      }
+  P.nseg = (int)P.seg_level.size();
+  P.seg_start.push_back(n);
+  if (batch) {
+    std::vector<int> ns(n);
+    for (int q = 0; q < P.nseg; ++q)
+      for (int g = P.seg_start[q]; g < P.seg_start[q + 1]; ++g) ns[g] = q;
+    to_device(P.node_seg, ns, s);
+  } else {
+    require(P.nseg == L, FMMB_ERR_DEVICE, "a level without nodes");
   }
 
   // the offset tables
@@ -192,13 +215,16 @@ void build_lists(Plan& P) {
   P.h_blocks.clear();
   P.level_pairs.assign(L, 0);
   int64_t base = 0;
-  for (int l = 2; l < L; ++l) {
-    for (int b0 = P.level_start[l]; b0 < P.level_start[l + 1]; b0 += P.TB) {
-      int c = std::min(P.TB, P.level_start[l + 1] - b0);
+  require(L < 256, FMMB_ERR_ARGUMENT, "too many levels");
+  for (int q = 0; q < P.nseg; ++q) {
+    const int l = P.seg_level[q], end = P.seg_start[q + 1];
+    if (l < 2) continue;
+    for (int b0 = P.seg_start[q]; b0 < end; b0 += P.TB) {
+      int c = std::min(P.TB, end - b0);
       int64_t np = 0;
       for (int g = b0; g < b0 + c; ++g) np += hc[g];
       if (np == 0) continue;
-      P.h_blocks.push_back({l, b0, c, (int)base});
+      P.h_blocks.push_back({l, q, b0, c, (int)base});
       base += np;
       P.level_pairs[l] += np;
     }
@@ -217,7 +243,7 @@ void build_lists(Plan& P) {
   std::vector<int4> hb(nb);
   for (int i = 0; i < nb; ++i) {
     const M2LBlock& B = P.h_blocks[order[i]];
-    hb[i] = make_int4(B.level, B.first, B.count, B.pair_base);
+    hb[i] = make_int4(B.level | B.seg << 8, B.first, B.count, B.pair_base);
   }
   to_device(P.blocks, hb, s);
   P.cls_off.alloc((size_t)std::max(nb, 1) * (NCLASS + 1));

@@ -63,12 +63,13 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
   int* pt = pf + NB;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4, warp = tid >> 5, lane = tid & 31;
   const int4 b = blocks[blockIdx.x];
-  const double alpha = m2l_scale[b.x];
+  const int level = b.x & 255;
+  const double alpha = m2l_scale[level];
   const int* co = cls_off + (int64_t)blockIdx.x * (NCLASS + 1);
   const int kmax = (NP + BK - 1) / BK * BK;
   for (int c = 0; c < NCLASS; ++c) {
     const int a0 = co[c], a1 = co[c + 1];
-    const double* A = reinterpret_cast<const double*>(reps_lv[b.x]) + (int64_t)c * LD * LD;   // the level's representatives
+    const double* A = reinterpret_cast<const double*>(reps_lv[level]) + (int64_t)c * LD * LD;   // the level's representatives
     for (int q0 = a0; q0 < a1; q0 += NB) {
       const int nc = min(NB, a1 - q0);
       __syncthreads();
@@ -172,7 +173,10 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
 #pragma unroll
           for (int i = 0; i < 2; ++i) G[(8 * nt + 2 * t + i) * GS + warp * (LD / 8) + 8 * mt + g] = acc[mt][nt][i];
       __syncthreads();
-      // scatter: thread j owns entry j of the targets' partial locals
+      // scatter: thread j owns entry j of the targets' partial locals; each target's entry takes
+      // its pairs one by one in the list's order (read once per run of the target, written
+      // once), so the sums do not depend on where the chunks of NB pairs end, nor on which
+      // other targets share the block
       for (int j = tid; j < NP; j += 256) {
         int n, m, part;
         coef_nmp(j, n, m, part);
@@ -182,16 +186,16 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
         for (int qq = 0; qq < nc; ++qq) {
           const int t = pt[qq], fac = c_d4h[pf[qq]];
           if (t != cur) {
-            if (cur >= 0) Pl[(int64_t)(b.y + cur) * pitch + (int64_t)comp * LD + j] += alpha * run;
+            if (cur >= 0) Pl[(int64_t)(b.y + cur) * pitch + (int64_t)comp * LD + j] = run;
             cur = t;
-            run = 0.0;
+            run = Pl[(int64_t)(b.y + t) * pitch + (int64_t)comp * LD + j];
           }
           const int q = (m * (fac & 3)) & 3;
           const bool sw = part != 0 && (q & 1);
           const double y = G[qq * GS + (sw ? partner : j)];
-          run += perm_sign(sw ? 3 - part : part, q, n + m, fac) < 0 ? -y : y;
+          run = fma(alpha, perm_sign(sw ? 3 - part : part, q, n + m, fac) < 0 ? -y : y, run);
         }
-        if (cur >= 0) Pl[(int64_t)(b.y + cur) * pitch + (int64_t)comp * LD + j] += alpha * run;
+        if (cur >= 0) Pl[(int64_t)(b.y + cur) * pitch + (int64_t)comp * LD + j] = run;
       }
     }
   }

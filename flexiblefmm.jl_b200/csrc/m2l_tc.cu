@@ -452,7 +452,7 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
     const int g0 = part * G::NG / RBQ, g1 = (part + 1) * G::NG / RBQ;
     const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
     float* xp = xps + warp * 32 * 17;
-    const double alpha = m2l_scale[b.x] * (double)lsc[b.x];     // the level factor and the multipoles' scale
+    const double alpha = m2l_scale[b.x & 255] * (double)lsc[b.x >> 8];   // the level factor, the segment's scale
     int i = 0;
     for (int c = 0; c < NCLASS && ok; ++c) {
       const int R = nr[c];
@@ -626,18 +626,20 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
-// the largest |entry| of the multipoles of each level (one warp per node): the bit patterns of
-// non-negative doubles order as integers (a non-finite entry makes its level's maximum
-// non-finite, and the level is then split unscaled)
-__global__ void k_level_absmax(const double* __restrict__ M, const int4* __restrict__ cell, int nnodes, int NP, int LD,
-                               unsigned long long* __restrict__ lvmax) {
+// the largest |entry| of the multipoles of each segment (one warp per node; a plan of one point
+// set has one segment per level, seg null): the bit patterns of non-negative doubles order as
+// integers (a non-finite entry makes its segment's maximum non-finite, and the segment is then
+// split unscaled)
+__global__ void k_level_absmax(const double* __restrict__ M, const int4* __restrict__ cell, const int* __restrict__ seg,
+                               int nnodes, int NP, int LD, unsigned long long* __restrict__ lvmax) {
   const int node = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (node >= nnodes) return;
   const double* m = M + (int64_t)node * LD;
   double mx = 0.0;
   for (int k = lane; k < NP; k += 32) mx = fmax(mx, fabs(m[k]));
   for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if (lane == 0 && mx != 0.0) atomicMax(&lvmax[cell[node].w], (unsigned long long)__double_as_longlong(mx));
+  if (lane == 0 && mx != 0.0)
+    atomicMax(&lvmax[seg ? seg[node] : cell[node].w], (unsigned long long)__double_as_longlong(mx));
 }
 
 // the exponent e of each level: its largest entry times 2^e lies in [2^13, 2^14); lsc = 2^-e
@@ -649,7 +651,7 @@ __device__ __forceinline__ int level_exponent(unsigned long long bits) {
   return max(-100, min(100, 14 - ex));             // keeps the inverse scale inside FP32's range
 }
 __global__ void k_level_scale(const unsigned long long* __restrict__ lvmax, int L, float* __restrict__ lsc) {
-  const int l = threadIdx.x;
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l < L) lsc[l] = (float)ldexp(1.0, -level_exponent(lvmax[l]));
 }
 
@@ -658,13 +660,13 @@ __global__ void k_level_scale(const unsigned long long* __restrict__ lvmax, int 
 // (vstride further). One scale per level keeps the sums of a target's pairs in one scale (no
 // per-pair factor in the read-back); an entry 2^-k of its level's largest keeps 22 significant
 // bits down to k ≈ 17 and an absolute error below 2^-38 of the level's largest entry beyond.
-__global__ void k_split16(const double* __restrict__ M, const int4* __restrict__ cell, int nnodes, int NP, int LD, int KP,
-                          int64_t vstride, const unsigned long long* __restrict__ lvmax, uint16_t* __restrict__ Mh,
-                          uint16_t* __restrict__ Ml) {
+__global__ void k_split16(const double* __restrict__ M, const int4* __restrict__ cell, const int* __restrict__ seg,
+                          int nnodes, int NP, int LD, int KP, int64_t vstride, const unsigned long long* __restrict__ lvmax,
+                          uint16_t* __restrict__ Mh, uint16_t* __restrict__ Ml) {
   const int node = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (node >= nnodes) return;
   const double* m = M + (int64_t)node * LD;
-  const int e = level_exponent(lvmax[cell[node].w]);
+  const int e = level_exponent(lvmax[seg ? seg[node] : cell[node].w]);
   for (int k = lane; k < KP; k += 32) {
     int n, mm, part;
     coef_nmp(k, n, mm, part);
@@ -788,18 +790,20 @@ void m2l_mixed(State& S) {
   const int KP = kp_of(C.np);
   const size_t ne = (size_t)P.nnodes * KP;
   if (S.Mh.n < 2 * ne) { S.Mh.alloc(2 * ne); S.Ml.alloc(2 * ne); }
-  if (S.Lsc.n < (size_t)P.L) { S.Lsc.alloc(P.L); S.Lmax.alloc(P.L); }
+  const int nseg = P.nseg;                         // one scale per segment (per level for one point set)
+  const int* seg = P.ninst > 1 ? P.node_seg.p : nullptr;
+  if (S.Lsc.n < (size_t)nseg) { S.Lsc.alloc(nseg); S.Lmax.alloc(nseg); }
   if (!S.err.p) {                                  // sticky until reported (mixed_error_flag clears it)
     S.err.alloc(1);
     FMMB_CUDA(cudaMemsetAsync(S.err.p, 0, sizeof(int), s));
   }
   const unsigned nbk = (unsigned)(((int64_t)P.nnodes * 32 + 255) / 256);
-  FMMB_CUDA(cudaMemsetAsync(S.Lmax.p, 0, sizeof(unsigned long long) * P.L, s));
-  k_level_absmax<<<nbk, 256, 0, s>>>(S.M.p, P.cell.p, P.nnodes, C.np, C.ld, S.Lmax.p);
+  FMMB_CUDA(cudaMemsetAsync(S.Lmax.p, 0, sizeof(unsigned long long) * nseg, s));
+  k_level_absmax<<<nbk, 256, 0, s>>>(S.M.p, P.cell.p, seg, P.nnodes, C.np, C.ld, S.Lmax.p);
   FMMB_LAUNCH_CHECK();
-  k_level_scale<<<1, 64, 0, s>>>(S.Lmax.p, P.L, S.Lsc.p);
+  k_level_scale<<<(nseg + 63) / 64, 64, 0, s>>>(S.Lmax.p, nseg, S.Lsc.p);
   FMMB_LAUNCH_CHECK();
-  k_split16<<<nbk, 256, 0, s>>>(S.M.p, P.cell.p, P.nnodes, C.np, C.ld, KP, (int64_t)ne, S.Lmax.p, S.Mh.p, S.Ml.p);
+  k_split16<<<nbk, 256, 0, s>>>(S.M.p, P.cell.p, seg, P.nnodes, C.np, C.ld, KP, (int64_t)ne, S.Lmax.p, S.Mh.p, S.Ml.p);
   FMMB_LAUNCH_CHECK();
   switch (KP) {
     case 16: launch_tc<16>(S, nb); break;

@@ -104,8 +104,9 @@ __global__ void k_p2m_dip(const int* __restrict__ nodes, int nn, const int4* __r
   if (m > P) return;
   const int node = nodes[qn];
   const int4 c = cell[node];
+  const Geometry gn = geo.at(node);
   const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
-  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w), cz = gn.center(2, c.z, w);
   double ar[P + 1], ai[P + 1];
 #pragma unroll
   for (int n = 0; n <= P; ++n) { ar[n] = 0; ai[n] = 0; }
@@ -199,8 +200,9 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
   if (m > P) return;
   int node = nodes[qn];
   int4 c = cell[node];
+  const Geometry gn = geo.at(node);
   double w = ldexp(geo.W0, -c.w), s = scale[c.w];
-  double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w), cz = gn.center(2, c.z, w);
   const double k2 = YK ? kh2[c.w] : 0.0;
   double ar[P + 1], ai[P + 1];
 #pragma unroll
@@ -419,6 +421,35 @@ __global__ void k_bounds(const double* __restrict__ xyz, int64_t n, double* __re
   if (threadIdx.x < 6) out[blockIdx.x * 6 + threadIdx.x] = s[threadIdx.x][0];
 }
 
+// the bounds of each instance of a batch: blockIdx.y the instance (points [off[i], off[i + 1])),
+// its gridDim.x blocks reduce over it as k_bounds does
+__global__ void k_bounds_batch(const double* __restrict__ xyz, const int64_t* __restrict__ off, double* __restrict__ out,
+                               unsigned long long* __restrict__ bad) {
+  const int64_t a = off[blockIdx.y], n = off[blockIdx.y + 1] - a;
+  __shared__ double s[6][256];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  unsigned long long nb = 0;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+    for (int d = 0; d < 3; ++d) {
+      double v = xyz[3 * (a + j) + d];
+      if (!isfinite(v)) { ++nb; continue; }
+      lo[d] = fmin(lo[d], v);
+      hi[d] = fmax(hi[d], v);
+    }
+  for (int d = 0; d < 3; ++d) { s[d][threadIdx.x] = lo[d]; s[3 + d][threadIdx.x] = hi[d]; }
+  if (nb) atomicAdd(bad, nb);
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (threadIdx.x < h)
+      for (int d = 0; d < 3; ++d) {
+        s[d][threadIdx.x] = fmin(s[d][threadIdx.x], s[d][threadIdx.x + h]);
+        s[3 + d][threadIdx.x] = fmax(s[3 + d][threadIdx.x], s[3 + d][threadIdx.x + h]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) out[((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = s[threadIdx.x][0];
+}
+
 // P2M of charges q (and, when d3 is given, dipoles d3: 3 × N planar) into M (pitch per node)
 template <int P>
 void launch_p2m(State& S, const double* q, const double* d3, double* M, int64_t pitch) {
@@ -493,6 +524,8 @@ Geometry geometry(const Plan& P) {
   Geometry g;
   for (int d = 0; d < 3; ++d) g.origin[d] = P.origin[d];
   g.W0 = P.W0;
+  g.node_inst = P.ninst > 1 ? P.node_inst.p : nullptr;
+  g.inst_box = P.ninst > 1 ? P.d_inst_box.p : nullptr;
   return g;
 }
 
@@ -565,7 +598,7 @@ int m2m_sweep(State& S) {
   cudaStream_t s = P.ctx->stream;
   int launches = 0;
   for (int l = P.L - 2; l >= 2; --l) {
-    int c0 = P.level_start[l + 1], ng = (P.level_start[l + 2] - c0) / NCH;
+    int c0 = P.level_start[l + 1], ng = P.level_groups[l + 1];
     if (ng == 0) continue;
     ColMap bm{S.M.p, nullptr, c0, NCH}, cm{S.M.p, P.group_parent[l + 1].p, 0, 0};
     gemm_cols(C.ld, NCH * C.ld, P.lv_m2m[l], bm, cm, ng, C.ld, C.np, 0, P.ctx->num_sms, s);
@@ -604,7 +637,7 @@ int l2l_sweep(State& S) {
   cudaStream_t s = P.ctx->stream;
   int launches = 0;
   for (int l = 3; l < P.L; ++l) {
-    int c0 = P.level_start[l], ng = (P.level_start[l + 1] - c0) / NCH;
+    int c0 = P.level_start[l], ng = P.level_groups[l];
     if (ng == 0) continue;
     ColMap bm{S.Pl.p, P.group_parent[l].p, 0, 0}, cm{S.Pl.p, nullptr, c0, NCH};
     gemm_cols(NCH * C.ld, C.ld, P.lv_l2l[l - 1], bm, cm, ng, C.ld, C.np, 1, P.ctx->num_sms, s);
@@ -658,6 +691,7 @@ void evaluate_targets(State& S, const double* tg, int64_t nt, int outputs, doubl
 int group_targets(State& S, const double* tg, int64_t nt) {
   Plan& P = *S.plan;
   cudaStream_t s = P.ctx->stream;
+  require(P.ninst == 1, FMMB_ERR_UNSUPPORTED, "a batch plan evaluates at its sources only");
   require(nt < (1ll << 31) - 1, FMMB_ERR_ARGUMENT, "too many targets");
   if ((int64_t)S.t_x.n < nt) {
     S.t_x.alloc(nt); S.t_y.alloc(nt); S.t_z.alloc(nt); S.t_out.alloc(nt); S.t_node.alloc(nt);
@@ -695,6 +729,33 @@ void bounds(Ctx& ctx, const double* xyz, int64_t n, double lo[3], double hi[3], 
   for (int d = 0; d < 3; ++d) { lo[d] = INFINITY; hi[d] = -INFINITY; }
   for (int b = 0; b < nb; ++b)
     for (int d = 0; d < 3; ++d) { lo[d] = std::min(lo[d], h[b * 6 + d]); hi[d] = std::max(hi[d], h[b * 6 + 3 + d]); }
+}
+
+void bounds_batch(Ctx& ctx, const double* xyz, const std::vector<int64_t>& off, std::vector<double>& lo,
+                  std::vector<double>& hi, int64_t* nonfinite) {
+  cudaStream_t s = ctx.stream;
+  const int ninst = (int)off.size() - 1;
+  int64_t nmax = 1;
+  for (int i = 0; i < ninst; ++i) nmax = std::max<int64_t>(nmax, off[i + 1] - off[i]);
+  // blocks per instance: enough for the largest, and about four waves over all instances
+  const int nbx = (int)std::max<int64_t>(1, std::min<int64_t>((nmax + 255) / 256, (4 * ctx.num_sms + ninst - 1) / ninst));
+  DBuf<int64_t> d_off;
+  to_device(d_off, off, s);
+  DBuf<double> out((size_t)ninst * nbx * 6);
+  DBuf<unsigned long long> bad(1);
+  FMMB_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(unsigned long long), s));
+  k_bounds_batch<<<dim3(nbx, ninst), 256, 0, s>>>(xyz, d_off.p, out.p, bad.p);
+  FMMB_LAUNCH_CHECK();
+  std::vector<double> h = to_host(out.p, (size_t)ninst * nbx * 6, s);
+  *nonfinite = (int64_t)read_one(bad.p, s);
+  lo.assign(3 * ninst, INFINITY);
+  hi.assign(3 * ninst, -INFINITY);
+  for (int i = 0; i < ninst; ++i)
+    for (int b = 0; b < nbx; ++b)
+      for (int d = 0; d < 3; ++d) {
+        lo[3 * i + d] = std::min(lo[3 * i + d], h[((size_t)i * nbx + b) * 6 + d]);
+        hi[3 * i + d] = std::max(hi[3 * i + d], h[((size_t)i * nbx + b) * 6 + 3 + d]);
+      }
 }
 
 void direct(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,

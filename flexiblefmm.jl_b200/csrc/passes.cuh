@@ -8,12 +8,23 @@ constexpr double KC = 0.079577471545947667884;  // 1/(4π), the Laplace3D consta
 __host__ __device__ constexpr int tri(int n, int m) { return n * (n + 1) / 2 + m; }
 constexpr int TRI_MAX = PMAX * (PMAX + 1) / 2 + PMAX + 1;
 
-// the root box; centres formed exactly as the tree builder forms them
+// the root box; centres formed exactly as the tree builder forms them. A batch's instances
+// have boxes of their own: at(node) gives the geometry with the node's instance's origin.
 struct Geometry {
   double origin[3];
   double W0;
+  const int* node_inst;     // a batch: per node its instance, and per instance its box (4 each)
+  const double* inst_box;
   __device__ __forceinline__ double center(int d, int c, double w) const {
     return __dadd_rn(origin[d], __dmul_rn(__dadd_rn((double)c, 0.5), w));
+  }
+  __device__ __forceinline__ Geometry at(int node) const {
+    Geometry g = *this;
+    if (node_inst) {
+      const double* b = inst_box + 4 * node_inst[node];
+      g.origin[0] = b[0]; g.origin[1] = b[1]; g.origin[2] = b[2];
+    }
+    return g;
   }
 };
 Geometry geometry(const Plan& P);

@@ -70,10 +70,12 @@ struct Cache {
   std::map<int, std::unique_ptr<CircleLevel>> kic_levels;
 };
 
-// One M2L work block: TB consecutive nodes of one level (the targets), their far pairs
-// grouped by symmetry class.
+// One M2L work block: TB consecutive nodes of one segment (the targets), their far pairs
+// grouped by symmetry class. On the device the level and the segment share one word
+// (level | segment << 8).
 struct M2LBlock {
   int level;
+  int seg;
   int first;     // first node (global)
   int count;     // nodes in the block
   int pair_base; // first pair of the block in the plan's pair array
@@ -128,6 +130,25 @@ struct Plan {
   // childless nodes with sources and of the real leaves (both lists are in node order)
   std::vector<const double*> kic_upv, kic_upsu, kic_downv, kic_downsu;
   std::vector<int> s2m_level_start, ki_leaf_level_start;
+  // per level its sibling groups: the level's first 8·level_groups[l] nodes (a batch's roots
+  // below level 0 follow them)
+  std::vector<int> level_groups;
+  // a batch (several independent point sets in one forest): instance i is the input points
+  // [inst_off[i], inst_off[i + 1]), its root box inst_box[4i..4i+3] (origin, width
+  // ldexp(cache W0, inst_e[i])), its root on level inst_root[i]; per node its instance; the
+  // segments (one instance's nodes of one level, contiguous): per node its segment (the mixed
+  // path's scale index; a plan of one point set has one segment per level and no array)
+  int ninst = 1;
+  std::vector<int64_t> inst_off;
+  std::vector<double> inst_box;
+  std::vector<int> inst_e, inst_root;
+  DBuf<int64_t> d_inst_off;
+  DBuf<double> d_inst_box;
+  DBuf<int> node_inst;
+  std::vector<int> h_inst;
+  std::vector<int> seg_start, seg_level, seg_inst;   // nseg (+ 1 for seg_start)
+  DBuf<int> node_seg;
+  int nseg = 0;
 };
 
 struct State {
@@ -196,6 +217,9 @@ bool split_evaluation(const State& S);
 void near_sources(State& S, int outputs, double* pot_dev, double* grad_dev, cudaStream_t st);
 void far_sources(State& S, int outputs, double* pot_dev, double* grad_dev);
 void bounds(Ctx& ctx, const double* xyz_dev, int64_t n, double lo[3], double hi[3], int64_t* nonfinite);
+// the bounds of each instance of a batch (points [off[i], off[i + 1]) of xyz_dev): lo, hi 3 × ninst
+void bounds_batch(Ctx& ctx, const double* xyz_dev, const std::vector<int64_t>& off, std::vector<double>& lo,
+                  std::vector<double>& hi, int64_t* nonfinite);
 void direct(Ctx& ctx, const double* src, const double* tau, int64_t ns, const double* tgt, const int64_t* self_idx,
             int64_t nt, double* pot, double* grad);
 // ki.cu: CubeKernelIndependent{3}(Laplace3D()): cache and plan setup, the passes

@@ -71,8 +71,9 @@ __global__ void k_stokes_q4(const int* __restrict__ nodes, int nn, const int4* _
   if (wid >= nn) return;
   const int node = nodes[wid];
   const int4 c = cell[node];
+  const Geometry gn = geo.at(node);
   const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
-  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w), cz = gn.center(2, c.z, w);
   for (int i = plo[node] + lane; i <= phi[node]; i += 32) {
     const double y[3] = {(xs[i] - cx) * s, (ys[i] - cy) * s, (zs[i] - cz) * s};
     q4[i] = y[0] * f3[i] + y[1] * f3[n + i] + y[2] * f3[2 * n + i];
@@ -144,8 +145,9 @@ __global__ void __launch_bounds__(SW * 32) k_stokes_l2p(const int* __restrict__ 
   for (int i = lane; i < 4 * LD; i += 32) L[i] = Pl[(int64_t)leaf * 4 * LD + i];
   __syncwarp();
   const int4 c = cell[leaf];
+  const Geometry gn = geo.at(leaf);
   const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
-  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w), cz = gn.center(2, c.z, w);
   const int t0 = gstart[grp], nt = gcount[grp];
   for (int base = 0; base < nt; base += 32) {
     const int k = t0 + base + lane;
@@ -231,8 +233,9 @@ __global__ void __launch_bounds__(GW * 32) k_stokes_l2p_grad(const int* __restri
   for (int a = 0; a < 4; ++a) grad_sets<P>(L + a * LD, A + 3 * a * NG, A + (3 * a + 1) * NG, A + (3 * a + 2) * NG, lane);
   __syncwarp();
   const int4 c = cell[leaf];
+  const Geometry gn = geo.at(leaf);
   const double w = ldexp(geo.W0, -c.w), s = scale[c.w];
-  const double cx = geo.center(0, c.x, w), cy = geo.center(1, c.y, w), cz = geo.center(2, c.z, w);
+  const double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w), cz = gn.center(2, c.z, w);
   const int t0 = gstart[grp], nt = gcount[grp];
   for (int base = 0; base < nt; base += 32) {
     const int k = t0 + base + lane;
@@ -468,7 +471,7 @@ void stokes_build(State& S, const double* xyz_dev, const StokesDensities& d) {
   p2m_block(S, S.q.p, dens ? S.dip4.p + 9 * n : nullptr, S.M.p + 3 * (int64_t)LD, pitch);
   // M2M, level by level: the stacked children of each block (Ψ̂ with the coupling), one product each
   for (int l = P.L - 2; l >= 2; --l) {
-    const int c0 = P.level_start[l + 1], ng = (P.level_start[l + 2] - c0) / NCH;
+    const int c0 = P.level_start[l + 1], ng = P.level_groups[l + 1];
     if (ng == 0) continue;
     DBuf<double> X((size_t)ng * NCH * LD);
     for (int a = 0; a < 4; ++a) {
@@ -481,7 +484,7 @@ void stokes_build(State& S, const double* xyz_dev, const StokesDensities& d) {
   // M2L of every block (the Ψ̂ launch with the coupling), then L2L level by level
   m2l_stage(S);
   for (int l = 3; l < P.L; ++l) {
-    const int c0 = P.level_start[l], ng = (P.level_start[l + 1] - c0) / NCH;
+    const int c0 = P.level_start[l], ng = P.level_groups[l];
     if (ng == 0) continue;
     const int64_t per = (int64_t)ng * NCH * LD;
     DBuf<double> R(4 * per);

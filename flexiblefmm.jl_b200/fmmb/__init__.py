@@ -99,6 +99,7 @@ EXPORTS = (
     "fmmb_stokes_eval_dev", "fmmb_build_expansions_dipoles", "fmmb_build_expansions_dipoles_dev",
     "fmmb_stokes_eval_densities", "fmmb_stokes_eval_densities_dev", "fmmb_stokes_eval_src_trg",
     "fmmb_stokes_eval_src_trg_dev", "fmmb_state_synchronize", "fmmb_test_m2l_stall",
+    "fmmb_batch_plan_create", "fmmb_batch_plan_create_dev", "fmmb_batch_plan_instances",
 )
 
 
@@ -128,6 +129,9 @@ def lib():
         "fmmb_plan_create": [vp, dp, i64, C.POINTER(_TreeOpts), C.POINTER(vp)],
         "fmmb_plan_create_dev": [vp, dp, i64, C.POINTER(_TreeOpts), C.POINTER(vp)],
         "fmmb_plan_destroy": [vp],
+        "fmmb_batch_plan_create": [vp, dp, dp, i64, C.POINTER(_TreeOpts), dp, C.POINTER(vp)],
+        "fmmb_batch_plan_create_dev": [vp, dp, dp, i64, C.POINTER(_TreeOpts), dp, C.POINTER(vp)],
+        "fmmb_batch_plan_instances": [vp, C.POINTER(i64), dp, dp, dp, dp],
         "fmmb_plan_info": [vp, dp, i32],
         "fmmb_plan_box": [vp, dp, dp],
         "fmmb_plan_tree": [vp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp],
@@ -460,6 +464,70 @@ class FMM:
             self._h = None
 
 
+class BatchFMM(FMM):
+    """Several independent FMMs of one method in one plan (fmmb_batch_plan_create): each point set
+    of `sources` (a list of (N_i, 3) arrays) gets its own tree in its own box (`bbox`: None for each
+    set's square_bbox, one (origin, width) for all, or a list of them), fitted in order as FMM(...)
+    calls with the same cache would fit them. One tree build, one list build and one launch per
+    pass and level serve every instance, and each instance's results are bitwise those of its own
+    FMM. States, build_expansions and evaluate_at_sources take the plan like any other FMM, with
+    the instances' points, densities and outputs concatenated in order (`concat`, `split`)."""
+
+    def __init__(self, method, sources, ppl=50, bbox=None, cache=None, max_levels=30):
+        cache = cache if cache is not None else OperatorCache(method)
+        if cache.method is not method:
+            raise ArgumentError(1, "the cache was built for a different method")
+        if getattr(method, "dimension", 3) != 3:
+            raise Unsupported(6, "batch plans take the 3D harmonic methods")
+        self.method, self.cache = method, cache
+        xs = [_pts(method, x) for x in sources]
+        if not xs:
+            raise ArgumentError(1, "no instances")
+        self.counts = np.array([x.shape[0] for x in xs], np.int64)
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        self.sources = np.ascontiguousarray(np.concatenate(xs))
+        self.ninst, self.N = len(xs), int(self.offsets[-1])
+        opts = _TreeOpts()
+        opts.ppl, opts.max_levels = int(ppl), int(max_levels)
+        boxes = None
+        if bbox is not None:
+            bl = [bbox] * self.ninst if (len(bbox) == 2 and np.ndim(bbox[1]) == 0) else list(bbox)
+            if len(bl) != self.ninst:
+                raise DimensionMismatch(2, f"{len(bl)} boxes for {self.ninst} instances")
+            boxes = np.array([[*map(float, b[0]), float(b[1])] for b in bl], np.float64)
+        h = C.c_void_p()
+        _check(lib().fmmb_batch_plan_create(cache._h, _ptr(self.sources), _ptr(self.counts), self.ninst,
+                                            C.byref(opts), _ptr(boxes), C.byref(h)))
+        self._h = h
+        info = np.zeros(4 + 512, np.int64)
+        _check(lib().fmmb_plan_info(self._h, _ptr(info), len(info)))
+        self.nlevels, self.nnodes, self.npairs = int(info[0]), int(info[1]), int(info[3])
+        self.level_start = info[4:4 + self.nlevels + 1].copy()
+        n = C.c_int64()
+        self.boxes = np.zeros((self.ninst, 4))
+        self.root_level = np.zeros(self.ninst, np.int32)
+        self.node_instance = np.zeros(self.nnodes, np.int32)
+        _check(lib().fmmb_batch_plan_instances(self._h, C.byref(n), None, _ptr(self.boxes), _ptr(self.root_level),
+                                               _ptr(self.node_instance)))
+        o = np.zeros(3)
+        w = C.c_double()
+        _check(lib().fmmb_plan_box(self._h, _ptr(o), C.byref(w)))
+        self.origin, self.width = o, w.value
+
+    def split(self, a):
+        """The per-instance pieces of an array in the concatenated (instance) order."""
+        return [a[self.offsets[i]:self.offsets[i + 1]] for i in range(self.ninst)]
+
+    def concat(self, arrays):
+        """The per-instance arrays (densities), concatenated in instance order."""
+        if len(arrays) != self.ninst:
+            raise DimensionMismatch(2, f"{len(arrays)} arrays for {self.ninst} instances")
+        for i, a in enumerate(arrays):
+            if len(a) != self.counts[i]:
+                raise DimensionMismatch(2, f"instance {i}: {len(a)} values for {self.counts[i]} points")
+        return np.ascontiguousarray(np.concatenate([np.asarray(a, np.float64) for a in arrays]))
+
+
 class FMMState:
     """FMMState (src/fmm.jl:64-94): the expansions of one right-hand side on the device.
     precision: "fp64" (the plain drop-in path) or "mixed"."""
@@ -709,7 +777,7 @@ class StokesFMMPlan:
     provides the :harmonics method with Stokeslet, stresslet and doublet densities and velocity and
     pressure outputs."""
 
-    def __init__(self, sources, method="harmonics", p=16, ppl=200, bbox=None, targets=None):
+    def __init__(self, sources, method="harmonics", p=16, ppl=200, bbox=None, targets=None, cache=None):
         if method != "harmonics":
             raise Unsupported(6, "the device path provides method=:harmonics")
         self.sources = _points(sources)
@@ -717,8 +785,26 @@ class StokesFMMPlan:
         if bbox is None:
             bbox = square_bbox(self.sources if self.targets is None
                                else np.concatenate([self.sources, self.targets]))
-        self.method = StokesHarmonics(Stokeslet3D(), p=p)
-        self.fmm = FMM(self.method, self.sources, ppl=ppl, bbox=bbox)
+        # cache: an OperatorCache of a StokesHarmonics(Stokeslet3D(), p) method shared by plans
+        self.method = cache.method if cache is not None else StokesHarmonics(Stokeslet3D(), p=p)
+        self.fmm = FMM(self.method, self.sources, ppl=ppl, bbox=bbox, cache=cache)
+        self.state = FMMState(self.fmm, "fp64")
+
+
+class BatchStokesFMMPlan(StokesFMMPlan):
+    """Many StokesFMMPlans in one batch plan (fmmb_batch_plan_create): StokesHarmonics(Stokeslet3D();
+    p) self plans of the point sets in `sources` (a list of (N_i, 3) arrays), each in its own box
+    (`bbox` as BatchFMM takes it; None: each set's square_bbox), computed together; stokes_fmm_eval
+    takes the densities concatenated in instance order (plan.fmm.concat) and returns the outputs so
+    (plan.fmm.split)."""
+
+    def __init__(self, sources, method="harmonics", p=16, ppl=200, bbox=None, cache=None):
+        if method != "harmonics":
+            raise Unsupported(6, "the device path provides method=:harmonics")
+        self.method = cache.method if cache is not None else StokesHarmonics(Stokeslet3D(), p=p)
+        self.fmm = BatchFMM(self.method, sources, ppl=ppl, bbox=bbox, cache=cache)
+        self.sources = self.fmm.sources
+        self.targets = None
         self.state = FMMState(self.fmm, "fp64")
 
 

@@ -118,6 +118,29 @@ int fmmb_plan_tree(const fmmb_plan* plan, int32_t* cell, int32_t* level, int32_t
  * unspecified order (src/tree/lists.jl:15-70); returns the count in *npairs. */
 int fmmb_plan_pairs(const fmmb_plan* plan, int level, int32_t* tgt, int32_t* src, int32_t* far, int64_t cap, int64_t* npairs);
 
+/* A batch of independent FMMs in one plan (no counterpart in the reference, whose DevicePlan(m,
+ * groups) puts several point sets in ONE tree, src/device_passes.jl:112-134): ninst point sets,
+ * instance i the counts[i] points after those of instances 0..i-1 in xyz (3 × Σcounts), each with
+ * its own tree in its own box (boxes: 4 per instance, origin and width; NULL: each set's
+ * square_bbox), the boxes fitted by fit_box! in instance order exactly as plans created one after
+ * another with this cache would be. One tree build, one list build, and one launch per pass and
+ * level serve every instance; each instance's tree, far pairs and results are bitwise those of its
+ * own plan (fmmb_plan_create with the same cache, box and options). The states, builds and
+ * evaluations at the sources take the plan like any other, with all instances' points, densities
+ * and outputs concatenated in instance order; evaluations at targets are not provided for a batch
+ * (FMMB_ERR_UNSUPPORTED), nor the kernel-independent methods. Levels are global: level l holds the
+ * nodes of width ldexp(W, -l), W the widest root's, and an instance's root lies on the level of its
+ * width. */
+int fmmb_batch_plan_create(fmmb_cache* cache, const double* xyz, const int64_t* counts, int64_t ninst,
+                           const fmmb_tree_opts* opts, const double* boxes, fmmb_plan** out);
+int fmmb_batch_plan_create_dev(fmmb_cache* cache, const double* xyz_dev, const int64_t* counts, int64_t ninst,
+                               const fmmb_tree_opts* opts, const double* boxes, fmmb_plan** out);
+/* The instances of a plan (1 for a plan of one point set): *ninst, and where not NULL offsets
+ * (ninst + 1: the first point of each instance, then the total), boxes (4 × ninst), root_level
+ * (ninst: the global level of each root) and node_instance (nnodes). */
+int fmmb_batch_plan_instances(const fmmb_plan* plan, int64_t* ninst, int64_t* offsets, double* boxes,
+                              int32_t* root_level, int32_t* node_instance);
+
 /* FMMState (src/fmm.jl:64-94): the expansions of one right-hand side, in a precision path. */
 int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out);
 int fmmb_state_destroy(fmmb_state* state);
