@@ -3,13 +3,17 @@
 //
 // Per symmetry class and chunk of ≤ NB pairs of the block:
 //   gather  G = P_sᵀ M_src for the chunk's columns into shared memory ([column][entry], one
-//           coalesced load per lane and entry quartet, the D4h permutation computed from the
-//           offset's group element, partner entries by warp shuffles)
+//           coalesced load per lane and entry quartet, the D4h permutation of each entry looked
+//           up in a table of its swaps and signs over the 16 group elements, built once per
+//           CTA; partner entries by warp shuffles)
 //   product Y = A_class G on the FP64 tensor cores (mma.sync m8n8k4 f64, DMMA: there is no FP64
 //           tcgen05 kind), A streamed through shared memory in K-slabs of 16 with the next slab
 //           prefetched into registers; each warp an (LD/8 rows) × NB register tile
-//   scatter (P_t Y) summed over the consecutive pairs of each target, one update of the
-//           target's partial local per run (the block owns its targets: deterministic, no atomics)
+//   scatter (P_t Y) into the targets' partial locals: each target's entry takes its pairs one by
+//           one in the list's order, starting from the value in memory (the block owns its
+//           targets: deterministic, no atomics, and the sums do not depend on where the chunks
+//           end nor on the other targets of the block); the partial locals of four targets are
+//           read at once
 #include "d4h.cuh"
 #include "passes.cuh"
 
@@ -37,9 +41,29 @@ __device__ __forceinline__ void dmma(double* d, double a, double b) {
                : "d"(a), "d"(b));
 }
 
+// over the 16 D4h elements (bit f for element f): whether entry k takes its partner's value
+// (low half) and whether it is negated (high half); the source side (P_sᵀ, q = −m·rot) names the
+// sign by the entry's own part, the target side (P_t, q = +m·rot) by the part it reads
+__device__ __forceinline__ uint32_t perm_masks(int k, bool target) {
+  int n, m, part;
+  coef_nmp(k, n, m, part);
+  uint32_t swap = 0, neg = 0;
+  for (int f = 0; f < 16; ++f) {
+    const int q = ((target ? m : -m) * (f & 3)) & 3;
+    const bool sw = part != 0 && (q & 1);
+    swap |= (uint32_t)sw << f;
+    neg |= (uint32_t)(perm_sign(target && sw ? 3 - part : part, q, n + m, f) < 0) << f;
+  }
+  return swap | neg << 16;
+}
+
+template <int LD, int NB>
+constexpr size_t m2l_f64_smem() {
+  return sizeof(double) * (16 * (LD + 4) + NB * (LD + 4)) + sizeof(int) * 4 * NB + sizeof(uint32_t) * LD + LD;
+}
 // two CTAs per SM where their shared memory fits (the registers are then capped at 128)
 template <int LD, int NB>
-constexpr int m2l_f64_ctas() { return (16 + NB) * (LD + 4) * 8 + 12 * NB <= 113 * 1024 ? 2 : 1; }
+constexpr int m2l_f64_ctas() { return m2l_f64_smem<LD, NB>() <= 113 * 1024 ? 2 : 1; }
 
 template <int LD, int NB>
 __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const int4* __restrict__ blocks, const int* __restrict__ cls_off,
@@ -61,12 +85,37 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
   int* ps = (int*)(G + NB * GS);
   int* pf = ps + NB;
   int* pt = pf + NB;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4, warp = tid >> 5, lane = tid & 31;
+  int* pfac = pt + NB;               // the pairs' D4h elements
+  uint32_t* smsk = (uint32_t*)(pfac + NB);   // [LD]: the gather's masks per entry (0 past NP)
+  int8_t* sdir = (int8_t*)(smsk + LD);       // [LD]: where each entry's partner is (+1 Re, −1 Im, 0)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int4 b = blocks[blockIdx.x];
   const int level = b.x & 255;
   const double alpha = m2l_scale[level];
   const int* co = cls_off + (int64_t)blockIdx.x * (NCLASS + 1);
   const int kmax = (NP + BK - 1) / BK * BK;
+  for (int k = tid; k < LD; k += 256) {
+    int n, m, part;
+    coef_nmp(k, n, m, part);
+    smsk[k] = k < NP ? perm_masks(k, false) : 0u;
+    sdir[k] = (int8_t)(k < NP && part != 0 ? (part == 1 ? 1 : -1) : 0);
+  }
+  // the scatter's entries of this thread (j = tid + 256 i): their partners and target-side masks
+  constexpr int EPT = (LD + 255) / 256;
+  uint32_t tmsk[EPT];
+  int tpart[EPT];
+#pragma unroll
+  for (int i = 0; i < EPT; ++i) {
+    const int j = tid + 256 * i;
+    tmsk[i] = 0;
+    tpart[i] = j;
+    if (j < NP) {
+      int n, m, part;
+      coef_nmp(j, n, m, part);
+      tpart[i] = part == 0 ? j : (part == 1 ? j + 1 : j - 1);
+      tmsk[i] = perm_masks(j, true);
+    }
+  }
   for (int c = 0; c < NCLASS; ++c) {
     const int a0 = co[c], a1 = co[c + 1];
     const double* A = reinterpret_cast<const double*>(reps_lv[level]) + (int64_t)c * LD * LD;   // the level's representatives
@@ -76,13 +125,13 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
       for (int j = tid; j < NB; j += 256) {
         if (j < nc) {
           const int2 pr = pairs[b.w + q0 + j];
-          ps[j] = pr.x; pf[j] = pr.y >> 8; pt[j] = pr.y & 0xff;
-        } else { ps[j] = -1; pf[j] = 0; pt[j] = -1; }
+          ps[j] = pr.x; pf[j] = pr.y >> 8; pt[j] = pr.y & 0xff; pfac[j] = c_d4h[pr.y >> 8];
+        } else { ps[j] = -1; pf[j] = 0; pt[j] = -1; pfac[j] = 0; }
       }
       __syncthreads();
       // gather: warp w the columns w, w + 8, ...; lane l the entries 4(l + 32 r) .. + 3
       for (int j = warp; j < nc; j += 8) {
-        const int fac = c_d4h[pf[j]];
+        const int fac = pfac[j];
         const double* src = M + (int64_t)ps[j] * pitch + (int64_t)comp * LD;
         // the Stokes Ψ̂ block: its source is Ψ̂ + o·Φ of the source box, o the far offset
         // (harmonics_stokes.jl: M2L Ψ̂_B = Ψ̂_A + o·Φ, linear in the source)
@@ -110,15 +159,17 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
           const double nxt = __shfl_down_sync(0xffffffffu, a[0], 1);
           const double prv = __shfl_up_sync(0xffffffffu, a[3], 1);
           if (k0 < LD) {
+            // a swapped entry takes its partner: the next one for a real part, the previous for
+            // an imaginary part (parts alternate Re, Im from an odd offset within the degree)
+            const uint4 mk = *reinterpret_cast<const uint4*>(smsk + k0);
+            const char4 dr = *reinterpret_cast<const char4*>(sdir + k0);
+            const uint32_t mm[4] = {mk.x, mk.y, mk.z, mk.w};
+            const int dd[4] = {dr.x, dr.y, dr.z, dr.w};
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-              int n, m, part;
-              coef_nmp(k0 + e, n, m, part);
-              const int q = (-m * (fac & 3)) & 3;
-              const bool sw = part != 0 && (q & 1);
               double x = a[e];
-              if (sw) x = part == 1 ? (e < 3 ? a[e + 1] : nxt) : (e > 0 ? a[e - 1] : prv);
-              G[j * GS + k0 + e] = k0 + e < NP ? (perm_sign(part, q, n + m, fac) < 0 ? -x : x) : 0.0;
+              if ((mm[e] >> fac) & 1) x = dd[e] > 0 ? (e < 3 ? a[e + 1] : nxt) : (e > 0 ? a[e - 1] : prv);
+              G[j * GS + k0 + e] = k0 + e < NP ? ((mm[e] >> (16 + fac)) & 1 ? -x : x) : 0.0;
             }
           }
         }
@@ -173,29 +224,38 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
 #pragma unroll
           for (int i = 0; i < 2; ++i) G[(8 * nt + 2 * t + i) * GS + warp * (LD / 8) + 8 * mt + g] = acc[mt][nt][i];
       __syncthreads();
-      // scatter: thread j owns entry j of the targets' partial locals; each target's entry takes
-      // its pairs one by one in the list's order (read once per run of the target, written
-      // once), so the sums do not depend on where the chunks of NB pairs end, nor on which
-      // other targets share the block
-      for (int j = tid; j < NP; j += 256) {
-        int n, m, part;
-        coef_nmp(j, n, m, part);
-        const int partner = part == 0 ? j : (part == 1 ? j + 1 : j - 1);
-        int cur = -1;
-        double run = 0.0;
-        for (int qq = 0; qq < nc; ++qq) {
-          const int t = pt[qq], fac = c_d4h[pf[qq]];
-          if (t != cur) {
-            if (cur >= 0) Pl[(int64_t)(b.y + cur) * pitch + (int64_t)comp * LD + j] = run;
-            cur = t;
-            run = Pl[(int64_t)(b.y + t) * pitch + (int64_t)comp * LD + j];
+      // scatter: thread j owns entry j of the targets' partial locals, four targets (runs of the
+      // chunk's pairs) at a time
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int j = tid + 256 * i;
+        if (j >= NP) continue;
+        const int jp = tpart[i];
+        const uint32_t mk = tmsk[i];
+        double* plj = Pl + (int64_t)b.y * pitch + (int64_t)comp * LD + j;
+        for (int q = 0; q < nc;) {
+          int st[4], en[4], tg[4];
+          double pv[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            st[r] = q;
+            tg[r] = q < nc ? pt[q] : 0;
+            pv[r] = q < nc ? plj[(int64_t)tg[r] * pitch] : 0.0;
+            while (q < nc && pt[q] == tg[r]) ++q;
+            en[r] = q;
           }
-          const int q = (m * (fac & 3)) & 3;
-          const bool sw = part != 0 && (q & 1);
-          const double y = G[qq * GS + (sw ? partner : j)];
-          run = fma(alpha, perm_sign(sw ? 3 - part : part, q, n + m, fac) < 0 ? -y : y, run);
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            if (st[r] < en[r]) {
+              double run = pv[r];
+              for (int k = st[r]; k < en[r]; ++k) {
+                const int f = pfac[k];
+                const double y = G[k * GS + ((mk >> f) & 1 ? jp : j)];
+                run = fma(alpha, (mk >> (16 + f)) & 1 ? -y : y, run);
+              }
+              plj[(int64_t)tg[r] * pitch] = run;
+            }
         }
-        if (cur >= 0) Pl[(int64_t)(b.y + cur) * pitch + (int64_t)comp * LD + j] = run;
       }
     }
   }
@@ -209,7 +269,7 @@ void launch(State& S) {
   Cache& C = *P.cache;
   const int nb = (int)P.h_blocks.size();
   if (nb == 0) return;
-  const size_t smem = sizeof(double) * (16 * (LD + 4) + NB * (LD + 4)) + sizeof(int) * 3 * NB;
+  const size_t smem = m2l_f64_smem<LD, NB>();
   auto kern = k_m2l_f64<LD, NB>;
   FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // one launch: blockIdx.x the target block, blockIdx.y the expansion block (the CTAs of different
