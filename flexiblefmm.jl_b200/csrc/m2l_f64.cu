@@ -129,47 +129,65 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
         } else { ps[j] = -1; pf[j] = 0; pt[j] = -1; pfac[j] = 0; }
       }
       __syncthreads();
-      // gather: warp w the columns w, w + 8, ...; lane l the entries 4(l + 32 r) .. + 3
-      for (int j = warp; j < nc; j += 8) {
-        const int fac = pfac[j];
-        const double* src = M + (int64_t)ps[j] * pitch + (int64_t)comp * LD;
-        // the Stokes Ψ̂ block: its source is Ψ̂ + o·Φ of the source box, o the far offset
-        // (harmonics_stokes.jl: M2L Ψ̂_B = Ψ̂_A + o·Φ, linear in the source)
-        double o3[3] = {0.0, 0.0, 0.0};
-        if (psi)
-          for (int d = 0; d < 3; ++d) o3[d] = (double)c_faroff[3 * pf[j] + d];
+      // gather: warp w the columns w, w + 8, ..., two at a time (both columns' loads in flight
+      // before either is permuted); lane l the entries 4(l + 32 r) .. + 3
+      for (int j0 = warp; j0 < nc; j0 += 16) {
+        double a[2][Q][4];
 #pragma unroll
-        for (int r = 0; r < Q; ++r) {
-          const int k0 = 4 * (lane + 32 * r);
-          double a[4];
-          if (k0 < LD) {
-            const double2 u = __ldg(reinterpret_cast<const double2*>(src + k0));
-            const double2 w = __ldg(reinterpret_cast<const double2*>(src + k0 + 2));
-            a[0] = u.x; a[1] = u.y; a[2] = w.x; a[3] = w.y;
-            if (psi) {
-              const double* base = M + (int64_t)ps[j] * pitch;
+        for (int h = 0; h < 2; ++h) {
+          const int j = j0 + 8 * h;
+          const bool on = j < nc;
+          const double* src = M + (int64_t)(on ? ps[j] : 0) * pitch + (int64_t)comp * LD;
+          // the Stokes Ψ̂ block: its source is Ψ̂ + o·Φ of the source box, o the far offset
+          // (harmonics_stokes.jl: M2L Ψ̂_B = Ψ̂_A + o·Φ, linear in the source)
+          double o3[3] = {0.0, 0.0, 0.0};
+          if (psi && on)
+            for (int d = 0; d < 3; ++d) o3[d] = (double)c_faroff[3 * pf[j] + d];
 #pragma unroll
-              for (int d = 0; d < 3; ++d) {
-                const double2 u2 = __ldg(reinterpret_cast<const double2*>(base + (int64_t)d * LD + k0));
-                const double2 w2 = __ldg(reinterpret_cast<const double2*>(base + (int64_t)d * LD + k0 + 2));
-                a[0] += o3[d] * u2.x; a[1] += o3[d] * u2.y; a[2] += o3[d] * w2.x; a[3] += o3[d] * w2.y;
+          for (int r = 0; r < Q; ++r) {
+            const int k0 = 4 * (lane + 32 * r);
+            if (on && k0 < LD) {
+              const double2 u = __ldg(reinterpret_cast<const double2*>(src + k0));
+              const double2 w = __ldg(reinterpret_cast<const double2*>(src + k0 + 2));
+              a[h][r][0] = u.x; a[h][r][1] = u.y; a[h][r][2] = w.x; a[h][r][3] = w.y;
+              if (psi) {
+                const double* base = M + (int64_t)ps[j] * pitch;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                  const double2 u2 = __ldg(reinterpret_cast<const double2*>(base + (int64_t)d * LD + k0));
+                  const double2 w2 = __ldg(reinterpret_cast<const double2*>(base + (int64_t)d * LD + k0 + 2));
+                  a[h][r][0] += o3[d] * u2.x; a[h][r][1] += o3[d] * u2.y;
+                  a[h][r][2] += o3[d] * w2.x; a[h][r][3] += o3[d] * w2.y;
+                }
               }
+            } else {
+              a[h][r][0] = a[h][r][1] = a[h][r][2] = a[h][r][3] = 0.0;
             }
-          } else { a[0] = a[1] = a[2] = a[3] = 0.0; }
-          const double nxt = __shfl_down_sync(0xffffffffu, a[0], 1);
-          const double prv = __shfl_up_sync(0xffffffffu, a[3], 1);
-          if (k0 < LD) {
-            // a swapped entry takes its partner: the next one for a real part, the previous for
-            // an imaginary part (parts alternate Re, Im from an odd offset within the degree)
-            const uint4 mk = *reinterpret_cast<const uint4*>(smsk + k0);
-            const char4 dr = *reinterpret_cast<const char4*>(sdir + k0);
-            const uint32_t mm[4] = {mk.x, mk.y, mk.z, mk.w};
-            const int dd[4] = {dr.x, dr.y, dr.z, dr.w};
+          }
+        }
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              double x = a[e];
-              if ((mm[e] >> fac) & 1) x = dd[e] > 0 ? (e < 3 ? a[e + 1] : nxt) : (e > 0 ? a[e - 1] : prv);
-              G[j * GS + k0 + e] = k0 + e < NP ? ((mm[e] >> (16 + fac)) & 1 ? -x : x) : 0.0;
+        for (int h = 0; h < 2; ++h) {
+          const int j = j0 + 8 * h;
+          if (j >= nc) continue;                       // warp-uniform
+          const int fac = pfac[j];
+#pragma unroll
+          for (int r = 0; r < Q; ++r) {
+            const int k0 = 4 * (lane + 32 * r);
+            const double nxt = __shfl_down_sync(0xffffffffu, a[h][r][0], 1);
+            const double prv = __shfl_up_sync(0xffffffffu, a[h][r][3], 1);
+            if (k0 < LD) {
+              // a swapped entry takes its partner: the next one for a real part, the previous
+              // for an imaginary part
+              const uint4 mk = *reinterpret_cast<const uint4*>(smsk + k0);
+              const char4 dr = *reinterpret_cast<const char4*>(sdir + k0);
+              const uint32_t mm[4] = {mk.x, mk.y, mk.z, mk.w};
+              const int dd[4] = {dr.x, dr.y, dr.z, dr.w};
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                double x = a[h][r][e];
+                if ((mm[e] >> fac) & 1) x = dd[e] > 0 ? (e < 3 ? a[h][r][e + 1] : nxt) : (e > 0 ? a[h][r][e - 1] : prv);
+                G[j * GS + k0 + e] = k0 + e < NP ? ((mm[e] >> (16 + fac)) & 1 ? -x : x) : 0.0;
+              }
             }
           }
         }
