@@ -265,6 +265,16 @@ def serving(fmmb, device, count, slots):
     tk = [srv.submit(pts, tau, tol=tol, kappa=kappa) for pts, tau, tol, kappa in reqs]
     infos = [srv.wait(k)[2] for k in tk]
     t_batch = time.perf_counter() - t0
+    # where a request's time goes: its plan (tree, lists, operators, state) on the host against its
+    # matvec (host call and span on the slot's stream), summed per path over the batched pass
+    per_path = {}
+    for (pts, tau, tol, kappa), i in zip(reqs, infos):
+        key = ("yukawa" if kappa is not None else "laplace") + "_" + i["precision"]
+        d = per_path.setdefault(key, {"requests": 0, "points": 0, "plan_s": 0.0, "matvec_s": 0.0, "device_s": 0.0})
+        d["requests"] += 1
+        d["points"] += len(pts)
+        for k in ("plan_s", "matvec_s", "device_s"):
+            d[k] += i[k]
     rate = 0.8 * count / t_batch                                       # requests/s offered in the open loop
     rng = np.random.default_rng(60)
     gaps = rng.exponential(1.0 / rate, count)
@@ -279,7 +289,7 @@ def serving(fmmb, device, count, slots):
     lat = [srv.wait(k)[2]["latency_s"] for k in tk]
     t_open = time.perf_counter() - t0
     srv.close()
-    one = fmmb.Server(device, slots=1)
+    one = fmmb.Server(device, slots=1, group_max=1)
     for pts, tau, tol, kappa in reqs[:3]:
         one.wait(one.submit(pts, tau, tol=tol, precision="fp64", kappa=kappa))
     t0 = time.perf_counter()
@@ -291,15 +301,17 @@ def serving(fmmb, device, count, slots):
     q = lambda v, f: float(np.quantile(np.asarray(v) * 1e3, f))
     return {"requests": count, "slots": slots, "points": total,
             "workload": "Laplace3D or Yukawa3D(kappa=5) 50/50, N log-uniform [1e3, 5e5], uniform or 4-Gaussian (sigma 0.02) "
-                        "points, tol in {1e-3, 1e-6, 1e-9} (p and precision path chosen from tol; Yukawa on the FP64 "
-                        "path) (seed 6)",
+                        "points, tol in {1e-3, 1e-6, 1e-9} (p and precision path chosen from tol) (seed 6)",
             "batched": {"evals_per_s": total / t_batch, "requests_per_s": count / t_batch, "seconds": t_batch},
             "open_loop": {"offered_requests_per_s": rate, "evals_per_s": total / t_open,
                           "fraction_of_batched": (total / t_open) / (total / t_batch),
                           "latency_ms": {"p50": q(lat, 0.5), "p99": q(lat, 0.99)}},
             "one_at_a_time_fp64": {"evals_per_s": total / t_seq, "latency_ms": {"p50": q(seq_lat, 0.5), "p99": q(seq_lat, 0.99)}},
             "paths": {"mixed": sum(i["precision"] == "mixed" for i in infos), "fp64": sum(i["precision"] == "fp64" for i in infos),
-                      "yukawa": sum(r[3] is not None for r in reqs)}}
+                      "yukawa": sum(r[3] is not None for r in reqs)},
+            "time_per_path_s": per_path,
+            "host_device_s": {"plan": sum(i["plan_s"] for i in infos), "matvec": sum(i["matvec_s"] for i in infos),
+                              "device": sum(i["device_s"] for i in infos)}}
 
 # ---------------------------------------------------------------- batched Stokes
 def stokes_workload(count, seed=5):

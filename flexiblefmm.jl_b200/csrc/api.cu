@@ -359,6 +359,19 @@ int fmmb_ctx_create(int device, fmmb_ctx** out) {
     FMMB_CUDA(cudaStreamCreateWithPriority(&h->c.stream, cudaStreamNonBlocking, hi));
     h->c.own_stream = true;
     init_device_constants(h->c.stream);
+    // the device's stream-ordered pool keeps up to 16 GiB of freed memory mapped instead of
+    // returning it at every synchronisation, so that the buffers of one plan after another (a
+    // server's requests, a time-stepping loop) reuse memory instead of mapping it again
+    {
+      cudaMemPool_t pool;
+      FMMB_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+      uint64_t keep = 0;
+      FMMB_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+      if (keep < (16ull << 30)) {
+        keep = 16ull << 30;
+        FMMB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+      }
+    }
     direct_noalloc_prepare();                       // the no-allocation scratch's address, at set-up
     *out = h.release();
   });
@@ -643,8 +656,11 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
     require(plan && out, FMMB_ERR_ARGUMENT, "null argument");
     require(precision == FMMB_PRECISION_FP64 || precision == FMMB_PRECISION_MIXED, FMMB_ERR_ARGUMENT, "unknown precision path");
     Plan& P = plan->p;
-    require(P.cache->kernel == FMMB_KERNEL_LAPLACE3D || precision == FMMB_PRECISION_FP64, FMMB_ERR_UNSUPPORTED,
-            "the Stokeslet and Yukawa methods run on the FP64 path");
+    require(P.cache->kernel != FMMB_KERNEL_STOKESLET3D || precision == FMMB_PRECISION_FP64, FMMB_ERR_UNSUPPORTED,
+            "the Stokeslet method runs on the FP64 path");
+    require(P.cache->kernel != FMMB_KERNEL_YUKAWA3D || precision == FMMB_PRECISION_FP64 ||
+                P.cache->method == FMMB_METHOD_SPHERICAL_HARMONICS,
+            FMMB_ERR_UNSUPPORTED, "the Yukawa method's mixed path is the harmonic one");
     set_device(*P.ctx);
     cudaStream_t s = P.ctx->stream;
     std::unique_ptr<fmmb_state> h(new fmmb_state());
@@ -664,6 +680,7 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
     } else if (precision == FMMB_PRECISION_MIXED) {
       std::lock_guard<std::mutex> lk(P.cache->mu);
       prepare_mixed_operators(*P.cache);
+      prepare_mixed_levels(P);
     }
     FMMB_CUDA(cudaStreamSynchronize(s));
     h->parent = plan;

@@ -567,10 +567,12 @@ void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount
                 const double* tz, const int* tout, int outputs, double* pot, double* grad, int acc = 0) {
   Plan& P_ = *S.plan;
   const int warps = 8;
-  const bool mixed = S.precision == FMMB_PRECISION_MIXED;
+  // the mixed path evaluates Laplace3D in FP32; Yukawa3D keeps its radial weights in FP64 (its
+  // mixed path is the tensor-core M2L only)
+  const bool yk = P_.cache->kernel == FMMB_KERNEL_YUKAWA3D;
+  const bool mixed = S.precision == FMMB_PRECISION_MIXED && !yk;
   const size_t smem = (mixed ? sizeof(float) : sizeof(double)) * warps * P_.cache->ld;
-  auto kern = mixed ? k_l2p<P, float, false>
-                    : (P_.cache->kernel == FMMB_KERNEL_YUKAWA3D ? k_l2p<P, double, true> : k_l2p<P, double, false>);
+  auto kern = mixed ? k_l2p<P, float, false> : (yk ? k_l2p<P, double, true> : k_l2p<P, double, false>);
   kern<<<(ng + warps - 1) / warps, 32 * warps, smem, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, P_.cell.p,
                                                                       S.Pl.p, P_.cache->ld, geometry(P_), P_.d_scale.p,
                                                                       outputs, pot, grad, P_.d_kh2.p, acc);
@@ -644,8 +646,7 @@ void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* g
     FMMB_LAUNCH_CHECK();
     return;
   }
-  if (S.plan->cache->kernel == FMMB_KERNEL_YUKAWA3D) {
-    require(!mixed, FMMB_ERR_UNSUPPORTED, "Yukawa3D runs on the FP64 path");
+  if (S.plan->cache->kernel == FMMB_KERNEL_YUKAWA3D) {   // the near field in FP64 on both paths
     if (self) launch_near<double, true, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
     else launch_near<double, false, true>(S, gnode, gstart, gcount, ng, tx, ty, tz, tout, outputs, pot, grad);
     return;

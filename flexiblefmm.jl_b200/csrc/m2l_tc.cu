@@ -377,14 +377,15 @@ struct TcCtl {
 
 // blocks: (level, first node, count, pair base); cls_off: per block the class offsets of its
 // pairs; rtab/rounds: the round table (per class and target count << 16 | offset; per class the
-// rounds); reps16/row_scale: the class operators (head, tail) and their inverse row scales;
+// rounds); reps16_lv/rsc_lv: per level the class operators (head, tail) and their inverse row
+// scales;
 // perm16: the source-side sign words; Mh/Ml/lsc: the split multipoles (two copies vstride
 // apart) and the inverse scale of each level
 template <int KP>
 __global__ void __launch_bounds__(THREADS, 1)
 k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const int2* __restrict__ pairs,
-         const int* __restrict__ rtab, const int* __restrict__ rounds, int TB, const uint16_t* __restrict__ reps16,
-         const float* __restrict__ row_scale, const uint32_t* __restrict__ perm16, const double* __restrict__ m2l_scale,
+         const int* __restrict__ rtab, const int* __restrict__ rounds, int TB, const uint64_t* __restrict__ reps16_lv,
+         const uint64_t* __restrict__ rsc_lv, const uint32_t* __restrict__ perm16, const double* __restrict__ m2l_scale,
          int NP, int LD, int lo_off, int64_t vstride, const uint16_t* __restrict__ Mh, const uint16_t* __restrict__ Ml,
          const float* __restrict__ lsc, double* __restrict__ Pl, int* __restrict__ err, TcCtl ctl) {
   using G = Cfg<KP>;
@@ -411,6 +412,8 @@ k_m2l_tc(const int4* __restrict__ blocks, const int* __restrict__ cls_off, const
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int4 b = blocks[blockIdx.x];
+  const uint16_t* reps16 = reinterpret_cast<const uint16_t*>(reps16_lv[b.x & 255]);   // the block level's operators
+  const float* row_scale = reinterpret_cast<const float*>(rsc_lv[b.x & 255]);
   const int* co = cls_off + (int64_t)blockIdx.x * (NCLASS + 1);
   const int* nr = rounds + (int64_t)blockIdx.x * NCLASS;
   const int* rt = rtab + (int64_t)blockIdx.x * NCLASS * TB;
@@ -743,15 +746,57 @@ void prepare_mixed_operators(Cache& C) {
   if (C.split_ready) return;
   const int np = C.np;
   require(np <= NPMAX, FMMB_ERR_UNSUPPORTED, "the mixed path is built for p ≤ 11");
-  std::vector<uint16_t> h;
-  std::vector<float> rsc;
-  build_reps16(C.host, h, rsc);
   std::vector<uint32_t> perm = build_sign16(np);
-  to_device(C.reps16, h, C.ctx->stream);
-  to_device(C.row_scale, rsc, C.ctx->stream);
   to_device(C.perm16, perm, C.ctx->stream);
+  if (C.kernel != FMMB_KERNEL_YUKAWA3D) {          // Yukawa3D: the operators of each width, per level
+    std::vector<uint16_t> h;
+    std::vector<float> rsc;
+    build_reps16(C.host, h, rsc);
+    to_device(C.reps16, h, C.ctx->stream);
+    to_device(C.row_scale, rsc, C.ctx->stream);
+  }
   FMMB_CUDA(cudaStreamSynchronize(C.ctx->stream));
   C.split_ready = true;
+}
+
+// the per-level tables of the mixed path's operators (the cache locked by the caller): the
+// cache's split operators on every level, or for Yukawa3D each level width's, split from its
+// class operators (copied to the host once per width and shared by the plans that use it)
+void prepare_mixed_levels(Plan& P) {
+  Cache& C = *P.cache;
+  if (P.d_lv_reps16.n == (size_t)P.L) return;
+  cudaStream_t s = P.ctx->stream;
+  std::vector<uint64_t> r16(P.L, 0), rs(P.L, 0);
+  for (int l = 0; l < P.L; ++l) {
+    if (C.kernel != FMMB_KERNEL_YUKAWA3D) {
+      r16[l] = (uint64_t)(uintptr_t)C.reps16.p;
+      rs[l] = (uint64_t)(uintptr_t)C.row_scale.p;
+      continue;
+    }
+    if (l >= (int)P.lv_yukawa.size() || !P.lv_yukawa[l]) continue;   // no far pairs on this level
+    YukawaLevel& Y = *P.lv_yukawa[l];
+    std::lock_guard<std::mutex> lk(Y.mu);
+    if (!Y.reps16.p) {
+      HostOperators op;
+      op.p = C.p; op.np = C.np; op.ld = C.ld;
+      op.reps = to_host(Y.reps.p, (size_t)NCLASS * C.ld * C.ld, s);
+      std::vector<uint16_t> h;
+      std::vector<float> rsc;
+      build_reps16(op, h, rsc);
+      // held as long as the level's other operators, outside the stream-ordered pool
+      const cudaStream_t keep = g_alloc_stream;
+      g_alloc_stream = nullptr;
+      to_device(Y.reps16, h, s);
+      to_device(Y.row_scale, rsc, s);
+      g_alloc_stream = keep;
+      FMMB_CUDA(cudaStreamSynchronize(s));
+    }
+    r16[l] = (uint64_t)(uintptr_t)Y.reps16.p;
+    rs[l] = (uint64_t)(uintptr_t)Y.row_scale.p;
+  }
+  to_device(P.d_lv_reps16, r16, s);
+  to_device(P.d_lv_rsc, rs, s);
+  FMMB_CUDA(cudaStreamSynchronize(s));
 }
 
 // the bounded waits' limit and the test hook's stalled slab, for the next launches
@@ -774,8 +819,8 @@ void launch_tc(State& S, int nb) {
   require(P.TB <= LANES, FMMB_ERR_UNSUPPORTED, "M2L blocks hold at most 128 targets");
   FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
   const TcCtl ctl{g_wait_ns.load(), g_stall_slab.load()};
-  k_m2l_tc<KP><<<nb, THREADS, G::SMEM, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, P.rtab.p, P.rounds.p, P.TB, C.reps16.p,
-                                                        C.row_scale.p, C.perm16.p, P.d_m2l_scale.p, C.np, C.ld, lo_off,
+  k_m2l_tc<KP><<<nb, THREADS, G::SMEM, P.ctx->stream>>>(P.blocks.p, P.cls_off.p, P.pairs.p, P.rtab.p, P.rounds.p, P.TB,
+                                                        P.d_lv_reps16.p, P.d_lv_rsc.p, C.perm16.p, P.d_m2l_scale.p, C.np, C.ld, lo_off,
                                                         (int64_t)P.nnodes * KP, S.Mh.p, S.Ml.p, S.Lsc.p, S.Pl.p, S.err.p, ctl);
   FMMB_LAUNCH_CHECK();
 }

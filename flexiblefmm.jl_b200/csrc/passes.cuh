@@ -222,6 +222,7 @@ void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* g
                      const double* ty, const double* tz, const int* tout, bool self, int outputs, double* pot, double* grad);
 // the mixed path (m2l_tc.cu)
 void prepare_mixed_operators(Cache& C);
+void prepare_mixed_levels(Plan& P);   // the cache locked by the caller
 void m2l_mixed(State& S);
 int mixed_error_flag(State& S);   // 1 when a bounded wait of the tensor-core M2L gave up since the last call (then cleared)
 void set_m2l_stall(long long slab, double wait_s);   // the test hook of fmmb_test_m2l_stall

@@ -21,6 +21,11 @@ struct Ctx {
 // L2L (the parent into its children), in the Laplace layouts.
 struct YukawaLevel {
   DBuf<double> reps, m2m, l2l;
+  // the mixed path's split class operators of this width (built when a mixed state first needs
+  // them, like the cache's reps16/row_scale for the homogeneous kernels)
+  std::mutex mu;
+  DBuf<uint16_t> reps16;
+  DBuf<float> row_scale;
 };
 
 // OperatorCache (src/operators/cache.jl:5-83): the base width, the host operators at the base
@@ -121,6 +126,11 @@ struct Plan {
   std::vector<const double*> lv_reps, lv_m2m, lv_l2l;
   DBuf<uint64_t> d_lv_reps;
   DBuf<double> d_kh2;
+  // the mixed path: per level the split class operators and their inverse row scales (the cache's
+  // for the homogeneous kernels, the level width's own for Yukawa3D), built with the first mixed
+  // state; the Yukawa levels they come from stay held by the plan
+  DBuf<uint64_t> d_lv_reps16, d_lv_rsc;
+  std::vector<std::shared_ptr<YukawaLevel>> lv_yukawa;
   // the kernel-independent method: every target's far pairs (source, far index), target-major
   DBuf<int> tp_ptr;
   DBuf<int2> tp;

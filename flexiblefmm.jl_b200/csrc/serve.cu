@@ -6,12 +6,18 @@
 // threads, each owning a context (its own CUDA stream) and an operator cache per order that
 // stays resident across requests. A request is admitted when a slot is free and its estimated
 // device memory fits the budget left by the requests in flight; the front request waits for
-// memory rather than being overtaken. Admitted requests build their tree, expansions and
-// evaluation on their slot's stream, so the device work of different requests overlaps; device
+// memory rather than being overtaken. A slot takes the front request together with later queued
+// requests of the same kind (kernel, order, precision path, κ, ppl, outputs) that fit the budget,
+// up to a request and point cap, and runs the group as one batch plan: one tree build, one list
+// build and one launch per pass for all of them (the per-request cost of a plan, its host
+// synchronisations and small launches, is paid once per group). Admitted groups build their
+// trees, expansions and evaluations on their slot's stream, so the device work of different
+// groups overlaps; device
 // buffers come from the stream-ordered allocator, so no request's allocation or release
 // synchronises another's stream. Every request's computation is independent of the others and
-// deterministic (its box is snapped from its own points to a power-of-two width), so its results
-// are the same alone and in any mix, on any slot.
+// deterministic (its box is snapped from its own points to a power-of-two width, and a batch
+// plan computes each of its instances bitwise as the instance's own plan would), so its results
+// are the same alone and in any mix or group, on any slot.
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -41,6 +47,8 @@ struct Job {
   int p = 0, precision = 0, slot = -1;
   int64_t bytes = 0;
   clk::time_point t_submit, t_start, t_done;
+  double plan_s = 0, matvec_s = 0, device_s = 0;
+  int group = 1;
   bool done = false;
   int status = FMMB_OK;
   std::string error;
@@ -84,6 +92,8 @@ struct fmmb_server {
   int device = 0;
   int nslots = 1;
   int ppl = 64;
+  int group_max = 64;
+  int64_t group_points = 4000000;
   int64_t budget = 0, in_use = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -99,18 +109,27 @@ struct fmmb_server {
 
 namespace {
 
-// one request on a slot: plan, state, matvec through the host-pointer entry points of the
-// slot's context, then release; returns the status
-int run_job(fmmb_server& S, int slot, Job& j, std::string& err) {
-  const int kernel = j.r.kernel;
+// the kind of a request: requests of one kind can share a batch plan
+std::tuple<int, int, int, double, int, int> kind(const fmmb_server& S, const Job& j) {
+  return std::make_tuple(j.r.kernel, j.p, j.precision, j.r.kernel == FMMB_KERNEL_YUKAWA3D ? j.r.kappa : 0.0,
+                         j.r.ppl > 0 ? j.r.ppl : S.ppl, j.r.kernel == FMMB_KERNEL_STOKESLET3D ? 0 : j.r.outputs);
+}
+
+// a group of requests of one kind on a slot: one plan (a batch plan for more than one), one
+// state, one matvec through the host-pointer entry points of the slot's context, the outputs
+// copied to each request's buffers; then release. Returns the status
+int run_group(fmmb_server& S, int slot, std::vector<Job*>& g, std::string& err) {
+  Job& j0 = *g[0];
+  const int kernel = j0.r.kernel;
+  const bool stokes = kernel == FMMB_KERNEL_STOKESLET3D;
   fmmb_cache* cache = nullptr;
   {
     auto& cs = S.caches[slot];
-    const double kappa = kernel == FMMB_KERNEL_YUKAWA3D ? j.r.kappa : 0.0;
-    const auto key = std::make_tuple(kernel, j.p, kappa);
+    const double kappa = kernel == FMMB_KERNEL_YUKAWA3D ? j0.r.kappa : 0.0;
+    const auto key = std::make_tuple(kernel, j0.p, kappa);
     auto it = cs.find(key);
     if (it == cs.end()) {
-      fmmb_method_desc m{FMMB_METHOD_SPHERICAL_HARMONICS, kernel, j.p, 0, 0.0, kappa};
+      fmmb_method_desc m{FMMB_METHOD_SPHERICAL_HARMONICS, kernel, j0.p, 0, 0.0, kappa};
       int rc = fmmb_cache_create(S.ctx[slot], &m, &cache);
       if (rc) { err = fmmb_last_error(); return rc; }
       // a request's box depends on its own points only (not on which request the slot's cache
@@ -122,23 +141,78 @@ int run_job(fmmb_server& S, int slot, Job& j, std::string& err) {
     }
   }
   fmmb_tree_opts o{};
-  o.ppl = j.r.ppl > 0 ? j.r.ppl : S.ppl;
+  o.ppl = j0.r.ppl > 0 ? j0.r.ppl : S.ppl;
   o.max_levels = 30;
+  // the group's inputs and outputs, concatenated in group order (one request: its own buffers)
+  const size_t ng = g.size();
+  const int dens = stokes ? 3 : 1;
+  std::vector<int64_t> counts(ng);
+  int64_t n = 0;
+  for (size_t i = 0; i < ng; ++i) { counts[i] = g[i]->r.n; n += g[i]->r.n; }
+  std::vector<double> xyz, tau, pot, grad;
+  const double *px = j0.r.xyz, *pt = j0.r.tau;
+  double *pp = j0.r.pot, *pg = j0.r.grad;
+  const int outputs = stokes ? 0 : j0.r.outputs;
+  const int pot_w = stokes ? 3 : 1;
+  if (ng > 1) {
+    xyz.resize(3 * n); tau.resize(dens * n);
+    int64_t off = 0;
+    for (Job* j : g) {
+      std::copy(j->r.xyz, j->r.xyz + 3 * j->r.n, xyz.begin() + 3 * off);
+      std::copy(j->r.tau, j->r.tau + dens * j->r.n, tau.begin() + dens * off);
+      off += j->r.n;
+    }
+    px = xyz.data(); pt = tau.data();
+    if (stokes || (outputs & FMMB_OUTPUT_POTENTIAL)) { pot.resize(pot_w * n); pp = pot.data(); }
+    if (!stokes && (outputs & FMMB_OUTPUT_GRADIENT)) { grad.resize(3 * n); pg = grad.data(); }
+  }
   fmmb_plan* plan = nullptr;
   fmmb_state* st = nullptr;
-  int rc = fmmb_plan_create(cache, j.r.xyz, j.r.n, &o, &plan);
-  if (!rc) rc = fmmb_state_create(plan, j.precision, &st);
+  const clk::time_point t0 = clk::now();
+  int rc = ng > 1 ? fmmb_batch_plan_create(cache, px, counts.data(), (int64_t)ng, &o, nullptr, &plan)
+                  : fmmb_plan_create(cache, px, n, &o, &plan);
+  if (!rc) rc = fmmb_state_create(plan, j0.precision, &st);
+  const clk::time_point t1 = clk::now();
+  double plan_s = seconds(t0, t1), matvec_s = 0, device_s = 0;
   if (!rc) {
-    if (kernel == FMMB_KERNEL_STOKESLET3D) rc = fmmb_stokes_eval(st, j.r.xyz, j.r.tau, j.r.n, j.r.pot);
-    else rc = fmmb_matvec(st, j.r.xyz, j.r.tau, j.r.n, j.r.outputs, j.r.pot, j.r.grad);
+    // the matvec's span on the slot's stream, beside its host time
+    cudaStream_t stream = nullptr;
+    fmmb_ctx_stream(S.ctx[slot], (void**)&stream);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const bool ev = cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess &&
+                    cudaEventRecord(e0, stream) == cudaSuccess;
+    if (stokes) rc = fmmb_stokes_eval(st, px, pt, n, pp);
+    else rc = fmmb_matvec(st, px, pt, n, outputs, pp, pg);
+    matvec_s = seconds(t1, clk::now());
+    float ms = 0;
+    if (ev && cudaEventRecord(e1, stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+      device_s = ms * 1e-3;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
   }
   if (rc) err = fmmb_last_error();
   if (st) fmmb_state_destroy(st);
   if (plan) fmmb_plan_destroy(plan);
+  if (!rc && ng > 1) {
+    int64_t off = 0;
+    for (Job* j : g) {
+      if (!pot.empty()) std::copy(pot.begin() + pot_w * off, pot.begin() + pot_w * (off + j->r.n), j->r.pot);
+      if (!grad.empty()) std::copy(grad.begin() + 3 * off, grad.begin() + 3 * (off + j->r.n), j->r.grad);
+      off += j->r.n;
+    }
+  }
+  for (Job* j : g) {
+    j->plan_s = plan_s / ng;
+    j->matvec_s = matvec_s / ng;
+    j->device_s = device_s / ng;
+    j->group = (int)ng;
+  }
   return rc;
 }
 
 void worker(fmmb_server* S, int slot) {
+  std::vector<Job*> group;
   for (;;) {
     Job* j = nullptr;
     {
@@ -152,19 +226,37 @@ void worker(fmmb_server* S, int slot) {
       j = S->pending.front();
       S->pending.pop_front();
       S->in_use += j->bytes;
-      j->slot = slot;
-      j->t_start = clk::now();
+      group.assign(1, j);
+      // later queued requests of the same kind join while they fit the caps and the budget
+      int64_t pts = j->r.n;
+      const auto k = kind(*S, *j);
+      for (auto it = S->pending.begin(); it != S->pending.end() && (int)group.size() < S->group_max;) {
+        Job* c = *it;
+        if (kind(*S, *c) == k && pts + c->r.n <= S->group_points && S->in_use + c->bytes <= S->budget) {
+          S->in_use += c->bytes;
+          pts += c->r.n;
+          group.push_back(c);
+          it = S->pending.erase(it);
+        } else {
+          ++it;
+        }
+      }
+      const clk::time_point now = clk::now();
+      for (Job* c : group) { c->slot = slot; c->t_start = now; }
     }
     S->cv_work.notify_all();   // the next request may fit too
     std::string err;
-    const int rc = run_job(*S, slot, *j, err);
+    const int rc = run_group(*S, slot, group, err);
     {
       std::lock_guard<std::mutex> lk(S->mu);
-      S->in_use -= j->bytes;
-      j->status = rc;
-      j->error = err;
-      j->t_done = clk::now();
-      j->done = true;
+      const clk::time_point now = clk::now();
+      for (Job* c : group) {
+        S->in_use -= c->bytes;
+        c->status = rc;
+        c->error = err;
+        c->t_done = now;
+        c->done = true;
+      }
     }
     S->cv_done.notify_all();
     S->cv_work.notify_all();
@@ -183,6 +275,9 @@ int fmmb_server_create(int device, const fmmb_server_opts* opts, fmmb_server** o
   S->nslots = opts->slots;
   S->ppl = opts->ppl;
   S->budget = opts->hbm_budget;
+  if (opts->group_max < 0 || opts->group_points < 0) return FMMB_ERR_ARGUMENT;
+  S->group_max = opts->group_max > 0 ? opts->group_max : 64;
+  S->group_points = opts->group_points > 0 ? opts->group_points : 4000000;
   if (S->budget == 0) {
     size_t fr = 0, tot = 0;
     if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&fr, &tot) != cudaSuccess) return FMMB_ERR_DEVICE;
@@ -208,7 +303,6 @@ int fmmb_server_submit(fmmb_server* S, const fmmb_request* r, int64_t* ticket) {
   const bool stokes = r->kernel == FMMB_KERNEL_STOKESLET3D, yukawa = r->kernel == FMMB_KERNEL_YUKAWA3D;
   if (r->kernel != FMMB_KERNEL_LAPLACE3D && !stokes && !yukawa) return FMMB_ERR_UNSUPPORTED;
   if (yukawa && !(std::isfinite(r->kappa) && r->kappa > 0)) return FMMB_ERR_ARGUMENT;
-  if (yukawa && r->precision == FMMB_PRECISION_MIXED) return FMMB_ERR_UNSUPPORTED;
   if (!r->xyz || !r->tau || r->n <= 0 || r->ppl < 0) return FMMB_ERR_ARGUMENT;
   if (stokes) {
     // Stokeslets in tau (3×n), velocities in pot (3×n), on the FP64 path
@@ -225,7 +319,7 @@ int fmmb_server_submit(fmmb_server* S, const fmmb_request* r, int64_t* ticket) {
   j->p = r->p > 0 ? r->p : order_for_tol(r->tol, r->kernel);
   if (j->p < 1 || j->p > PMAX) return FMMB_ERR_ARGUMENT;
   // the precision path: FP64 below 1e-8 (or where the mixed path has no kernel), mixed above
-  if (stokes || yukawa) j->precision = FMMB_PRECISION_FP64;   // the paths these kernels have
+  if (stokes) j->precision = FMMB_PRECISION_FP64;   // the path this kernel has
   else
     j->precision = r->precision >= 0 ? r->precision
                                      : ((r->tol < 1e-8 || (j->p + 1) * (j->p + 1) > 144) ? FMMB_PRECISION_FP64 : FMMB_PRECISION_MIXED);
@@ -259,6 +353,10 @@ int fmmb_server_wait(fmmb_server* S, int64_t ticket, double timeout_s, fmmb_requ
     info->run_s = seconds(j->t_start, j->t_done);
     info->latency_s = seconds(j->t_submit, j->t_done);
     info->bytes_estimate = j->bytes;
+    info->plan_s = j->plan_s;
+    info->matvec_s = j->matvec_s;
+    info->device_s = j->device_s;
+    info->group = j->group;
   }
   const int status = j->status;
   fmmb::set_last_error(j->error);

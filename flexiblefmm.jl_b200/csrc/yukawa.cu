@@ -312,6 +312,8 @@ void yukawa_prepare(Plan& P) {
       if (l < 2) continue;                          // no translations touch levels 0 and 1
       auto it = C.yk_levels.find(e);
       if (it == C.yk_levels.end()) it = C.yk_levels.emplace(e, level_operators(C, e, s)).first;
+      if ((int)P.lv_yukawa.size() < P.L) P.lv_yukawa.resize(P.L);
+      P.lv_yukawa[l] = it->second;
       P.lv_reps[l] = it->second->reps.p;
       P.lv_m2m[l] = it->second->m2m.p;
       P.lv_l2l[l] = it->second->l2l.p;

@@ -67,7 +67,8 @@ class _TreeOpts(C.Structure):
 
 
 class _ServerOpts(C.Structure):
-    _fields_ = [("slots", C.c_int32), ("ppl", C.c_int32), ("hbm_budget", C.c_int64)]
+    _fields_ = [("slots", C.c_int32), ("ppl", C.c_int32), ("hbm_budget", C.c_int64), ("group_max", C.c_int32),
+                ("reserved", C.c_int32), ("group_points", C.c_int64)]
 
 
 class _Request(C.Structure):
@@ -84,7 +85,8 @@ class _StokesDensities(C.Structure):
 class _RequestInfo(C.Structure):
     _fields_ = [("status", C.c_int32), ("p", C.c_int32), ("precision", C.c_int32), ("slot", C.c_int32),
                 ("queued_s", C.c_double), ("run_s", C.c_double), ("latency_s", C.c_double),
-                ("bytes_estimate", C.c_int64)]
+                ("bytes_estimate", C.c_int64), ("plan_s", C.c_double), ("matvec_s", C.c_double),
+                ("device_s", C.c_double), ("group", C.c_int32), ("reserved", C.c_int32)]
 
 
 _lib = None
@@ -665,13 +667,15 @@ def device_matvec(fmm, state, sources, tau, output=Potential()):
 class Server:
     """A continuous-batching request server on one GPU (fmmb_server): requests of different
     sizes and tolerances are admitted in arrival order onto `slots` concurrent streams as slots
-    and device memory (hbm_budget bytes; 0 = 80 % of the free memory) free up. No counterpart in
-    the reference, which runs one FMM per call."""
+    and device memory (hbm_budget bytes; 0 = 80 % of the free memory) free up; a slot runs the
+    front request with later queued ones of the same kind as one batch plan (up to group_max
+    requests and group_points points; 0: 64 and 4e6; group_max=1: one at a time). No counterpart
+    in the reference, which runs one FMM per call."""
 
-    def __init__(self, device=0, slots=4, ppl=64, hbm_budget=0):
+    def __init__(self, device=0, slots=4, ppl=64, hbm_budget=0, group_max=0, group_points=0):
         h = C.c_void_p()
-        _check(lib().fmmb_server_create(int(device), C.byref(_ServerOpts(int(slots), int(ppl), int(hbm_budget))),
-                                        C.byref(h)))
+        o = _ServerOpts(int(slots), int(ppl), int(hbm_budget), int(group_max), 0, int(group_points))
+        _check(lib().fmmb_server_create(int(device), C.byref(o), C.byref(h)))
         self._h = h
         self._live = {}
 
@@ -712,7 +716,9 @@ class Server:
         return ticket.value
 
     def wait(self, ticket, timeout=-1.0):
-        """(pot, grad, info) of a request; info: p, precision, slot, queued_s, run_s, latency_s."""
+        """(pot, grad, info) of a request; info: p, precision, slot, queued_s, run_s, latency_s, plan_s
+        (host time of its plan and state), matvec_s (host time of its matvec) and device_s (the
+        matvec's time on the slot's stream)."""
         info = _RequestInfo()
         rc = lib().fmmb_server_wait(self._h, int(ticket), float(timeout), C.byref(info))
         if rc == 5 and info.latency_s == 0 and ticket in self._live:

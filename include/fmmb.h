@@ -257,13 +257,20 @@ int fmmb_direct_noalloc_dev(fmmb_ctx* ctx, const double* src_dev, const double* 
  * (stream) and an operator cache per order that stays resident, as soon as a slot is free and
  * the request's estimated device memory fits what the requests in flight leave of hbm_budget
  * (the front request waits rather than being overtaken; one that exceeds the budget alone runs
- * when nothing else does). The device work of admitted requests overlaps. Each request is
- * computed exactly as it would be alone (its results are bitwise the same in any mix). */
+ * when nothing else does). The device work of admitted requests overlaps. A slot takes the front
+ * request together with later queued requests of the same kind (kernel, order, precision path,
+ * κ, ppl, outputs), up to group_max requests and group_points points that fit the budget, and
+ * runs them as one batch plan (fmmb_batch_plan_create): one tree build, one list build and one
+ * launch per pass for the group. Each request is computed exactly as it would be alone (its
+ * results are bitwise the same in any mix and any group). */
 typedef struct fmmb_server fmmb_server;
 typedef struct {
-  int32_t slots;       /* concurrent requests (worker threads, one stream each), 1..64 */
+  int32_t slots;       /* concurrent groups (worker threads, one stream each), 1..64 */
   int32_t ppl;         /* points per leaf of every request's tree */
   int64_t hbm_budget;  /* bytes of device memory the admitted requests may hold; 0: 80 % of the free memory */
+  int32_t group_max;   /* requests per group; 0: 64; 1: every request alone */
+  int32_t reserved;
+  int64_t group_points; /* points per group (a larger request runs alone); 0: 4,000,000 */
 } fmmb_server_opts;
 typedef struct {
   const double* xyz;   /* 3×n host, original order; read while the request runs */
@@ -288,6 +295,12 @@ typedef struct {
   double run_s;        /* admission → results in host memory */
   double latency_s;    /* submission → results in host memory */
   int64_t bytes_estimate;
+  double plan_s;       /* host time of the plan (tree, lists, operators) and the state */
+  double matvec_s;     /* host time of the matvec (copies in, kernels, copies out) */
+  double device_s;     /* the matvec's span on the slot's stream (CUDA events around it) */
+  int32_t group;       /* requests in this request's group; the three times above are the group's
+                          divided by it (so that they sum to the group's over its requests) */
+  int32_t reserved;
 } fmmb_request_info;
 int fmmb_server_create(int device, const fmmb_server_opts* opts, fmmb_server** out);
 int fmmb_server_submit(fmmb_server* server, const fmmb_request* request, int64_t* ticket);

@@ -71,9 +71,34 @@ def test_yukawa_errors(fmmb):
     with pytest.raises(fmmb.ArgumentError):
         fmmb.OperatorCache(fmmb.SphericalHarmonics(fmmb.Yukawa3D(-1.0), p=6))
     pts = np.random.default_rng(1).random((3000, 3))
-    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Yukawa3D(2.0), p=6), pts, ppl=64)
-    with pytest.raises(fmmb.Unsupported):
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Yukawa3D(2.0), p=12), pts, ppl=64)
+    with pytest.raises(fmmb.Unsupported):                               # the tensor-core M2L takes p ≤ 11
         fmmb.FMMState(f, "mixed")
+
+
+@pytest.mark.parametrize("p,kappa,gen", [(11, 5.0, uniform3), (8, 10.0, clustered3), (6, 2.0, helix3)])
+def test_yukawa_mixed_path(fmmb, p, kappa, gen):
+    """The mixed path of Yukawa3D: the tensor-core M2L with each level width's class operators split
+    into FP16 head and tail (the rest of the matvec in FP64) against the FP64 path on the same
+    tree: potential within 1e-6 and gradient within 1e-5 relative L2 (the mixed path's stated
+    tolerance); the FP64 path's own error against direct sums bounds the mixed one's too."""
+    rng = np.random.default_rng(90 + p)
+    n = 40000
+    pts = gen(rng, n)
+    tau = rng.standard_normal(n)
+    f = fmmb.FMM(fmmb.SphericalHarmonics(fmmb.Yukawa3D(kappa), p=p), pts, ppl=64, bbox=((0.0, 0.0, 0.0), 1.0))
+    assert f.nlevels >= 4
+    ud, gd = fmmb.evaluate_at_sources_both(f, fmmb.build_expansions(f, pts, tau, precision="fp64"))
+    um, gm = fmmb.evaluate_at_sources_both(f, fmmb.build_expansions(f, pts, tau, precision="mixed"))
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert rel(um, ud) < 1e-6
+    assert rel(gm, gd) < 1e-5
+    sel = np.sort(rng.choice(n, 300, replace=False))
+    d = pts[sel, None, :] - pts[None, :, :]
+    r = np.sqrt(np.einsum("tsk,tsk->ts", d, d))
+    r[np.arange(len(sel)), sel] = np.inf                                 # the self terms
+    dp = (np.exp(-kappa * r) / r) @ tau / (4 * np.pi)
+    assert rel(um[sel], dp) < rel(ud[sel], dp) + 2e-6
 
 
 YK_PARITY = [("uniform", 20000, 40, 12, 5.0, 61), ("clustered", 8000, 30, 16, 4.0, 62), ("helix", 6000, 30, 8, 10.0, 63)]
