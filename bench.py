@@ -61,8 +61,8 @@ def args_():
     a.add_argument("--samples", type=int, default=4096)
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--no-p10", action="store_true", help="skip the side measurement at the configured order p = 10")
-    a.add_argument("--serve-requests", type=int, default=384, help="requests of the serving measurement (0: skip it)")
-    a.add_argument("--serve-slots", type=int, default=4)
+    a.add_argument("--serve-requests", type=int, default=4096, help="requests of the serving measurement (0: skip it)")
+    a.add_argument("--serve-slots", type=int, default=2)
     a.add_argument("--stokes-instances", type=int, default=64, help="instances of the batched Stokes measurement (0: skip it)")
     a.add_argument("--ki-points", type=int, default=2_000_000, help="points of the cube KI measurement (0: skip it)")
     a.add_argument("--no-circle-ki", action="store_true", help="skip the 2D circle KI measurement")
@@ -253,9 +253,10 @@ def serving_workload(count, seed=6):
 
 
 def serving(fmmb, device, count, slots):
-    """Throughput and latency of the request server: batched (all requests submitted at once),
-    then open-loop Poisson arrivals at 80 % of the batched request rate (p50/p99 latency), and
-    the same requests one at a time on the plain FP64 path."""
+    """Throughput and latency of the request server (same-kind requests grouped into batch plans,
+    `slots` groups in flight): batched (all requests submitted at once), then open-loop Poisson
+    arrivals at 80 % of the batched request rate (p50/p99 latency), and the same requests one at a
+    time on the plain FP64 path (one request per plan, one slot)."""
     reqs = serving_workload(count)
     total = sum(len(r[0]) for r in reqs)
     srv = fmmb.Server(device, slots=slots)
@@ -300,6 +301,7 @@ def serving(fmmb, device, count, slots):
     one.close()
     q = lambda v, f: float(np.quantile(np.asarray(v) * 1e3, f))
     return {"requests": count, "slots": slots, "points": total,
+            "group_mean": float(np.mean([i["group"] for i in infos])),
             "workload": "Laplace3D or Yukawa3D(kappa=5) 50/50, N log-uniform [1e3, 5e5], uniform or 4-Gaussian (sigma 0.02) "
                         "points, tol in {1e-3, 1e-6, 1e-9} (p and precision path chosen from tol) (seed 6)",
             "batched": {"evals_per_s": total / t_batch, "requests_per_s": count / t_batch, "seconds": t_batch},

@@ -125,6 +125,28 @@ function FMM(m::DeviceMethod, sources::AbstractVector{SVector{3,Float64}}; ppl::
     f = FMM(m, cache, r[], length(pts))
     finalizer(x -> ccall((:fmmb_plan_destroy, libfmmb), Cint, (Ptr{Cvoid},), x.h), f)
 end
+"""
+    BatchFMM(method, sets; ppl=50, cache=OperatorCache(method), max_levels=30)
+
+Several independent FMMs in one plan (no reference counterpart; fmmb_batch_plan_create): each
+point set of `sets` its own tree in its own box (each set's `square_bbox`, fitted by `fit_box!`
+in order), one tree build and one launch per pass for all of them; an `FMM` whose sources,
+densities and outputs are the sets' concatenated in order, each set's results bitwise those of
+its own `FMM` built with the same cache.
+"""
+function BatchFMM(m::DeviceMethod, sets::AbstractVector{<:AbstractVector{SVector{3,Float64}}}; ppl::Integer=50,
+                  cache::OperatorCache=OperatorCache(m), max_levels::Integer=30)
+    cache.method === m || throw(ArgumentError("the cache was built for a different method"))
+    pts = reduce(vcat, collect.(sets))
+    counts = Int64[length(x) for x in sets]
+    o = TreeOpts(ppl, max_levels, 0, 0, (0.0, 0.0, 0.0), 0.0)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:fmmb_batch_plan_create, libfmmb), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Int64}, Int64, Ref{TreeOpts}, Ptr{Float64}, Ref{Ptr{Cvoid}}),
+                cache.h, pts, counts, length(counts), Ref(o), C_NULL, r))
+    f = FMM(m, cache, r[], length(pts))
+    finalizer(x -> ccall((:fmmb_plan_destroy, libfmmb), Cint, (Ptr{Cvoid},), x.h), f)
+end
 # the circle method's 2D points and square: the plane z = 0 of the cube (the gradients it returns
 # are 3-vectors with a zero z component)
 function FMM(m::KernelIndependent, sources::AbstractVector{SVector{2,Float64}}; ppl::Integer=50, bbox=nothing,
@@ -213,7 +235,8 @@ function evaluate(f::FMM, st::FMMState, targets::AbstractVector{SVector{3,Float6
 end
 
 # ---------------------------------------------------------------- the request server (no reference counterpart)
-struct ServerOpts; slots::Int32; ppl::Int32; hbm_budget::Int64; end
+struct ServerOpts; slots::Int32; ppl::Int32; hbm_budget::Int64; group_max::Int32; reserved::Int32
+                   group_points::Int64; end
 struct Request
     xyz::Ptr{Float64}; tau::Ptr{Float64}; n::Int64; tol::Float64; kernel::Int32; p::Int32
     outputs::Int32; precision::Int32; ppl::Int32; pot::Ptr{Float64}; grad::Ptr{SVector{3,Float64}}
@@ -222,6 +245,7 @@ end
 struct RequestInfo
     status::Int32; p::Int32; precision::Int32; slot::Int32
     queued_s::Float64; run_s::Float64; latency_s::Float64; bytes_estimate::Int64
+    plan_s::Float64; matvec_s::Float64; device_s::Float64; group::Int32; reserved::Int32
 end
 
 """A continuous-batching FMM request server on one GPU: `submit` queues a Laplace3D FMM at the
@@ -230,10 +254,11 @@ sources (potential and gradient, self excluded) whose order and precision path f
 mutable struct Server
     h::Ptr{Cvoid}
     live::Dict{Int64,Any}
-    function Server(device::Integer=0; slots::Integer=4, ppl::Integer=64, hbm_budget::Integer=0)
+    function Server(device::Integer=0; slots::Integer=2, ppl::Integer=64, hbm_budget::Integer=0,
+                    group_max::Integer=0, group_points::Integer=0)
         r = Ref{Ptr{Cvoid}}(C_NULL)
         check(ccall((:fmmb_server_create, libfmmb), Cint, (Cint, Ref{ServerOpts}, Ref{Ptr{Cvoid}}),
-                    device, ServerOpts(slots, ppl, hbm_budget), r))
+                    device, ServerOpts(slots, ppl, hbm_budget, group_max, 0, group_points), r))
         s = new(r[], Dict{Int64,Any}())
         finalizer(x -> ccall((:fmmb_server_destroy, libfmmb), Cint, (Ptr{Cvoid},), x.h), s)
         return s

@@ -79,6 +79,35 @@ def test_struct_layouts_match_the_header(fmmb, tmp_path):
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
 
 
+def _julia_struct_offsets(src, name):
+    """Field names and C offsets of a Julia `struct` mirror of a header struct (Julia lays an
+    isbits struct out as C does), read from the shim's text."""
+    m = re.search(r"^struct " + name + r"\b(.*?)\bend\b", src, re.S | re.M)
+    assert m, name
+    sizes = {"Int32": 4, "Int64": 8, "Float64": 8, "NTuple{3,Float64}": 24}
+    fields, off = [], 0
+    for fname, ftype in re.findall(r"(\w+)::([\w{},]+)", m.group(1)):
+        size = 8 if ftype.startswith("Ptr") else sizes[ftype]
+        align = min(size, 8)
+        off = (off + align - 1) // align * align
+        fields.append((fname, off))
+        off += size
+    return fields
+
+
+def test_julia_struct_layouts_match_the_mirrors(fmmb):
+    """The Julia shim's structs have the fields and offsets of the ctypes mirrors (themselves
+    checked against the header above), so a struct the library fills or reads from Julia has the
+    header's layout."""
+    src = open(os.path.join(ROOT, "flexiblefmm.jl_b200", "julia", "FlexibleFMMB200.jl")).read()
+    pairs = {"MethodDesc": fmmb._MethodDesc, "TreeOpts": fmmb._TreeOpts, "ServerOpts": fmmb._ServerOpts,
+             "Request": fmmb._Request, "RequestInfo": fmmb._RequestInfo, "StokesDensitiesC": fmmb._StokesDensities}
+    for jname, py in pairs.items():
+        got = _julia_struct_offsets(src, jname)
+        want = [(f, getattr(py, f).offset) for f, _ in py._fields_]
+        assert got == want, jname
+
+
 def test_stokes_density_checks(fmmb):
     """stokes_densities (src/stokes_api.jl:72-83) rejects a stresslet without its stressvecs, no
     density at all, and arrays of the wrong length, before any device work."""
