@@ -62,7 +62,7 @@ def args_():
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--no-p10", action="store_true", help="skip the side measurement at the configured order p = 10")
     a.add_argument("--serve-requests", type=int, default=4096, help="requests of the serving measurement (0: skip it)")
-    a.add_argument("--serve-slots", type=int, default=2)
+    a.add_argument("--serve-slots", type=int, default=3)
     a.add_argument("--stokes-instances", type=int, default=64, help="instances of the batched Stokes measurement (0: skip it)")
     a.add_argument("--ki-points", type=int, default=2_000_000, help="points of the cube KI measurement (0: skip it)")
     a.add_argument("--no-circle-ki", action="store_true", help="skip the 2D circle KI measurement")
@@ -260,8 +260,10 @@ def serving(fmmb, device, count, slots):
     reqs = serving_workload(count)
     total = sum(len(r[0]) for r in reqs)
     srv = fmmb.Server(device, slots=slots)
-    for pts, tau, tol, kappa in reqs[:6]:                              # warm-up: operators resident
-        srv.wait(srv.submit(pts, tau, tol=tol, kappa=kappa))
+    # warm-up: the first eighth of the requests at once (operators of every order and width
+    # resident, the device pool grown)
+    for k in [srv.submit(pts, tau, tol=tol, kappa=kappa) for pts, tau, tol, kappa in reqs[:max(6, count // 8)]]:
+        srv.wait(k)
     t0 = time.perf_counter()
     tk = [srv.submit(pts, tau, tol=tol, kappa=kappa) for pts, tau, tol, kappa in reqs]
     infos = [srv.wait(k)[2] for k in tk]
@@ -368,6 +370,7 @@ def stokes_batch(fmmb, torch, ctx, count, p=16, ppl=200, samples=32, steps=3):
     bp = fmmb.BatchStokesFMMPlan(xs, ppl=ppl, bbox=box, cache=cache)
     t_plan = time.perf_counter() - t0
     F = bp.fmm.concat(fs)
+    tuned = fmmb.autotune(bp.state, bp.sources, F)                     # the launch shapes, on these inputs
     t0 = time.perf_counter()
     vel = fmmb.stokes_fmm_eval(bp, stokeslets=F)
     t_eval_host = time.perf_counter() - t0
@@ -421,7 +424,7 @@ def stokes_batch(fmmb, torch, ctx, count, p=16, ppl=200, samples=32, steps=3):
                            "equals_host_path": same_dev},
            "eval_host": {"evals_per_s": total / t_eval_host, "seconds": t_eval_host},
            "one_at_a_time": {"evals_per_s": total / t_seq, "seconds": t_seq},
-           "bitwise_equal_instances": bitwise,
+           "bitwise_equal_instances": bitwise, "tuned": tuned,
            "error": {"samples_per_instance": samples, "max": max(errs), "median": float(np.median(errs)),
                      "per_instance": [float(f"{e:.3g}") for e in errs]}}
     del bp, one
@@ -610,6 +613,11 @@ def run_ours(a):
         f = fmmb.FMM(m, pts, ppl=a.ppl, bbox=((0.0, 0.0, 0.0), 1.0))
         plan_s = time.perf_counter() - t0
         states = {"mixed": fmmb.FMMState(f, "mixed"), "fp64": fmmb.FMMState(f, "fp64")}
+        # the launch shapes tuned on these inputs (fmmb_autotune; no result depends on them): the
+        # FP64 path's chunk width and near-field warps, then the mixed path's, with the plan's M2L
+        # block size, which both paths share
+        tuned = {"fp64": fmmb.autotune(states["fp64"], pts, tau, tune_blocks=False),
+                 "mixed": fmmb.autotune(states["mixed"], pts, tau, tune_blocks=True)}
 
         def step(st):
             rc = L.fmmb_matvec_dev(st._h, P(xyz_d), P(tau_d), a.n, 3, P(pot_d), P(grad_d))
@@ -641,6 +649,7 @@ def run_ours(a):
         barrier()
         clk = clocks.stop() if clocks else None
         r = {"p": p, "f": f, "states": states, "step": step, "plan_s": plan_s, "t_mixed": t_mixed, "clocks": clk,
+             "tuned": tuned,
              "ms_mixed": max_over_ranks(statistics.mean(t_mixed), dist, "cuda"),
              "ms_fp64": max_over_ranks(statistics.mean(t_fp64), dist, "cuda")}
         err = {}
@@ -743,7 +752,7 @@ def run_ours(a):
     kic = None if a.no_circle_ki else circle_ki(fmmb)
     # every figure, on a line of its own before the headline
     detail = {"configured_order_p10": side, "serving": serve, "stokes_batched": stokes, "cube_ki": ki, "circle_ki": kic,
-              "parity": par, "stages_ms": stages, "error": {"samples": len(sel), **err}}
+              "parity": par, "stages_ms": stages, "error": {"samples": len(sel), **err}, "tuned": R["tuned"]}
     print(json.dumps({"bench_detail": detail}), flush=True)
     line = {
         "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -765,6 +774,8 @@ def run_ours(a):
         "mixed_vs_fp64": _sig(ms_fp64 / ms_mixed),
         "error": {"samples": len(sel), **_sig(err)},
         "stages_ms": {"plan_s": _sig(plan_s), **_sig(stages)},
+        "tuned": {k: {"tb": v["block_targets"], "nb_alt": v["f64_chunk_variant"], "near_w": v["near_warps"]}
+                  for k, v in R["tuned"].items()},
         "parity": compact_parity(par),
         "side": compact_side(side, serve, stokes, ki, kic),
     }

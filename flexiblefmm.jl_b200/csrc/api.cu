@@ -585,6 +585,7 @@ int fmmb_plan_info(const fmmb_plan* plan, int64_t* info, int cap) {
     info[2] = P.N;
     info[3] = P.npairs;
     for (int l = 0; l <= P.L; ++l) info[4 + l] = P.level_start[l];
+    if (cap >= 6 + P.L) info[5 + P.L] = P.TB;     // the M2L blocks' targets, where there is room
   });
 }
 
@@ -682,11 +683,42 @@ int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out) {
       prepare_mixed_operators(*P.cache);
       prepare_mixed_levels(P);
     }
+    apply_tuned_state(S);                         // the launch shapes tuned for states of this kind
     FMMB_CUDA(cudaStreamSynchronize(s));
     h->parent = plan;
     std::lock_guard<std::mutex> lk(g_handles);
     ++plan->deps;
     *out = h.release();
+  });
+}
+
+int fmmb_autotune_dev(fmmb_state* state, const double* xyz_dev, const double* tau_dev, int64_t n, int tune_blocks,
+                      double* out) {
+  return guard([&] {
+    require(state && xyz_dev && tau_dev, FMMB_ERR_ARGUMENT, "null argument");
+    State& S = state->s;
+    set_device(*S.plan->ctx);
+    require(n == S.plan->N, FMMB_ERR_DIMENSION, "the points must be the plan's");
+    require_device_ptr(*S.plan->ctx, xyz_dev, "points");
+    require_device_ptr(*S.plan->ctx, tau_dev, "densities");
+    autotune(S, xyz_dev, tau_dev, tune_blocks != 0, out);
+    check_state_errors(S);
+  });
+}
+
+int fmmb_autotune(fmmb_state* state, const double* xyz, const double* tau, int64_t n, int tune_blocks, double* out) {
+  return guard([&] {
+    require(state && xyz && tau, FMMB_ERR_ARGUMENT, "null argument");
+    State& S = state->s;
+    Ctx& ctx = *S.plan->ctx;
+    set_device(ctx);
+    require(n == S.plan->N, FMMB_ERR_DIMENSION, "the points must be the plan's");
+    const int dens = S.plan->cache->kernel == FMMB_KERNEL_STOKESLET3D ? 3 : 1;
+    DBuf<double> dx(3 * n), dt(dens * n);
+    FMMB_CUDA(cudaMemcpyAsync(dx.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx.stream));
+    FMMB_CUDA(cudaMemcpyAsync(dt.p, tau, sizeof(double) * dens * n, cudaMemcpyHostToDevice, ctx.stream));
+    autotune(S, dx.p, dt.p, tune_blocks != 0, out);
+    check_state_errors(S);
   });
 }
 

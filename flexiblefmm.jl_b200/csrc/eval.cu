@@ -235,8 +235,9 @@ __device__ __forceinline__ void near_batch_f32x2(const float4* __restrict__ pr, 
   }
 }
 
-template <typename R, bool SELF, int YK>
-__global__ void __launch_bounds__(NEAR_WARPS * 32, 5) k_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
+// W warps (leaf groups) per CTA: 4 or 8, chosen per state by the tuner (tune.cu)
+template <typename R, bool SELF, int YK, int W>
+__global__ void __launch_bounds__(W * 32, W == 4 ? 5 : 2) k_near(const int* __restrict__ gnode, const int* __restrict__ gstart,
                                                          const int* __restrict__ gcount, int ngroups,
                                                          const double* __restrict__ tx, const double* __restrict__ ty,
                                                          const double* __restrict__ tz, const int* __restrict__ tout,
@@ -247,9 +248,9 @@ __global__ void __launch_bounds__(NEAR_WARPS * 32, 5) k_near(const int* __restri
                                                          Geometry geo, int outputs, double* __restrict__ pot,
                                                          double* __restrict__ grad, double kappa, int first) {
   constexpr bool REL = sizeof(R) == 4;   // the mixed path works relative to the leaf's centre
-  __shared__ NearWarp<R> sws[NEAR_WARPS];
+  __shared__ NearWarp<R> sws[W];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int grp = blockIdx.x * NEAR_WARPS + warp;
+  const int grp = blockIdx.x * W + warp;
   if (grp >= ngroups) return;                      // the whole warp
   NearWarp<R>& sw = sws[warp];
   const int leaf = gnode[grp];
@@ -584,9 +585,15 @@ void launch_near(State& S, const int* gnode, const int* gstart, const int* gcoun
                  const double* tz, const int* tout, int outputs, double* pot, double* grad, int first = 0,
                  cudaStream_t st = nullptr) {
   Plan& P_ = *S.plan;
-  k_near<R, SELF, YK><<<(ng + NEAR_WARPS - 1) / NEAR_WARPS, 32 * NEAR_WARPS, 0, st ? st : P_.ctx->stream>>>(
-      gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p, S.zs.p, S.q.p, P_.cell.p, P_.plo.p, P_.phi.p, P_.col.p,
-      geometry(P_), outputs, pot, grad, P_.cache->kappa, first);
+  const cudaStream_t s = st ? st : P_.ctx->stream;
+  if (S.near_warps == 8)
+    k_near<R, SELF, YK, 8><<<(ng + 7) / 8, 32 * 8, 0, s>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p, S.zs.p,
+                                                          S.q.p, P_.cell.p, P_.plo.p, P_.phi.p, P_.col.p, geometry(P_),
+                                                          outputs, pot, grad, P_.cache->kappa, first);
+  else
+    k_near<R, SELF, YK, 4><<<(ng + 3) / 4, 32 * 4, 0, s>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, S.xs.p, S.ys.p, S.zs.p,
+                                                          S.q.p, P_.cell.p, P_.plo.p, P_.phi.p, P_.col.p, geometry(P_),
+                                                          outputs, pot, grad, P_.cache->kappa, first);
   FMMB_LAUNCH_CHECK();
 }
 

@@ -125,6 +125,60 @@ __global__ void k_block_fill(const int4* __restrict__ blocks, const int4* __rest
 
 }  // namespace
 
+// the M2L blocks of TB targets each, from the pairs per target (P.h_pair_count): per block its
+// class offsets, pairs and round table, launched heaviest first
+void build_blocks(Plan& P, int TB) {
+  cudaStream_t s = P.ctx->stream;
+  const int L = P.L;
+  require(TB >= 1 && TB <= 128, FMMB_ERR_ARGUMENT, "targets per M2L block must be in 1..128");
+  P.TB = TB;
+  P.h_blocks.clear();
+  P.level_pairs.assign(L, 0);
+  int64_t base = 0;
+  require(L < 256, FMMB_ERR_ARGUMENT, "too many levels");
+  for (int q = 0; q < P.nseg; ++q) {
+    const int l = P.seg_level[q], end = P.seg_start[q + 1];
+    if (l < 2) continue;
+    for (int b0 = P.seg_start[q]; b0 < end; b0 += P.TB) {
+      int c = std::min(P.TB, end - b0);
+      int64_t np = 0;
+      for (int g = b0; g < b0 + c; ++g) np += P.h_pair_count[g];
+      if (np == 0) continue;
+      P.h_blocks.push_back({l, q, b0, c, (int)base});
+      base += np;
+      P.level_pairs[l] += np;
+    }
+  }
+  require(base < (1ll << 31), FMMB_ERR_ARGUMENT, "too many far pairs for 32-bit offsets");
+  P.npairs = base;
+  int nb = (int)P.h_blocks.size();
+  // the M2L kernels take the blocks in launch order heaviest first (most far pairs): the CTA
+  // scheduler hands out blocks in index order, so the light ones fill the last wave (longest
+  // processing time first); every block owns its targets, so the order changes no sum
+  std::vector<int64_t> bp(nb);
+  for (int b = 0; b < nb; ++b) bp[b] = (b + 1 < nb ? P.h_blocks[b + 1].pair_base : base) - P.h_blocks[b].pair_base;
+  std::vector<int> order(nb);
+  for (int b = 0; b < nb; ++b) order[b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return bp[a] > bp[b]; });
+  std::vector<int4> hb(nb);
+  for (int i = 0; i < nb; ++i) {
+    const M2LBlock& B = P.h_blocks[order[i]];
+    hb[i] = make_int4(B.level | B.seg << 8, B.first, B.count, B.pair_base);
+  }
+  to_device(P.blocks, hb, s);
+  P.cls_off.alloc((size_t)std::max(nb, 1) * (NCLASS + 1));
+  P.pairs.alloc(std::max<int64_t>(base, 1));
+  P.rtab.alloc((size_t)std::max(nb, 1) * NCLASS * P.TB);
+  P.rounds.alloc((size_t)std::max(nb, 1) * NCLASS);
+  if (nb) {
+    size_t smem = sizeof(int) * (NCLASS * P.TB + NCLASS + 1);
+    k_block_fill<<<nb, std::max(P.TB, 64), smem, s>>>(P.blocks.p, P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p,
+                                                    P.cls_off.p, P.pairs.p, P.TB, P.rtab.p, P.rounds.p);
+    FMMB_LAUNCH_CHECK();
+  }
+  FMMB_CUDA(cudaStreamSynchronize(s));
+}
+
 void build_lists(Plan& P) {
   cudaStream_t s = P.ctx->stream;
   const int n = P.nnodes, L = P.L;
@@ -203,59 +257,18 @@ void build_lists(Plan& P) {
     k_pair_count<<<(nl + 127) / 128, 128, 0, s>>>(P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p, first, nl, cnt.p);
     FMMB_LAUNCH_CHECK();
   }
-  std::vector<int> hc = to_host(cnt.p, n, s);
-  // targets per block: 128, halved (down to 16) while the targets with far pairs fill fewer
-  // blocks than the device has SMs, so that small trees still spread over the whole GPU
-  {
+  P.h_pair_count = to_host(cnt.p, n, s);
+  // targets per block: a tuned size for plans of this kind (tune.cu), else 128, halved (down to
+  // 16) while the targets with far pairs fill fewer blocks than the device has SMs, so that small
+  // trees still spread over the whole GPU
+  int TB = tuned_block_size(P);
+  if (TB <= 0) {
     int64_t nt = 0;
-    for (int g = P.level_start[std::min(2, L)]; g < P.level_start[L]; ++g) nt += hc[g] > 0;
-    P.TB = 128;
-    while (P.TB > 16 && nt / P.TB < P.ctx->num_sms) P.TB /= 2;
+    for (int g = P.level_start[std::min(2, L)]; g < P.level_start[L]; ++g) nt += P.h_pair_count[g] > 0;
+    TB = 128;
+    while (TB > 16 && nt / TB < P.ctx->num_sms) TB /= 2;
   }
-  P.h_blocks.clear();
-  P.level_pairs.assign(L, 0);
-  int64_t base = 0;
-  require(L < 256, FMMB_ERR_ARGUMENT, "too many levels");
-  for (int q = 0; q < P.nseg; ++q) {
-    const int l = P.seg_level[q], end = P.seg_start[q + 1];
-    if (l < 2) continue;
-    for (int b0 = P.seg_start[q]; b0 < end; b0 += P.TB) {
-      int c = std::min(P.TB, end - b0);
-      int64_t np = 0;
-      for (int g = b0; g < b0 + c; ++g) np += hc[g];
-      if (np == 0) continue;
-      P.h_blocks.push_back({l, q, b0, c, (int)base});
-      base += np;
-      P.level_pairs[l] += np;
-    }
-  }
-  require(base < (1ll << 31), FMMB_ERR_ARGUMENT, "too many far pairs for 32-bit offsets");
-  P.npairs = base;
-  int nb = (int)P.h_blocks.size();
-  // the M2L kernels take the blocks in launch order heaviest first (most far pairs): the CTA
-  // scheduler hands out blocks in index order, so the light ones fill the last wave (longest
-  // processing time first); every block owns its targets, so the order changes no sum
-  std::vector<int64_t> bp(nb);
-  for (int b = 0; b < nb; ++b) bp[b] = (b + 1 < nb ? P.h_blocks[b + 1].pair_base : base) - P.h_blocks[b].pair_base;
-  std::vector<int> order(nb);
-  for (int b = 0; b < nb; ++b) order[b] = b;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return bp[a] > bp[b]; });
-  std::vector<int4> hb(nb);
-  for (int i = 0; i < nb; ++i) {
-    const M2LBlock& B = P.h_blocks[order[i]];
-    hb[i] = make_int4(B.level | B.seg << 8, B.first, B.count, B.pair_base);
-  }
-  to_device(P.blocks, hb, s);
-  P.cls_off.alloc((size_t)std::max(nb, 1) * (NCLASS + 1));
-  P.pairs.alloc(std::max<int64_t>(base, 1));
-  P.rtab.alloc((size_t)std::max(nb, 1) * NCLASS * P.TB);
-  P.rounds.alloc((size_t)std::max(nb, 1) * NCLASS);
-  if (nb) {
-    size_t smem = sizeof(int) * (NCLASS * P.TB + NCLASS + 1);
-    k_block_fill<<<nb, std::max(P.TB, 64), smem, s>>>(P.blocks.p, P.cell.p, P.parent.p, P.cf.p, P.col.p, P.flags.p,
-                                                    P.cls_off.p, P.pairs.p, P.TB, P.rtab.p, P.rounds.p);
-    FMMB_LAUNCH_CHECK();
-  }
+  build_blocks(P, TB);
   // per level factors
   std::vector<double> sc(L), ms(L);
   for (int l = 0; l < L; ++l) { sc[l] = P.scale[l]; ms[l] = P.m2l_scale[l]; }

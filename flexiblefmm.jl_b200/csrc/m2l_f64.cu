@@ -300,15 +300,18 @@ void launch(State& S) {
 
 }  // namespace
 
+// two chunk widths per expansion length: the default, and the alternative the tuner may choose
+// (S.f64_nb_alt); the sums do not depend on it
 void m2l_f64(State& S) {
+  const bool alt = S.f64_nb_alt != 0;
   switch (S.plan->cache->ld) {
-    case 64: launch<64, 64>(S); break;
-    case 128: launch<128, 64>(S); break;
-    case 192: launch<192, 32>(S); break;
-    case 256: launch<256, 32>(S); break;
-    case 320: launch<320, 48>(S); break;
-    case 384: launch<384, 40>(S); break;
-    case 448: launch<448, 32>(S); break;
+    case 64: alt ? launch<64, 32>(S) : launch<64, 64>(S); break;
+    case 128: alt ? launch<128, 32>(S) : launch<128, 64>(S); break;
+    case 192: alt ? launch<192, 64>(S) : launch<192, 32>(S); break;
+    case 256: alt ? launch<256, 16>(S) : launch<256, 32>(S); break;
+    case 320: alt ? launch<320, 32>(S) : launch<320, 48>(S); break;
+    case 384: alt ? launch<384, 24>(S) : launch<384, 40>(S); break;
+    case 448: alt ? launch<448, 16>(S) : launch<448, 32>(S); break;
     default: throw Error(FMMB_ERR_UNSUPPORTED, "no M2L kernel for this expansion length");
   }
 }

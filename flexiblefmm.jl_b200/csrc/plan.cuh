@@ -119,6 +119,7 @@ struct Plan {
   DBuf<int> rounds;                       // nblocks × 34: per class the largest count of a target
   int64_t npairs = 0;
   std::vector<int64_t> level_pairs;       // far pairs per level
+  std::vector<int> h_pair_count;          // far pairs per target node (the blocks are cut from it)
   DBuf<double> d_scale, d_m2l_scale;      // per level
   // the translation operators of each level (the cache's for the homogeneous kernels; the
   // level's own width for Yukawa3D): M2L representatives, M2M into and L2L out of the level's
@@ -164,6 +165,10 @@ struct Plan {
 struct State {
   Plan* plan = nullptr;
   int precision = FMMB_PRECISION_FP64;
+  // launch shapes chosen by the tuner (tune.cu): near-field warps per CTA (4 or 8), the FP64
+  // M2L's alternative chunk width
+  int near_warps = 4;
+  int f64_nb_alt = 0;
   DBuf<double> xs, ys, zs, q;             // sources and charges in tree order
   DBuf<double> f3;                        // Stokeslet states: the forces in tree order (fx, fy, fz)
   DBuf<double> sd;                        //   stresslet strengths, stressvecs, doublets (3 × N planar each)
@@ -207,6 +212,15 @@ struct State {
 void build_tree(Plan& P, const double* xyz_dev, int ppl, int max_levels);
 // lists.cu
 void build_lists(Plan& P);
+void build_blocks(Plan& P, int TB);       // the M2L blocks of TB targets (re)cut from P.h_pair_count
+// tune.cu: the tuned launch shapes of plans and states of a kind (method, kernel, p, precision,
+// N rounded down to a power of two); 0 / unchanged where none was tuned
+int tuned_block_size(const Plan& P);
+void apply_tuned_state(State& S);
+// times the launch shapes on the state's inputs, keeps the fastest for its kind and applies them
+// (tune_blocks: also the plan's M2L block size, shared by the plan's other states); out: the
+// chosen block size, FP64 chunk width variant, near-field warps, and the M2L and near-field ms
+void autotune(State& S, const double* xyz_dev, const double* tau_dev, bool tune_blocks, double* out);
 void build_target_pairs(Plan& P);
 // passes.cu
 void upload_operators(Cache& C);

@@ -44,7 +44,7 @@ using clk = std::chrono::steady_clock;
 struct Job {
   fmmb_request r;
   int64_t id = 0;
-  int p = 0, precision = 0, slot = -1;
+  int p = 0, precision = 0, slot = -1, ppl = 64;
   int64_t bytes = 0;
   clk::time_point t_submit, t_start, t_done;
   double plan_s = 0, matvec_s = 0, device_s = 0;
@@ -84,6 +84,18 @@ int64_t bytes_estimate(int64_t n, int p, int ppl, int precision, int kernel) {
   return b + (16 << 20);
 }
 
+// the leaf size of a request that names none, by order and precision path (measured on the
+// device, 2·10⁵ uniform and 4-cluster points, Laplace3D: the matvec time is flat or falling in ppl
+// up to these and the error unchanged; at p = 20 on the FP64 path ppl = 512 takes 12.5 / 20.6 ms
+// against 19.9 / 69.2 ms at 64, uniform / clustered). The mixed path's tensor-core M2L is cheap
+// enough that 64 stays best.
+int auto_ppl(int p, int precision) {
+  if (precision == FMMB_PRECISION_MIXED || p <= 8) return 64;
+  if (p <= 13) return 128;
+  if (p <= 17) return 256;
+  return 512;
+}
+
 double seconds(clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); }
 
 }  // namespace
@@ -112,7 +124,7 @@ namespace {
 // the kind of a request: requests of one kind can share a batch plan
 std::tuple<int, int, int, double, int, int> kind(const fmmb_server& S, const Job& j) {
   return std::make_tuple(j.r.kernel, j.p, j.precision, j.r.kernel == FMMB_KERNEL_YUKAWA3D ? j.r.kappa : 0.0,
-                         j.r.ppl > 0 ? j.r.ppl : S.ppl, j.r.kernel == FMMB_KERNEL_STOKESLET3D ? 0 : j.r.outputs);
+                         j.ppl, j.r.kernel == FMMB_KERNEL_STOKESLET3D ? 0 : j.r.outputs);
 }
 
 // a group of requests of one kind on a slot: one plan (a batch plan for more than one), one
@@ -141,7 +153,7 @@ int run_group(fmmb_server& S, int slot, std::vector<Job*>& g, std::string& err) 
     }
   }
   fmmb_tree_opts o{};
-  o.ppl = j0.r.ppl > 0 ? j0.r.ppl : S.ppl;
+  o.ppl = j0.ppl;
   o.max_levels = 30;
   // the group's inputs and outputs, concatenated in group order (one request: its own buffers)
   const size_t ng = g.size();
@@ -149,59 +161,90 @@ int run_group(fmmb_server& S, int slot, std::vector<Job*>& g, std::string& err) 
   std::vector<int64_t> counts(ng);
   int64_t n = 0;
   for (size_t i = 0; i < ng; ++i) { counts[i] = g[i]->r.n; n += g[i]->r.n; }
-  std::vector<double> xyz, tau, pot, grad;
-  const double *px = j0.r.xyz, *pt = j0.r.tau;
-  double *pp = j0.r.pot, *pg = j0.r.grad;
   const int outputs = stokes ? 0 : j0.r.outputs;
   const int pot_w = stokes ? 3 : 1;
+  cudaStream_t stream = nullptr;
+  fmmb_ctx_stream(S.ctx[slot], (void**)&stream);
+  // a group: its inputs copied request by request into device buffers on the slot's stream (no
+  // host-side concatenation), its outputs copied back into each request's buffers
+  double *dx = nullptr, *dt = nullptr, *dp = nullptr, *dg = nullptr;
+  int rc = FMMB_OK;
+  auto dev_alloc = [&](double** q, int64_t count) {
+    if (!rc && cudaMallocAsync((void**)q, sizeof(double) * count, stream) != cudaSuccess) {
+      rc = FMMB_ERR_DEVICE;
+      err = "device memory for a request group";
+    }
+  };
+  const bool want_pot = stokes || (outputs & FMMB_OUTPUT_POTENTIAL), want_grad = !stokes && (outputs & FMMB_OUTPUT_GRADIENT);
   if (ng > 1) {
-    xyz.resize(3 * n); tau.resize(dens * n);
+    dev_alloc(&dx, 3 * n);
+    dev_alloc(&dt, dens * n);
+    if (want_pot) dev_alloc(&dp, pot_w * n);
+    if (want_grad) dev_alloc(&dg, 3 * n);
     int64_t off = 0;
     for (Job* j : g) {
-      std::copy(j->r.xyz, j->r.xyz + 3 * j->r.n, xyz.begin() + 3 * off);
-      std::copy(j->r.tau, j->r.tau + dens * j->r.n, tau.begin() + dens * off);
+      if (!rc && (cudaMemcpyAsync(dx + 3 * off, j->r.xyz, sizeof(double) * 3 * j->r.n, cudaMemcpyHostToDevice, stream) ||
+                  cudaMemcpyAsync(dt + dens * off, j->r.tau, sizeof(double) * dens * j->r.n, cudaMemcpyHostToDevice,
+                                  stream))) {
+        rc = FMMB_ERR_DEVICE;
+        err = "copying a request's inputs";
+      }
       off += j->r.n;
     }
-    px = xyz.data(); pt = tau.data();
-    if (stokes || (outputs & FMMB_OUTPUT_POTENTIAL)) { pot.resize(pot_w * n); pp = pot.data(); }
-    if (!stokes && (outputs & FMMB_OUTPUT_GRADIENT)) { grad.resize(3 * n); pg = grad.data(); }
   }
   fmmb_plan* plan = nullptr;
   fmmb_state* st = nullptr;
   const clk::time_point t0 = clk::now();
-  int rc = ng > 1 ? fmmb_batch_plan_create(cache, px, counts.data(), (int64_t)ng, &o, nullptr, &plan)
-                  : fmmb_plan_create(cache, px, n, &o, &plan);
+  if (!rc)
+    rc = ng > 1 ? fmmb_batch_plan_create_dev(cache, dx, counts.data(), (int64_t)ng, &o, nullptr, &plan)
+                : fmmb_plan_create(cache, j0.r.xyz, n, &o, &plan);
   if (!rc) rc = fmmb_state_create(plan, j0.precision, &st);
   const clk::time_point t1 = clk::now();
   double plan_s = seconds(t0, t1), matvec_s = 0, device_s = 0;
   if (!rc) {
     // the matvec's span on the slot's stream, beside its host time
-    cudaStream_t stream = nullptr;
-    fmmb_ctx_stream(S.ctx[slot], (void**)&stream);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     const bool ev = cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess &&
                     cudaEventRecord(e0, stream) == cudaSuccess;
-    if (stokes) rc = fmmb_stokes_eval(st, px, pt, n, pp);
-    else rc = fmmb_matvec(st, px, pt, n, outputs, pp, pg);
-    matvec_s = seconds(t1, clk::now());
+    if (ng == 1) {
+      if (stokes) rc = fmmb_stokes_eval(st, j0.r.xyz, j0.r.tau, n, j0.r.pot);
+      else rc = fmmb_matvec(st, j0.r.xyz, j0.r.tau, n, outputs, j0.r.pot, j0.r.grad);
+    } else {
+      if (stokes) rc = fmmb_stokes_eval_dev(st, dx, dt, n, dp);
+      else rc = fmmb_matvec_dev(st, dx, dt, n, outputs, dp, dg);
+      if (!rc) rc = fmmb_state_synchronize(st);
+    }
     float ms = 0;
     if (ev && cudaEventRecord(e1, stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
         cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
       device_s = ms * 1e-3;
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
+    if (!rc && ng > 1) {
+      int64_t off = 0;
+      for (Job* j : g) {
+        if ((want_pot && cudaMemcpyAsync(j->r.pot, dp + pot_w * off, sizeof(double) * pot_w * j->r.n, cudaMemcpyDeviceToHost,
+                                         stream)) ||
+            (want_grad && cudaMemcpyAsync(j->r.grad, dg + 3 * off, sizeof(double) * 3 * j->r.n, cudaMemcpyDeviceToHost,
+                                          stream))) {
+          rc = FMMB_ERR_DEVICE;
+          err = "copying a request's outputs";
+          break;
+        }
+        off += j->r.n;
+      }
+      if (cudaStreamSynchronize(stream) != cudaSuccess && !rc) {
+        rc = FMMB_ERR_DEVICE;
+        err = "copying a request's outputs";
+      }
+    }
+    matvec_s = seconds(t1, clk::now());
   }
-  if (rc) err = fmmb_last_error();
+  if (rc && err.empty()) err = fmmb_last_error();
   if (st) fmmb_state_destroy(st);
   if (plan) fmmb_plan_destroy(plan);
-  if (!rc && ng > 1) {
-    int64_t off = 0;
-    for (Job* j : g) {
-      if (!pot.empty()) std::copy(pot.begin() + pot_w * off, pot.begin() + pot_w * (off + j->r.n), j->r.pot);
-      if (!grad.empty()) std::copy(grad.begin() + 3 * off, grad.begin() + 3 * (off + j->r.n), j->r.grad);
-      off += j->r.n;
-    }
-  }
+  for (double* q : {dx, dt, dp, dg})
+    if (q) cudaFreeAsync(q, stream);
   for (Job* j : g) {
     j->plan_s = plan_s / ng;
     j->matvec_s = matvec_s / ng;
@@ -269,7 +312,7 @@ extern "C" {
 
 int fmmb_server_create(int device, const fmmb_server_opts* opts, fmmb_server** out) {
   if (!opts || !out) return FMMB_ERR_ARGUMENT;
-  if (opts->slots < 1 || opts->slots > 64 || opts->ppl < 1 || opts->hbm_budget < 0) return FMMB_ERR_ARGUMENT;
+  if (opts->slots < 1 || opts->slots > 64 || opts->ppl < 0 || opts->hbm_budget < 0) return FMMB_ERR_ARGUMENT;
   std::unique_ptr<fmmb_server> S(new fmmb_server());
   S->device = device;
   S->nslots = opts->slots;
@@ -323,7 +366,8 @@ int fmmb_server_submit(fmmb_server* S, const fmmb_request* r, int64_t* ticket) {
   else
     j->precision = r->precision >= 0 ? r->precision
                                      : ((r->tol < 1e-8 || (j->p + 1) * (j->p + 1) > 144) ? FMMB_PRECISION_FP64 : FMMB_PRECISION_MIXED);
-  j->bytes = bytes_estimate(r->n, j->p, r->ppl > 0 ? r->ppl : S->ppl, j->precision, r->kernel);
+  j->ppl = r->ppl > 0 ? r->ppl : (S->ppl > 0 ? S->ppl : auto_ppl(j->p, j->precision));
+  j->bytes = bytes_estimate(r->n, j->p, j->ppl, j->precision, r->kernel);
   j->t_submit = clk::now();
   std::lock_guard<std::mutex> lk(S->mu);
   if (S->stop) return FMMB_ERR_ARGUMENT;

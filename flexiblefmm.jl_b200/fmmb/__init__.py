@@ -101,7 +101,8 @@ EXPORTS = (
     "fmmb_stokes_eval_dev", "fmmb_build_expansions_dipoles", "fmmb_build_expansions_dipoles_dev",
     "fmmb_stokes_eval_densities", "fmmb_stokes_eval_densities_dev", "fmmb_stokes_eval_src_trg",
     "fmmb_stokes_eval_src_trg_dev", "fmmb_state_synchronize", "fmmb_test_m2l_stall",
-    "fmmb_batch_plan_create", "fmmb_batch_plan_create_dev", "fmmb_batch_plan_instances",
+    "fmmb_batch_plan_create", "fmmb_batch_plan_create_dev", "fmmb_batch_plan_instances", "fmmb_autotune",
+    "fmmb_autotune_dev",
 )
 
 
@@ -134,6 +135,8 @@ def lib():
         "fmmb_batch_plan_create": [vp, dp, dp, i64, C.POINTER(_TreeOpts), dp, C.POINTER(vp)],
         "fmmb_batch_plan_create_dev": [vp, dp, dp, i64, C.POINTER(_TreeOpts), dp, C.POINTER(vp)],
         "fmmb_batch_plan_instances": [vp, C.POINTER(i64), dp, dp, dp, dp],
+        "fmmb_autotune": [vp, dp, dp, i64, i32, dp],
+        "fmmb_autotune_dev": [vp, dp, dp, i64, i32, dp],
         "fmmb_plan_info": [vp, dp, i32],
         "fmmb_plan_box": [vp, dp, dp],
         "fmmb_plan_tree": [vp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp],
@@ -433,6 +436,7 @@ class FMM:
         _check(lib().fmmb_plan_info(self._h, _ptr(info), len(info)))
         self.nlevels, self.nnodes, self.npairs = int(info[0]), int(info[1]), int(info[3])
         self.level_start = info[4:4 + self.nlevels + 1].copy()
+        self.block_targets = int(info[5 + self.nlevels])
         o = np.zeros(3)
         w = C.c_double()
         _check(lib().fmmb_plan_box(self._h, _ptr(o), C.byref(w)))
@@ -505,6 +509,7 @@ class BatchFMM(FMM):
         _check(lib().fmmb_plan_info(self._h, _ptr(info), len(info)))
         self.nlevels, self.nnodes, self.npairs = int(info[0]), int(info[1]), int(info[3])
         self.level_start = info[4:4 + self.nlevels + 1].copy()
+        self.block_targets = int(info[5 + self.nlevels])
         n = C.c_int64()
         self.boxes = np.zeros((self.ninst, 4))
         self.root_level = np.zeros(self.ninst, np.int32)
@@ -582,6 +587,19 @@ class Dipoles:
 
     def __init__(self, d):
         self.d = np.ascontiguousarray(d, dtype=np.float64)
+
+
+def autotune(state, sources, densities, tune_blocks=True):
+    """The autotuner (fmmb_autotune): times the launch shapes of the state's matvec on these
+    inputs (the plan's sources; charges, or (N, 3) Stokeslets), applies the fastest and records
+    them for later plans and states of the same kind; returns the choices. The state's
+    expansions must be built again afterwards."""
+    x = _pts(state.fmm, sources)
+    t = np.ascontiguousarray(densities, dtype=np.float64)
+    out = np.zeros(5)
+    _check(lib().fmmb_autotune(state._h, _ptr(x), _ptr(t), x.shape[0], 1 if tune_blocks else 0, _ptr(out)))
+    return {"block_targets": int(out[0]), "f64_chunk_variant": int(out[1]), "near_warps": int(out[2]),
+            "m2l_ms": float(out[3]), "near_ms": float(out[4])}
 
 
 def build_expansions_(state, fmm, sources, tau):
@@ -669,10 +687,11 @@ class Server:
     sizes and tolerances are admitted in arrival order onto `slots` concurrent streams as slots
     and device memory (hbm_budget bytes; 0 = 80 % of the free memory) free up; a slot runs the
     front request with later queued ones of the same kind as one batch plan (up to group_max
-    requests and group_points points; 0: 64 and 4e6; group_max=1: one at a time). No counterpart
-    in the reference, which runs one FMM per call."""
+    requests and group_points points; 0: 64 and 4e6; group_max=1: one at a time); ppl 0: the leaf
+    size by each request's order and path. No counterpart in the reference, which runs one FMM
+    per call."""
 
-    def __init__(self, device=0, slots=4, ppl=64, hbm_budget=0, group_max=0, group_points=0):
+    def __init__(self, device=0, slots=2, ppl=0, hbm_budget=0, group_max=0, group_points=0):
         h = C.c_void_p()
         o = _ServerOpts(int(slots), int(ppl), int(hbm_budget), int(group_max), 0, int(group_points))
         _check(lib().fmmb_server_create(int(device), C.byref(o), C.byref(h)))

@@ -254,7 +254,7 @@ sources (potential and gradient, self excluded) whose order and precision path f
 mutable struct Server
     h::Ptr{Cvoid}
     live::Dict{Int64,Any}
-    function Server(device::Integer=0; slots::Integer=2, ppl::Integer=64, hbm_budget::Integer=0,
+    function Server(device::Integer=0; slots::Integer=2, ppl::Integer=0, hbm_budget::Integer=0,
                     group_max::Integer=0, group_points::Integer=0)
         r = Ref{Ptr{Cvoid}}(C_NULL)
         check(ccall((:fmmb_server_create, libfmmb), Cint, (Cint, Ref{ServerOpts}, Ref{Ptr{Cvoid}}),

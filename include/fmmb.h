@@ -105,7 +105,8 @@ int fmmb_plan_create(fmmb_cache* cache, const double* xyz, int64_t n, const fmmb
 int fmmb_plan_create_dev(fmmb_cache* cache, const double* xyz_dev, int64_t n, const fmmb_tree_opts* opts, fmmb_plan** out);
 int fmmb_plan_destroy(fmmb_plan* plan);
 /* info[0] = levels, info[1] = nodes, info[2] = points, info[3] = far pairs,
- * info[4 .. 4+levels] = first node of each level and the node count (cap: entries of info). */
+ * info[4 .. 4+levels] = first node of each level and the node count, then (if cap allows) the
+ * targets per M2L block (cap: entries of info, at least 5 + levels). */
 int fmmb_plan_info(const fmmb_plan* plan, int64_t* info, int cap);
 int fmmb_plan_box(const fmmb_plan* plan, double* origin3, double* width);
 /* The flat tree (src/tree/tree.jl:40-71), downloaded: any pointer may be NULL.
@@ -140,6 +141,18 @@ int fmmb_batch_plan_create_dev(fmmb_cache* cache, const double* xyz_dev, const i
  * (ninst: the global level of each root) and node_instance (nnodes). */
 int fmmb_batch_plan_instances(const fmmb_plan* plan, int64_t* ninst, int64_t* offsets, double* boxes,
                               int32_t* root_level, int32_t* node_instance);
+
+/* The autotuner (no counterpart in the reference): times the launch shapes of a state's matvec on
+ * the given inputs (the plan's points, n of them, and its charges, or 3×n Stokeslets) — the M2L
+ * block size (32, 64, 128 targets; when tune_blocks, re-cutting the plan's blocks, which its other
+ * states share), the FP64 M2L's chunk width, the near field's warps per CTA — keeps the fastest
+ * and applies it, and records it for later plans and states of the same method, kernel, order,
+ * precision path and N rounded down to a power of two. No result depends on these shapes. The
+ * state's expansions must be built again afterwards. out (may be NULL): 5 doubles, the block
+ * size, the chunk-width variant, the warps, and the chosen M2L and near-field times in ms. */
+int fmmb_autotune(fmmb_state* state, const double* xyz, const double* tau, int64_t n, int tune_blocks, double* out);
+int fmmb_autotune_dev(fmmb_state* state, const double* xyz_dev, const double* tau_dev, int64_t n, int tune_blocks,
+                      double* out);
 
 /* FMMState (src/fmm.jl:64-94): the expansions of one right-hand side, in a precision path. */
 int fmmb_state_create(fmmb_plan* plan, int precision, fmmb_state** out);
@@ -266,7 +279,8 @@ int fmmb_direct_noalloc_dev(fmmb_ctx* ctx, const double* src_dev, const double* 
 typedef struct fmmb_server fmmb_server;
 typedef struct {
   int32_t slots;       /* concurrent groups (worker threads, one stream each), 1..64 */
-  int32_t ppl;         /* points per leaf of every request's tree */
+  int32_t ppl;         /* points per leaf of every request's tree; 0: by the request's order and path
+                          (64 on the mixed path and up to p = 8, 128 to p = 13, 256 to 17, 512 above) */
   int64_t hbm_budget;  /* bytes of device memory the admitted requests may hold; 0: 80 % of the free memory */
   int32_t group_max;   /* requests per group; 0: 64; 1: every request alone */
   int32_t reserved;
