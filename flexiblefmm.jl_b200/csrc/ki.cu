@@ -9,7 +9,7 @@
 //               transformed (k_ki_forward, half spectrum, FP32); per target the Hadamard sums
 //               Σ κ̂_o ⊙ σ̂_s over its far pairs (k_ki_hadamard: one frequency block of 64 per
 //               CTA, the block of the 316 kernel tables in shared memory, a warp per target,
-//               float4 loads of the sources' spectra, 8 pairs in flight); the inverse transform at the target's
+//               float4 loads of the sources' spectra, 16 pairs in flight); the inverse transform at the target's
 //               small-surface points added to its check potentials (k_ki_inverse)
 //   locals      the leaves' densities on their large surfaces, V·(S⁺Uᴴ·check) (DMMA GEMMs)
 //   L2T (a22)   the surface sums of the leaves' local densities (eval.cu) and the near field
@@ -32,7 +32,7 @@ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 constexpr int FB = 64;             // frequencies per block of the Hadamard stage
 constexpr int HAD_THREADS = 512;   // 16 warps, one target at a time each
-constexpr int HAD_UNROLL = 8;
+constexpr int HAD_UNROLL = 16;
 constexpr int SIDE = 2 * KI_PMAX;
 
 
@@ -106,12 +106,12 @@ __global__ void __launch_bounds__(128) k_ki_forward(int first, int p, int ns, in
                                                     const double* __restrict__ M, const float2* __restrict__ tw,
                                                     const int* __restrict__ embed, float2* __restrict__ spec) {
   extern __shared__ float2 smf[];
-  __shared__ float2 c_tw[SIDE];                     // e^{−2πi k/n}, n = 2p
+  __shared__ float2 c_tw[SIDE * SIDE];              // [j·n + k] = e^{−2πi jk/n}, n = 2p
   const int g = first + blockIdx.x, n = 2 * p, nh = p + 1, tid = threadIdx.x;
   float2* a1 = smf;                                 // [nh·p·p]
   float2* a2 = a1 + nh * p * p;                     // [nh·n·p]
   float* x = reinterpret_cast<float*>(a2 + nh * n * p);   // [p³]
-  for (int i = tid; i < n; i += 128) c_tw[i] = tw[i];
+  for (int i = tid; i < n * n; i += 128) c_tw[i] = tw[(i / n) * (i % n) % n];
   for (int i = tid; i < p * p * p; i += 128) x[i] = 0.f;
   __syncthreads();
   const double* col = M + (int64_t)g * LD;
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(128) k_ki_forward(int first, int p, int ns, in
     float re = 0.f, im = 0.f;
     for (int j1 = 0; j1 < p; ++j1) {
       const float v = x[j1 + p * r];
-      const float2 t = c_tw[(j1 * k1) % n];
+      const float2 t = c_tw[j1 * n + k1];
       re = fmaf(v, t.x, re);
       im = fmaf(v, t.y, im);
     }
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(128) k_ki_forward(int first, int p, int ns, in
     const int k1 = o % nh, k2 = (o / nh) % n, j3 = o / (nh * n);
     float re = 0.f, im = 0.f;
     for (int j2 = 0; j2 < p; ++j2) {
-      const float2 a = a1[k1 + nh * (j2 + p * j3)], t = c_tw[(j2 * k2) % n];
+      const float2 a = a1[k1 + nh * (j2 + p * j3)], t = c_tw[j2 * n + k2];
       re = fmaf(a.x, t.x, fmaf(-a.y, t.y, re));
       im = fmaf(a.x, t.y, fmaf(a.y, t.x, im));
     }
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(128) k_ki_forward(int first, int p, int ns, in
     const int k12 = o % (nh * n), k3 = o / (nh * n);
     float re = 0.f, im = 0.f;
     for (int j3 = 0; j3 < p; ++j3) {
-      const float2 a = a2[k12 + nh * n * j3], t = c_tw[(j3 * k3) % n];
+      const float2 a = a2[k12 + nh * n * j3], t = c_tw[j3 * n + k3];
       re = fmaf(a.x, t.x, fmaf(-a.y, t.y, re));
       im = fmaf(a.x, t.y, fmaf(a.y, t.x, im));
     }
@@ -220,10 +220,10 @@ __global__ void __launch_bounds__(128) k_ki_inverse(int first, int p, int ns, in
                                                     const int* __restrict__ embed, const float2* __restrict__ U,
                                                     double* __restrict__ Pl) {
   extern __shared__ float2 sm2[];
-  __shared__ float2 c_tw[SIDE];
+  __shared__ float2 c_tw[SIDE * SIDE];              // [j·n + k] = e^{−2πi jk/n}
   const int g = first + blockIdx.x, n = 2 * p, nh = p + 1, tid = threadIdx.x;
   if (ptr[g] == ptr[g + 1]) return;                 // no far pairs: nothing to add
-  for (int i = tid; i < n; i += 128) c_tw[i] = tw[i];
+  for (int i = tid; i < n * n; i += 128) c_tw[i] = tw[(i / n) * (i % n) % n];
   float2* u = sm2;                                  // [nh·n·n]
   float2* b3 = u + nh * n * n;                      // [nh·n·p]: b3[k1 + nh·(k2 + n·j3)]
   float2* b2 = b3 + nh * n * p;                     // [nh·p·p]: b2[k1 + nh·(j2 + p·j3)]
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(128) k_ki_inverse(int first, int p, int ns, in
     const int k12 = o % (nh * n), j3 = o / (nh * n);
     float re = 0.f, im = 0.f;
     for (int k3 = 0; k3 < n; ++k3) {
-      const float2 a = u[k12 + nh * n * k3], t = c_tw[(j3 * k3) % n];   // × conj(t)
+      const float2 a = u[k12 + nh * n * k3], t = c_tw[j3 * n + k3];   // × conj(t)
       re = fmaf(a.x, t.x, fmaf(a.y, t.y, re));
       im = fmaf(a.y, t.x, fmaf(-a.x, t.y, im));
     }
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(128) k_ki_inverse(int first, int p, int ns, in
     const int k1 = o % nh, j2 = (o / nh) % p, j3 = o / (nh * p);
     float re = 0.f, im = 0.f;
     for (int k2 = 0; k2 < n; ++k2) {
-      const float2 a = b3[k1 + nh * (k2 + n * j3)], t = c_tw[(j2 * k2) % n];
+      const float2 a = b3[k1 + nh * (k2 + n * j3)], t = c_tw[j2 * n + k2];
       re = fmaf(a.x, t.x, fmaf(a.y, t.y, re));
       im = fmaf(a.y, t.x, fmaf(-a.x, t.y, im));
     }
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(128) k_ki_inverse(int first, int p, int ns, in
     const float2* b = b2 + nh * r;
     float v = b[0].x + ((j1 & 1) ? -b[p].x : b[p].x);   // k1 = 0 and k1 = n/2 = p
     for (int k1 = 1; k1 < p; ++k1) {
-      const float2 t = c_tw[(j1 * k1) % n];         // Re(b · e^{+iθ}) = b.x cos θ − b.y sin θ, t.y = −sin θ
+      const float2 t = c_tw[j1 * n + k1];           // Re(b · e^{+iθ}) = b.x cos θ − b.y sin θ, t.y = −sin θ
       v += 2.f * fmaf(b[k1].x, t.x, b[k1].y * t.y);
     }
     xo[o] = v;

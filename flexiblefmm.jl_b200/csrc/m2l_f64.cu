@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
   const int level = b.x & 255;
   const double alpha = m2l_scale[level];
   const int* co = cls_off + (int64_t)blockIdx.x * (NCLASS + 1);
-  const int kmax = (NP + BK - 1) / BK * BK;
+  const int kmax = (NP + BK - 1) / BK * BK, RT = (NP + 7) / 8;
   for (int k = tid; k < LD; k += 256) {
     int n, m, part;
     coef_nmp(k, n, m, part);
@@ -194,9 +194,10 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
       }
       for (int j = nc + warp; j < NB; j += 8)
         for (int k = lane; k < LD; k += 32) G[j * GS + k] = 0.0;
-      // product Y = A·G on the FP64 tensor cores: warp w the rows [w·LD/8, (w+1)·LD/8) (MT tiles of
-      // 8) × all NB columns (NT tiles of 8), K-steps of 4; A streamed through shared memory in
-      // slabs of BK rows of K, the next slab prefetched into registers
+      // product Y = A·G on the FP64 tensor cores: warp w the row tiles w, w + 8, w + 16, ... below
+      // the last real row (RT tiles of 8 rows; the rows past NP are zero and are not multiplied)
+      // × all NB columns (NT tiles of 8), K-steps of 4; A streamed through shared memory in slabs
+      // of BK rows of K, the next slab prefetched into registers
       double acc[MT][NT][2];
 #pragma unroll
       for (int mt = 0; mt < MT; ++mt)
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
 #pragma unroll
         for (int u = 0; u < AL; ++u) {
           const int e = tid + 256 * u, i = e % LD, k = e / LD;
-          ra[u] = (e < BK * LD && k0 + k < kmax) ? A[(int64_t)(k0 + k) * LD + i] : 0.0;
+          ra[u] = (e < BK * LD && k0 + k < kmax && i < 8 * RT) ? A[(int64_t)(k0 + k) * LD + i] : 0.0;
         }
       };
       load_a(0);
@@ -225,22 +226,24 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
         for (int ks = 0; ks < BK; ks += 4) {
           double af[MT], bf[NT];
 #pragma unroll
-          for (int mt = 0; mt < MT; ++mt) af[mt] = As[(ks + t) * LDA + warp * (LD / 8) + 8 * mt + g];
+          for (int mt = 0; mt < MT; ++mt) af[mt] = As[(ks + t) * LDA + 8 * (warp + 8 * mt) + g];
 #pragma unroll
           for (int nt = 0; nt < NT; ++nt) bf[nt] = G[(8 * nt + g) * GS + k0 + ks + t];
 #pragma unroll
           for (int mt = 0; mt < MT; ++mt)
+            if (warp + 8 * mt < RT)                    // warp-uniform
 #pragma unroll
-            for (int nt = 0; nt < NT; ++nt) dmma(acc[mt][nt], af[mt], bf[nt]);
+              for (int nt = 0; nt < NT; ++nt) dmma(acc[mt][nt], af[mt], bf[nt]);
         }
       }
       __syncthreads();
 #pragma unroll
       for (int mt = 0; mt < MT; ++mt)
+        if (warp + 8 * mt < RT)
 #pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
+          for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-          for (int i = 0; i < 2; ++i) G[(8 * nt + 2 * t + i) * GS + warp * (LD / 8) + 8 * mt + g] = acc[mt][nt][i];
+            for (int i = 0; i < 2; ++i) G[(8 * nt + 2 * t + i) * GS + 8 * (warp + 8 * mt) + g] = acc[mt][nt][i];
       __syncthreads();
       // scatter: thread j owns entry j of the targets' partial locals, four targets (runs of the
       // chunk's pairs) at a time
