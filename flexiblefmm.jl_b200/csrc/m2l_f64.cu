@@ -7,13 +7,18 @@
 //           up in a table of its swaps and signs over the 16 group elements, built once per
 //           CTA; partner entries by warp shuffles)
 //   product Y = A_class G on the FP64 tensor cores (mma.sync m8n8k4 f64, DMMA: there is no FP64
-//           tcgen05 kind), A streamed through shared memory in K-slabs of 16 with the next slab
-//           prefetched into registers; each warp an (LD/8 rows) × NB register tile
+//           tcgen05 kind); each warp owns the row tiles w, w + 8, ... below (p+1)² (the padded
+//           rows are not multiplied) × all NB columns, and copies its own rows of A, slab by slab
+//           of K, into two shared-memory stages of its own with cp.async (no CTA barrier inside
+//           the product; the first two slabs are in flight during the gather)
 //   scatter (P_t Y) into the targets' partial locals: each target's entry takes its pairs one by
 //           one in the list's order, starting from the value in memory (the block owns its
 //           targets: deterministic, no atomics, and the sums do not depend on where the chunks
-//           end nor on the other targets of the block); the partial locals of four targets are
-//           read at once
+//           end nor on the other targets of the block); the chunk's runs of one target are found
+//           once, and four runs' sums are stepped together, branch-free
+// The time per chunk goes to the product (DMMA-bound while both CTAs of an SM multiply), the
+// scatter (its dependent FP64 FMAs queue behind the other CTA's DMMAs on the shared FP64 pipe)
+// and the gather, in that order.
 #include "d4h.cuh"
 #include "passes.cuh"
 
@@ -57,10 +62,24 @@ __device__ __forceinline__ uint32_t perm_masks(int k, bool target) {
   return swap | neg << 16;
 }
 
+// the class operator's rows reach each warp through its own two shared-memory stages of BK rows
+// of K (cp.async, no CTA barrier): its MT row tiles, S = 8·MT + 4 doubles apart (≡ 4 or 12 mod 16:
+// the fragment loads are free of bank conflicts)
+template <int LD> constexpr int f64_bk() { return LD / 64 <= 3 ? 16 : 8; }
+template <int LD> constexpr int f64_s() { return 8 * (LD / 64) + 4; }
 template <int LD, int NB>
 constexpr size_t m2l_f64_smem() {
-  return sizeof(double) * (16 * (LD + 4) + NB * (LD + 4)) + sizeof(int) * 4 * NB + sizeof(uint32_t) * LD + LD;
+  return sizeof(double) * (8 * 2 * f64_bk<LD>() * f64_s<LD>() + NB * (LD + 4)) + sizeof(int) * (5 * NB + 4) +
+         sizeof(uint32_t) * LD + LD;
 }
+
+__device__ __forceinline__ void cpa16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 // two CTAs per SM where their shared memory fits (the registers are then capped at 128)
 template <int LD, int NB>
 constexpr int m2l_f64_ctas() { return m2l_f64_smem<LD, NB>() <= 113 * 1024 ? 2 : 1; }
@@ -74,21 +93,26 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
   const int comp = blockIdx.y, psi = stokes && comp == 3;
   // row tiles per warp, column tiles; strides ≡ 4 (mod 16) doubles keep the fragment loads free
   // of shared-memory bank conflicts
-  constexpr int BK = 16, MT = LD / 64, NT = NB / 8, GS = LD + 4, LDA = LD + 4, AL = (BK * LD + 255) / 256;
+  constexpr int BK = f64_bk<LD>(), MT = LD / 64, NT = NB / 8, GS = LD + 4, S = f64_s<LD>(), ASTG = BK * S;
+  constexpr int CPL = BK * MT * 4 / 32;   // 16-byte copies per lane and stage
+  static_assert(BK * MT * 4 % 32 == 0, "a stage is whole copies per lane");
+  static_assert(NB % 4 == 0, "the entry masks are read as uint4: 5·NB + 4 ints before them keep 16-byte alignment");
   // entry quartets per lane (LD = 64: lanes ≥ 16 idle). A pair of entries never straddles a
   // multiple of 128 (entries 128, 256, 384 are real parts or m = 0), so the partner of a
   // lane's first and last entry is always in the neighbouring lane of the same quartet row.
   constexpr int Q = (LD + 127) / 128;
+  constexpr int HC = 2 < NB / 8 ? 2 : NB / 8;   // columns per warp with their loads in flight together
   extern __shared__ double sm[];
-  double* As = sm;                 // [BK][LDA]
-  double* G = As + BK * LDA;       // [NB][GS]: the gathered columns, then the product
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double* Aw = sm + warp * 2 * ASTG;   // this warp's two stages, [BK][S] each
+  double* G = sm + 8 * 2 * ASTG;       // [NB][GS]: the gathered columns, then the product
   int* ps = (int*)(G + NB * GS);
   int* pf = ps + NB;
   int* pt = pf + NB;
   int* pfac = pt + NB;               // the pairs' D4h elements
-  uint32_t* smsk = (uint32_t*)(pfac + NB);   // [LD]: the gather's masks per entry (0 past NP)
+  int* rst = pfac + NB;              // [NB + 4]: the chunk's runs of one target (starts, nc), their count
+  uint32_t* smsk = (uint32_t*)(rst + NB + 4);   // [LD]: the gather's masks per entry (0 past NP), 16-byte aligned
   int8_t* sdir = (int8_t*)(smsk + LD);       // [LD]: where each entry's partner is (+1 Re, −1 Im, 0)
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int4 b = blocks[blockIdx.x];
   const int level = b.x & 255;
   const double alpha = m2l_scale[level];
@@ -116,6 +140,16 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
       tmsk[i] = perm_masks(j, true);
     }
   }
+  // this warp's rows of the slab of A at K-row k0 into stage st (rows of tiles past RT skipped)
+  auto stage_a = [&](const double* A, int k0, int st) {
+    double* dst = Aw + st * ASTG;
+#pragma unroll
+    for (int u = 0; u < CPL; ++u) {
+      const int c = lane + 32 * u, k = c / (4 * MT), rem = c % (4 * MT), mt = rem >> 2, q = rem & 3;
+      if (warp + 8 * mt < RT) cpa16(dst + k * S + 8 * mt + 2 * q, A + (int64_t)(k0 + k) * LD + 8 * (warp + 8 * mt) + 2 * q);
+    }
+    cpa_commit();
+  };
   for (int c = 0; c < NCLASS; ++c) {
     const int a0 = co[c], a1 = co[c + 1];
     const double* A = reinterpret_cast<const double*>(reps_lv[level]) + (int64_t)c * LD * LD;   // the level's representatives
@@ -128,13 +162,29 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
           ps[j] = pr.x; pf[j] = pr.y >> 8; pt[j] = pr.y & 0xff; pfac[j] = c_d4h[pr.y >> 8];
         } else { ps[j] = -1; pf[j] = 0; pt[j] = -1; pfac[j] = 0; }
       }
+      // the first two slabs of A on their way while the columns are gathered
+      stage_a(A, 0, 0);
+      if (BK < kmax) stage_a(A, BK, 1);
       __syncthreads();
-      // gather: warp w the columns w, w + 8, ..., two at a time (both columns' loads in flight
-      // before either is permuted); lane l the entries 4(l + 32 r) .. + 3
-      for (int j0 = warp; j0 < nc; j0 += 16) {
-        double a[2][Q][4];
+      // the runs of the chunk's pairs (the pairs of a class are grouped by target: each target
+      // has one run), by the last warp
+      if (warp == 7) {
+        int base = 0;
+        for (int q1 = 0; q1 < nc; q1 += 32) {
+          const int q = q1 + lane;
+          const bool start = q < nc && (q == 0 || pt[q] != pt[q - 1]);
+          const unsigned bal = __ballot_sync(0xffffffffu, start);
+          if (start) rst[base + __popc(bal & ((1u << lane) - 1u))] = q;
+          base += __popc(bal);
+        }
+        if (lane == 0) { rst[base] = nc; rst[NB + 1] = base; }
+      }
+      // gather: warp w the columns w, w + 8, ..., HC at a time (their loads all in flight before
+      // any is permuted); lane l the entries 4(l + 32 r) .. + 3
+      for (int j0 = warp; j0 < nc; j0 += 8 * HC) {
+        double a[HC][Q][4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < HC; ++h) {
           const int j = j0 + 8 * h;
           const bool on = j < nc;
           const double* src = M + (int64_t)(on ? ps[j] : 0) * pitch + (int64_t)comp * LD;
@@ -166,7 +216,7 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
           }
         }
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < HC; ++h) {
           const int j = j0 + 8 * h;
           if (j >= nc) continue;                       // warp-uniform
           const int fac = pfac[j];
@@ -194,39 +244,27 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
       }
       for (int j = nc + warp; j < NB; j += 8)
         for (int k = lane; k < LD; k += 32) G[j * GS + k] = 0.0;
+      __syncthreads();
       // product Y = A·G on the FP64 tensor cores: warp w the row tiles w, w + 8, w + 16, ... below
       // the last real row (RT tiles of 8 rows; the rows past NP are zero and are not multiplied)
-      // × all NB columns (NT tiles of 8), K-steps of 4; A streamed through shared memory in slabs
-      // of BK rows of K, the next slab prefetched into registers
+      // × all NB columns (NT tiles of 8), K-steps of 4; A through the warp's two stages, the slab
+      // after next copied while this one is multiplied
       double acc[MT][NT][2];
 #pragma unroll
       for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
         for (int nt = 0; nt < NT; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
       const int g = lane >> 2, t = lane & 3;
-      double ra[AL];
-      auto load_a = [&](int k0) {
-#pragma unroll
-        for (int u = 0; u < AL; ++u) {
-          const int e = tid + 256 * u, i = e % LD, k = e / LD;
-          ra[u] = (e < BK * LD && k0 + k < kmax && i < 8 * RT) ? A[(int64_t)(k0 + k) * LD + i] : 0.0;
-        }
-      };
-      load_a(0);
-      for (int k0 = 0; k0 < kmax; k0 += BK) {
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < AL; ++u) {
-          const int e = tid + 256 * u;
-          if (e < BK * LD) As[(e / LD) * LDA + e % LD] = ra[u];
-        }
-        __syncthreads();
-        if (k0 + BK < kmax) load_a(k0 + BK);
+      int st = 0;
+      for (int k0 = 0; k0 < kmax; k0 += BK, st ^= 1) {
+        if (k0 + BK < kmax) cpa_wait<1>(); else cpa_wait<0>();
+        __syncwarp();
+        const double* As = Aw + st * ASTG;
 #pragma unroll
         for (int ks = 0; ks < BK; ks += 4) {
           double af[MT], bf[NT];
 #pragma unroll
-          for (int mt = 0; mt < MT; ++mt) af[mt] = As[(ks + t) * LDA + 8 * (warp + 8 * mt) + g];
+          for (int mt = 0; mt < MT; ++mt) af[mt] = As[(ks + t) * S + 8 * mt + g];
 #pragma unroll
           for (int nt = 0; nt < NT; ++nt) bf[nt] = G[(8 * nt + g) * GS + k0 + ks + t];
 #pragma unroll
@@ -235,6 +273,8 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
 #pragma unroll
               for (int nt = 0; nt < NT; ++nt) dmma(acc[mt][nt], af[mt], bf[nt]);
         }
+        __syncwarp();                                  // the stage is read: refill it
+        if (k0 + 2 * BK < kmax) stage_a(A, k0 + 2 * BK, st);
       }
       __syncthreads();
 #pragma unroll
@@ -245,8 +285,10 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
 #pragma unroll
             for (int i = 0; i < 2; ++i) G[(8 * nt + 2 * t + i) * GS + 8 * (warp + 8 * mt) + g] = acc[mt][nt][i];
       __syncthreads();
-      // scatter: thread j owns entry j of the targets' partial locals, four targets (runs of the
-      // chunk's pairs) at a time
+      // scatter: thread j owns entry j of the targets' partial locals; RB runs (targets) at a time,
+      // each summed in the list's order from its value in memory, the runs stepped together
+      constexpr int RB = 4;
+      const int nrun = rst[NB + 1];
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
         const int j = tid + 256 * i;
@@ -254,28 +296,41 @@ __global__ void __launch_bounds__(256, m2l_f64_ctas<LD, NB>()) k_m2l_f64(const i
         const int jp = tpart[i];
         const uint32_t mk = tmsk[i];
         double* plj = Pl + (int64_t)b.y * pitch + (int64_t)comp * LD + j;
-        for (int q = 0; q < nc;) {
-          int st[4], en[4], tg[4];
-          double pv[4];
+        for (int r0 = 0; r0 < nrun; r0 += RB) {
+          int rs[RB], re[RB];
+          int64_t to[RB];
+          double run[RB];
+          int len = 0;
 #pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            st[r] = q;
-            tg[r] = q < nc ? pt[q] : 0;
-            pv[r] = q < nc ? plj[(int64_t)tg[r] * pitch] : 0.0;
-            while (q < nc && pt[q] == tg[r]) ++q;
-            en[r] = q;
+          for (int r = 0; r < RB; ++r) {
+            const bool on = r0 + r < nrun;
+            rs[r] = on ? rst[r0 + r] : 0;
+            re[r] = on ? rst[r0 + r + 1] : 0;
+            to[r] = (int64_t)(on ? pt[rs[r]] : 0) * pitch;
+            run[r] = on ? plj[to[r]] : 0.0;
+            len = max(len, re[r] - rs[r]);
+          }
+          // branch-free steps: every run's loads issued before any sum (a run past its end reads
+          // pair 0 and keeps its value)
+          for (int e = 0; e < len; ++e) {
+            double y[RB];
+            uint32_t ng[RB];
+#pragma unroll
+            for (int r = 0; r < RB; ++r) {
+              const int k = rs[r] + e < re[r] ? rs[r] + e : 0;
+              const int f = pfac[k];
+              y[r] = G[k * GS + ((mk >> f) & 1 ? jp : j)];
+              ng[r] = (mk >> (16 + f)) & 1;
+            }
+#pragma unroll
+            for (int r = 0; r < RB; ++r) {
+              const double v = fma(alpha, ng[r] ? -y[r] : y[r], run[r]);
+              run[r] = rs[r] + e < re[r] ? v : run[r];
+            }
           }
 #pragma unroll
-          for (int r = 0; r < 4; ++r)
-            if (st[r] < en[r]) {
-              double run = pv[r];
-              for (int k = st[r]; k < en[r]; ++k) {
-                const int f = pfac[k];
-                const double y = G[k * GS + ((mk >> f) & 1 ? jp : j)];
-                run = fma(alpha, (mk >> (16 + f)) & 1 ? -y : y, run);
-              }
-              plj[(int64_t)tg[r] * pitch] = run;
-            }
+          for (int r = 0; r < RB; ++r)
+            if (r0 + r < nrun) plj[to[r]] = run[r];
         }
       }
     }
