@@ -66,6 +66,8 @@ def args_():
     a.add_argument("--stokes-instances", type=int, default=64, help="instances of the batched Stokes measurement (0: skip it)")
     a.add_argument("--ki-points", type=int, default=2_000_000, help="points of the cube KI measurement (0: skip it)")
     a.add_argument("--no-circle-ki", action="store_true", help="skip the 2D circle KI measurement")
+    a.add_argument("--peaks", action="store_true",
+                   help="measure the FP64 (DGEMM) and FP32 (SGEMM, no TF32) rates of this GPU and exit")
     return a.parse_args()
 
 
@@ -504,18 +506,24 @@ def cube_ki(fmmb, torch, ctx, n, steps, warmup, samples=4096):
     err = {"pot_rel_l2": float(np.linalg.norm(u[sel] - dp_h) / np.linalg.norm(dp_h)),
            "grad_rel_l2": float(np.linalg.norm(g[sel] - dg_h) / np.linalg.norm(dg_h))}
     nfreq = 9 * 16 * 16
-    ntarget = f.nnodes - int(f.level_start[2])
-    # the spectral stage streams each far pair's source spectrum (FP32 complex) once and writes
-    # one spectrum per box twice (the transform and the target sums)
-    fft_bytes = 8.0 * nfreq * (f.npairs + 2 * ntarget)
+    # the Hadamard pull (k_ki_hadamard), the spectral stage's largest kernel, moves 16 B per far pair
+    # and frequency through the SM's L1/shared-memory data pipe: the source's spectrum (FP32
+    # complex, served by L1 and L2) and the offset's table entry (shared memory). That pipe, at
+    # 128 B per cycle per SM, bounds it; DRAM stays near 5 % busy.
+    l1_bytes = 16.0 * nfreq * f.npairs
+    l1_peak = 148 * 128 * 1.965e9
     return {"workload": f"{n:,} points from 16 Gaussians (sigma 0.01, centres U[0.1, 0.9]^3, seed 4), charges U(-1,1) "
                         "as FP32 values; CubeKernelIndependent{3}(Laplace3D; p=8, pc=16, d=0.1), ppl=64, bbox (0,1); "
                         "potential + gradient at the sources",
             "precision": "FP32 spectra, far field (surface sums) and near field; FP64 dense translations",
             "evals_per_s": n / (ms / 1e3), "ms_per_step": ms, "plan_s": plan_s, "levels": f.nlevels, "nodes": f.nnodes,
             "far_pairs": f.npairs, "stages_ms": stages, "error": {"samples": len(sel), **err},
-            "spectral_m2l": {"bytes": fft_bytes, "GB_per_s": fft_bytes / (stages["m2l"] / 1e3) / 1e9,
-                             "note": "source spectra per far pair + spectra and target sums per box, / the m2l stage"}}
+            "spectral_m2l": {"bound": "L1/shared-memory data pipe", "l1_bytes": l1_bytes,
+                             "l1_TB_per_s_over_stage": l1_bytes / (stages["m2l"] / 1e3) / 1e12,
+                             "l1_peak_TB_per_s": l1_peak / 1e12,
+                             "note": "16 B per far pair and frequency (source spectrum + table entry) through L1/shared "
+                                     "memory, over the whole spectral stage (forward transforms + Hadamard pull + "
+                                     "inverse transforms); the peak is 148 SMs x 128 B/cycle at 1965 MHz"}}
 
 
 # ---------------------------------------------------------------- the 2D circle KI method
@@ -828,8 +836,53 @@ def compact_side(p10, serve, stokes, ki, kic):
     return s
 
 
+def measure_peaks(reps=10):
+    """The FP64 and FP32 denominators of the FP64 kernels' rooflines: cuBLAS DGEMM (FP64 tensor
+    cores, DMMA) and SGEMM with TF32 off (FP32 FMA on the CUDA cores), square n = 8192, the best
+    of `reps` CUDA-event timings after three warm-ups (2n³ flop each), then the same back to back
+    for about three seconds (sustained), with the SM clocks sampled meanwhile."""
+    import torch
+    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cudnn.allow_tf32 = False
+    out = {"gpu_name": torch.cuda.get_device_name(0), "n": 8192}
+    clk = Clocks(torch.cuda.current_device())
+    for key, dt in (("fp64_dgemm_tflops", torch.float64), ("fp32_sgemm_tflops", torch.float32)):
+        n = 8192
+        g = torch.Generator(device="cuda").manual_seed(1)
+        x = torch.randn(n, n, dtype=dt, device="cuda", generator=g)
+        y = torch.randn(n, n, dtype=dt, device="cuda", generator=g)
+        z = torch.empty(n, n, dtype=dt, device="cuda")
+        for _ in range(3):
+            torch.matmul(x, y, out=z)
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(x, y, out=z)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k = max(1, int(3000.0 / best))
+        e0.record()
+        for _ in range(k):
+            torch.matmul(x, y, out=z)
+        e1.record()
+        e1.synchronize()
+        flop = 2.0 * n ** 3
+        out[key] = round(flop / (best * 1e-3) / 1e12, 2)
+        out[key + "_sustained"] = round(flop * k / (e0.elapsed_time(e1) * 1e-3) / 1e12, 2)
+        del x, y, z
+    out["clocks"] = clk.stop()
+    print(json.dumps(out))
+
+
 def main():
     a = args_()
+    if a.peaks:
+        measure_peaks()
+        return
     if a.impl == "reference":
         run_reference(a)
     else:
