@@ -24,6 +24,91 @@ namespace {
 
 constexpr int NEAR_WARPS = 4;
 
+// The leaf's local expansion prepared for L2P (harmonics.jl:447-486): per (m, n), m-major, eight
+// values — the potential's coefficient pair and the three gradient components' pairs (each from
+// the degree-(n+1) coefficients and the recurrence tables), the factor 2 of the m ≥ 1 terms
+// folded in — so that every term of the point loop is a complex dot product a·v with the
+// regular harmonic v = Υ̃_n^m(x̂). Built once per leaf (FP64, then rounded to R).
+template <int P>
+__host__ __device__ constexpr int l2p_entries() { return (P + 1) * (P + 2) / 2; }
+__device__ __forceinline__ int l2p_entry(int P, int m, int n) { return m * (P + 1) - m * (m - 1) / 2 + n - m; }
+
+template <int P, typename R>
+__device__ void l2p_prepare(const double* __restrict__ L, R* __restrict__ E, int lane) {
+  for (int q = lane; q < l2p_entries<P>(); q += 32) {
+    int m = 0, rem = q;
+    while (rem >= P + 1 - m) { rem -= P + 1 - m; ++m; }
+    const int n = m + rem;
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // potential: Σ L_n^m conj Υ̃ (harmonics.jl:455-462)
+    if (m == 0) v[0] = L[n * n];
+    else { v[0] = 2 * L[n * n + 2 * m - 1]; v[1] = 2 * L[n * n + 2 * m]; }
+    // gradient from degree n + 1 (harmonics.jl:465-486)
+    if (n < P) {
+      const int n1 = n + 1;
+      if (m == 0) {
+        const double cmv = ctab<double>(3 * TRI_MAX + tri(n1, 1));
+        v[2] = -cmv * L[n1 * n1 + 1];
+        v[4] = -cmv * L[n1 * n1 + 2];
+        v[6] = ctab<double>(2 * TRI_MAX + tri(n1, 0)) * L[n1 * n1];
+      } else {
+        const double ur = L[n1 * n1 + 2 * (m + 1) - 1], ui = L[n1 * n1 + 2 * (m + 1)];
+        double dr, di;
+        if (m == 1) { dr = L[n1 * n1]; di = 0; }
+        else { dr = L[n1 * n1 + 2 * (m - 1) - 1]; di = L[n1 * n1 + 2 * (m - 1)]; }
+        const double cu = 0.5 * ctab<double>(3 * TRI_MAX + tri(n1, m + 1));
+        const double cd = 0.5 * ctab<double>(4 * TRI_MAX + tri(n1, m - 1));
+        const double czv = ctab<double>(2 * TRI_MAX + tri(n1, m));
+        v[2] = 2 * (-cu * ur + cd * dr); v[3] = 2 * (-cu * ui + cd * di);
+        v[4] = -2 * (cu * ui + cd * di); v[5] = 2 * (cu * ur + cd * dr);
+        v[6] = 2 * czv * L[n1 * n1 + 2 * m - 1]; v[7] = 2 * czv * L[n1 * n1 + 2 * m];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) E[8 * q + i] = (R)v[i];
+  }
+}
+
+template <typename R> struct alignas(4 * sizeof(R)) Quad { R a, b, c, d; };
+
+// L2P at x̂ from the prepared entries (potential and the gradient before the 1/w factor)
+template <int P, typename R>
+__device__ __forceinline__ void l2p_prepared(const R* __restrict__ E, R x, R y, R z, R& u, R& gx, R& gy, R& gz) {
+  const R r2 = x * x + y * y + z * z;
+  R sr = 1, si = 0;
+  u = 0; gx = 0; gy = 0; gz = 0;
+#pragma unroll 1
+  for (int m = 0; m <= P; ++m) {
+    R pr = 0, pi = 0, cr = sr, ci = si;
+    const Quad<R>* Em = reinterpret_cast<const Quad<R>*>(E + 8 * l2p_entry(P, m, m));
+#pragma unroll 2
+    for (int n = m; n <= P; ++n) {
+      R vr, vi;
+      if (n == m) { vr = sr; vi = si; }
+      else {
+        const int t = tri(n, m);
+        const R az = ctab<R>(t) * z, br = ctab<R>(TRI_MAX + t) * r2;
+        vr = az * cr - br * pr; vi = az * ci - br * pi;
+        pr = cr; pi = ci; cr = vr; ci = vi;
+      }
+      const Quad<R> a = Em[2 * (n - m)], b = Em[2 * (n - m) + 1];
+      u += a.a * vr + a.b * vi;
+      gx += a.c * vr + a.d * vi;
+      gy += b.a * vr + b.b * vi;
+      gz += b.c * vr + b.d * vi;
+    }
+    if (m < P) {
+      const R e = ce<R>(m);
+      const R nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
+      sr = nr; si = ni;
+    }
+  }
+}
+
+// per-warp shared memory of k_l2p: the prepared entries, or (Yukawa3D) the local itself
+template <int P, typename R, bool YK>
+size_t l2p_warp_bytes(int LD) { return YK ? sizeof(R) * LD : sizeof(R) * 8 * l2p_entries<P>(); }
+
 // YK: Yukawa3D's weighted L2P (FP64), κ̂² = kh2[level]
 template <int P, typename R, bool YK>
 __global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, const int* __restrict__ gstart,
@@ -37,9 +122,13 @@ __global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, cons
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = blockIdx.x * (blockDim.x >> 5) + warp;
   if (grp >= ngroups) return;
-  R* L = reinterpret_cast<R*>(sl_raw) + warp * LD;
   const int leaf = gnode[grp];
-  for (int i = lane; i < LD; i += 32) L[i] = (R)Pl[(int64_t)leaf * LD + i];
+  R* L = reinterpret_cast<R*>(sl_raw) + warp * (YK ? LD : 8 * l2p_entries<P>());
+  if constexpr (YK) {
+    for (int i = lane; i < LD; i += 32) L[i] = (R)Pl[(int64_t)leaf * LD + i];
+  } else {
+    l2p_prepare<P, R>(Pl + (int64_t)leaf * LD, L, lane);
+  }
   __syncwarp();
   const int4 c = cell[leaf];
   const Geometry gn = geo.at(leaf);
@@ -52,7 +141,7 @@ __global__ void __launch_bounds__(256) k_l2p(const int* __restrict__ gnode, cons
     const double x = act ? tx[k] : cx, y = act ? ty[k] : cy, z = act ? tz[k] : cz;
     R u, gx, gy, gz;
     if constexpr (YK) l2p_yukawa<P>(L, kh2[c.w], (x - cx) * s, (y - cy) * s, (z - cz) * s, u, gx, gy, gz);
-    else l2p<P, R>(L, (R)((x - cx) * s), (R)((y - cy) * s), (R)((z - cz) * s), u, gx, gy, gz);
+    else l2p_prepared<P, R>(L, (R)((x - cx) * s), (R)((y - cy) * s), (R)((z - cz) * s), u, gx, gy, gz);
     if (act) {
       const int o = tout[k];
       // acc: the near field is already in the outputs (x + y = y + x: the same sums either way)
@@ -567,13 +656,16 @@ template <int P>
 void launch_l2p(State& S, const int* gnode, const int* gstart, const int* gcount, int ng, const double* tx, const double* ty,
                 const double* tz, const int* tout, int outputs, double* pot, double* grad, int acc = 0) {
   Plan& P_ = *S.plan;
-  const int warps = 8;
   // the mixed path evaluates Laplace3D in FP32; Yukawa3D keeps its radial weights in FP64 (its
   // mixed path is the tensor-core M2L only)
   const bool yk = P_.cache->kernel == FMMB_KERNEL_YUKAWA3D;
   const bool mixed = S.precision == FMMB_PRECISION_MIXED && !yk;
-  const size_t smem = (mixed ? sizeof(float) : sizeof(double)) * warps * P_.cache->ld;
+  const size_t per_warp = mixed ? l2p_warp_bytes<P, float, false>(P_.cache->ld)
+                                : (yk ? l2p_warp_bytes<P, double, true>(P_.cache->ld) : l2p_warp_bytes<P, double, false>(P_.cache->ld));
+  const int warps = per_warp > 8192 ? 4 : 8;
+  const size_t smem = per_warp * warps;
   auto kern = mixed ? k_l2p<P, float, false> : (yk ? k_l2p<P, double, true> : k_l2p<P, double, false>);
+  FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(ng + warps - 1) / warps, 32 * warps, smem, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout, P_.cell.p,
                                                                       S.Pl.p, P_.cache->ld, geometry(P_), P_.d_scale.p,
                                                                       outputs, pot, grad, P_.d_kh2.p, acc);

@@ -179,19 +179,22 @@ __global__ void k_p2m_dip(const int* __restrict__ nodes, int nn, const int4* __r
 // one thread per (node, order m): M_n^m += τ conj Υ̃_n^m((y − c)/w) over the node's sources,
 // n = m..P, the chain of order m started from its own sectoral value (harmonics.jl:682-743)
 // Yukawa3D (YK): the degree-n terms weighted by u_n(κ̂|x̂|), κ̂² = kh2[level]
-// (harmonics_yukawa.jl:281-296)
-template <int P, bool YK>
+// (harmonics_yukawa.jl:281-296). R = float on the mixed path of Laplace3D (box-centred, scaled
+// coordinates in [−½, ½]³, sums over the box's sources in FP32, written as doubles: about 2⁻²⁴
+// per coefficient, below the FP16x3 M2L's 2⁻²² that consumes them).
+template <int P, bool YK, typename R>
 __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restrict__ cell, const int* __restrict__ plo,
                       const int* __restrict__ phi, const double* __restrict__ xs, const double* __restrict__ ys,
                       const double* __restrict__ zs, const double* __restrict__ q, Geometry geo,
                       const double* __restrict__ scale, int64_t pitch, double* __restrict__ M,
                       const double* __restrict__ kh2) {
+  static_assert(!YK || sizeof(R) == 8, "Yukawa3D's P2M runs in FP64");
   // the recurrence tables in shared memory: the lanes of a warp run different orders and would
   // serialise on the constant cache
-  __shared__ double s_ab[2 * TRI_MAX];
-  __shared__ double s_e[PMAX];
-  for (int i = threadIdx.x; i < 2 * TRI_MAX; i += blockDim.x) s_ab[i] = c_tab[i];
-  for (int i = threadIdx.x; i < PMAX; i += blockDim.x) s_e[i] = c_e[i];
+  __shared__ R s_ab[2 * TRI_MAX];
+  __shared__ R s_e[PMAX];
+  for (int i = threadIdx.x; i < 2 * TRI_MAX; i += blockDim.x) s_ab[i] = ctab<R>(i);
+  for (int i = threadIdx.x; i < PMAX; i += blockDim.x) s_e[i] = ce<R>(i);
   __syncthreads();
   // thread g: order m = g / nn of node g % nn; the lanes of a warp share the order, so the
   // recurrence's branches on n versus m are uniform
@@ -204,33 +207,34 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
   double w = ldexp(geo.W0, -c.w), s = scale[c.w];
   double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w), cz = gn.center(2, c.z, w);
   const double k2 = YK ? kh2[c.w] : 0.0;
-  double ar[P + 1], ai[P + 1];
+  R ar[P + 1], ai[P + 1];
 #pragma unroll
   for (int n = 0; n <= P; ++n) { ar[n] = 0; ai[n] = 0; }
   int j1 = phi[node];
   for (int j = plo[node]; j <= j1; ++j) {
-    double x = (xs[j] - cx) * s, y = (ys[j] - cy) * s, z = (zs[j] - cz) * s;
-    double r2 = x * x + y * y + z * z;
-    double sr = 1.0, si = 0.0;
+    const R x = R((xs[j] - cx) * s), y = R((ys[j] - cy) * s), z = R((zs[j] - cz) * s);
+    const R r2 = x * x + y * y + z * z;
+    R sr = 1, si = 0;
     for (int k = 1; k <= m; ++k) {
-      double e = s_e[k - 1];
-      double nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
+      const R e = s_e[k - 1];
+      const R nr = -e * (x * sr - y * si), ni = -e * (x * si + y * sr);
       sr = nr; si = ni;
     }
-    double tau = q[j];
+    const R tau = R(q[j]);
     double u[P + 1];
-    if constexpr (YK) yukawa_u<P>(k2 * r2, u);
-    double pr = 0, pi = 0, cr = 0, ci = 0;
+    if constexpr (YK) yukawa_u<P>(k2 * (double)r2, u);
+    R pr = 0, pi = 0, cr = 0, ci = 0;
 #pragma unroll
     for (int n = 0; n <= P; ++n) {
-      const double tn = YK ? tau * u[n] : tau;
+      R tn = tau;
+      if constexpr (YK) tn = tau * u[n];
       if (n == m) {
         cr = sr; ci = si; pr = 0; pi = 0;
         ar[n] += tn * cr; ai[n] -= tn * ci;
       } else if (n > m) {
         int t = tri(n, m);
-        double az = s_ab[t] * z, br = s_ab[TRI_MAX + t] * r2;
-        double nr = az * cr - br * pr, ni = az * ci - br * pi;
+        const R az = s_ab[t] * z, br = s_ab[TRI_MAX + t] * r2;
+        const R nr = az * cr - br * pr, ni = az * ci - br * pi;
         pr = cr; pi = ci; cr = nr; ci = ni;
         ar[n] += tn * nr; ai[n] -= tn * ni;
       }
@@ -240,8 +244,8 @@ __global__ void k_p2m(const int* __restrict__ nodes, int nn, const int4* __restr
 #pragma unroll
   for (int n = 0; n <= P; ++n) {
     if (n < m) continue;
-    if (m == 0) col[n * n] = ar[n];
-    else { col[n * n + 2 * m - 1] = ar[n]; col[n * n + 2 * m] = ai[n]; }
+    if (m == 0) col[n * n] = (double)ar[n];
+    else { col[n * n + 2 * m - 1] = (double)ar[n]; col[n * n + 2 * m] = (double)ai[n]; }
   }
 }
 
@@ -255,19 +259,31 @@ __device__ __forceinline__ void dmma_gemm(double* d, double a, double b) {
                : "d"(a), "d"(b));
 }
 
-// C(:, g) (=|+=) A · B(:, g) for mapped columns g; A column-major M × K (M a multiple of 128);
-// rows r with r mod LD ≥ NP written as 0. 128 × BN tiles on the FP64 tensor cores (DMMA): warp w
-// the rows [16w, 16w + 16) × all BN columns; K-slabs of 32 in shared memory (row strides of 4 mod
-// 16 doubles: conflict-free fragment loads), the next slab prefetched into registers.
+// C(:, g) (=|+=) A · B(:, g) for mapped columns g; A column-major M × K; rows r with r mod LD ≥ NP
+// written as 0. 128 × BN tiles on the FP64 tensor cores (DMMA): warp w the rows [16w, 16w + 16) ×
+// all BN columns; K-slabs of 32 in shared memory (row strides of 4 mod 16 doubles: conflict-free
+// fragment loads), the next slab prefetched into registers. Padding is not multiplied where it
+// fills whole units of the loop: a warp whose 16 rows all have r mod LD ≥ NP (or lie past M)
+// skips its MMAs, and, when KLD > 0, a slab whose columns k all have k mod KLD ≥ KNP is skipped —
+// the caller guarantees that those columns of A are zero (M2M and L2L: the expansions' padded
+// entries). The inner loop itself stays branch-free.
 template <int BN>
 __global__ void __launch_bounds__(256) k_gemm_tiles(int M, int K, const double* __restrict__ A, ColMap bm, ColMap cm,
-                                                    int ncols, int LD, int NP, int accumulate) {
+                                                    int ncols, int LD, int NP, int accumulate, int KLD, int KNP) {
   constexpr int BM = 128, BK = 32, NT = BN / 8, LDA = BM + 4, LDB = BN + 4;
   constexpr int AL = BM * BK / 256, BL = (BK * BN + 255) / 256;
   __shared__ double As[BK * LDA];
   __shared__ double Bs[BK * LDB];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
+  // padding: rows (8-row sub-tiles of this warp) and K ranges with nothing to multiply
+  auto pad_rows = [&](int r, int n) { const int m = r % LD; return r >= M || (m >= NP && m + n <= LD); };
+  auto pad_k = [&](int k, int n) {
+    if (KLD <= 0) return false;
+    const int m = k % KLD;
+    return m >= KNP && m + n <= KLD;
+  };
+  const bool live = !pad_rows(row0 + 16 * warp, 16);
   double acc[2][NT][2];
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt)
@@ -292,27 +308,37 @@ __global__ void __launch_bounds__(256) k_gemm_tiles(int M, int K, const double* 
       rb[u] = (bcol[u] && k0 + k < K) ? bcol[u][k0 + k] : 0.0;
     }
   };
-  load(0);
-  for (int k0 = 0; k0 < K; k0 += BK) {
+  // the slabs with something to multiply, in order
+  auto next_slab = [&](int k) {
+    while (k < K && pad_k(k, BK)) k += BK;
+    return k;
+  };
+  int k0 = next_slab(0);
+  if (k0 < K) load(k0);
+  for (; k0 < K;) {
+    const int k1 = next_slab(k0 + BK);
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < AL; ++u) { const int e = tid + 256 * u; As[(e / BM) * LDA + e % BM] = ra[u]; }
 #pragma unroll
     for (int u = 0; u < BL; ++u) { const int e = tid + 256 * u; if (e < BK * BN) Bs[(e % BK) * LDB + e / BK] = rb[u]; }
     __syncthreads();
-    if (k0 + BK < K) load(k0 + BK);
+    if (k1 < K) load(k1);
+    if (live) {                                        // uniform across the warp
 #pragma unroll
-    for (int ks = 0; ks < BK; ks += 4) {
-      double af[2], bf[NT];
+      for (int ks = 0; ks < BK; ks += 4) {
+        double af[2], bf[NT];
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt) af[mt] = As[(ks + t) * LDA + 16 * warp + 8 * mt + g];
+        for (int mt = 0; mt < 2; ++mt) af[mt] = As[(ks + t) * LDA + 16 * warp + 8 * mt + g];
 #pragma unroll
-      for (int nt = 0; nt < NT; ++nt) bf[nt] = Bs[(ks + t) * LDB + 8 * nt + g];
+        for (int nt = 0; nt < NT; ++nt) bf[nt] = Bs[(ks + t) * LDB + 8 * nt + g];
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
+        for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < NT; ++nt) dmma_gemm(acc[mt][nt], af[mt], bf[nt]);
+          for (int nt = 0; nt < NT; ++nt) dmma_gemm(acc[mt][nt], af[mt], bf[nt]);
+      }
     }
+    k0 = k1;
   }
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt)
@@ -333,14 +359,14 @@ __global__ void __launch_bounds__(256) k_gemm_tiles(int M, int K, const double* 
 
 // the column-tile width: enough tiles to cover the SMs
 void gemm_cols(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols, int LD, int NP, int accumulate, int num_sms,
-               cudaStream_t s) {
+               cudaStream_t s, int KLD = 0, int KNP = 0) {
   const int rows = (M + 127) / 128;
   if ((int64_t)rows * ((ncols + 31) / 32) >= num_sms) {
-    k_gemm_tiles<32><<<dim3((ncols + 31) / 32, rows), 256, 0, s>>>(M, K, A, bm, cm, ncols, LD, NP, accumulate);
+    k_gemm_tiles<32><<<dim3((ncols + 31) / 32, rows), 256, 0, s>>>(M, K, A, bm, cm, ncols, LD, NP, accumulate, KLD, KNP);
   } else if ((int64_t)rows * ((ncols + 15) / 16) >= num_sms) {
-    k_gemm_tiles<16><<<dim3((ncols + 15) / 16, rows), 256, 0, s>>>(M, K, A, bm, cm, ncols, LD, NP, accumulate);
+    k_gemm_tiles<16><<<dim3((ncols + 15) / 16, rows), 256, 0, s>>>(M, K, A, bm, cm, ncols, LD, NP, accumulate, KLD, KNP);
   } else {
-    k_gemm_tiles<8><<<dim3((ncols + 7) / 8, rows), 256, 0, s>>>(M, K, A, bm, cm, ncols, LD, NP, accumulate);
+    k_gemm_tiles<8><<<dim3((ncols + 7) / 8, rows), 256, 0, s>>>(M, K, A, bm, cm, ncols, LD, NP, accumulate, KLD, KNP);
   }
   FMMB_LAUNCH_CHECK();
 }
@@ -463,7 +489,10 @@ void launch_p2m(State& S, const double* q, const double* d3, double* M, int64_t 
     FMMB_LAUNCH_CHECK();
     return;
   }
-  auto kern = P_.cache->kernel == FMMB_KERNEL_YUKAWA3D ? k_p2m<P, true> : k_p2m<P, false>;
+  // FP32 on the mixed path of Laplace3D (charges only), FP64 otherwise
+  auto kern = P_.cache->kernel == FMMB_KERNEL_YUKAWA3D ? k_p2m<P, true, double>
+              : (S.precision == FMMB_PRECISION_MIXED && P_.cache->kernel == FMMB_KERNEL_LAPLACE3D) ? k_p2m<P, false, float>
+                                                                                                  : k_p2m<P, false, double>;
   kern<<<nblk(nth, 128), 128, 0, P_.ctx->stream>>>(P_.s2m_nodes.p, P_.n_s2m, P_.cell.p, P_.plo.p, P_.phi.p, S.xs.p, S.ys.p,
                                                  S.zs.p, q, geometry(P_), P_.d_scale.p, pitch, M, P_.d_kh2.p);
   FMMB_LAUNCH_CHECK();
@@ -580,6 +609,11 @@ void gemm_columns(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols
   gemm_cols(M, K, A, bm, cm, ncols, LD, NP, accumulate, num_sms, s);
 }
 
+void gemm_expansions(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols, int LD, int NP, int accumulate,
+                     int num_sms, cudaStream_t s) {
+  gemm_cols(M, K, A, bm, cm, ncols, LD, NP, accumulate, num_sms, s, LD, NP);
+}
+
 int p2m(State& S) {
   if (S.plan->cache->method == FMMB_METHOD_CUBE_KI) return ki_p2m(S);
   if (S.plan->cache->method == FMMB_METHOD_KI_CIRCLE) return kic_p2m(S);
@@ -601,7 +635,7 @@ int m2m_sweep(State& S) {
     int c0 = P.level_start[l + 1], ng = P.level_groups[l + 1];
     if (ng == 0) continue;
     ColMap bm{S.M.p, nullptr, c0, NCH}, cm{S.M.p, P.group_parent[l + 1].p, 0, 0};
-    gemm_cols(C.ld, NCH * C.ld, P.lv_m2m[l], bm, cm, ng, C.ld, C.np, 0, P.ctx->num_sms, s);
+    gemm_cols(C.ld, NCH * C.ld, P.lv_m2m[l], bm, cm, ng, C.ld, C.np, 0, P.ctx->num_sms, s, C.ld, C.np);
     ++launches;
   }
   return launches;
@@ -640,7 +674,7 @@ int l2l_sweep(State& S) {
     int c0 = P.level_start[l], ng = P.level_groups[l];
     if (ng == 0) continue;
     ColMap bm{S.Pl.p, P.group_parent[l].p, 0, 0}, cm{S.Pl.p, nullptr, c0, NCH};
-    gemm_cols(NCH * C.ld, C.ld, P.lv_l2l[l - 1], bm, cm, ng, C.ld, C.np, 1, P.ctx->num_sms, s);
+    gemm_cols(NCH * C.ld, C.ld, P.lv_l2l[l - 1], bm, cm, ng, C.ld, C.np, 1, P.ctx->num_sms, s, C.ld, C.np);
     ++launches;
   }
   // the kernel-independent method: the leaves' local densities from their check potentials

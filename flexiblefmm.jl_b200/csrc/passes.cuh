@@ -209,6 +209,10 @@ struct ColMap {
 // C(:, g) (=|+=) A · B(:, g) on the FP64 tensor cores; rows r with r mod LD ≥ NP written as 0
 void gemm_columns(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols, int LD, int NP, int accumulate,
                   int num_sms, cudaStream_t s);
+// the same over expansions (K in blocks of LD whose entries k mod LD ≥ NP are zero columns of A:
+// M2M and L2L), without multiplying that padding
+void gemm_expansions(int M, int K, const double* A, ColMap bm, ColMap cm, int ncols, int LD, int NP, int accumulate,
+                     int num_sms, cudaStream_t s);
 // P2M of the childless sourced nodes with charges q (tree order) into the block at M (node pitch)
 // P2M of charges q and, when d3 (3 × N planar) is given, dipoles into M (pitch doubles per node)
 void p2m_block(State& S, const double* q, const double* d3, double* M, int64_t pitch);

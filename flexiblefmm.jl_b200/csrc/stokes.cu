@@ -478,7 +478,7 @@ void stokes_build(State& S, const double* xyz_dev, const StokesDensities& d) {
       k_stokes_m2m_in<<<nblk((int64_t)ng * NCH * LD), 256, 0, s>>>(S.M.p, c0, ng, LD, a, X.p);
       FMMB_LAUNCH_CHECK();
       ColMap bm{X.p, nullptr, 0, NCH}, cm{S.M.p + (int64_t)a * LD, P.group_parent[l + 1].p, 0, 0, pitch};
-      gemm_columns(LD, NCH * LD, P.lv_m2m[l], bm, cm, ng, LD, C.np, 0, P.ctx->num_sms, s);
+      gemm_expansions(LD, NCH * LD, P.lv_m2m[l], bm, cm, ng, LD, C.np, 0, P.ctx->num_sms, s);
     }
   }
   // M2L of every block (the Ψ̂ launch with the coupling), then L2L level by level
@@ -490,7 +490,7 @@ void stokes_build(State& S, const double* xyz_dev, const StokesDensities& d) {
     DBuf<double> R(4 * per);
     for (int a = 0; a < 4; ++a) {
       ColMap bm{S.Pl.p + (int64_t)a * LD, P.group_parent[l].p, 0, 0, pitch}, cm{R.p + a * per, nullptr, 0, NCH};
-      gemm_columns(NCH * LD, LD, P.lv_l2l[l - 1], bm, cm, ng, LD, C.np, 0, P.ctx->num_sms, s);
+      gemm_expansions(NCH * LD, LD, P.lv_l2l[l - 1], bm, cm, ng, LD, C.np, 0, P.ctx->num_sms, s);
     }
     k_stokes_l2l_out<<<nblk(per), 256, 0, s>>>(S.Pl.p, R.p, c0, ng, LD, C.np);
     FMMB_LAUNCH_CHECK();

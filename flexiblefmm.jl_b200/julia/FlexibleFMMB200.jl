@@ -181,6 +181,21 @@ function build_expansions!(st::FMMState, f::FMM, sources::AbstractVector{SVector
                 st.h, pts, tau, f.n))
     return st
 end
+# The launch shapes of this state timed on its own inputs and the fastest kept (fmmb_autotune);
+# no result depends on them. Returns (block targets, FP64 chunk variant, near-field warps,
+# M2L ms, near-field ms).
+function autotune!(st::FMMState, f::FMM, sources::AbstractVector{SVector{3,Float64}}, τ::AbstractVector{<:Real};
+                   tune_blocks::Bool=true)
+    length(sources) == f.n || throw(DimensionMismatch("expected $(f.n) sources"))
+    length(τ) == f.n || throw(DimensionMismatch("expected $(f.n) densities"))
+    pts = collect(sources)
+    tau = Vector{Float64}(τ)
+    out = zeros(Float64, 5)
+    check(ccall((:fmmb_autotune, libfmmb), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Cint, Ptr{Float64}),
+                st.h, pts, tau, f.n, tune_blocks ? 1 : 0, out))
+    return (Int(out[1]), Int(out[2]), Int(out[3]), out[4], out[5])
+end
+
 # Dipole densities, alone or as (charge, Dipole) tuples per source (src/sources.jl:16-31)
 function build_expansions!(st::FMMState, f::FMM, sources::AbstractVector{SVector{3,Float64}},
                            τ::AbstractVector{<:Union{Dipole{3,Float64},Tuple{Float64,Dipole{3,Float64}}}})
