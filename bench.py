@@ -765,7 +765,7 @@ def run_ours(a):
     line = {
         "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "fp16x3 M2L (tcgen05 kind::f16, FP32 accumulation) + f32 near field (FP64 batch sums), f64 elsewhere",
+        "dtype": "fp16x3 M2L (tcgen05 kind::f16, FP32 accumulation); f32 P2M, L2P and near field (FP64 batch sums); f64 M2M/L2L (DMMA)",
         "data": "synthetic (seeded uniform points, N(0,1) charges)",
         "config": config(a, {"precision": "mixed", "levels": f.nlevels, "nodes": f.nnodes, "far_pairs": f.npairs}),
         "roofline": {"bound": "tensor", "kernel": "k_m2l_tc (M2L, all levels, one launch)", "achieved": achieved,
