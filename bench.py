@@ -760,7 +760,8 @@ def run_ours(a):
     kic = None if a.no_circle_ki else circle_ki(fmmb)
     # every figure, on a line of its own before the headline
     detail = {"configured_order_p10": side, "serving": serve, "stokes_batched": stokes, "cube_ki": ki, "circle_ki": kic,
-              "parity": par, "stages_ms": stages, "error": {"samples": len(sel), **err}, "tuned": R["tuned"]}
+              "parity": par, "plan_s": plan_s, "stages_ms": stages, "error": {"samples": len(sel), **err},
+              "tuned": R["tuned"]}
     print(json.dumps({"bench_detail": detail}), flush=True)
     line = {
         "metric": METRIC, "value": replica_throughput(a.n, ms_mixed, world), "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -781,9 +782,6 @@ def run_ours(a):
         "fp64": {"value": _sig(replica_throughput(a.n, ms_fp64, world)), "ms_per_step": _sig(ms_fp64)},
         "mixed_vs_fp64": _sig(ms_fp64 / ms_mixed),
         "error": {"samples": len(sel), **_sig(err)},
-        "stages_ms": {"plan_s": _sig(plan_s), **_sig(stages)},
-        "tuned": {k: {"tb": v["block_targets"], "nb_alt": v["f64_chunk_variant"], "near_w": v["near_warps"]}
-                  for k, v in R["tuned"].items()},
         "parity": compact_parity(par),
         "side": compact_side(side, serve, stokes, ki, kic),
     }
@@ -807,8 +805,8 @@ def _sig(x, d=4):
 def compact_parity(par):
     out = {}
     for k, r in par.items():
-        out[k] = {"pass": r["pass"], "tree_equal": r["tree_equal"], "far_pairs_equal": r["far_pairs_equal"],
-                  "fp64_maxrel": _sig(r["fp64_vs_oracle_maxrel"], 3), "mixed_rel_l2": _sig(r["mixed_vs_oracle_rel_l2"], 3)}
+        out[k] = {"pass": r["pass"], "fp64_maxrel": _sig(r["fp64_vs_oracle_maxrel"], 3),
+                  "mixed_rel_l2": _sig(r["mixed_vs_oracle_rel_l2"], 3)}
     return out
 
 
@@ -822,8 +820,6 @@ def compact_side(p10, serve, stokes, ki, kic):
                         "open_frac": _sig(serve["open_loop"]["fraction_of_batched"], 3),
                         "p50_ms": _sig(serve["open_loop"]["latency_ms"]["p50"], 3), "p99_ms": _sig(serve["open_loop"]["latency_ms"]["p99"], 3),
                         "fp64_one": _sig(serve["one_at_a_time_fp64"]["evals_per_s"])}
-        if "host_device_s" in serve:
-            s["serving"]["host_device_s"] = _sig(serve["host_device_s"], 3)
     if stokes:
         s["stokes"] = {"instances": stokes["instances"], "batched": _sig(stokes["batched"]["evals_per_s"]),
                        "eval_dev": _sig(stokes["eval_device"]["evals_per_s"]), "one": _sig(stokes["one_at_a_time"]["evals_per_s"]),
