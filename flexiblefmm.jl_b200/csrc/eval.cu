@@ -431,10 +431,63 @@ __global__ void __launch_bounds__(W * 32, W == 4 ? 5 : 2) k_near(const int* __re
 }
 
 // The kernel-independent far field (l2t, src/operators/ki_common.jl:293-327): at each target
-// Σ_k G(x − y_k) L_k over the leaf's large surface y_k = c + w·ŷ_k (ŷ at width 1), the local
-// density L staged per warp in shared memory, times w (the pseudo-inverse's scale). R = float:
-// leaf-centred FP32 terms summed in FP32 per 32 surface points, the partial sums in FP64;
+// Σ_k G(x − y_k) L_k over the leaf's large surface y_k = c + w·ŷ_k (ŷ at width 1), times w (the
+// pseudo-inverse's scale). A warp per leaf, lanes over the surface points (a lane takes every
+// 32nd): each lane reads its points and densities once per batch of up to TB targets held in
+// registers, then the batch's sums are reduced across the lanes in FP64. (Leaves of the adaptive
+// configurations hold a few points each, so lanes over the targets would mostly idle.)
+// R = float: leaf-centred FP32 terms, each lane's partial sums in FP32, the reduction in FP64;
 // R = double: FP64 throughout. Writes the outputs (the near field adds to them).
+template <typename R, int TB>
+__device__ __forceinline__ void ki_l2t_batch(int k0, int nb, const double* __restrict__ tx, const double* __restrict__ ty,
+                                             const double* __restrict__ tz, const int* __restrict__ tout,
+                                             const double* __restrict__ L, const double* __restrict__ large, int nl,
+                                             double w, double cx, double cy, double cz, int lane, int outputs,
+                                             double* __restrict__ pot, double* __restrict__ grad) {
+  R px[TB], py[TB], pz[TB], au[TB], ax[TB], ay[TB], az[TB];
+#pragma unroll
+  for (int i = 0; i < TB; ++i) {
+    const int k = k0 + (i < nb ? i : 0);             // slots past the batch repeat its first target
+    px[i] = (R)(tx[k] - cx); py[i] = (R)(ty[k] - cy); pz[i] = (R)(tz[k] - cz);
+    au[i] = 0; ax[i] = 0; ay[i] = 0; az[i] = 0;
+  }
+  for (int q = lane; q < nl; q += 32) {
+    const R yx = (R)(w * large[3 * q]), yy = (R)(w * large[3 * q + 1]), yz = (R)(w * large[3 * q + 2]);
+    const R l = (R)L[q];
+#pragma unroll
+    for (int i = 0; i < TB; ++i) {
+      const R dx = px[i] - yx, dy = py[i] - yy, dz = pz[i] - yz;
+      const R ir = rsqrt(dx * dx + dy * dy + dz * dz);
+      const R li = l * ir;
+      au[i] += li;
+      const R li3 = li * ir * ir;
+      ax[i] += li3 * dx;
+      ay[i] += li3 * dy;
+      az[i] += li3 * dz;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < TB; ++i) {
+    double u = au[i], gx = ax[i], gy = ay[i], gz = az[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      u += __shfl_xor_sync(0xffffffffu, u, o);
+      gx += __shfl_xor_sync(0xffffffffu, gx, o);
+      gy += __shfl_xor_sync(0xffffffffu, gy, o);
+      gz += __shfl_xor_sync(0xffffffffu, gz, o);
+    }
+    if (lane == i && i < nb) {
+      const int t = tout[k0 + i];
+      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[t] = KC * w * u;
+      if (outputs & FMMB_OUTPUT_GRADIENT) {
+        grad[3 * (int64_t)t] = -KC * w * gx;
+        grad[3 * (int64_t)t + 1] = -KC * w * gy;
+        grad[3 * (int64_t)t + 2] = -KC * w * gz;
+      }
+    }
+  }
+}
+
 template <typename R>
 __global__ void __launch_bounds__(128) k_ki_l2t(const int* __restrict__ gnode, const int* __restrict__ gstart,
                                                 const int* __restrict__ gcount, int ngroups, const double* __restrict__ tx,
@@ -443,54 +496,25 @@ __global__ void __launch_bounds__(128) k_ki_l2t(const int* __restrict__ gnode, c
                                                 const double* __restrict__ Ll, int nl, int nld,
                                                 const double* __restrict__ large, Geometry geo, int outputs,
                                                 double* __restrict__ pot, double* __restrict__ grad) {
-  extern __shared__ __align__(16) unsigned char sk_raw[];
+  constexpr int TB = sizeof(R) == 4 ? 8 : 4;         // targets per batch
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = blockIdx.x * (blockDim.x >> 5) + warp;
   if (grp >= ngroups) return;
-  R* L = reinterpret_cast<R*>(sk_raw) + (size_t)warp * 4 * nl;   // [nl] densities, then [3·nl] points
-  R* Y = L + nl;
   const int leaf = gnode[grp];
   const int4 c = cell[leaf];
   const Geometry gn = geo.at(leaf);
   const double w = ldexp(geo.W0, -c.w);
   const double cx = gn.center(0, c.x, w), cy = gn.center(1, c.y, w), cz = gn.center(2, c.z, w);
-  for (int k = lane; k < nl; k += 32) {
-    L[k] = (R)Ll[(int64_t)leaf * nld + k];
-    Y[3 * k] = (R)(w * large[3 * k]);
-    Y[3 * k + 1] = (R)(w * large[3 * k + 1]);
-    Y[3 * k + 2] = (R)(w * large[3 * k + 2]);
-  }
-  __syncwarp();
+  const double* L = Ll + (int64_t)leaf * nld;
   const int t0 = gstart[grp], nt = gcount[grp];
-  for (int base = 0; base < nt; base += 32) {
-    const int k = t0 + base + lane;
-    const bool act = base + lane < nt;
-    const R x = act ? (R)(tx[k] - cx) : R(0), y = act ? (R)(ty[k] - cy) : R(0), z = act ? (R)(tz[k] - cz) : R(0);
-    double u = 0, gx = 0, gy = 0, gz = 0;
-    for (int k0 = 0; k0 < nl; k0 += 32) {
-      R bu = 0, bx = 0, by = 0, bz = 0;
-      const int k1 = min(nl, k0 + 32);
-      for (int q = k0; q < k1; ++q) {
-        const R dx = x - Y[3 * q], dy = y - Y[3 * q + 1], dz = z - Y[3 * q + 2];
-        const R ir = rsqrt(dx * dx + dy * dy + dz * dz);
-        const R li = L[q] * ir;
-        bu += li;
-        const R li3 = li * ir * ir;
-        bx += li3 * dx;
-        by += li3 * dy;
-        bz += li3 * dz;
-      }
-      u += bu; gx += bx; gy += by; gz += bz;
-    }
-    if (act) {
-      const int o = tout[k];
-      if (outputs & FMMB_OUTPUT_POTENTIAL) pot[o] = KC * w * u;
-      if (outputs & FMMB_OUTPUT_GRADIENT) {
-        grad[3 * (int64_t)o] = -KC * w * gx;
-        grad[3 * (int64_t)o + 1] = -KC * w * gy;
-        grad[3 * (int64_t)o + 2] = -KC * w * gz;
-      }
-    }
+  for (int b = 0; b < nt; b += TB) {
+    const int nb = min(TB, nt - b);                  // uniform across the warp
+    if (nb > TB / 2)
+      ki_l2t_batch<R, TB>(t0 + b, nb, tx, ty, tz, tout, L, large, nl, w, cx, cy, cz, lane, outputs, pot, grad);
+    else if (nb > TB / 4)
+      ki_l2t_batch<R, TB / 2>(t0 + b, nb, tx, ty, tz, tout, L, large, nl, w, cx, cy, cz, lane, outputs, pot, grad);
+    else
+      ki_l2t_batch<R, TB / 4>(t0 + b, nb, tx, ty, tz, tout, L, large, nl, w, cx, cy, cz, lane, outputs, pot, grad);
   }
 }
 
@@ -707,12 +731,9 @@ void evaluate_groups(State& S, const int* gnode, const int* gstart, const int* g
     Plan& P_ = *S.plan;
     Cache& C = *P_.cache;
     const bool mixed = S.precision == FMMB_PRECISION_MIXED;
-    const size_t per_warp = (mixed ? sizeof(float) : sizeof(double)) * 4 * C.ki_nl;
-    const int warps = (int)std::max<size_t>(1, std::min<size_t>(4, (200u << 10) / per_warp));
-    const size_t smem = per_warp * warps;
+    const int warps = 4;
     auto kern = mixed ? k_ki_l2t<float> : k_ki_l2t<double>;
-    FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<(ng + warps - 1) / warps, 32 * warps, smem, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout,
+    kern<<<(ng + warps - 1) / warps, 32 * warps, 0, P_.ctx->stream>>>(gnode, gstart, gcount, ng, tx, ty, tz, tout,
                                                                        P_.cell.p, S.ki_ll.p, C.ki_nl, C.ki_nld,
                                                                        C.ki_large.p, geometry(P_), outputs, pot, grad);
     FMMB_LAUNCH_CHECK();
