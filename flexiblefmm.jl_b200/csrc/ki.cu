@@ -61,15 +61,20 @@ std::vector<double> pad(const std::vector<double>& a, int rows, int cols, int R,
 // ---------------------------------------------------------------- P2M: check potentials
 // one CTA per childless node with sources: pM[k] = w · Σ_j G(w·y_k − (x_j − c)) τ_j at the
 // large-surface points y_k (width 1), the factor w being the pseudo-inverse's scale; the
-// sources staged in shared memory 256 at a time, each thread owning its check points
+// sources staged in shared memory 256 at a time, each thread owning its check points.
+// R = float on the mixed path (box-centred FP32 terms and sums, the method's FP32 far field
+// consumes them), double on the plain path.
 constexpr int CHK_SRC = 256;
+__device__ __forceinline__ double rsqrt_r(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
+template <typename R>
 __global__ void __launch_bounds__(128) k_ki_check(const int* __restrict__ nodes, const int4* __restrict__ cell,
                                                   const int* __restrict__ plo, const int* __restrict__ phi,
                                                   const double* __restrict__ xs, const double* __restrict__ ys,
                                                   const double* __restrict__ zs, const double* __restrict__ q,
                                                   Geometry geo, const double* __restrict__ large, int nl, int nld,
                                                   double* __restrict__ pM) {
-  __shared__ double sx[CHK_SRC], sy[CHK_SRC], sz[CHK_SRC], sq[CHK_SRC];
+  __shared__ R sx[CHK_SRC], sy[CHK_SRC], sz[CHK_SRC], sq[CHK_SRC];
   const int node = nodes[blockIdx.x];
   const int4 c = cell[node];
   const double w = ldexp(geo.W0, -c.w);
@@ -79,21 +84,21 @@ __global__ void __launch_bounds__(128) k_ki_check(const int* __restrict__ nodes,
   for (int b = j0; b <= j1; b += CHK_SRC) {
     __syncthreads();
     for (int i = threadIdx.x; i < CHK_SRC && b + i <= j1; i += 128) {
-      sx[i] = xs[b + i] - cx;
-      sy[i] = ys[b + i] - cy;
-      sz[i] = zs[b + i] - cz;
-      sq[i] = q[b + i];
+      sx[i] = (R)(xs[b + i] - cx);
+      sy[i] = (R)(ys[b + i] - cy);
+      sz[i] = (R)(zs[b + i] - cz);
+      sq[i] = (R)q[b + i];
     }
     __syncthreads();
     const int m = min(CHK_SRC, j1 - b + 1);
     for (int k = threadIdx.x; k < nl; k += 128) {
-      const double yx = w * large[3 * k], yy = w * large[3 * k + 1], yz = w * large[3 * k + 2];
-      double a = b == j0 ? 0.0 : out[k];
+      const R yx = (R)(w * large[3 * k]), yy = (R)(w * large[3 * k + 1]), yz = (R)(w * large[3 * k + 2]);
+      R a = b == j0 ? R(0) : (R)out[k];
       for (int s = 0; s < m; ++s) {
-        const double dx = yx - sx[s], dy = yy - sy[s], dz = yz - sz[s];
-        a = fma(sq[s], rsqrt(fma(dz, dz, fma(dy, dy, dx * dx))), a);
+        const R dx = yx - sx[s], dy = yy - sy[s], dz = yz - sz[s];
+        a = fma(sq[s], rsqrt_r(fma(dz, dz, fma(dy, dy, dx * dx))), a);
       }
-      out[k] = a;
+      out[k] = (double)a;
     }
   }
   for (int k = threadIdx.x; k < nl; k += 128) out[k] *= w * KC;
@@ -351,7 +356,8 @@ int ki_p2m(State& S) {
   Cache& C = *P.cache;
   cudaStream_t s = P.ctx->stream;
   if (P.n_s2m == 0) return 0;
-  k_ki_check<<<P.n_s2m, 128, 0, s>>>(P.s2m_nodes.p, P.cell.p, P.plo.p, P.phi.p, S.xs.p, S.ys.p, S.zs.p, S.q.p, geometry(P),
+  auto chk = S.precision == FMMB_PRECISION_MIXED ? k_ki_check<float> : k_ki_check<double>;
+  chk<<<P.n_s2m, 128, 0, s>>>(P.s2m_nodes.p, P.cell.p, P.plo.p, P.phi.p, S.xs.p, S.ys.p, S.zs.p, S.q.p, geometry(P),
                                      C.ki_large.p, C.ki_nl, C.ki_nld, S.ki_pm.p);
   FMMB_LAUNCH_CHECK();
   const int sms = P.ctx->num_sms;
