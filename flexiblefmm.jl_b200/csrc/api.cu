@@ -350,7 +350,7 @@ int fmmb_ctx_create(int device, fmmb_ctx** out) {
     FMMB_CUDA(cudaSetDevice(device));
     cudaDeviceProp prop;
     FMMB_CUDA(cudaGetDeviceProperties(&prop, device));
-    require(prop.major == 10, FMMB_ERR_UNSUPPORTED, "this build targets sm_100a (B200)");
+    require(prop.major == 10, FMMB_ERR_UNSUPPORTED, "the library targets sm_100a (B200)");
     h->c.num_sms = prop.multiProcessorCount;
     // the highest priority: the split matvec's near field (on a lowest-priority side stream)
     // fills what the passes leave of the SMs

@@ -1,5 +1,5 @@
-// The autotuner of the launch shapes (north_star's batching form asks for tile shapes chosen by
-// a project-written autotuner; the reference has none).
+// The autotuner of the launch shapes: tile and block shapes chosen by timing them on the
+// caller's own inputs (the reference has no tuner).
 //
 // Three shapes are free, in that no result depends on them (each target's sums are taken in the
 // list's order whatever the blocking, and a near-field warp owns its leaf group):

@@ -30,7 +30,7 @@ extern "C" {
 #define FMMB_ERR_MEMORY 3      /* device or host allocation failed */
 #define FMMB_ERR_DEVICE 4      /* a CUDA error */
 #define FMMB_ERR_TIMEOUT 5     /* a bounded device wait gave up */
-#define FMMB_ERR_UNSUPPORTED 6 /* a method, kernel, density or output this build does not provide */
+#define FMMB_ERR_UNSUPPORTED 6 /* a method, kernel, density or output the library does not provide */
 
 #define FMMB_KERNEL_LAPLACE3D 1
 #define FMMB_KERNEL_YUKAWA3D 2    /* e^{−κr}/(4πr), SphericalHarmonics(Yukawa3D(κ); p): FP64 path, operators per width */
@@ -63,7 +63,7 @@ typedef struct {
   int32_t kernel;  /* FMMB_KERNEL_* (the cube KI method: FMMB_KERNEL_LAPLACE3D) */
   int32_t p;       /* harmonics: expansion degree, 1..20; cube KI: points per edge, 2..12; circle KI: nequiv, 4..64 */
   int32_t reserved;
-  double tol;      /* 0: dense class operators (the only form this build provides) */
+  double tol;      /* 0: dense class operators (the only form the library provides) */
   double kappa;    /* the Yukawa screening κ > 0 (FMMB_KERNEL_YUKAWA3D); ignored otherwise */
   int32_t pc;      /* cube KI: points per edge of the large surface; 0: 2p */
   int32_t reserved2;
