@@ -203,6 +203,42 @@ def kernel_matrix3(sources, targets):
     return C3 / np.sqrt(np.einsum("tsk,tsk->ts", d, d))
 
 
+def cube_boundary_lattice(p):
+    """The lattice indices (i1, i2, i3) in [0, p)³ of the boundary points, in the order of
+    cube_boundary_points (coordinate 1 fastest): the embedding of the spectral translation
+    (src/operators/spectral_m2l.jl:103-115)."""
+    out = []
+    for k in range(p):
+        for j in range(p):
+            for i in range(p):
+                if i in (0, p - 1) or j in (0, p - 1) or k in (0, p - 1):
+                    out.append((i, j, k))
+    return np.array(out)
+
+
+def spectral_m2l(p, a, off, w, sigma):
+    """The spectral M2L of one far pair (src/operators/spectral_m2l.jl: `_kernel_tables` :117-135
+    and the single-vector `apply!` :144-173), FP64 with numpy's FFT: the source box's density σ on
+    its p-per-edge boundary lattice of half-width a (spacing h = 2a/(p − 1)) embedded in the
+    zero-padded (2p)³ lattice, transformed, multiplied by the transform of the circulant kernel
+    table κ(m) = G(h·m − off·w), m ∈ [−(p − 1), p − 1]³ at the wrapped index m mod 2p, transformed
+    back, and read at the target box's boundary lattice points: the check potentials
+    Σ_j G(y_i − x_j) σ_j with y on the target's surface and x = y' + off·w on the source's."""
+    n = 2 * p
+    h = 2.0 * a / (p - 1)
+    m = np.arange(-(p - 1), p)
+    M1, M2, M3 = np.meshgrid(m, m, m, indexing="ij")
+    o = np.asarray(off, float) * w
+    r = np.sqrt((h * M1 - o[0]) ** 2 + (h * M2 - o[1]) ** 2 + (h * M3 - o[2]) ** 2)
+    tab = np.zeros((n, n, n))
+    tab[M1 % n, M2 % n, M3 % n] = C3 / r
+    lat = cube_boundary_lattice(p)
+    sg = np.zeros((n, n, n))
+    sg[lat[:, 0], lat[:, 1], lat[:, 2]] = sigma
+    u = np.fft.ifftn(np.fft.fftn(tab) * np.fft.fftn(sg)).real
+    return u[lat[:, 0], lat[:, 1], lat[:, 2]]
+
+
 class CubeLevel:
     """level_operators(m::CubeKernelIndependent{3}, w) (src/operators/cubeki.jl:55-79) with
     _ki_dense_operators (src/operators/ki_common.jl:185-207), the M2L dense."""
